@@ -1,0 +1,159 @@
+/*
+ * bem_b200 -- C ABI of the B200 Galerkin BEM engine (libbem_b200.so).
+ *
+ * The reference (GeCao/taichi-BEM) is Python + Taichi; its hot path is the
+ * dense assembly of the boundary integral operators and the dense solve.
+ * Each entry point below replaces one reference interface (cited per
+ * function).  Conventions:
+ *   - all array arguments are DEVICE pointers owned by the caller, except
+ *     where a comment says "host";
+ *   - calls are stream-ordered on the given stream, do not synchronise the
+ *     device, and return BEM_OK (0) or a negative BEM_ERR_* code; the message
+ *     of the last failure is bem_last_error(ctx);
+ *   - complex values are interleaved (re, im) doubles, as torch.complex128
+ *     and the reference's ti.Vector(2) [re, im];
+ *   - matrices are row-major with a leading dimension `ld` (elements);
+ *   - a context is used by one host thread at a time.
+ */
+#ifndef BEM_B200_H
+#define BEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define BEM_OK 0
+#define BEM_ERR_INVALID (-1)     /* bad argument (sizes, enums, null pointers) */
+#define BEM_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define BEM_ERR_NOMESH (-3)      /* no mesh set on the context */
+#define BEM_ERR_NOCONVERGE (-4)  /* iterative refinement did not reach tol */
+#define BEM_ERR_SINGULAR (-5)    /* zero pivot in the LU factorisation */
+#define BEM_ERR_TIMEOUT (-6)     /* a device-side wait hit its iteration cap */
+#define BEM_ERR_MESH (-7)        /* degenerate or non-finite mesh */
+
+/* ---- enums (values follow src/BEM_functions/utils/types.py) -------------- */
+#define BEM_OP_V 0   /* single layer      (single_layer_3d.py)          */
+#define BEM_OP_K 1   /* double layer      (double_layer_3d.py)          */
+#define BEM_OP_KP 2  /* adjoint double    (adj_double_layer_3d.py)      */
+#define BEM_OP_W 3   /* hypersingular     (hypersingular_layer_3d.py)   */
+
+#define BEM_KERNEL_LAPLACE 0
+#define BEM_KERNEL_HELMHOLTZ 1
+
+#define BEM_PREC_FP64 0   /* every quadrature point in FP64 (the plain path)           */
+#define BEM_PREC_MIXED 1  /* separate pairs in FP32, coincident/edge/vertex pairs in FP64 */
+
+#define BEM_F64 0   /* real double     */
+#define BEM_C128 1  /* complex double  */
+#define BEM_F32 2   /* real float      */
+#define BEM_C64 3   /* complex float   */
+
+typedef struct bem_ctx bem_ctx;
+
+/* One operator evaluation (the arguments of the reference's
+   `forward(scope_type, k, sqrt_n)`, single_layer_3d.py:371-372). */
+typedef struct {
+    int op;          /* BEM_OP_*                                                 */
+    int kernel;      /* BEM_KERNEL_*                                             */
+    double k;        /* kernel wavenumber: k, or k*sqrt_n for the transmission kernel */
+    double k2;       /* coefficient of the W mass term, (k*sqrt_n)^2 (0 for Laplace) */
+    int quirk;       /* 1: the reference's Sauter-Schwab orientation/basis handling;
+                        0: shared vertex/edge moved to the map's singular point   */
+    int precision;   /* BEM_PREC_*                                               */
+} bem_op_desc;
+
+/* One side (test or trial) of an operator block: the reference's local panel
+   loop (`for local_I in range(num_of_panels_X)` + map_local_X_index_to_panel_index)
+   with the charge index of each basis function
+   (proj_from_local_panel_index_to_local_charge_index, BEM_manager.py:244-277). */
+typedef struct {
+    int n_panels;            /* panels on this side                                 */
+    const int32_t* panels;   /* device [n_panels]: global panel index               */
+    int nb;                  /* 1 = P0 (constant), 3 = P1 (hat at each vertex)      */
+    const int32_t* dof;      /* device [n_panels*nb]: row/column index, <0 = skipped */
+} bem_space;
+
+/* ---- context ------------------------------------------------------------- */
+/* No reference counterpart (the reference keeps its state in Taichi fields). */
+int bem_ctx_create(bem_ctx** out_ctx);
+int bem_ctx_destroy(bem_ctx* ctx);
+const char* bem_last_error(const bem_ctx* ctx);
+/* Number of kernels this library launched through ctx since creation. */
+int64_t bem_launch_count(const bem_ctx* ctx);
+
+/* ---- mesh ------------------------------------------------------------------
+ * Replaces MeshManager.initialization geometry (mesh_manager.py:84-139) and the
+ * per-pair get_panels_relation (mesh_manager.py:538-573): uploads the mesh,
+ * computes areas/normals/curls and the separate-pair quadrature points for
+ * gauss_qr on the device, and builds the coincident/edge/vertex pair list.
+ * verts (host) [nv*3] double, tris (host) [nt*3] int32.  Synchronous. */
+int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv, int nt, int gauss_qr);
+/* Number of coincident + edge + vertex pairs of the current mesh (ordered). */
+int64_t bem_near_pair_count(const bem_ctx* ctx);
+/* Copies the per-panel areas [nt] and unit normals [nt*3] (device pointers). */
+int bem_mesh_geometry(const bem_ctx* ctx, double* areas, double* normals, void* stream);
+
+/* ---- assembly ---------------------------------------------------------------
+ * Dense block: out[row*ld+col] += scale*A(row,col) for every (test basis,
+ * trial basis) pair with both dof >= 0; when out_t != NULL also
+ * out_t[col*ld+row] += scale_t*A(row,col).  Replaces the operator forward
+ * passes SingleLayer3d.forward (single_layer_3d.py:371-433),
+ * DoubleLayer3d.forward (double_layer_3d.py:376-438),
+ * HypersingularLayer3d.forward (hypersingular_layer_3d.py:437-500) and the
+ * block scatter BEMManager.matA_add_M (BEM_manager.py:608-628, out_t = the
+ * -K^T block).  out_dtype: BEM_F64 (Laplace) or BEM_C128 (Helmholtz). */
+int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                 int out_dtype, void* out, int64_t ld, double scale, void* out_t, double scale_t,
+                 void* stream);
+
+/* Matrix-free apply: y[row] += scale * sum_col A(row,col) * x[col]
+ * (x conjugated when conj_x != 0, the reference's cmul(integrand, cconj(g))).
+ * Replaces apply_V_dot_N_boundary (single_layer_3d.py:435-498),
+ * apply_K_dot_D_boundary (double_layer_3d.py:440-501),
+ * apply_K_dot_N_boundary (adj_double_layer_3d.py:444-506) and
+ * apply_W_dot_D_boundary (hypersingular_layer_3d.py:502-565).
+ * dtype: BEM_F64 or BEM_C128 for both x and y. */
+int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+              int dtype, const void* x, void* y, double scale, int conj_x, void* stream);
+
+/* Identity (mass) block on one panel list (test and trial share `panels`):
+ * dense (out/out_t) or apply (x != NULL: y += scale*M*x).  Replaces
+ * IdentityLayer3d.matA_add_global_Identity_matrix (identity_layer_3d.py:148-196)
+ * and RHSConstructor3d.multiply_identity_to_vector (rhs_constructor_3d.py:256-359). */
+int bem_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int dtype,
+             void* out, int64_t ld, double scale, void* out_t, double scale_t,
+             const void* x, void* y, int conj_x, void* stream);
+
+/* ---- dense linear algebra (replaces torch.linalg.solve, BEM_manager.py:1056) --
+ * LU with partial pivoting in place (row-major, n x n, lda).  dtype
+ * BEM_F64/BEM_C128 (plain FP64 path) or BEM_F32/BEM_C64 (low-precision factor
+ * of the mixed path; trailing updates on the tensor cores).  piv: device
+ * int32[n] (LAPACK-style: row i was swapped with piv[i]).  info: device int32,
+ * set to 0 or to 1+index of the first zero pivot. */
+int bem_lu_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, int32_t* info,
+                  void* stream);
+/* Solve with the factors: b (n x nrhs, row-major, ldb) overwritten by x. */
+int bem_lu_solve(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
+                 void* b, int64_t nrhs, int64_t ldb, void* stream);
+/* y = alpha*A*x + beta*y for one vector (dtype of A: F64/C128/F32/C64; x, y in
+ * the matching FP64 type F64/C128).  Used for the refinement residual. */
+int bem_gemv(bem_ctx* ctx, int a_dtype, const void* A, int64_t m, int64_t n, int64_t lda,
+             const void* x, void* y, double alpha, double beta, void* stream);
+
+/* Mixed-precision solve: x = A_hi^{-1} b to relative residual tol by FP64
+ * iterative refinement on the residual b - A_hi x, each correction solved with
+ * the low-precision factors (LU_lo, piv) of A_hi.  A_hi: F64/C128, LU_lo:
+ * F32/C64.  iters/relres: host pointers (may be NULL).  Returns
+ * BEM_ERR_NOCONVERGE if maxit is reached. */
+int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv,
+                     int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit,
+                     int* iters, double* relres, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEM_B200_H */

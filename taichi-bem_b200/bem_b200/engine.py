@@ -1,0 +1,215 @@
+"""Device engine: one libbem_b200 context, a mesh on the GPU, and typed calls.
+
+All tensors passed in are CUDA tensors; every call is issued on the current
+torch CUDA stream.  Nothing here computes on the CPU: the engine raises when
+the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _stream_ptr():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _dtype_code(t: torch.Tensor) -> int:
+    return {torch.float64: L.F64, torch.complex128: L.C128, torch.float32: L.F32,
+            torch.complex64: L.C64}[t.dtype]
+
+
+@dataclass
+class DeviceSpace:
+    """One side of an operator block: global panel ids and a dof table
+    [n_panels, nb] (-1 = skipped), both int32 on the device.  ``max_panel``
+    and ``max_dof`` are checked against the mesh and the output extents
+    before every launch (an out-of-range index is rejected on the host)."""
+    panels: torch.Tensor
+    nb: int
+    dof: torch.Tensor
+    max_panel: int = -1
+    max_dof: int = -1
+
+    @staticmethod
+    def from_numpy(panels, nb, dof, device):
+        pn = np.ascontiguousarray(panels, dtype=np.int32).reshape(-1)
+        dn = np.ascontiguousarray(dof, dtype=np.int32).reshape(-1)
+        if dn.size != pn.size * nb:
+            raise ValueError("dof table must have n_panels * nb entries")
+        if pn.size and pn.min() < 0:
+            raise ValueError("negative panel index")
+        if pn.size != np.unique(pn).size:
+            raise ValueError("a panel may appear only once per space")
+        p = torch.as_tensor(pn, device=device)
+        d = torch.as_tensor(dn, device=device)
+        return DeviceSpace(p, int(nb), d, int(pn.max()) if pn.size else -1, int(dn.max()) if dn.size else -1)
+
+    def shifted(self, offset: int):
+        """Same space with every valid dof moved by `offset` (block placement)."""
+        d = torch.where(self.dof >= 0, self.dof + int(offset), self.dof)
+        return DeviceSpace(self.panels, self.nb, d, self.max_panel, self.max_dof + int(offset) if self.max_dof >= 0
+                           else -1)
+
+    def c(self):
+        return L.Space(int(self.panels.numel()), self.panels.data_ptr() if self.panels.numel() else None, self.nb,
+                       self.dof.data_ptr() if self.dof.numel() else None)
+
+    @property
+    def n_panels(self):
+        return int(self.panels.numel())
+
+
+class Engine:
+    """Owns one bem_ctx.  ``set_mesh`` uploads a mesh and builds the device
+    geometry and the near-pair list; ``assemble``/``apply``/``mass`` evaluate
+    operator blocks; ``lu_factor``/``lu_solve``/``refine_solve`` solve."""
+
+    def __init__(self, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("bem_b200 needs a CUDA device (no CPU fallback)")
+        self.device = torch.device(device if device is not None else "cuda")
+        self.lib = L.load()
+        with torch.cuda.device(self.device):
+            h = ctypes.c_void_p()
+            rc = self.lib.bem_ctx_create(ctypes.byref(h))
+            if rc != 0:
+                raise L.BemError(rc, "bem_ctx_create failed")
+        self.ctx = h
+        self.nt = self.nv = 0
+        self.Q = 0
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.bem_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise L.BemError(rc, self.lib.bem_last_error(self.ctx).decode())
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.bem_launch_count(self.ctx))
+
+    # -- mesh ---------------------------------------------------------------
+    def set_mesh(self, vertices, panels, gauss_qr: int):
+        v = np.ascontiguousarray(np.asarray(vertices, dtype=np.float64).reshape(-1, 3))
+        f = np.ascontiguousarray(np.asarray(panels, dtype=np.int32).reshape(-1, 3))
+        with torch.cuda.device(self.device):
+            self._check(self.lib.bem_mesh_set(self.ctx, v.ctypes.data, f.ctypes.data, len(v), len(f), int(gauss_qr)))
+        self.nv, self.nt, self.Q = len(v), len(f), int(gauss_qr)
+        self.vertices_host, self.panels_host = v, f
+
+    @property
+    def near_pairs(self) -> int:
+        return int(self.lib.bem_near_pair_count(self.ctx))
+
+    def geometry(self):
+        areas = torch.empty(self.nt, dtype=torch.float64, device=self.device)
+        normals = torch.empty(self.nt, 3, dtype=torch.float64, device=self.device)
+        self._check(self.lib.bem_mesh_geometry(self.ctx, _ptr(areas), _ptr(normals), _stream_ptr()))
+        return areas, normals
+
+    # -- operators ------------------------------------------------------------
+    @staticmethod
+    def op_desc(op, helmholtz, k=0.0, k2=0.0, quirk=True, precision=L.PREC_FP64):
+        return L.OpDesc(int(op), L.KERNEL_HELMHOLTZ if helmholtz else L.KERNEL_LAPLACE, float(k), float(k2),
+                        1 if quirk else 0, int(precision))
+
+    def _check_spaces(self, test, trial, nrow, ncol):
+        for sp in (test, trial):
+            if sp.max_panel >= self.nt:
+                raise ValueError(f"panel index {sp.max_panel} out of range for a mesh of {self.nt} panels")
+        if test.max_dof >= nrow or trial.max_dof >= ncol:
+            raise ValueError(f"dof out of range: rows {test.max_dof} >= {nrow} or cols {trial.max_dof} >= {ncol}")
+
+    def assemble(self, desc: L.OpDesc, test: DeviceSpace, trial: DeviceSpace, out: torch.Tensor, scale=1.0,
+                 out_t: torch.Tensor | None = None, scale_t=0.0):
+        """out[row, col] += scale * A(row, col) (and out_t[col, row] += scale_t * A)."""
+        assert out.is_cuda and out.dim() == 2 and out.stride(1) == 1
+        self._check_spaces(test, trial, out.shape[0], out.shape[1])
+        if out_t is not None:
+            assert out_t.dtype == out.dtype and out_t.stride(0) == out.stride(0)
+            self._check_spaces(trial, test, out_t.shape[0], out_t.shape[1])
+        ts, rs = test.c(), trial.c()
+        self._check(self.lib.bem_assemble(self.ctx, ctypes.byref(desc), ctypes.byref(ts), ctypes.byref(rs),
+                                          _dtype_code(out), _ptr(out), out.stride(0), float(scale), _ptr(out_t),
+                                          float(scale_t), _stream_ptr()))
+
+    def apply(self, desc: L.OpDesc, test: DeviceSpace, trial: DeviceSpace, x: torch.Tensor, y: torch.Tensor,
+              scale=1.0, conj_x=False):
+        """y[row] += scale * sum_col A(row, col) x[col] (x conjugated if conj_x)."""
+        assert x.dtype == y.dtype and x.is_contiguous() and y.is_contiguous()
+        self._check_spaces(test, trial, y.numel(), x.numel())
+        ts, rs = test.c(), trial.c()
+        self._check(self.lib.bem_apply(self.ctx, ctypes.byref(desc), ctypes.byref(ts), ctypes.byref(rs),
+                                       _dtype_code(y), _ptr(x), _ptr(y), float(scale), int(bool(conj_x)),
+                                       _stream_ptr()))
+
+    def mass(self, test: DeviceSpace, trial: DeviceSpace, out=None, scale=1.0, out_t=None, scale_t=0.0, x=None,
+             y=None, conj_x=False):
+        ts, rs = test.c(), trial.c()
+        if x is not None:
+            self._check_spaces(test, trial, y.numel(), x.numel())
+            self._check(self.lib.bem_mass(self.ctx, ctypes.byref(ts), ctypes.byref(rs), _dtype_code(y), None, 0,
+                                          float(scale), None, 0.0, _ptr(x), _ptr(y), int(bool(conj_x)),
+                                          _stream_ptr()))
+        else:
+            self._check_spaces(test, trial, out.shape[0], out.shape[1])
+            if out_t is not None:
+                self._check_spaces(trial, test, out_t.shape[0], out_t.shape[1])
+            self._check(self.lib.bem_mass(self.ctx, ctypes.byref(ts), ctypes.byref(rs), _dtype_code(out), _ptr(out),
+                                          out.stride(0), float(scale), _ptr(out_t), float(scale_t), None, None, 0,
+                                          _stream_ptr()))
+
+    # -- dense solve ---------------------------------------------------------------
+    def lu_factor(self, A: torch.Tensor):
+        """In-place LU with partial pivoting; returns (piv, info) device int32."""
+        n = A.shape[0]
+        assert A.is_cuda and A.shape[0] == A.shape[1] and A.stride(1) == 1
+        piv = torch.empty(n, dtype=torch.int32, device=A.device)
+        info = torch.zeros(1, dtype=torch.int32, device=A.device)
+        self._check(self.lib.bem_lu_factor(self.ctx, _dtype_code(A), _ptr(A), n, A.stride(0), _ptr(piv), _ptr(info),
+                                           _stream_ptr()))
+        return piv, info
+
+    def lu_solve(self, LU: torch.Tensor, piv: torch.Tensor, b: torch.Tensor):
+        """b (n or n x nrhs, FP64 real/complex) overwritten by the solution."""
+        n = LU.shape[0]
+        b2 = b.view(n, -1)
+        assert b2.is_contiguous()
+        self._check(self.lib.bem_lu_solve(self.ctx, _dtype_code(LU), _ptr(LU), n, LU.stride(0), _ptr(piv), _ptr(b2),
+                                          b2.shape[1], b2.shape[1], _stream_ptr()))
+        return b
+
+    def gemv(self, A, x, y, alpha=1.0, beta=0.0):
+        m, n = A.shape
+        self._check(self.lib.bem_gemv(self.ctx, _dtype_code(A), _ptr(A), m, n, A.stride(0), _ptr(x), _ptr(y),
+                                      float(alpha), float(beta), _stream_ptr()))
+        return y
+
+    def refine_solve(self, A_hi, LU_lo, piv, b, x, tol=1e-12, maxit=50):
+        it = ctypes.c_int(0)
+        rr = ctypes.c_double(0.0)
+        n = A_hi.shape[0]
+        rc = self.lib.bem_refine_solve(self.ctx, _dtype_code(A_hi), _ptr(A_hi), _ptr(LU_lo), _ptr(piv), n,
+                                       A_hi.stride(0), _ptr(b), _ptr(x), float(tol), int(maxit), ctypes.byref(it),
+                                       ctypes.byref(rr), _stream_ptr())
+        self._check(rc)
+        return it.value, rr.value

@@ -1,0 +1,322 @@
+// C ABI entry points: context, mesh upload + near-pair list, assembly dispatch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "bem_internal.cuh"
+
+int bem_fail(bem_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int bem_check_cuda(bem_ctx* ctx, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return BEM_OK;
+    return bem_fail(ctx, BEM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int bem_ws_reserve(bem_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->ws_bytes) return BEM_OK;
+    if (ctx->ws) cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+    if (int rc = bem_check_cuda(ctx, cudaMalloc(&ctx->ws, bytes), "cudaMalloc(workspace)")) return rc;
+    ctx->ws_bytes = bytes;
+    return BEM_OK;
+}
+
+namespace {
+
+// Gauss-Legendre rule on [0,1] (the reference's tables in
+// src/BEM_functions/utils/functions.py:5-85 are this rule to 16 digits),
+// computed by Newton iteration on the three-term Legendre recurrence.
+void gauss01(int n, double* p, double* w) {
+    if (n == 1) {
+        p[0] = 0.5;
+        w[0] = 1.0;
+        return;
+    }
+    for (int i = 0; i < n; ++i) {
+        double x = std::cos(BEM_PI * (i + 0.75) / (n + 0.5));
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = x;
+            for (int k = 2; k <= n; ++k) {
+                double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            double dp = n * (x * p1 - p0) / (x * x - 1.0);
+            double dx = p1 / dp;
+            x -= dx;
+            if (std::fabs(dx) < 1e-16) break;
+        }
+        double p0 = 1.0, p1 = x;
+        for (int k = 2; k <= n; ++k) {
+            double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+            p0 = p1;
+            p1 = p2;
+        }
+        double dp = n * (x * p1 - p0) / (x * x - 1.0);
+        p[n - 1 - i] = (x + 1.0) / 2.0;
+        w[n - 1 - i] = 1.0 / ((1.0 - x * x) * dp * dp);
+    }
+}
+
+// Corrected-mode parameter orders of a near pair (packed 2 bits per slot):
+// shared vertex at slot 0 of both panels, or shared edge at slots (0,1) of
+// both panels with matching endpoints.
+int near_perm(const int32_t* a, const int32_t* b, int rel) {
+    int px[3] = {0, 1, 2}, py[3] = {0, 1, 2};
+    if (rel == REL_VERTEX) {
+        bool done = false;
+        for (int s = 0; s < 3 && !done; ++s)
+            for (int t = 0; t < 3 && !done; ++t)
+                if (a[s] == b[t]) {
+                    px[0] = s; px[1] = (s + 1) % 3; px[2] = (s + 2) % 3;
+                    py[0] = t; py[1] = (t + 1) % 3; py[2] = (t + 2) % 3;
+                    done = true;
+                }
+    } else if (rel == REL_EDGE) {
+        for (int s = 0; s < 3; ++s) {
+            int v0 = a[s], v1 = a[(s + 1) % 3], t0 = -1, t1 = -1;
+            for (int t = 0; t < 3; ++t) {
+                if (b[t] == v0) t0 = t;
+                if (b[t] == v1) t1 = t;
+            }
+            if (t0 >= 0 && t1 >= 0) {
+                px[0] = s; px[1] = (s + 1) % 3; px[2] = (s + 2) % 3;
+                py[0] = t0; py[1] = t1; py[2] = 3 - t0 - t1;
+                break;
+            }
+        }
+    }
+    int bx = px[0] | (px[1] << 2) | (px[2] << 4);
+    int by = py[0] | (py[1] << 2) | (py[2] << 4);
+    return bx | (by << 6);
+}
+
+void free_mesh(bem_ctx* ctx) {
+    void* ptrs[] = {ctx->verts, ctx->tris, ctx->area, ctx->normal, ctx->centroid, ctx->curl, ctx->pts64,
+                    ctx->pts32, ctx->phi64, ctx->phi32, ctx->gp, ctx->gw, ctx->near, ctx->test_local,
+                    ctx->trial_local};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    ctx->verts = nullptr; ctx->tris = nullptr; ctx->area = nullptr; ctx->normal = nullptr;
+    ctx->centroid = nullptr; ctx->curl = nullptr; ctx->pts64 = nullptr; ctx->pts32 = nullptr;
+    ctx->phi64 = nullptr; ctx->phi32 = nullptr; ctx->gp = nullptr; ctx->gw = nullptr; ctx->near = nullptr;
+    ctx->test_local = nullptr; ctx->trial_local = nullptr;
+    ctx->nv = ctx->nt = ctx->Q = ctx->Q2 = 0;
+    ctx->n_near = 0;
+}
+
+template <typename T>
+int dmalloc(bem_ctx* ctx, T** p, size_t n) {
+    return bem_check_cuda(ctx, cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(n, 1)), "cudaMalloc(mesh)");
+}
+
+int check_space(bem_ctx* ctx, const bem_space* sp, const char* name) {
+    if (!sp) return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " space is NULL");
+    if (sp->n_panels < 0 || (sp->n_panels > 0 && (!sp->panels || !sp->dof)))
+        return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " space has no panel/dof arrays");
+    if (sp->nb != 1 && sp->nb != 3) return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " nb must be 1 or 3");
+    if (sp->n_panels > ctx->nt) return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " has more panels than the mesh");
+    return BEM_OK;
+}
+
+int check_op(bem_ctx* ctx, const bem_op_desc* op) {
+    if (!op) return bem_fail(ctx, BEM_ERR_INVALID, "op is NULL");
+    if (op->op < BEM_OP_V || op->op > BEM_OP_W) return bem_fail(ctx, BEM_ERR_INVALID, "unknown operator");
+    if (op->kernel != BEM_KERNEL_LAPLACE && op->kernel != BEM_KERNEL_HELMHOLTZ)
+        return bem_fail(ctx, BEM_ERR_INVALID, "unknown kernel");
+    if (op->precision != BEM_PREC_FP64 && op->precision != BEM_PREC_MIXED)
+        return bem_fail(ctx, BEM_ERR_INVALID, "unknown precision");
+    if (!std::isfinite(op->k) || !std::isfinite(op->k2)) return bem_fail(ctx, BEM_ERR_INVALID, "non-finite wavenumber");
+    return BEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bem_ctx_create(bem_ctx** out_ctx) {
+    if (!out_ctx) return BEM_ERR_INVALID;
+    *out_ctx = nullptr;
+    bem_ctx* ctx = new (std::nothrow) bem_ctx();
+    if (!ctx) return BEM_ERR_INVALID;
+    if (cudaGetDevice(&ctx->device) != cudaSuccess) {
+        delete ctx;
+        return BEM_ERR_CUDA;
+    }
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (cudaMalloc((void**)&ctx->flags, 16 * sizeof(int32_t)) != cudaSuccess) {
+        delete ctx;
+        return BEM_ERR_CUDA;
+    }
+    cudaMemset(ctx->flags, 0, 16 * sizeof(int32_t));
+    *out_ctx = ctx;
+    return BEM_OK;
+}
+
+int bem_ctx_destroy(bem_ctx* ctx) {
+    if (!ctx) return BEM_OK;
+    free_mesh(ctx);
+    if (ctx->ws) cudaFree(ctx->ws);
+    if (ctx->flags) cudaFree(ctx->flags);
+    delete ctx;
+    return BEM_OK;
+}
+
+const char* bem_last_error(const bem_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int64_t bem_launch_count(const bem_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int64_t bem_near_pair_count(const bem_ctx* ctx) { return ctx ? ctx->n_near : 0; }
+
+int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv, int nt, int gauss_qr) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!verts || !tris || nv <= 0 || nt <= 0) return bem_fail(ctx, BEM_ERR_INVALID, "empty mesh");
+    if (gauss_qr < 1 || gauss_qr > BEM_MAX_Q) return bem_fail(ctx, BEM_ERR_INVALID, "GaussQR must be in 1..12");
+    for (int64_t i = 0; i < 3LL * nv; ++i)
+        if (!std::isfinite(verts[i])) return bem_fail(ctx, BEM_ERR_MESH, "non-finite vertex coordinate");
+    for (int64_t i = 0; i < 3LL * nt; ++i)
+        if (tris[i] < 0 || tris[i] >= nv) return bem_fail(ctx, BEM_ERR_MESH, "panel vertex index out of range");
+
+    // near-pair list: every ordered pair sharing at least one vertex index
+    std::vector<std::vector<int>> vp(nv);
+    for (int p = 0; p < nt; ++p)
+        for (int c = 0; c < 3; ++c) vp[tris[3 * p + c]].push_back(p);
+    std::vector<int4> near;
+    near.reserve((size_t)nt * 14);
+    std::vector<int> cand;
+    for (int i = 0; i < nt; ++i) {
+        cand.clear();
+        for (int c = 0; c < 3; ++c)
+            for (int j : vp[tris[3 * i + c]]) cand.push_back(j);
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        for (int j : cand) {
+            int rel = bem_relation(tris + 3 * i, tris + 3 * j, i == j);
+            if (rel == REL_SEPARATE) continue;
+            near.push_back(make_int4(i, j, rel, near_perm(tris + 3 * i, tris + 3 * j, rel)));
+        }
+    }
+
+    free_mesh(ctx);
+    const int Q = gauss_qr, Q2 = Q * Q;
+    std::vector<double> gp(Q), gw(Q);
+    gauss01(Q, gp.data(), gw.data());
+    std::vector<double> phi64((size_t)Q2 * 3);
+    std::vector<float> phi32((size_t)Q2 * 3);
+    for (int ix = 0; ix < Q; ++ix)
+        for (int iy = 0; iy < Q; ++iy) {
+            double r1 = gp[ix], r2 = gp[iy] * r1;
+            double v[3] = {1.0 - r1, r1 - r2, r2};
+            for (int b = 0; b < 3; ++b) {
+                phi64[(ix * Q + iy) * 3 + b] = v[b];
+                phi32[(ix * Q + iy) * 3 + b] = (float)v[b];
+            }
+        }
+    int rc = 0;
+    if ((rc = dmalloc(ctx, &ctx->verts, 3 * (size_t)nv)) || (rc = dmalloc(ctx, &ctx->tris, 3 * (size_t)nt)) ||
+        (rc = dmalloc(ctx, &ctx->area, nt)) || (rc = dmalloc(ctx, &ctx->normal, 3 * (size_t)nt)) ||
+        (rc = dmalloc(ctx, &ctx->centroid, 3 * (size_t)nt)) || (rc = dmalloc(ctx, &ctx->curl, 9 * (size_t)nt)) ||
+        (rc = dmalloc(ctx, &ctx->pts64, (size_t)nt * Q2)) || (rc = dmalloc(ctx, &ctx->pts32, (size_t)nt * Q2)) ||
+        (rc = dmalloc(ctx, &ctx->phi64, (size_t)Q2 * 3)) || (rc = dmalloc(ctx, &ctx->phi32, (size_t)Q2 * 3)) ||
+        (rc = dmalloc(ctx, &ctx->gp, Q)) || (rc = dmalloc(ctx, &ctx->gw, Q)) ||
+        (rc = dmalloc(ctx, &ctx->near, near.size())) || (rc = dmalloc(ctx, &ctx->test_local, nt)) ||
+        (rc = dmalloc(ctx, &ctx->trial_local, nt))) {
+        free_mesh(ctx);
+        return rc;
+    }
+    ctx->nv = nv;
+    ctx->nt = nt;
+    ctx->Q = Q;
+    ctx->Q2 = Q2;
+    ctx->n_near = (int64_t)near.size();
+    cudaMemcpy(ctx->verts, verts, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->tris, tris, sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->gp, gp.data(), sizeof(double) * Q, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->gw, gw.data(), sizeof(double) * Q, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->phi64, phi64.data(), sizeof(double) * Q2 * 3, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->phi32, phi32.data(), sizeof(float) * Q2 * 3, cudaMemcpyHostToDevice);
+    if (!near.empty()) cudaMemcpy(ctx->near, near.data(), sizeof(int4) * near.size(), cudaMemcpyHostToDevice);
+    cudaMemset(ctx->flags, 0, 16 * sizeof(int32_t));
+    if ((rc = bem_launch_geometry(ctx, 0))) return rc;
+    if ((rc = bem_check_cuda(ctx, cudaDeviceSynchronize(), "mesh geometry"))) return rc;
+    int32_t flags[16];
+    cudaMemcpy(flags, ctx->flags, sizeof(flags), cudaMemcpyDeviceToHost);
+    if (flags[0] != 0) {
+        int bad = flags[0] - 1;
+        free_mesh(ctx);
+        return bem_fail(ctx, BEM_ERR_MESH, "degenerate panel " + std::to_string(bad) + " (zero or non-finite area)");
+    }
+    return BEM_OK;
+}
+
+int bem_mesh_geometry(const bem_ctx* cctx, double* areas, double* normals, void* stream) {
+    bem_ctx* ctx = const_cast<bem_ctx*>(cctx);
+    if (!ctx) return BEM_ERR_INVALID;
+    if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (areas)
+        if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(areas, ctx->area, sizeof(double) * ctx->nt,
+                                                          cudaMemcpyDeviceToDevice, s), "copy areas"))
+            return rc;
+    if (normals)
+        if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(normals, ctx->normal, sizeof(double) * 3 * ctx->nt,
+                                                          cudaMemcpyDeviceToDevice, s), "copy normals"))
+            return rc;
+    return BEM_OK;
+}
+
+int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial, int out_dtype,
+                 void* out, int64_t ld, double scale, void* out_t, double scale_t, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
+    if (int rc = check_op(ctx, op)) return rc;
+    if (int rc = check_space(ctx, test, "test")) return rc;
+    if (int rc = check_space(ctx, trial, "trial")) return rc;
+    int want = op->kernel == BEM_KERNEL_HELMHOLTZ ? BEM_C128 : BEM_F64;
+    if (out_dtype != want)
+        return bem_fail(ctx, BEM_ERR_INVALID, "out dtype must be BEM_F64 for Laplace and BEM_C128 for Helmholtz");
+    if (!out || ld <= 0) return bem_fail(ctx, BEM_ERR_INVALID, "out is NULL or ld <= 0");
+    return bem_launch_assemble(ctx, op, test, trial, 0, out, ld, scale, out_t, scale_t, nullptr, nullptr, 0,
+                               (cudaStream_t)stream);
+}
+
+int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial, int dtype,
+              const void* x, void* y, double scale, int conj_x, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
+    if (int rc = check_op(ctx, op)) return rc;
+    if (int rc = check_space(ctx, test, "test")) return rc;
+    if (int rc = check_space(ctx, trial, "trial")) return rc;
+    int want = op->kernel == BEM_KERNEL_HELMHOLTZ ? BEM_C128 : BEM_F64;
+    if (dtype != want)
+        return bem_fail(ctx, BEM_ERR_INVALID, "x/y dtype must be BEM_F64 for Laplace and BEM_C128 for Helmholtz");
+    if (!x || !y) return bem_fail(ctx, BEM_ERR_INVALID, "x or y is NULL");
+    return bem_launch_assemble(ctx, op, test, trial, 1, nullptr, 0, scale, nullptr, 0.0, x, y, conj_x,
+                               (cudaStream_t)stream);
+}
+
+int bem_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int dtype, void* out, int64_t ld,
+             double scale, void* out_t, double scale_t, const void* x, void* y, int conj_x, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
+    if (int rc = check_space(ctx, test, "test")) return rc;
+    if (int rc = check_space(ctx, trial, "trial")) return rc;
+    if (test->n_panels != trial->n_panels || test->panels != trial->panels)
+        return bem_fail(ctx, BEM_ERR_INVALID, "mass: test and trial must share the panel list");
+    if (dtype != BEM_F64 && dtype != BEM_C128) return bem_fail(ctx, BEM_ERR_INVALID, "mass: dtype must be F64/C128");
+    int mode = x ? 1 : 0;
+    if (mode == 0 && (!out || ld <= 0)) return bem_fail(ctx, BEM_ERR_INVALID, "mass: out is NULL");
+    if (mode == 1 && !y) return bem_fail(ctx, BEM_ERR_INVALID, "mass: y is NULL");
+    return bem_launch_mass(ctx, test, trial, dtype == BEM_C128, mode, out, ld, scale, out_t, scale_t, x, y, conj_x,
+                           (cudaStream_t)stream);
+}
+
+}  // extern "C"

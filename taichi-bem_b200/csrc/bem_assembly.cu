@@ -1,0 +1,906 @@
+// Galerkin BEM operator assembly on sm_100a.
+//
+// The reference evaluates every operator with one Taichi thread per test
+// panel that loops serially over trial panels x basis pairs x GaussQR^4
+// points and recomputes the integrand per basis pair
+// (src/BEM_functions/single_layer/single_layer_3d.py:371-433 and its double /
+// adjoint / hypersingular twins).  Here:
+//
+//  * separate pairs (the O(nt^2) bulk) run in `far_kernel`: one thread per
+//    (test panel, trial panel) pair, 128 trial panels per CTA and TI test
+//    panels staged in shared memory.  The separate-pair rule factorises into
+//    Q^2 points per panel (x(xsi, eta1) on the test panel, y(eta2, eta3) on the
+//    trial panel), so each thread loops over its trial points (registers) and
+//    the test points (shared-memory broadcast), and ONE kernel evaluation
+//    serves every basis pair (P0/P1 test x P0/P1 trial).  Coordinates are
+//    stored relative to the panel centroid and the centroid difference is
+//    formed in FP64, so the FP32 variant (mixed precision) keeps its relative
+//    accuracy for close pairs.
+//  * coincident / edge / vertex pairs (about 13 per panel on an icosphere)
+//    run in `near_kernel` in FP64: one warp per pair, lanes split the
+//    GaussQR^4 Sauter-Schwab points, warp-shuffle reduction.
+//  * P0 rows/columns are written in place (each entry has one writer); P1
+//    entries receive contributions from several panel pairs and use FP64
+//    atomics, as the reference's Taichi `+=` does (hypersingular_layer_3d.py:500).
+#include <cuda_runtime.h>
+
+#include "bem_internal.cuh"
+
+namespace {
+
+template <typename T>
+struct V4T;
+template <>
+struct V4T<float> {
+    using type = float4;
+};
+template <>
+struct V4T<double> {
+    using type = double4;
+};
+
+__device__ __forceinline__ float dev_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double dev_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ void dev_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void dev_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+
+struct cxd {
+    double re, im;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ----------------------------------------------------------------------------
+// geometry: areas/normals/centroids/curls and the separate-rule points
+// (mesh_manager.py:114-125, hypersingular_layer_3d.py:55-64,163-169,
+//  single_layer_3d.py:143-177)
+// ----------------------------------------------------------------------------
+__global__ void geometry_kernel(int nt, int Q, const double* __restrict__ verts, const int32_t* __restrict__ tris,
+                                const double* __restrict__ gp, const double* __restrict__ gw, double* area,
+                                double* normal, double* centroid, double* curl, double4* pts64, float4* pts32,
+                                int32_t* flags) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nt) return;
+    double v[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) v[a][c] = verts[3 * tris[3 * p + a] + c];
+    double e1[3], e2[3];
+    for (int c = 0; c < 3; ++c) {
+        e1[c] = v[1][c] - v[0][c];
+        e2[c] = v[2][c] - v[1][c];
+    }
+    double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    double nrm = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    if (!(nrm > 0.0) || !isfinite(nrm)) {
+        atomicExch(&flags[0], 1 + p);  // degenerate or non-finite panel
+        nrm = 1.0;
+    }
+    double A = 0.5 * nrm;
+    double n[3] = {cr[0] / nrm, cr[1] / nrm, cr[2] / nrm};
+    area[p] = A;
+    double cen[3];
+    for (int c = 0; c < 3; ++c) {
+        normal[3 * p + c] = n[c];
+        cen[c] = (v[0][c] + v[1][c] + v[2][c]) / 3.0;
+        centroid[3 * p + c] = cen[c];
+    }
+    // curl of the hat of vertex b: n x ((n x edge_opposite_b) / (2A))
+    const double* opp[3][2] = {{v[2], v[1]}, {v[0], v[2]}, {v[1], v[0]}};
+    for (int b = 0; b < 3; ++b) {
+        double d[3] = {opp[b][0][0] - opp[b][1][0], opp[b][0][1] - opp[b][1][1], opp[b][0][2] - opp[b][1][2]};
+        double g[3] = {(n[1] * d[2] - n[2] * d[1]) / (2.0 * A), (n[2] * d[0] - n[0] * d[2]) / (2.0 * A),
+                       (n[0] * d[1] - n[1] * d[0]) / (2.0 * A)};
+        curl[9 * p + 3 * b + 0] = n[1] * g[2] - n[2] * g[1];
+        curl[9 * p + 3 * b + 1] = n[2] * g[0] - n[0] * g[2];
+        curl[9 * p + 3 * b + 2] = n[0] * g[1] - n[1] * g[0];
+    }
+    int Q2 = Q * Q;
+    for (int ix = 0; ix < Q; ++ix)
+        for (int iy = 0; iy < Q; ++iy) {
+            double r1 = gp[ix], r2 = gp[iy] * r1;
+            double w = gw[ix] * gw[iy] * (A * 2.0) * r1;
+            double o[3];
+            for (int c = 0; c < 3; ++c) o[c] = ((1.0 - r1) * v[0][c] + (r1 - r2) * v[1][c] + r2 * v[2][c]) - cen[c];
+            pts64[(size_t)p * Q2 + ix * Q + iy] = make_double4(o[0], o[1], o[2], w);
+            pts32[(size_t)p * Q2 + ix * Q + iy] = make_float4((float)o[0], (float)o[1], (float)o[2], (float)w);
+        }
+}
+
+__global__ void scatter_local_kernel(int n, const int32_t* __restrict__ panels, int32_t* local_of_global, int nt,
+                                     int32_t* flags) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int g = panels[i];
+    if (g < 0 || g >= nt) {
+        atomicExch(&flags[1], 1 + i);
+        return;
+    }
+    local_of_global[g] = i;
+}
+
+// ----------------------------------------------------------------------------
+// kernel functions
+// ----------------------------------------------------------------------------
+// Kernel value at d = x - y (without the 1/(4 pi) factor):
+//   V, W: e^{ikr}/r                           (G, BEM_manager.py:474-483)
+//   K:    (d.n_y)/r^3 (1 - ikr) e^{ikr}       (grad_G_y, BEM_manager.py:510-523)
+//   KP:   (-d.n_x)/r^3 (1 - ikr) e^{ikr}      (grad_G_y with x,y swapped and n_x)
+template <int OP, bool HELM, typename T>
+__device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T& re, T& im) {
+    T r2 = dx * dx + dy * dy + dz * dz;
+    T rinv = dev_rsqrt(r2);
+    if (OP == BEM_OP_V || OP == BEM_OP_W) {
+        if (!HELM) {
+            re = rinv;
+            im = T(0);
+        } else {
+            T r = r2 * rinv;
+            T s, c;
+            dev_sincos(k * r, &s, &c);
+            re = rinv * c;
+            im = rinv * s;
+        }
+    } else {
+        T dn = dx * nx + dy * ny + dz * nz;
+        if (OP == BEM_OP_KP) dn = -dn;
+        T t = dn * rinv * rinv * rinv;
+        if (!HELM) {
+            re = t;
+            im = T(0);
+        } else {
+            T r = r2 * rinv;
+            T kr = k * r;
+            T s, c;
+            dev_sincos(kr, &s, &c);
+            re = t * (c + kr * s);
+            im = t * (s - kr * c);
+        }
+    }
+}
+
+struct FarArgs {
+    int n_test, n_trial;
+    const int32_t* test_panels;
+    const int32_t* test_dof;
+    const int32_t* trial_panels;
+    const int32_t* trial_dof;
+    const int32_t* tris;
+    const double* centroid;
+    const double* normal;
+    const double* curl;
+    const void* pts;
+    const void* phi;
+    int Q2;
+    double k, k2;
+    int mode;
+    double* out;
+    int64_t ld;
+    double scale;
+    double* out_t;
+    double scale_t;
+    const double* x;
+    double* y;
+    int conj_x;
+};
+
+constexpr int FAR_THREADS = 128;
+constexpr int FAR_TI = 8;
+
+template <bool CPLX>
+__device__ __forceinline__ void add_entry(double* base, int64_t idx, double re, double im, bool atomic) {
+    if (CPLX) {
+        if (atomic) {
+            atomicAdd(base + 2 * idx, re);
+            atomicAdd(base + 2 * idx + 1, im);
+        } else {
+            base[2 * idx] += re;
+            base[2 * idx + 1] += im;
+        }
+    } else {
+        if (atomic)
+            atomicAdd(base + idx, re);
+        else
+            base[idx] += re;
+    }
+}
+
+template <int OP, bool HELM, int NBX, int NBY, typename T>
+__global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
+    using V4 = typename V4T<T>::type;
+    constexpr bool W_OP = (OP == BEM_OP_W);
+    // accumulate phi-weighted moments for every op except Laplace W, whose
+    // only term is the curl-curl one (k2 = 0)
+    constexpr bool NEED_PHI = !(W_OP && !HELM);
+    constexpr int AX = NEED_PHI ? NBX : 1;
+    constexpr int AY = NEED_PHI ? NBY : 1;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V4* sx = reinterpret_cast<V4*>(smem_raw);                 // [FAR_TI][Q2]
+    T* sphi = reinterpret_cast<T*>(sx + FAR_TI * a.Q2);      // [Q2*3]
+    __shared__ int s_gi[FAR_TI];
+    __shared__ int s_tri[FAR_TI][3];
+    __shared__ double s_cen[FAR_TI][3];
+    __shared__ double s_nrm[FAR_TI][3];
+
+    const int Q2 = a.Q2;
+    const int lj = blockIdx.x * FAR_THREADS + threadIdx.x;
+    const int li0 = blockIdx.y * FAR_TI;
+    const V4* pts = reinterpret_cast<const V4*>(a.pts);
+
+    for (int idx = threadIdx.x; idx < FAR_TI * Q2; idx += FAR_THREADS) {
+        int t = idx / Q2, q = idx - t * Q2;
+        int li = li0 + t;
+        if (li < a.n_test) sx[idx] = pts[(size_t)a.test_panels[li] * Q2 + q];
+    }
+    if (NBX == 3 || NBY == 3) {
+        const T* phi = reinterpret_cast<const T*>(a.phi);
+        for (int idx = threadIdx.x; idx < Q2 * 3; idx += FAR_THREADS) sphi[idx] = phi[idx];
+    }
+    if (threadIdx.x < FAR_TI) {
+        int li = li0 + threadIdx.x;
+        int gi = li < a.n_test ? a.test_panels[li] : -1;
+        s_gi[threadIdx.x] = gi;
+        for (int c = 0; c < 3; ++c) {
+            s_tri[threadIdx.x][c] = gi >= 0 ? a.tris[3 * gi + c] : -1;
+            s_cen[threadIdx.x][c] = gi >= 0 ? a.centroid[3 * gi + c] : 0.0;
+            s_nrm[threadIdx.x][c] = gi >= 0 ? a.normal[3 * gi + c] : 0.0;
+        }
+    }
+    __syncthreads();
+
+    const bool valid_j = lj < a.n_trial;
+    const int gj = valid_j ? a.trial_panels[lj] : 0;
+    int tri_j[3];
+    double cen_j[3], nrm_j[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        tri_j[c] = a.tris[3 * gj + c];
+        cen_j[c] = a.centroid[3 * gj + c];
+        nrm_j[c] = a.normal[3 * gj + c];
+    }
+    const V4* ptsj = pts + (size_t)gj * Q2;
+    const T kk = T(a.k);
+    const int lane = threadIdx.x & 31;
+
+    for (int t = 0; t < FAR_TI; ++t) {
+        const int li = li0 + t;
+        if (li >= a.n_test) break;  // uniform across the CTA
+        const int gi = s_gi[t];
+        const bool sep = valid_j && (bem_relation(s_tri[t], tri_j, gi == gj) == REL_SEPARATE);
+
+        double acc_re[AX][AY], acc_im[AX][AY];
+        double acc0_re = 0.0, acc0_im = 0.0;  // W curl-curl moment (sum of weights * kernel)
+#pragma unroll
+        for (int bx = 0; bx < AX; ++bx)
+#pragma unroll
+            for (int by = 0; by < AY; ++by) acc_re[bx][by] = acc_im[bx][by] = 0.0;
+
+        if (sep) {
+            const T dcx = T(s_cen[t][0] - cen_j[0]);
+            const T dcy = T(s_cen[t][1] - cen_j[1]);
+            const T dcz = T(s_cen[t][2] - cen_j[2]);
+            T nx, ny, nz;
+            if (OP == BEM_OP_KP) {
+                nx = T(s_nrm[t][0]);
+                ny = T(s_nrm[t][1]);
+                nz = T(s_nrm[t][2]);
+            } else {
+                nx = T(nrm_j[0]);
+                ny = T(nrm_j[1]);
+                nz = T(nrm_j[2]);
+            }
+            const V4* sxt = sx + t * Q2;
+            for (int b = 0; b < Q2; ++b) {
+                const V4 yb = ptsj[b];
+                const T ex = dcx - yb.x, ey = dcy - yb.y, ez = dcz - yb.z;
+                T s_re[AX], s_im[AX];
+                T c_re = T(0), c_im = T(0);
+#pragma unroll
+                for (int bx = 0; bx < AX; ++bx) s_re[bx] = s_im[bx] = T(0);
+#pragma unroll 5
+                for (int q = 0; q < Q2; ++q) {
+                    const V4 xa = sxt[q];
+                    T re, im;
+                    kval<OP, HELM, T>(xa.x + ex, xa.y + ey, xa.z + ez, nx, ny, nz, kk, re, im);
+                    if (W_OP) {
+                        c_re += xa.w * re;
+                        if (HELM) c_im += xa.w * im;
+                    }
+                    if (NEED_PHI) {
+                        if (AX == 1) {
+                            s_re[0] += xa.w * re;
+                            if (HELM) s_im[0] += xa.w * im;
+                        } else {
+#pragma unroll
+                            for (int bx = 0; bx < AX; ++bx) {
+                                T wp = xa.w * sphi[3 * q + bx];
+                                s_re[bx] += wp * re;
+                                if (HELM) s_im[bx] += wp * im;
+                            }
+                        }
+                    }
+                }
+                const double wb = double(yb.w);
+                if (W_OP) {
+                    acc0_re += wb * double(c_re);
+                    acc0_im += wb * double(c_im);
+                }
+                if (NEED_PHI) {
+#pragma unroll
+                    for (int by = 0; by < AY; ++by) {
+                        double wpb = (AY == 1) ? wb : wb * double(sphi[3 * b + by]);
+#pragma unroll
+                        for (int bx = 0; bx < AX; ++bx) {
+                            acc_re[bx][by] += wpb * double(s_re[bx]);
+                            acc_im[bx][by] += wpb * double(s_im[bx]);
+                        }
+                    }
+                }
+            }
+        }
+
+        // ---- epilogue: values of all basis pairs ----
+        double val_re[NBX][NBY], val_im[NBX][NBY];
+#pragma unroll
+        for (int bx = 0; bx < NBX; ++bx)
+#pragma unroll
+            for (int by = 0; by < NBY; ++by) {
+                double vr, vi;
+                if (W_OP) {
+                    // W = G curl.curl - k2 (n_x.n_y) G phi_x phi_y (hypersingular_layer_3d.py:206-211)
+                    double cd = 0.0;
+                    if (NBX == 3 && NBY == 3 && sep) {
+                        const double* cx = a.curl + 9 * gi + 3 * bx;
+                        const double* cy = a.curl + 9 * gj + 3 * by;
+                        cd = cx[0] * cy[0] + cx[1] * cy[1] + cx[2] * cy[2];
+                    }
+                    vr = acc0_re * cd;
+                    vi = acc0_im * cd;
+                    if (NEED_PHI) {
+                        double nd = s_nrm[t][0] * nrm_j[0] + s_nrm[t][1] * nrm_j[1] + s_nrm[t][2] * nrm_j[2];
+                        int ix = AX == 1 ? 0 : bx, iy = AY == 1 ? 0 : by;
+                        vr -= a.k2 * nd * acc_re[ix][iy];
+                        vi -= a.k2 * nd * acc_im[ix][iy];
+                    }
+                } else {
+                    int ix = AX == 1 ? 0 : bx, iy = AY == 1 ? 0 : by;
+                    vr = acc_re[ix][iy];
+                    vi = acc_im[ix][iy];
+                }
+                val_re[bx][by] = vr * BEM_INV4PI;
+                val_im[bx][by] = vi * BEM_INV4PI;
+            }
+
+        if (a.mode == 0) {
+            if (sep) {
+                constexpr bool ATOMIC = (NBX == 3 || NBY == 3);
+#pragma unroll
+                for (int bx = 0; bx < NBX; ++bx) {
+                    const int row = a.test_dof[li * NBX + bx];
+                    if (row < 0) continue;
+#pragma unroll
+                    for (int by = 0; by < NBY; ++by) {
+                        const int col = a.trial_dof[lj * NBY + by];
+                        if (col < 0) continue;
+                        add_entry<HELM>(a.out, (int64_t)row * a.ld + col, a.scale * val_re[bx][by],
+                                        a.scale * val_im[bx][by], ATOMIC);
+                        if (a.out_t)
+                            add_entry<HELM>(a.out_t, (int64_t)col * a.ld + row, a.scale_t * val_re[bx][by],
+                                            a.scale_t * val_im[bx][by], true);
+                    }
+                }
+            }
+        } else {
+            // apply: y[row] += scale * sum_col val * x[col]
+#pragma unroll
+            for (int bx = 0; bx < NBX; ++bx) {
+                double cr = 0.0, ci = 0.0;
+                if (sep) {
+#pragma unroll
+                    for (int by = 0; by < NBY; ++by) {
+                        const int col = a.trial_dof[lj * NBY + by];
+                        if (col < 0) continue;
+                        if (HELM) {
+                            double xr = a.x[2 * col], xi = a.x[2 * col + 1];
+                            if (a.conj_x) xi = -xi;
+                            cr += val_re[bx][by] * xr - val_im[bx][by] * xi;
+                            ci += val_re[bx][by] * xi + val_im[bx][by] * xr;
+                        } else {
+                            cr += val_re[bx][by] * a.x[col];
+                        }
+                    }
+                }
+                cr = warp_sum(cr);
+                if (HELM) ci = warp_sum(ci);
+                if (lane == 0) {
+                    const int row = a.test_dof[li * NBX + bx];
+                    if (row >= 0) {
+                        if (HELM) {
+                            atomicAdd(a.y + 2 * row, a.scale * cr);
+                            atomicAdd(a.y + 2 * row + 1, a.scale * ci);
+                        } else {
+                            atomicAdd(a.y + row, a.scale * cr);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// near field: coincident / edge / vertex pairs in FP64 (Sauter-Schwab maps of
+// single_layer_3d.py:178-367, identical in the other operators)
+// ----------------------------------------------------------------------------
+struct NearArgs {
+    int64_t n_near;
+    const int4* near;
+    const int32_t* test_local;
+    const int32_t* trial_local;
+    const int32_t* test_dof;
+    const int32_t* trial_dof;
+    const int32_t* tris;
+    const double* verts;
+    const double* area;
+    const double* normal;
+    const double* curl;
+    const double* gp;
+    const double* gw;
+    int Q;
+    double k, k2;
+    int quirk;
+    int mode;
+    double* out;
+    int64_t ld;
+    double scale;
+    double* out_t;
+    double scale_t;
+    const double* x;
+    double* y;
+    int conj_x;
+};
+
+struct NearPanel {
+    double x1[3], x2[3], x3[3];
+    double n[3];
+    double area;
+    int slot[3];  // parameter slot of original vertex b
+};
+
+__device__ __forceinline__ void load_near_panel(NearPanel& P, const NearArgs& a, int g, int perm) {
+    int pm[3] = {perm & 3, (perm >> 2) & 3, (perm >> 4) & 3};
+    const int32_t* t = a.tris + 3 * g;
+    for (int c = 0; c < 3; ++c) {
+        P.x1[c] = a.verts[3 * t[pm[0]] + c];
+        P.x2[c] = a.verts[3 * t[pm[1]] + c];
+        P.x3[c] = a.verts[3 * t[pm[2]] + c];
+        P.n[c] = a.normal[3 * g + c];
+    }
+    P.area = a.area[g];
+    for (int s = 0; s < 3; ++s) P.slot[pm[s]] = s;
+}
+
+__device__ __forceinline__ double shape_slot(double r1, double r2, int s) {
+    return s == 0 ? 1.0 - r1 : (s == 1 ? r1 - r2 : r2);
+}
+
+template <int OP, bool HELM, int NBX, int NBY>
+__global__ void __launch_bounds__(128) near_kernel(NearArgs a) {
+    constexpr bool W_OP = (OP == BEM_OP_W);
+    constexpr bool NEED_PHI = !(W_OP && !HELM);
+    const int lane = threadIdx.x & 31;
+    const int64_t pid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (pid >= a.n_near) return;
+    const int4 e = a.near[pid];
+    const int gi = e.x, gj = e.y, rel = e.z;
+    const int li = a.test_local[gi], lj = a.trial_local[gj];
+    if (li < 0 || lj < 0) return;  // warp-uniform
+    const int permx = a.quirk ? (0 | (1 << 2) | (2 << 4)) : (e.w & 63);
+    const int permy = a.quirk ? (0 | (1 << 2) | (2 << 4)) : ((e.w >> 6) & 63);
+    NearPanel X, Y;
+    load_near_panel(X, a, gi, permx);
+    load_near_panel(Y, a, gj, permy);
+    const double* nKx = X.n;  // normal used by KP
+    const double* nKy = Y.n;  // normal used by K
+
+    double acc_re[NBX][NBY], acc_im[NBX][NBY], acc0_re = 0.0, acc0_im = 0.0;
+#pragma unroll
+    for (int bx = 0; bx < NBX; ++bx)
+#pragma unroll
+        for (int by = 0; by < NBY; ++by) acc_re[bx][by] = acc_im[bx][by] = 0.0;
+
+    int sx[NBX], sy[NBY];
+#pragma unroll
+    for (int bx = 0; bx < NBX; ++bx) sx[bx] = NBX == 1 ? -1 : X.slot[bx];
+#pragma unroll
+    for (int by = 0; by < NBY; ++by) sy[by] = NBY == 1 ? -1 : Y.slot[by];
+
+    const int Q = a.Q;
+    const int Q4 = Q * Q * Q * Q;
+    // One kernel evaluation at parameters (r1x,r2x) on X and (r1y,r2y) on Y,
+    // argument order `second` (the swapped coincide term), basis values taken
+    // at (px1,px2) for the test side and (py1,py2) for the trial side.
+    auto add = [&](double r1x, double r2x, double r1y, double r2y, double wj, bool second, double px1, double px2,
+                   double py1, double py2) {
+        double x[3], yv[3];
+        for (int c = 0; c < 3; ++c) {
+            x[c] = (1.0 - r1x) * X.x1[c] + (r1x - r2x) * X.x2[c] + r2x * X.x3[c];
+            yv[c] = (1.0 - r1y) * Y.x1[c] + (r1y - r2y) * Y.x2[c] + r2y * Y.x3[c];
+        }
+        double dx = x[0] - yv[0], dy = x[1] - yv[1], dz = x[2] - yv[2];
+        double re, im;
+        if (OP == BEM_OP_K) {
+            // first: grad_G_y(x, y, n_y); second: grad_G_y(y, x, n_y)
+            double sgn = second ? -1.0 : 1.0;
+            kval<BEM_OP_K, HELM, double>(sgn * dx, sgn * dy, sgn * dz, nKy[0], nKy[1], nKy[2], a.k, re, im);
+        } else if (OP == BEM_OP_KP) {
+            // first: grad_G_y(y, x, n_x); second: grad_G_y(x, y, n_x)
+            double sgn = second ? -1.0 : 1.0;
+            kval<BEM_OP_KP, HELM, double>(sgn * dx, sgn * dy, sgn * dz, nKx[0], nKx[1], nKx[2], a.k, re, im);
+        } else {
+            kval<BEM_OP_V, HELM, double>(dx, dy, dz, 0.0, 0.0, 0.0, a.k, re, im);
+        }
+        re *= wj;
+        im *= wj;
+        if (W_OP) {
+            acc0_re += re;
+            acc0_im += im;
+        }
+        if (NEED_PHI) {
+#pragma unroll
+            for (int bx = 0; bx < NBX; ++bx) {
+                double phx = NBX == 1 ? 1.0 : shape_slot(px1, px2, sx[bx]);
+#pragma unroll
+                for (int by = 0; by < NBY; ++by) {
+                    double phy = NBY == 1 ? 1.0 : shape_slot(py1, py2, sy[by]);
+                    acc_re[bx][by] += re * phx * phy;
+                    acc_im[bx][by] += im * phx * phy;
+                }
+            }
+        }
+    };
+
+    for (int p = lane; p < Q4; p += 32) {
+        int iw = p % Q, iz = (p / Q) % Q, iy = (p / (Q * Q)) % Q, ix = p / (Q * Q * Q);
+        const double xsi = a.gp[ix], eta1 = a.gp[iy], eta2 = a.gp[iz], eta3 = a.gp[iw];
+        const double weight = (a.gw[ix] * a.gw[iy] * (X.area * 2.0)) * (a.gw[iz] * a.gw[iw] * (Y.area * 2.0));
+        if (rel == REL_COINCIDE) {
+            const double jac = xsi * xsi * xsi * eta1 * eta1 * eta2;
+            const double w0 = xsi, w1 = xsi * eta1, w2 = xsi * eta1 * eta2, w3 = xsi * eta1 * eta2 * eta3;
+            // m_mats_coincide (BEM_manager.py:141-165) applied to w
+            double z[3][4] = {{w0, w0 - w1 + w2, w3, w2},
+                              {w0, w1 - w2 + w3, w2, w3},
+                              {w0 - w3, w1 - w3, -w3, w2 - w3}};
+            for (int m = 0; m < 3; ++m) {
+                double r1x = z[m][0], r2x = z[m][1], r1y = z[m][0] - z[m][2], r2y = z[m][1] - z[m][3];
+                add(r1x, r2x, r1y, r2y, weight * jac, false, r1x, r2x, r1y, r2y);
+                if (a.quirk)
+                    add(r1x, r2x, r1y, r2y, weight * jac, true, r1x, r2x, r1y, r2y);
+                else
+                    add(r1x, r2x, r1y, r2y, weight * jac, true, r1y, r2y, r1x, r2x);
+            }
+        } else if (rel == REL_VERTEX) {
+            const double jac = xsi * xsi * xsi * eta2;
+            add(xsi, xsi * eta1, xsi * eta2, xsi * eta2 * eta3, weight * jac, false, xsi, xsi * eta1, xsi * eta2,
+                xsi * eta2 * eta3);
+            add(xsi * eta2, xsi * eta2 * eta3, xsi, xsi * eta1, weight * jac, false, xsi * eta2, xsi * eta2 * eta3,
+                xsi, xsi * eta1);
+        } else {  // REL_EDGE
+            double w0, w1, w2, w3;
+            const double jac1 = xsi * xsi * xsi * eta1 * eta1;
+            const double jac = jac1 * eta2;
+            w0 = xsi; w1 = -xsi * eta1 * eta2; w2 = xsi * eta1 * (1.0 - eta2); w3 = xsi * eta1 * eta3;
+            add(w0, w3, w0 + w1, w2, weight * jac1, false, w0, w3, w0 + w1, w2);
+            w0 = xsi; w1 = -xsi * eta1 * eta2 * eta3; w2 = xsi * eta1 * eta2 * (1.0 - eta3); w3 = xsi * eta1;
+            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
+            w0 = xsi * (1.0 - eta1 * eta2); w1 = xsi * eta1 * eta2; w2 = xsi * eta1 * eta2 * eta3;
+            w3 = xsi * eta1 * (1.0 - eta2);
+            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
+            w0 = xsi * (1.0 - eta1 * eta2 * eta3); w1 = xsi * eta1 * eta2 * eta3; w2 = xsi * eta1;
+            w3 = xsi * eta1 * eta2 * (1.0 - eta3);
+            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
+            w0 = xsi * (1.0 - eta1 * eta2 * eta3); w1 = xsi * eta1 * eta2 * eta3; w2 = xsi * eta1 * eta2;
+            w3 = xsi * eta1 * (1.0 - eta2 * eta3);
+            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
+        }
+    }
+
+    // warp reduction of every moment
+    acc0_re = warp_sum(acc0_re);
+    acc0_im = warp_sum(acc0_im);
+#pragma unroll
+    for (int bx = 0; bx < NBX; ++bx)
+#pragma unroll
+        for (int by = 0; by < NBY; ++by) {
+            acc_re[bx][by] = warp_sum(acc_re[bx][by]);
+            acc_im[bx][by] = warp_sum(acc_im[bx][by]);
+        }
+    if (lane != 0) return;
+
+    const double nd = X.n[0] * Y.n[0] + X.n[1] * Y.n[1] + X.n[2] * Y.n[2];
+#pragma unroll
+    for (int bx = 0; bx < NBX; ++bx) {
+        const int row = a.test_dof[li * NBX + bx];
+        if (row < 0) continue;
+        double cr = 0.0, ci = 0.0;
+#pragma unroll
+        for (int by = 0; by < NBY; ++by) {
+            const int col = a.trial_dof[lj * NBY + by];
+            if (col < 0) continue;
+            double vr, vi;
+            if (W_OP) {
+                double cd = 0.0;
+                if (NBX == 3 && NBY == 3) {
+                    const double* cx = a.curl + 9 * gi + 3 * bx;
+                    const double* cy = a.curl + 9 * gj + 3 * by;
+                    cd = cx[0] * cy[0] + cx[1] * cy[1] + cx[2] * cy[2];
+                }
+                vr = acc0_re * cd;
+                vi = acc0_im * cd;
+                if (NEED_PHI) {
+                    vr -= a.k2 * nd * acc_re[bx][by];
+                    vi -= a.k2 * nd * acc_im[bx][by];
+                }
+            } else {
+                vr = acc_re[bx][by];
+                vi = acc_im[bx][by];
+            }
+            vr *= BEM_INV4PI;
+            vi *= BEM_INV4PI;
+            if (a.mode == 0) {
+                add_entry<HELM>(a.out, (int64_t)row * a.ld + col, a.scale * vr, a.scale * vi, true);
+                if (a.out_t) add_entry<HELM>(a.out_t, (int64_t)col * a.ld + row, a.scale_t * vr, a.scale_t * vi, true);
+            } else {
+                if (HELM) {
+                    double xr = a.x[2 * col], xi = a.x[2 * col + 1];
+                    if (a.conj_x) xi = -xi;
+                    cr += vr * xr - vi * xi;
+                    ci += vr * xi + vi * xr;
+                } else {
+                    cr += vr * a.x[col];
+                }
+            }
+        }
+        if (a.mode != 0) {
+            if (HELM) {
+                atomicAdd(a.y + 2 * row, a.scale * cr);
+                atomicAdd(a.y + 2 * row + 1, a.scale * ci);
+            } else {
+                atomicAdd(a.y + row, a.scale * cr);
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// mass (identity) block: Q^2 rule on one triangle (identity_layer_3d.py:45-146)
+// ----------------------------------------------------------------------------
+struct MassArgs {
+    int n_panels;
+    const int32_t* panels;
+    int nbx, nby;
+    const int32_t* test_dof;
+    const int32_t* trial_dof;
+    const double* area;
+    const double* gp;
+    const double* gw;
+    int Q;
+    int cplx;
+    int mode;
+    double* out;
+    int64_t ld;
+    double scale;
+    double* out_t;
+    double scale_t;
+    const double* x;
+    double* y;
+    int conj_x;
+};
+
+__global__ void mass_kernel(MassArgs a) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    int per = a.nbx * a.nby;
+    if (id >= a.n_panels * per) return;
+    int li = id / per, r = id - li * per, ii = r / a.nby, jj = r - ii * a.nby;
+    int row = a.test_dof[li * a.nbx + ii], col = a.trial_dof[li * a.nby + jj];
+    if (row < 0 || col < 0) return;
+    int bx = a.nbx == 1 ? -1 : ii, by = a.nby == 1 ? -1 : jj;
+    double A = a.area[a.panels[li]];
+    double acc = 0.0;
+    for (int ix = 0; ix < a.Q; ++ix)
+        for (int iy = 0; iy < a.Q; ++iy) {
+            double r1 = a.gp[ix], r2 = a.gp[iy] * r1;
+            double w = a.gw[ix] * a.gw[iy] * (A * 2.0);
+            double px = bx < 0 ? 1.0 : shape_slot(r1, r2, bx);
+            double py = by < 0 ? 1.0 : shape_slot(r1, r2, by);
+            acc += (px * py) * w * r1;
+        }
+    if (a.mode == 0) {
+        if (a.cplx) {
+            atomicAdd(a.out + 2 * ((int64_t)row * a.ld + col), a.scale * acc);
+            if (a.out_t) atomicAdd(a.out_t + 2 * ((int64_t)col * a.ld + row), a.scale_t * acc);
+        } else {
+            atomicAdd(a.out + (int64_t)row * a.ld + col, a.scale * acc);
+            if (a.out_t) atomicAdd(a.out_t + (int64_t)col * a.ld + row, a.scale_t * acc);
+        }
+    } else {
+        if (a.cplx) {
+            double xr = a.x[2 * col], xi = a.x[2 * col + 1];
+            if (a.conj_x) xi = -xi;
+            atomicAdd(a.y + 2 * row, a.scale * acc * xr);
+            atomicAdd(a.y + 2 * row + 1, a.scale * acc * xi);
+        } else {
+            atomicAdd(a.y + row, a.scale * acc * a.x[col]);
+        }
+    }
+}
+
+template <int OP, bool HELM, int NBX, int NBY>
+int launch_op(bem_ctx* ctx, const FarArgs& fa, const NearArgs& na, bool fp32, cudaStream_t s) {
+    dim3 grid((fa.n_trial + FAR_THREADS - 1) / FAR_THREADS, (fa.n_test + FAR_TI - 1) / FAR_TI);
+    if (grid.y > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "too many test panels for one launch");
+    if (fa.n_test > 0 && fa.n_trial > 0) {
+        size_t smem;
+        if (fp32) {
+            smem = FAR_TI * fa.Q2 * sizeof(float4) + fa.Q2 * 3 * sizeof(float);
+            far_kernel<OP, HELM, NBX, NBY, float><<<grid, FAR_THREADS, smem, s>>>(fa);
+        } else {
+            smem = FAR_TI * fa.Q2 * sizeof(double4) + fa.Q2 * 3 * sizeof(double);
+            far_kernel<OP, HELM, NBX, NBY, double><<<grid, FAR_THREADS, smem, s>>>(fa);
+        }
+        ctx->launches++;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "far_kernel launch")) return rc;
+    }
+    if (na.n_near > 0) {
+        int warps = 4;
+        int64_t blocks = (na.n_near + warps - 1) / warps;
+        near_kernel<OP, HELM, NBX, NBY><<<(unsigned)blocks, 32 * warps, 0, s>>>(na);
+        ctx->launches++;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "near_kernel launch")) return rc;
+    }
+    return BEM_OK;
+}
+
+template <int OP, bool HELM>
+int dispatch_nb(bem_ctx* ctx, int nbx, int nby, const FarArgs& fa, const NearArgs& na, bool fp32, cudaStream_t s) {
+    if (nbx == 1 && nby == 1) return launch_op<OP, HELM, 1, 1>(ctx, fa, na, fp32, s);
+    if (nbx == 1 && nby == 3) return launch_op<OP, HELM, 1, 3>(ctx, fa, na, fp32, s);
+    if (nbx == 3 && nby == 1) return launch_op<OP, HELM, 3, 1>(ctx, fa, na, fp32, s);
+    if (nbx == 3 && nby == 3) return launch_op<OP, HELM, 3, 3>(ctx, fa, na, fp32, s);
+    return bem_fail(ctx, BEM_ERR_INVALID, "nb must be 1 (P0) or 3 (P1)");
+}
+
+template <int OP>
+int dispatch_helm(bem_ctx* ctx, bool helm, int nbx, int nby, const FarArgs& fa, const NearArgs& na, bool fp32,
+                  cudaStream_t s) {
+    return helm ? dispatch_nb<OP, true>(ctx, nbx, nby, fa, na, fp32, s)
+                : dispatch_nb<OP, false>(ctx, nbx, nby, fa, na, fp32, s);
+}
+
+}  // namespace
+
+int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s) {
+    int threads = 128;
+    int blocks = (ctx->nt + threads - 1) / threads;
+    geometry_kernel<<<blocks, threads, 0, s>>>(ctx->nt, ctx->Q, ctx->verts, ctx->tris, ctx->gp, ctx->gw, ctx->area,
+                                                ctx->normal, ctx->centroid, ctx->curl, ctx->pts64, ctx->pts32,
+                                                ctx->flags);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "geometry_kernel launch");
+}
+
+static int fill_local_map(bem_ctx* ctx, const bem_space* sp, int32_t* map, cudaStream_t s) {
+    if (int rc = bem_check_cuda(ctx, cudaMemsetAsync(map, 0xff, sizeof(int32_t) * ctx->nt, s), "memset")) return rc;
+    if (sp->n_panels > 0) {
+        scatter_local_kernel<<<(sp->n_panels + 127) / 128, 128, 0, s>>>(sp->n_panels, sp->panels, map, ctx->nt,
+                                                                        ctx->flags);
+        ctx->launches++;
+        return bem_check_cuda(ctx, cudaGetLastError(), "scatter_local_kernel launch");
+    }
+    return BEM_OK;
+}
+
+int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                        int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
+                        void* y, int conj_x, cudaStream_t s) {
+    if (int rc = fill_local_map(ctx, test, ctx->test_local, s)) return rc;
+    if (int rc = fill_local_map(ctx, trial, ctx->trial_local, s)) return rc;
+    bool fp32 = op->precision == BEM_PREC_MIXED;
+    FarArgs fa;
+    fa.n_test = test->n_panels;
+    fa.n_trial = trial->n_panels;
+    fa.test_panels = test->panels;
+    fa.test_dof = test->dof;
+    fa.trial_panels = trial->panels;
+    fa.trial_dof = trial->dof;
+    fa.tris = ctx->tris;
+    fa.centroid = ctx->centroid;
+    fa.normal = ctx->normal;
+    fa.curl = ctx->curl;
+    fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
+    fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
+    fa.Q2 = ctx->Q2;
+    fa.k = op->k;
+    fa.k2 = op->k2;
+    fa.mode = mode;
+    fa.out = (double*)out;
+    fa.ld = ld;
+    fa.scale = scale;
+    fa.out_t = (double*)out_t;
+    fa.scale_t = scale_t;
+    fa.x = (const double*)x;
+    fa.y = (double*)y;
+    fa.conj_x = conj_x;
+
+    NearArgs na;
+    na.n_near = ctx->n_near;
+    na.near = ctx->near;
+    na.test_local = ctx->test_local;
+    na.trial_local = ctx->trial_local;
+    na.test_dof = test->dof;
+    na.trial_dof = trial->dof;
+    na.tris = ctx->tris;
+    na.verts = ctx->verts;
+    na.area = ctx->area;
+    na.normal = ctx->normal;
+    na.curl = ctx->curl;
+    na.gp = ctx->gp;
+    na.gw = ctx->gw;
+    na.Q = ctx->Q;
+    na.k = op->k;
+    na.k2 = op->k2;
+    na.quirk = op->quirk;
+    na.mode = mode;
+    na.out = (double*)out;
+    na.ld = ld;
+    na.scale = scale;
+    na.out_t = (double*)out_t;
+    na.scale_t = scale_t;
+    na.x = (const double*)x;
+    na.y = (double*)y;
+    na.conj_x = conj_x;
+
+    bool helm = op->kernel == BEM_KERNEL_HELMHOLTZ;
+    switch (op->op) {
+        case BEM_OP_V: return dispatch_helm<BEM_OP_V>(ctx, helm, test->nb, trial->nb, fa, na, fp32, s);
+        case BEM_OP_K: return dispatch_helm<BEM_OP_K>(ctx, helm, test->nb, trial->nb, fa, na, fp32, s);
+        case BEM_OP_KP: return dispatch_helm<BEM_OP_KP>(ctx, helm, test->nb, trial->nb, fa, na, fp32, s);
+        case BEM_OP_W: return dispatch_helm<BEM_OP_W>(ctx, helm, test->nb, trial->nb, fa, na, fp32, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "unknown operator");
+    }
+}
+
+int bem_launch_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int is_complex, int mode, void* out,
+                    int64_t ld, double scale, void* out_t, double scale_t, const void* x, void* y, int conj_x,
+                    cudaStream_t s) {
+    MassArgs m;
+    m.n_panels = test->n_panels;
+    m.panels = test->panels;
+    m.nbx = test->nb;
+    m.nby = trial->nb;
+    m.test_dof = test->dof;
+    m.trial_dof = trial->dof;
+    m.area = ctx->area;
+    m.gp = ctx->gp;
+    m.gw = ctx->gw;
+    m.Q = ctx->Q;
+    m.cplx = is_complex;
+    m.mode = mode;
+    m.out = (double*)out;
+    m.ld = ld;
+    m.scale = scale;
+    m.out_t = (double*)out_t;
+    m.scale_t = scale_t;
+    m.x = (const double*)x;
+    m.y = (double*)y;
+    m.conj_x = conj_x;
+    int total = m.n_panels * m.nbx * m.nby;
+    if (total == 0) return BEM_OK;
+    mass_kernel<<<(total + 127) / 128, 128, 0, s>>>(m);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "mass_kernel launch");
+}

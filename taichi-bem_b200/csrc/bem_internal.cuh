@@ -1,0 +1,80 @@
+// Internal declarations shared by the bem_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/bem_b200.h"
+
+#define BEM_PI 3.14159265358979323846
+#define BEM_INV4PI 0.079577471545947667884  // 1 / (4 pi)
+
+// Maximum Gauss order (the reference ships tables for 1..8 and 12).
+#define BEM_MAX_Q 12
+
+struct bem_ctx {
+    std::string err;
+    int64_t launches = 0;
+    int device = 0;
+    int num_sms = 148;
+
+    // ---- mesh (device) ----
+    int nv = 0, nt = 0, Q = 0, Q2 = 0;
+    double* verts = nullptr;     // [nv*3]
+    int32_t* tris = nullptr;     // [nt*3]
+    double* area = nullptr;      // [nt]
+    double* normal = nullptr;    // [nt*3]
+    double* centroid = nullptr;  // [nt*3]
+    double* curl = nullptr;      // [nt*9]  curl of P1 hat b: [p*9 + b*3 + c]
+    double4* pts64 = nullptr;    // [nt*Q2] separate-rule point offset from centroid (xyz) + weight (w)
+    float4* pts32 = nullptr;     // [nt*Q2] same in FP32
+    double* phi64 = nullptr;     // [Q2*3] P1 hat values at the separate-rule points
+    float* phi32 = nullptr;      // [Q2*3]
+    double* gp = nullptr;        // [Q]   Gauss points on [0,1]
+    double* gw = nullptr;        // [Q]   Gauss weights on [0,1]
+    int64_t n_near = 0;
+    int4* near = nullptr;        // [n_near] (i, j, rel, perm bits)
+
+    // ---- workspace (device) ----
+    int32_t* test_local = nullptr;   // [nt] global panel -> local test index, -1 = absent
+    int32_t* trial_local = nullptr;  // [nt]
+    int32_t* flags = nullptr;        // [16] device-side status words
+    void* ws = nullptr;              // linear-algebra workspace
+    size_t ws_bytes = 0;
+};
+
+// Host helpers (bem_api.cu)
+int bem_fail(bem_ctx* ctx, int code, const std::string& msg);
+int bem_check_cuda(bem_ctx* ctx, cudaError_t e, const char* what);
+int bem_ws_reserve(bem_ctx* ctx, size_t bytes);
+
+// Launch wrappers (bem_assembly.cu)
+int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s);
+int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                        int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
+                        void* y, int conj_x, cudaStream_t s);
+int bem_launch_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int is_complex, int mode, void* out,
+                    int64_t ld, double scale, void* out_t, double scale_t, const void* x, void* y, int conj_x,
+                    cudaStream_t s);
+
+// Relation / near-pair encoding shared by host and device.
+enum { REL_SEPARATE = 0, REL_COINCIDE = 1, REL_VERTEX = 2, REL_EDGE = 3 };
+
+__host__ __device__ inline int bem_relation(const int32_t* a, const int32_t* b, bool same) {
+    // get_panels_relation, src/managers/mesh_manager.py:538-573 (3D branch)
+    if (same) return REL_COINCIDE;
+    int rel = REL_SEPARATE;
+    bool cv = false;
+    for (int ii = 0; ii < 3; ++ii) {
+        int a1 = a[ii], a2 = a[(ii + 1) % 3];
+        for (int jj = 0; jj < 3; ++jj) {
+            int b1 = b[jj], b2 = b[(jj + 1) % 3];
+            if ((a1 == b1 && a2 == b2) || (a1 == b2 && a2 == b1)) rel = REL_EDGE;
+            if (a1 == b1) cv = true;
+        }
+    }
+    if (cv && rel != REL_EDGE) rel = REL_VERTEX;
+    return rel;
+}

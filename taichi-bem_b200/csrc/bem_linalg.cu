@@ -1,0 +1,712 @@
+// Dense LU with partial pivoting, triangular solves, GEMV and mixed-precision
+// iterative refinement (replaces torch.linalg.solve at
+// src/managers/BEM_manager.py:1056; no cuSOLVER).
+//
+// Factorisation (right-looking, block width LU_NB):
+//   panel   : one cooperative launch per column panel; each CTA owns a slice
+//             of the panel's rows; per column one grid barrier publishes every
+//             CTA's pivot candidate, after which all CTAs agree on the pivot,
+//             swap it in and apply the rank-1 update to their rows.
+//   laswp   : the panel's row swaps applied to the columns outside the panel.
+//   trsm    : U12 = L11^-1 A12, L11 staged in shared memory.
+//   update  : A22 -= L21 U12 (bem_gemm.cu: FP64 SIMT tiles for the plain path,
+//             tcgen05 TF32 tensor-core tiles for the FP32 factor).
+// Every device-side wait (grid barriers) is bounded; a timeout sets a flag and
+// the host call returns BEM_ERR_TIMEOUT.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "bem_gemm.cuh"
+#include "bem_internal.cuh"
+
+namespace {
+
+constexpr int LU_NB = 64;
+constexpr unsigned SPIN_CAP = 1u << 22;  // x ~256 ns sleep ~ 1 s
+
+struct GridBar {
+    unsigned count;
+    unsigned gen;
+};
+
+// Bounded software grid barrier (the launch is cooperative, so all CTAs are
+// co-resident).  Returns false when the wait hit its cap (flag set).
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int32_t* flag) {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &bar->gen;
+        unsigned g = *vgen;
+        __threadfence();
+        unsigned arrived = atomicAdd(&bar->count, 1u);
+        int ok = 1;
+        if (arrived == nblocks - 1) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            unsigned it = 0;
+            while (*vgen == g) {
+                if (*(volatile int32_t*)flag != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (++it > SPIN_CAP) {
+                    atomicExch(flag, BEM_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <typename T, bool C>
+struct El {
+    T re, im;
+};
+
+template <typename T, bool C>
+__device__ __forceinline__ El<T, C> ld(const T* A, int64_t i) {
+    El<T, C> e;
+    if (C) {
+        e.re = A[2 * i];
+        e.im = A[2 * i + 1];
+    } else {
+        e.re = A[i];
+        e.im = T(0);
+    }
+    return e;
+}
+template <typename T, bool C>
+__device__ __forceinline__ void st(T* A, int64_t i, El<T, C> e) {
+    if (C) {
+        A[2 * i] = e.re;
+        A[2 * i + 1] = e.im;
+    } else {
+        A[i] = e.re;
+    }
+}
+template <typename T, bool C>
+__device__ __forceinline__ T mag1(El<T, C> e) {
+    return C ? fabs(e.re) + fabs(e.im) : fabs(e.re);
+}
+
+struct PivSlot {
+    double val;
+    int idx;
+    int pad;
+};
+
+// ----------------------------------------------------------------------------
+// panel factorisation (cooperative)
+// ----------------------------------------------------------------------------
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int64_t lda, int n, int k0, int nb, int32_t* piv,
+                                                       int32_t* info, GridBar* bar, PivSlot* slots, int32_t* flag) {
+    using E = El<T, C>;
+    const unsigned nblk = gridDim.x;
+    const int rows = n - k0;
+    const int chunk = (rows + nblk - 1) / nblk;
+    const int r_begin = k0 + blockIdx.x * chunk;
+    const int r_end = min(n, r_begin + chunk);
+    __shared__ E s_prow[LU_NB];  // old pivot row (panel columns)
+    __shared__ E s_jrow[LU_NB];  // old row jj
+    __shared__ double s_red_v[8];
+    __shared__ int s_red_i[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+
+    for (int j = 0; j < nb; ++j) {
+        const int jj = k0 + j;
+        // 1. local pivot candidate
+        double best = -1.0;
+        int bidx = 0x7fffffff;
+        for (int r = max(r_begin, jj) + threadIdx.x; r < r_end; r += blockDim.x) {
+            double v = (double)mag1<T, C>(ld<T, C>(A, (int64_t)r * lda + jj));
+            if (v > best || (v == best && r < bidx)) {
+                best = v;
+                bidx = r;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+            if (ov > best || (ov == best && oi < bidx)) {
+                best = ov;
+                bidx = oi;
+            }
+        }
+        if (lane == 0) {
+            s_red_v[wid] = best;
+            s_red_i[wid] = bidx;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+                if (s_red_v[w] > best || (s_red_v[w] == best && s_red_i[w] < bidx)) {
+                    best = s_red_v[w];
+                    bidx = s_red_i[w];
+                }
+            slots[blockIdx.x].val = best;
+            slots[blockIdx.x].idx = bidx;
+        }
+        // 2. publish
+        if (!grid_barrier(bar, nblk, flag)) return;
+        // 3. global pivot (every CTA computes the same answer)
+        __shared__ int s_p;
+        __shared__ double s_pv;
+        if (threadIdx.x == 0) {
+            double bv = -1.0;
+            int bi = 0x7fffffff;
+            for (unsigned b = 0; b < nblk; ++b) {
+                double v = ((volatile PivSlot*)slots)[b].val;
+                int i = ((volatile PivSlot*)slots)[b].idx;
+                if (v > bv || (v == bv && i < bi)) {
+                    bv = v;
+                    bi = i;
+                }
+            }
+            if (bi < jj || bi >= n) bi = jj;
+            s_p = bi;
+            s_pv = bv;
+            if (blockIdx.x == 0) {
+                piv[jj] = bi;
+                if (!(bv > 0.0) && *info == 0) *info = jj + 1;
+            }
+        }
+        __syncthreads();
+        const int p = s_p;
+        // 4. both rows (all panel columns) into shared memory, then swap
+        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
+            s_prow[c] = ld<T, C>(A, (int64_t)p * lda + k0 + c);
+            s_jrow[c] = ld<T, C>(A, (int64_t)jj * lda + k0 + c);
+        }
+        __syncthreads();
+        if (p != jj) {
+            if (jj >= r_begin && jj < r_end)
+                for (int c = threadIdx.x; c < nb; c += blockDim.x) st<T, C>(A, (int64_t)jj * lda + k0 + c, s_prow[c]);
+            if (p >= r_begin && p < r_end)
+                for (int c = threadIdx.x; c < nb; c += blockDim.x) st<T, C>(A, (int64_t)p * lda + k0 + c, s_jrow[c]);
+        }
+        __syncthreads();
+        // 5. scale column jj below the diagonal and rank-1 update of the panel
+        const E pv = s_prow[j];
+        const bool nonzero = s_pv > 0.0;
+        // reciprocal of the pivot
+        E inv;
+        if (C) {
+            T d = pv.re * pv.re + pv.im * pv.im;
+            inv.re = nonzero ? pv.re / d : T(0);
+            inv.im = nonzero ? -pv.im / d : T(0);
+        } else {
+            inv.re = nonzero ? T(1) / pv.re : T(0);
+            inv.im = T(0);
+        }
+        const int nwarps = blockDim.x >> 5;
+        for (int r = max(r_begin, jj + 1) + wid; r < r_end; r += nwarps) {
+            T* row = A + (C ? 2 : 1) * ((int64_t)r * lda + k0);
+            E a = ld<T, C>(row, j);
+            E l;
+            l.re = a.re * inv.re - (C ? a.im * inv.im : T(0));
+            l.im = C ? a.re * inv.im + a.im * inv.re : T(0);
+            for (int c = j + 1 + lane; c < nb; c += 32) {
+                E v = ld<T, C>(row, c);
+                E u = s_prow[c];
+                v.re -= l.re * u.re - (C ? l.im * u.im : T(0));
+                if (C) v.im -= l.re * u.im + l.im * u.re;
+                st<T, C>(row, c, v);
+            }
+            if (lane == 0) st<T, C>(row, j, l);
+        }
+        // the next column's barrier publishes these writes
+    }
+}
+
+// row swaps of one panel applied to the columns outside it
+template <typename T, bool C>
+__global__ void laswp_kernel(T* A, int64_t lda, int n, int k0, int nb, const int32_t* piv) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || (c >= k0 && c < k0 + nb)) return;
+    for (int j = 0; j < nb; ++j) {
+        int r1 = k0 + j, r2 = piv[k0 + j];
+        if (r1 == r2) continue;
+        El<T, C> a = ld<T, C>(A, (int64_t)r1 * lda + c);
+        El<T, C> b = ld<T, C>(A, (int64_t)r2 * lda + c);
+        st<T, C>(A, (int64_t)r1 * lda + c, b);
+        st<T, C>(A, (int64_t)r2 * lda + c, a);
+    }
+}
+
+// U12 = L11^{-1} A12 (unit lower L11 = rows/cols k0..k0+nb)
+template <typename T, bool C>
+__global__ void __launch_bounds__(128) trsm_kernel(T* A, int64_t lda, int n, int k0, int nb) {
+    using E = El<T, C>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    E* L = reinterpret_cast<E*>(smem_raw);  // [nb][nb]
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        int r = idx / nb, c = idx - r * nb;
+        L[idx] = ld<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c);
+    }
+    __syncthreads();
+    int col = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= n) return;
+    // column in registers would need nb values; keep the running solution in
+    // global memory (the column is written back in place row by row)
+    for (int r = 1; r < nb; ++r) {
+        E acc = ld<T, C>(A, (int64_t)(k0 + r) * lda + col);
+        for (int q = 0; q < r; ++q) {
+            E l = L[r * nb + q];
+            E x = ld<T, C>(A, (int64_t)(k0 + q) * lda + col);
+            acc.re -= l.re * x.re - (C ? l.im * x.im : T(0));
+            if (C) acc.im -= l.re * x.im + l.im * x.re;
+        }
+        st<T, C>(A, (int64_t)(k0 + r) * lda + col, acc);
+    }
+}
+
+// perm[i] = original row that ends up at row i after the LAPACK swap sequence
+__global__ void piv_to_perm_kernel(const int32_t* piv, int32_t* perm, int n) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int i = 0; i < n; ++i) {
+        int p = piv[i];
+        if (p != i && p >= 0 && p < n) {
+            int t = perm[i];
+            perm[i] = perm[p];
+            perm[p] = t;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// triangular solves: x = U^{-1} L^{-1} P b, one cooperative launch.
+// Vectors are FP64 (real or complex) whatever the factor storage type.
+// ----------------------------------------------------------------------------
+constexpr int TRSV_NB = 64;
+
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) lu_solve_kernel(const T* LU, int64_t lda, int n, const int32_t* perm,
+                                                        const double* b, double* x, double* tmp, int64_t nrhs,
+                                                        int64_t ldb, GridBar* bar, int32_t* flag) {
+    const unsigned nblk = gridDim.x;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nwarp_total = nblk * (blockDim.x >> 5);
+    const int W = C ? 2 : 1;
+    // y = P b  (x used as the work vector)
+    for (int64_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < (int64_t)n * nrhs;
+         idx += (int64_t)nblk * blockDim.x) {
+        int i = (int)(idx / nrhs), c = (int)(idx % nrhs);
+        int src = perm[i];
+        for (int w = 0; w < W; ++w) x[W * ((int64_t)i * ldb + c) + w] = b[W * ((int64_t)src * ldb + c) + w];
+    }
+    if (!grid_barrier(bar, nblk, flag)) return;
+    const int nblocks_r = (n + TRSV_NB - 1) / TRSV_NB;
+    // forward: L y = P b (unit diagonal)
+    for (int kb = 0; kb < nblocks_r; ++kb) {
+        const int r0 = kb * TRSV_NB, r1 = min(n, r0 + TRSV_NB);
+        if (blockIdx.x == 0 && (threadIdx.x >> 5) < nrhs) {
+            const int c = threadIdx.x >> 5;
+            for (int r = r0 + 1; r < r1; ++r) {
+                double sr = 0.0, si = 0.0;
+                for (int q = r0 + lane; q < r; q += 32) {
+                    El<T, C> l = ld<T, C>(LU, (int64_t)r * lda + q);
+                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
+                    sr += (double)l.re * xr - (C ? (double)l.im * xi : 0.0);
+                    if (C) si += (double)l.re * xi + (double)l.im * xr;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                    if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
+                }
+                if (lane == 0) {
+                    x[W * ((int64_t)r * ldb + c)] -= sr;
+                    if (C) x[W * ((int64_t)r * ldb + c) + 1] -= si;
+                }
+                __syncwarp();
+            }
+        }
+        if (!grid_barrier(bar, nblk, flag)) return;
+        // rows below: x[i] -= L[i, r0:r1] x[r0:r1]
+        for (int i = r1 + gwarp; i < n; i += nwarp_total) {
+            for (int c = 0; c < nrhs; ++c) {
+                double sr = 0.0, si = 0.0;
+                for (int q = r0 + lane; q < r1; q += 32) {
+                    El<T, C> l = ld<T, C>(LU, (int64_t)i * lda + q);
+                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
+                    sr += (double)l.re * xr - (C ? (double)l.im * xi : 0.0);
+                    if (C) si += (double)l.re * xi + (double)l.im * xr;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                    if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
+                }
+                if (lane == 0) {
+                    x[W * ((int64_t)i * ldb + c)] -= sr;
+                    if (C) x[W * ((int64_t)i * ldb + c) + 1] -= si;
+                }
+            }
+        }
+        if (!grid_barrier(bar, nblk, flag)) return;
+    }
+    // backward: U x = y
+    for (int kb = nblocks_r - 1; kb >= 0; --kb) {
+        const int r0 = kb * TRSV_NB, r1 = min(n, r0 + TRSV_NB);
+        if (blockIdx.x == 0 && (threadIdx.x >> 5) < nrhs) {
+            const int c = threadIdx.x >> 5;
+            for (int r = r1 - 1; r >= r0; --r) {
+                double sr = 0.0, si = 0.0;
+                for (int q = r + 1 + lane; q < r1; q += 32) {
+                    El<T, C> u = ld<T, C>(LU, (int64_t)r * lda + q);
+                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
+                    sr += (double)u.re * xr - (C ? (double)u.im * xi : 0.0);
+                    if (C) si += (double)u.re * xi + (double)u.im * xr;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                    if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
+                }
+                if (lane == 0) {
+                    El<T, C> d = ld<T, C>(LU, (int64_t)r * lda + r);
+                    double vr = x[W * ((int64_t)r * ldb + c)] - sr;
+                    double vi = C ? x[W * ((int64_t)r * ldb + c) + 1] - si : 0.0;
+                    if (C) {
+                        double dr = d.re, di = d.im, den = dr * dr + di * di;
+                        x[W * ((int64_t)r * ldb + c)] = (vr * dr + vi * di) / den;
+                        x[W * ((int64_t)r * ldb + c) + 1] = (vi * dr - vr * di) / den;
+                    } else {
+                        x[(int64_t)r * ldb + c] = vr / (double)d.re;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (!grid_barrier(bar, nblk, flag)) return;
+        for (int i = gwarp; i < r0; i += nwarp_total) {
+            for (int c = 0; c < nrhs; ++c) {
+                double sr = 0.0, si = 0.0;
+                for (int q = r0 + lane; q < r1; q += 32) {
+                    El<T, C> u = ld<T, C>(LU, (int64_t)i * lda + q);
+                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
+                    sr += (double)u.re * xr - (C ? (double)u.im * xi : 0.0);
+                    if (C) si += (double)u.re * xi + (double)u.im * xr;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                    if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
+                }
+                if (lane == 0) {
+                    x[W * ((int64_t)i * ldb + c)] -= sr;
+                    if (C) x[W * ((int64_t)i * ldb + c) + 1] -= si;
+                }
+            }
+        }
+        if (!grid_barrier(bar, nblk, flag)) return;
+    }
+    (void)tmp;
+}
+
+// y = alpha A x + beta y, A stored as T (real/complex), x/y FP64
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) gemv_kernel(const T* A, int64_t m, int64_t n, int64_t lda, const double* x,
+                                                    double* y, double alpha, double beta) {
+    const int lane = threadIdx.x & 31;
+    const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= m) return;
+    double sr = 0.0, si = 0.0;
+    const T* a = A + (C ? 2 : 1) * row * lda;
+    for (int64_t q = lane; q < n; q += 32) {
+        El<T, C> e = ld<T, C>(a, q);
+        double xr = C ? x[2 * q] : x[q], xi = C ? x[2 * q + 1] : 0.0;
+        sr += (double)e.re * xr - (C ? (double)e.im * xi : 0.0);
+        if (C) si += (double)e.re * xi + (double)e.im * xr;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) {
+        if (C) {
+            double yr = beta == 0.0 ? 0.0 : beta * y[2 * row];
+            double yi = beta == 0.0 ? 0.0 : beta * y[2 * row + 1];
+            y[2 * row] = yr + alpha * sr;
+            y[2 * row + 1] = yi + alpha * si;
+        } else {
+            double yr = beta == 0.0 ? 0.0 : beta * y[row];
+            y[row] = yr + alpha * sr;
+        }
+    }
+}
+
+__global__ void sumsq_kernel(const double* v, int64_t n, double* out) {
+    __shared__ double s[8];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += v[i] * v[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
+        atomicAdd(out, t);
+    }
+}
+
+__global__ void axpy_kernel(double* y, const double* x, int64_t n, double a) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) y[i] += a * x[i];
+}
+
+struct LinWs {
+    GridBar* bar;
+    PivSlot* slots;
+    int32_t* perm;
+    double* vec;  // scratch vectors for refinement
+};
+
+int linws(bem_ctx* ctx, int64_t n, int64_t nvec_doubles, LinWs* w) {
+    size_t off_bar = 0;
+    size_t off_slots = 256;
+    size_t off_perm = off_slots + sizeof(PivSlot) * 2048;
+    size_t off_vec = (off_perm + sizeof(int32_t) * (size_t)n + 255) & ~size_t(255);
+    size_t total = off_vec + sizeof(double) * (size_t)nvec_doubles;
+    if (int rc = bem_ws_reserve(ctx, total)) return rc;
+    char* base = (char*)ctx->ws;
+    w->bar = (GridBar*)(base + off_bar);
+    w->slots = (PivSlot*)(base + off_slots);
+    w->perm = (int32_t*)(base + off_perm);
+    w->vec = (double*)(base + off_vec);
+    return BEM_OK;
+}
+
+int coop_blocks(bem_ctx* ctx, const void* fn, int threads, size_t smem, int want) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+    int maxb = per_sm * ctx->num_sms;
+    if (maxb < 1) return 0;
+    return std::max(1, std::min(want, std::min(maxb, ctx->num_sms)));
+}
+
+int check_flag(bem_ctx* ctx, cudaStream_t s, const char* what) {
+    int32_t f = 0;
+    if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(&f, ctx->flags + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                                "flag readback"))
+        return rc;
+    if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), what)) return rc;
+    if (f != 0) {
+        cudaMemsetAsync(ctx->flags + 2, 0, sizeof(int32_t), s);
+        return bem_fail(ctx, BEM_ERR_TIMEOUT, std::string(what) + ": device wait hit its iteration cap");
+    }
+    return BEM_OK;
+}
+
+template <typename T, bool C>
+int lu_factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, int32_t* info, cudaStream_t s) {
+    LinWs w;
+    if (int rc = linws(ctx, n, 0, &w)) return rc;
+    cudaMemsetAsync(w.bar, 0, sizeof(GridBar), s);
+    cudaMemsetAsync(info, 0, sizeof(int32_t), s);
+    cudaMemsetAsync(ctx->flags + 2, 0, sizeof(int32_t), s);
+    const int threads = 256;
+    int nblk = coop_blocks(ctx, (const void*)lu_panel_kernel<T, C>, threads, 0, ctx->num_sms);
+    if (nblk < 1) return bem_fail(ctx, BEM_ERR_CUDA, "lu_panel_kernel cannot be made co-resident");
+    int32_t* flag = ctx->flags + 2;
+    for (int64_t k0 = 0; k0 < n; k0 += LU_NB) {
+        int nb = (int)std::min<int64_t>(LU_NB, n - k0);
+        int rows = (int)(n - k0);
+        int blocks = std::min(nblk, std::max(1, (rows + 31) / 32));
+        int ni = (int)n, k0i = (int)k0;
+        void* args[] = {&A, &lda, &ni, &k0i, &nb, &piv, &info, &w.bar, &w.slots, &flag};
+        if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)lu_panel_kernel<T, C>, blocks,
+                                                                    threads, args, 0, s),
+                                    "lu_panel_kernel"))
+            return rc;
+        ctx->launches++;
+        laswp_kernel<T, C><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, lda, ni, k0i, nb, piv);
+        ctx->launches++;
+        int64_t rest = n - k0 - nb;
+        if (rest > 0) {
+            size_t smem = sizeof(El<T, C>) * nb * nb;
+            if (smem > 48 * 1024)
+                cudaFuncSetAttribute(trsm_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            trsm_kernel<T, C><<<(unsigned)((rest + 127) / 128), 128, smem, s>>>(A, lda, ni, k0i, nb);
+            ctx->launches++;
+            // A22 -= L21 U12
+            T* A22 = A + (C ? 2 : 1) * ((k0 + nb) * lda + k0 + nb);
+            const T* L21 = A + (C ? 2 : 1) * ((k0 + nb) * lda + k0);
+            const T* U12 = A + (C ? 2 : 1) * (k0 * lda + k0 + nb);
+            if (int rc = bem_gemm_update<T, C>(ctx, A22, L21, U12, rest, rest, nb, lda, s)) return rc;
+        }
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "lu step")) return rc;
+    }
+    return check_flag(ctx, s, "lu_factor");
+}
+
+template <typename T, bool C>
+int lu_solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t* piv, double* b, int64_t nrhs,
+               int64_t ldb, cudaStream_t s) {
+    if (nrhs < 1 || nrhs > 8) return bem_fail(ctx, BEM_ERR_INVALID, "lu_solve supports 1..8 right-hand sides");
+    const int W = C ? 2 : 1;
+    LinWs w;
+    if (int rc = linws(ctx, n, (int64_t)W * n * ldb, &w)) return rc;
+    cudaMemsetAsync(w.bar, 0, sizeof(GridBar), s);
+    cudaMemsetAsync(ctx->flags + 2, 0, sizeof(int32_t), s);
+    piv_to_perm_kernel<<<1, 1, 0, s>>>(piv, w.perm, (int)n);
+    ctx->launches++;
+    const int threads = 256;
+    int nblk = coop_blocks(ctx, (const void*)lu_solve_kernel<T, C>, threads, 0, ctx->num_sms);
+    if (nblk < 1) return bem_fail(ctx, BEM_ERR_CUDA, "lu_solve_kernel cannot be made co-resident");
+    int ni = (int)n;
+    double* xw = w.vec;
+    double* tmp = nullptr;
+    int32_t* flag = ctx->flags + 2;
+    const double* bc = b;
+    void* args[] = {(void*)&LU, &lda, &ni, &w.perm, &bc, &xw, &tmp, &nrhs, &ldb, &w.bar, &flag};
+    if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)lu_solve_kernel<T, C>, nblk, threads,
+                                                                args, 0, s),
+                                "lu_solve_kernel"))
+        return rc;
+    ctx->launches++;
+    if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(b, xw, sizeof(double) * W * n * ldb, cudaMemcpyDeviceToDevice, s),
+                                "lu_solve copy"))
+        return rc;
+    return check_flag(ctx, s, "lu_solve");
+}
+
+template <typename T, bool C>
+int gemv_t(bem_ctx* ctx, const T* A, int64_t m, int64_t n, int64_t lda, const double* x, double* y, double alpha,
+           double beta, cudaStream_t s) {
+    unsigned blocks = (unsigned)((m + 7) / 8);
+    gemv_kernel<T, C><<<blocks, 256, 0, s>>>(A, m, n, lda, x, y, alpha, beta);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "gemv_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+int bem_lu_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, int32_t* info,
+                  void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A || !piv || !info || n <= 0 || lda < n) return bem_fail(ctx, BEM_ERR_INVALID, "lu_factor: bad arguments");
+    if (n > (int64_t)1 << 30) return bem_fail(ctx, BEM_ERR_INVALID, "lu_factor: n too large");
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (dtype) {
+        case BEM_F64: return lu_factor_t<double, false>(ctx, (double*)A, n, lda, piv, info, s);
+        case BEM_C128: return lu_factor_t<double, true>(ctx, (double*)A, n, lda, piv, info, s);
+        case BEM_F32: return lu_factor_t<float, false>(ctx, (float*)A, n, lda, piv, info, s);
+        case BEM_C64: return lu_factor_t<float, true>(ctx, (float*)A, n, lda, piv, info, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "lu_factor: unknown dtype");
+    }
+}
+
+int bem_lu_solve(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv, void* b,
+                 int64_t nrhs, int64_t ldb, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!LU || !piv || !b || n <= 0 || lda < n || ldb < nrhs)
+        return bem_fail(ctx, BEM_ERR_INVALID, "lu_solve: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (dtype) {
+        case BEM_F64: return lu_solve_t<double, false>(ctx, (const double*)LU, n, lda, piv, (double*)b, nrhs, ldb, s);
+        case BEM_C128: return lu_solve_t<double, true>(ctx, (const double*)LU, n, lda, piv, (double*)b, nrhs, ldb, s);
+        case BEM_F32: return lu_solve_t<float, false>(ctx, (const float*)LU, n, lda, piv, (double*)b, nrhs, ldb, s);
+        case BEM_C64: return lu_solve_t<float, true>(ctx, (const float*)LU, n, lda, piv, (double*)b, nrhs, ldb, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "lu_solve: unknown dtype");
+    }
+}
+
+int bem_gemv(bem_ctx* ctx, int a_dtype, const void* A, int64_t m, int64_t n, int64_t lda, const void* x, void* y,
+             double alpha, double beta, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A || !x || !y || m <= 0 || n <= 0 || lda < n) return bem_fail(ctx, BEM_ERR_INVALID, "gemv: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (a_dtype) {
+        case BEM_F64: return gemv_t<double, false>(ctx, (const double*)A, m, n, lda, (const double*)x, (double*)y, alpha, beta, s);
+        case BEM_C128: return gemv_t<double, true>(ctx, (const double*)A, m, n, lda, (const double*)x, (double*)y, alpha, beta, s);
+        case BEM_F32: return gemv_t<float, false>(ctx, (const float*)A, m, n, lda, (const double*)x, (double*)y, alpha, beta, s);
+        case BEM_C64: return gemv_t<float, true>(ctx, (const float*)A, m, n, lda, (const double*)x, (double*)y, alpha, beta, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "gemv: unknown dtype");
+    }
+}
+
+int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv, int64_t n,
+                     int64_t lda, const void* b, void* x, double tol, int maxit, int* iters, double* relres,
+                     void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A_hi || !LU_lo || !piv || !b || !x || n <= 0 || lda < n || maxit < 1 || !(tol > 0))
+        return bem_fail(ctx, BEM_ERR_INVALID, "refine_solve: bad arguments");
+    if (dtype_hi != BEM_F64 && dtype_hi != BEM_C128)
+        return bem_fail(ctx, BEM_ERR_INVALID, "refine_solve: A_hi must be F64 or C128");
+    const bool C = dtype_hi == BEM_C128;
+    const int W = C ? 2 : 1;
+    const int64_t nd = W * n;
+    cudaStream_t s = (cudaStream_t)stream;
+    // workspace beyond the lu_solve scratch: r (nd), d (nd), norms (2)
+    double* r = nullptr;
+    if (int rc = bem_check_cuda(ctx, cudaMallocAsync((void**)&r, sizeof(double) * (2 * nd + 4), s), "refine alloc"))
+        return rc;
+    double* d = r + nd;
+    double* nrm = d + nd;
+    const double* bd = (const double*)b;
+    double* xd = (double*)x;
+    int rc = BEM_OK;
+    double bnorm = 0.0, rnorm = 0.0;
+    int it = 0;
+    auto norm2 = [&](const double* v, double* out_host) -> int {
+        cudaMemsetAsync(nrm, 0, sizeof(double), s);
+        sumsq_kernel<<<std::min<int64_t>(ctx->num_sms * 4, (nd + 255) / 256), 256, 0, s>>>(v, nd, nrm);
+        ctx->launches++;
+        if (int e = bem_check_cuda(ctx, cudaMemcpyAsync(out_host, nrm, sizeof(double), cudaMemcpyDeviceToHost, s),
+                                   "norm readback"))
+            return e;
+        if (int e = bem_check_cuda(ctx, cudaStreamSynchronize(s), "norm")) return e;
+        *out_host = std::sqrt(*out_host);
+        return BEM_OK;
+    };
+    rc = norm2(bd, &bnorm);
+    if (rc == BEM_OK) rc = bem_check_cuda(ctx, cudaMemsetAsync(xd, 0, sizeof(double) * nd, s), "x=0");
+    if (rc == BEM_OK) rc = bem_check_cuda(ctx, cudaMemcpyAsync(r, bd, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "r=b");
+    rnorm = bnorm;
+    if (bnorm == 0.0) {
+        cudaFreeAsync(r, s);
+        if (iters) *iters = 0;
+        if (relres) *relres = 0.0;
+        return rc;
+    }
+    while (rc == BEM_OK && it < maxit) {
+        // d = LU_lo^{-1} r
+        rc = bem_check_cuda(ctx, cudaMemcpyAsync(d, r, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "d=r");
+        if (rc) break;
+        rc = bem_lu_solve(ctx, C ? BEM_C64 : BEM_F32, LU_lo, n, lda, piv, d, 1, 1, s);
+        if (rc) break;
+        axpy_kernel<<<(unsigned)((nd + 255) / 256), 256, 0, s>>>(xd, d, nd, 1.0);
+        ctx->launches++;
+        // r = b - A_hi x
+        rc = bem_check_cuda(ctx, cudaMemcpyAsync(r, bd, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "r=b");
+        if (rc) break;
+        rc = bem_gemv(ctx, dtype_hi, A_hi, n, n, lda, xd, r, -1.0, 1.0, s);
+        if (rc) break;
+        ++it;
+        rc = norm2(r, &rnorm);
+        if (rc) break;
+        if (rnorm <= tol * bnorm) break;
+    }
+    cudaFreeAsync(r, s);
+    if (iters) *iters = it;
+    if (relres) *relres = rnorm / bnorm;
+    if (rc == BEM_OK && rnorm > tol * bnorm)
+        return bem_fail(ctx, BEM_ERR_NOCONVERGE, "refinement did not reach tol in maxit iterations");
+    return rc;
+}
+
+}  // extern "C"

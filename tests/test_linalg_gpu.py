@@ -1,0 +1,88 @@
+"""Dense LU / triangular solves / refinement (libbem_b200) against numpy
+(LAPACK) on the same inputs."""
+import numpy as np
+import pytest
+import torch
+
+from tests._util import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from bem_b200.engine import Engine
+    e = Engine()
+    yield e
+    e.close()
+
+
+def _mat(n, cplx, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((n, n))
+    if cplx:
+        A = A + 1j * rng.standard_normal((n, n))
+    return A + n ** 0.5 * np.eye(n) * 0.5
+
+
+@pytest.mark.parametrize("n", [1, 37, 64, 200, 321])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_lu_fp64_solve(engine, n, cplx):
+    A = _mat(n, cplx, n)
+    rng = np.random.default_rng(7)
+    b = rng.standard_normal((n, 2)) + (1j * rng.standard_normal((n, 2)) if cplx else 0)
+    x_ref = np.linalg.solve(A, b)
+    Ad = torch.as_tensor(A, device="cuda").contiguous()
+    piv, info = engine.lu_factor(Ad)
+    assert int(info.item()) == 0
+    bd = torch.as_tensor(b, device="cuda").contiguous()
+    engine.lu_solve(Ad, piv, bd)
+    assert rel_err(bd.cpu().numpy(), x_ref) < 1e-11
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_lu_matches_lapack_factors(engine, cplx):
+    import scipy.linalg
+    n = 150
+    A = _mat(n, cplx, 3)
+    Ad = torch.as_tensor(A, device="cuda").contiguous()
+    piv, info = engine.lu_factor(Ad)
+    lu, piv_ref = scipy.linalg.lu_factor(A)
+    assert (piv.cpu().numpy() == piv_ref).all()
+    assert rel_err(Ad.cpu().numpy(), lu) < 1e-12
+
+
+def test_lu_singular_reports_info(engine):
+    A = np.ones((10, 10))
+    Ad = torch.as_tensor(A, device="cuda").contiguous()
+    piv, info = engine.lu_factor(Ad)
+    assert int(info.item()) > 0
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_fp32_factor_with_fp64_refinement(engine, cplx):
+    n = 300
+    A = _mat(n, cplx, 11)
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(n) + (1j * rng.standard_normal(n) if cplx else 0)
+    x_ref = np.linalg.solve(A, b)
+    A_hi = torch.as_tensor(A, device="cuda").contiguous()
+    LU = A_hi.to(torch.complex64 if cplx else torch.float32).contiguous()
+    piv, info = engine.lu_factor(LU)
+    assert int(info.item()) == 0
+    bd = torch.as_tensor(b, device="cuda").contiguous()
+    xd = torch.zeros_like(bd)
+    it, rr = engine.refine_solve(A_hi, LU, piv, bd, xd, tol=1e-13, maxit=30)
+    assert rr <= 1e-13 and it >= 1
+    assert rel_err(xd.cpu().numpy(), x_ref) < 1e-11
+
+
+def test_gemv(engine):
+    rng = np.random.default_rng(2)
+    A = rng.standard_normal((70, 50)) + 1j * rng.standard_normal((70, 50))
+    x = rng.standard_normal(50) + 1j * rng.standard_normal(50)
+    y0 = rng.standard_normal(70) + 1j * rng.standard_normal(70)
+    Ad = torch.as_tensor(A, device="cuda")
+    yd = torch.as_tensor(y0.copy(), device="cuda")
+    engine.gemv(Ad, torch.as_tensor(x, device="cuda"), yd, alpha=-2.0, beta=0.5)
+    assert rel_err(yd.cpu().numpy(), 0.5 * y0 - 2.0 * A @ x) < 1e-13

@@ -1,0 +1,57 @@
+"""Pin the CPU oracle to the reference: every golden fixture was produced by
+running the reference's own kernels (tests/golden/gen_golden.py)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._util import FIXTURES, data_callbacks, load_fixture, rel_err, to_complex
+
+TOL = 1e-12  # FP64 restatement vs the reference's algorithm in FP64
+
+
+def _problem(d, quirk=True):
+    params = eval(str(d["params"]))
+    fD, fN = data_callbacks(str(d["data_kind"]), float(params.get("k", 0.0)), d["direction"])
+    return O.Problem(d["vertices"], d["panels"], params, fD, fN, quirk=quirk)
+
+
+def test_gauss_tables_match_legendre():
+    for n in list(range(1, 9)) + [12]:
+        p, w = O.gauss(n)
+        x, wl = np.polynomial.legendre.leggauss(n)
+        assert np.allclose(p, (x + 1) / 2, atol=1e-15, rtol=0)
+        assert np.allclose(w, wl / 2, atol=1e-15, rtol=0)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_oracle_matches_reference(name):
+    d = load_fixture(name)
+    P = _problem(d)
+    assert (P.mesh.panel_types == d["panel_types"]).all()
+    assert (P.mesh.vert_types == d["vertice_types"]).all()
+    assert P.mesh.N_N == int(d["N_Neumann"]) and P.mesh.M_D == int(d["M_Dirichlet"])
+    assert np.allclose(P.mesh.panel_areas, d["panel_areas"], rtol=1e-14)
+    assert np.allclose(P.mesh.panel_normals, d["panel_normals"], atol=1e-14)
+    r = P.run()
+    nf = int(d["n_forward"])
+    for i in range(nf):
+        lay = r["layers"] if "layers" in r else (r["layers_o"] if i == 0 else r["layers_i"])
+        for key in ("V", "K", "W"):
+            if f"{key}_{i}" in d:
+                assert rel_err(lay[key], to_complex(d[f"{key}_{i}"])) < TOL, (key, i)
+    assert rel_err(r["A"], to_complex(d["A"])) < TOL
+    assert rel_err(r["rhs"], to_complex(d["rhs"])) < TOL
+    if "solve_error" in d:
+        assert r["raw_solved"] is None or np.linalg.cond(r["A"]) > 1e12
+    elif np.linalg.cond(r["A"]) < 1e8:
+        assert rel_err(r["raw_solved"], to_complex(d["raw_solved"])) < 1e-10
+
+
+def test_relation_rule_cube():
+    d = load_fixture("cube_lap_dir_q5")
+    tris = d["panels"]
+    for i in range(len(tris)):
+        for j in range(len(tris)):
+            shared = len(set(tris[i]) & set(tris[j]))
+            want = 1 if i == j else {0: 0, 1: 2, 2: 3, 3: 3}[shared]
+            assert O.relation(tris, i, j) == want
