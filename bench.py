@@ -1,0 +1,383 @@
+"""Benchmark: Galerkin BEM assembly + solve on B200.
+
+Workload (one GPU): Helmholtz 3D interior Dirichlet, k = 3, unit icosphere
+subdivision 4 (5120 panels, 2562 vertices), GaussQR = 5, plane-wave data
+exp(i k d.x) with a seeded random unit direction d.  One step = the whole hot
+path of BEMManager.run with inputs resident in HBM: single-layer assembly V
+(26.2 M complex entries; separate pairs in FP32, coincident/edge/vertex pairs
+in FP64), the matrix-free right-hand side 1/2 M g + K g, the FP32 LU factor and
+FP64 iterative refinement to relative residual 1e-12.
+
+  value  = V entries / time-to-solution (entries/s), device-timed with CUDA
+           events per step, L2 flushed (256 MiB write) between steps;
+  e2e    = the same metric through the public API (CoreManager with host mesh
+           and host-resident results: mesh upload, set-up, run, solution read
+           back), one full lifecycle per step;
+  plain_fp64 = the same step on the plain FP64 path (all quadrature and the LU
+           in FP64), whose solution is the FP64 oracle the mixed result's
+           relative error is quoted against.
+
+`--impl reference` times the reference's CPU algorithm (the oracle's FP32
+restatement of its loops, all host threads) on a bounded sample of the same
+workload.  Multi-GPU: one independent replica per rank (the dense solve does
+not shard); value = sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "taichi-bem_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "assembly entries/s + time-to-solution at ≤1e-6 rel err: mixed/batched vs plain GPU"
+WORKLOAD = "Helmholtz 3D interior Dirichlet k=3, icosphere s4 (5120 panels), GaussQR=5, plane wave"
+# Algorithmic FP32 operations per separate-pair kernel evaluation of the
+# Helmholtz single layer (far_kernel): 3 (x-y) + 5 (r^2) + 1 (r) + 1 (kr)
+# + 2 (e^{ikr}/r) + 4 (two weighted accumulations) = 16, plus rsqrt, sin, cos
+# counted as one operation each = 19.
+OPS_PER_EVAL = 19
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(steps: int, warmup: int, threads: int | None = None, sample_rows: int | None = None,
+                  target_s: float = 10.0):
+    """Reference algorithm on the host: the FP32 restatement of the reference's
+    loops (one outer iteration per test panel, serial over trial panels x
+    GaussQR^4, per-basis recompute) for V and the matrix-free K g of the
+    workload, on a sample of test panels; scaled to entries/s."""
+    import numpy as np
+
+    from bem_b200 import icosphere
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    O.set_threads(threads)
+    v, f = icosphere(4)
+    nt, nv = len(f), len(v)
+    Q = 5
+    k = 3.0
+    panels = np.arange(nt, dtype=np.int32)
+
+    def one(rows):
+        tp = panels[:rows]
+        out = np.zeros((rows, nt), np.complex128)
+        t0 = time.perf_counter()
+        O.assemble(v, f, O.OP_V, True, k, k * k, Q, True, (tp, 1, tp.copy()), (panels, 1, panels.copy()), out=out,
+                   fp32=True)
+        g = np.exp(1j * k * (v @ np.array([0.0, 0.0, 1.0])))
+        y = np.zeros(rows, np.complex128)
+        O.assemble(v, f, O.OP_K, True, k, k * k, Q, True, (tp, 1, tp.copy()),
+                   (panels, 3, f.reshape(-1).astype(np.int32)), x=g, y=y, conj_x=True, fp32=True)
+        return time.perf_counter() - t0
+
+    # size the sample so that one timed sample is ~`target_s` of CPU work
+    t1 = one(threads)
+    rows = sample_rows or int(min(nt, threads * max(1, round(target_s / max(t1, 1e-3)))))
+    for _ in range(warmup):
+        one(max(1, rows // 4))
+    times = [one(rows) for _ in range(steps)]
+    t = statistics.mean(times)
+    # entries/s of V assembled per second of (V + K g) work, as for the GPU step
+    value = rows * nt / t
+    return {"value": value, "unit": "entries/s", "cores": threads, "kind": "port",
+            "sample": f"{rows} of {nt} test panels (rows of V and K g), FP32, {steps} timed samples",
+            "seconds_per_sample": t}
+
+
+def phase_breakdown(b):
+    """Device time of each phase of one BEMManager.run step (CUDA events)."""
+    import torch
+    from bem_b200.utils.types import AssembleType
+    out = {}
+
+    def timed(name, fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1)
+        return r
+
+    b._mat_A.zero_()
+    timed("assemble_V", lambda: b.matrix_layer_forward(k=b._k, scope_type=b._scope_type))
+    timed("block_add", lambda: b.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0))
+    timed("boundary_data", lambda: b.rhs_constructor.set_boundaries(b._scope_type, b._sqrt_ni, b._sqrt_no))
+    timed("rhs_half_M_plus_K_g", lambda: b.rhs_layer_forward(k=b._k, scope_type=b._scope_type))
+    timed("rhs_copy", b.assemble_rhs)
+    A = b._mat_A
+    lo = torch.complex64 if A.is_complex() else torch.float32
+    LU = timed("cast_fp32", lambda: A.to(lo))
+    piv, dinv, info = timed("lu_factor_fp32_tiled", lambda: b.engine.lu_factor_tiled(LU))
+    x = torch.zeros_like(b.rhs)
+    timed("refine_fp64", lambda: b.engine.refine_solve(A, LU, piv, b.rhs, x, tol=b.refine_tol, maxit=b.refine_maxit,
+                                                       dinv=dinv))
+    xs = b.rhs.clone()
+    timed("lu_solve_fp32_tiled", lambda: b.engine.lu_solve_tiled(LU, piv, dinv, xs))
+    LU2 = A.to(lo)
+    timed("lu_factor_fp32_partial_pivoting", lambda: b.engine.lu_factor(LU2))
+    y = torch.zeros_like(b.rhs)
+    timed("gemv_c128", lambda: b.engine.gemv(A, x, y))
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    args = ap.parse_args()
+    ws, rank, local = _dist()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = {"metric": METRIC, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": {"workload": WORKLOAD, "host": "cpu"}}
+        cb = cpu_reference(args.steps, max(1, min(args.warmup, 1)))
+        base.update(value=cb["value"], unit="entries/s", ms_per_step=cb["seconds_per_sample"] * 1e3,
+                    cpu_baseline=cb, e2e={"value": cb["value"], "unit": "entries/s", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0})
+        print(json.dumps(base))
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from bem_b200.engine import measure_peaks
+    from bem_b200.managers import CoreManager
+    from bem_b200.workloads import config2
+
+    def make(precision, extra=None):
+        params, fD, fN = config2(precision=precision)
+        params["device"] = f"cuda:{local}"
+        if extra:
+            params.update(extra)
+        core = CoreManager(params)
+        core.initialization(fD, fN)
+        return core
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def flush_l2():
+        flush.fill_(1.0)
+
+    # ---- mixed path: device-timed steps ----
+    core = make("mixed")
+    b = core._BEM_manager
+    nt = b.num_of_panels
+    entries = nt * nt
+    eng = b.engine
+    peaks = measure_peaks(eng)
+    for _ in range(args.warmup):
+        b.run()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = eng.launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for s in range(args.steps):
+        flush_l2()
+        ev[s][0].record()
+        b.run()
+        ev[s][1].record()
+    torch.cuda.synchronize()
+    launches = eng.launches - launches0
+    step_ms = [a.elapsed_time(z) for a, z in ev]
+    # V assembly alone (the dominant kernel) for the roofline
+    va = []
+    for s in range(args.steps):
+        flush_l2()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.single_layer.forward(b._scope_type, b._k, 1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        va.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    breakdown = phase_breakdown(b)
+    info = dict(b.solve_info)
+    sol_mixed = b.raw_solved.clone()
+    ms = statistics.mean(step_ms)
+    if ws > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = entries / (ms * 1e-3) * ws
+
+    # ---- plain FP64 path (the FP64 oracle of the mixed result) ----
+    core64 = make("fp64")
+    b64 = core64._BEM_manager
+    b64.run()
+    torch.cuda.synchronize()
+    ms64 = []
+    for _ in range(2):
+        flush_l2()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b64.run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms64.append(e0.elapsed_time(e1))
+    va64 = []
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b64.single_layer.forward(b64._scope_type, b64._k, 1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        va64.append(e0.elapsed_time(e1))
+    sol64 = b64.raw_solved
+    rel = float((sol_mixed - sol64).abs().max() / sol64.abs().max())
+    rel2 = float(torch.linalg.norm(sol_mixed - sol64) / torch.linalg.norm(sol64))
+    core64.kill()
+
+    # ---- e2e through the public API, host inputs, solution read back ----
+    from bem_b200 import icosphere
+    vh, fh = icosphere(4)
+    vpin = torch.as_tensor(vh).pin_memory()
+    fpin = torch.as_tensor(fh).pin_memory()
+    e2e_ms = []
+    h2d = vh.nbytes + fh.nbytes
+    d2h = 0
+    for s in range(max(2, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        params, fD, fN = config2(precision="mixed")
+        params.update(device=f"cuda:{local}", vertices=vpin.numpy(), panels=fpin.numpy())
+        c2 = CoreManager(params)
+        c2.initialization(fD, fN)
+        c2._BEM_manager.run()
+        host = c2._BEM_manager.raw_solved.to("cpu")
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        d2h = host.numel() * host.element_size()
+        c2.kill()
+    e2e = statistics.mean(e2e_ms[1:]) if len(e2e_ms) > 1 else e2e_ms[0]
+
+    # roofline of the dominant kernel: V far field (FP32) in assembly
+    q4 = 625
+    near = eng.near_pairs
+    evals = (nt * nt - near) * q4
+    va_ms = statistics.mean(va)
+    achieved = evals * OPS_PER_EVAL / (va_ms * 1e-3) / 1e12
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peaks[0], "unit": "TFLOP/s",
+            "frac": achieved / peaks[0], "traffic": None,
+            "kernel": "far_kernel<V, Helmholtz, P0, P0, float> (+ near_kernel FP64)",
+            "peak_source": "bem_measure_peaks FP32 FMA probe on this GPU (MEASURED_PEAKS.json has HBM and bf16 only)",
+            "ops_per_eval": OPS_PER_EVAL, "evals_per_launch": evals, "assembly_ms": va_ms,
+            "mufu_peak_gops": peaks[2], "fp64_peak_tflops": peaks[1]}
+
+    cpu = None
+    if rank == 0 and ws == 1:
+        try:
+            cpu = cpu_reference(1, 0)
+        except Exception as exc:  # the baseline never blocks the GPU line
+            cpu = {"value": None, "error": repr(exc)}
+
+    if ws > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 far field / c128 near field + FP32 LU + FP64 refinement",
+            "data": "synthetic (generated icosphere, analytic plane wave)",
+            "config": {"workload": WORKLOAD, "panels": nt, "entries": entries, "precision": "mixed",
+                       "quirk": "reference quadrature", "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas x{ws}"},
+            "time_to_solution_ms": ms,
+            "assembly_entries_per_s": entries / (va_ms * 1e-3),
+            "plain_fp64": {"time_to_solution_ms": statistics.mean(ms64),
+                           "assembly_entries_per_s": entries / (statistics.mean(va64) * 1e-3),
+                           "assembly_ms": statistics.mean(va64)},
+            "speedup_vs_plain_fp64": statistics.mean(ms64) / ms,
+            "rel_err_vs_fp64": {"max_abs_rel": rel, "l2_rel": rel2},
+            "refinement": {k: (v if not hasattr(v, "item") else v.item()) for k, v in info.items()},
+            "e2e": {"value": entries / (e2e * 1e-3), "unit": "entries/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "breakdown_ms": breakdown,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    core.kill()
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -119,7 +119,8 @@ int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, con
 int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
               int dtype, const void* x, void* y, double scale, int conj_x, void* stream);
 
-/* Identity (mass) block on one panel list (test and trial share `panels`):
+/* Identity (mass) block on one panel list (the test side's `panels`; the
+ * trial side must have the same n_panels and only contributes its dof table):
  * dense (out/out_t) or apply (x != NULL: y += scale*M*x).  Replaces
  * IdentityLayer3d.matA_add_global_Identity_matrix (identity_layer_3d.py:148-196)
  * and RHSConstructor3d.multiply_identity_to_vector (rhs_constructor_3d.py:256-359). */
@@ -143,14 +144,36 @@ int bem_lu_solve(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda
 int bem_gemv(bem_ctx* ctx, int a_dtype, const void* A, int64_t m, int64_t n, int64_t lda,
              const void* x, void* y, double alpha, double beta, void* stream);
 
+/* Tile-pivoted LU (the low-precision factor of the mixed path; replaces the
+ * same torch.linalg.solve call): partial pivoting restricted to each 64x64
+ * diagonal tile, explicit inverses of the diagonal tiles written to `dinv`
+ * (device, bem_lu_dinv_elems(n) elements of the dtype's complex-pair width:
+ * 2 x float / 2 x double per element).  No grid-wide synchronisation. */
+int64_t bem_lu_dinv_elems(int64_t n);
+int bem_lu_factor_tiled(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, void* dinv,
+                        int32_t* info, void* stream);
+/* x = U^{-1} L^{-1} P b for one FP64 right-hand side b (overwritten), with the
+ * factors of bem_lu_factor_tiled; a persistent kernel driven by per-tile ready
+ * flags (bounded waits; BEM_ERR_TIMEOUT if one runs out). */
+int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
+                       const void* dinv, void* b, void* stream);
+
 /* Mixed-precision solve: x = A_hi^{-1} b to relative residual tol by FP64
  * iterative refinement on the residual b - A_hi x, each correction solved with
- * the low-precision factors (LU_lo, piv) of A_hi.  A_hi: F64/C128, LU_lo:
+ * the low-precision factors (LU_lo, piv[, dinv]) of A_hi: tile-pivoted factors
+ * when dinv != NULL, else partial-pivoting factors.  A_hi: F64/C128, LU_lo:
  * F32/C64.  iters/relres: host pointers (may be NULL).  Returns
- * BEM_ERR_NOCONVERGE if maxit is reached. */
+ * BEM_ERR_NOCONVERGE if maxit is reached or the residual stops decreasing. */
 int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv,
-                     int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit,
+                     const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit,
                      int* iters, double* relres, void* stream);
+
+/* ---- device probes ------------------------------------------------------------
+ * No reference counterpart.  Measures the throughput of the pipes the assembly
+ * kernels are bound by (they are neither HBM- nor tensor-core-bound):
+ * out[0] = FP32 FMA TFLOP/s, out[1] = FP64 FMA TFLOP/s, out[2] = MUFU (rsqrt)
+ * Gop/s.  Synchronous; allocates a small buffer. */
+int bem_measure_peaks(bem_ctx* ctx, double* out, void* stream);
 
 #ifdef __cplusplus
 }

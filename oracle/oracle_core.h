@@ -229,7 +229,9 @@ static FN(cplx) FN(pair_integral)(const FN(opctx_t)* o0, const FN(panel_t)* X, c
                                   int bx, int by, int Q, const REAL* gp, const REAL* gw, int quirk) {
     FN(opctx_t) o = *o0;
     if (o.op == OP_W) {
-        o.curldot = X->curl[bx][0] * Y->curl[by][0] + X->curl[bx][1] * Y->curl[by][1] + X->curl[bx][2] * Y->curl[by][2];
+        /* a P0 side has no hat function: surface_grad sees phi1=phi2=phi3=0 (basis index -1) */
+        o.curldot = (bx < 0 || by < 0) ? (REAL)0
+                    : X->curl[bx][0] * Y->curl[by][0] + X->curl[bx][1] * Y->curl[by][1] + X->curl[bx][2] * Y->curl[by][2];
         o.ndot = X->normal[0] * Y->normal[0] + X->normal[1] * Y->normal[1] + X->normal[2] * Y->normal[2];
     }
     FN(cplx) acc = FN(c_make)(0, 0);

@@ -32,7 +32,8 @@ F64, C128, F32, C64 = 0, 1, 2, 3
 EXPORTS = [
     "bem_ctx_create", "bem_ctx_destroy", "bem_last_error", "bem_launch_count", "bem_mesh_set",
     "bem_near_pair_count", "bem_mesh_geometry", "bem_assemble", "bem_apply", "bem_mass", "bem_lu_factor",
-    "bem_lu_solve", "bem_gemv", "bem_refine_solve",
+    "bem_lu_solve", "bem_gemv", "bem_refine_solve", "bem_measure_peaks", "bem_lu_dinv_elems",
+    "bem_lu_factor_tiled", "bem_lu_solve_tiled",
 ]
 
 
@@ -83,12 +84,15 @@ def load():
     L.bem_lu_factor.argtypes = [vp, i32, vp, i64, i64, vp, vp, vp]
     L.bem_lu_solve.argtypes = [vp, i32, vp, i64, i64, vp, vp, i64, i64, vp]
     L.bem_gemv.argtypes = [vp, i32, vp, i64, i64, i64, vp, vp, dbl, dbl, vp]
-    L.bem_refine_solve.argtypes = [vp, i32, vp, vp, vp, i64, i64, vp, vp, dbl, i32, ctypes.POINTER(ctypes.c_int),
-                                   ctypes.POINTER(ctypes.c_double), vp]
+    L.bem_refine_solve.argtypes = [vp, i32, vp, vp, vp, vp, i64, i64, vp, vp, dbl, i32,
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), vp]
+    L.bem_lu_dinv_elems.argtypes = [i64]
+    L.bem_lu_dinv_elems.restype = i64
+    L.bem_lu_factor_tiled.argtypes = [vp, i32, vp, i64, i64, vp, vp, vp, vp]
+    L.bem_lu_solve_tiled.argtypes = [vp, i32, vp, i64, i64, vp, vp, vp, vp]
+    L.bem_measure_peaks.argtypes = [vp, ctypes.POINTER(ctypes.c_double), vp]
     for name in EXPORTS:
-        f = getattr(L, name)
-        if f.restype is None or name not in ("bem_last_error", "bem_launch_count", "bem_near_pair_count"):
-            if name not in ("bem_last_error", "bem_launch_count", "bem_near_pair_count"):
-                f.restype = ctypes.c_int
+        if name not in ("bem_last_error", "bem_launch_count", "bem_near_pair_count", "bem_lu_dinv_elems"):
+            getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

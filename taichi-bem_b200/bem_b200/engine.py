@@ -204,12 +204,38 @@ class Engine:
                                       float(alpha), float(beta), _stream_ptr()))
         return y
 
-    def refine_solve(self, A_hi, LU_lo, piv, b, x, tol=1e-12, maxit=50):
+    def lu_factor_tiled(self, A: torch.Tensor):
+        """In-place tile-pivoted LU; returns (piv, dinv, info)."""
+        n = A.shape[0]
+        assert A.is_cuda and A.shape[0] == A.shape[1] and A.stride(1) == 1
+        piv = torch.empty(n, dtype=torch.int32, device=A.device)
+        info = torch.zeros(1, dtype=torch.int32, device=A.device)
+        cdt = A.dtype if A.is_complex() else (torch.complex64 if A.dtype == torch.float32 else torch.complex128)
+        dinv = torch.empty(int(self.lib.bem_lu_dinv_elems(n)), dtype=cdt, device=A.device)
+        self._check(self.lib.bem_lu_factor_tiled(self.ctx, _dtype_code(A), _ptr(A), n, A.stride(0), _ptr(piv),
+                                                 _ptr(dinv), _ptr(info), _stream_ptr()))
+        return piv, dinv, info
+
+    def lu_solve_tiled(self, LU, piv, dinv, b):
+        n = LU.shape[0]
+        assert b.is_contiguous() and b.numel() == n
+        self._check(self.lib.bem_lu_solve_tiled(self.ctx, _dtype_code(LU), _ptr(LU), n, LU.stride(0), _ptr(piv),
+                                                _ptr(dinv), _ptr(b), _stream_ptr()))
+        return b
+
+    def refine_solve(self, A_hi, LU_lo, piv, b, x, tol=1e-12, maxit=50, dinv=None):
         it = ctypes.c_int(0)
         rr = ctypes.c_double(0.0)
         n = A_hi.shape[0]
-        rc = self.lib.bem_refine_solve(self.ctx, _dtype_code(A_hi), _ptr(A_hi), _ptr(LU_lo), _ptr(piv), n,
-                                       A_hi.stride(0), _ptr(b), _ptr(x), float(tol), int(maxit), ctypes.byref(it),
+        rc = self.lib.bem_refine_solve(self.ctx, _dtype_code(A_hi), _ptr(A_hi), _ptr(LU_lo), _ptr(piv), _ptr(dinv),
+                                       n, A_hi.stride(0), _ptr(b), _ptr(x), float(tol), int(maxit), ctypes.byref(it),
                                        ctypes.byref(rr), _stream_ptr())
         self._check(rc)
         return it.value, rr.value
+
+
+def measure_peaks(engine: Engine):
+    """(FP32 TFLOP/s, FP64 TFLOP/s, MUFU Gop/s) measured on this device."""
+    out = (ctypes.c_double * 3)()
+    engine._check(engine.lib.bem_measure_peaks(engine.ctx, out, _stream_ptr()))
+    return float(out[0]), float(out[1]), float(out[2])

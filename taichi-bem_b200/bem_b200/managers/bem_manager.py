@@ -1,0 +1,409 @@
+"""BEMManager: the assembly and solve driver (src/managers/BEM_manager.py).
+
+Same method names and sequencing as the reference; every O(n^2) and heavier
+step runs on the GPU through libbem_b200 (operator blocks, matrix-free
+products, mass blocks, LU, triangular solves, refinement).  Block placement
+follows the reference: DOF order [Dirichlet (M_D) | Neumann (N_N)]
+(BEM_manager.py:104-111) and
+
+    M = [ K  -V ]      matA_add_M(c):  A_NN += -c V,  A_ND += c K,
+        [-W  -K']                      A_DN += -c K^T, A_DD += -c W.
+
+Extra simulation_parameters keys (all optional):
+  precision: "fp64" (plain path: every quadrature point and the LU in FP64)
+             or "mixed" (separate pairs in FP32, near field in FP64, FP32 LU
+             with FP64 iterative refinement against the FP64-stored matrix)
+  quirk:     True (default) reproduces the reference's quadrature exactly;
+             False uses the corrected Sauter-Schwab orientation and g (not
+             conj g) in the Helmholtz right-hand side
+  solver:    "lstsq" (transmission default, the reference's least squares on
+             [A; P+_i] via normal equations) or "lu" (square A)
+  refine_tol / refine_maxit: iterative-refinement controls of the mixed path
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from .. import _lib as L
+from ..BEM_functions.layers import (AdjDoubleLayer3d, DoubleLayer3d, HypersingularLayer3d, IdentityLayer3d,
+                                    RHSConstructor3d, SingleLayer3d)
+from ..engine import DeviceSpace, Engine
+from ..utils.types import AssembleType, CellFluxType, KernelType, ScopeType, VertAttachType
+
+
+class BEMManager:
+    def __init__(self, core_manager):
+        self._core_manager = core_manager
+        self._log_manager = core_manager._log_manager
+        self._is_transmission = core_manager._is_transmission
+        p = core_manager._simulation_parameters
+        self._simulation_parameters = p
+        kern = p["kernel"]
+        if kern == "Laplace":
+            self._kernel_type, self._n = int(KernelType.LAPLACE), 1
+        elif kern == "Helmholtz":
+            self._kernel_type, self._n = int(KernelType.HELMHOLTZ), 2
+        elif kern == "Helmholtz_Transmission":
+            self._kernel_type, self._n = int(KernelType.HELMHOLTZ_TRANSMISSION), 2
+        else:
+            raise RuntimeError("Kernel Type only support Laplace and Helmholtz for now")
+        show = p.get("show", "Default")
+        if show not in ("Neumann", "Dirichlet", "Default"):
+            raise RuntimeError("The supported type for visualization is only Neumann/Dirichlet/Default")
+        self._show = {"Neumann": int(VertAttachType.NEUMANN_TOBESOLVED),
+                      "Dirichlet": int(VertAttachType.DIRICHLET_TOBESOLVED), "Default": -1}[show]
+        if self._show == -1 and self._is_transmission:
+            self._show = int(VertAttachType.NEUMANN_TOBESOLVED)
+        self._k = float(p.get("k", 0.0)) if self._n == 2 else 0.0
+        self._sqrt_ni = self._sqrt_no = 1.0
+        if self._kernel_type == int(KernelType.HELMHOLTZ_TRANSMISSION):
+            self._sqrt_ni = float(math.sqrt(p["n_i"]))
+            self._sqrt_no = float(math.sqrt(p["n_o"]))
+        self._dim = int(p.get("dim", 3))
+        self._GaussQR = int(p["GaussQR"])
+        self._scope_type = int(ScopeType.NOT_DEFINED)
+        if p.get("scope") == "Interior":
+            self._scope_type = int(ScopeType.INTERIOR)
+        elif p.get("scope") == "Exterior":
+            self._scope_type = int(ScopeType.EXTERIOR)
+        self.precision = p.get("precision", "fp64")
+        if self.precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.quirk = bool(p.get("quirk", True))
+        self.solver = p.get("solver", "lstsq" if self._is_transmission else "lu")
+        self.refine_tol = float(p.get("refine_tol", 1e-12))
+        self.refine_maxit = int(p.get("refine_maxit", 60))
+        self.device = torch.device(p.get("device", "cuda"))
+        self.torch_dtype = torch.complex128 if self._n == 2 else torch.float64
+        self.conj_data = (self._n == 2) and self.quirk
+        self._L1_inv_H = None
+        self._L2_inv_H = None
+        self.solve_info = {}
+        self.initialized = False
+
+    # -- set-up -------------------------------------------------------------------
+    def initialization(self, analytical_function_Dirichlet, analytical_function_Neumann):
+        mm = self._core_manager._mesh_manager
+        if not mm.initialized:
+            raise RuntimeError("The initialization of Mesh Manager should always before the BEM Manager")
+        self.mesh = mm
+        self.num_of_vertices = mm.get_num_of_vertices()
+        self.num_of_panels = mm.get_num_of_panels()
+        self.N_Neumann = mm.get_N_Neumann()
+        self.M_Dirichlet = mm.get_M_Dirichlet()
+        self.shape_func_degree_Neumann = mm.get_shape_func_degree_Neumann()
+        self.shape_func_degree_Dirichlet = mm.get_shape_func_degree_Dirichlet()
+        self.num_of_panels_Neumann = mm.get_num_of_panels_Neumann()
+        self.num_of_panels_Dirichlet = mm.get_num_of_panels_Dirichlet()
+        self._Dirichlet_offset_i = self._Dirichlet_offset_j = 0
+        self._Neumann_offset_i = self._Neumann_offset_j = self.M_Dirichlet
+        self.analytical_function_Dirichlet = analytical_function_Dirichlet
+        self.analytical_function_Neumann = analytical_function_Neumann
+        n = self.N_Neumann + self.M_Dirichlet
+        if n <= 0:
+            raise AssertionError("no unknowns")
+        self.engine = Engine(self.device)
+        self.engine.set_mesh(mm.vertices, mm.panels, self._GaussQR)
+        self._spaces = {}
+        z = lambda *s: torch.zeros(*s, dtype=self.torch_dtype, device=self.device)
+        self._mat_A = z(n, n)
+        self.rhs = z(2 * n if self._is_transmission else n)
+        self.raw_solved = z(n)
+        self.raw_analytical_solved = z(n)
+        self.solved = z(self.num_of_vertices)
+        self.analytical_solved = z(self.num_of_vertices)
+        self.identity_layer = IdentityLayer3d(self)
+        self.single_layer = SingleLayer3d(self)
+        self.double_layer = DoubleLayer3d(self)
+        self.adj_double_layer = AdjDoubleLayer3d(self)
+        self.hypersingular_layer = HypersingularLayer3d(self)
+        self.rhs_constructor = RHSConstructor3d(self)
+        self.initialized = True
+
+    def space(self, kind: str, Q: int, side: str, as_type: int = 0, offset: int = 0) -> DeviceSpace:
+        """Device (panel list, dof table) of one operator side, cached."""
+        key = (kind, Q, side, as_type, offset)
+        sp = self._spaces.get(key)
+        if sp is None:
+            mm = self.mesh
+            if kind == "charge":
+                panels, nb, dof = mm.charge_dofs(Q, side, as_type)
+            elif kind == "data":
+                panels, nb, dof = mm.data_dofs(Q, side)
+            elif kind == "gcharge":
+                panels, nb, dof = mm.global_charge(Q, side, as_type)
+            else:
+                raise ValueError(kind)
+            dof = np.where(dof >= 0, dof + offset, -1)
+            sp = DeviceSpace.from_numpy(panels, nb, dof, self.device)
+            self._spaces[key] = sp
+        return sp
+
+    def op_desc(self, op: int, k: float, sqrt_n: float) -> L.OpDesc:
+        helm = self._n == 2
+        uses_n = self._kernel_type == int(KernelType.HELMHOLTZ_TRANSMISSION)
+        k_kernel = k * sqrt_n if uses_n else k
+        k2 = k * k * sqrt_n * sqrt_n
+        prec = L.PREC_MIXED if self.precision == "mixed" else L.PREC_FP64
+        return Engine.op_desc(op, helm, k_kernel if helm else 0.0, k2 if helm else 0.0, quirk=self.quirk,
+                              precision=prec)
+
+    # -- accessors ------------------------------------------------------------------
+    def get_GaussQR(self):
+        return self._GaussQR
+
+    def get_num_of_vertices(self):
+        return self.num_of_vertices
+
+    def get_num_of_panels(self):
+        return self.num_of_panels
+
+    def get_M_Dirichlet(self):
+        return self.M_Dirichlet
+
+    def get_N_Neumann(self):
+        return self.N_Neumann
+
+    def get_mat_A(self):
+        return self._mat_A
+
+    def get_scope_type(self):
+        return self._scope_type
+
+    def set_scope_type(self, scope_type):
+        self._scope_type = scope_type
+
+    # -- operators and block system ------------------------------------------------------
+    def matrix_layer_init(self):
+        for lay in (self.single_layer, self.double_layer, self.hypersingular_layer):
+            for name in ("_Vmat", "_Kmat", "_Wmat"):
+                t = getattr(lay, name, None)
+                if t is not None:
+                    t.zero_()
+
+    def matrix_layer_forward(self, k: float, sqrt_n: float = 1.0, scope_type: int = int(ScopeType.NOT_DEFINED)):
+        if scope_type == int(ScopeType.NOT_DEFINED):
+            raise RuntimeError("Did not indicate a correct scope type!")
+        self.set_scope_type(scope_type)
+        self.single_layer.forward(scope_type, k, sqrt_n)
+        self.double_layer.forward(scope_type, k, sqrt_n)
+        self.adj_double_layer.forward(scope_type, k, sqrt_n)
+        self.hypersingular_layer.forward(scope_type, k, sqrt_n)
+
+    def rhs_layer_forward(self, scope_type, k: float, sqrt_n: float = 1.0):
+        self.rhs_constructor.forward(scope_type=scope_type, k=k, sqrt_n=sqrt_n)
+
+    def matA_add_M(self, multiplier: float):
+        A = self._mat_A
+        No, Do = self._Neumann_offset_i, self._Dirichlet_offset_i
+        N, M = self.N_Neumann, self.M_Dirichlet
+        if N > 0:
+            A[No:No + N, No:No + N].add_(self.single_layer._Vmat, alpha=-multiplier)
+        if N > 0 and M > 0:
+            K = self.double_layer._Kmat
+            A[No:No + N, Do:Do + M].add_(K, alpha=multiplier)
+            A[Do:Do + M, No:No + N].add_(K.transpose(0, 1), alpha=-multiplier)
+        if M > 0:
+            A[Do:Do + M, Do:Do + M].add_(self.hypersingular_layer._Wmat, alpha=-multiplier)
+
+    def assemble_matA(self, assemble_type: int, multiplier: float):
+        """M = [K, -V; -W, -K'] (BEM_manager.py:630-645)."""
+        if assemble_type == int(AssembleType.ADD_M):
+            self.matA_add_M(multiplier)
+        elif assemble_type == int(AssembleType.ADD_HALF_IDENTITY):
+            self.identity_layer.matA_add_global_Identity_matrix(0.5 * multiplier)
+        elif assemble_type == int(AssembleType.ADD_P_MINUS):
+            self.identity_layer.matA_add_global_Identity_matrix(0.5 * multiplier)
+            self.matA_add_M(-multiplier)
+        elif assemble_type == int(AssembleType.ADD_P_PLUS):
+            self.identity_layer.matA_add_global_Identity_matrix(0.5 * multiplier)
+            self.matA_add_M(multiplier)
+
+    def assemble_rhs(self):
+        """Transmission: rhs[:n] = A conj(f) (BEM_manager.py:647-662); else a copy."""
+        n = self.N_Neumann + self.M_Dirichlet
+        if self._is_transmission:
+            self.rhs.zero_()
+            f = self.rhs_constructor._f_boundary
+            f = f.conj().resolve_conj() if self.conj_data else f
+            self.engine.gemv(self._mat_A, f.contiguous(), self.rhs[:n], alpha=1.0, beta=0.0)
+        else:
+            self.rhs.copy_(self.rhs_constructor._rhs_vec)
+
+    # -- solve --------------------------------------------------------------------------
+    def _lu_solve_square(self, A: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+        """x = A^{-1} b with the hand-written LU: FP64 factor (plain path) or
+        FP32 factor + FP64 refinement against A (mixed path)."""
+        if self.precision == "fp64":
+            LU = A.clone()
+            piv, info = self.engine.lu_factor(LU)
+            x = b.clone().contiguous()
+            self.engine.lu_solve(LU, piv, x)
+            self.solve_info = {"factor": "fp64", "info": info}
+            return x
+        lo = torch.complex64 if A.is_complex() else torch.float32
+        LU = A.to(lo)
+        piv, dinv, info = self.engine.lu_factor_tiled(LU)
+        x = torch.zeros_like(b)
+        try:
+            it, rr = self.engine.refine_solve(A, LU, piv, b.contiguous(), x, tol=self.refine_tol,
+                                              maxit=self.refine_maxit, dinv=dinv)
+            kind = "fp32 tile-pivoted"
+        except L.BemError as exc:
+            if exc.code != -4:
+                raise
+            # the tile-pivoted factor was not a good enough preconditioner:
+            # fall back to partial pivoting over full columns
+            LU = A.to(lo)
+            piv, info = self.engine.lu_factor(LU)
+            x.zero_()
+            it, rr = self.engine.refine_solve(A, LU, piv, b.contiguous(), x, tol=self.refine_tol,
+                                              maxit=self.refine_maxit)
+            kind = "fp32 partial pivoting (fallback)"
+        self.solve_info = {"factor": kind, "info": info, "refine_iters": it, "relres": rr}
+        return x
+
+    def solve(self):
+        n = self.N_Neumann + self.M_Dirichlet
+        if self._is_transmission:
+            # the reference stacks [A; P+_i] and calls lstsq (BEM_manager.py:1039-1050)
+            A_top = self._mat_A.clone()
+            self._mat_A.zero_()
+            self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
+            P = self._mat_A.clone()
+            if self.solver == "lstsq":
+                # normal equations of the stacked system: (A^H A + P^H P) x = A^H b_top
+                AH = A_top.conj().transpose(0, 1)
+                Mn = (AH @ A_top + P.conj().transpose(0, 1) @ P).contiguous()
+                bn = (AH @ self.rhs[:n]).contiguous()
+                sol = self._lu_solve_square(Mn, bn)
+            else:
+                sol = self._lu_solve_square(A_top.contiguous(), self.rhs[:n].contiguous())
+            self._mat_A.copy_(A_top)
+        else:
+            sol = self._lu_solve_square(self._mat_A, self.rhs)
+        self.raw_solved.copy_(sol)
+
+    # -- post-processing (headless device buffers) ------------------------------------------
+    def compute_analytical_raw_solved(self):
+        """Exact traces at the DOFs (BEM_manager.py:664-750)."""
+        self.raw_analytical_solved.zero_()
+        mm = self.mesh
+        rc = self.rhs_constructor
+        dev = self.device
+        v, f = mm.vertices, mm.panels
+        if self._is_transmission:
+            Do, No = self._Dirichlet_offset_j, self._Neumann_offset_j
+            nD = len(rc._Dirichlet_boundary)
+            nN = len(rc._Neumann_boundary)
+            self.raw_analytical_solved[Do:Do + min(nD, self.M_Dirichlet)] = rc._Dirichlet_boundary[:self.M_Dirichlet]
+            self.raw_analytical_solved[No:No + min(nN, self.N_Neumann)] = rc._Neumann_boundary[:self.N_Neumann]
+            return
+        cent = (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
+        if self.N_Neumann > 0:
+            if self.shape_func_degree_Neumann == 0:
+                gp = mm.loop_panels("N")
+                val = rc._eval(self.analytical_function_Neumann, cent[gp], mm.panel_normals[gp])
+                self.raw_analytical_solved[self._Neumann_offset_j:self._Neumann_offset_j + len(gp)] = val
+            else:
+                vv = np.nonzero(mm.vertice_types == int(VertAttachType.NEUMANN_TOBESOLVED))[0]
+                loc = mm._vert_local("N", vv)
+                ok = loc >= 0
+                val = rc._eval(self.analytical_function_Neumann, v[vv[ok]], mm.vert_normals[vv[ok]])
+                self.raw_analytical_solved[torch.as_tensor(loc[ok] + self._Neumann_offset_j, device=dev)] = val
+        if self.M_Dirichlet > 0:
+            if self.shape_func_degree_Dirichlet == 0:
+                gp = mm.loop_panels("D")
+                val = rc._eval(self.analytical_function_Dirichlet, cent[gp])
+                self.raw_analytical_solved[self._Dirichlet_offset_j:self._Dirichlet_offset_j + len(gp)] = val
+            else:
+                vv = np.nonzero(mm.vertice_types == int(VertAttachType.DIRICHLET_TOBESOLVED))[0]
+                loc = mm._vert_local("D", vv)
+                ok = loc >= 0
+                val = rc._eval(self.analytical_function_Dirichlet, v[vv[ok]])
+                self.raw_analytical_solved[torch.as_tensor(loc[ok] + self._Dirichlet_offset_j, device=dev)] = val
+
+    def splat_u_from_raw_solved_to_vertices(self):
+        """Per-vertex values (BEM_manager.py:752-801): P0 values are
+        area-weighted onto the panel's vertices, P1 values copied."""
+        self.solved.zero_()
+        self.analytical_solved.zero_()
+        mm = self.mesh
+        dev = self.device
+        f = torch.as_tensor(mm.panels, device=dev, dtype=torch.long)
+        pa = torch.as_tensor(mm.panel_areas, device=dev)
+        va = torch.as_tensor(mm.vert_areas, device=dev)
+
+        def splat_p0(side, offset, excluded):
+            gp = mm.loop_panels(side)
+            if len(gp) == 0:
+                return
+            ok = mm.panel_types[gp] != excluded
+            idx = np.arange(len(gp))[ok]
+            gpt = torch.as_tensor(gp[ok], device=dev, dtype=torch.long)
+            w = (pa[gpt] / 3.0).unsqueeze(1) / va[f[gpt]]
+            for src, dst in ((self.raw_solved, self.solved), (self.raw_analytical_solved, self.analytical_solved)):
+                vals = src[torch.as_tensor(idx + offset, device=dev)].unsqueeze(1) * w
+                dst.index_add_(0, f[gpt].reshape(-1), vals.reshape(-1))
+
+        def splat_p1(side, offset, excluded):
+            vv = np.nonzero(mm.vertice_types != excluded)[0]
+            loc = mm._vert_local(side, vv)
+            ok = loc >= 0
+            if not ok.any():
+                return
+            vt = torch.as_tensor(vv[ok], device=dev)
+            lt = torch.as_tensor(loc[ok] + offset, device=dev)
+            self.solved[vt] += self.raw_solved[lt]
+            self.analytical_solved[vt] += self.raw_analytical_solved[lt]
+
+        if self._show != int(VertAttachType.DIRICHLET_TOBESOLVED):
+            if self.shape_func_degree_Neumann == 0:
+                splat_p0("N", self._Neumann_offset_j, int(CellFluxType.DIRICHLET_TOBESOLVED))
+            else:
+                splat_p1("N", self._Neumann_offset_j, int(VertAttachType.DIRICHLET_TOBESOLVED))
+        if self._show != int(VertAttachType.NEUMANN_TOBESOLVED):
+            if self.shape_func_degree_Dirichlet == 0:
+                splat_p0("D", self._Dirichlet_offset_j, int(CellFluxType.NEUMANN_TOBESOLVED))
+            else:
+                splat_p1("D", self._Dirichlet_offset_j, int(VertAttachType.NEUMANN_TOBESOLVED))
+
+    # -- driver ----------------------------------------------------------------------------
+    def run(self):
+        """BEMManager.run (BEM_manager.py:990-1030) without the GUI colouring."""
+        self._mat_A.zero_()
+        if self._is_transmission:
+            self.matrix_layer_forward(k=self._k, sqrt_n=self._sqrt_no, scope_type=int(ScopeType.EXTERIOR))
+            self.assemble_matA(assemble_type=int(AssembleType.ADD_P_MINUS), multiplier=1.0)
+            self.rhs_constructor.set_boundaries(scope_type=int(ScopeType.INTERIOR), sqrt_ni=self._sqrt_ni,
+                                                sqrt_no=self._sqrt_no)
+            self.assemble_rhs()
+            self.matrix_layer_forward(k=self._k, sqrt_n=self._sqrt_ni, scope_type=int(ScopeType.INTERIOR))
+            self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
+        else:
+            self.matrix_layer_forward(k=self._k, scope_type=self._scope_type)
+            self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)
+            self.rhs_constructor.set_boundaries(scope_type=self._scope_type, sqrt_ni=self._sqrt_ni,
+                                                sqrt_no=self._sqrt_no)
+            self.rhs_layer_forward(k=self._k, scope_type=self._scope_type)
+            self.assemble_rhs()
+        self.solve()
+        self.compute_analytical_raw_solved()
+        self.splat_u_from_raw_solved_to_vertices()
+
+    def kill(self):
+        self.initialized = False
+        for lay in ("single_layer", "double_layer", "adj_double_layer", "hypersingular_layer", "identity_layer",
+                    "rhs_constructor"):
+            obj = getattr(self, lay, None)
+            if obj is not None:
+                obj.kill()
+        self._mat_A = None
+        self.rhs = None
+        self.raw_solved = None
+        if getattr(self, "engine", None) is not None:
+            self.engine.close()
+            self.engine = None

@@ -1,0 +1,19 @@
+"""[..., 1|2] real/complex packing (src/BEM_functions/utils/io.py:4-30)."""
+import torch
+
+
+def warp_tensor(x: torch.Tensor):
+    n_ = x.shape[-1]
+    if n_ == 1:
+        return x.squeeze(-1)
+    if n_ == 2:
+        return torch.complex(x[..., 0], x[..., 1])
+    raise NotImplementedError(
+        "A Tensor with shape = (*, {}) can not be warped, we only support 1 (Scalar) or 2 (Complex) for the last dim"
+        .format(n_))
+
+
+def unwarp_tensor(x: torch.Tensor):
+    if x.is_complex():
+        return torch.stack((x.real, x.imag), -1)
+    return x.unsqueeze(-1)

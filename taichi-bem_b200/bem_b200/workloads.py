@@ -1,0 +1,69 @@
+"""The benchmark configurations as simulation_parameters + boundary data.
+
+Each builder returns (params, fD, fN) for CoreManager.  The meshes are
+generated unit icospheres (the reference's own sphere assets have the same
+sizes: sphere.obj 1280 panels = subdivision 3, fined_sphere.obj 5120 =
+subdivision 4); data are the configurations' analytic fields.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+def plane_wave_direction(seed: int = 0) -> np.ndarray:
+    g = torch.Generator().manual_seed(seed)
+    d = torch.randn(3, generator=g, dtype=torch.float64)
+    return (d / d.norm()).numpy()
+
+
+def laplace_point_source(x0=(2.0, 2.0, 2.0)):
+    """u = 1/|x - x0| (harmonic inside the unit sphere); returns (fD, fN)."""
+    def fD(x, s=1.0):
+        c = torch.as_tensor(x0, dtype=x.dtype, device=x.device)
+        return 1.0 / torch.linalg.norm(x - c, dim=1)
+
+    def fN(x, n, s=1.0):
+        c = torch.as_tensor(x0, dtype=x.dtype, device=x.device)
+        d = x - c
+        return -(d * n).sum(1) / torch.linalg.norm(d, dim=1) ** 3
+    return fD, fN
+
+
+def plane_wave(k: float, direction):
+    """u = exp(i k sqrt_n d.x); returns (fD, fN) (fN = du/dn)."""
+    dvec = np.asarray(direction, dtype=np.float64)
+
+    def fD(x, s=1.0):
+        d = torch.as_tensor(dvec, dtype=x.dtype, device=x.device)
+        return torch.exp(1j * (k * s) * (x @ d))
+
+    def fN(x, n, s=1.0):
+        d = torch.as_tensor(dvec, dtype=x.dtype, device=x.device)
+        return 1j * (k * s) * (n @ d) * torch.exp(1j * (k * s) * (x @ d))
+    return fD, fN
+
+
+def _base(**kw):
+    p = dict(dim=3, object="icosphere3", GaussQR=5, n_i=1, n_o=1, k=0.0, kernel="Laplace", boundary="Dirichlet",
+             scope="Interior", show="Default", Q_Neumann=0, Q_Dirichlet=1, log_to_disk=False, make_video=False,
+             show_wireframe=False, vis=False)
+    p.update(kw)
+    return p
+
+
+def config1(precision="fp64"):
+    """Laplace 3D interior Dirichlet on icosphere s3 (1280 panels), GaussQR=5,
+    u = 1/|x - x0|, x0 = (2,2,2): V t = (1/2 M + K) g."""
+    fD, fN = laplace_point_source()
+    return _base(object="icosphere3", precision=precision), fD, fN
+
+
+def config2(precision="mixed", seed=0):
+    """Helmholtz 3D interior Dirichlet, k = 3, icosphere s4 (5120 panels),
+    GaussQR=5, plane wave exp(i k d.x) with a seeded random unit d."""
+    fD, fN = plane_wave(3.0, plane_wave_direction(seed))
+    return _base(object="icosphere4", kernel="Helmholtz", k=3.0, precision=precision), fD, fN
+
+
+CONFIGS = {1: config1, 2: config2}

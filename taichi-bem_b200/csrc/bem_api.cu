@@ -16,6 +16,7 @@ int bem_fail(bem_ctx* ctx, int code, const std::string& msg) {
 
 int bem_check_cuda(bem_ctx* ctx, cudaError_t e, const char* what) {
     if (e == cudaSuccess) return BEM_OK;
+    cudaGetLastError();  // clear a non-sticky launch error so later calls start clean
     return bem_fail(ctx, BEM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
@@ -309,8 +310,8 @@ int bem_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int dt
     if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
     if (int rc = check_space(ctx, test, "test")) return rc;
     if (int rc = check_space(ctx, trial, "trial")) return rc;
-    if (test->n_panels != trial->n_panels || test->panels != trial->panels)
-        return bem_fail(ctx, BEM_ERR_INVALID, "mass: test and trial must share the panel list");
+    if (test->n_panels != trial->n_panels)
+        return bem_fail(ctx, BEM_ERR_INVALID, "mass: test and trial must run over the same panel list");
     if (dtype != BEM_F64 && dtype != BEM_C128) return bem_fail(ctx, BEM_ERR_INVALID, "mass: dtype must be F64/C128");
     int mode = x ? 1 : 0;
     if (mode == 0 && (!out || ld <= 0)) return bem_fail(ctx, BEM_ERR_INVALID, "mass: out is NULL");

@@ -32,34 +32,49 @@ struct GridBar {
     unsigned gen;
 };
 
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Bounded software grid barrier (the launch is cooperative, so all CTAs are
-// co-resident).  Returns false when the wait hit its cap (flag set).
+// co-resident).  The last CTA to arrive resets the counter and releases the
+// generation word; the others poll it with acquire loads, first without and
+// then with a short sleep.  Returns false when the wait hit its cap (flag set)
+// or another CTA reported a failure.
 __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int32_t* flag) {
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = &bar->gen;
-        unsigned g = *vgen;
-        __threadfence();
-        unsigned arrived = atomicAdd(&bar->count, 1u);
         int ok = 1;
+        const unsigned g = ld_acquire(&bar->gen);
+        __threadfence();
+        const unsigned arrived = atom_add_acq_rel(&bar->count, 1u);
         if (arrived == nblocks - 1) {
-            atomicExch(&bar->count, 0u);
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
+            bar->count = 0u;
+            st_release(&bar->gen, g + 1u);
         } else {
             unsigned it = 0;
-            while (*vgen == g) {
-                if (*(volatile int32_t*)flag != 0) {
-                    ok = 0;
-                    break;
-                }
+            while (ld_acquire(&bar->gen) == g) {
                 if (++it > SPIN_CAP) {
                     atomicExch(flag, BEM_ERR_TIMEOUT);
                     ok = 0;
                     break;
                 }
-                __nanosleep(128);
+                if ((it & 63u) == 0u && *(volatile int32_t*)flag != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (it > 4096u) __nanosleep(64);
             }
         }
         __threadfence();
@@ -99,6 +114,14 @@ template <typename T, bool C>
 __device__ __forceinline__ T mag1(El<T, C> e) {
     return C ? fabs(e.re) + fabs(e.im) : fabs(e.re);
 }
+template <typename T, bool C>
+__device__ __forceinline__ El<T, C> ld_volatile(const El<T, C>* p) {
+    const volatile T* v = reinterpret_cast<const volatile T*>(p);
+    El<T, C> e;
+    e.re = v[0];
+    e.im = C ? v[1] : T(0);
+    return e;
+}
 
 struct PivSlot {
     double val;
@@ -108,29 +131,67 @@ struct PivSlot {
 
 // ----------------------------------------------------------------------------
 // panel factorisation (cooperative)
+//
+// Each CTA owns a contiguous slice of the panel's rows, held in shared memory
+// for the whole panel (SMEM_ROWS) or read from global memory when the slice
+// does not fit.  Per column j: every CTA publishes its best pivot candidate
+// (value, row) and a copy of that row, and the owner of row jj publishes row
+// jj, into buffers indexed by the parity of j; one grid barrier; every CTA
+// reads the winner's row and row jj from those buffers (never from another
+// CTA's slice), swaps, and updates its own rows.  Double buffering by parity
+// keeps a CTA that is one column ahead from overwriting buffers still read.
 // ----------------------------------------------------------------------------
-template <typename T, bool C>
-__global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int64_t lda, int n, int k0, int nb, int32_t* piv,
-                                                       int32_t* info, GridBar* bar, PivSlot* slots, int32_t* flag) {
+constexpr int PANEL_MAXB = 256;
+
+template <typename T, bool C, bool SMEM_ROWS>
+__global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int64_t lda, int n, int k0, int nb, int chunk,
+                                                       int32_t* piv, int32_t* info, GridBar* bar, PivSlot* slots,
+                                                       El<T, C>* rowbuf, int32_t* flag) {
     using E = El<T, C>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    E* srows = reinterpret_cast<E*>(smem_raw);  // [chunk][nb] when SMEM_ROWS
     const unsigned nblk = gridDim.x;
-    const int rows = n - k0;
-    const int chunk = (rows + nblk - 1) / nblk;
     const int r_begin = k0 + blockIdx.x * chunk;
     const int r_end = min(n, r_begin + chunk);
-    __shared__ E s_prow[LU_NB];  // old pivot row (panel columns)
-    __shared__ E s_jrow[LU_NB];  // old row jj
+    __shared__ E s_prow[LU_NB];
+    __shared__ E s_jrow[LU_NB];
     __shared__ double s_red_v[8];
     __shared__ int s_red_i[8];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __shared__ int s_red_b[8];
+    __shared__ int s_best_idx;
+    __shared__ int s_p, s_pb;
+    __shared__ double s_pv;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+    auto row_ptr_g = [&](int r) { return A + (C ? 2 : 1) * ((int64_t)r * lda + k0); };
+    auto get = [&](int r, int c) -> E {
+        if (SMEM_ROWS) return srows[(r - r_begin) * nb + c];
+        return ld<T, C>(row_ptr_g(r), c);
+    };
+    auto put = [&](int r, int c, E v) {
+        if (SMEM_ROWS)
+            srows[(r - r_begin) * nb + c] = v;
+        else
+            st<T, C>(row_ptr_g(r), c, v);
+    };
+    if (SMEM_ROWS) {
+        for (int e = threadIdx.x; e < (r_end - r_begin) * nb; e += blockDim.x) {
+            int r = e / nb, c = e - r * nb;
+            srows[e] = ld<T, C>(row_ptr_g(r_begin + r), c);
+        }
+        __syncthreads();
+    }
 
     for (int j = 0; j < nb; ++j) {
         const int jj = k0 + j;
+        const int par = j & 1;
+        PivSlot* slot = slots + par * PANEL_MAXB;
+        E* rb = rowbuf + (size_t)par * (PANEL_MAXB + 1) * LU_NB;
         // 1. local pivot candidate
         double best = -1.0;
         int bidx = 0x7fffffff;
         for (int r = max(r_begin, jj) + threadIdx.x; r < r_end; r += blockDim.x) {
-            double v = (double)mag1<T, C>(ld<T, C>(A, (int64_t)r * lda + jj));
+            double v = (double)mag1<T, C>(get(r, j));
             if (v > best || (v == best && r < bidx)) {
                 best = v;
                 bidx = r;
@@ -150,57 +211,92 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int64_t lda, int n,
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+            for (int w = 1; w < nwarps; ++w)
                 if (s_red_v[w] > best || (s_red_v[w] == best && s_red_i[w] < bidx)) {
                     best = s_red_v[w];
                     bidx = s_red_i[w];
                 }
-            slots[blockIdx.x].val = best;
-            slots[blockIdx.x].idx = bidx;
+            slot[blockIdx.x].val = best;
+            slot[blockIdx.x].idx = bidx;
+            s_best_idx = bidx;
         }
+        __syncthreads();
+        const int cand = s_best_idx;
+        if (cand >= r_begin && cand < r_end)
+            for (int c = threadIdx.x; c < nb; c += blockDim.x) rb[(size_t)blockIdx.x * LU_NB + c] = get(cand, c);
+        if (jj >= r_begin && jj < r_end)
+            for (int c = threadIdx.x; c < nb; c += blockDim.x) rb[(size_t)PANEL_MAXB * LU_NB + c] = get(jj, c);
         // 2. publish
         if (!grid_barrier(bar, nblk, flag)) return;
-        // 3. global pivot (every CTA computes the same answer)
-        __shared__ int s_p;
-        __shared__ double s_pv;
-        if (threadIdx.x == 0) {
+        // 3. global pivot, slots read in parallel
+        {
             double bv = -1.0;
-            int bi = 0x7fffffff;
-            for (unsigned b = 0; b < nblk; ++b) {
-                double v = ((volatile PivSlot*)slots)[b].val;
-                int i = ((volatile PivSlot*)slots)[b].idx;
+            int bi = 0x7fffffff, bb = -1;
+            for (unsigned b = threadIdx.x; b < nblk; b += blockDim.x) {
+                double v = ((volatile PivSlot*)slot)[b].val;
+                int i = ((volatile PivSlot*)slot)[b].idx;
                 if (v > bv || (v == bv && i < bi)) {
                     bv = v;
                     bi = i;
+                    bb = (int)b;
                 }
             }
-            if (bi < jj || bi >= n) bi = jj;
-            s_p = bi;
-            s_pv = bv;
-            if (blockIdx.x == 0) {
-                piv[jj] = bi;
-                if (!(bv > 0.0) && *info == 0) *info = jj + 1;
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                int ob = __shfl_xor_sync(0xffffffffu, bb, o);
+                if (ov > bv || (ov == bv && oi < bi)) {
+                    bv = ov;
+                    bi = oi;
+                    bb = ob;
+                }
             }
+            if (lane == 0) {
+                s_red_v[wid] = bv;
+                s_red_i[wid] = bi;
+                s_red_b[wid] = bb;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int w = 1; w < nwarps; ++w)
+                    if (s_red_v[w] > bv || (s_red_v[w] == bv && s_red_i[w] < bi)) {
+                        bv = s_red_v[w];
+                        bi = s_red_i[w];
+                        bb = s_red_b[w];
+                    }
+                if (bb < 0 || bi < jj || bi >= n) {  // no candidate: keep the diagonal
+                    bi = jj;
+                    bb = -1;
+                    bv = 0.0;
+                }
+                s_p = bi;
+                s_pb = bb;
+                s_pv = bv;
+                if (blockIdx.x == 0) {
+                    piv[jj] = bi;
+                    if (!(bv > 0.0) && *info == 0) *info = jj + 1;
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
         const int p = s_p;
-        // 4. both rows (all panel columns) into shared memory, then swap
         for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-            s_prow[c] = ld<T, C>(A, (int64_t)p * lda + k0 + c);
-            s_jrow[c] = ld<T, C>(A, (int64_t)jj * lda + k0 + c);
+            E ej = ld_volatile<T, C>(rb + (size_t)PANEL_MAXB * LU_NB + c);
+            s_jrow[c] = ej;
+            s_prow[c] = s_pb >= 0 ? ld_volatile<T, C>(rb + (size_t)s_pb * LU_NB + c) : ej;
         }
         __syncthreads();
+        // 4. swap rows jj and p (panel columns)
         if (p != jj) {
             if (jj >= r_begin && jj < r_end)
-                for (int c = threadIdx.x; c < nb; c += blockDim.x) st<T, C>(A, (int64_t)jj * lda + k0 + c, s_prow[c]);
+                for (int c = threadIdx.x; c < nb; c += blockDim.x) put(jj, c, s_prow[c]);
             if (p >= r_begin && p < r_end)
-                for (int c = threadIdx.x; c < nb; c += blockDim.x) st<T, C>(A, (int64_t)p * lda + k0 + c, s_jrow[c]);
+                for (int c = threadIdx.x; c < nb; c += blockDim.x) put(p, c, s_jrow[c]);
         }
         __syncthreads();
-        // 5. scale column jj below the diagonal and rank-1 update of the panel
+        // 5. scale column jj below the diagonal, rank-1 update of the panel
         const E pv = s_prow[j];
         const bool nonzero = s_pv > 0.0;
-        // reciprocal of the pivot
         E inv;
         if (C) {
             T d = pv.re * pv.re + pv.im * pv.im;
@@ -210,23 +306,28 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int64_t lda, int n,
             inv.re = nonzero ? T(1) / pv.re : T(0);
             inv.im = T(0);
         }
-        const int nwarps = blockDim.x >> 5;
         for (int r = max(r_begin, jj + 1) + wid; r < r_end; r += nwarps) {
-            T* row = A + (C ? 2 : 1) * ((int64_t)r * lda + k0);
-            E a = ld<T, C>(row, j);
+            E a = get(r, j);
             E l;
             l.re = a.re * inv.re - (C ? a.im * inv.im : T(0));
             l.im = C ? a.re * inv.im + a.im * inv.re : T(0);
             for (int c = j + 1 + lane; c < nb; c += 32) {
-                E v = ld<T, C>(row, c);
+                E v = get(r, c);
                 E u = s_prow[c];
                 v.re -= l.re * u.re - (C ? l.im * u.im : T(0));
                 if (C) v.im -= l.re * u.im + l.im * u.re;
-                st<T, C>(row, c, v);
+                put(r, c, v);
             }
-            if (lane == 0) st<T, C>(row, j, l);
+            __syncwarp();
+            if (lane == 0) put(r, j, l);
         }
-        // the next column's barrier publishes these writes
+        __syncthreads();
+    }
+    if (SMEM_ROWS) {
+        for (int e = threadIdx.x; e < (r_end - r_begin) * nb; e += blockDim.x) {
+            int r = e / nb, c = e - r * nb;
+            st<T, C>(row_ptr_g(r_begin + r), c, srows[e]);
+        }
     }
 }
 
@@ -245,45 +346,64 @@ __global__ void laswp_kernel(T* A, int64_t lda, int n, int k0, int nb, const int
     }
 }
 
-// U12 = L11^{-1} A12 (unit lower L11 = rows/cols k0..k0+nb)
+// U12 = L11^{-1} A12 (unit lower L11 = rows/cols k0..k0+nb): L11 and a tile
+// of TRSM_COLS columns of A12 are staged in shared memory; one thread per
+// column runs the forward substitution out of shared memory.
+constexpr int TRSM_COLS = 64;
+
 template <typename T, bool C>
-__global__ void __launch_bounds__(128) trsm_kernel(T* A, int64_t lda, int n, int k0, int nb) {
+__global__ void __launch_bounds__(TRSM_COLS) trsm_kernel(T* A, int64_t lda, int n, int k0, int nb) {
     using E = El<T, C>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     E* L = reinterpret_cast<E*>(smem_raw);  // [nb][nb]
+    E* X = L + nb * nb;                     // [nb][TRSM_COLS]
+    const int c0 = k0 + nb + blockIdx.x * TRSM_COLS;
+    const int ncol = min(TRSM_COLS, n - c0);
     for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
         int r = idx / nb, c = idx - r * nb;
         L[idx] = ld<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c);
     }
+    for (int idx = threadIdx.x; idx < nb * TRSM_COLS; idx += blockDim.x) {
+        int r = idx / TRSM_COLS, c = idx - r * TRSM_COLS;
+        X[idx] = c < ncol ? ld<T, C>(A, (int64_t)(k0 + r) * lda + c0 + c) : E{T(0), T(0)};
+    }
     __syncthreads();
-    int col = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= n) return;
-    // column in registers would need nb values; keep the running solution in
-    // global memory (the column is written back in place row by row)
+    const int c = threadIdx.x;
     for (int r = 1; r < nb; ++r) {
-        E acc = ld<T, C>(A, (int64_t)(k0 + r) * lda + col);
+        E acc = X[r * TRSM_COLS + c];
         for (int q = 0; q < r; ++q) {
             E l = L[r * nb + q];
-            E x = ld<T, C>(A, (int64_t)(k0 + q) * lda + col);
+            E x = X[q * TRSM_COLS + c];
             acc.re -= l.re * x.re - (C ? l.im * x.im : T(0));
             if (C) acc.im -= l.re * x.im + l.im * x.re;
         }
-        st<T, C>(A, (int64_t)(k0 + r) * lda + col, acc);
+        X[r * TRSM_COLS + c] = acc;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nb * TRSM_COLS; idx += blockDim.x) {
+        int r = idx / TRSM_COLS, cc = idx - r * TRSM_COLS;
+        if (cc < ncol) st<T, C>(A, (int64_t)(k0 + r) * lda + c0 + cc, X[idx]);
     }
 }
 
 // perm[i] = original row that ends up at row i after the LAPACK swap sequence
+// (sequential by nature; run in shared memory by one thread)
 __global__ void piv_to_perm_kernel(const int32_t* piv, int32_t* perm, int n) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (int i = 0; i < n; ++i) perm[i] = i;
-    for (int i = 0; i < n; ++i) {
-        int p = piv[i];
-        if (p != i && p >= 0 && p < n) {
-            int t = perm[i];
-            perm[i] = perm[p];
-            perm[p] = t;
+    extern __shared__ int32_t sp[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < n; ++i) {
+            int p = piv[i];
+            if (p != i && p >= 0 && p < n) {
+                int t = sp[i];
+                sp[i] = sp[p];
+                sp[p] = t;
+            }
         }
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sp[i];
 }
 
 // ----------------------------------------------------------------------------
@@ -296,12 +416,16 @@ template <typename T, bool C>
 __global__ void __launch_bounds__(256) lu_solve_kernel(const T* LU, int64_t lda, int n, const int32_t* perm,
                                                         const double* b, double* x, double* tmp, int64_t nrhs,
                                                         int64_t ldb, GridBar* bar, int32_t* flag) {
+    using E = El<T, C>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    E* sL = reinterpret_cast<E*>(smem_raw);                                  // [TRSV_NB][TRSV_NB]
+    double* sx = reinterpret_cast<double*>(sL + TRSV_NB * TRSV_NB);          // [TRSV_NB][8][2]
     const unsigned nblk = gridDim.x;
-    const int lane = threadIdx.x & 31;
-    const int gwarp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int gwarp = blockIdx.x * (blockDim.x >> 5) + wid;
     const int nwarp_total = nblk * (blockDim.x >> 5);
     const int W = C ? 2 : 1;
-    // y = P b  (x used as the work vector)
+    // y = P b  (x is the work vector)
     for (int64_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < (int64_t)n * nrhs;
          idx += (int64_t)nblk * blockDim.x) {
         int i = (int)(idx / nrhs), c = (int)(idx % nrhs);
@@ -310,16 +434,30 @@ __global__ void __launch_bounds__(256) lu_solve_kernel(const T* LU, int64_t lda,
     }
     if (!grid_barrier(bar, nblk, flag)) return;
     const int nblocks_r = (n + TRSV_NB - 1) / TRSV_NB;
-    // forward: L y = P b (unit diagonal)
-    for (int kb = 0; kb < nblocks_r; ++kb) {
-        const int r0 = kb * TRSV_NB, r1 = min(n, r0 + TRSV_NB);
-        if (blockIdx.x == 0 && (threadIdx.x >> 5) < nrhs) {
-            const int c = threadIdx.x >> 5;
-            for (int r = r0 + 1; r < r1; ++r) {
+
+    // Diagonal block solve on CTA 0: the block of LU and the x segment are
+    // staged in shared memory, one warp per right-hand side.
+    auto diag_solve = [&](int r0, int r1, bool lower) {
+        const int m = r1 - r0;
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+            int r = e / m, q = e - r * m;
+            sL[r * TRSV_NB + q] = ld<T, C>(LU, (int64_t)(r0 + r) * lda + r0 + q);
+        }
+        for (int e = threadIdx.x; e < m * nrhs; e += blockDim.x) {
+            int r = e / (int)nrhs, c = e - r * (int)nrhs;
+            sx[(r * 8 + c) * 2] = __ldcg(&x[W * ((int64_t)(r0 + r) * ldb + c)]);
+            sx[(r * 8 + c) * 2 + 1] = C ? __ldcg(&x[W * ((int64_t)(r0 + r) * ldb + c) + 1]) : 0.0;
+        }
+        __syncthreads();
+        if (wid < nrhs) {
+            const int c = wid;
+            for (int t = 0; t < m; ++t) {
+                const int r = lower ? t : m - 1 - t;
                 double sr = 0.0, si = 0.0;
-                for (int q = r0 + lane; q < r; q += 32) {
-                    El<T, C> l = ld<T, C>(LU, (int64_t)r * lda + q);
-                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
+                const int q0 = lower ? 0 : r + 1, q1 = lower ? r : m;
+                for (int q = q0 + lane; q < q1; q += 32) {
+                    E l = sL[r * TRSV_NB + q];
+                    double xr = sx[(q * 8 + c) * 2], xi = sx[(q * 8 + c) * 2 + 1];
                     sr += (double)l.re * xr - (C ? (double)l.im * xi : 0.0);
                     if (C) si += (double)l.re * xi + (double)l.im * xr;
                 }
@@ -328,20 +466,40 @@ __global__ void __launch_bounds__(256) lu_solve_kernel(const T* LU, int64_t lda,
                     if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
                 }
                 if (lane == 0) {
-                    x[W * ((int64_t)r * ldb + c)] -= sr;
-                    if (C) x[W * ((int64_t)r * ldb + c) + 1] -= si;
+                    double vr = sx[(r * 8 + c) * 2] - sr, vi = sx[(r * 8 + c) * 2 + 1] - si;
+                    if (!lower) {
+                        E d = sL[r * TRSV_NB + r];
+                        if (C) {
+                            double dr = d.re, di = d.im, den = dr * dr + di * di;
+                            double tr = (vr * dr + vi * di) / den;
+                            vi = (vi * dr - vr * di) / den;
+                            vr = tr;
+                        } else {
+                            vr = vr / (double)d.re;
+                        }
+                    }
+                    sx[(r * 8 + c) * 2] = vr;
+                    sx[(r * 8 + c) * 2 + 1] = vi;
                 }
                 __syncwarp();
             }
         }
-        if (!grid_barrier(bar, nblk, flag)) return;
-        // rows below: x[i] -= L[i, r0:r1] x[r0:r1]
-        for (int i = r1 + gwarp; i < n; i += nwarp_total) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < m * nrhs; e += blockDim.x) {
+            int r = e / (int)nrhs, c = e - r * (int)nrhs;
+            x[W * ((int64_t)(r0 + r) * ldb + c)] = sx[(r * 8 + c) * 2];
+            if (C) x[W * ((int64_t)(r0 + r) * ldb + c) + 1] = sx[(r * 8 + c) * 2 + 1];
+        }
+    };
+    // rows [i0, i1) (distributed over all warps): x[i] -= LU[i, r0:r1] x[r0:r1]
+    auto update = [&](int i0, int i1, int r0, int r1) {
+        for (int i = i0 + gwarp; i < i1; i += nwarp_total) {
             for (int c = 0; c < nrhs; ++c) {
                 double sr = 0.0, si = 0.0;
                 for (int q = r0 + lane; q < r1; q += 32) {
-                    El<T, C> l = ld<T, C>(LU, (int64_t)i * lda + q);
-                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
+                    E l = ld<T, C>(LU, (int64_t)i * lda + q);
+                    double xr = __ldcg(&x[W * ((int64_t)q * ldb + c)]);
+                    double xi = C ? __ldcg(&x[W * ((int64_t)q * ldb + c) + 1]) : 0.0;
                     sr += (double)l.re * xr - (C ? (double)l.im * xi : 0.0);
                     if (C) si += (double)l.re * xi + (double)l.im * xr;
                 }
@@ -350,66 +508,31 @@ __global__ void __launch_bounds__(256) lu_solve_kernel(const T* LU, int64_t lda,
                     if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
                 }
                 if (lane == 0) {
-                    x[W * ((int64_t)i * ldb + c)] -= sr;
-                    if (C) x[W * ((int64_t)i * ldb + c) + 1] -= si;
+                    x[W * ((int64_t)i * ldb + c)] = __ldcg(&x[W * ((int64_t)i * ldb + c)]) - sr;
+                    if (C) x[W * ((int64_t)i * ldb + c) + 1] = __ldcg(&x[W * ((int64_t)i * ldb + c) + 1]) - si;
                 }
             }
         }
+    };
+    // forward: L y = P b (unit diagonal)
+    for (int kb = 0; kb < nblocks_r; ++kb) {
+        const int r0 = kb * TRSV_NB, r1 = min(n, r0 + TRSV_NB);
+        if (blockIdx.x == 0) diag_solve(r0, r1, true);
         if (!grid_barrier(bar, nblk, flag)) return;
+        if (r1 < n) {
+            update(r1, n, r0, r1);
+            if (!grid_barrier(bar, nblk, flag)) return;
+        }
     }
     // backward: U x = y
     for (int kb = nblocks_r - 1; kb >= 0; --kb) {
         const int r0 = kb * TRSV_NB, r1 = min(n, r0 + TRSV_NB);
-        if (blockIdx.x == 0 && (threadIdx.x >> 5) < nrhs) {
-            const int c = threadIdx.x >> 5;
-            for (int r = r1 - 1; r >= r0; --r) {
-                double sr = 0.0, si = 0.0;
-                for (int q = r + 1 + lane; q < r1; q += 32) {
-                    El<T, C> u = ld<T, C>(LU, (int64_t)r * lda + q);
-                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
-                    sr += (double)u.re * xr - (C ? (double)u.im * xi : 0.0);
-                    if (C) si += (double)u.re * xi + (double)u.im * xr;
-                }
-                for (int o = 16; o > 0; o >>= 1) {
-                    sr += __shfl_xor_sync(0xffffffffu, sr, o);
-                    if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
-                }
-                if (lane == 0) {
-                    El<T, C> d = ld<T, C>(LU, (int64_t)r * lda + r);
-                    double vr = x[W * ((int64_t)r * ldb + c)] - sr;
-                    double vi = C ? x[W * ((int64_t)r * ldb + c) + 1] - si : 0.0;
-                    if (C) {
-                        double dr = d.re, di = d.im, den = dr * dr + di * di;
-                        x[W * ((int64_t)r * ldb + c)] = (vr * dr + vi * di) / den;
-                        x[W * ((int64_t)r * ldb + c) + 1] = (vi * dr - vr * di) / den;
-                    } else {
-                        x[(int64_t)r * ldb + c] = vr / (double)d.re;
-                    }
-                }
-                __syncwarp();
-            }
-        }
+        if (blockIdx.x == 0) diag_solve(r0, r1, false);
         if (!grid_barrier(bar, nblk, flag)) return;
-        for (int i = gwarp; i < r0; i += nwarp_total) {
-            for (int c = 0; c < nrhs; ++c) {
-                double sr = 0.0, si = 0.0;
-                for (int q = r0 + lane; q < r1; q += 32) {
-                    El<T, C> u = ld<T, C>(LU, (int64_t)i * lda + q);
-                    double xr = x[W * ((int64_t)q * ldb + c)], xi = C ? x[W * ((int64_t)q * ldb + c) + 1] : 0.0;
-                    sr += (double)u.re * xr - (C ? (double)u.im * xi : 0.0);
-                    if (C) si += (double)u.re * xi + (double)u.im * xr;
-                }
-                for (int o = 16; o > 0; o >>= 1) {
-                    sr += __shfl_xor_sync(0xffffffffu, sr, o);
-                    if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
-                }
-                if (lane == 0) {
-                    x[W * ((int64_t)i * ldb + c)] -= sr;
-                    if (C) x[W * ((int64_t)i * ldb + c) + 1] -= si;
-                }
-            }
+        if (r0 > 0) {
+            update(0, r0, r0, r1);
+            if (!grid_barrier(bar, nblk, flag)) return;
         }
-        if (!grid_barrier(bar, nblk, flag)) return;
     }
     (void)tmp;
 }
@@ -468,21 +591,24 @@ __global__ void axpy_kernel(double* y, const double* x, int64_t n, double a) {
 
 struct LinWs {
     GridBar* bar;
-    PivSlot* slots;
+    PivSlot* slots;  // [2][PANEL_MAXB]
+    void* rowbuf;    // [2][PANEL_MAXB+1][LU_NB] panel-row copies (16 B per element)
     int32_t* perm;
-    double* vec;  // scratch vectors for refinement
+    double* vec;     // scratch vectors for the triangular solves
 };
 
 int linws(bem_ctx* ctx, int64_t n, int64_t nvec_doubles, LinWs* w) {
     size_t off_bar = 0;
     size_t off_slots = 256;
-    size_t off_perm = off_slots + sizeof(PivSlot) * 2048;
+    size_t off_rows = off_slots + sizeof(PivSlot) * 2 * PANEL_MAXB;
+    size_t off_perm = off_rows + 16 * (size_t)2 * (PANEL_MAXB + 1) * LU_NB;
     size_t off_vec = (off_perm + sizeof(int32_t) * (size_t)n + 255) & ~size_t(255);
     size_t total = off_vec + sizeof(double) * (size_t)nvec_doubles;
     if (int rc = bem_ws_reserve(ctx, total)) return rc;
     char* base = (char*)ctx->ws;
     w->bar = (GridBar*)(base + off_bar);
     w->slots = (PivSlot*)(base + off_slots);
+    w->rowbuf = (void*)(base + off_rows);
     w->perm = (int32_t*)(base + off_perm);
     w->vec = (double*)(base + off_vec);
     return BEM_OK;
@@ -517,17 +643,31 @@ int lu_factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, int32_
     cudaMemsetAsync(info, 0, sizeof(int32_t), s);
     cudaMemsetAsync(ctx->flags + 2, 0, sizeof(int32_t), s);
     const int threads = 256;
-    int nblk = coop_blocks(ctx, (const void*)lu_panel_kernel<T, C>, threads, 0, ctx->num_sms);
-    if (nblk < 1) return bem_fail(ctx, BEM_ERR_CUDA, "lu_panel_kernel cannot be made co-resident");
     int32_t* flag = ctx->flags + 2;
+    // CTAs of the panel: at most one per SM and at most PANEL_MAXB; each keeps
+    // its row slice in shared memory when it fits in PANEL_SMEM bytes
+    const size_t PANEL_SMEM = 200 * 1024;
+    const int maxb = std::min(PANEL_MAXB, ctx->num_sms);
+    const size_t smem_full = sizeof(El<T, C>) * (size_t)((n + maxb - 1) / maxb) * LU_NB;
+    const bool use_smem = smem_full <= PANEL_SMEM;
+    const void* pk = use_smem ? (const void*)lu_panel_kernel<T, C, true> : (const void*)lu_panel_kernel<T, C, false>;
+    if (use_smem)
+        cudaFuncSetAttribute(lu_panel_kernel<T, C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)PANEL_SMEM);
+    int nblk = std::min(maxb, coop_blocks(ctx, pk, threads, use_smem ? smem_full : 0, maxb));
+    if (nblk < 1) return bem_fail(ctx, BEM_ERR_CUDA, "lu_panel_kernel cannot be made co-resident");
+    if (use_smem && sizeof(El<T, C>) * (size_t)std::max<int64_t>(32, (n + nblk - 1) / nblk) * LU_NB > PANEL_SMEM)
+        return bem_fail(ctx, BEM_ERR_CUDA, "lu_panel_kernel: fewer co-resident CTAs than SMs");
     for (int64_t k0 = 0; k0 < n; k0 += LU_NB) {
         int nb = (int)std::min<int64_t>(LU_NB, n - k0);
         int rows = (int)(n - k0);
         int blocks = std::min(nblk, std::max(1, (rows + 31) / 32));
+        int chunk = (rows + blocks - 1) / blocks;
         int ni = (int)n, k0i = (int)k0;
-        void* args[] = {&A, &lda, &ni, &k0i, &nb, &piv, &info, &w.bar, &w.slots, &flag};
-        if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)lu_panel_kernel<T, C>, blocks,
-                                                                    threads, args, 0, s),
+        El<T, C>* rb = (El<T, C>*)w.rowbuf;
+        size_t smem = use_smem ? sizeof(El<T, C>) * (size_t)chunk * LU_NB : 0;
+        void* args[] = {&A, &lda, &ni, &k0i, &nb, &chunk, &piv, &info, &w.bar, &w.slots, &rb, &flag};
+        if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel(pk, blocks, threads, args, smem, s),
                                     "lu_panel_kernel"))
             return rc;
         ctx->launches++;
@@ -535,10 +675,10 @@ int lu_factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, int32_
         ctx->launches++;
         int64_t rest = n - k0 - nb;
         if (rest > 0) {
-            size_t smem = sizeof(El<T, C>) * nb * nb;
-            if (smem > 48 * 1024)
-                cudaFuncSetAttribute(trsm_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            trsm_kernel<T, C><<<(unsigned)((rest + 127) / 128), 128, smem, s>>>(A, lda, ni, k0i, nb);
+            size_t tsmem = sizeof(El<T, C>) * nb * (nb + TRSM_COLS);
+            cudaFuncSetAttribute(trsm_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+            trsm_kernel<T, C><<<(unsigned)((rest + TRSM_COLS - 1) / TRSM_COLS), TRSM_COLS, tsmem, s>>>(A, lda, ni,
+                                                                                                   k0i, nb);
             ctx->launches++;
             // A22 -= L21 U12
             T* A22 = A + (C ? 2 : 1) * ((k0 + nb) * lda + k0 + nb);
@@ -560,10 +700,15 @@ int lu_solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t*
     if (int rc = linws(ctx, n, (int64_t)W * n * ldb, &w)) return rc;
     cudaMemsetAsync(w.bar, 0, sizeof(GridBar), s);
     cudaMemsetAsync(ctx->flags + 2, 0, sizeof(int32_t), s);
-    piv_to_perm_kernel<<<1, 1, 0, s>>>(piv, w.perm, (int)n);
+    if ((size_t)n * sizeof(int32_t) > 200 * 1024) return bem_fail(ctx, BEM_ERR_INVALID, "lu_solve: n > 51200");
+    cudaFuncSetAttribute(piv_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(n * sizeof(int32_t)));
+    piv_to_perm_kernel<<<1, 256, n * sizeof(int32_t), s>>>(piv, w.perm, (int)n);
     ctx->launches++;
     const int threads = 256;
-    int nblk = coop_blocks(ctx, (const void*)lu_solve_kernel<T, C>, threads, 0, ctx->num_sms);
+    const size_t smem = sizeof(El<T, C>) * TRSV_NB * TRSV_NB + sizeof(double) * TRSV_NB * 8 * 2;
+    cudaFuncSetAttribute(lu_solve_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nblk = coop_blocks(ctx, (const void*)lu_solve_kernel<T, C>, threads, smem, ctx->num_sms);
     if (nblk < 1) return bem_fail(ctx, BEM_ERR_CUDA, "lu_solve_kernel cannot be made co-resident");
     int ni = (int)n;
     double* xw = w.vec;
@@ -572,7 +717,7 @@ int lu_solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t*
     const double* bc = b;
     void* args[] = {(void*)&LU, &lda, &ni, &w.perm, &bc, &xw, &tmp, &nrhs, &ldb, &w.bar, &flag};
     if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)lu_solve_kernel<T, C>, nblk, threads,
-                                                                args, 0, s),
+                                                                args, smem, s),
                                 "lu_solve_kernel"))
         return rc;
     ctx->launches++;
@@ -639,9 +784,9 @@ int bem_gemv(bem_ctx* ctx, int a_dtype, const void* A, int64_t m, int64_t n, int
     }
 }
 
-int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv, int64_t n,
-                     int64_t lda, const void* b, void* x, double tol, int maxit, int* iters, double* relres,
-                     void* stream) {
+int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv,
+                     const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit,
+                     int* iters, double* relres, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
     if (!A_hi || !LU_lo || !piv || !b || !x || n <= 0 || lda < n || maxit < 1 || !(tol > 0))
         return bem_fail(ctx, BEM_ERR_INVALID, "refine_solve: bad arguments");
@@ -687,7 +832,10 @@ int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* L
         // d = LU_lo^{-1} r
         rc = bem_check_cuda(ctx, cudaMemcpyAsync(d, r, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s), "d=r");
         if (rc) break;
-        rc = bem_lu_solve(ctx, C ? BEM_C64 : BEM_F32, LU_lo, n, lda, piv, d, 1, 1, s);
+        if (dinv)
+            rc = bem_lu_solve_tiled(ctx, C ? BEM_C64 : BEM_F32, LU_lo, n, lda, piv, dinv, d, s);
+        else
+            rc = bem_lu_solve(ctx, C ? BEM_C64 : BEM_F32, LU_lo, n, lda, piv, d, 1, 1, s);
         if (rc) break;
         axpy_kernel<<<(unsigned)((nd + 255) / 256), 256, 0, s>>>(xd, d, nd, 1.0);
         ctx->launches++;
@@ -697,9 +845,11 @@ int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* L
         rc = bem_gemv(ctx, dtype_hi, A_hi, n, n, lda, xd, r, -1.0, 1.0, s);
         if (rc) break;
         ++it;
+        const double prev = rnorm;
         rc = norm2(r, &rnorm);
         if (rc) break;
         if (rnorm <= tol * bnorm) break;
+        if (it >= 3 && rnorm > 0.5 * prev) break;  // stagnation: the factor is not a good enough preconditioner
     }
     cudaFreeAsync(r, s);
     if (iters) *iters = it;

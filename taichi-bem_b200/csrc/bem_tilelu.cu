@@ -1,0 +1,525 @@
+// Tile-pivoted LU and barrier-free triangular solves (the low-precision factor
+// of the mixed path).
+//
+// Factorisation, per diagonal block k (LU_T = 64 columns):
+//   diag   : one CTA factors the 64x64 diagonal block with partial pivoting
+//            restricted to the block's rows, and forms the explicit inverses
+//            Linv_k (unit lower) and Uinv_k (upper), stored in `dinv`;
+//   laswp  : the block's row swaps applied to the other columns;
+//   U12 = Linv_k A12 and L21 = A21 Uinv_k: one CTA per 64-wide tile, products
+//            out of shared memory (no sequential substitution);
+//   update : A22 -= L21 U12 (the trailing GEMM of bem_gemm.cuh).
+// No grid-wide synchronisation is needed.  Pivoting within the diagonal tile
+// is weaker than full partial pivoting; the FP64 iterative refinement that
+// consumes this factor corrects the difference (and reports non-convergence).
+//
+// Solve: a persistent kernel in which CTA b owns block rows b, b+P, b+2P...;
+// block row k accumulates L_kj x_j for every finished j < k (ready flags,
+// acquire/release, bounded waits), applies Linv_k, publishes x_k and its flag.
+// Each CTA handles its block rows in increasing order and all CTAs are
+// co-resident (cooperative launch), so every wait ends.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "bem_gemm.cuh"
+#include "bem_internal.cuh"
+
+namespace {
+
+constexpr int LU_T = 64;
+constexpr unsigned FLAG_SPIN_CAP = 1u << 22;
+
+template <typename T>
+struct CE {
+    T re, im;
+};
+
+template <typename T, bool C>
+__device__ __forceinline__ CE<T> ldE(const T* A, int64_t i) {
+    CE<T> e;
+    e.re = C ? A[2 * i] : A[i];
+    e.im = C ? A[2 * i + 1] : T(0);
+    return e;
+}
+template <typename T, bool C>
+__device__ __forceinline__ void stE(T* A, int64_t i, CE<T> e) {
+    if (C) {
+        A[2 * i] = e.re;
+        A[2 * i + 1] = e.im;
+    } else {
+        A[i] = e.re;
+    }
+}
+template <typename T>
+__device__ __forceinline__ CE<T> cmul(CE<T> a, CE<T> b) {
+    return CE<T>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T>
+__device__ __forceinline__ CE<T> cinv(CE<T> a) {
+    T d = a.re * a.re + a.im * a.im;
+    return d > T(0) ? CE<T>{a.re / d, -a.im / d} : CE<T>{T(0), T(0)};
+}
+
+// --------------------------------------------------------------------------
+// diagonal tile: GEPP inside the tile + explicit inverses
+// --------------------------------------------------------------------------
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n, int k0, int32_t* piv,
+                                                        CE<T>* dinv, int32_t* info) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CE<T>* S = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][LU_T]
+    CE<T>* Li = S + LU_T * LU_T;
+    CE<T>* Ui = Li + LU_T * LU_T;
+    __shared__ int s_p;
+    const int m = min(LU_T, n - k0);
+    for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
+        int r = e / LU_T, c = e - r * LU_T;
+        S[e] = (r < m && c < m) ? ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c) : CE<T>{T(0), T(0)};
+    }
+    __syncthreads();
+    for (int j = 0; j < m; ++j) {
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = j;
+            for (int r = j + threadIdx.x; r < m; r += 32) {
+                CE<T> v = S[r * LU_T + j];
+                double a = fabs((double)v.re) + fabs((double)v.im);
+                if (a > best || (a == best && r < bi)) {
+                    best = a;
+                    bi = r;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (threadIdx.x == 0) {
+                s_p = bi;
+                piv[k0 + j] = k0 + bi;
+                if (!(best > 0.0) && *info == 0) *info = k0 + j + 1;
+            }
+        }
+        __syncthreads();
+        const int p = s_p;
+        if (p != j)
+            for (int c = threadIdx.x; c < LU_T; c += blockDim.x) {
+                CE<T> t = S[j * LU_T + c];
+                S[j * LU_T + c] = S[p * LU_T + c];
+                S[p * LU_T + c] = t;
+            }
+        __syncthreads();
+        const CE<T> inv = cinv(S[j * LU_T + j]);
+        for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) S[r * LU_T + j] = cmul(S[r * LU_T + j], inv);
+        __syncthreads();
+        const int w = m - j - 1;
+        for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+            int r = j + 1 + e / w, c = j + 1 + e % w;
+            CE<T> l = S[r * LU_T + j], u = S[j * LU_T + c], v = S[r * LU_T + c];
+            CE<T> lu = cmul(l, u);
+            S[r * LU_T + c] = CE<T>{v.re - lu.re, v.im - lu.im};
+        }
+        __syncthreads();
+    }
+    // explicit inverses: column c of Linv solves L y = e_c, of Uinv solves U y = e_c
+    if (threadIdx.x < LU_T) {
+        const int c = threadIdx.x;
+        for (int r = 0; r < LU_T; ++r) {
+            CE<T> s = CE<T>{r == c ? T(1) : T(0), T(0)};
+            if (r < m)
+                for (int q = c; q < r; ++q) {
+                    CE<T> t = cmul(S[r * LU_T + q], Li[q * LU_T + c]);
+                    s.re -= t.re;
+                    s.im -= t.im;
+                }
+            Li[r * LU_T + c] = (r < c) ? CE<T>{T(0), T(0)} : s;
+        }
+    } else if (threadIdx.x < 2 * LU_T) {
+        const int c = threadIdx.x - LU_T;
+        for (int r = LU_T - 1; r >= 0; --r) {
+            CE<T> s = CE<T>{r == c ? T(1) : T(0), T(0)};
+            if (r < m && r <= c) {
+                for (int q = r + 1; q <= c && q < m; ++q) {
+                    CE<T> t = cmul(S[r * LU_T + q], Ui[q * LU_T + c]);
+                    s.re -= t.re;
+                    s.im -= t.im;
+                }
+                s = cmul(s, cinv(S[r * LU_T + r]));
+            } else if (r >= m) {
+                s = CE<T>{r == c ? T(1) : T(0), T(0)};
+            } else {
+                s = CE<T>{T(0), T(0)};
+            }
+            Ui[r * LU_T + c] = s;
+        }
+    }
+    __syncthreads();
+    CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T;
+    for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
+        D[e] = Li[e];
+        D[LU_T * LU_T + e] = Ui[e];
+        int r = e / LU_T, c = e - r * LU_T;
+        if (r < m && c < m) stE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c, S[e]);
+    }
+}
+
+template <typename T, bool C>
+__global__ void tile_laswp_kernel(T* A, int64_t lda, int n, int k0, int m, const int32_t* piv) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || (c >= k0 && c < k0 + m)) return;
+    for (int j = 0; j < m; ++j) {
+        int r1 = k0 + j, r2 = piv[k0 + j];
+        if (r1 == r2) continue;
+        CE<T> a = ldE<T, C>(A, (int64_t)r1 * lda + c);
+        CE<T> b = ldE<T, C>(A, (int64_t)r2 * lda + c);
+        stE<T, C>(A, (int64_t)r1 * lda + c, b);
+        stE<T, C>(A, (int64_t)r2 * lda + c, a);
+    }
+}
+
+// mode 0: U12 tile (rows k0.., 64 columns) <- Linv * tile
+// mode 1: L21 tile (64 rows, columns k0..) <- tile * Uinv
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int n, int k0, int m, const CE<T>* dinv,
+                                                         int mode) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CE<T>* M = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][LU_T] inverse
+    CE<T>* X = M + LU_T * LU_T;                     // [LU_T][LU_T] tile
+    const CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T + (mode == 0 ? 0 : LU_T * LU_T);
+    const int base = k0 + m + blockIdx.x * LU_T;  // first column (mode 0) / row (mode 1) of the tile
+    const int cnt = min(LU_T, n - base);
+    for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
+        M[e] = D[e];
+        int r = e / LU_T, c = e - r * LU_T;
+        CE<T> v = CE<T>{T(0), T(0)};
+        if (mode == 0) {
+            if (r < m && c < cnt) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + base + c);
+        } else {
+            if (r < cnt && c < m) v = ldE<T, C>(A, (int64_t)(base + r) * lda + k0 + c);
+        }
+        X[e] = v;
+    }
+    __syncthreads();
+    // each thread: 16 outputs (4 rows x 4 columns)
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    CE<T> acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = CE<T>{T(0), T(0)};
+    for (int q = 0; q < m; ++q) {
+        CE<T> a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            a[i] = mode == 0 ? M[(ty * 4 + i) * LU_T + q] : X[(ty * 4 + i) * LU_T + q];
+            b[i] = mode == 0 ? X[q * LU_T + tx * 4 + i] : M[q * LU_T + tx * 4 + i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                acc[i][j].re += a[i].re * b[j].re - (C ? a[i].im * b[j].im : T(0));
+                if (C) acc[i][j].im += a[i].re * b[j].im + a[i].im * b[j].re;
+            }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int r = ty * 4 + i, c = tx * 4 + j;
+            if (mode == 0) {
+                if (r < m && c < cnt) stE<T, C>(A, (int64_t)(k0 + r) * lda + base + c, acc[i][j]);
+            } else {
+                if (r < cnt && c < m) stE<T, C>(A, (int64_t)(base + r) * lda + k0 + c, acc[i][j]);
+            }
+        }
+}
+
+// --------------------------------------------------------------------------
+// barrier-free triangular solves
+// --------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire_i(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_i(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits (bounded) until flags[j] == epoch.  Returns false on timeout / failure.
+__device__ __forceinline__ bool wait_flag(const int* flags, int j, int epoch, int32_t* err) {
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned it = 0;
+        while (ld_acquire_i(flags + j) != epoch) {
+            if (++it > FLAG_SPIN_CAP) {
+                atomicExch(err, BEM_ERR_TIMEOUT);
+                ok = 0;
+                break;
+            }
+            if ((it & 63u) == 0u && *(volatile int32_t*)err != 0) {
+                ok = 0;
+                break;
+            }
+            if (it > 256u) __nanosleep(64);
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// x (FP64, real or complex interleaved, one right-hand side) overwritten by
+// U^{-1} L^{-1} x; the input must already be permuted (x = P b).
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) tile_solve_kernel(const T* LU, int64_t lda, int n, const CE<T>* dinv,
+                                                         double* x, int* flags, int epoch, int32_t* err) {
+    __shared__ double s_acc[LU_T][2];
+    __shared__ double s_part[8][LU_T][2];
+    __shared__ double s_y[LU_T][2];
+    const int nbk = (n + LU_T - 1) / LU_T;
+    const int P = gridDim.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int W = C ? 2 : 1;
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool fwd = pass == 0;
+        for (int t = blockIdx.x; t < nbk; t += P) {
+            const int k = fwd ? t : nbk - 1 - t;
+            const int r0 = k * LU_T, m = min(LU_T, n - r0);
+            // partial sums over finished blocks: warp w handles dependency blocks j = w, w+8, ...
+            for (int i = threadIdx.x; i < 8 * LU_T * 2; i += blockDim.x) (&s_part[0][0][0])[i] = 0.0;
+            __syncthreads();
+            const int ndep = fwd ? k : nbk - 1 - k;
+            for (int d = 0; d < ndep; ++d) {
+                const int j = fwd ? d : nbk - 1 - d;
+                if (!wait_flag(flags, pass * nbk + j, epoch, err)) return;
+                const int c0 = j * LU_T, mj = min(LU_T, n - c0);
+                // x_j segment
+                double xr0 = 0, xi0 = 0, xr1 = 0, xi1 = 0;
+                if (lane < mj) {
+                    xr0 = __ldcg(&x[W * (c0 + lane)]);
+                    xi0 = C ? __ldcg(&x[W * (c0 + lane) + 1]) : 0.0;
+                }
+                if (lane + 32 < mj) {
+                    xr1 = __ldcg(&x[W * (c0 + lane + 32)]);
+                    xi1 = C ? __ldcg(&x[W * (c0 + lane + 32) + 1]) : 0.0;
+                }
+                for (int r = wid; r < m; r += 8) {
+                    const T* row = LU + (C ? 2 : 1) * ((int64_t)(r0 + r) * lda + c0);
+                    double sr = 0.0, si = 0.0;
+                    if (lane < mj) {
+                        CE<T> l = ldE<T, C>(row, lane);
+                        sr += (double)l.re * xr0 - (double)l.im * xi0;
+                        si += (double)l.re * xi0 + (double)l.im * xr0;
+                    }
+                    if (lane + 32 < mj) {
+                        CE<T> l = ldE<T, C>(row, lane + 32);
+                        sr += (double)l.re * xr1 - (double)l.im * xi1;
+                        si += (double)l.re * xi1 + (double)l.im * xr1;
+                    }
+                    for (int o = 16; o > 0; o >>= 1) {
+                        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                        si += __shfl_xor_sync(0xffffffffu, si, o);
+                    }
+                    if (lane == 0) {
+                        s_part[wid][r][0] += sr;
+                        s_part[wid][r][1] += si;
+                    }
+                }
+                __syncthreads();
+            }
+            // rhs of block k minus the dependencies
+            for (int r = threadIdx.x; r < LU_T; r += blockDim.x) {
+                double ar = 0.0, ai = 0.0;
+                if (r < m) {
+                    ar = __ldcg(&x[W * (r0 + r)]);
+                    ai = C ? __ldcg(&x[W * (r0 + r) + 1]) : 0.0;
+                    for (int w = 0; w < 8; ++w) {
+                        ar -= s_part[w][r][0];
+                        ai -= s_part[w][r][1];
+                    }
+                }
+                s_acc[r][0] = ar;
+                s_acc[r][1] = ai;
+            }
+            __syncthreads();
+            // y = inverse(diagonal block) * acc
+            const CE<T>* Dk = dinv + (size_t)k * 2 * LU_T * LU_T + (fwd ? 0 : LU_T * LU_T);
+            for (int r = wid; r < m; r += 8) {
+                double sr = 0.0, si = 0.0;
+                for (int q = lane; q < m; q += 32) {
+                    CE<T> d = Dk[r * LU_T + q];
+                    sr += (double)d.re * s_acc[q][0] - (double)d.im * s_acc[q][1];
+                    si += (double)d.re * s_acc[q][1] + (double)d.im * s_acc[q][0];
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                    si += __shfl_xor_sync(0xffffffffu, si, o);
+                }
+                if (lane == 0) {
+                    s_y[r][0] = sr;
+                    s_y[r][1] = si;
+                }
+            }
+            __syncthreads();
+            for (int r = threadIdx.x; r < m; r += blockDim.x) {
+                x[W * (r0 + r)] = s_y[r][0];
+                if (C) x[W * (r0 + r) + 1] = s_y[r][1];
+            }
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) st_release_i(flags + pass * nbk + k, epoch);
+        }
+        // the backward pass of block k needs x_k from the forward pass: every
+        // block row's forward flag is checked before its value is read below
+        if (fwd) {
+            for (int t = blockIdx.x; t < nbk; t += P) {
+                const int k = nbk - 1 - t;
+                if (!wait_flag(flags, k, epoch, err)) return;
+            }
+        }
+    }
+}
+
+__global__ void permute_kernel(const double* b, const int32_t* perm, double* x, int n, int W) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = perm[i];
+    for (int w = 0; w < W; ++w) x[W * i + w] = b[W * s + w];
+}
+
+__global__ void tile_piv_to_perm_kernel(const int32_t* piv, int32_t* perm, int n) {
+    extern __shared__ int32_t sp[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < n; ++i) {
+            int p = piv[i];
+            if (p != i && p >= 0 && p < n) {
+                int t = sp[i];
+                sp[i] = sp[p];
+                sp[p] = t;
+            }
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sp[i];
+}
+
+template <typename T, bool C>
+int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* dinv, int32_t* info,
+             cudaStream_t s) {
+    cudaMemsetAsync(info, 0, sizeof(int32_t), s);
+    const size_t dsmem = sizeof(CE<T>) * 3 * LU_T * LU_T;
+    const size_t asmem = sizeof(CE<T>) * 2 * LU_T * LU_T;
+    cudaFuncSetAttribute(tile_diag_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem);
+    cudaFuncSetAttribute(tile_apply_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem);
+    const int ni = (int)n;
+    for (int64_t k0 = 0; k0 < n; k0 += LU_T) {
+        const int m = (int)std::min<int64_t>(LU_T, n - k0);
+        const int k0i = (int)k0;
+        tile_diag_kernel<T, C><<<1, 256, dsmem, s>>>(A, lda, ni, k0i, piv, dinv, info);
+        tile_laswp_kernel<T, C><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, lda, ni, k0i, m, piv);
+        ctx->launches += 2;
+        const int64_t rest = n - k0 - m;
+        if (rest > 0) {
+            const unsigned tiles = (unsigned)((rest + LU_T - 1) / LU_T);
+            tile_apply_kernel<T, C><<<tiles, 256, asmem, s>>>(A, lda, ni, k0i, m, dinv, 0);
+            tile_apply_kernel<T, C><<<tiles, 256, asmem, s>>>(A, lda, ni, k0i, m, dinv, 1);
+            ctx->launches += 2;
+            T* A22 = A + (C ? 2 : 1) * ((k0 + m) * lda + k0 + m);
+            const T* L21 = A + (C ? 2 : 1) * ((k0 + m) * lda + k0);
+            const T* U12 = A + (C ? 2 : 1) * (k0 * lda + k0 + m);
+            if (int rc = bem_gemm_update<T, C>(ctx, A22, L21, U12, rest, rest, m, lda, s)) return rc;
+        }
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "tiled lu step")) return rc;
+    }
+    return BEM_OK;
+}
+
+template <typename T, bool C>
+int solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t* piv, const CE<T>* dinv, double* b,
+            cudaStream_t s) {
+    const int W = C ? 2 : 1;
+    const int nbk = (int)((n + LU_T - 1) / LU_T);
+    // workspace: perm [n], flags [2*nbk], x [W*n]
+    size_t off_flags = ((size_t)n * 4 + 255) & ~size_t(255);
+    size_t off_x = off_flags + (((size_t)2 * nbk * 4 + 255) & ~size_t(255));
+    size_t total = off_x + sizeof(double) * W * (size_t)n;
+    if (int rc = bem_ws_reserve(ctx, total)) return rc;
+    char* base = (char*)ctx->ws;
+    int32_t* perm = (int32_t*)base;
+    int* flags = (int*)(base + off_flags);
+    double* x = (double*)(base + off_x);
+    if ((size_t)n * sizeof(int32_t) > 200 * 1024) return bem_fail(ctx, BEM_ERR_INVALID, "tiled solve: n > 51200");
+    cudaFuncSetAttribute(tile_piv_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(n * sizeof(int32_t)));
+    tile_piv_to_perm_kernel<<<1, 256, n * sizeof(int32_t), s>>>(piv, perm, (int)n);
+    permute_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, perm, x, (int)n, W);
+    cudaMemsetAsync(flags, 0, sizeof(int) * 2 * nbk, s);
+    cudaMemsetAsync(ctx->flags + 3, 0, sizeof(int32_t), s);
+    ctx->launches += 2;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, 0);
+    int P = std::max(1, std::min(nbk, per_sm * ctx->num_sms));
+    P = std::min(P, ctx->num_sms);
+    int ni = (int)n, epoch = 1;
+    int32_t* err = ctx->flags + 3;
+    void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err};
+    if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args,
+                                                                0, s),
+                                "tile_solve_kernel"))
+        return rc;
+    ctx->launches++;
+    if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(b, x, sizeof(double) * W * n, cudaMemcpyDeviceToDevice, s),
+                                "tiled solve copy"))
+        return rc;
+    int32_t e = 0;
+    cudaMemcpyAsync(&e, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "tiled solve")) return rc;
+    if (e != 0) return bem_fail(ctx, BEM_ERR_TIMEOUT, "tiled solve: a ready-flag wait hit its iteration cap");
+    return BEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t bem_lu_dinv_elems(int64_t n) { return ((n + LU_T - 1) / LU_T) * 2 * LU_T * LU_T; }
+
+int bem_lu_factor_tiled(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, void* dinv,
+                        int32_t* info, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A || !piv || !dinv || !info || n <= 0 || lda < n || n > (1 << 30))
+        return bem_fail(ctx, BEM_ERR_INVALID, "lu_factor_tiled: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (dtype) {
+        case BEM_F64: return factor_t<double, false>(ctx, (double*)A, n, lda, piv, (CE<double>*)dinv, info, s);
+        case BEM_C128: return factor_t<double, true>(ctx, (double*)A, n, lda, piv, (CE<double>*)dinv, info, s);
+        case BEM_F32: return factor_t<float, false>(ctx, (float*)A, n, lda, piv, (CE<float>*)dinv, info, s);
+        case BEM_C64: return factor_t<float, true>(ctx, (float*)A, n, lda, piv, (CE<float>*)dinv, info, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "lu_factor_tiled: unknown dtype");
+    }
+}
+
+int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
+                       const void* dinv, void* b, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!LU || !piv || !dinv || !b || n <= 0 || lda < n)
+        return bem_fail(ctx, BEM_ERR_INVALID, "lu_solve_tiled: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (dtype) {
+        case BEM_F64: return solve_t<double, false>(ctx, (const double*)LU, n, lda, piv, (const CE<double>*)dinv, (double*)b, s);
+        case BEM_C128: return solve_t<double, true>(ctx, (const double*)LU, n, lda, piv, (const CE<double>*)dinv, (double*)b, s);
+        case BEM_F32: return solve_t<float, false>(ctx, (const float*)LU, n, lda, piv, (const CE<float>*)dinv, (double*)b, s);
+        case BEM_C64: return solve_t<float, true>(ctx, (const float*)LU, n, lda, piv, (const CE<float>*)dinv, (double*)b, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "lu_solve_tiled: unknown dtype");
+    }
+}
+
+}  // extern "C"
