@@ -159,11 +159,14 @@ def phase_breakdown(b):
         return r
 
     b._mat_A.zero_()
-    timed("assemble_V", lambda: b.matrix_layer_forward(k=b._k, scope_type=b._scope_type))
-    timed("block_add", lambda: b.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0))
-    timed("boundary_data", lambda: b.rhs_constructor.set_boundaries(b._scope_type, b._sqrt_ni, b._sqrt_no))
-    timed("rhs_half_M_plus_K_g", lambda: b.rhs_layer_forward(k=b._k, scope_type=b._scope_type))
-    timed("rhs_copy", b.assemble_rhs)
+    if b._fusable():
+        timed("assemble_V_and_Kg_fused_plus_rhs", b._run_dirichlet_fused)
+    else:
+        timed("assemble_V", lambda: b.matrix_layer_forward(k=b._k, scope_type=b._scope_type))
+        timed("block_add", lambda: b.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0))
+        timed("boundary_data", lambda: b.rhs_constructor.set_boundaries(b._scope_type, b._sqrt_ni, b._sqrt_no))
+        timed("rhs_half_M_plus_K_g", lambda: b.rhs_layer_forward(k=b._k, scope_type=b._scope_type))
+        timed("rhs_copy", b.assemble_rhs)
     A = b._mat_A
     lo = torch.complex64 if A.is_complex() else torch.float32
     LU = timed("cast_fp32", lambda: A.to(lo))
@@ -180,14 +183,40 @@ def phase_breakdown(b):
     return out
 
 
+def profile_step(precision: str):
+    """One warm-up and one timed step of the workload, nothing else (the
+    command the committed ncu summaries under profiles/ were captured with)."""
+    import torch
+    from bem_b200.managers import CoreManager
+    from bem_b200.workloads import config2
+    params, fD, fN = config2(precision=precision)
+    core = CoreManager(params)
+    core.initialization(fD, fN)
+    b = core._BEM_manager
+    b.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.run()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_step": precision, "ms": e0.elapsed_time(e1), "launches": b.engine.launches}))
+    core.kill()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--profile-step", default=None, choices=["mixed", "fp64"],
+                    help="run one warm-up and one step of the workload and exit (for ncu captures)")
     args = ap.parse_args()
     ws, rank, local = _dist()
+    if args.profile_step:
+        profile_step(args.profile_step)
+        return
 
     if args.impl == "reference":
         if rank != 0:

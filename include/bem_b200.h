@@ -119,6 +119,18 @@ int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, con
 int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
               int dtype, const void* x, void* y, double scale, int conj_x, void* stream);
 
+/* Fused Dirichlet-system pass: out[row*ld+col] += scale*V(row,col) over
+ * test x trial (both P0) AND y[rows(i)] += scale_k * sum_j K(i,j) g over the
+ * same panel pairs, K's trial basis and data indices given by `data` (same
+ * panel list as `trial`, nb = 1 or 3, indices into g; g conjugated when
+ * conj_g).  One sweep over the quadrature points serves both integrands; it
+ * replaces SingleLayer3d.forward (single_layer_3d.py:371-433) followed by
+ * DoubleLayer3d.apply_K_dot_D_boundary (double_layer_3d.py:440-501) in
+ * BEMManager.run for the Dirichlet problem.  op->op must be BEM_OP_V. */
+int bem_assemble_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                           void* out, int64_t ld, double scale, const bem_space* rows, const bem_space* data,
+                           const void* g, void* y, double scale_k, int conj_g, void* stream);
+
 /* Identity (mass) block on one panel list (the test side's `panels`; the
  * trial side must have the same n_panels and only contributes its dof table):
  * dense (out/out_t) or apply (x != NULL: y += scale*M*x).  Replaces

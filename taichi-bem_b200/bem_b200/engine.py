@@ -162,6 +162,19 @@ class Engine:
                                        _dtype_code(y), _ptr(x), _ptr(y), float(scale), int(bool(conj_x)),
                                        _stream_ptr()))
 
+    def assemble_dirichlet(self, desc: L.OpDesc, test: DeviceSpace, trial: DeviceSpace, out: torch.Tensor,
+                           rows: DeviceSpace, data: DeviceSpace, g: torch.Tensor, y: torch.Tensor, scale=1.0,
+                           scale_k=1.0, conj_g=False):
+        """One pass: out += scale * V (test x trial) and y += scale_k * K g."""
+        assert out.is_cuda and out.dim() == 2 and out.stride(1) == 1 and g.is_contiguous() and y.is_contiguous()
+        self._check_spaces(test, trial, out.shape[0], out.shape[1])
+        self._check_spaces(rows, data, y.numel(), g.numel())
+        ts, rs, ws, ds = test.c(), trial.c(), rows.c(), data.c()
+        self._check(self.lib.bem_assemble_dirichlet(self.ctx, ctypes.byref(desc), ctypes.byref(ts), ctypes.byref(rs),
+                                                    _ptr(out), out.stride(0), float(scale), ctypes.byref(ws),
+                                                    ctypes.byref(ds), _ptr(g), _ptr(y), float(scale_k),
+                                                    int(bool(conj_g)), _stream_ptr()))
+
     def mass(self, test: DeviceSpace, trial: DeviceSpace, out=None, scale=1.0, out_t=None, scale_t=0.0, x=None,
              y=None, conj_x=False):
         ts, rs = test.c(), trial.c()

@@ -73,6 +73,9 @@ class BEMManager:
         if self.precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.quirk = bool(p.get("quirk", True))
+        # one sweep for V and K g in the Dirichlet problem (the plain path keeps
+        # one kernel per operator)
+        self.fuse = bool(p.get("fuse", self.precision == "mixed"))
         self.solver = p.get("solver", "lstsq" if self._is_transmission else "lu")
         self.refine_tol = float(p.get("refine_tol", 1e-12))
         self.refine_maxit = int(p.get("refine_maxit", 60))
@@ -372,6 +375,35 @@ class BEMManager:
                 splat_p1("D", self._Dirichlet_offset_j, int(VertAttachType.NEUMANN_TOBESOLVED))
 
     # -- driver ----------------------------------------------------------------------------
+    def _fusable(self) -> bool:
+        """Dirichlet problem with P0 Neumann unknowns: V and K g share every
+        panel pair (Neumann x Neumann), so one sweep serves both."""
+        return (self.fuse and not self._is_transmission and self.M_Dirichlet == 0 and self.N_Neumann > 0
+                and self.shape_func_degree_Neumann == 0 and self.num_of_panels_Dirichlet == 0)
+
+    def _run_dirichlet_fused(self):
+        """matrix_layer_forward + assemble_matA(ADD_M, -1) + set_boundaries +
+        rhs_layer_forward + assemble_rhs with V and K g assembled in one pass."""
+        rc = self.rhs_constructor
+        rc.set_boundaries(scope_type=self._scope_type, sqrt_ni=self._sqrt_ni, sqrt_no=self._sqrt_no)
+        lay = self.single_layer
+        if lay._Vmat is None:
+            lay._Vmat = lay._zeros(self.N_Neumann, self.N_Neumann)
+        else:
+            lay._Vmat.zero_()
+        rc._rhs_vec.zero_()
+        sp = self.space("charge", self.shape_func_degree_Neumann, "N", int(CellFluxType.NEUMANN_TOBESOLVED))
+        rows = self.space("charge", self.shape_func_degree_Neumann, "N", int(CellFluxType.NEUMANN_TOBESOLVED),
+                          offset=self._Neumann_offset_i)
+        data = self.space("data", self.shape_func_degree_Dirichlet, "N")
+        desc = self.op_desc(L.OP_V, self._k, 1.0)
+        self.engine.assemble_dirichlet(desc, sp, sp, lay._Vmat, rows, data, rc._Dirichlet_boundary, rc._rhs_vec,
+                                       scale=1.0, scale_k=1.0, conj_g=self.conj_data)
+        half = 0.5 if self._scope_type == int(ScopeType.INTERIOR) else -0.5
+        rc.multiply_identity_to_vector(multiplier=half)
+        self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)
+        self.assemble_rhs()
+
     def run(self):
         """BEMManager.run (BEM_manager.py:990-1030) without the GUI colouring."""
         self._mat_A.zero_()
@@ -383,6 +415,8 @@ class BEMManager:
             self.assemble_rhs()
             self.matrix_layer_forward(k=self._k, sqrt_n=self._sqrt_ni, scope_type=int(ScopeType.INTERIOR))
             self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
+        elif self._fusable():
+            self._run_dirichlet_fused()
         else:
             self.matrix_layer_forward(k=self._k, scope_type=self._scope_type)
             self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)

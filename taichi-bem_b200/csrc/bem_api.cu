@@ -304,6 +304,26 @@ int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const 
                                (cudaStream_t)stream);
 }
 
+int bem_assemble_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                           void* out, int64_t ld, double scale, const bem_space* rows, const bem_space* data,
+                           const void* g, void* y, double scale_k, int conj_g, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
+    if (int rc = check_op(ctx, op)) return rc;
+    if (op->op != BEM_OP_V) return bem_fail(ctx, BEM_ERR_INVALID, "assemble_dirichlet: op must be BEM_OP_V");
+    if (int rc = check_space(ctx, test, "test")) return rc;
+    if (int rc = check_space(ctx, trial, "trial")) return rc;
+    if (int rc = check_space(ctx, rows, "rows")) return rc;
+    if (int rc = check_space(ctx, data, "data")) return rc;
+    if (test->nb != 1 || trial->nb != 1 || rows->nb != 1)
+        return bem_fail(ctx, BEM_ERR_INVALID, "assemble_dirichlet: V test/trial and rhs rows must be P0");
+    if (rows->n_panels != test->n_panels || data->n_panels != trial->n_panels)
+        return bem_fail(ctx, BEM_ERR_INVALID, "assemble_dirichlet: rows/data must run over the test/trial panels");
+    if (!out || ld <= 0 || !g || !y) return bem_fail(ctx, BEM_ERR_INVALID, "assemble_dirichlet: NULL buffer");
+    return bem_launch_dirichlet(ctx, op, test, trial, out, ld, scale, rows, data, g, y, scale_k, conj_g,
+                                (cudaStream_t)stream);
+}
+
 int bem_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int dtype, void* out, int64_t ld,
              double scale, void* out_t, double scale_t, const void* x, void* y, int conj_x, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;

@@ -41,7 +41,35 @@ struct V4T<double> {
 
 __device__ __forceinline__ float dev_rsqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double dev_rsqrt(double x) { return rsqrt(x); }
-__device__ __forceinline__ void dev_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+// FP32 sine/cosine of the Helmholtz phase k r (k r >= 0 and moderate): Cody-
+// Waite reduction by pi/2 with a two-term split of pi/2 (exact FMA products
+// for |n| < 2^12), Taylor polynomials of sin (through y^9) and cos (through
+// y^10) on |y| <= pi/4 (truncation below 3e-9), and the quadrant rotation.
+__device__ __forceinline__ void dev_sincos(float x, float* s, float* c) {
+    const float kTwoOverPi = 0.636619772367581343f;
+    const float kPio2Hi = 1.57079637050628662109375f;  // pi/2 rounded to float
+    const float kPio2Lo = -4.37113900018624283e-08f;   // pi/2 - kPio2Hi
+    const float fn = rintf(x * kTwoOverPi);
+    const int q = (int)fn;
+    float y = fmaf(-fn, kPio2Hi, x);
+    y = fmaf(-fn, kPio2Lo, y);
+    const float y2 = y * y;
+    // sin y = y (1 - y^2/3! + y^4/5! - y^6/7! + y^8/9!)
+    float ps = fmaf(y2, 2.75573192239858907e-06f, -1.98412698412698413e-04f);
+    ps = fmaf(y2, ps, 8.33333333333333333e-03f);
+    ps = fmaf(y2, ps, -1.66666666666666667e-01f);
+    const float sy = fmaf(y * y2, ps, y);
+    // cos y = 1 - y^2/2! + y^4/4! - y^6/6! + y^8/8! - y^10/10!
+    float pc = fmaf(y2, -2.75573192239858907e-07f, 2.48015873015873016e-05f);
+    pc = fmaf(y2, pc, -1.38888888888888889e-03f);
+    pc = fmaf(y2, pc, 4.16666666666666667e-02f);
+    pc = fmaf(y2, pc, -0.5f);
+    const float cy = fmaf(y2, pc, 1.0f);
+    float ss = (q & 1) ? cy : sy;
+    float cc = (q & 1) ? sy : cy;
+    *s = (q & 2) ? -ss : ss;
+    *c = ((q + 1) & 2) ? -cc : cc;
+}
 __device__ __forceinline__ void dev_sincos(double x, double* s, double* c) { sincos(x, s, c); }
 
 struct cxd {
@@ -280,9 +308,13 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
             for (int by = 0; by < AY; ++by) acc_re[bx][by] = acc_im[bx][by] = 0.0;
 
         if (sep) {
-            const T dcx = T(s_cen[t][0] - cen_j[0]);
-            const T dcy = T(s_cen[t][1] - cen_j[1]);
-            const T dcz = T(s_cen[t][2] - cen_j[2]);
+            // centroid difference as an unevaluated pair hi + lo: in FP32 a
+            // single rounding of it would be one systematic error shared by
+            // all GaussQR^4 terms of the pair
+            const double dcx64 = s_cen[t][0] - cen_j[0], dcy64 = s_cen[t][1] - cen_j[1],
+                         dcz64 = s_cen[t][2] - cen_j[2];
+            const T dcx = T(dcx64), dcy = T(dcy64), dcz = T(dcz64);
+            const T dlx = T(dcx64 - double(dcx)), dly = T(dcy64 - double(dcy)), dlz = T(dcz64 - double(dcz));
             T nx, ny, nz;
             if (OP == BEM_OP_KP) {
                 nx = T(s_nrm[t][0]);
@@ -296,7 +328,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
             const V4* sxt = sx + t * Q2;
             for (int b = 0; b < Q2; ++b) {
                 const V4 yb = ptsj[b];
-                const T ex = dcx - yb.x, ey = dcy - yb.y, ez = dcz - yb.z;
+                const T ex = (dcx - yb.x) + dlx, ey = (dcy - yb.y) + dly, ez = (dcz - yb.z) + dlz;
                 T s_re[AX], s_im[AX];
                 T c_re = T(0), c_im = T(0);
 #pragma unroll
@@ -739,6 +771,362 @@ __global__ void mass_kernel(MassArgs a) {
     }
 }
 
+// ----------------------------------------------------------------------------
+// Fused Dirichlet-system pass: V (P0 x P0, dense) and the matrix-free K g
+// (P0 test rows, g interpolated from P1 vertex data) over the same separate
+// panel pairs.  Both integrands share the points, r, 1/r and e^{ikr}; the
+// reference computes them in two sweeps (SingleLayer3d.forward,
+// single_layer_3d.py:371-433, and DoubleLayer3d.apply_K_dot_D_boundary,
+// double_layer_3d.py:440-501).
+// ----------------------------------------------------------------------------
+struct VkgArgs {
+    const double* g;      // boundary data (real or complex interleaved)
+    const int32_t* gdof;  // [n_trial * gnb] data index per trial panel basis
+    int gnb;              // 1 (P0 data) or 3 (P1 data)
+    const int32_t* rows;  // [n_test] rhs row of each test panel, <0 = skipped
+    double* y;
+    double scale;
+    int conj;
+};
+
+template <bool HELM, typename T>
+__global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs v) {
+    using V4 = typename V4T<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V4* sx = reinterpret_cast<V4*>(smem_raw);
+    T* sphi = reinterpret_cast<T*>(sx + FAR_TI * a.Q2);
+    __shared__ int s_gi[FAR_TI];
+    __shared__ int s_tri[FAR_TI][3];
+    __shared__ double s_cen[FAR_TI][3];
+
+    const int Q2 = a.Q2;
+    const int lj = blockIdx.x * FAR_THREADS + threadIdx.x;
+    const int li0 = blockIdx.y * FAR_TI;
+    const V4* pts = reinterpret_cast<const V4*>(a.pts);
+    for (int idx = threadIdx.x; idx < FAR_TI * Q2; idx += FAR_THREADS) {
+        int t = idx / Q2, q = idx - t * Q2;
+        int li = li0 + t;
+        if (li < a.n_test) sx[idx] = pts[(size_t)a.test_panels[li] * Q2 + q];
+    }
+    {
+        const T* phi = reinterpret_cast<const T*>(a.phi);
+        for (int idx = threadIdx.x; idx < Q2 * 3; idx += FAR_THREADS) sphi[idx] = phi[idx];
+    }
+    if (threadIdx.x < FAR_TI) {
+        int li = li0 + threadIdx.x;
+        int gi = li < a.n_test ? a.test_panels[li] : -1;
+        s_gi[threadIdx.x] = gi;
+        for (int c = 0; c < 3; ++c) {
+            s_tri[threadIdx.x][c] = gi >= 0 ? a.tris[3 * gi + c] : -1;
+            s_cen[threadIdx.x][c] = gi >= 0 ? a.centroid[3 * gi + c] : 0.0;
+        }
+    }
+    __syncthreads();
+
+    const bool valid_j = lj < a.n_trial;
+    const int gj = valid_j ? a.trial_panels[lj] : 0;
+    int tri_j[3];
+    double cen_j[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        tri_j[c] = a.tris[3 * gj + c];
+        cen_j[c] = a.centroid[3 * gj + c];
+    }
+    const T nx = T(a.normal[3 * gj + 0]), ny = T(a.normal[3 * gj + 1]), nz = T(a.normal[3 * gj + 2]);
+    // trial data at the trial panel's basis functions (conjugated when asked)
+    T gr[3] = {T(0), T(0), T(0)}, gim[3] = {T(0), T(0), T(0)};
+    if (valid_j) {
+        for (int by = 0; by < v.gnb; ++by) {
+            int d = v.gdof[lj * v.gnb + by];
+            if (d < 0) continue;
+            gr[by] = T(HELM ? v.g[2 * d] : v.g[d]);
+            gim[by] = HELM ? T(v.conj ? -v.g[2 * d + 1] : v.g[2 * d + 1]) : T(0);
+        }
+    }
+    const V4* ptsj = pts + (size_t)gj * Q2;
+    const T kk = T(a.k);
+    const int lane = threadIdx.x & 31;
+
+    for (int t = 0; t < FAR_TI; ++t) {
+        const int li = li0 + t;
+        if (li >= a.n_test) break;
+        const int gi = s_gi[t];
+        const bool sep = valid_j && (bem_relation(s_tri[t], tri_j, gi == gj) == REL_SEPARATE);
+        double av_re = 0.0, av_im = 0.0, ak_re = 0.0, ak_im = 0.0;
+        if (sep) {
+            // centroid difference as an unevaluated pair hi + lo: in FP32 a
+            // single rounding of it would be one systematic error shared by
+            // all GaussQR^4 terms of the pair
+            const double dcx64 = s_cen[t][0] - cen_j[0], dcy64 = s_cen[t][1] - cen_j[1],
+                         dcz64 = s_cen[t][2] - cen_j[2];
+            const T dcx = T(dcx64), dcy = T(dcy64), dcz = T(dcz64);
+            const T dlx = T(dcx64 - double(dcx)), dly = T(dcy64 - double(dcy)), dlz = T(dcz64 - double(dcz));
+            const V4* sxt = sx + t * Q2;
+            for (int b = 0; b < Q2; ++b) {
+                const V4 yb = ptsj[b];
+                const T ex = (dcx - yb.x) + dlx, ey = (dcy - yb.y) + dly, ez = (dcz - yb.z) + dlz;
+                T sv_re = T(0), sv_im = T(0), sk_re = T(0), sk_im = T(0);
+#pragma unroll 5
+                for (int q = 0; q < Q2; ++q) {
+                    const V4 xa = sxt[q];
+                    const T dx = xa.x + ex, dy = xa.y + ey, dz = xa.z + ez;
+                    const T r2 = dx * dx + dy * dy + dz * dz;
+                    const T rinv = dev_rsqrt(r2);
+                    const T dn = dx * nx + dy * ny + dz * nz;
+                    const T wr = xa.w * rinv;
+                    const T tk = xa.w * dn * rinv * rinv * rinv;
+                    if (HELM) {
+                        const T kr = kk * (r2 * rinv);
+                        T sn, cs;
+                        dev_sincos(kr, &sn, &cs);
+                        sv_re += wr * cs;
+                        sv_im += wr * sn;
+                        sk_re += tk * fma(kr, sn, cs);
+                        sk_im += tk * fma(-kr, cs, sn);
+                    } else {
+                        sv_re += wr;
+                        sk_re += tk;
+                    }
+                }
+                const double wb = double(yb.w);
+                av_re += wb * double(sv_re);
+                av_im += wb * double(sv_im);
+                // g interpolated at trial point b
+                T gb_re = gr[0], gb_im = gim[0];
+                if (v.gnb == 3) {
+                    const T p0 = sphi[3 * b], p1 = sphi[3 * b + 1], p2 = sphi[3 * b + 2];
+                    gb_re = p0 * gr[0] + p1 * gr[1] + p2 * gr[2];
+                    gb_im = p0 * gim[0] + p1 * gim[1] + p2 * gim[2];
+                }
+                ak_re += wb * (double(sk_re) * double(gb_re) - double(sk_im) * double(gb_im));
+                ak_im += wb * (double(sk_re) * double(gb_im) + double(sk_im) * double(gb_re));
+            }
+            const int row = a.test_dof[li];
+            const int col = a.trial_dof[lj];
+            if (row >= 0 && col >= 0)
+                add_entry<HELM>(a.out, (int64_t)row * a.ld + col, a.scale * BEM_INV4PI * av_re,
+                                a.scale * BEM_INV4PI * av_im, false);
+        }
+        ak_re = warp_sum(ak_re);
+        if (HELM) ak_im = warp_sum(ak_im);
+        if (lane == 0) {
+            const int row = v.rows[li];
+            if (row >= 0) {
+                if (HELM) {
+                    atomicAdd(v.y + 2 * row, v.scale * BEM_INV4PI * ak_re);
+                    atomicAdd(v.y + 2 * row + 1, v.scale * BEM_INV4PI * ak_im);
+                } else {
+                    atomicAdd(v.y + row, v.scale * BEM_INV4PI * ak_re);
+                }
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Symmetric fused Dirichlet pass: the test and trial sides run over the same
+// panel list, and the separate-pair rule places the same Q^2 points on a
+// panel whether it is the test or the trial panel, so for i < j one
+// evaluation at (x_a in i, y_b in j) gives
+//   V_ij = V_ji          += w_a w_b e^{ikr}/r
+//   (K g)_i              += w_a w_b ( d.n_j)/r^3 (1-ikr) e^{ikr} g_j(y_b)
+//   (K g)_j              += w_a w_b (-d.n_i)/r^3 (1-ikr) e^{ikr} g_i(x_a)
+// (d = x_a - y_b, g interpolated from the P1 vertex data).  Only tiles on or
+// above the diagonal are launched; rows i are reduced across the warp, rows j
+// accumulate per thread over the CTA's test panels.
+// ----------------------------------------------------------------------------
+template <bool HELM, typename T>
+__global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, VkgArgs v) {
+    using V4 = typename V4T<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V4* sx = reinterpret_cast<V4*>(smem_raw);                        // [FAR_TI][Q2] test points
+    T* sgx = reinterpret_cast<T*>(sx + FAR_TI * a.Q2);                // [FAR_TI][Q2][2] g at test points
+    T* sphi = sgx + FAR_TI * a.Q2 * 2;                                // [Q2*3]
+    __shared__ int s_gi[FAR_TI];
+    __shared__ int s_tri[FAR_TI][3];
+    __shared__ double s_cen[FAR_TI][3];
+    __shared__ double s_nrm[FAR_TI][3];
+
+    const int Q2 = a.Q2;
+    const int n = a.n_test;  // == n_trial
+    // tile (bx = trial tile of FAR_THREADS panels, by = test tile of FAR_TI panels);
+    // skip tiles strictly below the diagonal
+    const int j0 = blockIdx.x * FAR_THREADS;
+    const int li0 = blockIdx.y * FAR_TI;
+    if (j0 + FAR_THREADS - 1 <= li0) return;
+    const int lj = j0 + threadIdx.x;
+    const V4* pts = reinterpret_cast<const V4*>(a.pts);
+    {
+        const T* phi = reinterpret_cast<const T*>(a.phi);
+        for (int idx = threadIdx.x; idx < Q2 * 3; idx += FAR_THREADS) sphi[idx] = phi[idx];
+    }
+    if (threadIdx.x < FAR_TI) {
+        int li = li0 + threadIdx.x;
+        int gi = li < n ? a.test_panels[li] : -1;
+        s_gi[threadIdx.x] = gi;
+        for (int c = 0; c < 3; ++c) {
+            s_tri[threadIdx.x][c] = gi >= 0 ? a.tris[3 * gi + c] : -1;
+            s_cen[threadIdx.x][c] = gi >= 0 ? a.centroid[3 * gi + c] : 0.0;
+            s_nrm[threadIdx.x][c] = gi >= 0 ? a.normal[3 * gi + c] : 0.0;
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < FAR_TI * Q2; idx += FAR_THREADS) {
+        int t = idx / Q2, q = idx - t * Q2;
+        int li = li0 + t;
+        T gre = T(0), gim = T(0);
+        if (li < n) {
+            sx[idx] = pts[(size_t)s_gi[t] * Q2 + q];
+            for (int bx = 0; bx < v.gnb; ++bx) {
+                int d = v.gdof[li * v.gnb + bx];
+                if (d < 0) continue;
+                T ph = v.gnb == 3 ? sphi[3 * q + bx] : T(1);
+                gre += ph * T(HELM ? v.g[2 * d] : v.g[d]);
+                if (HELM) gim += ph * T(v.conj ? -v.g[2 * d + 1] : v.g[2 * d + 1]);
+            }
+        }
+        sgx[2 * idx] = gre;
+        sgx[2 * idx + 1] = gim;
+    }
+    __syncthreads();
+
+    const bool valid_j = lj < n;
+    const int gj = valid_j ? a.trial_panels[lj] : 0;
+    int tri_j[3];
+    double cen_j[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        tri_j[c] = a.tris[3 * gj + c];
+        cen_j[c] = a.centroid[3 * gj + c];
+    }
+    const T njx = T(a.normal[3 * gj + 0]), njy = T(a.normal[3 * gj + 1]), njz = T(a.normal[3 * gj + 2]);
+    T gr[3] = {T(0), T(0), T(0)}, gim[3] = {T(0), T(0), T(0)};
+    if (valid_j)
+        for (int by = 0; by < v.gnb; ++by) {
+            int d = v.gdof[lj * v.gnb + by];
+            if (d < 0) continue;
+            gr[by] = T(HELM ? v.g[2 * d] : v.g[d]);
+            gim[by] = HELM ? T(v.conj ? -v.g[2 * d + 1] : v.g[2 * d + 1]) : T(0);
+        }
+    const V4* ptsj = pts + (size_t)gj * Q2;
+    const T kk = T(a.k);
+    const int lane = threadIdx.x & 31;
+    double rj_re = 0.0, rj_im = 0.0;  // this thread's contribution to row j
+
+    for (int t = 0; t < FAR_TI; ++t) {
+        const int li = li0 + t;
+        if (li >= n) break;
+        const int gi = s_gi[t];
+        const bool sep = valid_j && li < lj && (bem_relation(s_tri[t], tri_j, gi == gj) == REL_SEPARATE);
+        double av_re = 0.0, av_im = 0.0, ak_re = 0.0, ak_im = 0.0;
+        if (sep) {
+            // centroid difference as an unevaluated pair hi + lo: in FP32 a
+            // single rounding of it would be one systematic error shared by
+            // all GaussQR^4 terms of the pair
+            const double dcx64 = s_cen[t][0] - cen_j[0], dcy64 = s_cen[t][1] - cen_j[1],
+                         dcz64 = s_cen[t][2] - cen_j[2];
+            const T dcx = T(dcx64), dcy = T(dcy64), dcz = T(dcz64);
+            const T dlx = T(dcx64 - double(dcx)), dly = T(dcy64 - double(dcy)), dlz = T(dcz64 - double(dcz));
+            const T nix = T(s_nrm[t][0]), niy = T(s_nrm[t][1]), niz = T(s_nrm[t][2]);
+            const V4* sxt = sx + t * Q2;
+            const T* sgt = sgx + 2 * t * Q2;
+            for (int b = 0; b < Q2; ++b) {
+                const V4 yb = ptsj[b];
+                const T ex = (dcx - yb.x) + dlx, ey = (dcy - yb.y) + dly, ez = (dcz - yb.z) + dlz;
+                // two independent accumulator sets (even / odd test points):
+                // shorter FP32 summation chains and more independent work
+                T acc[2][6];
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+#pragma unroll
+                    for (int w = 0; w < 6; ++w) acc[u][w] = T(0);
+                auto term = [&](int q, T* A) {
+                    const V4 xa = sxt[q];
+                    const T dx = xa.x + ex, dy = xa.y + ey, dz = xa.z + ez;
+                    const T r2 = dx * dx + dy * dy + dz * dz;
+                    const T rinv = dev_rsqrt(r2);
+                    const T wr = xa.w * rinv;
+                    const T wr3 = wr * (rinv * rinv);
+                    const T tj = wr3 * (dx * njx + dy * njy + dz * njz);
+                    const T ti = -wr3 * (dx * nix + dy * niy + dz * niz);
+                    if (HELM) {
+                        const T kr = kk * (r2 * rinv);
+                        T sn, cs;
+                        dev_sincos(kr, &sn, &cs);
+                        const T f_re = fma(kr, sn, cs), f_im = fma(-kr, cs, sn);
+                        A[0] = fma(wr, cs, A[0]);
+                        A[1] = fma(wr, sn, A[1]);
+                        A[2] = fma(tj, f_re, A[2]);
+                        A[3] = fma(tj, f_im, A[3]);
+                        const T h_re = ti * f_re, h_im = ti * f_im;
+                        const T gre = sgt[2 * q], gimv = sgt[2 * q + 1];
+                        A[4] += h_re * gre - h_im * gimv;
+                        A[5] += h_re * gimv + h_im * gre;
+                    } else {
+                        A[0] += wr;
+                        A[2] += tj;
+                        A[4] = fma(ti, sgt[2 * q], A[4]);
+                    }
+                };
+                int q = 0;
+#pragma unroll 2
+                for (; q + 1 < Q2; q += 2) {
+                    term(q, acc[0]);
+                    term(q + 1, acc[1]);
+                }
+                if (q < Q2) term(q, acc[0]);
+                const T sv_re = acc[0][0] + acc[1][0], sv_im = acc[0][1] + acc[1][1];
+                const T sk_re = acc[0][2] + acc[1][2], sk_im = acc[0][3] + acc[1][3];
+                const T s2_re = acc[0][4] + acc[1][4], s2_im = acc[0][5] + acc[1][5];
+                const double wb = double(yb.w);
+                av_re += wb * double(sv_re);
+                av_im += wb * double(sv_im);
+                T gb_re = gr[0], gb_im = gim[0];
+                if (v.gnb == 3) {
+                    const T p0 = sphi[3 * b], p1 = sphi[3 * b + 1], p2 = sphi[3 * b + 2];
+                    gb_re = p0 * gr[0] + p1 * gr[1] + p2 * gr[2];
+                    gb_im = p0 * gim[0] + p1 * gim[1] + p2 * gim[2];
+                }
+                ak_re += wb * (double(sk_re) * double(gb_re) - double(sk_im) * double(gb_im));
+                ak_im += wb * (double(sk_re) * double(gb_im) + double(sk_im) * double(gb_re));
+                rj_re += wb * double(s2_re);
+                rj_im += wb * double(s2_im);
+            }
+            const int row = a.test_dof[li];
+            const int col = a.trial_dof[lj];
+            if (row >= 0 && col >= 0) {
+                const double vr = a.scale * BEM_INV4PI * av_re, vi = a.scale * BEM_INV4PI * av_im;
+                add_entry<HELM>(a.out, (int64_t)row * a.ld + col, vr, vi, false);
+                add_entry<HELM>(a.out, (int64_t)col * a.ld + row, vr, vi, false);
+            }
+        }
+        ak_re = warp_sum(ak_re);
+        if (HELM) ak_im = warp_sum(ak_im);
+        if (lane == 0) {
+            const int row = v.rows[li];
+            if (row >= 0) {
+                if (HELM) {
+                    atomicAdd(v.y + 2 * row, v.scale * BEM_INV4PI * ak_re);
+                    atomicAdd(v.y + 2 * row + 1, v.scale * BEM_INV4PI * ak_im);
+                } else {
+                    atomicAdd(v.y + row, v.scale * BEM_INV4PI * ak_re);
+                }
+            }
+        }
+    }
+    if (valid_j) {
+        const int row = v.rows[lj];
+        if (row >= 0 && (rj_re != 0.0 || rj_im != 0.0)) {
+            if (HELM) {
+                atomicAdd(v.y + 2 * row, v.scale * BEM_INV4PI * rj_re);
+                atomicAdd(v.y + 2 * row + 1, v.scale * BEM_INV4PI * rj_im);
+            } else {
+                atomicAdd(v.y + row, v.scale * BEM_INV4PI * rj_re);
+            }
+        }
+    }
+}
+
 template <int OP, bool HELM, int NBX, int NBY>
 int launch_op(bem_ctx* ctx, const FarArgs& fa, const NearArgs& na, bool fp32, cudaStream_t s) {
     dim3 grid((fa.n_trial + FAR_THREADS - 1) / FAR_THREADS, (fa.n_test + FAR_TI - 1) / FAR_TI);
@@ -872,6 +1260,125 @@ int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* te
         case BEM_OP_W: return dispatch_helm<BEM_OP_W>(ctx, helm, test->nb, trial->nb, fa, na, fp32, s);
         default: return bem_fail(ctx, BEM_ERR_INVALID, "unknown operator");
     }
+}
+
+int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                         void* out, int64_t ld, double scale, const bem_space* rows, const bem_space* data,
+                         const void* g, void* y, double scale_k, int conj_g, cudaStream_t s) {
+    if (int rc = fill_local_map(ctx, test, ctx->test_local, s)) return rc;
+    if (int rc = fill_local_map(ctx, trial, ctx->trial_local, s)) return rc;
+    const bool fp32 = op->precision == BEM_PREC_MIXED;
+    const bool helm = op->kernel == BEM_KERNEL_HELMHOLTZ;
+    FarArgs fa{};
+    fa.n_test = test->n_panels;
+    fa.n_trial = trial->n_panels;
+    fa.test_panels = test->panels;
+    fa.test_dof = test->dof;
+    fa.trial_panels = trial->panels;
+    fa.trial_dof = trial->dof;
+    fa.tris = ctx->tris;
+    fa.centroid = ctx->centroid;
+    fa.normal = ctx->normal;
+    fa.curl = ctx->curl;
+    fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
+    fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
+    fa.Q2 = ctx->Q2;
+    fa.k = op->k;
+    fa.k2 = op->k2;
+    fa.mode = 0;
+    fa.out = (double*)out;
+    fa.ld = ld;
+    fa.scale = scale;
+    VkgArgs va{(const double*)g, data->dof, data->nb, rows->dof, (double*)y, scale_k, conj_g};
+    dim3 grid((fa.n_trial + FAR_THREADS - 1) / FAR_THREADS, (fa.n_test + FAR_TI - 1) / FAR_TI);
+    if (grid.y > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "too many test panels for one launch");
+    // same panels and dofs on both sides: the symmetric sweep over i < j
+    const bool sym = test->n_panels == trial->n_panels && test->panels == trial->panels &&
+                     test->dof == trial->dof && rows->n_panels == test->n_panels;
+    if (fa.n_test > 0 && fa.n_trial > 0 && sym) {
+        if (fp32) {
+            size_t smem = FAR_TI * fa.Q2 * (sizeof(float4) + 2 * sizeof(float)) + fa.Q2 * 3 * sizeof(float);
+            if (helm)
+                far_vkg_sym_kernel<true, float><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+            else
+                far_vkg_sym_kernel<false, float><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+        } else {
+            size_t smem = FAR_TI * fa.Q2 * (sizeof(double4) + 2 * sizeof(double)) + fa.Q2 * 3 * sizeof(double);
+            if (helm)
+                far_vkg_sym_kernel<true, double><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+            else
+                far_vkg_sym_kernel<false, double><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+        }
+        ctx->launches++;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "far_vkg_sym_kernel launch")) return rc;
+    } else if (fa.n_test > 0 && fa.n_trial > 0) {
+        if (fp32) {
+            size_t smem = FAR_TI * fa.Q2 * sizeof(float4) + fa.Q2 * 3 * sizeof(float);
+            if (helm)
+                far_vkg_kernel<true, float><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+            else
+                far_vkg_kernel<false, float><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+        } else {
+            size_t smem = FAR_TI * fa.Q2 * sizeof(double4) + fa.Q2 * 3 * sizeof(double);
+            if (helm)
+                far_vkg_kernel<true, double><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+            else
+                far_vkg_kernel<false, double><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+        }
+        ctx->launches++;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "far_vkg_kernel launch")) return rc;
+    }
+    // near field: V dense and K g apply, FP64, with the operator's own kernels
+    NearArgs na{};
+    na.n_near = ctx->n_near;
+    na.near = ctx->near;
+    na.test_local = ctx->test_local;
+    na.trial_local = ctx->trial_local;
+    na.tris = ctx->tris;
+    na.verts = ctx->verts;
+    na.area = ctx->area;
+    na.normal = ctx->normal;
+    na.curl = ctx->curl;
+    na.gp = ctx->gp;
+    na.gw = ctx->gw;
+    na.Q = ctx->Q;
+    na.k = op->k;
+    na.k2 = op->k2;
+    na.quirk = op->quirk;
+    if (na.n_near > 0) {
+        const unsigned blocks = (unsigned)((na.n_near + 3) / 4);
+        NearArgs nv = na;
+        nv.test_dof = test->dof;
+        nv.trial_dof = trial->dof;
+        nv.mode = 0;
+        nv.out = (double*)out;
+        nv.ld = ld;
+        nv.scale = scale;
+        NearArgs nk = na;
+        nk.test_dof = rows->dof;
+        nk.trial_dof = data->dof;
+        nk.mode = 1;
+        nk.x = (const double*)g;
+        nk.y = (double*)y;
+        nk.scale = scale_k;
+        nk.conj_x = conj_g;
+        if (helm) {
+            near_kernel<BEM_OP_V, true, 1, 1><<<blocks, 128, 0, s>>>(nv);
+            if (data->nb == 3)
+                near_kernel<BEM_OP_K, true, 1, 3><<<blocks, 128, 0, s>>>(nk);
+            else
+                near_kernel<BEM_OP_K, true, 1, 1><<<blocks, 128, 0, s>>>(nk);
+        } else {
+            near_kernel<BEM_OP_V, false, 1, 1><<<blocks, 128, 0, s>>>(nv);
+            if (data->nb == 3)
+                near_kernel<BEM_OP_K, false, 1, 3><<<blocks, 128, 0, s>>>(nk);
+            else
+                near_kernel<BEM_OP_K, false, 1, 1><<<blocks, 128, 0, s>>>(nk);
+        }
+        ctx->launches += 2;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "near_kernel launch")) return rc;
+    }
+    return BEM_OK;
 }
 
 int bem_launch_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int is_complex, int mode, void* out,

@@ -55,6 +55,9 @@ int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s);
 int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                         int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
                         void* y, int conj_x, cudaStream_t s);
+int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                         void* out, int64_t ld, double scale, const bem_space* rows, const bem_space* data,
+                         const void* g, void* y, double scale_k, int conj_g, cudaStream_t s);
 int bem_launch_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int is_complex, int mode, void* out,
                     int64_t ld, double scale, void* out_t, double scale_t, const void* x, void* y, int conj_x,
                     cudaStream_t s);

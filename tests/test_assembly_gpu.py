@@ -164,3 +164,35 @@ def test_bad_mesh_rejected(engine):
         engine.set_mesh(v, np.array([[0, 1, 2]]), 3)
     with pytest.raises(BemError):
         engine.set_mesh(v, np.array([[0, 1, 5]]), 3)
+
+
+@pytest.mark.parametrize("sym", [True, False])
+@pytest.mark.parametrize("helm", [False, True])
+@pytest.mark.parametrize("fp32", [False, True])
+def test_fused_dirichlet_pass(engine, helm, fp32, sym):
+    """V and K g in one sweep == V assembly + K g apply (oracle)."""
+    from bem_b200 import _lib as L
+    v, f = MESHES["ico2"]
+    Q = 4
+    engine.set_mesh(v, f, Q)
+    k = 2.0 if helm else 0.0
+    ts, tsd = _space(engine, v, f, 1)
+    ds, dsd = _space(engine, v, f, 3)
+    nt, nv = len(f), len(v)
+    rng = np.random.default_rng(3)
+    g = rng.standard_normal(nv) + (1j * rng.standard_normal(nv) if helm else 0)
+    Vref = _oracle_block(v, f, O.OP_V, helm, k, k * k, Q, True, ts, ts, nt, nt)
+    yref = np.zeros(nt, np.complex128 if helm else np.float64)
+    O.assemble(v, f, O.OP_K, helm, k, k * k, Q, True, ts, ds, x=g, y=yref, scale=0.75, conj_x=helm)
+    dt = torch.complex128 if helm else torch.float64
+    V = torch.zeros(nt, nt, dtype=dt, device="cuda")
+    y = torch.zeros(nt, dtype=dt, device="cuda")
+    gd = torch.as_tensor(g, device="cuda")
+    desc = engine.op_desc(O.OP_V, helm, k, k * k, precision=L.PREC_MIXED if fp32 else L.PREC_FP64)
+    # sym: identical test/trial spaces select the symmetric i<j sweep; a copy
+    # of the trial space (other device pointers) selects the general sweep
+    trial = tsd if sym else _space(engine, v, f, 1)[1]
+    engine.assemble_dirichlet(desc, tsd, trial, V, tsd, dsd, gd, y, scale=1.0, scale_k=0.75, conj_g=helm)
+    tol = MIXED_TOL if fp32 else FP64_TOL
+    assert rel_err(V.cpu().numpy(), Vref) < tol
+    assert rel_err(y.cpu().numpy(), yref) < tol

@@ -21,18 +21,17 @@ def _run(d, **extra):
     return core, b
 
 
+@pytest.mark.parametrize("fuse", [False, True])
 @pytest.mark.parametrize("name", FIXTURES)
-def test_driver_matches_reference_fp64(name):
+def test_driver_matches_reference_fp64(name, fuse):
     d = load_fixture(name)
-    core, b = _run(d)
+    core, b = _run(d, fuse=fuse)
     b._mat_A.zero_()
     # run the same sequence as BEMManager.run, stopping to compare A and rhs
     core._BEM_manager.run()
     A = b._mat_A.cpu().numpy()
     assert rel_err(A, to_complex(d["A"])) < 1e-12
     assert rel_err(b.rhs.cpu().numpy(), to_complex(d["rhs"])) < 1e-12
-    for i in range(int(d["n_forward"])):
-        pass
     if "raw_solved" in d and "solve_error" not in d:
         cond = np.linalg.cond(to_complex(d["A"]).reshape(A.shape)) if A.shape[0] < 2000 else 0
         if cond < 1e8:
