@@ -170,6 +170,25 @@ int bem_lu_factor_tiled(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda
 int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                        const void* dinv, void* b, void* stream);
 
+/* Allocation-free variant of bem_lu_solve_tiled (no counterpart in the
+ * reference).  For callers that must not allocate device memory once they are
+ * running -- for example an application whose device memory is owned by
+ * another allocator, or a latency-critical loop where cudaMalloc's implicit
+ * device synchronisation is not acceptable -- and that therefore cannot create
+ * a bem_ctx workspace.  It takes no context and performs no allocation: its
+ * scratch is a file-scope device array sized for n <= BEM_STATIC_SOLVE_MAX_N
+ * (about 0.65 MB, held by every GPU that loads the library until the process
+ * exits); larger n is rejected with BEM_ERR_INVALID.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture.  All calls
+ * share the one array, so calls that overlap on the GPU (other streams, other
+ * host threads) race; serialise them.  Same arguments and result as
+ * bem_lu_solve_tiled; returns BEM_OK, BEM_ERR_INVALID, BEM_ERR_CUDA or
+ * BEM_ERR_TIMEOUT. */
+#define BEM_STATIC_SOLVE_MAX_N 32768
+int bem_lu_solve_tiled_static(int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
+                              const void* dinv, void* b, void* stream);
+
 /* Mixed-precision solve: x = A_hi^{-1} b to relative residual tol by FP64
  * iterative refinement on the residual b - A_hi x, each correction solved with
  * the low-precision factors (LU_lo, piv[, dinv]) of A_hi: tile-pivoted factors

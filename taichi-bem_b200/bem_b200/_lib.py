@@ -33,8 +33,9 @@ EXPORTS = [
     "bem_ctx_create", "bem_ctx_destroy", "bem_last_error", "bem_launch_count", "bem_mesh_set",
     "bem_near_pair_count", "bem_mesh_geometry", "bem_assemble", "bem_apply", "bem_mass", "bem_lu_factor",
     "bem_lu_solve", "bem_gemv", "bem_refine_solve", "bem_measure_peaks", "bem_lu_dinv_elems",
-    "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet",
+    "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet", "bem_lu_solve_tiled_static",
 ]
+STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 
 
 class BemError(RuntimeError):
@@ -89,6 +90,7 @@ def load():
     L.bem_assemble_dirichlet.argtypes = [vp, ctypes.POINTER(OpDesc), ctypes.POINTER(Space), ctypes.POINTER(Space),
                                          vp, i64, dbl, ctypes.POINTER(Space), ctypes.POINTER(Space), vp, vp, dbl,
                                          i32, vp]
+    L.bem_lu_solve_tiled_static.argtypes = [i32, vp, i64, i64, vp, vp, vp, vp]
     L.bem_lu_dinv_elems.argtypes = [i64]
     L.bem_lu_dinv_elems.restype = i64
     L.bem_lu_factor_tiled.argtypes = [vp, i32, vp, i64, i64, vp, vp, vp, vp]

@@ -523,3 +523,123 @@ int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------------------
+// Allocation-free variant of bem_lu_solve_tiled.
+//
+// Its scratch (row permutation, ready flags, error word, work vector) lives in
+// one file-scope __device__ array instead of a context workspace, so the call
+// needs no bem_ctx and performs no device allocation.  The array is sized for
+// n <= BEM_STATIC_SOLVE_MAX_N and is held by every GPU that loads this library
+// until the process exits.  Host code only ever sees the array's host-side
+// stand-in name; its device address comes from cudaGetSymbolAddress, taken
+// once per device (with that device current) on the first call there.
+// ----------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr int64_t kStaticSolveMaxN = BEM_STATIC_SOLVE_MAX_N;
+constexpr int kStaticSolveMaxTiles = (int)((kStaticSolveMaxN + LU_T - 1) / LU_T);
+
+struct StaticSolveScratch {
+    int32_t perm[kStaticSolveMaxN];
+    int flags[2 * kStaticSolveMaxTiles];
+    int32_t err[4];
+    double x[2 * kStaticSolveMaxN];
+};
+
+__device__ __align__(256) StaticSolveScratch g_static_solve_scratch;
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+StaticSolveScratch* g_static_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (set-up on the
+// first call per device).
+int static_scratch(StaticSolveScratch** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kMaxDevices) return BEM_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_solve_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            return BEM_ERR_CUDA;
+        }
+        g_static_addr[dev] = static_cast<StaticSolveScratch*>(p);
+    }
+    *out = g_static_addr[dev];
+    return BEM_OK;
+}
+
+template <typename T, bool C>
+int solve_static_t(const T* LU, int64_t n, int64_t lda, const int32_t* piv, const CE<T>* dinv, double* b,
+                   cudaStream_t s) {
+    StaticSolveScratch* sc = nullptr;
+    if (int rc = static_scratch(&sc)) return rc;
+    const int W = C ? 2 : 1;
+    const int nbk = (int)((n + LU_T - 1) / LU_T);
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int32_t* perm = sc->perm;
+    int* flags = sc->flags;
+    int32_t* err = sc->err;
+    double* x = sc->x;
+    if (cudaFuncSetAttribute(tile_piv_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(n * sizeof(int32_t))) != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    tile_piv_to_perm_kernel<<<1, 256, n * sizeof(int32_t), s>>>(piv, perm, (int)n);
+    permute_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, perm, x, (int)n, W);
+    // the array keeps the previous call's contents: the flags and the error
+    // word must start at zero
+    if (cudaMemsetAsync(flags, 0, sizeof(int) * 2 * nbk, s) != cudaSuccess ||
+        cudaMemsetAsync(err, 0, sizeof(int32_t), s) != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, 0);
+    int P = std::max(1, std::min(nbk, std::min(per_sm * sms, sms)));
+    int ni = (int)n, epoch = 1;
+    void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err};
+    if (cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args, 0, s) != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    if (cudaMemcpyAsync(b, x, sizeof(double) * W * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    int32_t e = 0;
+    if (cudaMemcpyAsync(&e, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    return e != 0 ? BEM_ERR_TIMEOUT : BEM_OK;
+}
+
+}  // namespace
+
+extern "C" int bem_lu_solve_tiled_static(int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
+                                         const void* dinv, void* b, void* stream) {
+    if (!LU || !piv || !dinv || !b || n <= 0 || lda < n) return BEM_ERR_INVALID;
+    if (n > kStaticSolveMaxN) return BEM_ERR_INVALID;  // beyond the static scratch
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (dtype) {
+        case BEM_F64: return solve_static_t<double, false>((const double*)LU, n, lda, piv, (const CE<double>*)dinv, (double*)b, s);
+        case BEM_C128: return solve_static_t<double, true>((const double*)LU, n, lda, piv, (const CE<double>*)dinv, (double*)b, s);
+        case BEM_F32: return solve_static_t<float, false>((const float*)LU, n, lda, piv, (const CE<float>*)dinv, (double*)b, s);
+        case BEM_C64: return solve_static_t<float, true>((const float*)LU, n, lda, piv, (const CE<float>*)dinv, (double*)b, s);
+        default: return BEM_ERR_INVALID;
+    }
+}
