@@ -72,13 +72,16 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
     CE<T>* Li = S + LU_T * LU_T;
     CE<T>* Ui = Li + LU_T * LU_T;
     __shared__ int s_p;
+    __shared__ int s_zero_pivot;  // first zero pivot of this tile (1-based), 0 = none
     const int m = min(LU_T, n - k0);
+    if (threadIdx.x == 0) s_zero_pivot = 0;
     for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
         int r = e / LU_T, c = e - r * LU_T;
         S[e] = (r < m && c < m) ? ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c) : CE<T>{T(0), T(0)};
     }
     __syncthreads();
     for (int j = 0; j < m; ++j) {
+        // pivot search in column j (warp 0), then swap rows j and p
         if (threadIdx.x < 32) {
             double best = -1.0;
             int bi = j;
@@ -101,63 +104,111 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
             if (threadIdx.x == 0) {
                 s_p = bi;
                 piv[k0 + j] = k0 + bi;
-                if (!(best > 0.0) && *info == 0) *info = k0 + j + 1;
+                if (!(best > 0.0) && s_zero_pivot == 0) s_zero_pivot = k0 + j + 1;
+            }
+            const int p = __shfl_sync(0xffffffffu, bi, 0);
+            if (p != j)
+                for (int c = threadIdx.x; c < LU_T; c += 32) {
+                    CE<T> t = S[j * LU_T + c];
+                    S[j * LU_T + c] = S[p * LU_T + c];
+                    S[p * LU_T + c] = t;
+                }
+        }
+        __syncthreads();
+        // multipliers and rank-1 update in one pass: element (r, c), c > j,
+        // uses l_r = S[r][j] / S[j][j]; column j itself is scaled by the
+        // threads of c == j after everyone has read it (second sync)
+        const CE<T> inv = cinv(S[j * LU_T + j]);
+        // thread t owns columns c = j + (t % 64) ... of rows j+1+(t/64), +4, ...:
+        // fixed (row, column) ownership keeps the buffered values in registers
+        const int cc = j + (threadIdx.x & 63);
+        const int r0 = j + 1 + (threadIdx.x >> 6);
+        constexpr int RPT = LU_T / 4;  // rows per thread
+        CE<T> upd[RPT];
+#pragma unroll
+        for (int it = 0; it < RPT; ++it) {
+            const int r = r0 + 4 * it;
+            upd[it] = CE<T>{T(0), T(0)};
+            if (r < m && cc < m) {
+                const CE<T> l = cmul(S[r * LU_T + j], inv);
+                if (cc == j) {
+                    upd[it] = l;
+                } else {
+                    const CE<T> lu = cmul(l, S[j * LU_T + cc]), v = S[r * LU_T + cc];
+                    upd[it] = CE<T>{v.re - lu.re, v.im - lu.im};
+                }
             }
         }
         __syncthreads();
-        const int p = s_p;
-        if (p != j)
-            for (int c = threadIdx.x; c < LU_T; c += blockDim.x) {
-                CE<T> t = S[j * LU_T + c];
-                S[j * LU_T + c] = S[p * LU_T + c];
-                S[p * LU_T + c] = t;
-            }
-        __syncthreads();
-        const CE<T> inv = cinv(S[j * LU_T + j]);
-        for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) S[r * LU_T + j] = cmul(S[r * LU_T + j], inv);
-        __syncthreads();
-        const int w = m - j - 1;
-        for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-            int r = j + 1 + e / w, c = j + 1 + e % w;
-            CE<T> l = S[r * LU_T + j], u = S[j * LU_T + c], v = S[r * LU_T + c];
-            CE<T> lu = cmul(l, u);
-            S[r * LU_T + c] = CE<T>{v.re - lu.re, v.im - lu.im};
+#pragma unroll
+        for (int it = 0; it < RPT; ++it) {
+            const int r = r0 + 4 * it;
+            if (r < m && cc < m) S[r * LU_T + cc] = upd[it];
         }
         __syncthreads();
     }
-    // explicit inverses: column c of Linv solves L y = e_c, of Uinv solves U y = e_c
-    if (threadIdx.x < LU_T) {
-        const int c = threadIdx.x;
-        for (int r = 0; r < LU_T; ++r) {
-            CE<T> s = CE<T>{r == c ? T(1) : T(0), T(0)};
-            if (r < m)
-                for (int q = c; q < r; ++q) {
-                    CE<T> t = cmul(S[r * LU_T + q], Li[q * LU_T + c]);
-                    s.re -= t.re;
-                    s.im -= t.im;
+    // explicit inverses, rows in sequence, all columns of a row in parallel:
+    // threads 0..127 build Linv (two threads per column, partial sums combined
+    // with a shuffle), threads 128..255 build Uinv the same way from the
+    // bottom row up.  Named barriers keep the two halves independent.
+    {
+        const int half = threadIdx.x >> 7;  // 0: Linv, 1: Uinv
+        const int t = threadIdx.x & 127;
+        const int c = t >> 1, part = t & 1;
+        CE<T>* X = half == 0 ? Li : Ui;
+        for (int e = t; e < LU_T * LU_T; e += 128) X[e] = CE<T>{T(0), T(0)};
+        if (half == 0)
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+        else
+            asm volatile("bar.sync 2, 128;" ::: "memory");
+        for (int step = 0; step < LU_T; ++step) {
+            const int r = half == 0 ? step : LU_T - 1 - step;
+            CE<T> sum = CE<T>{T(0), T(0)};
+            if (r < m) {
+                if (half == 0) {
+                    // Linv[r][c] = delta_rc - sum_{c <= q < r} L[r][q] Linv[q][c]   (c <= r)
+                    if (c < r)
+                        for (int q = c + part; q < r; q += 2) {
+                            CE<T> tt = cmul(S[r * LU_T + q], X[q * LU_T + c]);
+                            sum.re += tt.re;
+                            sum.im += tt.im;
+                        }
+                } else {
+                    // Uinv[r][c] = (delta_rc - sum_{r < q <= c} U[r][q] Uinv[q][c]) / U[r][r]   (r <= c)
+                    if (c > r)
+                        for (int q = r + 1 + part; q <= c && q < m; q += 2) {
+                            CE<T> tt = cmul(S[r * LU_T + q], X[q * LU_T + c]);
+                            sum.re += tt.re;
+                            sum.im += tt.im;
+                        }
                 }
-            Li[r * LU_T + c] = (r < c) ? CE<T>{T(0), T(0)} : s;
-        }
-    } else if (threadIdx.x < 2 * LU_T) {
-        const int c = threadIdx.x - LU_T;
-        for (int r = LU_T - 1; r >= 0; --r) {
-            CE<T> s = CE<T>{r == c ? T(1) : T(0), T(0)};
-            if (r < m && r <= c) {
-                for (int q = r + 1; q <= c && q < m; ++q) {
-                    CE<T> t = cmul(S[r * LU_T + q], Ui[q * LU_T + c]);
-                    s.re -= t.re;
-                    s.im -= t.im;
-                }
-                s = cmul(s, cinv(S[r * LU_T + r]));
-            } else if (r >= m) {
-                s = CE<T>{r == c ? T(1) : T(0), T(0)};
-            } else {
-                s = CE<T>{T(0), T(0)};
             }
-            Ui[r * LU_T + c] = s;
+            sum.re += __shfl_xor_sync(0xffffffffu, sum.re, 1);
+            sum.im += __shfl_xor_sync(0xffffffffu, sum.im, 1);
+            if (part == 0) {
+                CE<T> val;
+                if (r >= m) {
+                    val = CE<T>{r == c ? T(1) : T(0), T(0)};  // identity padding of a short last tile
+                } else if (half == 0) {
+                    val = c < r ? CE<T>{-sum.re, -sum.im} : CE<T>{r == c ? T(1) : T(0), T(0)};
+                } else if (c < r) {
+                    val = CE<T>{T(0), T(0)};
+                } else if (c >= m) {
+                    val = CE<T>{T(0), T(0)};
+                } else {
+                    CE<T> d = CE<T>{(r == c ? T(1) : T(0)) - sum.re, -sum.im};
+                    val = cmul(d, cinv(S[r * LU_T + r]));
+                }
+                X[r * LU_T + c] = val;
+            }
+            if (half == 0)
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+            else
+                asm volatile("bar.sync 2, 128;" ::: "memory");
         }
     }
     __syncthreads();
+    if (threadIdx.x == 0 && s_zero_pivot != 0 && *info == 0) *info = s_zero_pivot;
     CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T;
     for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
         D[e] = Li[e];
@@ -420,6 +471,7 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
     cudaFuncSetAttribute(tile_diag_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem);
     cudaFuncSetAttribute(tile_apply_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem);
     const int ni = (int)n;
+    const int W = C ? 2 : 1;
     for (int64_t k0 = 0; k0 < n; k0 += LU_T) {
         const int m = (int)std::min<int64_t>(LU_T, n - k0);
         const int k0i = (int)k0;
@@ -432,12 +484,22 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
             tile_apply_kernel<T, C><<<tiles, 256, asmem, s>>>(A, lda, ni, k0i, m, dinv, 0);
             tile_apply_kernel<T, C><<<tiles, 256, asmem, s>>>(A, lda, ni, k0i, m, dinv, 1);
             ctx->launches += 2;
-            T* A22 = A + (C ? 2 : 1) * ((k0 + m) * lda + k0 + m);
-            const T* L21 = A + (C ? 2 : 1) * ((k0 + m) * lda + k0);
-            const T* U12 = A + (C ? 2 : 1) * (k0 * lda + k0 + m);
+            T* A22 = A + W * ((k0 + m) * lda + k0 + m);
+            const T* L21 = A + W * ((k0 + m) * lda + k0);
+            const T* U12 = A + W * (k0 * lda + k0 + m);
             if (int rc = bem_gemm_update<T, C>(ctx, A22, L21, U12, rest, rest, m, lda, s)) return rc;
         }
         if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "tiled lu step")) return rc;
+    }
+    // the tensor-core update records a bounded-wait timeout in flags[4]
+    int32_t tc_err = 0;
+    if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(&tc_err, ctx->flags + 4, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                                     s), "flag readback"))
+        return rc;
+    if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "tiled lu")) return rc;
+    if (tc_err != 0) {
+        cudaMemsetAsync(ctx->flags + 4, 0, sizeof(int32_t), s);
+        return bem_fail(ctx, BEM_ERR_TIMEOUT, "tiled lu: a tensor-core wait hit its iteration cap");
     }
     return BEM_OK;
 }
