@@ -210,6 +210,15 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
     const int Q = gauss_qr, Q2 = Q * Q;
     std::vector<double> gp(Q), gw(Q);
     gauss01(Q, gp.data(), gw.data());
+    // FP32 separate rule: reference weights (gw_x gw_y r1, rounded once to
+    // float, as geometry_kernel does) rescaled to the exact weight sum
+    double wsum = 0.0, wsum32 = 0.0;
+    for (int ix = 0; ix < Q; ++ix)
+        for (int iy = 0; iy < Q; ++iy) {
+            const double wref = (gw[ix] * gw[iy]) * gp[ix];
+            wsum += wref;
+            wsum32 += (double)(float)wref;
+        }
     std::vector<double> phi64((size_t)Q2 * 3);
     std::vector<float> phi32((size_t)Q2 * 3);
     for (int ix = 0; ix < Q; ++ix)
@@ -237,6 +246,7 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
     ctx->nt = nt;
     ctx->Q = Q;
     ctx->Q2 = Q2;
+    ctx->wcorr32 = (wsum / wsum32) * (wsum / wsum32);
     ctx->n_near = (int64_t)near.size();
     cudaMemcpy(ctx->verts, verts, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->tris, tris, sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice);

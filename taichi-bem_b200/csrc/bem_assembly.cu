@@ -39,8 +39,78 @@ struct V4T<double> {
     using type = double4;
 };
 
-__device__ __forceinline__ float dev_rsqrt(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double dev_rsqrt(double x) { return rsqrt(x); }
+// r = |d| and 1/r from r2 = |d|^2.  In FP32 the MUFU reciprocal square root
+// carries a deterministic error of up to ~1e-7 that varies slowly with r2, so
+// every quadrature point of a pair (and every nearby pair) would share it: a
+// relative error of r acts on e^{ikr} like a perturbation of k.  One Newton
+// step whose residual 1 - r2 y0^2 is formed with a single rounding (FMA) leaves
+// only the independent rounding errors of the products.
+__device__ __forceinline__ void dev_r_rinv(float r2, float& r, float& rinv) {
+    const float y0 = rsqrtf(r2);
+    const float p = r2 * y0;
+    const float e = fmaf(-p, y0, 1.0f);
+    rinv = fmaf(0.5f * y0, e, y0);
+    r = fmaf(0.5f * p, e, p);
+}
+__device__ __forceinline__ void dev_r_rinv(double r2, double& r, double& rinv) {
+    rinv = rsqrt(r2);
+    r = r2 * rinv;
+}
+
+// Pair frame of an FP32 separate pair.  With D = c_i - c_j (FP64 centroid
+// difference) and e = x_a - y_b (centroid-relative point offsets, |e| at most
+// the two panel diameters):
+//   r^2 = R^2 + s,   s = e.(2D + e),   r - R = s / (r + R),   d.n = D.n + e.n,
+// so each FP32 rounding is relative to a quantity of size |e| or to a per-pair
+// constant, and none is shared by the quadrature points of a pair (rounding
+// D - y_b once per trial point, say, would be shared by all test points and
+// would not average out over the GaussQR^4 sum).  The Helmholtz factor is
+//   e^{ikr} = e^{ikR} e^{ik(r-R)}:
+// e^{ikR} is evaluated once per pair in FP64 and FP32 carries only the phase
+// k (r - R) = O(k h), whose error no longer grows with k R.  In FP64
+// (SPLIT = false) the kernels use d = x - y directly and the frame is inert.
+//
+// FP32 points carry the reference-triangle weights, identical on every panel;
+// the pair factor pf = (2 A_i)(2 A_j) wcorr is applied in FP64, where wcorr =
+// (W / W_f)^2 rescales the sum W_f of the FP32 weights to the exact sum W.  A
+// rounding that differed per panel would scale whole rows of the far field
+// against the FP64 near field and identity terms.
+template <typename T, bool HELM>
+struct Frame {
+    static constexpr bool SPLIT = sizeof(T) == 4;
+    T ux = T(0), uy = T(0), uz = T(0);  // 2D
+    T R2 = T(0), Rf = T(0);
+    double cR = 1.0, sR = 0.0, pf = 1.0;
+    __device__ __forceinline__ void init(double dx, double dy, double dz, double k, double Ai, double Aj,
+                                         double wcorr) {
+        if (SPLIT) {
+            pf = 4.0 * Ai * Aj * wcorr;
+            ux = T(2.0 * dx);
+            uy = T(2.0 * dy);
+            uz = T(2.0 * dz);
+            const double R2d = dx * dx + dy * dy + dz * dz;
+            R2 = T(R2d);
+            if (HELM) {
+                const double R = sqrt(R2d);
+                Rf = T(R);
+                sincos(k * R, &sR, &cR);
+            }
+        }
+    }
+    // (re, im) <- (re, im) pf e^{ikR}
+    __device__ __forceinline__ void rotate(double& re, double& im) const {
+        if (SPLIT) {
+            re *= pf;
+            im *= pf;
+        }
+        if (SPLIT && HELM) {
+            const double a = re * cR - im * sR, b = re * sR + im * cR;
+            re = a;
+            im = b;
+        }
+    }
+};
+
 // FP32 sine/cosine of the Helmholtz phase k r (k r >= 0 and moderate): Cody-
 // Waite reduction by pi/2 with a two-term split of pi/2 (exact FMA products
 // for |n| < 2^12), Taylor polynomials of sin (through y^9) and cos (through
@@ -130,11 +200,15 @@ __global__ void geometry_kernel(int nt, int Q, const double* __restrict__ verts,
     for (int ix = 0; ix < Q; ++ix)
         for (int iy = 0; iy < Q; ++iy) {
             double r1 = gp[ix], r2 = gp[iy] * r1;
-            double w = gw[ix] * gw[iy] * (A * 2.0) * r1;
+            // reference-triangle weight; FP64 points carry the Jacobian 2A,
+            // FP32 points the panel-independent weight (the pair's 4 A_i A_j
+            // is applied in FP64, so the FP32 rounding of a weight is the same
+            // for every panel)
+            const double wref = (gw[ix] * gw[iy]) * r1;
             double o[3];
             for (int c = 0; c < 3; ++c) o[c] = ((1.0 - r1) * v[0][c] + (r1 - r2) * v[1][c] + r2 * v[2][c]) - cen[c];
-            pts64[(size_t)p * Q2 + ix * Q + iy] = make_double4(o[0], o[1], o[2], w);
-            pts32[(size_t)p * Q2 + ix * Q + iy] = make_float4((float)o[0], (float)o[1], (float)o[2], (float)w);
+            pts64[(size_t)p * Q2 + ix * Q + iy] = make_double4(o[0], o[1], o[2], wref * (A * 2.0));
+            pts32[(size_t)p * Q2 + ix * Q + iy] = make_float4((float)o[0], (float)o[1], (float)o[2], (float)wref);
         }
 }
 
@@ -159,14 +233,14 @@ __global__ void scatter_local_kernel(int n, const int32_t* __restrict__ panels, 
 //   KP:   (-d.n_x)/r^3 (1 - ikr) e^{ikr}      (grad_G_y with x,y swapped and n_x)
 template <int OP, bool HELM, typename T>
 __device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T& re, T& im) {
-    T r2 = dx * dx + dy * dy + dz * dz;
-    T rinv = dev_rsqrt(r2);
+    const T r2 = dx * dx + dy * dy + dz * dz;
+    T r, rinv;
+    dev_r_rinv(r2, r, rinv);
     if (OP == BEM_OP_V || OP == BEM_OP_W) {
         if (!HELM) {
             re = rinv;
             im = T(0);
         } else {
-            T r = r2 * rinv;
             T s, c;
             dev_sincos(k * r, &s, &c);
             re = rinv * c;
@@ -180,12 +254,42 @@ __device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T&
             re = t;
             im = T(0);
         } else {
-            T r = r2 * rinv;
             T kr = k * r;
             T s, c;
             dev_sincos(kr, &s, &c);
             re = t * (c + kr * s);
             im = t * (s - kr * c);
+        }
+    }
+}
+
+// The same values in a pair frame (FP32): r2 = R^2 + s, dn = d.n (-d.n_x for
+// K'), Rf = R; the result lacks the pair's factor e^{ikR} (Frame::rotate).
+template <int OP, bool HELM>
+__device__ __forceinline__ void kval_split(float r2, float s, float dn, float k, float Rf, float& re, float& im) {
+    float r, rinv;
+    dev_r_rinv(r2, r, rinv);
+    if (OP == BEM_OP_V || OP == BEM_OP_W) {
+        if (!HELM) {
+            re = rinv;
+            im = 0.0f;
+        } else {
+            float sn, cs;
+            dev_sincos(k * __fdividef(s, r + Rf), &sn, &cs);
+            re = rinv * cs;
+            im = rinv * sn;
+        }
+    } else {
+        const float t = dn * rinv * rinv * rinv;
+        if (!HELM) {
+            re = t;
+            im = 0.0f;
+        } else {
+            const float kr = k * r;
+            float sn, cs;
+            dev_sincos(k * __fdividef(s, r + Rf), &sn, &cs);
+            re = t * fmaf(kr, sn, cs);
+            im = t * fmaf(-kr, cs, sn);
         }
     }
 }
@@ -200,8 +304,11 @@ struct FarArgs {
     const double* centroid;
     const double* normal;
     const double* curl;
+    const double* area;
+    double wcorr;  // (exact / FP32 weight sum)^2 of the FP32 separate rule
     const void* pts;
     const void* phi;
+    const double* phi64;  // [Q2*3] P1 basis at the separate-rule points, FP64
     int Q2;
     double k, k2;
     int mode;
@@ -302,6 +409,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
 
         double acc_re[AX][AY], acc_im[AX][AY];
         double acc0_re = 0.0, acc0_im = 0.0;  // W curl-curl moment (sum of weights * kernel)
+        Frame<T, HELM> fr;
 #pragma unroll
         for (int bx = 0; bx < AX; ++bx)
 #pragma unroll
@@ -315,20 +423,23 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
                          dcz64 = s_cen[t][2] - cen_j[2];
             const T dcx = T(dcx64), dcy = T(dcy64), dcz = T(dcz64);
             const T dlx = T(dcx64 - double(dcx)), dly = T(dcy64 - double(dcy)), dlz = T(dcz64 - double(dcz));
-            T nx, ny, nz;
-            if (OP == BEM_OP_KP) {
-                nx = T(s_nrm[t][0]);
-                ny = T(s_nrm[t][1]);
-                nz = T(s_nrm[t][2]);
-            } else {
-                nx = T(nrm_j[0]);
-                ny = T(nrm_j[1]);
-                nz = T(nrm_j[2]);
-            }
+            fr.init(dcx64, dcy64, dcz64, a.k, a.area[gi], a.area[gj], a.wcorr);
+            // normal of K (trial panel) or K' (test panel), and D.n in FP64
+            const double n0 = (OP == BEM_OP_KP) ? s_nrm[t][0] : nrm_j[0];
+            const double n1 = (OP == BEM_OP_KP) ? s_nrm[t][1] : nrm_j[1];
+            const double n2 = (OP == BEM_OP_KP) ? s_nrm[t][2] : nrm_j[2];
+            const T nx = T(n0), ny = T(n1), nz = T(n2);
+            const T Dn = T(dcx64 * n0 + dcy64 * n1 + dcz64 * n2);
+            // n_j - n_i: x_a.n_j = x_a.(n_j - n_i) and y_b.n_i = -y_b.(n_j - n_i), exact for
+            // points in their panel's plane, and small for nearly coplanar close pairs
+            const T mx = T(nrm_j[0] - s_nrm[t][0]), my = T(nrm_j[1] - s_nrm[t][1]), mz = T(nrm_j[2] - s_nrm[t][2]);
             const V4* sxt = sx + t * Q2;
             for (int b = 0; b < Q2; ++b) {
                 const V4 yb = ptsj[b];
                 const T ex = (dcx - yb.x) + dlx, ey = (dcy - yb.y) + dly, ez = (dcz - yb.z) + dlz;
+                // frame: 2D - y_b, and -d.n_x = -(D.n_x - y_b.n_x) for K' (x_a lies in the plane of panel i)
+                const T wx = fr.ux - yb.x, wy = fr.uy - yb.y, wz = fr.uz - yb.z;
+                const T dnb = -(Dn + (yb.x * mx + yb.y * my + yb.z * mz));
                 T s_re[AX], s_im[AX];
                 T c_re = T(0), c_im = T(0);
 #pragma unroll
@@ -337,7 +448,15 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
                 for (int q = 0; q < Q2; ++q) {
                     const V4 xa = sxt[q];
                     T re, im;
-                    kval<OP, HELM, T>(xa.x + ex, xa.y + ey, xa.z + ez, nx, ny, nz, kk, re, im);
+                    if constexpr (Frame<T, HELM>::SPLIT) {
+                        const T e_x = xa.x - yb.x, e_y = xa.y - yb.y, e_z = xa.z - yb.z;
+                        const T sq = e_x * (xa.x + wx) + e_y * (xa.y + wy) + e_z * (xa.z + wz);
+                        // K: d.n_y = D.n_y + x_a.n_y (y_b lies in the plane of panel j)
+                        const T dn = (OP == BEM_OP_K) ? fma(xa.x, mx, fma(xa.y, my, fma(xa.z, mz, Dn))) : dnb;
+                        kval_split<OP, HELM>(fr.R2 + sq, sq, dn, kk, fr.Rf, re, im);
+                    } else {
+                        kval<OP, HELM, T>(xa.x + ex, xa.y + ey, xa.z + ez, nx, ny, nz, kk, re, im);
+                    }
                     if (W_OP) {
                         c_re += xa.w * re;
                         if (HELM) c_im += xa.w * im;
@@ -364,7 +483,8 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
                 if (NEED_PHI) {
 #pragma unroll
                     for (int by = 0; by < AY; ++by) {
-                        double wpb = (AY == 1) ? wb : wb * double(sphi[3 * b + by]);
+                        // trial basis in FP64: an exact partition of unity for the trial side
+                        double wpb = (AY == 1) ? wb : wb * a.phi64[3 * b + by];
 #pragma unroll
                         for (int bx = 0; bx < AX; ++bx) {
                             acc_re[bx][by] += wpb * double(s_re[bx]);
@@ -403,6 +523,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
                     vr = acc_re[ix][iy];
                     vi = acc_im[ix][iy];
                 }
+                fr.rotate(vr, vi);
                 val_re[bx][by] = vr * BEM_INV4PI;
                 val_im[bx][by] = vi * BEM_INV4PI;
             }
@@ -789,6 +910,39 @@ struct VkgArgs {
     int conj;
 };
 
+// Boundary data on one panel, interpolated as g0 + phi1 (g1 - g0) + phi2 (g2 - g0)
+// (P0 data: g0).  Constants are reproduced exactly whatever the FP32 rounding
+// of the basis values: phi0 + phi1 + phi2 differs from 1 after rounding with the
+// same pattern on every panel, which in the form sum_b phi_b g_b would act as a
+// uniform weight error of the far field against the FP64 identity term.
+template <bool HELM, typename T>
+struct PanelData {
+    T g0r = T(0), g0i = T(0), d1r = T(0), d1i = T(0), d2r = T(0), d2i = T(0);
+    __device__ __forceinline__ void load(const VkgArgs& v, int l) {
+        double gr[3] = {0.0, 0.0, 0.0}, gi[3] = {0.0, 0.0, 0.0};
+        for (int b = 0; b < v.gnb; ++b) {
+            const int d = v.gdof[l * v.gnb + b];
+            if (d < 0) continue;
+            gr[b] = HELM ? v.g[2 * d] : v.g[d];
+            gi[b] = HELM ? (v.conj ? -v.g[2 * d + 1] : v.g[2 * d + 1]) : 0.0;
+        }
+        if (v.gnb != 3) {
+            gr[1] = gr[2] = gr[0];
+            gi[1] = gi[2] = gi[0];
+        }
+        g0r = T(gr[0]);
+        g0i = T(gi[0]);
+        d1r = T(gr[1] - gr[0]);
+        d1i = T(gi[1] - gi[0]);
+        d2r = T(gr[2] - gr[0]);
+        d2i = T(gi[2] - gi[0]);
+    }
+    __device__ __forceinline__ void at(T p1, T p2, T& re, T& im) const {
+        re = fma(p2, d2r, fma(p1, d1r, g0r));
+        im = HELM ? fma(p2, d2i, fma(p1, d1i, g0i)) : T(0);
+    }
+};
+
 template <bool HELM, typename T>
 __global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs v) {
     using V4 = typename V4T<T>::type;
@@ -798,6 +952,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs
     __shared__ int s_gi[FAR_TI];
     __shared__ int s_tri[FAR_TI][3];
     __shared__ double s_cen[FAR_TI][3];
+    __shared__ double s_nrm[FAR_TI][3];
 
     const int Q2 = a.Q2;
     const int lj = blockIdx.x * FAR_THREADS + threadIdx.x;
@@ -819,6 +974,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs
         for (int c = 0; c < 3; ++c) {
             s_tri[threadIdx.x][c] = gi >= 0 ? a.tris[3 * gi + c] : -1;
             s_cen[threadIdx.x][c] = gi >= 0 ? a.centroid[3 * gi + c] : 0.0;
+            s_nrm[threadIdx.x][c] = gi >= 0 ? a.normal[3 * gi + c] : 0.0;
         }
     }
     __syncthreads();
@@ -832,17 +988,11 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs
         tri_j[c] = a.tris[3 * gj + c];
         cen_j[c] = a.centroid[3 * gj + c];
     }
-    const T nx = T(a.normal[3 * gj + 0]), ny = T(a.normal[3 * gj + 1]), nz = T(a.normal[3 * gj + 2]);
+    const double nj64[3] = {a.normal[3 * gj + 0], a.normal[3 * gj + 1], a.normal[3 * gj + 2]};
+    const T nx = T(nj64[0]), ny = T(nj64[1]), nz = T(nj64[2]);
     // trial data at the trial panel's basis functions (conjugated when asked)
-    T gr[3] = {T(0), T(0), T(0)}, gim[3] = {T(0), T(0), T(0)};
-    if (valid_j) {
-        for (int by = 0; by < v.gnb; ++by) {
-            int d = v.gdof[lj * v.gnb + by];
-            if (d < 0) continue;
-            gr[by] = T(HELM ? v.g[2 * d] : v.g[d]);
-            gim[by] = HELM ? T(v.conj ? -v.g[2 * d + 1] : v.g[2 * d + 1]) : T(0);
-        }
-    }
+    PanelData<HELM, T> gj_data;
+    if (valid_j) gj_data.load(v, lj);
     const V4* ptsj = pts + (size_t)gj * Q2;
     const T kk = T(a.k);
     const int lane = threadIdx.x & 31;
@@ -861,24 +1011,39 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs
                          dcz64 = s_cen[t][2] - cen_j[2];
             const T dcx = T(dcx64), dcy = T(dcy64), dcz = T(dcz64);
             const T dlx = T(dcx64 - double(dcx)), dly = T(dcy64 - double(dcy)), dlz = T(dcz64 - double(dcz));
+            Frame<T, HELM> fr;
+            fr.init(dcx64, dcy64, dcz64, a.k, a.area[gi], a.area[gj], a.wcorr);
+            const T Dn = T(dcx64 * nj64[0] + dcy64 * nj64[1] + dcz64 * nj64[2]);
+            // x_a.n_j = x_a.(n_j - n_i) (x_a lies in the plane of panel i)
+            const T mx = T(nj64[0] - s_nrm[t][0]), my = T(nj64[1] - s_nrm[t][1]), mz = T(nj64[2] - s_nrm[t][2]);
             const V4* sxt = sx + t * Q2;
             for (int b = 0; b < Q2; ++b) {
                 const V4 yb = ptsj[b];
                 const T ex = (dcx - yb.x) + dlx, ey = (dcy - yb.y) + dly, ez = (dcz - yb.z) + dlz;
+                const T wx = fr.ux - yb.x, wy = fr.uy - yb.y, wz = fr.uz - yb.z;
                 T sv_re = T(0), sv_im = T(0), sk_re = T(0), sk_im = T(0);
 #pragma unroll 5
                 for (int q = 0; q < Q2; ++q) {
                     const V4 xa = sxt[q];
-                    const T dx = xa.x + ex, dy = xa.y + ey, dz = xa.z + ez;
-                    const T r2 = dx * dx + dy * dy + dz * dz;
-                    const T rinv = dev_rsqrt(r2);
-                    const T dn = dx * nx + dy * ny + dz * nz;
+                    T r, rinv, dn, phase;
+                    if constexpr (Frame<T, HELM>::SPLIT) {
+                        const T e_x = xa.x - yb.x, e_y = xa.y - yb.y, e_z = xa.z - yb.z;
+                        const T sq = e_x * (xa.x + wx) + e_y * (xa.y + wy) + e_z * (xa.z + wz);
+                        dev_r_rinv(fr.R2 + sq, r, rinv);
+                        dn = fma(xa.x, mx, fma(xa.y, my, fma(xa.z, mz, Dn)));
+                        phase = HELM ? kk * __fdividef(sq, r + fr.Rf) : T(0);
+                    } else {
+                        const T dx = xa.x + ex, dy = xa.y + ey, dz = xa.z + ez;
+                        dev_r_rinv(dx * dx + dy * dy + dz * dz, r, rinv);
+                        dn = dx * nx + dy * ny + dz * nz;
+                        phase = kk * r;
+                    }
                     const T wr = xa.w * rinv;
                     const T tk = xa.w * dn * rinv * rinv * rinv;
                     if (HELM) {
-                        const T kr = kk * (r2 * rinv);
+                        const T kr = kk * r;
                         T sn, cs;
-                        dev_sincos(kr, &sn, &cs);
+                        dev_sincos(phase, &sn, &cs);
                         sv_re += wr * cs;
                         sv_im += wr * sn;
                         sk_re += tk * fma(kr, sn, cs);
@@ -892,15 +1057,13 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs
                 av_re += wb * double(sv_re);
                 av_im += wb * double(sv_im);
                 // g interpolated at trial point b
-                T gb_re = gr[0], gb_im = gim[0];
-                if (v.gnb == 3) {
-                    const T p0 = sphi[3 * b], p1 = sphi[3 * b + 1], p2 = sphi[3 * b + 2];
-                    gb_re = p0 * gr[0] + p1 * gr[1] + p2 * gr[2];
-                    gb_im = p0 * gim[0] + p1 * gim[1] + p2 * gim[2];
-                }
+                T gb_re, gb_im;
+                gj_data.at(sphi[3 * b + 1], sphi[3 * b + 2], gb_re, gb_im);
                 ak_re += wb * (double(sk_re) * double(gb_re) - double(sk_im) * double(gb_im));
                 ak_im += wb * (double(sk_re) * double(gb_im) + double(sk_im) * double(gb_re));
             }
+            fr.rotate(av_re, av_im);
+            fr.rotate(ak_re, ak_im);
             const int row = a.test_dof[li];
             const int col = a.trial_dof[lj];
             if (row >= 0 && col >= 0)
@@ -977,13 +1140,9 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, Vkg
         T gre = T(0), gim = T(0);
         if (li < n) {
             sx[idx] = pts[(size_t)s_gi[t] * Q2 + q];
-            for (int bx = 0; bx < v.gnb; ++bx) {
-                int d = v.gdof[li * v.gnb + bx];
-                if (d < 0) continue;
-                T ph = v.gnb == 3 ? sphi[3 * q + bx] : T(1);
-                gre += ph * T(HELM ? v.g[2 * d] : v.g[d]);
-                if (HELM) gim += ph * T(v.conj ? -v.g[2 * d + 1] : v.g[2 * d + 1]);
-            }
+            PanelData<HELM, T> gd;
+            gd.load(v, li);
+            gd.at(sphi[3 * q + 1], sphi[3 * q + 2], gre, gim);
         }
         sgx[2 * idx] = gre;
         sgx[2 * idx + 1] = gim;
@@ -999,15 +1158,10 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, Vkg
         tri_j[c] = a.tris[3 * gj + c];
         cen_j[c] = a.centroid[3 * gj + c];
     }
-    const T njx = T(a.normal[3 * gj + 0]), njy = T(a.normal[3 * gj + 1]), njz = T(a.normal[3 * gj + 2]);
-    T gr[3] = {T(0), T(0), T(0)}, gim[3] = {T(0), T(0), T(0)};
-    if (valid_j)
-        for (int by = 0; by < v.gnb; ++by) {
-            int d = v.gdof[lj * v.gnb + by];
-            if (d < 0) continue;
-            gr[by] = T(HELM ? v.g[2 * d] : v.g[d]);
-            gim[by] = HELM ? T(v.conj ? -v.g[2 * d + 1] : v.g[2 * d + 1]) : T(0);
-        }
+    const double nj64[3] = {a.normal[3 * gj + 0], a.normal[3 * gj + 1], a.normal[3 * gj + 2]};
+    const T njx = T(nj64[0]), njy = T(nj64[1]), njz = T(nj64[2]);
+    PanelData<HELM, T> gj_data;
+    if (valid_j) gj_data.load(v, lj);
     const V4* ptsj = pts + (size_t)gj * Q2;
     const T kk = T(a.k);
     const int lane = threadIdx.x & 31;
@@ -1028,11 +1182,22 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, Vkg
             const T dcx = T(dcx64), dcy = T(dcy64), dcz = T(dcz64);
             const T dlx = T(dcx64 - double(dcx)), dly = T(dcy64 - double(dcy)), dlz = T(dcz64 - double(dcz));
             const T nix = T(s_nrm[t][0]), niy = T(s_nrm[t][1]), niz = T(s_nrm[t][2]);
+            Frame<T, HELM> fr;
+            fr.init(dcx64, dcy64, dcz64, a.k, a.area[gi], a.area[gj], a.wcorr);
+            const T Dnj = T(dcx64 * nj64[0] + dcy64 * nj64[1] + dcz64 * nj64[2]);
+            const T Dni = T(dcx64 * s_nrm[t][0] + dcy64 * s_nrm[t][1] + dcz64 * s_nrm[t][2]);
+            // n_j - n_i: x_a.n_j = x_a.(n_j - n_i), y_b.n_i = -y_b.(n_j - n_i) (points lie in their
+            // panel's plane); small for the nearly coplanar close pairs
+            const T mx = T(nj64[0] - s_nrm[t][0]), my = T(nj64[1] - s_nrm[t][1]), mz = T(nj64[2] - s_nrm[t][2]);
+            double pj_re = 0.0, pj_im = 0.0;  // this pair's contribution to row j
             const V4* sxt = sx + t * Q2;
             const T* sgt = sgx + 2 * t * Q2;
             for (int b = 0; b < Q2; ++b) {
                 const V4 yb = ptsj[b];
                 const T ex = (dcx - yb.x) + dlx, ey = (dcy - yb.y) + dly, ez = (dcz - yb.z) + dlz;
+                const T wx = fr.ux - yb.x, wy = fr.uy - yb.y, wz = fr.uz - yb.z;
+                // d.n_i = D.n_i - y_b.n_i (x_a lies in the plane of panel i)
+                const T dni = Dni + (yb.x * mx + yb.y * my + yb.z * mz);
                 // two independent accumulator sets (even / odd test points):
                 // shorter FP32 summation chains and more independent work
                 T acc[2][6];
@@ -1042,17 +1207,30 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, Vkg
                     for (int w = 0; w < 6; ++w) acc[u][w] = T(0);
                 auto term = [&](int q, T* A) {
                     const V4 xa = sxt[q];
-                    const T dx = xa.x + ex, dy = xa.y + ey, dz = xa.z + ez;
-                    const T r2 = dx * dx + dy * dy + dz * dz;
-                    const T rinv = dev_rsqrt(r2);
+                    T r, rinv, dnj, dnx, phase;
+                    if constexpr (Frame<T, HELM>::SPLIT) {
+                        const T e_x = xa.x - yb.x, e_y = xa.y - yb.y, e_z = xa.z - yb.z;
+                        const T sq = e_x * (xa.x + wx) + e_y * (xa.y + wy) + e_z * (xa.z + wz);
+                        dev_r_rinv(fr.R2 + sq, r, rinv);
+                        // d.n_j = D.n_j + x_a.n_j (y_b lies in the plane of panel j)
+                        dnj = fma(xa.x, mx, fma(xa.y, my, fma(xa.z, mz, Dnj)));
+                        dnx = dni;
+                        phase = HELM ? kk * __fdividef(sq, r + fr.Rf) : T(0);
+                    } else {
+                        const T dx = xa.x + ex, dy = xa.y + ey, dz = xa.z + ez;
+                        dev_r_rinv(dx * dx + dy * dy + dz * dz, r, rinv);
+                        dnj = dx * njx + dy * njy + dz * njz;
+                        dnx = dx * nix + dy * niy + dz * niz;
+                        phase = kk * r;
+                    }
                     const T wr = xa.w * rinv;
                     const T wr3 = wr * (rinv * rinv);
-                    const T tj = wr3 * (dx * njx + dy * njy + dz * njz);
-                    const T ti = -wr3 * (dx * nix + dy * niy + dz * niz);
+                    const T tj = wr3 * dnj;
+                    const T ti = -wr3 * dnx;
                     if (HELM) {
-                        const T kr = kk * (r2 * rinv);
+                        const T kr = kk * r;
                         T sn, cs;
-                        dev_sincos(kr, &sn, &cs);
+                        dev_sincos(phase, &sn, &cs);
                         const T f_re = fma(kr, sn, cs), f_im = fma(-kr, cs, sn);
                         A[0] = fma(wr, cs, A[0]);
                         A[1] = fma(wr, sn, A[1]);
@@ -1081,17 +1259,18 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, Vkg
                 const double wb = double(yb.w);
                 av_re += wb * double(sv_re);
                 av_im += wb * double(sv_im);
-                T gb_re = gr[0], gb_im = gim[0];
-                if (v.gnb == 3) {
-                    const T p0 = sphi[3 * b], p1 = sphi[3 * b + 1], p2 = sphi[3 * b + 2];
-                    gb_re = p0 * gr[0] + p1 * gr[1] + p2 * gr[2];
-                    gb_im = p0 * gim[0] + p1 * gim[1] + p2 * gim[2];
-                }
+                T gb_re, gb_im;
+                gj_data.at(sphi[3 * b + 1], sphi[3 * b + 2], gb_re, gb_im);
                 ak_re += wb * (double(sk_re) * double(gb_re) - double(sk_im) * double(gb_im));
                 ak_im += wb * (double(sk_re) * double(gb_im) + double(sk_im) * double(gb_re));
-                rj_re += wb * double(s2_re);
-                rj_im += wb * double(s2_im);
+                pj_re += wb * double(s2_re);
+                pj_im += wb * double(s2_im);
             }
+            fr.rotate(av_re, av_im);
+            fr.rotate(ak_re, ak_im);
+            fr.rotate(pj_re, pj_im);
+            rj_re += pj_re;
+            rj_im += pj_im;
             const int row = a.test_dof[li];
             const int col = a.trial_dof[lj];
             if (row >= 0 && col >= 0) {
@@ -1209,8 +1388,11 @@ int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* te
     fa.centroid = ctx->centroid;
     fa.normal = ctx->normal;
     fa.curl = ctx->curl;
+    fa.area = ctx->area;
+    fa.wcorr = ctx->wcorr32;
     fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
     fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
+    fa.phi64 = ctx->phi64;
     fa.Q2 = ctx->Q2;
     fa.k = op->k;
     fa.k2 = op->k2;
@@ -1280,8 +1462,11 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
     fa.centroid = ctx->centroid;
     fa.normal = ctx->normal;
     fa.curl = ctx->curl;
+    fa.area = ctx->area;
+    fa.wcorr = ctx->wcorr32;
     fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
     fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
+    fa.phi64 = ctx->phi64;
     fa.Q2 = ctx->Q2;
     fa.k = op->k;
     fa.k2 = op->k2;

@@ -29,7 +29,8 @@ struct bem_ctx {
     double* centroid = nullptr;  // [nt*3]
     double* curl = nullptr;      // [nt*9]  curl of P1 hat b: [p*9 + b*3 + c]
     double4* pts64 = nullptr;    // [nt*Q2] separate-rule point offset from centroid (xyz) + weight (w)
-    float4* pts32 = nullptr;     // [nt*Q2] same in FP32
+    float4* pts32 = nullptr;     // [nt*Q2] same in FP32, weight of the reference triangle (no 2A)
+    double wcorr32 = 1.0;        // (exact / FP32 reference weight sum)^2
     double* phi64 = nullptr;     // [Q2*3] P1 hat values at the separate-rule points
     float* phi32 = nullptr;      // [Q2*3]
     double* gp = nullptr;        // [Q]   Gauss points on [0,1]
