@@ -223,7 +223,7 @@ class RHSConstructor3d(_Layer):
 
     def _eval(self, fn, x, *args):
         b = self._BEM_manager
-        xt = torch.as_tensor(x, dtype=torch.float64, device=b.device)
+        xt = x if isinstance(x, torch.Tensor) else torch.as_tensor(x, dtype=torch.float64, device=b.device)
         targs = [torch.as_tensor(a, dtype=torch.float64, device=b.device) if isinstance(a, np.ndarray) else a
                  for a in args]
         val = fn(xt, *targs)
@@ -234,60 +234,65 @@ class RHSConstructor3d(_Layer):
         b = self._BEM_manager
         mm = b.mesh
         v, f = mm.vertices, mm.panels
+        C = b.cached
         self._Dirichlet_boundary.zero_()
         self._Neumann_boundary.zero_()
         self._f_boundary.zero_()
-        cent = (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
+        cent = lambda: (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
         No, Do = b._Neumann_offset_j, b._Dirichlet_offset_j
         fD, fN = self.analytical_function_Dirichlet, self.analytical_function_Neumann
         if b._is_transmission:
             if self._Q_Neumann == 0:
                 gp = mm.loop_panels("N")
-                x, nrm = cent[gp], mm.panel_normals[gp]
+                x, nrm = C(("bd_cent", "N"), lambda: cent()[gp]), C(("bd_pn", "N"), lambda: mm.panel_normals[gp])
                 fi = self._eval(fN, x, nrm, sqrt_ni)
                 fo = self._eval(fN, x, nrm, sqrt_no)
-                self._Neumann_boundary[torch.as_tensor(gp, device=b.device, dtype=torch.long)] += fi
+                self._Neumann_boundary[C(("bd_gp", "N"), lambda: gp.astype(np.int64))] += fi
                 self._f_boundary[No:No + len(gp)] += fi - fo
             else:
                 vv = np.nonzero(np.isin(mm.vertice_types, (2, 0)))[0]
                 loc = mm._vert_local("N", vv)
-                fi = self._eval(fN, v[vv], mm.vert_normals[vv], sqrt_ni)
-                fo = self._eval(fN, v[vv], mm.vert_normals[vv], sqrt_no)
-                self._Neumann_boundary[torch.as_tensor(vv, device=b.device)] += fi
-                self._f_boundary[torch.as_tensor(No + loc, device=b.device, dtype=torch.long)] += fi - fo
+                x, nrm = C(("bd_v", "N"), lambda: v[vv]), C(("bd_vn", "N"), lambda: mm.vert_normals[vv])
+                fi = self._eval(fN, x, nrm, sqrt_ni)
+                fo = self._eval(fN, x, nrm, sqrt_no)
+                self._Neumann_boundary[C(("bd_vv", "N"), lambda: vv)] += fi
+                self._f_boundary[C(("bd_loc", "N"), lambda: (No + loc).astype(np.int64))] += fi - fo
             if self._Q_Dirichlet == 0:
                 gp = mm.loop_panels("D")
-                fi = self._eval(fD, cent[gp], sqrt_ni)
-                fo = self._eval(fD, cent[gp], sqrt_no)
-                self._Dirichlet_boundary[torch.as_tensor(gp, device=b.device, dtype=torch.long)] += fi
+                x = C(("bd_cent", "D"), lambda: cent()[gp])
+                fi = self._eval(fD, x, sqrt_ni)
+                fo = self._eval(fD, x, sqrt_no)
+                self._Dirichlet_boundary[C(("bd_gp", "D"), lambda: gp.astype(np.int64))] += fi
                 self._f_boundary[Do:Do + len(gp)] += fi - fo
             else:
                 vv = np.nonzero(np.isin(mm.vertice_types, (2, 1)))[0]
                 loc = mm._vert_local("D", vv)
-                fi = self._eval(fD, v[vv], sqrt_ni)
-                fo = self._eval(fD, v[vv], sqrt_no)
-                self._Dirichlet_boundary[torch.as_tensor(vv, device=b.device)] += fi
-                self._f_boundary[torch.as_tensor(Do + loc, device=b.device, dtype=torch.long)] += fi - fo
+                x = C(("bd_v", "D"), lambda: v[vv])
+                fi = self._eval(fD, x, sqrt_ni)
+                fo = self._eval(fD, x, sqrt_no)
+                self._Dirichlet_boundary[C(("bd_vv", "D"), lambda: vv)] += fi
+                self._f_boundary[C(("bd_loc", "D"), lambda: (Do + loc).astype(np.int64))] += fi - fo
         else:
             if self._Q_Neumann == 0:
                 gp = mm.loop_panels("D")
                 if len(gp):
-                    self._Neumann_boundary[torch.as_tensor(gp, device=b.device, dtype=torch.long)] += self._eval(
-                        fN, cent[gp], mm.panel_normals[gp])
+                    self._Neumann_boundary[C(("bd_gp", "D"), lambda: gp.astype(np.int64))] += self._eval(
+                        fN, C(("bd_cent", "D"), lambda: cent()[gp]), C(("bd_pn", "D"), lambda: mm.panel_normals[gp]))
             else:
                 vv = np.nonzero(mm.vertice_types == 1)[0]
                 if len(vv):
-                    self._Neumann_boundary[torch.as_tensor(vv, device=b.device)] += self._eval(
-                        fN, v[vv], mm.vert_normals[vv])
+                    self._Neumann_boundary[C(("bd_v1",), lambda: vv)] += self._eval(
+                        fN, C(("bd_v1x",), lambda: v[vv]), C(("bd_v1n",), lambda: mm.vert_normals[vv]))
             if self._Q_Dirichlet == 0:
                 gp = mm.loop_panels("N")
                 if len(gp):
-                    self._Dirichlet_boundary[torch.as_tensor(gp, device=b.device, dtype=torch.long)] += self._eval(
-                        fD, cent[gp])
+                    self._Dirichlet_boundary[C(("bd_gp", "N"), lambda: gp.astype(np.int64))] += self._eval(
+                        fD, C(("bd_cent", "N"), lambda: cent()[gp]))
             else:
                 vv = np.nonzero(mm.vertice_types == 0)[0]
                 if len(vv):
-                    self._Dirichlet_boundary[torch.as_tensor(vv, device=b.device)] += self._eval(fD, v[vv])
+                    self._Dirichlet_boundary[C(("bd_v0",), lambda: vv)] += self._eval(
+                        fD, C(("bd_v0x",), lambda: v[vv]))
 
     def multiply_identity_to_vector(self, multiplier: float):
         """rhs += multiplier * M (g | f) (rhs_constructor_3d.py:256-359)."""

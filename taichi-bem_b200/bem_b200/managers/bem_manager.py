@@ -111,6 +111,7 @@ class BEMManager:
         self.engine = Engine(self.device)
         self.engine.set_mesh(mm.vertices, mm.panels, self._GaussQR)
         self._spaces = {}
+        self._dev_cache = {}
         z = lambda *s: torch.zeros(*s, dtype=self.torch_dtype, device=self.device)
         self._mat_A = z(n, n)
         self.rhs = z(2 * n if self._is_transmission else n)
@@ -144,6 +145,18 @@ class BEMManager:
             sp = DeviceSpace.from_numpy(panels, nb, dof, self.device)
             self._spaces[key] = sp
         return sp
+
+    def cached(self, key, make, dtype=None) -> torch.Tensor:
+        """Device copy of a mesh-derived host array, made once per mesh (the
+        boundary data, post-processing and index gathers of every run reuse
+        it instead of copying from pageable host memory)."""
+        t = self._dev_cache.get(key)
+        if t is None:
+            t = torch.as_tensor(np.ascontiguousarray(make()), device=self.device)
+            if dtype is not None:
+                t = t.to(dtype)
+            self._dev_cache[key] = t
+        return t
 
     def op_desc(self, op: int, k: float, sqrt_n: float) -> L.OpDesc:
         helm = self._n == 2
@@ -305,29 +318,32 @@ class BEMManager:
             self.raw_analytical_solved[Do:Do + min(nD, self.M_Dirichlet)] = rc._Dirichlet_boundary[:self.M_Dirichlet]
             self.raw_analytical_solved[No:No + min(nN, self.N_Neumann)] = rc._Neumann_boundary[:self.N_Neumann]
             return
-        cent = (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
+        C = self.cached
+        cent = lambda: (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
         if self.N_Neumann > 0:
             if self.shape_func_degree_Neumann == 0:
                 gp = mm.loop_panels("N")
-                val = rc._eval(self.analytical_function_Neumann, cent[gp], mm.panel_normals[gp])
+                val = rc._eval(self.analytical_function_Neumann, C(("ex_cent", "N"), lambda: cent()[gp]),
+                               C(("ex_pn", "N"), lambda: mm.panel_normals[gp]))
                 self.raw_analytical_solved[self._Neumann_offset_j:self._Neumann_offset_j + len(gp)] = val
             else:
                 vv = np.nonzero(mm.vertice_types == int(VertAttachType.NEUMANN_TOBESOLVED))[0]
                 loc = mm._vert_local("N", vv)
                 ok = loc >= 0
-                val = rc._eval(self.analytical_function_Neumann, v[vv[ok]], mm.vert_normals[vv[ok]])
-                self.raw_analytical_solved[torch.as_tensor(loc[ok] + self._Neumann_offset_j, device=dev)] = val
+                val = rc._eval(self.analytical_function_Neumann, C(("ex_v", "N"), lambda: v[vv[ok]]),
+                               C(("ex_vn", "N"), lambda: mm.vert_normals[vv[ok]]))
+                self.raw_analytical_solved[C(("ex_loc", "N"), lambda: loc[ok] + self._Neumann_offset_j)] = val
         if self.M_Dirichlet > 0:
             if self.shape_func_degree_Dirichlet == 0:
                 gp = mm.loop_panels("D")
-                val = rc._eval(self.analytical_function_Dirichlet, cent[gp])
+                val = rc._eval(self.analytical_function_Dirichlet, C(("ex_cent", "D"), lambda: cent()[gp]))
                 self.raw_analytical_solved[self._Dirichlet_offset_j:self._Dirichlet_offset_j + len(gp)] = val
             else:
                 vv = np.nonzero(mm.vertice_types == int(VertAttachType.DIRICHLET_TOBESOLVED))[0]
                 loc = mm._vert_local("D", vv)
                 ok = loc >= 0
-                val = rc._eval(self.analytical_function_Dirichlet, v[vv[ok]])
-                self.raw_analytical_solved[torch.as_tensor(loc[ok] + self._Dirichlet_offset_j, device=dev)] = val
+                val = rc._eval(self.analytical_function_Dirichlet, C(("ex_v", "D"), lambda: v[vv[ok]]))
+                self.raw_analytical_solved[C(("ex_loc", "D"), lambda: loc[ok] + self._Dirichlet_offset_j)] = val
 
     def splat_u_from_raw_solved_to_vertices(self):
         """Per-vertex values (BEM_manager.py:752-801): P0 values are
@@ -335,22 +351,21 @@ class BEMManager:
         self.solved.zero_()
         self.analytical_solved.zero_()
         mm = self.mesh
-        dev = self.device
-        f = torch.as_tensor(mm.panels, device=dev, dtype=torch.long)
-        pa = torch.as_tensor(mm.panel_areas, device=dev)
-        va = torch.as_tensor(mm.vert_areas, device=dev)
+        C = self.cached
 
         def splat_p0(side, offset, excluded):
             gp = mm.loop_panels(side)
             if len(gp) == 0:
                 return
             ok = mm.panel_types[gp] != excluded
-            idx = np.arange(len(gp))[ok]
-            gpt = torch.as_tensor(gp[ok], device=dev, dtype=torch.long)
-            w = (pa[gpt] / 3.0).unsqueeze(1) / va[f[gpt]]
+            gsel = gp[ok]
+            # per-panel weight area/3 / vertex area, the panel's vertices and DOF rows
+            w = C(("sp_w", side), lambda: (mm.panel_areas[gsel] / 3.0)[:, None] / mm.vert_areas[mm.panels[gsel]])
+            fv = C(("sp_f", side), lambda: mm.panels[gsel].reshape(-1).astype(np.int64))
+            rows = C(("sp_rows", side, offset), lambda: np.arange(len(gp))[ok] + offset)
             for src, dst in ((self.raw_solved, self.solved), (self.raw_analytical_solved, self.analytical_solved)):
-                vals = src[torch.as_tensor(idx + offset, device=dev)].unsqueeze(1) * w
-                dst.index_add_(0, f[gpt].reshape(-1), vals.reshape(-1))
+                vals = src[rows].unsqueeze(1) * w
+                dst.index_add_(0, fv, vals.reshape(-1))
 
         def splat_p1(side, offset, excluded):
             vv = np.nonzero(mm.vertice_types != excluded)[0]
@@ -358,8 +373,8 @@ class BEMManager:
             ok = loc >= 0
             if not ok.any():
                 return
-            vt = torch.as_tensor(vv[ok], device=dev)
-            lt = torch.as_tensor(loc[ok] + offset, device=dev)
+            vt = C(("sp_vt", side, excluded), lambda: vv[ok])
+            lt = C(("sp_lt", side, excluded, offset), lambda: loc[ok] + offset)
             self.solved[vt] += self.raw_solved[lt]
             self.analytical_solved[vt] += self.raw_analytical_solved[lt]
 

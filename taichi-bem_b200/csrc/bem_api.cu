@@ -141,6 +141,19 @@ int check_op(bem_ctx* ctx, const bem_op_desc* op) {
 
 }  // namespace
 
+int bem_lookahead_stream(bem_ctx* ctx) {
+    if (ctx->aux) return BEM_OK;
+    int least = 0, greatest = 0;
+    if (int rc = bem_check_cuda(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities"))
+        return rc;
+    if (int rc = bem_check_cuda(ctx, cudaStreamCreateWithPriority(&ctx->aux, cudaStreamNonBlocking, greatest),
+                                "side stream"))
+        return rc;
+    if (int rc = bem_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_next, cudaEventDisableTiming), "event"))
+        return rc;
+    return bem_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_diag, cudaEventDisableTiming), "event");
+}
+
 extern "C" {
 
 int bem_ctx_create(bem_ctx** out_ctx) {
@@ -165,6 +178,9 @@ int bem_ctx_create(bem_ctx** out_ctx) {
 int bem_ctx_destroy(bem_ctx* ctx) {
     if (!ctx) return BEM_OK;
     free_mesh(ctx);
+    if (ctx->ev_next) cudaEventDestroy(ctx->ev_next);
+    if (ctx->ev_diag) cudaEventDestroy(ctx->ev_diag);
+    if (ctx->aux) cudaStreamDestroy(ctx->aux);
     if (ctx->ws) cudaFree(ctx->ws);
     if (ctx->flags) cudaFree(ctx->flags);
     delete ctx;
@@ -247,6 +263,21 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
     ctx->Q = Q;
     ctx->Q2 = Q2;
     ctx->wcorr32 = (wsum / wsum32) * (wsum / wsum32);
+    double rho = 0.0;
+    for (int t = 0; t < nt; ++t) {
+        double c[3] = {0.0, 0.0, 0.0};
+        for (int a = 0; a < 3; ++a)
+            for (int d = 0; d < 3; ++d) c[d] += verts[3 * tris[3 * t + a] + d] / 3.0;
+        for (int a = 0; a < 3; ++a) {
+            double q = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                const double e = verts[3 * tris[3 * t + a] + d] - c[d];
+                q += e * e;
+            }
+            rho = std::max(rho, std::sqrt(q));
+        }
+    }
+    ctx->rho_max = rho;
     ctx->n_near = (int64_t)near.size();
     cudaMemcpy(ctx->verts, verts, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->tris, tris, sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice);

@@ -115,6 +115,21 @@ struct Frame {
 // Waite reduction by pi/2 with a two-term split of pi/2 (exact FMA products
 // for |n| < 2^12), Taylor polynomials of sin (through y^9) and cos (through
 // y^10) on |y| <= pi/4 (truncation below 3e-9), and the quadrant rotation.
+// sin/cos polynomials on |y| <= pi/4
+__device__ __forceinline__ void dev_sincos_poly(float y, float* s, float* c) {
+    const float y2 = y * y;
+    // sin y = y (1 - y^2/3! + y^4/5! - y^6/7! + y^8/9!)
+    float ps = fmaf(y2, 2.75573192239858907e-06f, -1.98412698412698413e-04f);
+    ps = fmaf(y2, ps, 8.33333333333333333e-03f);
+    ps = fmaf(y2, ps, -1.66666666666666667e-01f);
+    *s = fmaf(y * y2, ps, y);
+    // cos y = 1 - y^2/2! + y^4/4! - y^6/6! + y^8/8! - y^10/10!
+    float pc = fmaf(y2, -2.75573192239858907e-07f, 2.48015873015873016e-05f);
+    pc = fmaf(y2, pc, -1.38888888888888889e-03f);
+    pc = fmaf(y2, pc, 4.16666666666666667e-02f);
+    pc = fmaf(y2, pc, -0.5f);
+    *c = fmaf(y2, pc, 1.0f);
+}
 __device__ __forceinline__ void dev_sincos(float x, float* s, float* c) {
     const float kTwoOverPi = 0.636619772367581343f;
     const float kPio2Hi = 1.57079637050628662109375f;  // pi/2 rounded to float
@@ -123,22 +138,21 @@ __device__ __forceinline__ void dev_sincos(float x, float* s, float* c) {
     const int q = (int)fn;
     float y = fmaf(-fn, kPio2Hi, x);
     y = fmaf(-fn, kPio2Lo, y);
-    const float y2 = y * y;
-    // sin y = y (1 - y^2/3! + y^4/5! - y^6/7! + y^8/9!)
-    float ps = fmaf(y2, 2.75573192239858907e-06f, -1.98412698412698413e-04f);
-    ps = fmaf(y2, ps, 8.33333333333333333e-03f);
-    ps = fmaf(y2, ps, -1.66666666666666667e-01f);
-    const float sy = fmaf(y * y2, ps, y);
-    // cos y = 1 - y^2/2! + y^4/4! - y^6/6! + y^8/8! - y^10/10!
-    float pc = fmaf(y2, -2.75573192239858907e-07f, 2.48015873015873016e-05f);
-    pc = fmaf(y2, pc, -1.38888888888888889e-03f);
-    pc = fmaf(y2, pc, 4.16666666666666667e-02f);
-    pc = fmaf(y2, pc, -0.5f);
-    const float cy = fmaf(y2, pc, 1.0f);
+    float sy, cy;
+    dev_sincos_poly(y, &sy, &cy);
     float ss = (q & 1) ? cy : sy;
     float cc = (q & 1) ? sy : cy;
     *s = (q & 2) ? -ss : ss;
     *c = ((q + 1) & 2) ? -cc : cc;
+}
+// Split phase k (r - R): |k (r - R)| <= k |x_a - y_b - (c_i - c_j)| <= k (rho_i + rho_j)
+// with rho the largest centroid-to-vertex distance; when the host has bounded
+// that by pi/4 (`small`, uniform over the launch) the reduction is skipped.
+__device__ __forceinline__ void dev_sincos_phase(float x, bool small, float* s, float* c) {
+    if (small)
+        dev_sincos_poly(x, s, c);
+    else
+        dev_sincos(x, s, c);
 }
 __device__ __forceinline__ void dev_sincos(double x, double* s, double* c) { sincos(x, s, c); }
 
@@ -266,7 +280,8 @@ __device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T&
 // The same values in a pair frame (FP32): r2 = R^2 + s, dn = d.n (-d.n_x for
 // K'), Rf = R; the result lacks the pair's factor e^{ikR} (Frame::rotate).
 template <int OP, bool HELM>
-__device__ __forceinline__ void kval_split(float r2, float s, float dn, float k, float Rf, float& re, float& im) {
+__device__ __forceinline__ void kval_split(float r2, float s, float dn, float k, float Rf, bool small, float& re,
+                                           float& im) {
     float r, rinv;
     dev_r_rinv(r2, r, rinv);
     if (OP == BEM_OP_V || OP == BEM_OP_W) {
@@ -275,7 +290,7 @@ __device__ __forceinline__ void kval_split(float r2, float s, float dn, float k,
             im = 0.0f;
         } else {
             float sn, cs;
-            dev_sincos(k * __fdividef(s, r + Rf), &sn, &cs);
+            dev_sincos_phase(k * __fdividef(s, r + Rf), small, &sn, &cs);
             re = rinv * cs;
             im = rinv * sn;
         }
@@ -287,7 +302,7 @@ __device__ __forceinline__ void kval_split(float r2, float s, float dn, float k,
         } else {
             const float kr = k * r;
             float sn, cs;
-            dev_sincos(k * __fdividef(s, r + Rf), &sn, &cs);
+            dev_sincos_phase(k * __fdividef(s, r + Rf), small, &sn, &cs);
             re = t * fmaf(kr, sn, cs);
             im = t * fmaf(-kr, cs, sn);
         }
@@ -305,7 +320,8 @@ struct FarArgs {
     const double* normal;
     const double* curl;
     const double* area;
-    double wcorr;  // (exact / FP32 weight sum)^2 of the FP32 separate rule
+    double wcorr;     // (exact / FP32 weight sum)^2 of the FP32 separate rule
+    int small_phase;  // FP32 split phase bounded by pi/4: sine/cosine without reduction
     const void* pts;
     const void* phi;
     const double* phi64;  // [Q2*3] P1 basis at the separate-rule points, FP64
@@ -453,7 +469,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
                         const T sq = e_x * (xa.x + wx) + e_y * (xa.y + wy) + e_z * (xa.z + wz);
                         // K: d.n_y = D.n_y + x_a.n_y (y_b lies in the plane of panel j)
                         const T dn = (OP == BEM_OP_K) ? fma(xa.x, mx, fma(xa.y, my, fma(xa.z, mz, Dn))) : dnb;
-                        kval_split<OP, HELM>(fr.R2 + sq, sq, dn, kk, fr.Rf, re, im);
+                        kval_split<OP, HELM>(fr.R2 + sq, sq, dn, kk, fr.Rf, a.small_phase != 0, re, im);
                     } else {
                         kval<OP, HELM, T>(xa.x + ex, xa.y + ey, xa.z + ez, nx, ny, nz, kk, re, im);
                     }
@@ -1043,7 +1059,10 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_kernel(FarArgs a, VkgArgs
                     if (HELM) {
                         const T kr = kk * r;
                         T sn, cs;
-                        dev_sincos(phase, &sn, &cs);
+                        if constexpr (Frame<T, HELM>::SPLIT)
+                            dev_sincos_phase(phase, a.small_phase != 0, &sn, &cs);
+                        else
+                            dev_sincos(phase, &sn, &cs);
                         sv_re += wr * cs;
                         sv_im += wr * sn;
                         sk_re += tk * fma(kr, sn, cs);
@@ -1230,7 +1249,10 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, Vkg
                     if (HELM) {
                         const T kr = kk * r;
                         T sn, cs;
-                        dev_sincos(phase, &sn, &cs);
+                        if constexpr (Frame<T, HELM>::SPLIT)
+                            dev_sincos_phase(phase, a.small_phase != 0, &sn, &cs);
+                        else
+                            dev_sincos(phase, &sn, &cs);
                         const T f_re = fma(kr, sn, cs), f_im = fma(-kr, cs, sn);
                         A[0] = fma(wr, cs, A[0]);
                         A[1] = fma(wr, sn, A[1]);
@@ -1390,6 +1412,7 @@ int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* te
     fa.curl = ctx->curl;
     fa.area = ctx->area;
     fa.wcorr = ctx->wcorr32;
+    fa.small_phase = (fp32 && op->kernel == BEM_KERNEL_HELMHOLTZ && op->k * 2.0 * ctx->rho_max <= 0.78) ? 1 : 0;
     fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
     fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
     fa.phi64 = ctx->phi64;
@@ -1464,6 +1487,7 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
     fa.curl = ctx->curl;
     fa.area = ctx->area;
     fa.wcorr = ctx->wcorr32;
+    fa.small_phase = (fp32 && op->kernel == BEM_KERNEL_HELMHOLTZ && op->k * 2.0 * ctx->rho_max <= 0.78) ? 1 : 0;
     fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
     fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
     fa.phi64 = ctx->phi64;

@@ -31,6 +31,7 @@ struct bem_ctx {
     double4* pts64 = nullptr;    // [nt*Q2] separate-rule point offset from centroid (xyz) + weight (w)
     float4* pts32 = nullptr;     // [nt*Q2] same in FP32, weight of the reference triangle (no 2A)
     double wcorr32 = 1.0;        // (exact / FP32 reference weight sum)^2
+    double rho_max = 0.0;        // largest centroid-to-vertex distance of a panel
     double* phi64 = nullptr;     // [Q2*3] P1 hat values at the separate-rule points
     float* phi32 = nullptr;      // [Q2*3]
     double* gp = nullptr;        // [Q]   Gauss points on [0,1]
@@ -44,6 +45,9 @@ struct bem_ctx {
     int32_t* flags = nullptr;        // [16] device-side status words
     void* ws = nullptr;              // linear-algebra workspace
     size_t ws_bytes = 0;
+    // high-priority side stream and events of the LU lookahead (made on first use)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_next = nullptr, ev_diag = nullptr;
 };
 
 // Host helpers (bem_api.cu)
@@ -53,6 +57,7 @@ int bem_ws_reserve(bem_ctx* ctx, size_t bytes);
 
 // Launch wrappers (bem_assembly.cu)
 int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s);
+int bem_lookahead_stream(bem_ctx* ctx);
 int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                         int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
                         void* y, int conj_x, cudaStream_t s);

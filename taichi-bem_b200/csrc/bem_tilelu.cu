@@ -64,157 +64,226 @@ __device__ __forceinline__ CE<T> cinv(CE<T> a) {
 // --------------------------------------------------------------------------
 // diagonal tile: GEPP inside the tile + explicit inverses
 // --------------------------------------------------------------------------
+// Pivot key of a candidate: |re| + |im| as float bits (monotonic for
+// non-negative floats) above 63 - row, so that atomicMax picks the largest
+// magnitude and, among equal ones, the smallest row (the first maximum).  NaN
+// counts as 0.
+template <typename T>
+__device__ __forceinline__ unsigned long long pivot_key(CE<T> v, int r) {
+    float a = (float)(fabs((double)v.re) + fabs((double)v.im));
+    if (!(a == a)) a = 0.0f;
+    return ((unsigned long long)__float_as_uint(a) << 32) | (unsigned)(LU_T - 1 - r);
+}
+
+constexpr int DIAG_LD = LU_T + 1;  // padded row stride: column reads hit distinct banks
+constexpr int DIAG_PW = 8;         // panel width of the blocked factorisation
+constexpr size_t diag_smem_bytes(size_t elem) { return elem * (LU_T * DIAG_LD + LU_T * LU_T); }
+
+// One CTA of 256 threads factors the 64x64 diagonal tile (GEPP restricted to
+// the tile's rows) and forms the explicit inverses.  Blocked by panels of
+// DIAG_PW columns:
+//   panel  : warp 0 alone, warp-synchronous (no CTA barrier per column): pivot
+//            search by a warp max over packed keys, full-row swap, multipliers
+//            and the update inside the panel;
+//   U12    : the panel's rows right of it, L11^{-1} applied by substitution
+//            (one thread per column);
+//   update : rank-DIAG_PW update of the trailing block, one column per thread
+//            with the column's U12 values held in registers.
+// Inverses: Linv (unit lower) and Uinv (upper) by block substitution over
+// DIAG_PW-row blocks against the identity, one after the other in one buffer.
+// Shared memory stays under 65 KB so the kernel fits beside the trailing
+// GEMM's CTAs on an SM.
 template <typename T, bool C>
 __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n, int k0, int32_t* piv,
                                                         CE<T>* dinv, int32_t* info) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    CE<T>* S = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][LU_T]
-    CE<T>* Li = S + LU_T * LU_T;
-    CE<T>* Ui = Li + LU_T * LU_T;
-    __shared__ int s_p;
-    __shared__ int s_zero_pivot;  // first zero pivot of this tile (1-based), 0 = none
+    CE<T>* S = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][DIAG_LD]
+    CE<T>* X = S + LU_T * DIAG_LD;                  // [LU_T][LU_T] inverse being built
+    __shared__ int s_zero_pivot;                    // first zero pivot of this tile (1-based), 0 = none
     const int m = min(LU_T, n - k0);
-    if (threadIdx.x == 0) s_zero_pivot = 0;
-    for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
-        int r = e / LU_T, c = e - r * LU_T;
-        S[e] = (r < m && c < m) ? ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c) : CE<T>{T(0), T(0)};
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) s_zero_pivot = 0;
+    for (int e = tid; e < LU_T * LU_T; e += blockDim.x) {
+        const int r = e / LU_T, c = e - r * LU_T;
+        CE<T> v = CE<T>{T(0), T(0)};
+        if (r < m && c < m) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c);
+        S[r * DIAG_LD + c] = v;
     }
     __syncthreads();
-    for (int j = 0; j < m; ++j) {
-        // pivot search in column j (warp 0), then swap rows j and p
-        if (threadIdx.x < 32) {
-            double best = -1.0;
-            int bi = j;
-            for (int r = j + threadIdx.x; r < m; r += 32) {
-                CE<T> v = S[r * LU_T + j];
-                double a = fabs((double)v.re) + fabs((double)v.im);
-                if (a > best || (a == best && r < bi)) {
-                    best = a;
-                    bi = r;
+    for (int j0 = 0; j0 < m; j0 += DIAG_PW) {
+        const int w = min(DIAG_PW, m - j0);
+        if (wid == 0) {
+            for (int j = j0; j < j0 + w; ++j) {
+                // pivot: largest |re| + |im| in column j among rows j..m-1, first one on ties
+                unsigned long long key = 0ull;
+                for (int r = j + lane; r < m; r += 32) {
+                    const unsigned long long kr = pivot_key(S[r * DIAG_LD + j], r);
+                    key = kr > key ? kr : key;
                 }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (ob > best || (ob == best && oi < bi)) {
-                    best = ob;
-                    bi = oi;
+                for (int o = 16; o > 0; o >>= 1) {
+                    const unsigned long long ko = __shfl_xor_sync(0xffffffffu, key, o);
+                    key = ko > key ? ko : key;
                 }
-            }
-            if (threadIdx.x == 0) {
-                s_p = bi;
-                piv[k0 + j] = k0 + bi;
-                if (!(best > 0.0) && s_zero_pivot == 0) s_zero_pivot = k0 + j + 1;
-            }
-            const int p = __shfl_sync(0xffffffffu, bi, 0);
-            if (p != j)
-                for (int c = threadIdx.x; c < LU_T; c += 32) {
-                    CE<T> t = S[j * LU_T + c];
-                    S[j * LU_T + c] = S[p * LU_T + c];
-                    S[p * LU_T + c] = t;
+                const int p = LU_T - 1 - (int)(key & 0xffffffffull);
+                const int pr = (p >= j && p < m) ? p : j;  // all-zero or NaN column: no swap
+                if (pr != j)
+                    for (int c = lane; c < LU_T; c += 32) {
+                        const CE<T> t = S[j * DIAG_LD + c];
+                        S[j * DIAG_LD + c] = S[pr * DIAG_LD + c];
+                        S[pr * DIAG_LD + c] = t;
+                    }
+                __syncwarp();
+                const CE<T> pv = S[j * DIAG_LD + j];
+                if (lane == 0) {
+                    piv[k0 + j] = k0 + pr;
+                    if (!((double)pv.re != 0.0 || (double)pv.im != 0.0) && s_zero_pivot == 0)
+                        s_zero_pivot = k0 + j + 1;
                 }
+                const CE<T> ip = cinv(pv);
+                for (int r = j + 1 + lane; r < m; r += 32) {
+                    const CE<T> l = cmul(S[r * DIAG_LD + j], ip);
+                    S[r * DIAG_LD + j] = l;
+                    for (int c = j + 1; c < j0 + w; ++c) {
+                        const CE<T> u = S[j * DIAG_LD + c];
+                        CE<T> v = S[r * DIAG_LD + c];
+                        v.re -= l.re * u.re - l.im * u.im;
+                        v.im -= l.re * u.im + l.im * u.re;
+                        S[r * DIAG_LD + c] = v;
+                    }
+                }
+                __syncwarp();
+            }
         }
         __syncthreads();
-        // multipliers and rank-1 update in one pass: element (r, c), c > j,
-        // uses l_r = S[r][j] / S[j][j]; column j itself is scaled by the
-        // threads of c == j after everyone has read it (second sync)
-        const CE<T> inv = cinv(S[j * LU_T + j]);
-        // thread t owns columns c = j + (t % 64) ... of rows j+1+(t/64), +4, ...:
-        // fixed (row, column) ownership keeps the buffered values in registers
-        const int cc = j + (threadIdx.x & 63);
-        const int r0 = j + 1 + (threadIdx.x >> 6);
-        constexpr int RPT = LU_T / 4;  // rows per thread
-        CE<T> upd[RPT];
+        const int c1 = j0 + w;  // first column right of the panel
+        if (c1 < m) {
+            // U12 = L11^{-1} A12: rows j0..c1-1, one thread per column
+            for (int c = c1 + tid; c < m; c += blockDim.x) {
+                CE<T> u[DIAG_PW];
 #pragma unroll
-        for (int it = 0; it < RPT; ++it) {
-            const int r = r0 + 4 * it;
-            upd[it] = CE<T>{T(0), T(0)};
-            if (r < m && cc < m) {
-                const CE<T> l = cmul(S[r * LU_T + j], inv);
-                if (cc == j) {
-                    upd[it] = l;
-                } else {
-                    const CE<T> lu = cmul(l, S[j * LU_T + cc]), v = S[r * LU_T + cc];
-                    upd[it] = CE<T>{v.re - lu.re, v.im - lu.im};
-                }
-            }
-        }
-        __syncthreads();
+                for (int i = 0; i < DIAG_PW; ++i) {
+                    if (i < w) {
+                        CE<T> v = S[(j0 + i) * DIAG_LD + c];
 #pragma unroll
-        for (int it = 0; it < RPT; ++it) {
-            const int r = r0 + 4 * it;
-            if (r < m && cc < m) S[r * LU_T + cc] = upd[it];
-        }
-        __syncthreads();
-    }
-    // explicit inverses, rows in sequence, all columns of a row in parallel:
-    // threads 0..127 build Linv (two threads per column, partial sums combined
-    // with a shuffle), threads 128..255 build Uinv the same way from the
-    // bottom row up.  Named barriers keep the two halves independent.
-    {
-        const int half = threadIdx.x >> 7;  // 0: Linv, 1: Uinv
-        const int t = threadIdx.x & 127;
-        const int c = t >> 1, part = t & 1;
-        CE<T>* X = half == 0 ? Li : Ui;
-        for (int e = t; e < LU_T * LU_T; e += 128) X[e] = CE<T>{T(0), T(0)};
-        if (half == 0)
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-        else
-            asm volatile("bar.sync 2, 128;" ::: "memory");
-        for (int step = 0; step < LU_T; ++step) {
-            const int r = half == 0 ? step : LU_T - 1 - step;
-            CE<T> sum = CE<T>{T(0), T(0)};
-            if (r < m) {
-                if (half == 0) {
-                    // Linv[r][c] = delta_rc - sum_{c <= q < r} L[r][q] Linv[q][c]   (c <= r)
-                    if (c < r)
-                        for (int q = c + part; q < r; q += 2) {
-                            CE<T> tt = cmul(S[r * LU_T + q], X[q * LU_T + c]);
-                            sum.re += tt.re;
-                            sum.im += tt.im;
+                        for (int q = 0; q < i; ++q) {
+                            const CE<T> l = S[(j0 + i) * DIAG_LD + j0 + q];
+                            v.re -= l.re * u[q].re - l.im * u[q].im;
+                            v.im -= l.re * u[q].im + l.im * u[q].re;
                         }
-                } else {
-                    // Uinv[r][c] = (delta_rc - sum_{r < q <= c} U[r][q] Uinv[q][c]) / U[r][r]   (r <= c)
-                    if (c > r)
-                        for (int q = r + 1 + part; q <= c && q < m; q += 2) {
-                            CE<T> tt = cmul(S[r * LU_T + q], X[q * LU_T + c]);
-                            sum.re += tt.re;
-                            sum.im += tt.im;
-                        }
+                        u[i] = v;
+                        S[(j0 + i) * DIAG_LD + c] = v;
+                    }
                 }
             }
-            sum.re += __shfl_xor_sync(0xffffffffu, sum.re, 1);
-            sum.im += __shfl_xor_sync(0xffffffffu, sum.im, 1);
-            if (part == 0) {
-                CE<T> val;
-                if (r >= m) {
-                    val = CE<T>{r == c ? T(1) : T(0), T(0)};  // identity padding of a short last tile
-                } else if (half == 0) {
-                    val = c < r ? CE<T>{-sum.re, -sum.im} : CE<T>{r == c ? T(1) : T(0), T(0)};
-                } else if (c < r) {
-                    val = CE<T>{T(0), T(0)};
-                } else if (c >= m) {
-                    val = CE<T>{T(0), T(0)};
-                } else {
-                    CE<T> d = CE<T>{(r == c ? T(1) : T(0)) - sum.re, -sum.im};
-                    val = cmul(d, cinv(S[r * LU_T + r]));
+            __syncthreads();
+            // A22 -= L21 U12: thread column c1 + (tid & 63), rows (tid >> 6) + 4k
+            const int cc = c1 + (tid & 63);
+            if (cc < m) {
+                CE<T> u[DIAG_PW];
+#pragma unroll
+                for (int q = 0; q < DIAG_PW; ++q)
+                    u[q] = q < w ? S[(j0 + q) * DIAG_LD + cc] : CE<T>{T(0), T(0)};
+                for (int r = c1 + (tid >> 6); r < m; r += 4) {
+                    CE<T> v = S[r * DIAG_LD + cc];
+#pragma unroll
+                    for (int q = 0; q < DIAG_PW; ++q) {
+                        const CE<T> l = S[r * DIAG_LD + j0 + q];
+                        v.re -= l.re * u[q].re - l.im * u[q].im;
+                        v.im -= l.re * u[q].im + l.im * u[q].re;
+                    }
+                    S[r * DIAG_LD + cc] = v;
                 }
-                X[r * LU_T + c] = val;
             }
-            if (half == 0)
-                asm volatile("bar.sync 1, 128;" ::: "memory");
-            else
-                asm volatile("bar.sync 2, 128;" ::: "memory");
+            __syncthreads();
         }
     }
-    __syncthreads();
-    if (threadIdx.x == 0 && s_zero_pivot != 0 && *info == 0) *info = s_zero_pivot;
+    // ---- explicit inverses by block substitution against the identity ----
+    // Linv: for row block i: X_i = L_ii^{-1} (E_i - sum_{k<i} L_ik X_k)
+    // Uinv: for row block i (descending): X_i = U_ii^{-1} (E_i - sum_{k>i} U_ik X_k)
+    // thread: column c = tid & 63, rows (tid >> 6) * 2 + {0, 1} of the block
     CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T;
-    for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
-        D[e] = Li[e];
-        D[LU_T * LU_T + e] = Ui[e];
-        int r = e / LU_T, c = e - r * LU_T;
-        if (r < m && c < m) stE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c, S[e]);
+    const int c = tid & 63, rq = (tid >> 6) * 2;
+    for (int which = 0; which < 2; ++which) {
+        for (int bs = 0; bs < LU_T / DIAG_PW; ++bs) {
+            const int ib = which == 0 ? bs : LU_T / DIAG_PW - 1 - bs;
+            const int r0 = ib * DIAG_PW;
+            // T = E_i - sum over finished blocks, two rows per thread
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = r0 + rq + h;
+                CE<T> v = CE<T>{r == c ? T(1) : T(0), T(0)};
+                if (r < m) {
+                    if (which == 0) {
+                        for (int q = 0; q < r0; ++q) {
+                            const CE<T> l = S[r * DIAG_LD + q], x = X[q * LU_T + c];
+                            v.re -= l.re * x.re - l.im * x.im;
+                            v.im -= l.re * x.im + l.im * x.re;
+                        }
+                    } else {
+                        for (int q = r0 + DIAG_PW; q < m; ++q) {
+                            const CE<T> uu = S[r * DIAG_LD + q], x = X[q * LU_T + c];
+                            v.re -= uu.re * x.re - uu.im * x.im;
+                            v.im -= uu.re * x.im + uu.im * x.re;
+                        }
+                    }
+                }
+                X[r * LU_T + c] = v;
+            }
+            __syncthreads();
+            // diagonal block: substitution down (Linv) or up (Uinv) the 8 rows, one thread per column
+            if (tid < LU_T) {
+                CE<T> y[DIAG_PW];
+#pragma unroll
+                for (int i = 0; i < DIAG_PW; ++i) y[i] = X[(r0 + i) * LU_T + c];
+                if (which == 0) {
+#pragma unroll
+                    for (int i = 0; i < DIAG_PW; ++i) {
+                        const int r = r0 + i;
+                        if (r >= m) {
+                            y[i] = CE<T>{r == c ? T(1) : T(0), T(0)};  // identity padding of a short last tile
+                            continue;
+                        }
+#pragma unroll
+                        for (int q = 0; q < i; ++q) {
+                            const CE<T> l = S[r * DIAG_LD + r0 + q];
+                            y[i].re -= l.re * y[q].re - l.im * y[q].im;
+                            y[i].im -= l.re * y[q].im + l.im * y[q].re;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int i = DIAG_PW - 1; i >= 0; --i) {
+                        const int r = r0 + i;
+                        if (r >= m) {
+                            y[i] = CE<T>{r == c ? T(1) : T(0), T(0)};
+                            continue;
+                        }
+                        if (c >= m) {
+                            y[i] = CE<T>{T(0), T(0)};
+                            continue;
+                        }
+#pragma unroll
+                        for (int q = i + 1; q < DIAG_PW; ++q) {
+                            if (r0 + q >= m) continue;
+                            const CE<T> uu = S[r * DIAG_LD + r0 + q];
+                            y[i].re -= uu.re * y[q].re - uu.im * y[q].im;
+                            y[i].im -= uu.re * y[q].im + uu.im * y[q].re;
+                        }
+                        y[i] = cmul(y[i], cinv(S[r * DIAG_LD + r]));
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < DIAG_PW; ++i) X[(r0 + i) * LU_T + c] = y[i];
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < LU_T * LU_T; e += blockDim.x) D[which * LU_T * LU_T + e] = X[e];
+        __syncthreads();
+    }
+    if (tid == 0 && s_zero_pivot != 0 && *info == 0) *info = s_zero_pivot;
+    for (int e = tid; e < LU_T * LU_T; e += blockDim.x) {
+        const int r = e / LU_T, cc = e - r * LU_T;
+        if (r < m && cc < m) stE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + cc, S[r * DIAG_LD + cc]);
     }
 }
 
@@ -326,106 +395,201 @@ __device__ __forceinline__ bool wait_flag(const int* flags, int j, int epoch, in
     return s_ok != 0;
 }
 
+// Warp-level bounded wait for a ready flag: lane 0 spins with acquire loads,
+// the warp barrier that follows orders the other lanes' reads after it.
+__device__ __forceinline__ bool warp_wait_flag(const int* flags, int j, int epoch, int32_t* err) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        unsigned it = 0;
+        while (ld_acquire_i(flags + j) != epoch) {
+            if (++it > FLAG_SPIN_CAP) {
+                atomicExch(err, BEM_ERR_TIMEOUT);
+                ok = 0;
+                break;
+            }
+            if ((it & 63u) == 0u && *(volatile int32_t*)err != 0) {
+                ok = 0;
+                break;
+            }
+            if (it > 256u) __nanosleep(64);
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
+}
+
 // x (FP64, real or complex interleaved, one right-hand side) overwritten by
 // U^{-1} L^{-1} x; the input must already be permuted (x = P b).
+// Block row k, per pass (forward with L, backward with U):
+//   * the block of the last dependency (L_k,k-1 or U_k,k+1) and the diagonal
+//     inverse (Linv_k or Uinv_k) are prefetched into shared memory;
+//   * every other finished block j is streamed from memory: warp w owns rows
+//     w, w+8, ... and keeps per-lane partial sums of L_kj x_j (in the factor's
+//     precision), two blocks per iteration, no CTA barrier, one cross-lane
+//     reduction at the end;
+//   * once the last dependency's flag is set only two GEMVs out of shared
+//     memory remain on the critical path; x_k is then published with a
+//     release store of its flag.
+constexpr int SOLVE_LD = LU_T + 4;  // padded row stride of the staged blocks
+constexpr size_t solve_smem_bytes(size_t elem) { return 2 * elem * LU_T * SOLVE_LD; }
+
 template <typename T, bool C>
 __global__ void __launch_bounds__(256) tile_solve_kernel(const T* LU, int64_t lda, int n, const CE<T>* dinv,
                                                          double* x, int* flags, int epoch, int32_t* err) {
+    constexpr int RW = LU_T / 8;  // rows per warp in the streamed part
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CE<T>* sB = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][SOLVE_LD] last dependency block
+    CE<T>* sD = sB + LU_T * SOLVE_LD;                 // [LU_T][SOLVE_LD] diagonal inverse
     __shared__ double s_acc[LU_T][2];
-    __shared__ double s_part[8][LU_T][2];
-    __shared__ double s_y[LU_T][2];
+    __shared__ double s_x[LU_T][2];
+    __shared__ int s_abort;
     const int nbk = (n + LU_T - 1) / LU_T;
     const int P = gridDim.x;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int gr = tid >> 2, gq = tid & 3;  // GEMV mapping: row gr, columns gq + 4i
     const int W = C ? 2 : 1;
+    if (tid == 0) s_abort = 0;
+    __syncthreads();
     for (int pass = 0; pass < 2; ++pass) {
         const bool fwd = pass == 0;
         for (int t = blockIdx.x; t < nbk; t += P) {
             const int k = fwd ? t : nbk - 1 - t;
             const int r0 = k * LU_T, m = min(LU_T, n - r0);
-            // partial sums over finished blocks: warp w handles dependency blocks j = w, w+8, ...
-            for (int i = threadIdx.x; i < 8 * LU_T * 2; i += blockDim.x) (&s_part[0][0][0])[i] = 0.0;
-            __syncthreads();
             const int ndep = fwd ? k : nbk - 1 - k;
-            for (int d = 0; d < ndep; ++d) {
-                const int j = fwd ? d : nbk - 1 - d;
-                if (!wait_flag(flags, pass * nbk + j, epoch, err)) return;
+            const int jc = ndep > 0 ? (fwd ? k - 1 : k + 1) : -1;  // critical (last) dependency
+            // prefetch: diagonal inverse and the critical block
+            const CE<T>* Dk = dinv + (size_t)k * 2 * LU_T * LU_T + (fwd ? 0 : LU_T * LU_T);
+            for (int e = tid; e < LU_T * LU_T; e += blockDim.x) {
+                const int r = e / LU_T, c = e - r * LU_T;
+                sD[r * SOLVE_LD + c] = Dk[e];
+                CE<T> v = CE<T>{T(0), T(0)};
+                if (jc >= 0) {
+                    const int c0 = jc * LU_T;
+                    if (r < m && c0 + c < n) v = ldE<T, C>(LU, (int64_t)(r0 + r) * lda + c0 + c);
+                }
+                sB[r * SOLVE_LD + c] = v;
+            }
+            // streamed dependencies
+            T acc_re[RW], acc_im[RW];
+#pragma unroll
+            for (int i = 0; i < RW; ++i) acc_re[i] = acc_im[i] = T(0);
+            auto accum = [&](int j) {
                 const int c0 = j * LU_T, mj = min(LU_T, n - c0);
-                // x_j segment
-                double xr0 = 0, xi0 = 0, xr1 = 0, xi1 = 0;
+                T xr0 = T(0), xi0 = T(0), xr1 = T(0), xi1 = T(0);
                 if (lane < mj) {
-                    xr0 = __ldcg(&x[W * (c0 + lane)]);
-                    xi0 = C ? __ldcg(&x[W * (c0 + lane) + 1]) : 0.0;
+                    xr0 = (T)__ldcg(&x[W * (c0 + lane)]);
+                    if (C) xi0 = (T)__ldcg(&x[W * (c0 + lane) + 1]);
                 }
                 if (lane + 32 < mj) {
-                    xr1 = __ldcg(&x[W * (c0 + lane + 32)]);
-                    xi1 = C ? __ldcg(&x[W * (c0 + lane + 32) + 1]) : 0.0;
+                    xr1 = (T)__ldcg(&x[W * (c0 + lane + 32)]);
+                    if (C) xi1 = (T)__ldcg(&x[W * (c0 + lane + 32) + 1]);
                 }
-                for (int r = wid; r < m; r += 8) {
-                    const T* row = LU + (C ? 2 : 1) * ((int64_t)(r0 + r) * lda + c0);
-                    double sr = 0.0, si = 0.0;
-                    if (lane < mj) {
-                        CE<T> l = ldE<T, C>(row, lane);
-                        sr += (double)l.re * xr0 - (double)l.im * xi0;
-                        si += (double)l.re * xi0 + (double)l.im * xr0;
-                    }
-                    if (lane + 32 < mj) {
-                        CE<T> l = ldE<T, C>(row, lane + 32);
-                        sr += (double)l.re * xr1 - (double)l.im * xi1;
-                        si += (double)l.re * xi1 + (double)l.im * xr1;
-                    }
-                    for (int o = 16; o > 0; o >>= 1) {
-                        sr += __shfl_xor_sync(0xffffffffu, sr, o);
-                        si += __shfl_xor_sync(0xffffffffu, si, o);
-                    }
-                    if (lane == 0) {
-                        s_part[wid][r][0] += sr;
-                        s_part[wid][r][1] += si;
+#pragma unroll
+                for (int i = 0; i < RW; ++i) {
+                    const int r = wid + 8 * i;
+                    if (r < m) {
+                        const T* row = LU + W * ((int64_t)(r0 + r) * lda + c0);
+                        if (lane < mj) {
+                            const CE<T> l = ldE<T, C>(row, lane);
+                            acc_re[i] += l.re * xr0 - l.im * xi0;
+                            acc_im[i] += l.re * xi0 + l.im * xr0;
+                        }
+                        if (lane + 32 < mj) {
+                            const CE<T> l = ldE<T, C>(row, lane + 32);
+                            acc_re[i] += l.re * xr1 - l.im * xi1;
+                            acc_im[i] += l.re * xi1 + l.im * xr1;
+                        }
                     }
                 }
-                __syncthreads();
+            };
+            const int nstream = ndep > 0 ? ndep - 1 : 0;  // all but the critical one
+            bool ok = true;
+            int d = 0;
+            for (; d + 1 < nstream && ok; d += 2) {
+                const int j0 = fwd ? d : nbk - 1 - d, j1 = fwd ? d + 1 : nbk - 2 - d;
+                ok = warp_wait_flag(flags, pass * nbk + j0, epoch, err) &&
+                     warp_wait_flag(flags, pass * nbk + j1, epoch, err);
+                if (ok) {
+                    accum(j0);
+                    accum(j1);
+                }
             }
-            // rhs of block k minus the dependencies
-            for (int r = threadIdx.x; r < LU_T; r += blockDim.x) {
-                double ar = 0.0, ai = 0.0;
-                if (r < m) {
-                    ar = __ldcg(&x[W * (r0 + r)]);
-                    ai = C ? __ldcg(&x[W * (r0 + r) + 1]) : 0.0;
-                    for (int w = 0; w < 8; ++w) {
-                        ar -= s_part[w][r][0];
-                        ai -= s_part[w][r][1];
-                    }
-                }
-                s_acc[r][0] = ar;
-                s_acc[r][1] = ai;
+            if (ok && d < nstream) {
+                const int j0 = fwd ? d : nbk - 1 - d;
+                ok = warp_wait_flag(flags, pass * nbk + j0, epoch, err);
+                if (ok) accum(j0);
             }
-            __syncthreads();
-            // y = inverse(diagonal block) * acc
-            const CE<T>* Dk = dinv + (size_t)k * 2 * LU_T * LU_T + (fwd ? 0 : LU_T * LU_T);
-            for (int r = wid; r < m; r += 8) {
-                double sr = 0.0, si = 0.0;
-                for (int q = lane; q < m; q += 32) {
-                    CE<T> d = Dk[r * LU_T + q];
-                    sr += (double)d.re * s_acc[q][0] - (double)d.im * s_acc[q][1];
-                    si += (double)d.re * s_acc[q][1] + (double)d.im * s_acc[q][0];
-                }
+            if (!ok && lane == 0) s_abort = 1;
+#pragma unroll
+            for (int i = 0; i < RW; ++i) {
+                T sr = acc_re[i], si = acc_im[i];
+#pragma unroll
                 for (int o = 16; o > 0; o >>= 1) {
                     sr += __shfl_xor_sync(0xffffffffu, sr, o);
                     si += __shfl_xor_sync(0xffffffffu, si, o);
                 }
+                const int r = wid + 8 * i;
                 if (lane == 0) {
-                    s_y[r][0] = sr;
-                    s_y[r][1] = si;
+                    double br = 0.0, bi = 0.0;
+                    if (r < m) {
+                        br = __ldcg(&x[W * (r0 + r)]) - (double)sr;
+                        bi = C ? __ldcg(&x[W * (r0 + r) + 1]) - (double)si : 0.0;
+                    }
+                    s_acc[r][0] = br;
+                    s_acc[r][1] = bi;
                 }
             }
             __syncthreads();
-            for (int r = threadIdx.x; r < m; r += blockDim.x) {
-                x[W * (r0 + r)] = s_y[r][0];
-                if (C) x[W * (r0 + r) + 1] = s_y[r][1];
+            if (s_abort) return;
+            // critical dependency out of shared memory
+            if (jc >= 0) {
+                if (!wait_flag(flags, pass * nbk + jc, epoch, err)) return;
+                const int c0 = jc * LU_T, mj = min(LU_T, n - c0);
+                if (tid < LU_T) {
+                    s_x[tid][0] = tid < mj ? __ldcg(&x[W * (c0 + tid)]) : 0.0;
+                    s_x[tid][1] = (C && tid < mj) ? __ldcg(&x[W * (c0 + tid) + 1]) : 0.0;
+                }
+                __syncthreads();
+                T sr = T(0), si = T(0);
+#pragma unroll
+                for (int i = 0; i < LU_T / 4; ++i) {
+                    const int c = gq + 4 * i;
+                    const CE<T> l = sB[gr * SOLVE_LD + c];
+                    const T xr = (T)s_x[c][0], xi = (T)s_x[c][1];
+                    sr += l.re * xr - l.im * xi;
+                    si += l.re * xi + l.im * xr;
+                }
+                sr += __shfl_xor_sync(0xffffffffu, sr, 1);
+                si += __shfl_xor_sync(0xffffffffu, si, 1);
+                sr += __shfl_xor_sync(0xffffffffu, sr, 2);
+                si += __shfl_xor_sync(0xffffffffu, si, 2);
+                if (gq == 0 && gr < m) {
+                    s_acc[gr][0] -= (double)sr;
+                    s_acc[gr][1] -= (double)si;
+                }
+                __syncthreads();
+            }
+            // y = inverse(diagonal block) * acc, in FP64
+            double yr = 0.0, yi = 0.0;
+#pragma unroll
+            for (int i = 0; i < LU_T / 4; ++i) {
+                const int c = gq + 4 * i;
+                const CE<T> dd = sD[gr * SOLVE_LD + c];
+                yr += (double)dd.re * s_acc[c][0] - (double)dd.im * s_acc[c][1];
+                yi += (double)dd.re * s_acc[c][1] + (double)dd.im * s_acc[c][0];
+            }
+            yr += __shfl_xor_sync(0xffffffffu, yr, 1);
+            yi += __shfl_xor_sync(0xffffffffu, yi, 1);
+            yr += __shfl_xor_sync(0xffffffffu, yr, 2);
+            yi += __shfl_xor_sync(0xffffffffu, yi, 2);
+            if (gq == 0 && gr < m) {
+                x[W * (r0 + gr)] = yr;
+                if (C) x[W * (r0 + gr) + 1] = yi;
             }
             __threadfence();
             __syncthreads();
-            if (threadIdx.x == 0) st_release_i(flags + pass * nbk + k, epoch);
+            if (tid == 0) st_release_i(flags + pass * nbk + k, epoch);
         }
         // the backward pass of block k needs x_k from the forward pass: every
         // block row's forward flag is checked before its value is read below
@@ -445,39 +609,48 @@ __global__ void permute_kernel(const double* b, const int32_t* perm, double* x, 
     for (int w = 0; w < W; ++w) x[W * i + w] = b[W * s + w];
 }
 
+// Row permutation of the tile-pivoted factor: every swap of diagonal tile k
+// stays inside the tile's rows, so each tile's permutation is built by its own
+// thread (64 sequential swaps in registers-free local order).
 __global__ void tile_piv_to_perm_kernel(const int32_t* piv, int32_t* perm, int n) {
-    extern __shared__ int32_t sp[];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = i;
-    __syncthreads();
-    if (threadIdx.x == 0)
-        for (int i = 0; i < n; ++i) {
-            int p = piv[i];
-            if (p != i && p >= 0 && p < n) {
-                int t = sp[i];
-                sp[i] = sp[p];
-                sp[p] = t;
-            }
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k0 = k * LU_T;
+    if (k0 >= n) return;
+    const int m = min(LU_T, n - k0);
+    for (int i = 0; i < m; ++i) perm[k0 + i] = k0 + i;
+    for (int i = 0; i < m; ++i) {
+        const int p = piv[k0 + i];
+        if (p != k0 + i && p >= k0 && p < k0 + m) {
+            const int t = perm[k0 + i];
+            perm[k0 + i] = perm[p];
+            perm[p] = t;
         }
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sp[i];
+    }
 }
 
 template <typename T, bool C>
 int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* dinv, int32_t* info,
              cudaStream_t s) {
     cudaMemsetAsync(info, 0, sizeof(int32_t), s);
-    const size_t dsmem = sizeof(CE<T>) * 3 * LU_T * LU_T;
+    const size_t dsmem = diag_smem_bytes(sizeof(CE<T>));
     const size_t asmem = sizeof(CE<T>) * 2 * LU_T * LU_T;
     cudaFuncSetAttribute(tile_diag_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem);
     cudaFuncSetAttribute(tile_apply_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem);
+    if (int rc = bem_lookahead_stream(ctx)) return rc;
     const int ni = (int)n;
     const int W = C ? 2 : 1;
+    // Lookahead: step k updates the next tile column first; the diagonal tile
+    // k+1 is then factored on the high-priority side stream while the rest
+    // of step k's trailing update runs (its CTAs take the first free SM).
+    tile_diag_kernel<T, C><<<1, 256, dsmem, s>>>(A, lda, ni, 0, piv, dinv, info);
+    ctx->launches++;
+    bool diag_on_aux = false;
     for (int64_t k0 = 0; k0 < n; k0 += LU_T) {
         const int m = (int)std::min<int64_t>(LU_T, n - k0);
         const int k0i = (int)k0;
-        tile_diag_kernel<T, C><<<1, 256, dsmem, s>>>(A, lda, ni, k0i, piv, dinv, info);
+        if (diag_on_aux) cudaStreamWaitEvent(s, ctx->ev_diag, 0);
         tile_laswp_kernel<T, C><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, lda, ni, k0i, m, piv);
-        ctx->launches += 2;
+        ctx->launches++;
         const int64_t rest = n - k0 - m;
         if (rest > 0) {
             const unsigned tiles = (unsigned)((rest + LU_T - 1) / LU_T);
@@ -487,7 +660,18 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
             T* A22 = A + W * ((k0 + m) * lda + k0 + m);
             const T* L21 = A + W * ((k0 + m) * lda + k0);
             const T* U12 = A + W * (k0 * lda + k0 + m);
-            if (int rc = bem_gemm_update<T, C>(ctx, A22, L21, U12, rest, rest, m, lda, s)) return rc;
+            const int64_t next = std::min<int64_t>(LU_T, rest);
+            if (int rc = bem_gemm_update<T, C>(ctx, A22, L21, U12, rest, next, m, lda, s)) return rc;
+            cudaEventRecord(ctx->ev_next, s);
+            cudaStreamWaitEvent(ctx->aux, ctx->ev_next, 0);
+            tile_diag_kernel<T, C><<<1, 256, dsmem, ctx->aux>>>(A, lda, ni, k0i + m, piv, dinv, info);
+            cudaEventRecord(ctx->ev_diag, ctx->aux);
+            ctx->launches++;
+            diag_on_aux = true;
+            if (rest > next)
+                if (int rc = bem_gemm_update<T, C>(ctx, A22 + W * next, L21, U12 + W * next, rest, rest - next, m,
+                                                   lda, s))
+                    return rc;
         }
         if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "tiled lu step")) return rc;
     }
@@ -519,22 +703,26 @@ int solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t* pi
     int* flags = (int*)(base + off_flags);
     double* x = (double*)(base + off_x);
     if ((size_t)n * sizeof(int32_t) > 200 * 1024) return bem_fail(ctx, BEM_ERR_INVALID, "tiled solve: n > 51200");
-    cudaFuncSetAttribute(tile_piv_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(n * sizeof(int32_t)));
-    tile_piv_to_perm_kernel<<<1, 256, n * sizeof(int32_t), s>>>(piv, perm, (int)n);
+    const unsigned ptiles = (unsigned)((n + LU_T - 1) / LU_T);
+    tile_piv_to_perm_kernel<<<(ptiles + 127) / 128, 128, 0, s>>>(piv, perm, (int)n);
     permute_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, perm, x, (int)n, W);
     cudaMemsetAsync(flags, 0, sizeof(int) * 2 * nbk, s);
     cudaMemsetAsync(ctx->flags + 3, 0, sizeof(int32_t), s);
     ctx->launches += 2;
+    const size_t ssmem = solve_smem_bytes(sizeof(CE<T>));
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(tile_solve_kernel<T, C>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem),
+                                "tile_solve_kernel smem"))
+        return rc;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, ssmem);
     int P = std::max(1, std::min(nbk, per_sm * ctx->num_sms));
     P = std::min(P, ctx->num_sms);
     int ni = (int)n, epoch = 1;
     int32_t* err = ctx->flags + 3;
     void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err};
     if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args,
-                                                                0, s),
+                                                                ssmem, s),
                                 "tile_solve_kernel"))
         return rc;
     ctx->launches++;
@@ -654,12 +842,7 @@ int solve_static_t(const T* LU, int64_t n, int64_t lda, const int32_t* piv, cons
     int* flags = sc->flags;
     int32_t* err = sc->err;
     double* x = sc->x;
-    if (cudaFuncSetAttribute(tile_piv_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(n * sizeof(int32_t))) != cudaSuccess) {
-        cudaGetLastError();
-        return BEM_ERR_CUDA;
-    }
-    tile_piv_to_perm_kernel<<<1, 256, n * sizeof(int32_t), s>>>(piv, perm, (int)n);
+    tile_piv_to_perm_kernel<<<(unsigned)((nbk + 127) / 128), 128, 0, s>>>(piv, perm, (int)n);
     permute_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, perm, x, (int)n, W);
     // the array keeps the previous call's contents: the flags and the error
     // word must start at zero
@@ -668,12 +851,18 @@ int solve_static_t(const T* LU, int64_t n, int64_t lda, const int32_t* piv, cons
         cudaGetLastError();
         return BEM_ERR_CUDA;
     }
+    const size_t ssmem = solve_smem_bytes(sizeof(CE<T>));
+    if (cudaFuncSetAttribute(tile_solve_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, ssmem);
     int P = std::max(1, std::min(nbk, std::min(per_sm * sms, sms)));
     int ni = (int)n, epoch = 1;
     void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err};
-    if (cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args, 0, s) != cudaSuccess) {
+    if (cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args, ssmem, s) != cudaSuccess) {
         cudaGetLastError();
         return BEM_ERR_CUDA;
     }
