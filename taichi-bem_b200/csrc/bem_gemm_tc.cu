@@ -101,6 +101,8 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.y * TC_BM;
     const int n0 = blockIdx.x * TC_BN;
+    // rows of A can be read as float4 when the base and the row stride are 16-byte aligned
+    const bool a_vec = ((reinterpret_cast<uintptr_t>(Am) & 15) == 0) && ((ldf & 3) == 0);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
@@ -120,6 +122,55 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
     const uint32_t tmem = tmem_slot;
 
     const int nchunks = (k_real + TC_KC - 1) / TC_KC;
+    // Software pipeline: the global loads of chunk c+1 are issued into
+    // registers right after chunk c is stored, so their latency overlaps the
+    // MMAs of chunk c and the wait for the stage to be free again.
+    constexpr int UPT = TC_BM * TC_KC / 4 / TC_THREADS;  // staging units per thread
+    float ra[UPT][4], rb[UPT][4];
+    auto load_chunk = [&](int c) {
+        const int kc = c * TC_KC;
+#pragma unroll
+        for (int h = 0; h < UPT; ++h) {
+            const int u = tid + h * TC_THREADS;
+            const int r = 8 * (u / (2 * TC_KC)) + (u & 7), k4 = (u >> 3) % (TC_KC / 4);
+            const int kk0 = kc + 4 * k4;
+            const bool rowok = m0 + r < m;
+            const float* arow = Am + (int64_t)(m0 + r) * ldf + kk0;
+            if (rowok && kk0 + 3 < k_real && a_vec) {
+                const float4 v = *reinterpret_cast<const float4*>(arow);
+                ra[h][0] = v.x;
+                ra[h][1] = v.y;
+                ra[h][2] = v.z;
+                ra[h][3] = v.w;
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) ra[h][i] = (rowok && kk0 + i < k_real) ? arow[i] : 0.f;
+            }
+            if (!cplx) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int kk = kk0 + i;
+                    rb[h][i] = (n0 + r < n_real && kk < k_real) ? Bm[(int64_t)kk * ldf + n0 + r] : 0.f;
+                }
+            } else {
+                // complex rows q0, q0+1 of column col: (re, im) of each
+                const int jc = r >> 1;
+                const int q0 = kc / 2 + 2 * k4, col = n0 / 2 + jc;
+                rb[h][0] = rb[h][1] = rb[h][2] = rb[h][3] = 0.f;
+                if (2 * col < n_real) {
+                    if (2 * q0 < k_real) {
+                        rb[h][0] = Bm[(int64_t)q0 * ldf + 2 * col];
+                        rb[h][1] = Bm[(int64_t)q0 * ldf + 2 * col + 1];
+                    }
+                    if (2 * (q0 + 1) < k_real) {
+                        rb[h][2] = Bm[(int64_t)(q0 + 1) * ldf + 2 * col];
+                        rb[h][3] = Bm[(int64_t)(q0 + 1) * ldf + 2 * col + 1];
+                    }
+                }
+            }
+        }
+    };
+    if (nchunks > 0) load_chunk(0);
     for (int c = 0; c < nchunks; ++c) {
         const int stage = c & 1;
         unsigned char* st = smem + stage * TC_STAGE_BYTES;
@@ -129,55 +180,31 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
         }
         __syncthreads();
         if (s_abort) break;
-        const int kc = c * TC_KC;
         // Staging: thread unit u owns one 16-byte core-matrix row, (row
         // 8*(u/(2*TC_KC)) + u%8, k-quad (u/8)%(TC_KC/4)), which sits at byte
         // 16*u of the tile, so a warp's shared-memory stores are contiguous.
-        for (int u = tid; u < TC_BM * TC_KC / 4; u += TC_THREADS) {
-            const int r = 8 * (u / (2 * TC_KC)) + (u & 7), k4 = (u >> 3) % (TC_KC / 4);
-            // A: rows of the real view, 4 consecutive k
-            float4 hi, lo;
-            float va[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int kk = kc + 4 * k4 + i;
-                va[i] = (m0 + r < m && kk < k_real) ? Am[(int64_t)(m0 + r) * ldf + kk] : 0.f;
-            }
-            split_tf32(va[0], hi.x, lo.x);
-            split_tf32(va[1], hi.y, lo.y);
-            split_tf32(va[2], hi.z, lo.z);
-            split_tf32(va[3], hi.w, lo.w);
+        for (int h = 0; h < UPT; ++h) {
+            const int u = tid + h * TC_THREADS;
+            float4 hi, lo;
+            split_tf32(ra[h][0], hi.x, lo.x);
+            split_tf32(ra[h][1], hi.y, lo.y);
+            split_tf32(ra[h][2], hi.z, lo.z);
+            split_tf32(ra[h][3], hi.w, lo.w);
             *reinterpret_cast<float4*>(st + 16 * u) = hi;
             *reinterpret_cast<float4*>(st + TC_TILE_BYTES + 16 * u) = lo;
-            // B (stored K-major: row = output column j), 4 consecutive k
+            // B stored K-major (row = output column); complex B expanded into
+            // the real column 2*jc+s of [[re, im], [-im, re]] blocks
             float vb[4];
             if (!cplx) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int kk = kc + 4 * k4 + i;
-                    vb[i] = (n0 + r < n_real && kk < k_real) ? Bm[(int64_t)kk * ldf + n0 + r] : 0.f;
-                }
+                vb[0] = rb[h][0];
+                vb[1] = rb[h][1];
+                vb[2] = rb[h][2];
+                vb[3] = rb[h][3];
+            } else if (((8 * (u / (2 * TC_KC)) + (u & 7)) & 1) == 0) {
+                vb[0] = rb[h][0]; vb[1] = -rb[h][1]; vb[2] = rb[h][2]; vb[3] = -rb[h][3];
             } else {
-                // real column 2*jc+s of the expanded B; its 4 rows are the two
-                // complex rows q0, q0+1 (real rows 2q+t, t = 0, 1)
-                const int jc = r >> 1, sidx = r & 1;
-                const int q0 = kc / 2 + 2 * k4, col = n0 / 2 + jc;
-                float b0r = 0.f, b0i = 0.f, b1r = 0.f, b1i = 0.f;
-                if (2 * col < n_real) {
-                    if (2 * q0 < k_real) {
-                        b0r = Bm[(int64_t)q0 * ldf + 2 * col];
-                        b0i = Bm[(int64_t)q0 * ldf + 2 * col + 1];
-                    }
-                    if (2 * (q0 + 1) < k_real) {
-                        b1r = Bm[(int64_t)(q0 + 1) * ldf + 2 * col];
-                        b1i = Bm[(int64_t)(q0 + 1) * ldf + 2 * col + 1];
-                    }
-                }
-                if (sidx == 0) {
-                    vb[0] = b0r; vb[1] = -b0i; vb[2] = b1r; vb[3] = -b1i;
-                } else {
-                    vb[0] = b0i; vb[1] = b0r; vb[2] = b1i; vb[3] = b1r;
-                }
+                vb[0] = rb[h][1]; vb[1] = rb[h][0]; vb[2] = rb[h][3]; vb[3] = rb[h][2];
             }
             split_tf32(vb[0], hi.x, lo.x);
             split_tf32(vb[1], hi.y, lo.y);
@@ -186,6 +213,7 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
             *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + 16 * u) = hi;
             *reinterpret_cast<float4*>(st + 3 * TC_TILE_BYTES + 16 * u) = lo;
         }
+        if (c + 1 < nchunks) load_chunk(c + 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {

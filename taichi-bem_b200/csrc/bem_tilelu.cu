@@ -70,7 +70,7 @@ __device__ __forceinline__ CE<T> cinv(CE<T> a) {
 // counts as 0.
 template <typename T>
 __device__ __forceinline__ unsigned long long pivot_key(CE<T> v, int r) {
-    float a = (float)(fabs((double)v.re) + fabs((double)v.im));
+    float a = (float)(fabs(v.re) + fabs(v.im));
     if (!(a == a)) a = 0.0f;
     return ((unsigned long long)__float_as_uint(a) << 32) | (unsigned)(LU_T - 1 - r);
 }
@@ -82,9 +82,12 @@ constexpr size_t diag_smem_bytes(size_t elem) { return elem * (LU_T * DIAG_LD + 
 // One CTA of 256 threads factors the 64x64 diagonal tile (GEPP restricted to
 // the tile's rows) and forms the explicit inverses.  Blocked by panels of
 // DIAG_PW columns:
-//   panel  : warp 0 alone, warp-synchronous (no CTA barrier per column): pivot
-//            search by a warp max over packed keys, full-row swap, multipliers
-//            and the update inside the panel;
+//   panel  : the 64 x DIAG_PW panel in registers (two elements per thread);
+//            per column a pivot max over packed keys (shuffles, then across
+//            the 8 warps), the pivot row exchanged through shared memory,
+//            multipliers shuffled within each row's four threads; two CTA
+//            barriers per column; the panel's row swaps are applied to the
+//            other columns once the panel is done;
 //   U12    : the panel's rows right of it, L11^{-1} applied by substitution
 //            (one thread per column);
 //   update : rank-DIAG_PW update of the trailing block, one column per thread
@@ -100,6 +103,9 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
     CE<T>* S = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][DIAG_LD]
     CE<T>* X = S + LU_T * DIAG_LD;                  // [LU_T][LU_T] inverse being built
     __shared__ int s_zero_pivot;                    // first zero pivot of this tile (1-based), 0 = none
+    __shared__ unsigned long long s_wkey[8];        // per-warp pivot keys
+    __shared__ CE<T> s_rowj[DIAG_PW], s_rowp[DIAG_PW];
+    __shared__ int s_perm[DIAG_PW];                 // pivot rows of the current panel
     const int m = min(LU_T, n - k0);
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     if (tid == 0) s_zero_pivot = 0;
@@ -110,48 +116,92 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
         S[r * DIAG_LD + c] = v;
     }
     __syncthreads();
+    // panel registers: thread t holds row pr = t >> 2, panel columns 2*pc, 2*pc+1 (pc = t & 3)
+    const int pr = tid >> 2, pc = tid & 3;
     for (int j0 = 0; j0 < m; j0 += DIAG_PW) {
         const int w = min(DIAG_PW, m - j0);
-        if (wid == 0) {
-            for (int j = j0; j < j0 + w; ++j) {
-                // pivot: largest |re| + |im| in column j among rows j..m-1, first one on ties
-                unsigned long long key = 0ull;
-                for (int r = j + lane; r < m; r += 32) {
-                    const unsigned long long kr = pivot_key(S[r * DIAG_LD + j], r);
-                    key = kr > key ? kr : key;
+        CE<T> e0 = S[pr * DIAG_LD + j0 + 2 * pc], e1 = S[pr * DIAG_LD + j0 + 2 * pc + 1];
+        for (int j = j0; j < j0 + w; ++j) {
+            const int jq = j - j0;  // panel column of j, held by threads with pc == jq / 2
+            // pivot: largest |re| + |im| in column j among rows j..m-1 (first one on ties):
+            // owners post keys, max over the warp's rows, then over the 8 warps
+            unsigned long long key = 0ull;
+            if (pc == (jq >> 1) && pr >= j && pr < m) key = pivot_key((jq & 1) ? e1 : e0, pr);
+#pragma unroll
+            for (int o = 4; o < 32; o <<= 1) {
+                const unsigned long long ko = __shfl_xor_sync(0xffffffffu, key, o);
+                key = ko > key ? ko : key;
+            }
+            if (lane == (jq >> 1)) s_wkey[wid] = key;
+            __syncthreads();
+            unsigned long long best = s_wkey[0];
+#pragma unroll
+            for (int q = 1; q < 8; ++q) best = s_wkey[q] > best ? s_wkey[q] : best;
+            const int p = LU_T - 1 - (int)(best & 0xffffffffull);
+            const int prow = (p >= j && p < m) ? p : j;  // all-zero or NaN column: no swap
+            // exchange rows j and prow inside the panel; everyone reads the new pivot row
+            if (pr == j) {
+                s_rowj[2 * pc] = e0;
+                s_rowj[2 * pc + 1] = e1;
+            }
+            if (pr == prow) {
+                s_rowp[2 * pc] = e0;
+                s_rowp[2 * pc + 1] = e1;
+            }
+            __syncthreads();
+            if (prow != j) {
+                if (pr == j) {
+                    e0 = s_rowp[2 * pc];
+                    e1 = s_rowp[2 * pc + 1];
+                } else if (pr == prow) {
+                    e0 = s_rowj[2 * pc];
+                    e1 = s_rowj[2 * pc + 1];
                 }
-                for (int o = 16; o > 0; o >>= 1) {
-                    const unsigned long long ko = __shfl_xor_sync(0xffffffffu, key, o);
-                    key = ko > key ? ko : key;
+            }
+            const CE<T> pv = s_rowp[jq];
+            if (tid == 0) {
+                s_perm[jq] = prow;
+                piv[k0 + j] = k0 + prow;
+                if (!((double)pv.re != 0.0 || (double)pv.im != 0.0) && s_zero_pivot == 0) s_zero_pivot = k0 + j + 1;
+            }
+            // multiplier of row pr (held by the thread of column j), shared within the row's 4 lanes
+            CE<T> l = CE<T>{T(0), T(0)};
+            if (pc == (jq >> 1)) l = cmul((jq & 1) ? e1 : e0, cinv(pv));
+            const int src = (lane & ~3) | (jq >> 1);
+            l.re = __shfl_sync(0xffffffffu, l.re, src);
+            l.im = __shfl_sync(0xffffffffu, l.im, src);
+            if (pr > j && pr < m) {
+                const int c0 = j0 + 2 * pc, c1e = c0 + 1;
+                if (c0 == j) {
+                    e0 = l;
+                } else if (c0 > j && c0 < j0 + w) {
+                    const CE<T> u = s_rowp[2 * pc];
+                    e0.re -= l.re * u.re - l.im * u.im;
+                    e0.im -= l.re * u.im + l.im * u.re;
                 }
-                const int p = LU_T - 1 - (int)(key & 0xffffffffull);
-                const int pr = (p >= j && p < m) ? p : j;  // all-zero or NaN column: no swap
-                if (pr != j)
-                    for (int c = lane; c < LU_T; c += 32) {
-                        const CE<T> t = S[j * DIAG_LD + c];
-                        S[j * DIAG_LD + c] = S[pr * DIAG_LD + c];
-                        S[pr * DIAG_LD + c] = t;
-                    }
-                __syncwarp();
-                const CE<T> pv = S[j * DIAG_LD + j];
-                if (lane == 0) {
-                    piv[k0 + j] = k0 + pr;
-                    if (!((double)pv.re != 0.0 || (double)pv.im != 0.0) && s_zero_pivot == 0)
-                        s_zero_pivot = k0 + j + 1;
+                if (c1e == j) {
+                    e1 = l;
+                } else if (c1e > j && c1e < j0 + w) {
+                    const CE<T> u = s_rowp[2 * pc + 1];
+                    e1.re -= l.re * u.re - l.im * u.im;
+                    e1.im -= l.re * u.im + l.im * u.re;
                 }
-                const CE<T> ip = cinv(pv);
-                for (int r = j + 1 + lane; r < m; r += 32) {
-                    const CE<T> l = cmul(S[r * DIAG_LD + j], ip);
-                    S[r * DIAG_LD + j] = l;
-                    for (int c = j + 1; c < j0 + w; ++c) {
-                        const CE<T> u = S[j * DIAG_LD + c];
-                        CE<T> v = S[r * DIAG_LD + c];
-                        v.re -= l.re * u.re - l.im * u.im;
-                        v.im -= l.re * u.im + l.im * u.re;
-                        S[r * DIAG_LD + c] = v;
-                    }
+            }
+            __syncthreads();  // s_rowj / s_rowp / s_wkey are reused by the next column
+        }
+        // panel back to shared memory; the panel's swaps applied to the other columns
+        if (pr < m) {
+            if (2 * pc < w) S[pr * DIAG_LD + j0 + 2 * pc] = e0;
+            if (2 * pc + 1 < w) S[pr * DIAG_LD + j0 + 2 * pc + 1] = e1;
+        }
+        if (tid < LU_T && (tid < j0 || tid >= j0 + w)) {
+            for (int q = 0; q < w; ++q) {
+                const int ra = j0 + q, rb = s_perm[q];
+                if (rb != ra) {
+                    const CE<T> t = S[ra * DIAG_LD + tid];
+                    S[ra * DIAG_LD + tid] = S[rb * DIAG_LD + tid];
+                    S[rb * DIAG_LD + tid] = t;
                 }
-                __syncwarp();
             }
         }
         __syncthreads();
@@ -202,6 +252,8 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
     // Uinv: for row block i (descending): X_i = U_ii^{-1} (E_i - sum_{k>i} U_ik X_k)
     // thread: column c = tid & 63, rows (tid >> 6) * 2 + {0, 1} of the block
     CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T;
+    __shared__ CE<T> s_rdiag[LU_T];  // 1 / U[r][r], formed in parallel off the substitution chain
+    if (tid < LU_T) s_rdiag[tid] = tid < m ? cinv(S[tid * DIAG_LD + tid]) : CE<T>{T(1), T(0)};
     const int c = tid & 63, rq = (tid >> 6) * 2;
     for (int which = 0; which < 2; ++which) {
         for (int bs = 0; bs < LU_T / DIAG_PW; ++bs) {
@@ -269,7 +321,7 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
                             y[i].re -= uu.re * y[q].re - uu.im * y[q].im;
                             y[i].im -= uu.re * y[q].im + uu.im * y[q].re;
                         }
-                        y[i] = cmul(y[i], cinv(S[r * DIAG_LD + r]));
+                        y[i] = cmul(y[i], s_rdiag[r]);
                     }
                 }
 #pragma unroll
@@ -301,31 +353,40 @@ __global__ void tile_laswp_kernel(T* A, int64_t lda, int n, int k0, int m, const
     }
 }
 
-// mode 0: U12 tile (rows k0.., 64 columns) <- Linv * tile
-// mode 1: L21 tile (64 rows, columns k0..) <- tile * Uinv
+// blockIdx.y = 0: U12 tile (rows k0.., 64 columns) <- Linv * tile
+// blockIdx.y = 1: L21 tile (64 rows, columns k0..) <- tile * Uinv
+// Both products run in one launch (they touch disjoint parts of A).  Thread
+// (tx, ty) owns outputs rows ty + 16 i, columns tx + 16 j: the column operand
+// is read as 16 consecutive elements per half-warp and the row operand from a
+// padded row stride, so the shared-memory reads are free of bank conflicts.
+constexpr int APPLY_LD = LU_T + 1;
+constexpr size_t apply_smem_bytes(size_t elem) { return 2 * elem * LU_T * APPLY_LD; }
+
 template <typename T, bool C>
-__global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int n, int k0, int m, const CE<T>* dinv,
-                                                         int mode) {
+__global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int n, int k0, int m,
+                                                         const CE<T>* dinv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    CE<T>* M = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][LU_T] inverse
-    CE<T>* X = M + LU_T * LU_T;                     // [LU_T][LU_T] tile
+    CE<T>* M = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][APPLY_LD] inverse
+    CE<T>* X = M + LU_T * APPLY_LD;                 // [LU_T][APPLY_LD] tile
+    const int mode = blockIdx.y;
     const CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T + (mode == 0 ? 0 : LU_T * LU_T);
     const int base = k0 + m + blockIdx.x * LU_T;  // first column (mode 0) / row (mode 1) of the tile
     const int cnt = min(LU_T, n - base);
     for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
-        M[e] = D[e];
-        int r = e / LU_T, c = e - r * LU_T;
+        const int r = e / LU_T, c = e - r * LU_T;
+        M[r * APPLY_LD + c] = D[e];
         CE<T> v = CE<T>{T(0), T(0)};
         if (mode == 0) {
             if (r < m && c < cnt) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + base + c);
         } else {
             if (r < cnt && c < m) v = ldE<T, C>(A, (int64_t)(base + r) * lda + k0 + c);
         }
-        X[e] = v;
+        X[r * APPLY_LD + c] = v;
     }
     __syncthreads();
-    // each thread: 16 outputs (4 rows x 4 columns)
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const CE<T>* Rop = mode == 0 ? M : X;  // row operand (left factor)
+    const CE<T>* Cop = mode == 0 ? X : M;  // column operand (right factor)
     CE<T> acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -335,8 +396,8 @@ __global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int 
         CE<T> a[4], b[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            a[i] = mode == 0 ? M[(ty * 4 + i) * LU_T + q] : X[(ty * 4 + i) * LU_T + q];
-            b[i] = mode == 0 ? X[q * LU_T + tx * 4 + i] : M[q * LU_T + tx * 4 + i];
+            a[i] = Rop[(ty + 16 * i) * APPLY_LD + q];
+            b[i] = Cop[q * APPLY_LD + tx + 16 * i];
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -350,7 +411,7 @@ __global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int 
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            int r = ty * 4 + i, c = tx * 4 + j;
+            const int r = ty + 16 * i, c = tx + 16 * j;
             if (mode == 0) {
                 if (r < m && c < cnt) stE<T, C>(A, (int64_t)(k0 + r) * lda + base + c, acc[i][j]);
             } else {
@@ -633,46 +694,66 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
              cudaStream_t s) {
     cudaMemsetAsync(info, 0, sizeof(int32_t), s);
     const size_t dsmem = diag_smem_bytes(sizeof(CE<T>));
-    const size_t asmem = sizeof(CE<T>) * 2 * LU_T * LU_T;
+    const size_t asmem = apply_smem_bytes(sizeof(CE<T>));
     cudaFuncSetAttribute(tile_diag_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem);
     cudaFuncSetAttribute(tile_apply_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem);
     if (int rc = bem_lookahead_stream(ctx)) return rc;
     const int ni = (int)n;
     const int W = C ? 2 : 1;
-    // Lookahead: step k updates the next tile column first; the diagonal tile
-    // k+1 is then factored on the high-priority side stream while the rest
-    // of step k's trailing update runs (its CTAs take the first free SM).
-    tile_diag_kernel<T, C><<<1, 256, dsmem, s>>>(A, lda, ni, 0, piv, dinv, info);
-    ctx->launches++;
-    bool diag_on_aux = false;
-    for (int64_t k0 = 0; k0 < n; k0 += LU_T) {
-        const int m = (int)std::min<int64_t>(LU_T, n - k0);
-        const int k0i = (int)k0;
-        if (diag_on_aux) cudaStreamWaitEvent(s, ctx->ev_diag, 0);
-        tile_laswp_kernel<T, C><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, lda, ni, k0i, m, piv);
+    auto at = [&](int64_t r, int64_t c) { return A + W * (r * lda + c); };
+    // A[r0:r0+rows, c0:c0+cols] -= A[r0:r0+rows, q0:q0+kk] A[q0:q0+kk, c0:c0+cols]
+    auto update = [&](int64_t r0, int64_t c0, int64_t rows, int64_t cols, int64_t q0, int64_t kk) -> int {
+        if (rows <= 0 || cols <= 0 || kk <= 0) return BEM_OK;
+        return bem_gemm_update<T, C>(ctx, at(r0, c0), at(r0, q0), at(q0, c0), rows, cols, kk, lda, s);
+    };
+    // diagonal tile at k0 on the high-priority side stream, after the work queued on s so far
+    auto diag_aside = [&](int64_t k0) {
+        cudaEventRecord(ctx->ev_next, s);
+        cudaStreamWaitEvent(ctx->aux, ctx->ev_next, 0);
+        tile_diag_kernel<T, C><<<1, 256, dsmem, ctx->aux>>>(A, lda, ni, (int)k0, piv, dinv, info);
+        cudaEventRecord(ctx->ev_diag, ctx->aux);
+        ctx->launches++;
+    };
+    // row swaps of tile k0 outside it, then U12 = Linv A12 and L21 = A21 Uinv
+    auto panel = [&](int64_t k0, int m) {
+        tile_laswp_kernel<T, C><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, lda, ni, (int)k0, m, piv);
         ctx->launches++;
         const int64_t rest = n - k0 - m;
         if (rest > 0) {
             const unsigned tiles = (unsigned)((rest + LU_T - 1) / LU_T);
-            tile_apply_kernel<T, C><<<tiles, 256, asmem, s>>>(A, lda, ni, k0i, m, dinv, 0);
-            tile_apply_kernel<T, C><<<tiles, 256, asmem, s>>>(A, lda, ni, k0i, m, dinv, 1);
-            ctx->launches += 2;
-            T* A22 = A + W * ((k0 + m) * lda + k0 + m);
-            const T* L21 = A + W * ((k0 + m) * lda + k0);
-            const T* U12 = A + W * (k0 * lda + k0 + m);
-            const int64_t next = std::min<int64_t>(LU_T, rest);
-            if (int rc = bem_gemm_update<T, C>(ctx, A22, L21, U12, rest, next, m, lda, s)) return rc;
-            cudaEventRecord(ctx->ev_next, s);
-            cudaStreamWaitEvent(ctx->aux, ctx->ev_next, 0);
-            tile_diag_kernel<T, C><<<1, 256, dsmem, ctx->aux>>>(A, lda, ni, k0i + m, piv, dinv, info);
-            cudaEventRecord(ctx->ev_diag, ctx->aux);
+            tile_apply_kernel<T, C><<<dim3(tiles, 2), 256, asmem, s>>>(A, lda, ni, (int)k0, m, dinv);
             ctx->launches++;
-            diag_on_aux = true;
-            if (rest > next)
-                if (int rc = bem_gemm_update<T, C>(ctx, A22 + W * next, L21, U12 + W * next, rest, rest - next, m,
-                                                   lda, s))
-                    return rc;
         }
+    };
+    // Tiles are taken in pairs (k, k+1) with a delayed update: step k updates
+    // only tile k+1's column block (so its diagonal factorisation can start on
+    // the side stream) and tile k+1's rows right of it; the trailing block then
+    // receives steps k and k+1 together as one rank-128 update (K = 128 halves
+    // the read-modify-write traffic of the trailing GEMMs).  The update's first
+    // tile column goes first so that the next pair's diagonal tile overlaps the
+    // rest of it.
+    tile_diag_kernel<T, C><<<1, 256, dsmem, s>>>(A, lda, ni, 0, piv, dinv, info);
+    ctx->launches++;
+    bool on_aux = false;
+    for (int64_t k0 = 0; k0 < n; k0 += 2 * LU_T) {
+        const int m1 = (int)std::min<int64_t>(LU_T, n - k0);
+        if (on_aux) cudaStreamWaitEvent(s, ctx->ev_diag, 0);
+        panel(k0, m1);
+        const int64_t k1 = k0 + m1, rest1 = n - k1;
+        if (rest1 <= 0) break;
+        const int m2 = (int)std::min<int64_t>(LU_T, rest1);
+        if (int rc = update(k1, k1, rest1, m2, k0, m1)) return rc;
+        diag_aside(k1);
+        on_aux = true;
+        const int64_t c2 = k1 + m2, rest2 = n - c2;
+        if (int rc = update(k1, c2, m2, rest2, k0, m1)) return rc;
+        cudaStreamWaitEvent(s, ctx->ev_diag, 0);
+        panel(k1, m2);
+        if (rest2 <= 0) break;
+        const int64_t next = std::min<int64_t>(LU_T, rest2);
+        if (int rc = update(c2, c2, rest2, next, k0, (int64_t)m1 + m2)) return rc;
+        diag_aside(c2);
+        if (int rc = update(c2, c2 + next, rest2, rest2 - next, k0, (int64_t)m1 + m2)) return rc;
         if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "tiled lu step")) return rc;
     }
     // the tensor-core update records a bounded-wait timeout in flags[4]
