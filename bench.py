@@ -39,11 +39,19 @@ for _p in (ROOT, os.path.join(ROOT, "taichi-bem_b200")):
 
 METRIC = "assembly entries/s + time-to-solution at ≤1e-6 rel err: mixed/batched vs plain GPU"
 WORKLOAD = "Helmholtz 3D interior Dirichlet k=3, icosphere s4 (5120 panels), GaussQR=5, plane wave"
-# Algorithmic FP32 operations per separate-pair kernel evaluation of the
-# Helmholtz single layer (far_kernel): 3 (x-y) + 5 (r^2) + 1 (r) + 1 (kr)
-# + 2 (e^{ikr}/r) + 4 (two weighted accumulations) = 16, plus rsqrt, sin, cos
-# counted as one operation each = 19.
-OPS_PER_EVAL = 19
+# Algorithmic FP32 flops (an FMA counts 2) per kernel evaluation of the fused
+# symmetric Helmholtz sweep (far_vkg_sym_kernel), counted once from its source:
+# offsets 3, s = e.(2D+e) 8, r^2 1, r and 1/r with the Newton step 9, d.n_j 6,
+# split phase 3, weights 5, k r 1, sine/cosine polynomials 20, (1-ikr) e^{ikr} 4,
+# V_ij and (K g)_i accumulation 8, (K g)_j term 10 = 78, plus two MUFU
+# operations (reciprocal square root, reciprocal).  One evaluation serves V_ij,
+# V_ji, (K g)_i and (K g)_j, so the sweep evaluates each unordered separate
+# pair once.
+FLOPS_PER_EVAL = 78
+MUFU_PER_EVAL = 2
+# dram__bytes_read.sum + dram__bytes_write.sum of far_vkg_sym_kernel on this
+# workload (424.3 MB + 380.5 MB, profiles/far_vkg_sym_helmholtz_s4.md)
+FAR_SWEEP_DRAM_BYTES = 804.8e6
 
 
 def _dist():
@@ -284,13 +292,15 @@ def main():
     torch.cuda.synchronize()
     launches = eng.launches - launches0
     step_ms = [a.elapsed_time(z) for a, z in ev]
-    # V assembly alone (the dominant kernel) for the roofline
+    # the dominant kernel of the step, the fused far-field sweep, through its
+    # C-ABI call (bem_assemble_dirichlet, which also launches the FP64
+    # near-pair kernels on the same stream), for the roofline
     va = []
     for s in range(args.steps):
         flush_l2()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        b.single_layer.forward(b._scope_type, b._k, 1.0)
+        b.fused_assembly_call()
         e1.record()
         torch.cuda.synchronize()
         va.append(e0.elapsed_time(e1))
@@ -319,11 +329,14 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         ms64.append(e0.elapsed_time(e1))
+    # the same assembly work on the plain path: V (one kernel per operator)
+    # and the right-hand side 1/2 M g + K g (matrix-free)
     va64 = []
     for _ in range(2):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         b64.single_layer.forward(b64._scope_type, b64._k, 1.0)
+        b64.rhs_layer_forward(k=b64._k, scope_type=b64._scope_type)
         e1.record()
         torch.cuda.synchronize()
         va64.append(e0.elapsed_time(e1))
@@ -355,18 +368,21 @@ def main():
         c2.kill()
     e2e = statistics.mean(e2e_ms[1:]) if len(e2e_ms) > 1 else e2e_ms[0]
 
-    # roofline of the dominant kernel: V far field (FP32) in assembly
+    # roofline of the dominant kernel: the fused symmetric far-field sweep
     q4 = 625
     near = eng.near_pairs
-    evals = (nt * nt - near) * q4
+    evals = (nt * nt - near) // 2 * q4  # unordered separate pairs x GaussQR^4
     va_ms = statistics.mean(va)
-    achieved = evals * OPS_PER_EVAL / (va_ms * 1e-3) / 1e12
+    achieved = evals * FLOPS_PER_EVAL / (va_ms * 1e-3) / 1e12
     roof = {"bound": "fp32", "achieved": achieved, "peak": peaks[0], "unit": "TFLOP/s",
-            "frac": achieved / peaks[0], "traffic": None,
-            "kernel": "far_kernel<V, Helmholtz, P0, P0, float> (+ near_kernel FP64)",
+            "frac": achieved / peaks[0],
+            # DRAM read + write of one far_vkg_sym_kernel launch of this workload, one ncu capture
+            "traffic": FAR_SWEEP_DRAM_BYTES,
+            "kernel": "far_vkg_sym_kernel<Helmholtz, float> (timed with its FP64 near-pair kernels in one call)",
             "peak_source": "bem_measure_peaks FP32 FMA probe on this GPU (MEASURED_PEAKS.json has HBM and bf16 only)",
-            "ops_per_eval": OPS_PER_EVAL, "evals_per_launch": evals, "assembly_ms": va_ms,
-            "mufu_peak_gops": peaks[2], "fp64_peak_tflops": peaks[1]}
+            "flops_per_eval": FLOPS_PER_EVAL, "evals_per_launch": evals, "call_ms": va_ms,
+            "mufu": {"achieved_gops": evals * MUFU_PER_EVAL / (va_ms * 1e-3) / 1e9, "peak_gops": peaks[2]},
+            "fp64_peak_tflops": peaks[1]}
 
     cpu = None
     if rank == 0 and ws == 1:
@@ -388,9 +404,12 @@ def main():
                        "parallelism": f"replicas x{ws}"},
             "time_to_solution_ms": ms,
             "assembly_entries_per_s": entries / (va_ms * 1e-3),
+            "assembly_ms": va_ms,
+            "assembly": "V and K g in one symmetric FP32 far sweep + FP64 near pairs",
             "plain_fp64": {"time_to_solution_ms": statistics.mean(ms64),
                            "assembly_entries_per_s": entries / (statistics.mean(va64) * 1e-3),
-                           "assembly_ms": statistics.mean(va64)},
+                           "assembly_ms": statistics.mean(va64),
+                           "assembly": "V (FP64, all ordered pairs) + matrix-free 1/2 M g + K g"},
             "speedup_vs_plain_fp64": statistics.mean(ms64) / ms,
             "rel_err_vs_fp64": {"max_abs_rel": rel, "l2_rel": rel2},
             "refinement": {k: (v if not hasattr(v, "item") else v.item()) for k, v in info.items()},

@@ -407,17 +407,24 @@ class BEMManager:
         else:
             lay._Vmat.zero_()
         rc._rhs_vec.zero_()
+        self.fused_assembly_call()
+        half = 0.5 if self._scope_type == int(ScopeType.INTERIOR) else -0.5
+        rc.multiply_identity_to_vector(multiplier=half)
+        self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)
+        self.assemble_rhs()
+
+    def fused_assembly_call(self):
+        """The one C-ABI call of the fused Dirichlet pass: V (far pairs in
+        the symmetric sweep, near pairs in FP64) accumulated into the V block
+        and K g into the right-hand side (both must be zeroed by the caller)."""
+        rc = self.rhs_constructor
         sp = self.space("charge", self.shape_func_degree_Neumann, "N", int(CellFluxType.NEUMANN_TOBESOLVED))
         rows = self.space("charge", self.shape_func_degree_Neumann, "N", int(CellFluxType.NEUMANN_TOBESOLVED),
                           offset=self._Neumann_offset_i)
         data = self.space("data", self.shape_func_degree_Dirichlet, "N")
         desc = self.op_desc(L.OP_V, self._k, 1.0)
-        self.engine.assemble_dirichlet(desc, sp, sp, lay._Vmat, rows, data, rc._Dirichlet_boundary, rc._rhs_vec,
-                                       scale=1.0, scale_k=1.0, conj_g=self.conj_data)
-        half = 0.5 if self._scope_type == int(ScopeType.INTERIOR) else -0.5
-        rc.multiply_identity_to_vector(multiplier=half)
-        self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)
-        self.assemble_rhs()
+        self.engine.assemble_dirichlet(desc, sp, sp, self.single_layer._Vmat, rows, data, rc._Dirichlet_boundary,
+                                       rc._rhs_vec, scale=1.0, scale_k=1.0, conj_g=self.conj_data)
 
     def run(self):
         """BEMManager.run (BEM_manager.py:990-1030) without the GUI colouring."""
