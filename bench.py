@@ -212,6 +212,47 @@ def profile_step(precision: str):
     core.kill()
 
 
+def sweep_bench(n_k: int):
+    """Config 3: the wavenumber sweep (managers/sweep.py) of the augmented
+    transmission operator, mixed precision against the plain FP64 path; one
+    JSON line with per-k times, errors and the norm estimates."""
+    import torch
+    from bem_b200.managers import CoreManager
+    from bem_b200.managers.sweep import wavenumber_sweep
+    from bem_b200.workloads import config3
+    res = {}
+    for prec in ("mixed", "fp64"):
+        params, fD, fN, ks = config3(prec, n_k)
+        core = CoreManager(params)
+        core.initialization(fD, fN)
+        # mixed: Krylov norm estimates; plain: the reference's own full SVD per k
+        kw = dict(nrhs=4, seed=0, norm_tol=1e-8, norm_method="iterative" if prec == "mixed" else "svd")
+        wavenumber_sweep(core._BEM_manager, ks[:1], **kw)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res[prec] = wavenumber_sweep(core._BEM_manager, ks, **kw)
+        torch.cuda.synchronize()
+        res[prec]["total_s"] = time.perf_counter() - t0
+        core.kill()
+    errs = [float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+            for a, b in zip(res["mixed"]["solutions"], res["fp64"]["solutions"])]
+    nerr = [abs(a - b) / b for a, b in zip(res["mixed"]["inv_norm"], res["fp64"]["inv_norm"])]
+    print(json.dumps({
+        "workload": "config 3: augmented transmission sweep, icosphere s4, P1/P1 (5124 unknowns), GaussQR=3, "
+                    "n_i=3, n_o=1, 4 complex Gaussian RHS per k",
+        "n_k": len(res["mixed"]["k"]), "k_range": [res["mixed"]["k"][0], res["mixed"]["k"][-1]],
+        "mixed_s": res["mixed"]["total_s"], "plain_fp64_s": res["fp64"]["total_s"],
+        "speedup": res["fp64"]["total_s"] / res["mixed"]["total_s"],
+        "ms_per_k_mixed": statistics.mean(res["mixed"]["ms"]), "ms_per_k_fp64": statistics.mean(res["fp64"]["ms"]),
+        "solution_rel_err_max": max(errs), "inv_norm_rel_diff_max": max(nerr),
+        "inv_norm": res["mixed"]["inv_norm"], "cond": res["mixed"]["cond"],
+        "norm_method": {"mixed": "block Krylov of (S^H S)^{-1} (8-vector blocks, FP64 LU solves) and of S^H S, "
+                                 "Rayleigh-Ritz, stop at 1e-8 relative change",
+                        "plain_fp64": "full SVD per k (torch.linalg.svdvals), as the reference"},
+        "norm_krylov_blocks": res["mixed"]["iterations"],
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,8 +261,15 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--profile-step", default=None, choices=["mixed", "fp64"],
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "sweep"],
+                    help="sweep: the config-3 wavenumber sweep measurement (its own JSON line)")
+    ap.add_argument("--sweep-k", type=int, default=60, help="number of wavenumbers of the sweep workload")
     args = ap.parse_args()
     ws, rank, local = _dist()
+    if args.workload == "sweep":
+        if rank == 0:
+            sweep_bench(args.sweep_k)
+        return
     if args.profile_step:
         profile_step(args.profile_step)
         return

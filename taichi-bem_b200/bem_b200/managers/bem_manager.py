@@ -79,6 +79,13 @@ class BEMManager:
         self.solver = p.get("solver", "lstsq" if self._is_transmission else "lu")
         self.refine_tol = float(p.get("refine_tol", 1e-12))
         self.refine_maxit = int(p.get("refine_maxit", 60))
+        # a refinement that stagnates at this relative residual or below is
+        # accepted (the attainable FP64 level of an ill-conditioned system)
+        self.refine_accept = float(p.get("refine_accept", 1e-8))
+        # iterative operator-norm estimates: relative change of the smallest
+        # Ritz value at which the block Krylov estimate stops, block cap
+        self.norm_tol = float(p.get("norm_tol", 1e-10))
+        self.norm_maxit = int(p.get("norm_maxit", 32))
         self.device = torch.device(p.get("device", "cuda"))
         self.torch_dtype = torch.complex128 if self._n == 2 else torch.float64
         self.conj_data = (self._n == 2) and self.quirk
@@ -252,35 +259,47 @@ class BEMManager:
     # -- solve --------------------------------------------------------------------------
     def _lu_solve_square(self, A: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
         """x = A^{-1} b with the hand-written LU: FP64 factor (plain path) or
-        FP32 factor + FP64 refinement against A (mixed path)."""
+        FP32 factor + FP64 refinement against A (mixed path).  b is a vector
+        or an n x nrhs matrix; A is factored once."""
+        cols = [b.contiguous()] if b.dim() == 1 else [b[:, j].contiguous() for j in range(b.shape[1])]
         if self.precision == "fp64":
             LU = A.clone()
             piv, info = self.engine.lu_factor(LU)
-            x = b.clone().contiguous()
-            self.engine.lu_solve(LU, piv, x)
+            xs = []
+            for c in cols:
+                x = c.clone()
+                self.engine.lu_solve(LU, piv, x)
+                xs.append(x)
             self.solve_info = {"factor": "fp64", "info": info}
-            return x
+            return xs[0] if b.dim() == 1 else torch.stack(xs, 1)
         lo = torch.complex64 if A.is_complex() else torch.float32
         LU = A.to(lo)
         piv, dinv, info = self.engine.lu_factor_tiled(LU)
-        x = torch.zeros_like(b)
-        try:
-            it, rr = self.engine.refine_solve(A, LU, piv, b.contiguous(), x, tol=self.refine_tol,
-                                              maxit=self.refine_maxit, dinv=dinv)
-            kind = "fp32 tile-pivoted"
-        except L.BemError as exc:
-            if exc.code != -4:
-                raise
-            # the tile-pivoted factor was not a good enough preconditioner:
-            # fall back to partial pivoting over full columns
-            LU = A.to(lo)
-            piv, info = self.engine.lu_factor(LU)
-            x.zero_()
-            it, rr = self.engine.refine_solve(A, LU, piv, b.contiguous(), x, tol=self.refine_tol,
-                                              maxit=self.refine_maxit)
-            kind = "fp32 partial pivoting (fallback)"
-        self.solve_info = {"factor": kind, "info": info, "refine_iters": it, "relres": rr}
-        return x
+        kind = "fp32 tile-pivoted"
+        xs, its, rrs = [], [], []
+        for c in cols:
+            x = torch.zeros_like(c)
+            try:
+                it, rr = self.engine.refine_solve(A, LU, piv, c, x, tol=self.refine_tol, maxit=self.refine_maxit,
+                                                  dinv=dinv, accept=self.refine_accept)
+            except L.BemError as exc:
+                if exc.code != -4:
+                    raise
+                # the tile-pivoted factor was not a good enough preconditioner:
+                # fall back to partial pivoting over full columns
+                if dinv is not None:
+                    LU = A.to(lo)
+                    piv, info = self.engine.lu_factor(LU)
+                    dinv = None
+                    kind = "fp32 partial pivoting (fallback)"
+                x.zero_()
+                it, rr = self.engine.refine_solve(A, LU, piv, c, x, tol=self.refine_tol, maxit=self.refine_maxit,
+                                                  accept=self.refine_accept)
+            xs.append(x)
+            its.append(it)
+            rrs.append(rr)
+        self.solve_info = {"factor": kind, "info": info, "refine_iters": max(its), "relres": max(rrs)}
+        return xs[0] if b.dim() == 1 else torch.stack(xs, 1)
 
     def solve(self):
         n = self.N_Neumann + self.M_Dirichlet
@@ -412,6 +431,128 @@ class BEMManager:
         rc.multiply_identity_to_vector(multiplier=half)
         self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)
         self.assemble_rhs()
+
+    # -- operator norms (BEM_manager.py:846-988) ------------------------------------
+    def matrix_layer_init(self):
+        """Zero the operator blocks (BEM_manager.py:823-827)."""
+        for lay in (self.single_layer, self.double_layer, self.adj_double_layer, self.hypersingular_layer):
+            for name in ("_Vmat", "_Kmat", "_Wmat"):
+                blk = getattr(lay, name, None)
+                if blk is not None:
+                    blk.zero_()
+
+    def get_V_part(self, A):
+        No, N = self._Neumann_offset_i, self.N_Neumann
+        return A[No:No + N, self._Neumann_offset_j:self._Neumann_offset_j + N]
+
+    def get_K_part(self, A):
+        return A[self._Neumann_offset_i:self._Neumann_offset_i + self.N_Neumann,
+                 self._Dirichlet_offset_j:self._Dirichlet_offset_j + self.M_Dirichlet]
+
+    def get_adj_K_part(self, A):
+        return A[self._Dirichlet_offset_i:self._Dirichlet_offset_i + self.M_Dirichlet,
+                 self._Neumann_offset_j:self._Neumann_offset_j + self.N_Neumann]
+
+    def get_W_part(self, A):
+        Do, M = self._Dirichlet_offset_i, self.M_Dirichlet
+        return A[Do:Do + M, self._Dirichlet_offset_j:self._Dirichlet_offset_j + M]
+
+    # relative diagonal shift of the energy-scaling block before its Cholesky factorisation
+    SCALING_SHIFT = 1e-10
+
+    @classmethod
+    def _shifted(cls, MV: torch.Tensor) -> torch.Tensor:
+        """MV + shift * max|MV| * I.  The reference factors MV itself, but the
+        W block of the k = 0 operator it is taken from is singular (constants
+        are in the null space of the Laplace hypersingular operator), so
+        whether that Cholesky succeeds depends on rounding; the fixed relative
+        shift makes the scaling well defined and reproducible."""
+        d = cls.SCALING_SHIFT * float(MV.abs().max())
+        return MV + d * torch.eye(MV.shape[0], dtype=MV.dtype, device=MV.device)
+
+    def compute_inv_norm(self, A: torch.Tensor, A_type: int, method: str = "svd", return_cond: bool = False):
+        """||A^{-1}|| in the energy-scaled norm (BEM_manager.py:874-920).
+
+        The scaling L^{-H} (L the Cholesky factor of blockdiag(W, V) of A for
+        A_type 1, of blockdiag(K', K) for A_type 2, shifted by `_shifted`) is
+        formed on the first call
+        and kept, as in the reference; the reference's sweep makes that call at
+        k = 0.  The scaled operator L^{-1} A L^{-H} (block-diagonal left factor
+        for the augmented 2n x n operator) has its smallest singular value
+        sigma_min; the result is 1 / sigma_min.  method "svd" takes all
+        singular values as the reference does; "iterative" estimates the
+        extreme ones by inverse / power iteration with this library's LU
+        (managers/sweep.py); "none" only forms the scaling.  With
+        return_cond the result is (1 / sigma_min, sigma_max / sigma_min,
+        iterations)."""
+        n = self.N_Neumann + self.M_Dirichlet
+        top = A[:n]
+        if self._L1_inv_H is None and A_type == 1:
+            MV = torch.zeros_like(top)
+            Do, No = self._Dirichlet_offset_i, self._Neumann_offset_i
+            MV[Do:Do + self.M_Dirichlet, self._Dirichlet_offset_j:self._Dirichlet_offset_j + self.M_Dirichlet] = \
+                self.get_W_part(top)
+            MV[No:No + self.N_Neumann, self._Neumann_offset_j:self._Neumann_offset_j + self.N_Neumann] = \
+                self.get_V_part(top)
+            MV = (MV + MV.transpose(0, 1)) / 2.0
+            self._L1_inv_H = torch.linalg.inv(torch.linalg.cholesky(self._shifted(MV), upper=False)) \
+                .transpose(0, 1).conj()
+            self._L2_inv_H = None
+        elif self._L2_inv_H is None and A_type == 2:
+            MV = torch.block_diag(self.get_adj_K_part(top), self.get_K_part(top))
+            self._L2_inv_H = torch.linalg.inv(torch.linalg.cholesky(self._shifted(MV), upper=False)) \
+                .transpose(0, 1).conj()
+            self._L1_inv_H = None
+        if method == "none":
+            return None
+        Linv_H = self._L1_inv_H if A_type == 1 else self._L2_inv_H
+        S = A @ Linv_H
+        LH = Linv_H.transpose(0, 1).conj().contiguous()
+        if A.shape[0] == n:
+            S = LH @ S
+        elif A.shape[0] == 2 * n:
+            S = torch.cat((LH @ S[:n], LH @ S[n:]), 0)
+        else:
+            raise NotImplementedError("We only support Non-Augmentd matrix and Augmented Matrix for Norm analysis")
+        if method == "svd":
+            sv = torch.linalg.svdvals(S)
+            smin, smax, its = float(sv.min()), float(sv.max()), 0
+        elif method == "iterative":
+            from .sweep import smallest_singular_value
+            smin, smax, its = smallest_singular_value(self.engine, S.contiguous(), tol=self.norm_tol,
+                                                      maxit=self.norm_maxit)
+        else:
+            raise ValueError(method)
+        inv = 1.0 / smin if smin > 0 else float("inf")
+        if return_cond:
+            return inv, smax * inv, its
+        return inv
+
+    def get_mat_A1_inv_norm(self, k: float, method: str = "svd"):
+        """A_I = P^-_o - P^+_i (BEM_manager.py:922-936)."""
+        from .sweep import transmission_operator
+        return self.compute_inv_norm(transmission_operator(self, k, 1, augmented=False), 1, method=method)
+
+    def get_mat_A2_inv_norm(self, k: float, method: str = "svd"):
+        """A_II = P^-_o + P^+_i (BEM_manager.py:938-950)."""
+        from .sweep import transmission_operator
+        return self.compute_inv_norm(transmission_operator(self, k, 2, augmented=False), 2, method=method)
+
+    def _augment(self, k, need_recompute_matrix_layers):
+        A = self._mat_A.clone()
+        self._mat_A.zero_()
+        if need_recompute_matrix_layers:
+            self.matrix_layer_forward(k=k, sqrt_n=self._sqrt_ni, scope_type=int(ScopeType.INTERIOR))
+        self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
+        return torch.cat((A, self._mat_A.clone()), 0)
+
+    def get_augment_mat_A1_inv_norm(self, k: float, need_recompute_matrix_layers: bool, method: str = "svd"):
+        """[A; P^+_i] with A the current operator (BEM_manager.py:952-969)."""
+        return self.compute_inv_norm(self._augment(k, need_recompute_matrix_layers), 1, method=method)
+
+    def get_augment_mat_A2_inv_norm(self, k: float, need_recompute_matrix_layers: bool, method: str = "svd"):
+        """(BEM_manager.py:971-988)."""
+        return self.compute_inv_norm(self._augment(k, need_recompute_matrix_layers), 2, method=method)
 
     def fused_assembly_call(self):
         """The one C-ABI call of the fused Dirichlet pass: V (far pairs in

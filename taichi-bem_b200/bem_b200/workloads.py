@@ -66,4 +66,16 @@ def config2(precision="mixed", seed=0):
     return _base(object="icosphere4", kernel="Helmholtz", k=3.0, precision=precision), fD, fN
 
 
-CONFIGS = {1: config1, 2: config2}
+def config3(precision="mixed", n_k=60):
+    """Wavenumber sweep of the augmented transmission operator on icosphere s4
+    (5120 panels, P1 Neumann and Dirichlet: 5124 unknowns), k_i = 16 + i/30,
+    with the reference sweep's parameters (demo_3d_plot_Sio.py: n_i = 3,
+    n_o = 1, GaussQR = 3).  Returns (params, fD, fN, ks)."""
+    fD, fN = plane_wave(16.0, plane_wave_direction(0))
+    params = _base(object="icosphere4", kernel="Helmholtz_Transmission", boundary="Full", k=16.0, n_i=3.0,
+                   n_o=1.0, GaussQR=3, Q_Neumann=1, Q_Dirichlet=1, precision=precision)
+    ks = [16.0 + i / 30.0 for i in range(n_k)]
+    return params, fD, fN, ks
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3}

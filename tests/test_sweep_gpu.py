@@ -1,0 +1,108 @@
+"""Operator-norm API and wavenumber sweep of the transmission operator
+(BEM_manager.py:874-988, demo/demo_3d_plot_Sio.py) against the oracle: the
+FP64 operators assembled by the CPU restatement, scaled as the reference
+does, and their singular values from numpy."""
+import numpy as np
+import pytest
+import torch
+
+from _util import rel_err
+
+pytestmark = pytest.mark.gpu
+
+KS = [1.5, 4.0]
+
+
+def _params(precision):
+    from bem_b200 import icosphere
+    v, f = icosphere(1)
+    return dict(dim=3, object="icosphere1", vertices=v, panels=f, GaussQR=3, n_i=3.0, n_o=1.0, k=0.0,
+                kernel="Helmholtz_Transmission", boundary="Full", scope="Interior", show="Default", Q_Neumann=1,
+                Q_Dirichlet=1, precision=precision, log_to_disk=False, make_video=False, show_wireframe=False,
+                vis=False), v, f
+
+
+def _manager(precision):
+    from bem_b200.managers import CoreManager
+    from bem_b200.workloads import plane_wave
+    params, v, f = _params(precision)
+    fD, fN = plane_wave(1.0, [0.0, 0.0, 1.0])
+    core = CoreManager(params)
+    core.initialization(fD, fN)
+    return core, v, f
+
+
+def _oracle_ops(v, f, k, A_type):
+    from oracle import oracle as O
+    params, _, _ = _params("fp64")
+    params["k"] = k
+    fD = lambda x, s=1.0: np.exp(1j * x[:, 2])
+    fN = lambda x, n, s=1.0: 1j * n[:, 2] * np.exp(1j * x[:, 2])
+    P = O.Problem(v, f, params, fD, fN)
+    lo, li = P.forward(P.sqrt_no), P.forward(P.sqrt_ni)
+    A = np.zeros((P.n, P.n), complex)
+    P.add_identity(A, 0.5)
+    P.add_M(A, lo, -1.0)
+    P.add_identity(A, -0.5 if A_type == 1 else 0.5)
+    P.add_M(A, li, -1.0 if A_type == 1 else 1.0)
+    Pp = np.zeros_like(A)
+    P.add_identity(Pp, 0.5)
+    P.add_M(Pp, li, 1.0)
+    return A, Pp, P.mesh
+
+
+def _oracle_inv_norms(v, f, A_type):
+    """Reference procedure: scaling from the k = 0 operator, then 1/sigma_min
+    of the scaled operator and of the scaled augmented operator."""
+    A0, _, m = _oracle_ops(v, f, 0.0, A_type)
+    M = m.M_D
+    if A_type == 1:
+        MV = np.zeros_like(A0)
+        MV[:M, :M] = A0[:M, :M]
+        MV[M:, M:] = A0[M:, M:]
+        MV = (MV + MV.T) / 2.0
+    else:
+        MV = np.zeros_like(A0)
+        MV[:M, :M] = A0[:M, M:]
+        MV[M:, M:] = A0[M:, :M]
+    # the manager's fixed relative shift of the scaling block (BEMManager._shifted)
+    L = np.linalg.cholesky(MV + 1e-10 * np.abs(MV).max() * np.eye(MV.shape[0]))
+    LinvH = np.linalg.inv(L).T.conj()
+    out = []
+    for k in KS:
+        A, Pp, _ = _oracle_ops(v, f, k, A_type)
+        S = LinvH.T.conj() @ A @ LinvH
+        Sa = np.concatenate([LinvH.T.conj() @ A @ LinvH, LinvH.T.conj() @ Pp @ LinvH], 0)
+        out.append((1.0 / np.linalg.svd(S, compute_uv=False).min(),
+                    1.0 / np.linalg.svd(Sa, compute_uv=False).min()))
+    return out
+
+
+@pytest.mark.parametrize("A_type", [1, 2])
+def test_inverse_norms_match_oracle(A_type):
+    core, v, f = _manager("fp64")
+    b = core._BEM_manager
+    ref = _oracle_inv_norms(v, f, A_type)
+    get = b.get_mat_A1_inv_norm if A_type == 1 else b.get_mat_A2_inv_norm
+    aug = b.get_augment_mat_A1_inv_norm if A_type == 1 else b.get_augment_mat_A2_inv_norm
+    get(0.0)  # the reference forms the energy scaling on its first call, at k = 0
+    for k, (r, ra) in zip(KS, ref):
+        for method in ("svd", "iterative"):
+            got = get(k, method=method)
+            assert abs(got - r) <= 1e-6 * r, (k, method, got, r)
+            got_a = aug(k, False, method=method)
+            assert abs(got_a - ra) <= 1e-6 * ra, (k, method, got_a, ra)
+    core.kill()
+
+
+def test_sweep_mixed_matches_fp64():
+    from bem_b200.managers.sweep import wavenumber_sweep
+    out = {}
+    for prec in ("fp64", "mixed"):
+        core, v, f = _manager(prec)
+        out[prec] = wavenumber_sweep(core._BEM_manager, KS, nrhs=4, seed=0)
+        core.kill()
+    for a, b_ in zip(out["fp64"]["solutions"], out["mixed"]["solutions"]):
+        assert rel_err(b_.cpu().numpy(), a.cpu().numpy()) < 1e-6
+    for a, b_ in zip(out["fp64"]["inv_norm"], out["mixed"]["inv_norm"]):
+        assert abs(a - b_) <= 1e-5 * a
