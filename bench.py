@@ -253,6 +253,68 @@ def sweep_bench(n_k: int):
     }))
 
 
+def shape_bench(subdiv: int, n_check: int):
+    """Config 4: shape gradient of the Laplace Dirichlet problem on a radially
+    perturbed icosphere (real spherical harmonics of degree <= 6, max |dr| =
+    0.05), J = ||t - t_target||^2 with t_target from the unperturbed sphere,
+    GaussQR = 5.  Times the mixed forward solve and the adjoint pass, and
+    checks the adjoint gradient against central differences (h = 1e-6) of the
+    FP64-assembled problem along seeded random directions at n_check vertices."""
+    import numpy as np
+    import torch
+    from bem_b200 import icosphere
+    from bem_b200.meshes import perturbed_sphere
+    from bem_b200.shape import DirichletShape, DirichletShapeSolve, point_source
+    v0, f = icosphere(subdiv)
+    v, _ = perturbed_sphere(subdiv, lmax=6, amplitude=0.05, seed=0)
+    u, gu = point_source()
+    dev = torch.device("cuda")
+    X0, X = torch.as_tensor(v0, device=dev), torch.as_tensor(v, device=dev)
+
+    def grad_of(prob, t_target):
+        Xg = X.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t = DirichletShapeSolve.apply(Xg, prob)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ((t - t_target) ** 2).sum().backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        return Xg.grad, (t1 - t0) * 1e3, (t2 - t1) * 1e3
+
+    pm = DirichletShape(f, u, gu, gauss_qr=5, precision="mixed")
+    tm = pm.forward(X0).clone()
+    grad_of(pm, tm)  # warm-up
+    Gm, fwd_ms, bwd_ms = grad_of(pm, tm)
+    p64 = DirichletShape(f, u, gu, gauss_qr=5, precision="fp64", solver="mixed")
+    t64 = p64.forward(X0).clone()
+    G64, fwd64_ms, _ = grad_of(p64, t64)
+    rng = np.random.default_rng(0)
+    h = 1e-6
+    errs = []
+    for vi in rng.choice(len(v), size=n_check, replace=False):
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        dt = torch.as_tensor(d, device=dev)
+        Js = []
+        for sgn in (1.0, -1.0):
+            Xs = X.clone()
+            Xs[int(vi)] += sgn * h * dt
+            Js.append(float(((p64.forward(Xs) - t64) ** 2).sum()))
+        fd = (Js[0] - Js[1]) / (2 * h)
+        ad = float(G64[int(vi)] @ dt)
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    gmax = float(G64.abs().max())
+    print(json.dumps({
+        "workload": f"config 4: shape gradient, Laplace Dirichlet, perturbed icosphere s{subdiv} ({len(f)} panels), "
+                    "GaussQR=5, J = ||t - t_target||^2",
+        "forward_ms_mixed": fwd_ms, "adjoint_ms": bwd_ms, "forward_ms_fp64_assembly": fwd64_ms,
+        "fd_check": {"vertices": n_check, "h": h, "max_rel_err": max(errs), "median_rel_err": float(np.median(errs))},
+        "mixed_vs_fp64_gradient_rel": float((Gm - G64).norm() / G64.norm()), "grad_max": gmax,
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -261,14 +323,21 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--profile-step", default=None, choices=["mixed", "fp64"],
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
-    ap.add_argument("--workload", default="config2", choices=["config2", "sweep"],
-                    help="sweep: the config-3 wavenumber sweep measurement (its own JSON line)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "sweep", "shape"],
+                    help="sweep: the config-3 wavenumber sweep, shape: the config-4 shape gradient "
+                         "(each its own JSON line)")
+    ap.add_argument("--shape-subdiv", type=int, default=5, help="icosphere subdivision of the shape workload")
+    ap.add_argument("--shape-check", type=int, default=32, help="vertices of the finite-difference check")
     ap.add_argument("--sweep-k", type=int, default=60, help="number of wavenumbers of the sweep workload")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.workload == "sweep":
         if rank == 0:
             sweep_bench(args.sweep_k)
+        return
+    if args.workload == "shape":
+        if rank == 0:
+            shape_bench(args.shape_subdiv, args.shape_check)
         return
     if args.profile_step:
         profile_step(args.profile_step)

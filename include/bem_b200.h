@@ -140,6 +140,18 @@ int bem_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int dt
              void* out, int64_t ld, double scale, void* out_t, double scale_t,
              const void* x, void* y, int conj_x, void* stream);
 
+/* Shape derivative of a Laplace bilinear form (no reference counterpart: the
+ * reference has no derivatives; this is the adjoint pass of the shape-gradient
+ * workload).  grad (device [nv*3], FP64) is accumulated:
+ *   grad[3 v + c] += d/dX_{v,c}  sum_{r, c'} lam[r] A(r, c') u[c']
+ * with A the block of op->op (BEM_OP_V with P0 test and P0 trial spaces, or
+ * BEM_OP_K with a P0 test and a P1 trial space), op->kernel BEM_KERNEL_LAPLACE,
+ * lam indexed by the test space's dof numbers and u by the trial space's.
+ * Every quadrature point is recomputed in FP64 (op->quirk selects the near-
+ * field maps as in bem_assemble); nothing is stored by the forward pass. */
+int bem_adjoint_vertices(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                         const double* lam, const double* u, double* grad, void* stream);
+
 /* ---- dense linear algebra (replaces torch.linalg.solve, BEM_manager.py:1056) --
  * LU with partial pivoting in place (row-major, n x n, lda).  dtype
  * BEM_F64/BEM_C128 (plain FP64 path) or BEM_F32/BEM_C64 (low-precision factor

@@ -175,6 +175,17 @@ class Engine:
                                                     ctypes.byref(ds), _ptr(g), _ptr(y), float(scale_k),
                                                     int(bool(conj_g)), _stream_ptr()))
 
+    def adjoint_vertices(self, desc: L.OpDesc, test: DeviceSpace, trial: DeviceSpace, lam: torch.Tensor,
+                         u: torch.Tensor, grad: torch.Tensor):
+        """grad [nv, 3] += d/dX sum lam[r] A(r, c) u[c] (Laplace V or K, FP64)."""
+        assert lam.dtype == torch.float64 and u.dtype == torch.float64 and grad.dtype == torch.float64
+        assert lam.is_contiguous() and u.is_contiguous() and grad.is_contiguous() and grad.numel() == 3 * self.nv
+        self._check_spaces(test, trial, lam.numel(), u.numel())
+        ts, rs = test.c(), trial.c()
+        self._check(self.lib.bem_adjoint_vertices(self.ctx, ctypes.byref(desc), ctypes.byref(ts), ctypes.byref(rs),
+                                                  _ptr(lam), _ptr(u), _ptr(grad), _stream_ptr()))
+        return grad
+
     def mass(self, test: DeviceSpace, trial: DeviceSpace, out=None, scale=1.0, out_t=None, scale_t=0.0, x=None,
              y=None, conj_x=False):
         ts, rs = test.c(), trial.c()

@@ -381,4 +381,18 @@ int bem_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int dt
                            (cudaStream_t)stream);
 }
 
+int bem_adjoint_vertices(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                         const double* lam, const double* u, double* grad, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
+    if (!op || !lam || !u || !grad) return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: null argument");
+    if (op->kernel != BEM_KERNEL_LAPLACE || (op->op != BEM_OP_V && op->op != BEM_OP_K))
+        return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: Laplace V or K only");
+    if (int rc = check_space(ctx, test, "test")) return rc;
+    if (int rc = check_space(ctx, trial, "trial")) return rc;
+    if (test->nb != 1 || trial->nb != (op->op == BEM_OP_V ? 1 : 3))
+        return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: V needs P0 x P0 spaces, K a P0 test and a P1 trial space");
+    return bem_launch_adjoint(ctx, op, test, trial, lam, u, grad, (cudaStream_t)stream);
+}
+
 }  // extern "C"

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include "bem_internal.cuh"
+#include "bem_quadrature.cuh"
 
 namespace {
 
@@ -737,45 +738,7 @@ __global__ void __launch_bounds__(128) near_kernel(NearArgs a) {
         int iw = p % Q, iz = (p / Q) % Q, iy = (p / (Q * Q)) % Q, ix = p / (Q * Q * Q);
         const double xsi = a.gp[ix], eta1 = a.gp[iy], eta2 = a.gp[iz], eta3 = a.gp[iw];
         const double weight = (a.gw[ix] * a.gw[iy] * (X.area * 2.0)) * (a.gw[iz] * a.gw[iw] * (Y.area * 2.0));
-        if (rel == REL_COINCIDE) {
-            const double jac = xsi * xsi * xsi * eta1 * eta1 * eta2;
-            const double w0 = xsi, w1 = xsi * eta1, w2 = xsi * eta1 * eta2, w3 = xsi * eta1 * eta2 * eta3;
-            // m_mats_coincide (BEM_manager.py:141-165) applied to w
-            double z[3][4] = {{w0, w0 - w1 + w2, w3, w2},
-                              {w0, w1 - w2 + w3, w2, w3},
-                              {w0 - w3, w1 - w3, -w3, w2 - w3}};
-            for (int m = 0; m < 3; ++m) {
-                double r1x = z[m][0], r2x = z[m][1], r1y = z[m][0] - z[m][2], r2y = z[m][1] - z[m][3];
-                add(r1x, r2x, r1y, r2y, weight * jac, false, r1x, r2x, r1y, r2y);
-                if (a.quirk)
-                    add(r1x, r2x, r1y, r2y, weight * jac, true, r1x, r2x, r1y, r2y);
-                else
-                    add(r1x, r2x, r1y, r2y, weight * jac, true, r1y, r2y, r1x, r2x);
-            }
-        } else if (rel == REL_VERTEX) {
-            const double jac = xsi * xsi * xsi * eta2;
-            add(xsi, xsi * eta1, xsi * eta2, xsi * eta2 * eta3, weight * jac, false, xsi, xsi * eta1, xsi * eta2,
-                xsi * eta2 * eta3);
-            add(xsi * eta2, xsi * eta2 * eta3, xsi, xsi * eta1, weight * jac, false, xsi * eta2, xsi * eta2 * eta3,
-                xsi, xsi * eta1);
-        } else {  // REL_EDGE
-            double w0, w1, w2, w3;
-            const double jac1 = xsi * xsi * xsi * eta1 * eta1;
-            const double jac = jac1 * eta2;
-            w0 = xsi; w1 = -xsi * eta1 * eta2; w2 = xsi * eta1 * (1.0 - eta2); w3 = xsi * eta1 * eta3;
-            add(w0, w3, w0 + w1, w2, weight * jac1, false, w0, w3, w0 + w1, w2);
-            w0 = xsi; w1 = -xsi * eta1 * eta2 * eta3; w2 = xsi * eta1 * eta2 * (1.0 - eta3); w3 = xsi * eta1;
-            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
-            w0 = xsi * (1.0 - eta1 * eta2); w1 = xsi * eta1 * eta2; w2 = xsi * eta1 * eta2 * eta3;
-            w3 = xsi * eta1 * (1.0 - eta2);
-            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
-            w0 = xsi * (1.0 - eta1 * eta2 * eta3); w1 = xsi * eta1 * eta2 * eta3; w2 = xsi * eta1;
-            w3 = xsi * eta1 * eta2 * (1.0 - eta3);
-            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
-            w0 = xsi * (1.0 - eta1 * eta2 * eta3); w1 = xsi * eta1 * eta2 * eta3; w2 = xsi * eta1 * eta2;
-            w3 = xsi * eta1 * (1.0 - eta2 * eta3);
-            add(w0, w3, w0 + w1, w2, weight * jac, false, w0, w3, w0 + w1, w2);
-        }
+        near_points(rel, a.quirk != 0, xsi, eta1, eta2, eta3, weight, add);
     }
 
     // warp reduction of every moment
@@ -1382,7 +1345,7 @@ int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s) {
     return bem_check_cuda(ctx, cudaGetLastError(), "geometry_kernel launch");
 }
 
-static int fill_local_map(bem_ctx* ctx, const bem_space* sp, int32_t* map, cudaStream_t s) {
+int bem_fill_local_map(bem_ctx* ctx, const bem_space* sp, int32_t* map, cudaStream_t s) {
     if (int rc = bem_check_cuda(ctx, cudaMemsetAsync(map, 0xff, sizeof(int32_t) * ctx->nt, s), "memset")) return rc;
     if (sp->n_panels > 0) {
         scatter_local_kernel<<<(sp->n_panels + 127) / 128, 128, 0, s>>>(sp->n_panels, sp->panels, map, ctx->nt,
@@ -1396,8 +1359,8 @@ static int fill_local_map(bem_ctx* ctx, const bem_space* sp, int32_t* map, cudaS
 int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                         int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
                         void* y, int conj_x, cudaStream_t s) {
-    if (int rc = fill_local_map(ctx, test, ctx->test_local, s)) return rc;
-    if (int rc = fill_local_map(ctx, trial, ctx->trial_local, s)) return rc;
+    if (int rc = bem_fill_local_map(ctx, test, ctx->test_local, s)) return rc;
+    if (int rc = bem_fill_local_map(ctx, trial, ctx->trial_local, s)) return rc;
     bool fp32 = op->precision == BEM_PREC_MIXED;
     FarArgs fa;
     fa.n_test = test->n_panels;
@@ -1470,8 +1433,8 @@ int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* te
 int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                          void* out, int64_t ld, double scale, const bem_space* rows, const bem_space* data,
                          const void* g, void* y, double scale_k, int conj_g, cudaStream_t s) {
-    if (int rc = fill_local_map(ctx, test, ctx->test_local, s)) return rc;
-    if (int rc = fill_local_map(ctx, trial, ctx->trial_local, s)) return rc;
+    if (int rc = bem_fill_local_map(ctx, test, ctx->test_local, s)) return rc;
+    if (int rc = bem_fill_local_map(ctx, trial, ctx->trial_local, s)) return rc;
     const bool fp32 = op->precision == BEM_PREC_MIXED;
     const bool helm = op->kernel == BEM_KERNEL_HELMHOLTZ;
     FarArgs fa{};

@@ -57,6 +57,9 @@ int bem_ws_reserve(bem_ctx* ctx, size_t bytes);
 
 // Launch wrappers (bem_assembly.cu)
 int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s);
+int bem_fill_local_map(bem_ctx* ctx, const bem_space* sp, int32_t* map, cudaStream_t s);
+int bem_launch_adjoint(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                       const double* lam, const double* u, double* grad, cudaStream_t s);
 int bem_lookahead_stream(bem_ctx* ctx);
 int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                         int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
