@@ -315,6 +315,59 @@ def shape_bench(subdiv: int, n_check: int):
     }))
 
 
+def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
+    """Config 5: the Helmholtz transmission system (k_out = 5, k_in = 7.5) on
+    icosphere s<subdiv> in mixed precision (FP32 far field, FP64 near field,
+    TF32 tile LU + FP64 refinement on the square system), its error against
+    the FP64-assembled system solved to FP64 accuracy, and dJ/dk of
+    J = ||x||^2 by the adjoint against a central difference of J."""
+    import torch
+    from bem_b200.managers import CoreManager
+    from bem_b200.managers.sweep import solution_norm_k_gradient
+    from bem_b200.workloads import config5
+    res = {}
+    params, pw = config5("mixed", subdiv, solver)
+    core = CoreManager(params)
+    core.initialization(pw.fD, pw.fN)
+    b = core._BEM_manager
+    b.run()  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run()
+    torch.cuda.synchronize()
+    res["mixed_ms"] = (time.perf_counter() - t0) * 1e3
+    res["refinement"] = {k: (v if not hasattr(v, "item") else v.item()) for k, v in b.solve_info.items()}
+    x_mixed = b.raw_solved.clone()
+    n = b.N_Neumann + b.M_Dirichlet
+    g = solution_norm_k_gradient(b, pw, delta=1e-3, check=True) if solver == "square" else None
+    res["dJdk"] = None if g is None else {"J": g["J"], "adjoint": g["dJdk"], "central_difference": g["dJdk_central_difference"],
+                   "rel_diff": abs(g["dJdk"] - g["dJdk_central_difference"]) / abs(g["dJdk_central_difference"]),
+                   "adjoint_ms": g["adjoint_ms"], "delta": 1e-3}
+    core.kill()
+    params, pw = config5("fp64", subdiv, solver)
+    params.update(solve_precision="mixed", refine_tol=1e-13)
+    core = CoreManager(params)
+    core.initialization(pw.fD, pw.fN)
+    core._BEM_manager.run()
+    x64 = core._BEM_manager.raw_solved.clone()
+    core.kill()
+    res["rel_err_vs_fp64"] = {"l2": float(torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)),
+                              "max": float((x_mixed - x64).abs().max() / x64.abs().max())}
+    if plain:
+        params, pw = config5("fp64", subdiv, solver)
+        core = CoreManager(params)
+        core.initialization(pw.fD, pw.fN)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        core._BEM_manager.run()
+        torch.cuda.synchronize()
+        res["plain_fp64_ms"] = (time.perf_counter() - t0) * 1e3
+        res["speedup"] = res["plain_fp64_ms"] / res["mixed_ms"]
+        core.kill()
+    print(json.dumps(dict(workload=f"config 5: Helmholtz transmission, icosphere s{subdiv}, {n} unknowns, k_out=5, "
+                                   f"k_in=7.5, GaussQR=5, solver {solver}", **res)))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -323,11 +376,14 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--profile-step", default=None, choices=["mixed", "fp64"],
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
-    ap.add_argument("--workload", default="config2", choices=["config2", "sweep", "shape"],
+    ap.add_argument("--workload", default="config2", choices=["config2", "sweep", "shape", "transmission"],
                     help="sweep: the config-3 wavenumber sweep, shape: the config-4 shape gradient "
                          "(each its own JSON line)")
     ap.add_argument("--shape-subdiv", type=int, default=5, help="icosphere subdivision of the shape workload")
     ap.add_argument("--shape-check", type=int, default=32, help="vertices of the finite-difference check")
+    ap.add_argument("--trans-subdiv", type=int, default=5, help="icosphere subdivision of the transmission workload")
+    ap.add_argument("--trans-plain", action="store_true", help="also time the plain FP64 path (FP64 LU)")
+    ap.add_argument("--trans-solver", default="square", choices=["square", "lstsq"])
     ap.add_argument("--sweep-k", type=int, default=60, help="number of wavenumbers of the sweep workload")
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -338,6 +394,10 @@ def main():
     if args.workload == "shape":
         if rank == 0:
             shape_bench(args.shape_subdiv, args.shape_check)
+        return
+    if args.workload == "transmission":
+        if rank == 0:
+            transmission_bench(args.trans_subdiv, args.trans_plain, args.trans_solver)
         return
     if args.profile_step:
         profile_step(args.profile_step)

@@ -30,7 +30,7 @@ import torch
 from .. import _lib as L
 from ..BEM_functions.layers import (AdjDoubleLayer3d, DoubleLayer3d, HypersingularLayer3d, IdentityLayer3d,
                                     RHSConstructor3d, SingleLayer3d)
-from ..engine import DeviceSpace, Engine
+from ..engine import DeviceSpace, Engine, gmres_ir
 from ..utils.types import AssembleType, CellFluxType, KernelType, ScopeType, VertAttachType
 
 
@@ -72,6 +72,9 @@ class BEMManager:
         self.precision = p.get("precision", "fp64")
         if self.precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
+        # precision of the dense solve ("fp64": partial-pivoting LU; "mixed":
+        # FP32 tile LU + FP64 refinement), by default the assembly's
+        self.solve_precision = p.get("solve_precision", self.precision)
         self.quirk = bool(p.get("quirk", True))
         # one sweep for V and K g in the Dirichlet problem (the plain path keeps
         # one kernel per operator)
@@ -262,7 +265,7 @@ class BEMManager:
         FP32 factor + FP64 refinement against A (mixed path).  b is a vector
         or an n x nrhs matrix; A is factored once."""
         cols = [b.contiguous()] if b.dim() == 1 else [b[:, j].contiguous() for j in range(b.shape[1])]
-        if self.precision == "fp64":
+        if self.solve_precision == "fp64":
             LU = A.clone()
             piv, info = self.engine.lu_factor(LU)
             xs = []
@@ -275,26 +278,45 @@ class BEMManager:
         lo = torch.complex64 if A.is_complex() else torch.float32
         LU = A.to(lo)
         piv, dinv, info = self.engine.lu_factor_tiled(LU)
-        kind = "fp32 tile-pivoted"
+        kind = "fp32 tile-pivoted + refinement"
+        state = {"LU": LU, "piv": piv, "dinv": dinv}
+
+        def partial_pivoting():
+            # tile pivoting restricts row swaps to the 64-row diagonal tiles; a
+            # matrix whose large entries sit off the diagonal blocks needs
+            # partial pivoting over full columns
+            if state["dinv"] is not None:
+                state["LU"] = A.to(lo)
+                state["piv"], _ = self.engine.lu_factor(state["LU"])
+                state["dinv"] = None
+
         xs, its, rrs = [], [], []
         for c in cols:
             x = torch.zeros_like(c)
             try:
-                it, rr = self.engine.refine_solve(A, LU, piv, c, x, tol=self.refine_tol, maxit=self.refine_maxit,
-                                                  dinv=dinv, accept=self.refine_accept)
+                it, rr = self.engine.refine_solve(A, state["LU"], state["piv"], c, x, tol=self.refine_tol,
+                                                  maxit=self.refine_maxit, dinv=state["dinv"],
+                                                  accept=self.refine_accept)
             except L.BemError as exc:
                 if exc.code != -4:
                     raise
-                # the tile-pivoted factor was not a good enough preconditioner:
-                # fall back to partial pivoting over full columns
-                if dinv is not None:
-                    LU = A.to(lo)
-                    piv, info = self.engine.lu_factor(LU)
-                    dinv = None
-                    kind = "fp32 partial pivoting (fallback)"
+                partial_pivoting()
                 x.zero_()
-                it, rr = self.engine.refine_solve(A, LU, piv, c, x, tol=self.refine_tol, maxit=self.refine_maxit,
-                                                  accept=self.refine_accept)
+                try:
+                    it, rr = self.engine.refine_solve(A, state["LU"], state["piv"], c, x, tol=self.refine_tol,
+                                                      maxit=self.refine_maxit, accept=self.refine_accept)
+                    kind = "fp32 partial pivoting + refinement"
+                except L.BemError as exc2:
+                    if exc2.code != -4:
+                        raise
+                    # plain refinement contracts too slowly (cond(A) u_fp32 near 1):
+                    # GMRES in FP64 with the same factor as preconditioner
+                    x.zero_()
+                    LUp, pp = state["LU"], state["piv"]
+                    it, rr = gmres_ir(self.engine, A, lambda z: self.engine.lu_solve(LUp, pp, z), c, x,
+                                      tol=self.refine_tol, maxit=max(self.refine_maxit, 300),
+                                      accept=self.refine_accept)
+                    kind = "fp32 partial pivoting + GMRES-IR"
             xs.append(x)
             its.append(it)
             rrs.append(rr)
@@ -569,6 +591,14 @@ class BEMManager:
 
     def run(self):
         """BEMManager.run (BEM_manager.py:990-1030) without the GUI colouring."""
+        self.assemble_system()
+        self.solve()
+        self.compute_analytical_raw_solved()
+        self.splat_u_from_raw_solved_to_vertices()
+
+    def assemble_system(self):
+        """The part of `run` before the solve (BEM_manager.py:990-1018): the
+        operator into _mat_A and the right-hand side into rhs, at self._k."""
         self._mat_A.zero_()
         if self._is_transmission:
             self.matrix_layer_forward(k=self._k, sqrt_n=self._sqrt_no, scope_type=int(ScopeType.EXTERIOR))
@@ -587,9 +617,6 @@ class BEMManager:
                                                 sqrt_no=self._sqrt_no)
             self.rhs_layer_forward(k=self._k, scope_type=self._scope_type)
             self.assemble_rhs()
-        self.solve()
-        self.compute_analytical_raw_solved()
-        self.splat_u_from_raw_solved_to_vertices()
 
     def kill(self):
         self.initialized = False

@@ -44,6 +44,24 @@ def plane_wave(k: float, direction):
     return fD, fN
 
 
+class PlaneWave:
+    """u = exp(i k sqrt_n d.x) with a mutable wavenumber k (for derivatives in
+    k the boundary data follow the operator's k); fD and fN are the
+    reference's callback signatures."""
+
+    def __init__(self, k: float, direction):
+        self.k = float(k)
+        self.d = np.asarray(direction, dtype=np.float64)
+
+    def fD(self, x, s=1.0):
+        d = torch.as_tensor(self.d, dtype=x.dtype, device=x.device)
+        return torch.exp(1j * (self.k * s) * (x @ d))
+
+    def fN(self, x, n, s=1.0):
+        d = torch.as_tensor(self.d, dtype=x.dtype, device=x.device)
+        return 1j * (self.k * s) * (n @ d) * torch.exp(1j * (self.k * s) * (x @ d))
+
+
 def _base(**kw):
     p = dict(dim=3, object="icosphere3", GaussQR=5, n_i=1, n_o=1, k=0.0, kernel="Laplace", boundary="Dirichlet",
              scope="Interior", show="Default", Q_Neumann=0, Q_Dirichlet=1, log_to_disk=False, make_video=False,
@@ -78,4 +96,17 @@ def config3(precision="mixed", n_k=60):
     return params, fD, fN, ks
 
 
-CONFIGS = {1: config1, 2: config2, 3: config3}
+def config5(precision="mixed", subdiv=5, solver="square"):
+    """Helmholtz transmission (2x2 block Calderon system), icosphere s5 (20480
+    panels, P0 Neumann + P1 Dirichlet: 30722 unknowns), k_out = 5,
+    n_i = 2.25 (k_in = 7.5), n_o = 1, GaussQR = 5, incident plane wave with a
+    seeded direction; solver "square" (LU of the square system) or "lstsq"
+    (the reference's augmented least squares, by its normal equations).
+    Returns (params, PlaneWave)."""
+    pw = PlaneWave(5.0, plane_wave_direction(0))
+    params = _base(object=f"icosphere{subdiv}", kernel="Helmholtz_Transmission", boundary="Full", k=5.0, n_i=2.25,
+                   n_o=1.0, scope="Exterior", precision=precision, solver=solver)
+    return params, pw
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3, 5: config5}
