@@ -80,7 +80,11 @@ class BEMManager:
         # one kernel per operator)
         self.fuse = bool(p.get("fuse", self.precision == "mixed"))
         self.solver = p.get("solver", "lstsq" if self._is_transmission else "lu")
-        self.refine_tol = float(p.get("refine_tol", 1e-12))
+        # relative residual at which FP64 refinement stops: 1e-9 in mixed
+        # precision (its contribution to the solution error is at most
+        # cond(A) * 1e-9, ~1e-7 for cond(A) ~ 1e2, the order of the FP32
+        # assembly's own error and well inside the 1e-6 target), 1e-12 otherwise
+        self.refine_tol = float(p.get("refine_tol", 1e-9 if self.precision == "mixed" else 1e-12))
         self.refine_maxit = int(p.get("refine_maxit", 60))
         # a refinement that stagnates at this relative residual or below is
         # accepted (the attainable FP64 level of an ill-conditioned system)

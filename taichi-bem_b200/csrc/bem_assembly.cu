@@ -1435,6 +1435,16 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
                          const void* g, void* y, double scale_k, int conj_g, cudaStream_t s) {
     if (int rc = bem_fill_local_map(ctx, test, ctx->test_local, s)) return rc;
     if (int rc = bem_fill_local_map(ctx, trial, ctx->trial_local, s)) return rc;
+    // the FP64 near-pair kernels run on the side stream, concurrently with the
+    // FP32 far sweep (different pipes; they write other V entries and add to
+    // the right-hand side atomically); the caller's stream waits for both
+    if (int rc = bem_lookahead_stream(ctx)) return rc;
+    const bool side = ctx->n_near > 0;
+    if (side) {
+        cudaEventRecord(ctx->ev_next, s);
+        cudaStreamWaitEvent(ctx->aux, ctx->ev_next, 0);
+    }
+    const cudaStream_t sn = side ? ctx->aux : s;
     const bool fp32 = op->precision == BEM_PREC_MIXED;
     const bool helm = op->kernel == BEM_KERNEL_HELMHOLTZ;
     FarArgs fa{};
@@ -1535,22 +1545,26 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
         nk.scale = scale_k;
         nk.conj_x = conj_g;
         if (helm) {
-            near_kernel<BEM_OP_V, true, 1, 1><<<blocks, 128, 0, s>>>(nv);
+            near_kernel<BEM_OP_V, true, 1, 1><<<blocks, 128, 0, sn>>>(nv);
             if (data->nb == 3)
-                near_kernel<BEM_OP_K, true, 1, 3><<<blocks, 128, 0, s>>>(nk);
+                near_kernel<BEM_OP_K, true, 1, 3><<<blocks, 128, 0, sn>>>(nk);
             else
-                near_kernel<BEM_OP_K, true, 1, 1><<<blocks, 128, 0, s>>>(nk);
+                near_kernel<BEM_OP_K, true, 1, 1><<<blocks, 128, 0, sn>>>(nk);
         } else {
-            near_kernel<BEM_OP_V, false, 1, 1><<<blocks, 128, 0, s>>>(nv);
+            near_kernel<BEM_OP_V, false, 1, 1><<<blocks, 128, 0, sn>>>(nv);
             if (data->nb == 3)
-                near_kernel<BEM_OP_K, false, 1, 3><<<blocks, 128, 0, s>>>(nk);
+                near_kernel<BEM_OP_K, false, 1, 3><<<blocks, 128, 0, sn>>>(nk);
             else
-                near_kernel<BEM_OP_K, false, 1, 1><<<blocks, 128, 0, s>>>(nk);
+                near_kernel<BEM_OP_K, false, 1, 1><<<blocks, 128, 0, sn>>>(nk);
         }
         ctx->launches += 2;
         if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "near_kernel launch")) return rc;
     }
-    return BEM_OK;
+    if (side) {
+        cudaEventRecord(ctx->ev_diag, ctx->aux);
+        cudaStreamWaitEvent(s, ctx->ev_diag, 0);
+    }
+    return bem_check_cuda(ctx, cudaGetLastError(), "near-field join");
 }
 
 int bem_launch_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int is_complex, int mode, void* out,
