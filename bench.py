@@ -63,27 +63,80 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clocks and clock-event (throttle) reasons of this process's GPU
+    during the timed region: NVML polled every 200 ms from a background thread
+    (initialised and primed with one sample before the timed region starts,
+    so that no start-up work overlaps it); nvidia-smi in loop mode when NVML is
+    not available."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.samples, self.reasons, self.smax = [], set(), None
+        self.proc = self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.dev)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0".encode()
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _sample(self):
+        nv, h = self.nvml
+        self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        for name, bit in self.REASONS.items():
+            if mask & bit:
+                self.reasons.add(name)
 
     def start(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            self.nvml = self._nvml_handle()
+            nv, h = self.nvml
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._sample()
+            self.samples, self.reasons = [], set()  # the priming sample precedes the timed region
+        except Exception:
+            self.nvml = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,"
+                     "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                     "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                     "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                    stderr=subprocess.DEVNULL, text=True)
+                time.sleep(2.0)
+            except OSError:
+                self.proc = None
+            return
+        self.stop_flag = threading.Event()
+
+        def loop():
+            while not self.stop_flag.wait(0.2):
+                try:
+                    self._sample()
+                except Exception:
+                    break
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=2.0)
+            try:
+                self._sample()
+            except Exception:
+                pass
+            return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
+                    "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
         try:
             out, _ = self.proc.communicate(timeout=5)
@@ -93,19 +146,19 @@ class ClockSampler:
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in out.strip().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            parts = [q.strip() for q in line.split(",")]
+            if len(parts) < 6:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
             except ValueError:
                 continue
-            for nm, val in zip(names, parts[5:9]):
+            for nm, val in zip(names, parts[2:6]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 def cpu_reference(steps: int, warmup: int, threads: int | None = None, sample_rows: int | None = None,
@@ -458,15 +511,16 @@ def main():
         dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    time.sleep(0.3)
     launches0 = eng.launches
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
+    factors = []
     for s in range(args.steps):
         flush_l2()
         ev[s][0].record()
         b.run()
         ev[s][1].record()
+        factors.append(b.solve_info.get("factor"))
     torch.cuda.synchronize()
     launches = eng.launches - launches0
     step_ms = [a.elapsed_time(z) for a, z in ev]
@@ -492,6 +546,29 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = entries / (ms * 1e-3) * ws
+
+    # ---- e2e through the public API, host inputs, solution read back ----
+    from bem_b200 import icosphere
+    vh, fh = icosphere(4)
+    vpin = torch.as_tensor(vh).pin_memory()
+    fpin = torch.as_tensor(fh).pin_memory()
+    e2e_ms = []
+    h2d = vh.nbytes + fh.nbytes
+    d2h = 0
+    for s in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        params, fD, fN = config2(precision="mixed")
+        params.update(device=f"cuda:{local}", vertices=vpin.numpy(), panels=fpin.numpy())
+        c2 = CoreManager(params)
+        c2.initialization(fD, fN)
+        c2._BEM_manager.run()
+        host = c2._BEM_manager.raw_solved.to("cpu")
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        d2h = host.numel() * host.element_size()
+        c2.kill()
+    e2e = statistics.median(e2e_ms[1:])  # the first lifecycle of the loop is discarded
 
     # ---- plain FP64 path (the FP64 oracle of the mixed result) ----
     core64 = make("fp64")
@@ -522,29 +599,8 @@ def main():
     rel = float((sol_mixed - sol64).abs().max() / sol64.abs().max())
     rel2 = float(torch.linalg.norm(sol_mixed - sol64) / torch.linalg.norm(sol64))
     core64.kill()
-
-    # ---- e2e through the public API, host inputs, solution read back ----
-    from bem_b200 import icosphere
-    vh, fh = icosphere(4)
-    vpin = torch.as_tensor(vh).pin_memory()
-    fpin = torch.as_tensor(fh).pin_memory()
-    e2e_ms = []
-    h2d = vh.nbytes + fh.nbytes
-    d2h = 0
-    for s in range(5):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        params, fD, fN = config2(precision="mixed")
-        params.update(device=f"cuda:{local}", vertices=vpin.numpy(), panels=fpin.numpy())
-        c2 = CoreManager(params)
-        c2.initialization(fD, fN)
-        c2._BEM_manager.run()
-        host = c2._BEM_manager.raw_solved.to("cpu")
-        torch.cuda.synchronize()
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-        d2h = host.numel() * host.element_size()
-        c2.kill()
-    e2e = statistics.median(e2e_ms[1:])  # the first lifecycle of the loop is discarded
+    del core64, b64
+    torch.cuda.empty_cache()
 
     # roofline of the dominant kernel: the fused symmetric far-field sweep
     q4 = 625
@@ -581,6 +637,9 @@ def main():
                        "quirk": "reference quadrature", "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas x{ws}"},
             "time_to_solution_ms": ms,
+            "step_ms": step_ms,
+            "ms_per_step_median": statistics.median(step_ms),
+            "step_factor": factors,
             "assembly_entries_per_s": entries / (va_ms * 1e-3),
             "assembly_ms": va_ms,
             "assembly": "V and K g in one symmetric FP32 far sweep + FP64 near pairs",

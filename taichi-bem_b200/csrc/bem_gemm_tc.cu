@@ -156,15 +156,18 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
                 // complex rows q0, q0+1 of column col: (re, im) of each
                 const int jc = r >> 1;
                 const int q0 = kc / 2 + 2 * k4, col = n0 / 2 + jc;
+                // one 8-byte load per complex value (interleaved re, im; 2 * col is even)
                 rb[h][0] = rb[h][1] = rb[h][2] = rb[h][3] = 0.f;
                 if (2 * col < n_real) {
                     if (2 * q0 < k_real) {
-                        rb[h][0] = Bm[(int64_t)q0 * ldf + 2 * col];
-                        rb[h][1] = Bm[(int64_t)q0 * ldf + 2 * col + 1];
+                        const float2 v = *reinterpret_cast<const float2*>(Bm + (int64_t)q0 * ldf + 2 * col);
+                        rb[h][0] = v.x;
+                        rb[h][1] = v.y;
                     }
                     if (2 * (q0 + 1) < k_real) {
-                        rb[h][2] = Bm[(int64_t)(q0 + 1) * ldf + 2 * col];
-                        rb[h][3] = Bm[(int64_t)(q0 + 1) * ldf + 2 * col + 1];
+                        const float2 v = *reinterpret_cast<const float2*>(Bm + (int64_t)(q0 + 1) * ldf + 2 * col);
+                        rb[h][2] = v.x;
+                        rb[h][3] = v.y;
                     }
                 }
             }
