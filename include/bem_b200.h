@@ -72,7 +72,8 @@ typedef struct {
 typedef struct {
     int n_panels;            /* panels on this side                                 */
     const int32_t* panels;   /* device [n_panels]: global panel index               */
-    int nb;                  /* 1 = P0 (constant), 3 = P1 (hat at each vertex)      */
+    int nb;                  /* 1 = P0 (constant), P1 (hat at each vertex): 3 on a
+                                triangle mesh, 2 on a segment mesh                  */
     const int32_t* dof;      /* device [n_panels*nb]: row/column index, <0 = skipped */
 } bem_space;
 
@@ -91,7 +92,21 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  * gauss_qr on the device, and builds the coincident/edge/vertex pair list.
  * verts (host) [nv*3] double, tris (host) [nt*3] int32.  Synchronous. */
 int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv, int nt, int gauss_qr);
-/* Number of coincident + edge + vertex pairs of the current mesh (ordered). */
+/* 2D variant (the reference's dim = 2 path): line-segment panels.  Replaces
+ * MeshManager.initialization for dim = 2 (mesh_manager.py:74-75,108-113, e.g.
+ * the segments of load_analytical_disk, :520-536) and the 2D branch of
+ * get_panels_relation (mesh_manager.py:544-551).  verts (host) [nv*2] double,
+ * segs (host) [nt*2] int32 (panel p runs from vertex segs[2p] to segs[2p+1]).
+ * Lengths (the 2D "areas") and normals (e.y, -e.x)/|e| are computed here.
+ * Afterwards bem_assemble, bem_apply, bem_assemble_dirichlet, bem_mass and
+ * bem_mesh_geometry (normals [nt*2]) act on the 2D operators
+ * (single_layer_2d.py, double_layer_2d.py, adj_double_layer_2d.py,
+ * hypersingular_layer_2d.py, identity_layer_2d.py, rhs_constructor_2d.py),
+ * always in FP64; P1 spaces have nb = 2; bem_adjoint_vertices is 3D only.
+ * Synchronous. */
+int bem_mesh_set_2d(bem_ctx* ctx, const double* verts, const int32_t* segs, int nv, int nt, int gauss_qr);
+/* Number of ordered panel pairs of the current mesh that share a vertex
+ * (coincident + edge + vertex pairs; on a 2D mesh, coincident + vertex). */
 int64_t bem_near_pair_count(const bem_ctx* ctx);
 /* Copies the per-panel areas [nt] and unit normals [nt*3] (device pointers). */
 int bem_mesh_geometry(const bem_ctx* ctx, double* areas, double* normals, void* stream);

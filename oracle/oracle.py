@@ -154,22 +154,31 @@ def mass(verts, tris, Q, panels, nbx, test_dof, nby, trial_dof, out=None, out_t=
 # Mesh + BVP restatement (mesh_manager.py)
 # ---------------------------------------------------------------------------
 class Mesh:
-    def __init__(self, vertices, panels, boundary="Dirichlet", Q_Neumann=0, Q_Dirichlet=1, transmission=False):
+    def __init__(self, vertices, panels, boundary="Dirichlet", Q_Neumann=0, Q_Dirichlet=1, transmission=False,
+                 dim=3):
+        d = self.dim = int(dim)
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
-        self.panels = np.ascontiguousarray(panels, dtype=np.int32).reshape(-1, 3)
+        self.panels = np.ascontiguousarray(panels, dtype=np.int32).reshape(-1, d)
         self.nv = len(self.vertices)
         self.nt = len(self.panels)
         self.Q_N, self.Q_D = int(Q_Neumann), int(Q_Dirichlet)
         v, f = self.vertices, self.panels
-        cr = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 1]])
-        nrm = np.linalg.norm(cr, axis=1)
-        self.panel_areas = 0.5 * nrm
-        self.panel_normals = cr / nrm[:, None]
+        if d == 2:
+            # segment length and normal (e.y, -e.x)/|e| (mesh_manager.py:108-113)
+            e = v[f[:, 1]] - v[f[:, 0]]
+            self.panel_areas = np.linalg.norm(e, axis=1)
+            cr = np.stack([e[:, 1], -e[:, 0]], axis=1)
+            self.panel_normals = cr / np.linalg.norm(cr, axis=1)[:, None]
+        else:
+            cr = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 1]])
+            nrm = np.linalg.norm(cr, axis=1)
+            self.panel_areas = 0.5 * nrm
+            self.panel_normals = cr / nrm[:, None]
         self.vert_areas = np.zeros(self.nv)
-        self.vert_normals = np.zeros((self.nv, 3))
-        for i in range(self.nt * 3):
-            self.vert_areas[f.reshape(-1)[i]] += self.panel_areas[i // 3] / 3.0
-            self.vert_normals[f.reshape(-1)[i]] += self.panel_normals[i // 3]
+        self.vert_normals = np.zeros((self.nv, d))
+        for i in range(self.nt * d):
+            self.vert_areas[f.reshape(-1)[i]] += self.panel_areas[i // d] / float(d)
+            self.vert_normals[f.reshape(-1)[i]] += self.panel_normals[i // d]
         self.vert_normals /= np.linalg.norm(self.vert_normals, axis=1)[:, None]
         if boundary == "Full" or transmission:
             self._full()
@@ -225,8 +234,9 @@ class Mesh:
         mapN = np.full(self.nv, -1, np.int32)
         mapD = np.full(self.nv, -1, np.int32)
         nD = nN = 0
+        d = self.dim
         for i in range(self.nt):
-            y = (v[f[i, 0], 1] + v[f[i, 1], 1] + v[f[i, 2], 1]) / 3.0
+            y = sum(v[f[i, j], 1] for j in range(d)) / float(d)
             if y > 0:
                 nN += 1
                 pt[i] = NEUMANN
@@ -236,7 +246,7 @@ class Mesh:
         nvN = nvD = 0
         for i in range(self.nt):
             if pt[i] == NEUMANN:
-                for j in range(3):
+                for j in range(d):
                     a = f[i, j]
                     if vt[a] == -1:
                         vt[a] = V_NEUMANN
@@ -244,25 +254,25 @@ class Mesh:
                         nvN += 1
         for i in range(self.nt):
             if pt[i] == DIRICHLET:
-                for j in range(3):
+                for j in range(d):
                     a = f[i, j]
                     if vt[a] == -1:
                         vt[a] = V_DIRICHLET
                         mapD[a] = nvD
                         nvD += 1
         for i in range(self.nt):
-            ds = sum(1 for j in range(3) if vt[f[i, j]] == V_DIRICHLET)
-            ns = sum(1 for j in range(3) if vt[f[i, j]] == V_NEUMANN)
+            ds = sum(1 for j in range(d) if vt[f[i, j]] == V_DIRICHLET)
+            ns = sum(1 for j in range(d) if vt[f[i, j]] == V_NEUMANN)
             t = pt[i]
-            if ns == 3 and t == DIRICHLET:
+            if ns == d and t == DIRICHLET:
                 pt[i] = NEUMANN
                 nD -= 1
                 nN += 1
-            elif ds == 3 and t == NEUMANN:
+            elif ds == d and t == NEUMANN:
                 pt[i] = DIRICHLET
                 nD += 1
                 nN -= 1
-            elif ns != 3 and ds != 3:
+            elif ns != d and ds != d:
                 if t == NEUMANN:
                     nN -= 1
                 elif t == DIRICHLET:
@@ -331,7 +341,7 @@ class Mesh:
         local panel loop of that side, with BOTH_TOBESOLVED read as
         ``as_type`` and the charge index of each basis function."""
         idx = self.loop(side)
-        nb = 1 if Q == 0 else 3
+        nb = 1 if Q == 0 else self.dim
         dof = np.full(len(idx) * nb, -1, np.int32)
         for li, gp in enumerate(idx):
             pt = self.panel_types[gp]
@@ -345,7 +355,7 @@ class Mesh:
         """(panels, nb, dof) where dof is the index into the boundary-data
         field (P0: global panel, P1: global vertex), used by apply_*_boundary."""
         idx = self.loop(side)
-        nb = 1 if Q == 0 else 3
+        nb = 1 if Q == 0 else self.dim
         dof = np.zeros(len(idx) * nb, np.int32)
         for li, gp in enumerate(idx):
             for b in range(nb):
@@ -359,8 +369,9 @@ class Mesh:
 class Problem:
     """FP64 restatement of BEMManager for one simulation_parameters dict.
 
-    fD(x[m,3], sqrt_n) and fN(x[m,3], n[m,3], sqrt_n) are vectorised numpy
-    callables returning real (Laplace) or complex (Helmholtz) arrays.
+    fD(x[m,dim], sqrt_n) and fN(x[m,dim], n[m,dim], sqrt_n) are vectorised
+    numpy callables returning real (Laplace) or complex (Helmholtz) arrays.
+    params["dim"] = 2 selects the segment-mesh operators (oracle2d).
     quirk=True reproduces the reference bit-for-bit in structure; quirk=False
     uses the corrected near-field orientation/basis and g instead of conj(g).
     """
@@ -377,14 +388,29 @@ class Problem:
         self.Q = int(p["GaussQR"])
         self.scope = INTERIOR if p.get("scope", "Interior") == "Interior" else EXTERIOR
         self.quirk = quirk
+        self.dim = int(p.get("dim", 3))
         self.mesh = Mesh(vertices, panels, p["boundary"], p.get("Q_Neumann", 0), p.get("Q_Dirichlet", 1),
-                         self.transmission)
+                         self.transmission, dim=self.dim)
         self.fD, self.fN = fD, fN
         m = self.mesh
         self.n = m.N_N + m.M_D
         self.D_off = 0
         self.N_off = m.M_D
         self.dtype = np.complex128 if self.helm else np.float64
+
+    def _assemble(self, verts, panels, op, helm, k, k2, Q, quirk, test, trial, **kw):
+        if self.dim == 2:
+            from . import oracle2d
+            oracle2d.assemble(verts, panels, op, helm, k, k2, Q, test, trial, **kw)
+        else:
+            assemble(verts, panels, op, helm, k, k2, Q, quirk, test, trial, **kw)
+
+    def _mass(self, verts, panels, Q, *args, **kw):
+        if self.dim == 2:
+            from . import oracle2d
+            oracle2d.mass(verts, panels, Q, *args, **kw)
+        else:
+            mass(verts, panels, Q, *args, **kw)
 
     # -- forward (matrix_layer_forward) ----------------------------------------
     def _kk(self, sqrt_n):
@@ -400,17 +426,17 @@ class Problem:
         if m.N_N > 0:
             V = np.zeros((m.N_N, m.N_N), self.dtype)
             sN = m.side("N", m.Q_N, NEUMANN)
-            assemble(*args, OP_V, self.helm, k, k2, self.Q, self.quirk, sN, sN, out=V)
+            self._assemble(*args, OP_V, self.helm, k, k2, self.Q, self.quirk, sN, sN, out=V)
             out["V"] = V
         if m.N_N > 0 and m.M_D > 0:
             K = np.zeros((m.N_N, m.M_D), self.dtype)
-            assemble(*args, OP_K, self.helm, k, k2, self.Q, self.quirk, m.side("N", m.Q_N, NEUMANN),
-                     m.side("D", m.Q_D, DIRICHLET), out=K)
+            self._assemble(*args, OP_K, self.helm, k, k2, self.Q, self.quirk, m.side("N", m.Q_N, NEUMANN),
+                           m.side("D", m.Q_D, DIRICHLET), out=K)
             out["K"] = K
         if m.M_D > 0:
             W = np.zeros((m.M_D, m.M_D), self.dtype)
             sD = m.side("D", m.Q_D, DIRICHLET)
-            assemble(*args, OP_W, self.helm, k, k2, self.Q, self.quirk, sD, sD, out=W)
+            self._assemble(*args, OP_W, self.helm, k, k2, self.Q, self.quirk, sD, sD, out=W)
             out["W"] = W
         return out
 
@@ -429,8 +455,8 @@ class Problem:
     def add_identity(self, A, c):
         """IdentityLayer3d.matA_add_global_Identity_matrix (identity_layer_3d.py:148-196)."""
         m = self.mesh
-        nbN = 1 if m.Q_N == 0 else 3
-        nbD = 1 if m.Q_D == 0 else 3
+        nbN = 1 if m.Q_N == 0 else self.dim
+        nbD = 1 if m.Q_D == 0 else self.dim
         rows = np.zeros(m.nt * nbN, np.int32)
         cols = np.zeros(m.nt * nbD, np.int32)
         panels = np.zeros(m.nt, np.int32)
@@ -444,7 +470,8 @@ class Problem:
         Ablk = np.zeros((self.n, self.n), self.dtype)
         rows_o = np.where(rows >= 0, rows + self.N_off, -1).astype(np.int32)
         cols_o = np.where(cols >= 0, cols + self.D_off, -1).astype(np.int32)
-        mass(m.vertices, m.panels, self.Q, panels, nbN, rows_o, nbD, cols_o, out=Ablk, out_t=Ablk, scale=c, scale_t=c)
+        self._mass(m.vertices, m.panels, self.Q, panels, nbN, rows_o, nbD, cols_o, out=Ablk, out_t=Ablk, scale=c,
+                   scale_t=c)
         A += Ablk
 
     # -- boundary data (RHSConstructor3d.set_boundaries) -----------------------
@@ -454,21 +481,25 @@ class Problem:
         self.Db = np.zeros(m.nt if m.Q_D == 0 else m.nv, self.dtype)
         self.Nb = np.zeros(m.nt if m.Q_N == 0 else m.nv, self.dtype)
         self.fb = np.zeros(self.n, self.dtype)
-        cent = (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
+        cent = v[f].sum(axis=1) / float(self.dim)
+        # exterior normal of the transmission data: n in 3D (get_panel_normal
+        # ignores the scope, BEM_manager.py:330-335), -n in 2D
+        # (rhs_constructor_2d.py:70,84)
+        es = -1.0 if self.dim == 2 else 1.0
         if self.transmission:
             si, so = self.sqrt_ni, self.sqrt_no
             if m.Q_N == 0:
                 for li, gp in enumerate(m.loop("N")):
                     x, nrm = cent[gp:gp + 1], m.panel_normals[gp:gp + 1]
                     self.Nb[gp] += self.fN(x, nrm, si)[0]
-                    self.fb[self.N_off + li] += self.fN(x, nrm, si)[0] - self.fN(x, nrm, so)[0]
+                    self.fb[self.N_off + li] += self.fN(x, nrm, si)[0] - self.fN(x, es * nrm, so)[0]
             else:
                 for gv in range(m.nv):
                     if m.vert_types[gv] in (V_BOTH, V_NEUMANN):
                         lv = m.vert_local("N", gv)
                         x, nrm = v[gv:gv + 1], m.vert_normals[gv:gv + 1]
                         self.Nb[gv] += self.fN(x, nrm, si)[0]
-                        self.fb[self.N_off + lv] += self.fN(x, nrm, si)[0] - self.fN(x, nrm, so)[0]
+                        self.fb[self.N_off + lv] += self.fN(x, nrm, si)[0] - self.fN(x, es * nrm, so)[0]
             if m.Q_D == 0:
                 for li, gp in enumerate(m.loop("D")):
                     x = cent[gp:gp + 1]
@@ -508,7 +539,7 @@ class Problem:
         # multiply_identity_to_vector (rhs_constructor_3d.py:256-359)
         if m.N_N > 0:
             panels, nbx, rdof = m.side("N", m.Q_N, NEUMANN)
-            nby = 1 if m.Q_D == 0 else 3
+            nby = 1 if m.Q_D == 0 else self.dim
             cdof = np.zeros(len(panels) * nby, np.int32)
             for li in range(len(panels)):
                 pt = m.panel_types[panels[li]]
@@ -517,10 +548,10 @@ class Problem:
                     cdof[li * nby + b] = m.charge_global(m.Q_D, li, b if m.Q_D == 1 else -1, pt)
             rows = np.where(rdof >= 0, rdof + self.N_off, -1).astype(np.int32)
             cdof = np.where(cdof >= 0, cdof, -1).astype(np.int32)
-            mass(v, f, self.Q, panels, nbx, rows, nby, cdof, x=self.Db, y=rhs, scale=half, conj_x=conj)
+            self._mass(v, f, self.Q, panels, nbx, rows, nby, cdof, x=self.Db, y=rhs, scale=half, conj_x=conj)
         if m.M_D > 0:
             panels, nbx, rdof = m.side("D", m.Q_D, DIRICHLET)
-            nby = 1 if m.Q_N == 0 else 3
+            nby = 1 if m.Q_N == 0 else self.dim
             cdof = np.zeros(len(panels) * nby, np.int32)
             for li in range(len(panels)):
                 pt = m.panel_types[panels[li]]
@@ -528,24 +559,25 @@ class Problem:
                 for b in range(nby):
                     cdof[li * nby + b] = m.charge_global(m.Q_N, li, b if m.Q_N == 1 else -1, pt)
             rows = np.where(rdof >= 0, rdof + self.D_off, -1).astype(np.int32)
-            mass(v, f, self.Q, panels, nbx, rows, nby, cdof, x=self.Nb, y=rhs, scale=half, conj_x=conj)
+            self._mass(v, f, self.Q, panels, nbx, rows, nby, cdof, x=self.Nb, y=rhs, scale=half, conj_x=conj)
         # multiply_M_to_vector (rhs_constructor_3d.py:361-372)
         if m.N_N > 0:
             tp, nbx, tdof = m.side("N", m.Q_N, NEUMANN)
             rows = np.where(tdof >= 0, tdof + self.N_off, -1).astype(np.int32)
-            assemble(v, f, OP_K, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows), m.side_global("N", m.Q_D),
-                     x=self.Db, y=rhs, scale=1.0, conj_x=conj)
+            self._assemble(v, f, OP_K, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows), m.side_global("N", m.Q_D),
+                           x=self.Db, y=rhs, scale=1.0, conj_x=conj)
             if m.nP_D > 0:
-                assemble(v, f, OP_V, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows),
-                         m.side_global("D", m.Q_N), x=self.Nb, y=rhs, scale=-1.0, conj_x=conj)
+                self._assemble(v, f, OP_V, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows),
+                               m.side_global("D", m.Q_N), x=self.Nb, y=rhs, scale=-1.0, conj_x=conj)
         if m.M_D > 0:
             tp, nbx, tdof = m.side("D", m.Q_D, DIRICHLET)
             rows = np.where(tdof >= 0, tdof + self.D_off, -1).astype(np.int32)
-            assemble(v, f, OP_KP, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows), m.side_global("D", m.Q_N),
-                     x=self.Nb, y=rhs, scale=-1.0, conj_x=conj)
+            # the 2D K' product multiplies by f, not conj(f) (adj_double_layer_2d.py:344)
+            self._assemble(v, f, OP_KP, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows), m.side_global("D", m.Q_N),
+                           x=self.Nb, y=rhs, scale=-1.0, conj_x=conj and self.dim == 3)
             if m.nP_N > 0:
-                assemble(v, f, OP_W, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows),
-                         m.side_global("N", m.Q_D), x=self.Db, y=rhs, scale=-1.0, conj_x=conj)
+                self._assemble(v, f, OP_W, self.helm, k, k2, self.Q, self.quirk, (tp, nbx, rows),
+                               m.side_global("N", m.Q_D), x=self.Db, y=rhs, scale=-1.0, conj_x=conj)
         return rhs
 
     def run(self):

@@ -11,6 +11,16 @@ follow the reference operator by operator:
   HypersingularLayer3d  src/BEM_functions/hypersingular_layer/hypersingular_layer_3d.py:437-565
   IdentityLayer3d       src/BEM_functions/identity_layer/identity_layer_3d.py:148-196
   RHSConstructor3d      src/BEM_functions/rhs_constructor/rhs_constructor_3d.py:50-386
+
+and the 2D classes (`*2d`, the reference's *_2d.py modules), which run the
+same panel loops on segment panels (P1 spaces with two hats per panel):
+
+  SingleLayer2d         single_layer/single_layer_2d.py:217-341
+  DoubleLayer2d         double_layer/double_layer_2d.py:219-342
+  AdjDoubleLayer2d      adj_double_layer/adj_double_layer_2d.py:220-344
+  HypersingularLayer2d  hypersingular_layer/hypersingular_layer_2d.py:253-377
+  IdentityLayer2d       identity_layer/identity_layer_2d.py:120-161
+  RHSConstructor2d      rhs_constructor/rhs_constructor_2d.py:50-379
 """
 from __future__ import annotations
 
@@ -31,7 +41,7 @@ class _Layer:
         self._BEM_manager = BEM_manager
         b = BEM_manager
         self._GaussQR = b._GaussQR
-        self._dim = 3
+        self._dim = b._dim
         self._n = b._n
         self.N_Neumann = b.N_Neumann
         self.M_Dirichlet = b.M_Dirichlet
@@ -131,6 +141,9 @@ class DoubleLayer3d(_Layer):
 class AdjDoubleLayer3d(_Layer):
     """K' is only used matrix-free; its forward is a no-op in the reference
     (adj_double_layer_3d.py:383) and the block system uses -K^T instead."""
+    # whether the product takes conj(f), as the other operators do with quirk
+    # (adj_double_layer_3d.py:506); the 2D operator multiplies by f itself
+    _conj_data = True
 
     def __init__(self, BEM_manager):
         super().__init__(BEM_manager)
@@ -149,7 +162,7 @@ class AdjDoubleLayer3d(_Layer):
         trial = b.space("data", self._Q_Neumann, "D")
         rc = b.rhs_constructor
         b.engine.apply(self._desc(L.OP_KP, k, sqrt_n), test, trial, rc._Neumann_boundary, rc._rhs_vec,
-                       scale=multiplier, conj_x=b.conj_data)
+                       scale=multiplier, conj_x=b.conj_data and self._conj_data)
 
 
 class HypersingularLayer3d(_Layer):
@@ -202,6 +215,11 @@ class IdentityLayer3d(_Layer):
 
 
 class RHSConstructor3d(_Layer):
+    # normal of the exterior trace in the transmission data: the 3D reference
+    # takes get_panel_normal(..., EXTERIOR), which returns the same normal
+    # (BEM_manager.py:330-335, rhs_constructor_3d.py:69-70)
+    _ext_sign = 1.0
+
     def __init__(self, BEM_manager):
         super().__init__(BEM_manager)
         b = BEM_manager
@@ -238,7 +256,7 @@ class RHSConstructor3d(_Layer):
         self._Dirichlet_boundary.zero_()
         self._Neumann_boundary.zero_()
         self._f_boundary.zero_()
-        cent = lambda: (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
+        cent = lambda: v[f].sum(axis=1) / float(self._dim)
         No, Do = b._Neumann_offset_j, b._Dirichlet_offset_j
         fD, fN = self.analytical_function_Dirichlet, self.analytical_function_Neumann
         if b._is_transmission:
@@ -246,7 +264,7 @@ class RHSConstructor3d(_Layer):
                 gp = mm.loop_panels("N")
                 x, nrm = C(("bd_cent", "N"), lambda: cent()[gp]), C(("bd_pn", "N"), lambda: mm.panel_normals[gp])
                 fi = self._eval(fN, x, nrm, sqrt_ni)
-                fo = self._eval(fN, x, nrm, sqrt_no)
+                fo = self._eval(fN, x, nrm if self._ext_sign > 0 else -nrm, sqrt_no)
                 self._Neumann_boundary[C(("bd_gp", "N"), lambda: gp.astype(np.int64))] += fi
                 self._f_boundary[No:No + len(gp)] += fi - fo
             else:
@@ -254,7 +272,7 @@ class RHSConstructor3d(_Layer):
                 loc = mm._vert_local("N", vv)
                 x, nrm = C(("bd_v", "N"), lambda: v[vv]), C(("bd_vn", "N"), lambda: mm.vert_normals[vv])
                 fi = self._eval(fN, x, nrm, sqrt_ni)
-                fo = self._eval(fN, x, nrm, sqrt_no)
+                fo = self._eval(fN, x, nrm if self._ext_sign > 0 else -nrm, sqrt_no)
                 self._Neumann_boundary[C(("bd_vv", "N"), lambda: vv)] += fi
                 self._f_boundary[C(("bd_loc", "N"), lambda: (No + loc).astype(np.int64))] += fi - fo
             if self._Q_Dirichlet == 0:
@@ -339,3 +357,43 @@ class RHSConstructor3d(_Layer):
         self._Dirichlet_boundary = None
         self._Neumann_boundary = None
         self._f_boundary = None
+
+
+# ---------------------------------------------------------------------------
+# 2D (segment panels).  The host logic is the 3D classes'; the library
+# evaluates the 2D integrands on a mesh set with bem_mesh_set_2d.
+# ---------------------------------------------------------------------------
+class SingleLayer2d(SingleLayer3d):
+    rank = 2
+
+
+class DoubleLayer2d(DoubleLayer3d):
+    rank = 2
+
+
+class AdjDoubleLayer2d(AdjDoubleLayer3d):
+    """K' f with f itself, not conj(f), in the Helmholtz product
+    (adj_double_layer_2d.py:344)."""
+    rank = 2
+    _conj_data = False
+
+
+class HypersingularLayer2d(HypersingularLayer3d):
+    rank = 2
+
+
+class IdentityLayer2d(IdentityLayer3d):
+    """Transmission identity block.  identity_layer_2d.py:154-158 calls
+    integrate_on_single_panel without its `rands` argument (a TypeError in
+    Python, a compile error in Taichi); this class integrates with the Gauss
+    point of each loop iteration, as the loop over `iii` intends."""
+    rank = 2
+
+
+class RHSConstructor2d(RHSConstructor3d):
+    """Boundary data on segment panels.  In the transmission data the 2D
+    reference takes the exterior normal as -n (rhs_constructor_2d.py:70,84;
+    its lines 72 and 86 pass an undefined `normal_x`, read here as the
+    interior normal as in the 3D constructor)."""
+    rank = 2
+    _ext_sign = -1.0

@@ -34,7 +34,7 @@ EXPORTS = [
     "bem_near_pair_count", "bem_mesh_geometry", "bem_assemble", "bem_apply", "bem_mass", "bem_lu_factor",
     "bem_lu_solve", "bem_gemv", "bem_refine_solve", "bem_measure_peaks", "bem_lu_dinv_elems",
     "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet", "bem_lu_solve_tiled_static",
-    "bem_adjoint_vertices",
+    "bem_adjoint_vertices", "bem_mesh_set_2d",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 
@@ -74,6 +74,7 @@ def load():
     L.bem_launch_count.argtypes = [vp]
     L.bem_launch_count.restype = i64
     L.bem_mesh_set.argtypes = [vp, vp, vp, i32, i32, i32]
+    L.bem_mesh_set_2d.argtypes = [vp, vp, vp, i32, i32, i32]
     L.bem_near_pair_count.argtypes = [vp]
     L.bem_near_pair_count.restype = i64
     L.bem_mesh_geometry.argtypes = [vp, vp, vp, vp]

@@ -87,6 +87,7 @@ class Engine:
         self.ctx = h
         self.nt = self.nv = 0
         self.Q = 0
+        self.dim = 3
 
     def close(self):
         if getattr(self, "ctx", None):
@@ -108,12 +109,17 @@ class Engine:
         return int(self.lib.bem_launch_count(self.ctx))
 
     # -- mesh ---------------------------------------------------------------
-    def set_mesh(self, vertices, panels, gauss_qr: int):
-        v = np.ascontiguousarray(np.asarray(vertices, dtype=np.float64).reshape(-1, 3))
-        f = np.ascontiguousarray(np.asarray(panels, dtype=np.int32).reshape(-1, 3))
+    def set_mesh(self, vertices, panels, gauss_qr: int, dim: int = 3):
+        """Upload a triangle mesh (dim 3: vertices [nv,3], panels [nt,3]) or a
+        segment mesh (dim 2: vertices [nv,2], panels [nt,2])."""
+        if dim not in (2, 3):
+            raise ValueError("dim must be 2 or 3")
+        v = np.ascontiguousarray(np.asarray(vertices, dtype=np.float64).reshape(-1, dim))
+        f = np.ascontiguousarray(np.asarray(panels, dtype=np.int32).reshape(-1, dim))
+        fn = self.lib.bem_mesh_set if dim == 3 else self.lib.bem_mesh_set_2d
         with torch.cuda.device(self.device):
-            self._check(self.lib.bem_mesh_set(self.ctx, v.ctypes.data, f.ctypes.data, len(v), len(f), int(gauss_qr)))
-        self.nv, self.nt, self.Q = len(v), len(f), int(gauss_qr)
+            self._check(fn(self.ctx, v.ctypes.data, f.ctypes.data, len(v), len(f), int(gauss_qr)))
+        self.nv, self.nt, self.Q, self.dim = len(v), len(f), int(gauss_qr), dim
         self.vertices_host, self.panels_host = v, f
 
     @property
@@ -122,7 +128,7 @@ class Engine:
 
     def geometry(self):
         areas = torch.empty(self.nt, dtype=torch.float64, device=self.device)
-        normals = torch.empty(self.nt, 3, dtype=torch.float64, device=self.device)
+        normals = torch.empty(self.nt, self.dim, dtype=torch.float64, device=self.device)
         self._check(self.lib.bem_mesh_geometry(self.ctx, _ptr(areas), _ptr(normals), _stream_ptr()))
         return areas, normals
 

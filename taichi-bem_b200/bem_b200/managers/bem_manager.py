@@ -28,8 +28,9 @@ import numpy as np
 import torch
 
 from .. import _lib as L
-from ..BEM_functions.layers import (AdjDoubleLayer3d, DoubleLayer3d, HypersingularLayer3d, IdentityLayer3d,
-                                    RHSConstructor3d, SingleLayer3d)
+from ..BEM_functions.layers import (AdjDoubleLayer2d, AdjDoubleLayer3d, DoubleLayer2d, DoubleLayer3d,
+                                    HypersingularLayer2d, HypersingularLayer3d, IdentityLayer2d, IdentityLayer3d,
+                                    RHSConstructor2d, RHSConstructor3d, SingleLayer2d, SingleLayer3d)
 from ..engine import DeviceSpace, Engine, gmres_ir
 from ..utils.types import AssembleType, CellFluxType, KernelType, ScopeType, VertAttachType
 
@@ -123,7 +124,7 @@ class BEMManager:
         if n <= 0:
             raise AssertionError("no unknowns")
         self.engine = Engine(self.device)
-        self.engine.set_mesh(mm.vertices, mm.panels, self._GaussQR)
+        self.engine.set_mesh(mm.vertices, mm.panels, self._GaussQR, dim=self._dim)
         self._spaces = {}
         self._dev_cache = {}
         z = lambda *s: torch.zeros(*s, dtype=self.torch_dtype, device=self.device)
@@ -133,12 +134,21 @@ class BEMManager:
         self.raw_analytical_solved = z(n)
         self.solved = z(self.num_of_vertices)
         self.analytical_solved = z(self.num_of_vertices)
-        self.identity_layer = IdentityLayer3d(self)
-        self.single_layer = SingleLayer3d(self)
-        self.double_layer = DoubleLayer3d(self)
-        self.adj_double_layer = AdjDoubleLayer3d(self)
-        self.hypersingular_layer = HypersingularLayer3d(self)
-        self.rhs_constructor = RHSConstructor3d(self)
+        # BIO objects of the mesh's dimension (BEM_manager.py:175-191)
+        if self._dim == 2:
+            self.identity_layer = IdentityLayer2d(self)
+            self.single_layer = SingleLayer2d(self)
+            self.double_layer = DoubleLayer2d(self)
+            self.adj_double_layer = AdjDoubleLayer2d(self)
+            self.hypersingular_layer = HypersingularLayer2d(self)
+            self.rhs_constructor = RHSConstructor2d(self)
+        else:
+            self.identity_layer = IdentityLayer3d(self)
+            self.single_layer = SingleLayer3d(self)
+            self.double_layer = DoubleLayer3d(self)
+            self.adj_double_layer = AdjDoubleLayer3d(self)
+            self.hypersingular_layer = HypersingularLayer3d(self)
+            self.rhs_constructor = RHSConstructor3d(self)
         self.initialized = True
 
     def space(self, kind: str, Q: int, side: str, as_type: int = 0, offset: int = 0) -> DeviceSpace:
@@ -364,7 +374,7 @@ class BEMManager:
             self.raw_analytical_solved[No:No + min(nN, self.N_Neumann)] = rc._Neumann_boundary[:self.N_Neumann]
             return
         C = self.cached
-        cent = lambda: (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0
+        cent = lambda: v[f].sum(axis=1) / float(self._dim)
         if self.N_Neumann > 0:
             if self.shape_func_degree_Neumann == 0:
                 gp = mm.loop_panels("N")
@@ -404,8 +414,9 @@ class BEMManager:
                 return
             ok = mm.panel_types[gp] != excluded
             gsel = gp[ok]
-            # per-panel weight area/3 / vertex area, the panel's vertices and DOF rows
-            w = C(("sp_w", side), lambda: (mm.panel_areas[gsel] / 3.0)[:, None] / mm.vert_areas[mm.panels[gsel]])
+            # per-panel weight area/dim / vertex area, the panel's vertices and DOF rows
+            w = C(("sp_w", side), lambda: (mm.panel_areas[gsel] / float(self._dim))[:, None]
+                  / mm.vert_areas[mm.panels[gsel]])
             fv = C(("sp_f", side), lambda: mm.panels[gsel].reshape(-1).astype(np.int64))
             rows = C(("sp_rows", side, offset), lambda: np.arange(len(gp))[ok] + offset)
             for src, dst in ((self.raw_solved, self.solved), (self.raw_analytical_solved, self.analytical_solved)):

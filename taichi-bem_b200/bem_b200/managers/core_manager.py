@@ -7,9 +7,10 @@ graphics stack and are not part of this build: `vis`, `make_video` and
 `show_wireframe` are accepted and ignored, and the per-vertex results stay in
 device tensors (`BEMManager.solved`, `.analytical_solved`).
 
-Boundary-data callbacks are vectorised: fD(x[m,3] float64 tensor[, sqrt_n])
-and fN(x[m,3], normal[m,3][, sqrt_n]) return m real (Laplace) or complex
-(Helmholtz) values.
+Boundary-data callbacks are vectorised: fD(x[m,dim] float64 tensor[, sqrt_n])
+and fN(x[m,dim], normal[m,dim][, sqrt_n]) return m real (Laplace) or complex
+(Helmholtz) values (dim = 3, or 2 for the reference's 2D path on the
+analytical disk).
 """
 from __future__ import annotations
 
@@ -51,8 +52,8 @@ class CoreManager:
         if "Helmholtz" not in p["kernel"]:
             p["k"] = 0
         self._is_transmission = 1 if ("Full" in p["boundary"] or "Transmission" in p["kernel"]) else 0
-        if int(p.get("dim", 3)) != 3:
-            raise NotImplementedError("bem_b200 implements the 3D operators")
+        if int(p.get("dim", 3)) not in (2, 3):
+            raise NotImplementedError("dim must be 2 or 3")
         self._log_manager = _Log()
         self._mesh_manager = MeshManager(self)
         self._BEM_manager = BEMManager(self)

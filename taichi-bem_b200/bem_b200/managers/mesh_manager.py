@@ -14,7 +14,7 @@ import re
 
 import numpy as np
 
-from ..meshes import icosphere, load_obj, perturbed_sphere
+from ..meshes import analytical_disk, icosphere, load_obj, perturbed_sphere
 from ..utils.types import CellFluxType, VertAttachType
 
 _N = int(CellFluxType.NEUMANN_TOBESOLVED)
@@ -33,8 +33,8 @@ class MeshManager:
         p = core_manager._simulation_parameters
         self._params = p
         self._dim = int(p.get("dim", 3))
-        if self._dim != 3:
-            raise NotImplementedError("bem_b200 implements the 3D operators")
+        if self._dim not in (2, 3):
+            raise NotImplementedError("dim must be 2 or 3")
         self._boundary_type = p["boundary"]
         self._is_transmission = core_manager._is_transmission
         Q_Neumann = int(p.get("Q_Neumann", 0))
@@ -50,6 +50,9 @@ class MeshManager:
         p = self._params
         if p.get("vertices") is not None and p.get("panels") is not None:
             return np.asarray(p["vertices"], np.float64), np.asarray(p["panels"], np.int32)
+        if self._dim == 2:
+            # the reference's 2D meshes are its analytical disk (mesh_manager.py:74-75)
+            return analytical_disk(float(p.get("disk_r", 1.0)), int(p.get("disk_N", 256)))
         obj = str(p["object"])
         m = re.fullmatch(r"icosphere(\d+)", obj)
         if m:
@@ -65,8 +68,9 @@ class MeshManager:
 
     def initialization(self):
         v, f = self._load()
-        if v.ndim != 2 or v.shape[1] != 3 or f.ndim != 2 or f.shape[1] != 3:
-            raise ValueError("vertices must be [nv,3] and panels [nt,3]")
+        d = self._dim
+        if v.ndim != 2 or v.shape[1] != d or f.ndim != 2 or f.shape[1] != d:
+            raise ValueError(f"vertices must be [nv,{d}] and panels [nt,{d}]")
         if not np.isfinite(v).all():
             raise ValueError("non-finite vertex coordinates")
         if f.min() < 0 or f.max() >= len(v):
@@ -75,17 +79,25 @@ class MeshManager:
         self.panels = np.ascontiguousarray(f, np.int32)
         self.num_of_vertices = len(v)
         self.num_of_panels = len(f)
-        # areas/normals with the reference's formulas (mesh_manager.py:114-139)
-        cr = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 1]])
-        nrm = np.linalg.norm(cr, axis=1)
-        if (nrm <= 0).any():
-            raise ValueError(f"degenerate panel {int(np.argmin(nrm))} (zero area)")
-        self.panel_areas = 0.5 * nrm
-        self.panel_normals = cr / nrm[:, None]
+        # areas/normals with the reference's formulas (mesh_manager.py:108-139)
+        if d == 2:
+            e = v[f[:, 1]] - v[f[:, 0]]
+            self.panel_areas = np.linalg.norm(e, axis=1)
+            if (self.panel_areas <= 0).any():
+                raise ValueError(f"degenerate panel {int(np.argmin(self.panel_areas))} (zero length)")
+            cr = np.stack([e[:, 1], -e[:, 0]], axis=1)
+            self.panel_normals = cr / np.linalg.norm(cr, axis=1)[:, None]
+        else:
+            cr = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 1]])
+            nrm = np.linalg.norm(cr, axis=1)
+            if (nrm <= 0).any():
+                raise ValueError(f"degenerate panel {int(np.argmin(nrm))} (zero area)")
+            self.panel_areas = 0.5 * nrm
+            self.panel_normals = cr / nrm[:, None]
         self.vert_areas = np.zeros(self.num_of_vertices)
-        np.add.at(self.vert_areas, f.reshape(-1), np.repeat(self.panel_areas / 3.0, 3))
-        vn = np.zeros((self.num_of_vertices, 3))
-        np.add.at(vn, f.reshape(-1), np.repeat(self.panel_normals, 3, axis=0))
+        np.add.at(self.vert_areas, f.reshape(-1), np.repeat(self.panel_areas / float(d), d))
+        vn = np.zeros((self.num_of_vertices, d))
+        np.add.at(vn, f.reshape(-1), np.repeat(self.panel_normals, d, axis=0))
         self.vert_normals = vn / np.linalg.norm(vn, axis=1)[:, None]
         if self._boundary_type == "Full" or self._is_transmission > 0:
             self.set_full_bvp()
@@ -144,8 +156,8 @@ class MeshManager:
         the rest Neumann data; panels touching both vertex classes become
         MIX_NONRESOLVED (mesh_manager.py:266-389)."""
         f, v = self.panels, self.vertices
-        nt, nv = self.num_of_panels, self.num_of_vertices
-        y = v[f, 1].sum(axis=1) / 3.0
+        nt, nv, d = self.num_of_panels, self.num_of_vertices, self._dim
+        y = v[f, 1].sum(axis=1) / float(d)
         pt = np.where(y > 0, _N, _D).astype(np.int32)
         nN = int((pt == _N).sum())
         nD = nt - nN
@@ -170,15 +182,15 @@ class MeshManager:
             ds = int((vt[f[i]] == _VD).sum())
             ns = int((vt[f[i]] == _VN).sum())
             t = pt[i]
-            if ns == 3 and t == _D:
+            if ns == d and t == _D:
                 pt[i] = _N
                 nD -= 1
                 nN += 1
-            elif ds == 3 and t == _N:
+            elif ds == d and t == _N:
                 pt[i] = _D
                 nD += 1
                 nN -= 1
-            elif ns != 3 and ds != 3:
+            elif ns != d and ds != d:
                 if t == _N:
                     nN -= 1
                 elif t == _D:
@@ -272,8 +284,8 @@ class MeshManager:
         if Q == 0:
             dof = np.where(pt != _MIX, np.arange(n), -1).astype(np.int32).reshape(n, 1)
             return panels, 1, dof
-        dof = np.full((n, 3), -1, np.int32)
-        verts = self.panels[panels]  # [n,3]
+        dof = np.full((n, self._dim), -1, np.int32)
+        verts = self.panels[panels]  # [n, dim]
         vt = self.vertice_types[verts]
         for kind, vside, excluded in ((_N, "N", _VD), (_D, "D", _VN)):
             rows = pt == kind
@@ -281,7 +293,7 @@ class MeshManager:
                 continue
             loc = self._vert_local(vside, verts[rows])
             dof[rows] = np.where(vt[rows] != excluded, loc, -1)
-        return panels, 3, dof
+        return panels, self._dim, dof
 
     def data_dofs(self, Q: int, side: str):
         """Index into the boundary-data field (P0: global panel, P1: global
@@ -290,7 +302,7 @@ class MeshManager:
         panels = self.loop_panels(side)
         if Q == 0:
             return panels, 1, panels.reshape(-1, 1).copy()
-        return panels, 3, self.panels[panels].copy()
+        return panels, self._dim, self.panels[panels].copy()
 
     def global_charge(self, Q: int, side: str, panel_type_as: int):
         """proj_from_local_panel_index_to_global_charge_index (BEM_manager.py:279-310)
@@ -298,7 +310,7 @@ class MeshManager:
         panels = self.loop_panels(side)
         pt = self.panel_types[panels].copy()
         pt[pt == _BOTH] = panel_type_as
-        nb = 1 if Q == 0 else 3
+        nb = 1 if Q == 0 else self._dim
         out = np.full((len(panels), nb), -1, np.int32)
         for kind, s in ((_N, "N"), (_D, "D")):
             rows = pt == kind

@@ -109,3 +109,14 @@ def load_obj(path: str, normalise: bool = True):
         v = v - v.mean(axis=0, keepdims=True)
         v = v * (1.0 / np.abs(v).max())
     return v, np.array(faces, dtype=np.int32)
+
+
+def analytical_disk(r: float = 1.0, N: int = 256):
+    """Boundary of the disk of radius r as N segments, counter-clockwise
+    (MeshManager.load_analytical_disk, src/managers/mesh_manager.py:520-536):
+    vertex i at angle 2 pi i / N, segment i from vertex i to vertex (i+1) % N.
+    Returns (vertices [N,2] float64, panels [N,2] int32)."""
+    ang = [2.0 * math.pi * i / N for i in range(N)]
+    v = np.array([[r * math.cos(a) for a in ang], [r * math.sin(a) for a in ang]], dtype=np.float64).T
+    f = np.array([[i, (i + 1) % N] for i in range(N)], dtype=np.int32)
+    return np.ascontiguousarray(v), f

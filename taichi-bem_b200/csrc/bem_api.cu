@@ -103,14 +103,15 @@ int near_perm(const int32_t* a, const int32_t* b, int rel) {
 void free_mesh(bem_ctx* ctx) {
     void* ptrs[] = {ctx->verts, ctx->tris, ctx->area, ctx->normal, ctx->centroid, ctx->curl, ctx->pts64,
                     ctx->pts32, ctx->phi64, ctx->phi32, ctx->gp, ctx->gw, ctx->near, ctx->test_local,
-                    ctx->trial_local};
+                    ctx->trial_local, ctx->seg2, ctx->nrm2};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     ctx->verts = nullptr; ctx->tris = nullptr; ctx->area = nullptr; ctx->normal = nullptr;
     ctx->centroid = nullptr; ctx->curl = nullptr; ctx->pts64 = nullptr; ctx->pts32 = nullptr;
     ctx->phi64 = nullptr; ctx->phi32 = nullptr; ctx->gp = nullptr; ctx->gw = nullptr; ctx->near = nullptr;
-    ctx->test_local = nullptr; ctx->trial_local = nullptr;
+    ctx->test_local = nullptr; ctx->trial_local = nullptr; ctx->seg2 = nullptr; ctx->nrm2 = nullptr;
     ctx->nv = ctx->nt = ctx->Q = ctx->Q2 = 0;
+    ctx->dim = 3;
     ctx->n_near = 0;
 }
 
@@ -123,7 +124,10 @@ int check_space(bem_ctx* ctx, const bem_space* sp, const char* name) {
     if (!sp) return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " space is NULL");
     if (sp->n_panels < 0 || (sp->n_panels > 0 && (!sp->panels || !sp->dof)))
         return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " space has no panel/dof arrays");
-    if (sp->nb != 1 && sp->nb != 3) return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " nb must be 1 or 3");
+    if (ctx->dim == 3 && sp->nb != 1 && sp->nb != 3)
+        return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " nb must be 1 or 3");
+    if (ctx->dim == 2 && sp->nb != 1 && sp->nb != 2)
+        return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " nb must be 1 or 2 on a 2D mesh");
     if (sp->n_panels > ctx->nt) return bem_fail(ctx, BEM_ERR_INVALID, std::string(name) + " has more panels than the mesh");
     return BEM_OK;
 }
@@ -299,6 +303,78 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
     return BEM_OK;
 }
 
+int bem_mesh_set_2d(bem_ctx* ctx, const double* verts, const int32_t* segs, int nv, int nt, int gauss_qr) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!verts || !segs || nv <= 0 || nt <= 0) return bem_fail(ctx, BEM_ERR_INVALID, "empty mesh");
+    if (gauss_qr < 1 || gauss_qr > BEM_MAX_Q) return bem_fail(ctx, BEM_ERR_INVALID, "GaussQR must be in 1..12");
+    for (int64_t i = 0; i < 2LL * nv; ++i)
+        if (!std::isfinite(verts[i])) return bem_fail(ctx, BEM_ERR_MESH, "non-finite vertex coordinate");
+    for (int64_t i = 0; i < 2LL * nt; ++i)
+        if (segs[i] < 0 || segs[i] >= nv) return bem_fail(ctx, BEM_ERR_MESH, "panel vertex index out of range");
+    // length and normal (e.y, -e.x)/|e| of each segment, mesh_manager.py:108-113
+    std::vector<double> len(nt), nrm(2 * (size_t)nt);
+    std::vector<double4> seg(nt);
+    for (int p = 0; p < nt; ++p) {
+        const double* a = verts + 2 * segs[2 * p];
+        const double* b = verts + 2 * segs[2 * p + 1];
+        const double ex = b[0] - a[0], ey = b[1] - a[1];
+        const double L = std::sqrt(ex * ex + ey * ey);
+        if (!(L > 0.0) || !std::isfinite(L))
+            return bem_fail(ctx, BEM_ERR_MESH, "degenerate panel " + std::to_string(p) + " (zero length)");
+        len[p] = L;
+        nrm[2 * p] = ey / L;
+        nrm[2 * p + 1] = -ex / L;
+        seg[p] = make_double4(a[0], a[1], b[0], b[1]);
+    }
+    // ordered pairs that the reference integrates with its coincide or
+    // common-vertex branch (get_panels_relation, mesh_manager.py:539-551)
+    std::vector<std::vector<int>> vp(nv);
+    for (int p = 0; p < nt; ++p)
+        for (int c = 0; c < 2; ++c) vp[segs[2 * p + c]].push_back(p);
+    int64_t n_near = 0;
+    std::vector<int> cand;
+    for (int i = 0; i < nt; ++i) {
+        cand.clear();
+        for (int c = 0; c < 2; ++c)
+            for (int j : vp[segs[2 * i + c]]) cand.push_back(j);
+        std::sort(cand.begin(), cand.end());
+        n_near += std::unique(cand.begin(), cand.end()) - cand.begin();
+    }
+
+    free_mesh(ctx);
+    const int Q = gauss_qr;
+    std::vector<double> gp(Q), gw(Q);
+    gauss01(Q, gp.data(), gw.data());
+    int rc = 0;
+    if ((rc = dmalloc(ctx, &ctx->verts, 2 * (size_t)nv)) || (rc = dmalloc(ctx, &ctx->tris, 2 * (size_t)nt)) ||
+        (rc = dmalloc(ctx, &ctx->area, nt)) || (rc = dmalloc(ctx, &ctx->normal, 2 * (size_t)nt)) ||
+        (rc = dmalloc(ctx, &ctx->seg2, nt)) || (rc = dmalloc(ctx, &ctx->nrm2, nt)) ||
+        (rc = dmalloc(ctx, &ctx->gp, Q)) || (rc = dmalloc(ctx, &ctx->gw, Q))) {
+        free_mesh(ctx);
+        return rc;
+    }
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    if ((rc = bem_check_cuda(ctx, cudaMemcpy(ctx->verts, verts, sizeof(double) * 2 * nv, h2d), "upload")) ||
+        (rc = bem_check_cuda(ctx, cudaMemcpy(ctx->tris, segs, sizeof(int32_t) * 2 * nt, h2d), "upload")) ||
+        (rc = bem_check_cuda(ctx, cudaMemcpy(ctx->area, len.data(), sizeof(double) * nt, h2d), "upload")) ||
+        (rc = bem_check_cuda(ctx, cudaMemcpy(ctx->normal, nrm.data(), sizeof(double) * 2 * nt, h2d), "upload")) ||
+        (rc = bem_check_cuda(ctx, cudaMemcpy(ctx->seg2, seg.data(), sizeof(double4) * nt, h2d), "upload")) ||
+        (rc = bem_check_cuda(ctx, cudaMemcpy(ctx->nrm2, nrm.data(), sizeof(double2) * nt, h2d), "upload")) ||
+        (rc = bem_check_cuda(ctx, cudaMemcpy(ctx->gp, gp.data(), sizeof(double) * Q, h2d), "upload")) ||
+        (rc = bem_check_cuda(ctx, cudaMemcpy(ctx->gw, gw.data(), sizeof(double) * Q, h2d), "upload"))) {
+        free_mesh(ctx);
+        return rc;
+    }
+    cudaMemset(ctx->flags, 0, 16 * sizeof(int32_t));
+    ctx->dim = 2;
+    ctx->nv = nv;
+    ctx->nt = nt;
+    ctx->Q = Q;
+    ctx->Q2 = Q * Q;
+    ctx->n_near = n_near;
+    return BEM_OK;
+}
+
 int bem_mesh_geometry(const bem_ctx* cctx, double* areas, double* normals, void* stream) {
     bem_ctx* ctx = const_cast<bem_ctx*>(cctx);
     if (!ctx) return BEM_ERR_INVALID;
@@ -309,7 +385,7 @@ int bem_mesh_geometry(const bem_ctx* cctx, double* areas, double* normals, void*
                                                           cudaMemcpyDeviceToDevice, s), "copy areas"))
             return rc;
     if (normals)
-        if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(normals, ctx->normal, sizeof(double) * 3 * ctx->nt,
+        if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(normals, ctx->normal, sizeof(double) * ctx->dim * ctx->nt,
                                                           cudaMemcpyDeviceToDevice, s), "copy normals"))
             return rc;
     return BEM_OK;
@@ -326,6 +402,9 @@ int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, con
     if (out_dtype != want)
         return bem_fail(ctx, BEM_ERR_INVALID, "out dtype must be BEM_F64 for Laplace and BEM_C128 for Helmholtz");
     if (!out || ld <= 0) return bem_fail(ctx, BEM_ERR_INVALID, "out is NULL or ld <= 0");
+    if (ctx->dim == 2)
+        return bem_launch_assemble2d(ctx, op, test, trial, 0, out, ld, scale, out_t, scale_t, nullptr, nullptr, 0,
+                                     (cudaStream_t)stream);
     return bem_launch_assemble(ctx, op, test, trial, 0, out, ld, scale, out_t, scale_t, nullptr, nullptr, 0,
                                (cudaStream_t)stream);
 }
@@ -341,6 +420,9 @@ int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const 
     if (dtype != want)
         return bem_fail(ctx, BEM_ERR_INVALID, "x/y dtype must be BEM_F64 for Laplace and BEM_C128 for Helmholtz");
     if (!x || !y) return bem_fail(ctx, BEM_ERR_INVALID, "x or y is NULL");
+    if (ctx->dim == 2)
+        return bem_launch_assemble2d(ctx, op, test, trial, 1, nullptr, 0, scale, nullptr, 0.0, x, y, conj_x,
+                                     (cudaStream_t)stream);
     return bem_launch_assemble(ctx, op, test, trial, 1, nullptr, 0, scale, nullptr, 0.0, x, y, conj_x,
                                (cudaStream_t)stream);
 }
@@ -361,6 +443,16 @@ int bem_assemble_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space*
     if (rows->n_panels != test->n_panels || data->n_panels != trial->n_panels)
         return bem_fail(ctx, BEM_ERR_INVALID, "assemble_dirichlet: rows/data must run over the test/trial panels");
     if (!out || ld <= 0 || !g || !y) return bem_fail(ctx, BEM_ERR_INVALID, "assemble_dirichlet: NULL buffer");
+    if (ctx->dim == 2) {
+        // 2D: the V block and K g as two launches on the caller's stream
+        if (int rc = bem_launch_assemble2d(ctx, op, test, trial, 0, out, ld, scale, nullptr, 0.0, nullptr, nullptr,
+                                           0, (cudaStream_t)stream))
+            return rc;
+        bem_op_desc kop = *op;
+        kop.op = BEM_OP_K;
+        return bem_launch_assemble2d(ctx, &kop, rows, data, 1, nullptr, 0, scale_k, nullptr, 0.0, g, y, conj_g,
+                                     (cudaStream_t)stream);
+    }
     return bem_launch_dirichlet(ctx, op, test, trial, out, ld, scale, rows, data, g, y, scale_k, conj_g,
                                 (cudaStream_t)stream);
 }
@@ -377,6 +469,9 @@ int bem_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int dt
     int mode = x ? 1 : 0;
     if (mode == 0 && (!out || ld <= 0)) return bem_fail(ctx, BEM_ERR_INVALID, "mass: out is NULL");
     if (mode == 1 && !y) return bem_fail(ctx, BEM_ERR_INVALID, "mass: y is NULL");
+    if (ctx->dim == 2)
+        return bem_launch_mass2d(ctx, test, trial, dtype == BEM_C128, mode, out, ld, scale, out_t, scale_t, x, y,
+                                 conj_x, (cudaStream_t)stream);
     return bem_launch_mass(ctx, test, trial, dtype == BEM_C128, mode, out, ld, scale, out_t, scale_t, x, y, conj_x,
                            (cudaStream_t)stream);
 }
@@ -386,6 +481,7 @@ int bem_adjoint_vertices(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
     if (!ctx) return BEM_ERR_INVALID;
     if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
     if (!op || !lam || !u || !grad) return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: null argument");
+    if (ctx->dim != 3) return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: triangle meshes only");
     if (op->kernel != BEM_KERNEL_LAPLACE || (op->op != BEM_OP_V && op->op != BEM_OP_K))
         return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: Laplace V or K only");
     if (int rc = check_space(ctx, test, "test")) return rc;

@@ -21,11 +21,14 @@ struct bem_ctx {
     int num_sms = 148;
 
     // ---- mesh (device) ----
+    int dim = 3;                 // 3: triangles (bem_mesh_set), 2: segments (bem_mesh_set_2d)
     int nv = 0, nt = 0, Q = 0, Q2 = 0;
-    double* verts = nullptr;     // [nv*3]
-    int32_t* tris = nullptr;     // [nt*3]
-    double* area = nullptr;      // [nt]
-    double* normal = nullptr;    // [nt*3]
+    double* verts = nullptr;     // [nv*dim]
+    int32_t* tris = nullptr;     // [nt*dim]
+    double* area = nullptr;      // [nt] (2D: segment length)
+    double* normal = nullptr;    // [nt*dim]
+    double4* seg2 = nullptr;     // 2D: [nt] endpoints (x1, y1, x2, y2)
+    double2* nrm2 = nullptr;     // 2D: [nt] unit normals
     double* centroid = nullptr;  // [nt*3]
     double* curl = nullptr;      // [nt*9]  curl of P1 hat b: [p*9 + b*3 + c]
     double4* pts64 = nullptr;    // [nt*Q2] separate-rule point offset from centroid (xyz) + weight (w)
@@ -67,6 +70,13 @@ int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* te
 int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                          void* out, int64_t ld, double scale, const bem_space* rows, const bem_space* data,
                          const void* g, void* y, double scale_k, int conj_g, cudaStream_t s);
+// 2D operators (bem_assembly2d.cu)
+int bem_launch_assemble2d(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                          int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
+                          void* y, int conj_x, cudaStream_t s);
+int bem_launch_mass2d(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int is_complex, int mode,
+                      void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x, void* y,
+                      int conj_x, cudaStream_t s);
 int bem_launch_mass(bem_ctx* ctx, const bem_space* test, const bem_space* trial, int is_complex, int mode, void* out,
                     int64_t ld, double scale, void* out_t, double scale_t, const void* x, void* y, int conj_x,
                     cudaStream_t s);

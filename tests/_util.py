@@ -4,8 +4,12 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FIXTURES = ["cube_lap_dir_q5", "cube_lap_neu_q5", "cube_helm_mix_ext_q4", "cube_trans_q3", "ico1_lap_full_q3",
-            "ico1_helm_dir_p1_q3"]
+FIXTURES_3D = ["cube_lap_dir_q5", "cube_lap_neu_q5", "cube_helm_mix_ext_q4", "cube_trans_q3", "ico1_lap_full_q3",
+               "ico1_helm_dir_p1_q3"]
+# the reference's 2D path on its analytical disk (N segments)
+FIXTURES_2D = ["disk32_lap_dir_q4", "disk32_lap_neu_q4", "disk24_helm_mix_ext_q3", "disk24_helm_dir_p1_q3",
+               "disk256_lap_dir_q3"]
+FIXTURES = FIXTURES_3D + FIXTURES_2D
 
 
 def load_fixture(name):
@@ -36,6 +40,14 @@ def data_callbacks(kind, k=0.0, direction=None):
         def fN(x, n, s=1.0):
             return -np.sum((x - x0) * n, 1) / np.linalg.norm(x - x0, axis=1) ** 3
         return fD, fN
+    if kind == "laplace_2d":
+        # u = (x^2 - y^2) / 2 (the 2D data of the reference's Laplace demo)
+        def fD(x, s=1.0):
+            return 0.5 * x[:, 0] ** 2 - 0.5 * x[:, 1] ** 2
+
+        def fN(x, n, s=1.0):
+            return x[:, 0] * n[:, 0] - x[:, 1] * n[:, 1]
+        return fD, fN
     d = np.asarray(direction, dtype=np.float64)
 
     def fD(x, s=1.0):
@@ -52,7 +64,8 @@ def full_spaces(nv, tris, nb):
     panels = np.arange(nt, dtype=np.int32)
     if nb == 1:
         return panels, 1, panels.copy()
-    return panels, 3, np.asarray(tris, dtype=np.int32).reshape(-1).copy()
+    t = np.asarray(tris, dtype=np.int32)
+    return panels, t.shape[1], t.reshape(-1).copy()
 
 
 def rel_err(a, b):
@@ -73,6 +86,13 @@ def torch_callbacks(kind, k=0.0, direction=None):
         def fN(x, n, s=1.0):
             x0 = torch.tensor([2.0, 2.0, 2.0], dtype=x.dtype, device=x.device)
             return -((x - x0) * n).sum(1) / torch.linalg.norm(x - x0, dim=1) ** 3
+        return fD, fN
+    if kind == "laplace_2d":
+        def fD(x, s=1.0):
+            return 0.5 * x[:, 0] ** 2 - 0.5 * x[:, 1] ** 2
+
+        def fN(x, n, s=1.0):
+            return x[:, 0] * n[:, 0] - x[:, 1] * n[:, 1]
         return fD, fN
 
     def fD(x, s=1.0):

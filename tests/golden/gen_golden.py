@@ -93,16 +93,25 @@ def make_data(kind, k, direction):
         return fD, fN
     if kind == "plane_wave":
         dx = direction
+        dim = len(dx)
 
         def fD(x, sqrt_n=1.0):
-            ph = k * sqrt_n * (dx[0] * x[0] + dx[1] * x[1] + dx[2] * x[2])
+            ph = k * sqrt_n * sum(dx[c] * x[c] for c in range(dim))
             return ti.Vector([math.cos(ph), math.sin(ph)])
 
         def fN(x, n, sqrt_n=1.0):
             kk = k * sqrt_n
-            ph = kk * (dx[0] * x[0] + dx[1] * x[1] + dx[2] * x[2])
-            dn = dx[0] * n[0] + dx[1] * n[1] + dx[2] * n[2]
+            ph = kk * sum(dx[c] * x[c] for c in range(dim))
+            dn = sum(dx[c] * n[c] for c in range(dim))
             return ti.Vector([-kk * dn * math.sin(ph), kk * dn * math.cos(ph)])
+        return fD, fN
+    if kind == "laplace_2d":
+        # the 2D data of demo/demo_Laplace.py:65-72: u = (x^2 - y^2) / 2
+        def fD(x, sqrt_n=1.0):
+            return ti.Vector([0.5 * x[0] * x[0] - 0.5 * x[1] * x[1]])
+
+        def fN(x, n, sqrt_n=1.0):
+            return ti.Vector([x[0] * n[0] - x[1] * n[1]])
         return fD, fN
     raise ValueError(kind)
 
@@ -142,16 +151,30 @@ CASES = {
     "ico1_lap_full_q3": ("ico1", dict(kernel="Laplace", boundary="Full", scope="Interior", GaussQR=3), "laplace_point"),
     "ico1_helm_dir_p1_q3": ("ico1", dict(kernel="Helmholtz", boundary="Dirichlet", scope="Interior", GaussQR=3, k=3.0,
                                          Q_Neumann=1), "plane_wave"),
+    # 2D: MeshManager.load_analytical_disk (mesh_manager.py:520-536) with N segments
+    "disk32_lap_dir_q4": ("disk32", dict(dim=2, kernel="Laplace", boundary="Dirichlet", scope="Interior", GaussQR=4),
+                          "laplace_2d"),
+    "disk32_lap_neu_q4": ("disk32", dict(dim=2, kernel="Laplace", boundary="Neumann", scope="Interior", GaussQR=4),
+                          "laplace_2d"),
+    "disk24_helm_mix_ext_q3": ("disk24", dict(dim=2, kernel="Helmholtz", boundary="Mix", scope="Exterior", GaussQR=3,
+                                              k=2.0), "plane_wave"),
+    "disk24_helm_dir_p1_q3": ("disk24", dict(dim=2, kernel="Helmholtz", boundary="Dirichlet", scope="Interior",
+                                             GaussQR=3, k=3.0, Q_Neumann=1), "plane_wave"),
+    "disk256_lap_dir_q3": ("disk256", dict(dim=2, kernel="Laplace", boundary="Dirichlet", scope="Interior",
+                                           GaussQR=3), "laplace_2d"),
 }
 
 
 def run_case(ref, name):
     mesh, over, data_kind = CASES[name]
     tmp = tempfile.mkdtemp(prefix="bemgold_")
+    patched = []
     try:
         os.makedirs(os.path.join(tmp, "assets"))
         if mesh == "cube":
             shutil.copy(os.path.join(ref, "assets", "cube.obj"), os.path.join(tmp, "assets", "cube.obj"))
+        elif mesh.startswith("disk"):
+            pass
         else:
             v, f = icosphere(int(mesh[3:]))
             write_obj(os.path.join(tmp, "assets", mesh + ".obj"), v, f)
@@ -163,12 +186,19 @@ def run_case(ref, name):
         from src.managers.BEM_manager import BEMManager
         from src.BEM_functions.utils import AssembleType, ScopeType
 
+        dim = int(params["dim"])
+        if mesh.startswith("disk"):
+            # the reference's own disk generator with N segments instead of its default 256
+            n_seg = int(mesh[4:])
+            disk = MeshManager.load_analytical_disk
+            patched.append((MeshManager, "load_analytical_disk", disk))
+            MeshManager.load_analytical_disk = lambda self, r=1.0, N=n_seg: disk(self, r, N)
         core = _Core(tmp, params)
         core._mesh_manager = MeshManager(core)
         core._BEM_manager = BEMManager(core)
         core._mesh_manager.initialization()
         rng = np.random.default_rng(0)
-        d = rng.standard_normal(3)
+        d = rng.standard_normal(dim)
         d = d / np.linalg.norm(d)
         fD, fN = make_data(data_kind, float(params.get("k", 0.0)), d)
         bem = core._BEM_manager
@@ -233,7 +263,7 @@ def run_case(ref, name):
         out["n_forward"] = np.int64(len(snaps))
 
         out["vertices"] = mm.vertices.to_numpy()
-        out["panels"] = np.array(mm.panels.to_numpy(), dtype=np.int64).reshape(-1, 3)
+        out["panels"] = np.array(mm.panels.to_numpy(), dtype=np.int64).reshape(-1, dim)
         out["panel_types"] = np.array(mm.panel_types.to_numpy(), dtype=np.int64)
         out["vertice_types"] = np.array(mm.vertice_types.to_numpy(), dtype=np.int64)
         out["panel_areas"] = mm.panel_areas.to_numpy()
@@ -252,6 +282,8 @@ def run_case(ref, name):
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(f"{name}: done in {elapsed:.1f}s", flush=True)
     finally:
+        for owner, name, val in patched:
+            setattr(owner, name, val)
         shutil.rmtree(tmp, ignore_errors=True)
 
 
