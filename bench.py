@@ -422,6 +422,89 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
                                    f"k_in=7.5, GaussQR=5, solver {solver}", **res)))
 
 
+def disk2d_bench(n_seg: int, gauss_qr: int, k: float, reps: int = 5):
+    """The 2D path: Helmholtz interior Dirichlet on the reference's analytical
+    disk (radius 1) with n_seg segments, P0 Neumann unknowns, P1 Dirichlet
+    data of a plane wave.  Times the V block alone (CUDA events, mean of
+    `reps` launches; entries/s = n_seg^2 / time), the whole assembly of the
+    system (V + (1/2 M + K) g), the FP64 LU solve and the mixed solve, and
+    times the oracle's numpy restatement of the same V rows on a 16-row
+    sample on one host core."""
+    import numpy as np
+    import torch
+    from bem_b200 import _lib as L
+    from bem_b200.managers import CoreManager
+    from bem_b200.meshes import analytical_disk
+    from bem_b200.workloads import PlaneWave
+    rng = np.random.default_rng(0)
+    d = rng.standard_normal(2)
+    d /= np.linalg.norm(d)
+    pw = PlaneWave(k, d)
+    v, f = analytical_disk(1.0, n_seg)
+    # quirk=False: the right-hand side takes g, not conj(g), so that the
+    # solution can be compared with the exact Neumann trace of the plane wave
+    params = dict(dim=2, vertices=v, panels=f, kernel="Helmholtz", boundary="Dirichlet", scope="Interior",
+                  GaussQR=gauss_qr, k=k, Q_Neumann=0, Q_Dirichlet=1, precision="fp64", solve_precision="fp64",
+                  fuse=True, quirk=False)
+    res = {}
+    for solve in ("fp64", "mixed"):
+        core = CoreManager(dict(params, solve_precision=solve))
+        core.initialization(pw.fD, pw.fN)
+        b = core._BEM_manager
+        b.run()  # warm-up
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        b.assemble_system()
+        ev[1].record()
+        b.solve()
+        ev[2].record()
+        torch.cuda.synchronize()
+        res[solve] = {"assemble_ms": ev[0].elapsed_time(ev[1]), "solve_ms": ev[1].elapsed_time(ev[2]),
+                      "x": b.raw_solved.clone(), "exact": b.raw_analytical_solved.clone(),
+                      "info": {kk: (vv.item() if hasattr(vv, "item") else vv) for kk, vv in b.solve_info.items()}}
+        if solve == "fp64":
+            sp = b.space("charge", 0, "N", 0)
+            V = torch.zeros(n_seg, n_seg, dtype=torch.complex128, device="cuda")
+            desc = b.op_desc(L.OP_V, k, 1.0)
+            b.engine.assemble(desc, sp, sp, V)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                b.engine.assemble(desc, sp, sp, V)
+            e1.record()
+            torch.cuda.synchronize()
+            res["v_block_ms"] = e0.elapsed_time(e1) / reps
+            del V
+        core.kill()
+    x64, xmx, ex = res["fp64"]["x"], res["mixed"]["x"], res["fp64"]["exact"]
+    # CPU: the oracle's V rows for a sample of test segments
+    from oracle import oracle2d as O2
+    rows = 16
+    p = np.arange(n_seg, dtype=np.int32)
+    out = np.zeros((n_seg, n_seg), np.complex128)
+    t0 = time.perf_counter()
+    O2.assemble(v, f, 0, True, k, k * k, gauss_qr, (p[:rows], 1, p[:rows].copy()), (p, 1, p.copy()), out=out)
+    cpu_s = time.perf_counter() - t0
+    cpu_rate = rows * n_seg / cpu_s
+    gpu_rate = n_seg * n_seg / (res["v_block_ms"] * 1e-3)
+    print(json.dumps({
+        "workload": f"2D Helmholtz interior Dirichlet, analytical disk r=1, {n_seg} segments, k={k}, "
+                    f"GaussQR={gauss_qr}, P0 Neumann unknowns, plane-wave data, quirk=False",
+        "v_block_ms": res["v_block_ms"], "v_entries_per_s": gpu_rate,
+        "v_pair_points_per_s": gpu_rate * gauss_qr ** 2,
+        "assemble_system_ms": res["fp64"]["assemble_ms"],
+        "solve_fp64_lu_ms": res["fp64"]["solve_ms"], "solve_mixed_ms": res["mixed"]["solve_ms"],
+        "mixed_refinement": res["mixed"]["info"],
+        "mixed_vs_fp64_rel_err": float(torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64)),
+        "fp64_vs_exact_trace_rel_err": float(torch.linalg.norm(x64 - ex) / torch.linalg.norm(ex)),
+        "cpu_baseline": {"value": cpu_rate, "unit": "entries/s", "cores": 1, "kind": "port",
+                         "sample": f"oracle/oracle2d.py (numpy, scipy Hankel) V rows 0..{rows - 1} x {n_seg}"},
+        "gpu_vs_cpu_entries": gpu_rate / cpu_rate,
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -430,9 +513,10 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--profile-step", default=None, choices=["mixed", "fp64"],
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
-    ap.add_argument("--workload", default="config2", choices=["config2", "sweep", "shape", "transmission"],
-                    help="sweep: the config-3 wavenumber sweep, shape: the config-4 shape gradient "
-                         "(each its own JSON line)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "sweep", "shape", "transmission", "disk2d"],
+                    help="sweep: the config-3 wavenumber sweep, shape: the config-4 shape gradient, disk2d: the "
+                         "2D operators (each its own JSON line)")
+    ap.add_argument("--disk-n", type=int, default=8192, help="segments of the disk2d workload")
     ap.add_argument("--shape-subdiv", type=int, default=5, help="icosphere subdivision of the shape workload")
     ap.add_argument("--shape-check", type=int, default=32, help="vertices of the finite-difference check")
     ap.add_argument("--trans-subdiv", type=int, default=5, help="icosphere subdivision of the transmission workload")
@@ -452,6 +536,10 @@ def main():
     if args.workload == "transmission":
         if rank == 0:
             transmission_bench(args.trans_subdiv, args.trans_plain, args.trans_solver)
+        return
+    if args.workload == "disk2d":
+        if rank == 0:
+            disk2d_bench(args.disk_n, 5, 3.0)
         return
     if args.profile_step:
         profile_step(args.profile_step)
