@@ -41,18 +41,23 @@ for _p in (ROOT, os.path.join(ROOT, "taichi-bem_b200")):
 METRIC = "assembly entries/s + time-to-solution at ≤1e-6 rel err: mixed/batched vs plain GPU"
 WORKLOAD = "Helmholtz 3D interior Dirichlet k=3, icosphere s4 (5120 panels), GaussQR=5, plane wave"
 # Algorithmic FP32 flops (an FMA counts 2) per kernel evaluation of the fused
-# symmetric Helmholtz sweep (far_vkg_sym_kernel), counted once from its source:
+# symmetric Helmholtz sweep, counted once from the source of its scalar form
+# (far_vkg_sym_kernel<Helmholtz, float>) and kept fixed as the unit of work:
 # offsets 3, s = e.(2D+e) 8, r^2 1, r and 1/r with the Newton step 9, d.n_j 6,
 # split phase 3, weights 5, k r 1, sine/cosine polynomials 20, (1-ikr) e^{ikr} 4,
 # V_ij and (K g)_i accumulation 8, (K g)_j term 10 = 78, plus two MUFU
 # operations (reciprocal square root, reciprocal).  One evaluation serves V_ij,
 # V_ji, (K g)_i and (K g)_j, so the sweep evaluates each unordered separate
-# pair once.
+# pair once.  The launched kernel (far_vkg_sym_x2_kernel, packed FP32x2) gets
+# the same result with 63 flops per evaluation (s from per-point and
+# per-trial-point terms, d.n_j per pair, -d.n_i factored out of the sum over
+# test points, shorter polynomials for phases below 0.3); the rate against 78
+# is the rate of the unit of work.
 FLOPS_PER_EVAL = 78
 MUFU_PER_EVAL = 2
-# dram__bytes_read.sum + dram__bytes_write.sum of far_vkg_sym_kernel on this
-# workload (424.3 MB + 380.5 MB, profiles/far_vkg_sym_helmholtz_s4.md)
-FAR_SWEEP_DRAM_BYTES = 804.8e6
+# dram__bytes_read.sum + dram__bytes_write.sum of far_vkg_sym_x2_kernel on this
+# workload (423.5 MB + 379.3 MB, profiles/far_vkg_sym_helmholtz_s4.md)
+FAR_SWEEP_DRAM_BYTES = 802.8e6
 
 
 def _dist():
@@ -698,11 +703,13 @@ def main():
     achieved = evals * FLOPS_PER_EVAL / (va_ms * 1e-3) / 1e12
     roof = {"bound": "fp32", "achieved": achieved, "peak": peaks[0], "unit": "TFLOP/s",
             "frac": achieved / peaks[0],
-            # DRAM read + write of one far_vkg_sym_kernel launch of this workload, one ncu capture
+            # DRAM read + write of one far_vkg_sym_x2_kernel launch of this workload, one ncu capture
             "traffic": FAR_SWEEP_DRAM_BYTES,
-            "kernel": "far_vkg_sym_kernel<Helmholtz, float> (timed with its FP64 near-pair kernels in one call)",
+            "kernel": "far_vkg_sym_x2_kernel<Helmholtz> (packed FP32x2; timed with its FP64 near-pair kernels "
+                      "in one call)",
             "peak_source": "bem_measure_peaks FP32 FMA probe on this GPU (MEASURED_PEAKS.json has HBM and bf16 only)",
-            "flops_per_eval": FLOPS_PER_EVAL, "evals_per_launch": evals, "call_ms": va_ms,
+            "flops_per_eval": FLOPS_PER_EVAL, "flops_per_eval_executed": 63, "evals_per_launch": evals,
+            "call_ms": va_ms,
             "mufu": {"achieved_gops": evals * MUFU_PER_EVAL / (va_ms * 1e-3) / 1e9, "peak_gops": peaks[2]},
             "fp64_peak_tflops": peaks[1]}
 

@@ -322,7 +322,7 @@ struct FarArgs {
     const double* curl;
     const double* area;
     double wcorr;     // (exact / FP32 weight sum)^2 of the FP32 separate rule
-    int small_phase;  // FP32 split phase bounded by pi/4: sine/cosine without reduction
+    int small_phase;  // FP32 split phase bounded by pi/4 (1) or by 0.3 (2): sine/cosine without reduction
     const void* pts;
     const void* phi;
     const double* phi64;  // [Q2*3] P1 basis at the separate-rule points, FP64
@@ -1291,6 +1291,308 @@ __global__ void __launch_bounds__(FAR_THREADS) far_vkg_sym_kernel(FarArgs a, Vkg
     }
 }
 
+// ----------------------------------------------------------------------------
+// FP32 symmetric fused Dirichlet pass on packed FP32x2 arithmetic: the sweep
+// of far_vkg_sym_kernel<HELM, float> with two test points (q, q+1) in the two
+// lanes of every FFMA2/FMUL2/FADD2 (the lanes are the even/odd accumulator
+// sets, so the order of summation over q is that of the scalar kernel).  A
+// packed instruction does two FMAs in one issue slot at the per-lane FMA
+// rate; the scalar kernel is bound by instruction issue.  The per-point work
+// is also reduced, each step exact algebra on the scalar kernel's terms:
+//   s = e.(2D + e) = |x_a|^2 + x_a.U_b + C_b,  U_b = 2D - 2y_b,
+//                                              C_b = -y_b.(2D - y_b)
+//     (|x_a|^2 once per point, U_b and C_b once per trial point; the absolute
+//     FP32 error stays of order eps |D| |e|, as in the product form);
+//   d.n_j = D.n_j + x_a.(n_j - n_i) depends on the pair and the test point
+//     only: it is formed once per pair and kept in shared memory per thread;
+//   -d.n_i = -(D.n_i - y_b.(n_j - n_i)) is constant over the test points of a
+//     trial point and multiplies the (K g)_j sum after the loop over q;
+//   the sine/cosine polynomials drop their last term when the host has
+//     bounded the phase by 0.3 (small_phase == 2; truncation below 6e-11).
+// Shared memory holds the test points pairwise as structure-of-arrays:
+// (x0 x1 y0 y1), (z0 z1 w0 w1), g (re0 re1 im0 im1) and |x|^2 (xx0 xx1); an
+// odd Q^2 is padded by a copy of the last point with weight 0 and g = 0.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// dev_r_rinv on two lanes: one Newton step on the MUFU reciprocal square
+// root, written with e' = p y0 - 1 = -e so that no operand needs a negation
+__device__ __forceinline__ void dev_r_rinv2(float2 r2, float2& r, float2& rinv) {
+    const float2 y0 = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 p = fmul2(r2, y0);
+    const float2 e = ffma2(p, y0, f2(-1.0f));
+    rinv = ffma2(fmul2(f2(-0.5f), y0), e, y0);
+    r = ffma2(fmul2(f2(-0.5f), p), e, p);
+}
+
+// dev_sincos_poly on two lanes (|y| <= pi/4); SHORT drops the y^9 term of
+// sin and the y^10 term of cos (for |y| <= 0.3)
+template <bool SHORT>
+__device__ __forceinline__ void dev_sincos_poly2(float2 y, float2& s, float2& c) {
+    const float2 y2 = fmul2(y, y);
+    float2 ps;
+    if (SHORT) {
+        ps = ffma2(y2, f2(-1.98412698412698413e-04f), f2(8.33333333333333333e-03f));
+    } else {
+        ps = ffma2(y2, f2(2.75573192239858907e-06f), f2(-1.98412698412698413e-04f));
+        ps = ffma2(y2, ps, f2(8.33333333333333333e-03f));
+    }
+    ps = ffma2(y2, ps, f2(-1.66666666666666667e-01f));
+    s = ffma2(fmul2(y, y2), ps, y);
+    float2 pc;
+    if (SHORT) {
+        pc = ffma2(y2, f2(2.48015873015873016e-05f), f2(-1.38888888888888889e-03f));
+    } else {
+        pc = ffma2(y2, f2(-2.75573192239858907e-07f), f2(2.48015873015873016e-05f));
+        pc = ffma2(y2, pc, f2(-1.38888888888888889e-03f));
+    }
+    pc = ffma2(y2, pc, f2(4.16666666666666667e-02f));
+    pc = ffma2(y2, pc, f2(-0.5f));
+    c = ffma2(y2, pc, f2(1.0f));
+}
+
+// One trial point y_b against all test-point pairs of panel t: accumulates
+// the V sum (A0, A1), the (K g)_i kernel sum (A2, A3) and the (K g)_j sum
+// without its -d.n_i factor (A4 - A6, A5).
+template <bool HELM, int PH>
+__device__ __forceinline__ void x2_trial_point(int P2, const float4* __restrict__ sxyt,
+                                               const float4* __restrict__ szwt, const float4* __restrict__ sgt,
+                                               const float2* __restrict__ sxxt, const float2* __restrict__ sdn,
+                                               float2 U0, float2 U1, float2 U2, float2 CB, float2 R2, float2 RF,
+                                               float2 KK, float2 NKK, float2& A0, float2& A1, float2& A2,
+                                               float2& A3, float2& A4, float2& A5, float2& A6) {
+#pragma unroll 4
+    for (int p = 0; p < P2; ++p) {
+        const float4 xy = sxyt[p], zw = szwt[p];
+        const float2 X = make_float2(xy.x, xy.y), Y = make_float2(xy.z, xy.w);
+        const float2 Z = make_float2(zw.x, zw.y), W = make_float2(zw.z, zw.w);
+        const float2 sq = ffma2(X, U0, ffma2(Y, U1, ffma2(Z, U2, fadd2(sxxt[p], CB))));
+        float2 r, rinv;
+        dev_r_rinv2(fadd2(R2, sq), r, rinv);
+        const float2 dnj = sdn[p * FAR_THREADS];
+        const float2 wr = fmul2(W, rinv);
+        const float2 wr3 = fmul2(wr, fmul2(rinv, rinv));
+        if (HELM) {
+            const float2 rr = fadd2(r, RF);
+            const float2 inv = make_float2(__fdividef(1.0f, rr.x), __fdividef(1.0f, rr.y));
+            const float2 phase = fmul2(KK, fmul2(sq, inv));
+            float2 sn, cs;
+            if (PH == 2) {
+                dev_sincos_poly2<true>(phase, sn, cs);
+            } else if (PH == 1) {
+                dev_sincos_poly2<false>(phase, sn, cs);
+            } else {
+                dev_sincos(phase.x, &sn.x, &cs.x);
+                dev_sincos(phase.y, &sn.y, &cs.y);
+            }
+            const float2 kr = fmul2(KK, r), nkr = fmul2(NKK, r);
+            // u = wr3 (1 - ikr) e^{ik(r-R)}
+            const float2 u_re = fmul2(wr3, ffma2(kr, sn, cs)), u_im = fmul2(wr3, ffma2(nkr, cs, sn));
+            A0 = ffma2(wr, cs, A0);
+            A1 = ffma2(wr, sn, A1);
+            A2 = ffma2(dnj, u_re, A2);
+            A3 = ffma2(dnj, u_im, A3);
+            const float4 g = sgt[p];
+            const float2 GR = make_float2(g.x, g.y), GI = make_float2(g.z, g.w);
+            A4 = ffma2(u_re, GR, A4);
+            A6 = ffma2(u_im, GI, A6);
+            A5 = ffma2(u_re, GI, A5);
+            A5 = ffma2(u_im, GR, A5);
+        } else {
+            A0 = fadd2(A0, wr);
+            A2 = ffma2(dnj, wr3, A2);
+            const float4 g = sgt[p];
+            A4 = ffma2(wr3, make_float2(g.x, g.y), A4);
+        }
+    }
+}
+
+template <bool HELM>
+__global__ void __launch_bounds__(FAR_THREADS, 5) far_vkg_sym_x2_kernel(FarArgs a, VkgArgs v) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int Q2 = a.Q2;
+    const int P2 = (Q2 + 1) / 2;                                    // point pairs per panel
+    float4* sxy = reinterpret_cast<float4*>(smem_raw);              // [FAR_TI][P2] (x0 x1 y0 y1)
+    float4* szw = sxy + FAR_TI * P2;                                // [FAR_TI][P2] (z0 z1 w0 w1)
+    float4* sg = szw + FAR_TI * P2;                                 // [FAR_TI][P2] (re0 re1 im0 im1)
+    float2* sxx = reinterpret_cast<float2*>(sg + FAR_TI * P2);      // [FAR_TI][P2] (|x0|^2 |x1|^2)
+    float2* sdn = sxx + FAR_TI * P2;                                // [P2][FAR_THREADS] d.n_j of this thread's pair
+    float* sphi = reinterpret_cast<float*>(sdn + P2 * FAR_THREADS);  // [Q2*3]
+    __shared__ int s_gi[FAR_TI];
+    __shared__ int s_tri[FAR_TI][3];
+    __shared__ double s_cen[FAR_TI][3];
+    __shared__ double s_nrm[FAR_TI][3];
+
+    const int n = a.n_test;  // == n_trial
+    const int j0 = blockIdx.x * FAR_THREADS;
+    const int li0 = blockIdx.y * FAR_TI;
+    if (j0 + FAR_THREADS - 1 <= li0) return;
+    const int lj = j0 + threadIdx.x;
+    const float4* pts = reinterpret_cast<const float4*>(a.pts);
+    {
+        const float* phi = reinterpret_cast<const float*>(a.phi);
+        for (int idx = threadIdx.x; idx < Q2 * 3; idx += FAR_THREADS) sphi[idx] = phi[idx];
+    }
+    if (threadIdx.x < FAR_TI) {
+        int li = li0 + threadIdx.x;
+        int gi = li < n ? a.test_panels[li] : -1;
+        s_gi[threadIdx.x] = gi;
+        for (int c = 0; c < 3; ++c) {
+            s_tri[threadIdx.x][c] = gi >= 0 ? a.tris[3 * gi + c] : -1;
+            s_cen[threadIdx.x][c] = gi >= 0 ? a.centroid[3 * gi + c] : 0.0;
+            s_nrm[threadIdx.x][c] = gi >= 0 ? a.normal[3 * gi + c] : 0.0;
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < FAR_TI * P2; idx += FAR_THREADS) {
+        const int t = idx / P2, p = idx - t * P2;
+        const int li = li0 + t;
+        const int q0 = 2 * p, q1 = 2 * p + 1 < Q2 ? 2 * p + 1 : Q2 - 1;
+        float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
+        float g0r = 0.f, g0i = 0.f, g1r = 0.f, g1i = 0.f;
+        if (li < n) {
+            x0 = pts[(size_t)s_gi[t] * Q2 + q0];
+            x1 = pts[(size_t)s_gi[t] * Q2 + q1];
+            PanelData<HELM, float> gd;
+            gd.load(v, li);
+            gd.at(sphi[3 * q0 + 1], sphi[3 * q0 + 2], g0r, g0i);
+            gd.at(sphi[3 * q1 + 1], sphi[3 * q1 + 2], g1r, g1i);
+            if (2 * p + 1 >= Q2) {  // padding point: weight 0, data 0
+                x1.w = 0.f;
+                g1r = g1i = 0.f;
+            }
+        }
+        sxy[idx] = make_float4(x0.x, x1.x, x0.y, x1.y);
+        szw[idx] = make_float4(x0.z, x1.z, x0.w, x1.w);
+        sg[idx] = make_float4(g0r, g1r, g0i, g1i);
+        sxx[idx] = make_float2(fmaf(x0.x, x0.x, fmaf(x0.y, x0.y, x0.z * x0.z)),
+                               fmaf(x1.x, x1.x, fmaf(x1.y, x1.y, x1.z * x1.z)));
+    }
+    __syncthreads();
+
+    const bool valid_j = lj < n;
+    const int gj = valid_j ? a.trial_panels[lj] : 0;
+    int tri_j[3];
+    double cen_j[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        tri_j[c] = a.tris[3 * gj + c];
+        cen_j[c] = a.centroid[3 * gj + c];
+    }
+    const double nj64[3] = {a.normal[3 * gj + 0], a.normal[3 * gj + 1], a.normal[3 * gj + 2]};
+    PanelData<HELM, float> gj_data;
+    if (valid_j) gj_data.load(v, lj);
+    const float4* ptsj = pts + (size_t)gj * Q2;
+    const float2 KK = f2(float(a.k)), NKK = f2(-float(a.k));
+    const int lane = threadIdx.x & 31;
+    float2* sdn_me = sdn + threadIdx.x;
+    double rj_re = 0.0, rj_im = 0.0;
+
+    for (int t = 0; t < FAR_TI; ++t) {
+        const int li = li0 + t;
+        if (li >= n) break;
+        const int gi = s_gi[t];
+        const bool sep = valid_j && li < lj && (bem_relation(s_tri[t], tri_j, gi == gj) == REL_SEPARATE);
+        double av_re = 0.0, av_im = 0.0, ak_re = 0.0, ak_im = 0.0;
+        if (sep) {
+            const double dcx64 = s_cen[t][0] - cen_j[0], dcy64 = s_cen[t][1] - cen_j[1],
+                         dcz64 = s_cen[t][2] - cen_j[2];
+            Frame<float, HELM> fr;
+            fr.init(dcx64, dcy64, dcz64, a.k, a.area[gi], a.area[gj], a.wcorr);
+            const float Dnj = float(dcx64 * nj64[0] + dcy64 * nj64[1] + dcz64 * nj64[2]);
+            const float Dni = float(dcx64 * s_nrm[t][0] + dcy64 * s_nrm[t][1] + dcz64 * s_nrm[t][2]);
+            const float mx = float(nj64[0] - s_nrm[t][0]), my = float(nj64[1] - s_nrm[t][1]),
+                        mz = float(nj64[2] - s_nrm[t][2]);
+            const float4* sxyt = sxy + t * P2;
+            const float4* szwt = szw + t * P2;
+            const float4* sgt = sg + t * P2;
+            const float2* sxxt = sxx + t * P2;
+            {
+                // d.n_j = D.n_j + x_a.(n_j - n_i) of this pair's test points
+                const float2 MX = f2(mx), MY = f2(my), MZ = f2(mz), DNJ = f2(Dnj);
+                for (int p = 0; p < P2; ++p) {
+                    const float4 xy = sxyt[p], zw = szwt[p];
+                    sdn_me[p * FAR_THREADS] = ffma2(make_float2(xy.x, xy.y), MX,
+                                                    ffma2(make_float2(xy.z, xy.w), MY,
+                                                          ffma2(make_float2(zw.x, zw.y), MZ, DNJ)));
+                }
+            }
+            const float2 R2 = f2(fr.R2), RF = f2(fr.Rf);
+            double pj_re = 0.0, pj_im = 0.0;
+            for (int b = 0; b < Q2; ++b) {
+                const float4 yb = ptsj[b];
+                const float wx = fr.ux - yb.x, wy = fr.uy - yb.y, wz = fr.uz - yb.z;
+                const float2 U0 = f2(wx - yb.x), U1 = f2(wy - yb.y), U2 = f2(wz - yb.z);
+                const float2 CB = f2(-fmaf(yb.x, wx, fmaf(yb.y, wy, yb.z * wz)));
+                // -d.n_i = -(D.n_i - y_b.(n_j - n_i)), constant over the test points
+                const float ndni = -(Dni + (yb.x * mx + yb.y * my + yb.z * mz));
+                float2 A0 = f2(0.f), A1 = f2(0.f), A2 = f2(0.f), A3 = f2(0.f), A4 = f2(0.f), A5 = f2(0.f),
+                       A6 = f2(0.f);
+                if (!HELM || a.small_phase == 2)
+                    x2_trial_point<HELM, 2>(P2, sxyt, szwt, sgt, sxxt, sdn_me, U0, U1, U2, CB, R2, RF, KK, NKK, A0,
+                                            A1, A2, A3, A4, A5, A6);
+                else if (a.small_phase == 1)
+                    x2_trial_point<HELM, 1>(P2, sxyt, szwt, sgt, sxxt, sdn_me, U0, U1, U2, CB, R2, RF, KK, NKK, A0,
+                                            A1, A2, A3, A4, A5, A6);
+                else
+                    x2_trial_point<HELM, 0>(P2, sxyt, szwt, sgt, sxxt, sdn_me, U0, U1, U2, CB, R2, RF, KK, NKK, A0,
+                                            A1, A2, A3, A4, A5, A6);
+                const float sv_re = A0.x + A0.y, sv_im = A1.x + A1.y;
+                const float sk_re = A2.x + A2.y, sk_im = A3.x + A3.y;
+                const float s2_re = ndni * ((A4.x + A4.y) - (A6.x + A6.y)), s2_im = ndni * (A5.x + A5.y);
+                const double wb = double(yb.w);
+                av_re += wb * double(sv_re);
+                av_im += wb * double(sv_im);
+                float gb_re, gb_im;
+                gj_data.at(sphi[3 * b + 1], sphi[3 * b + 2], gb_re, gb_im);
+                ak_re += wb * (double(sk_re) * double(gb_re) - double(sk_im) * double(gb_im));
+                ak_im += wb * (double(sk_re) * double(gb_im) + double(sk_im) * double(gb_re));
+                pj_re += wb * double(s2_re);
+                pj_im += wb * double(s2_im);
+            }
+            fr.rotate(av_re, av_im);
+            fr.rotate(ak_re, ak_im);
+            fr.rotate(pj_re, pj_im);
+            rj_re += pj_re;
+            rj_im += pj_im;
+            const int row = a.test_dof[li];
+            const int col = a.trial_dof[lj];
+            if (row >= 0 && col >= 0) {
+                const double vr = a.scale * BEM_INV4PI * av_re, vi = a.scale * BEM_INV4PI * av_im;
+                add_entry<HELM>(a.out, (int64_t)row * a.ld + col, vr, vi, false);
+                add_entry<HELM>(a.out, (int64_t)col * a.ld + row, vr, vi, false);
+            }
+        }
+        ak_re = warp_sum(ak_re);
+        if (HELM) ak_im = warp_sum(ak_im);
+        if (lane == 0) {
+            const int row = v.rows[li];
+            if (row >= 0) {
+                if (HELM) {
+                    atomicAdd(v.y + 2 * row, v.scale * BEM_INV4PI * ak_re);
+                    atomicAdd(v.y + 2 * row + 1, v.scale * BEM_INV4PI * ak_im);
+                } else {
+                    atomicAdd(v.y + row, v.scale * BEM_INV4PI * ak_re);
+                }
+            }
+        }
+    }
+    if (valid_j) {
+        const int row = v.rows[lj];
+        if (row >= 0 && (rj_re != 0.0 || rj_im != 0.0)) {
+            if (HELM) {
+                atomicAdd(v.y + 2 * row, v.scale * BEM_INV4PI * rj_re);
+                atomicAdd(v.y + 2 * row + 1, v.scale * BEM_INV4PI * rj_im);
+            } else {
+                atomicAdd(v.y + row, v.scale * BEM_INV4PI * rj_re);
+            }
+        }
+    }
+}
+
 template <int OP, bool HELM, int NBX, int NBY>
 int launch_op(bem_ctx* ctx, const FarArgs& fa, const NearArgs& na, bool fp32, cudaStream_t s) {
     dim3 grid((fa.n_trial + FAR_THREADS - 1) / FAR_THREADS, (fa.n_test + FAR_TI - 1) / FAR_TI);
@@ -1345,6 +1647,10 @@ int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s) {
     return bem_check_cuda(ctx, cudaGetLastError(), "geometry_kernel launch");
 }
 
+// Class of the bound on the FP32 split phase |k (r - R)| <= k (rho_i + rho_j):
+// 2 when <= 0.3 (short polynomials), 1 when <= 0.78 < pi/4 (no reduction), 0 otherwise
+static int phase_class(double bound) { return bound <= 0.3 ? 2 : (bound <= 0.78 ? 1 : 0); }
+
 int bem_fill_local_map(bem_ctx* ctx, const bem_space* sp, int32_t* map, cudaStream_t s) {
     if (int rc = bem_check_cuda(ctx, cudaMemsetAsync(map, 0xff, sizeof(int32_t) * ctx->nt, s), "memset")) return rc;
     if (sp->n_panels > 0) {
@@ -1375,7 +1681,7 @@ int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* te
     fa.curl = ctx->curl;
     fa.area = ctx->area;
     fa.wcorr = ctx->wcorr32;
-    fa.small_phase = (fp32 && op->kernel == BEM_KERNEL_HELMHOLTZ && op->k * 2.0 * ctx->rho_max <= 0.78) ? 1 : 0;
+    fa.small_phase = fp32 && op->kernel == BEM_KERNEL_HELMHOLTZ ? phase_class(op->k * 2.0 * ctx->rho_max) : 0;
     fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
     fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
     fa.phi64 = ctx->phi64;
@@ -1460,7 +1766,7 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
     fa.curl = ctx->curl;
     fa.area = ctx->area;
     fa.wcorr = ctx->wcorr32;
-    fa.small_phase = (fp32 && op->kernel == BEM_KERNEL_HELMHOLTZ && op->k * 2.0 * ctx->rho_max <= 0.78) ? 1 : 0;
+    fa.small_phase = fp32 && op->kernel == BEM_KERNEL_HELMHOLTZ ? phase_class(op->k * 2.0 * ctx->rho_max) : 0;
     fa.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
     fa.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
     fa.phi64 = ctx->phi64;
@@ -1479,11 +1785,13 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
                      test->dof == trial->dof && rows->n_panels == test->n_panels;
     if (fa.n_test > 0 && fa.n_trial > 0 && sym) {
         if (fp32) {
-            size_t smem = FAR_TI * fa.Q2 * (sizeof(float4) + 2 * sizeof(float)) + fa.Q2 * 3 * sizeof(float);
+            const int P2 = (fa.Q2 + 1) / 2;
+            size_t smem = 3 * FAR_TI * P2 * sizeof(float4) + FAR_TI * P2 * sizeof(float2) +
+                          P2 * FAR_THREADS * sizeof(float2) + fa.Q2 * 3 * sizeof(float);
             if (helm)
-                far_vkg_sym_kernel<true, float><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+                far_vkg_sym_x2_kernel<true><<<grid, FAR_THREADS, smem, s>>>(fa, va);
             else
-                far_vkg_sym_kernel<false, float><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+                far_vkg_sym_x2_kernel<false><<<grid, FAR_THREADS, smem, s>>>(fa, va);
         } else {
             size_t smem = FAR_TI * fa.Q2 * (sizeof(double4) + 2 * sizeof(double)) + fa.Q2 * 3 * sizeof(double);
             if (helm)
