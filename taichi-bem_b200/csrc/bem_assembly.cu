@@ -1410,7 +1410,7 @@ __device__ __forceinline__ void x2_trial_point(int P2, const float4* __restrict_
     }
 }
 
-template <bool HELM>
+template <bool HELM, int PH>
 __global__ void __launch_bounds__(FAR_THREADS, 5) far_vkg_sym_x2_kernel(FarArgs a, VkgArgs v) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int Q2 = a.Q2;
@@ -1531,15 +1531,8 @@ __global__ void __launch_bounds__(FAR_THREADS, 5) far_vkg_sym_x2_kernel(FarArgs 
                 const float ndni = -(Dni + (yb.x * mx + yb.y * my + yb.z * mz));
                 float2 A0 = f2(0.f), A1 = f2(0.f), A2 = f2(0.f), A3 = f2(0.f), A4 = f2(0.f), A5 = f2(0.f),
                        A6 = f2(0.f);
-                if (!HELM || a.small_phase == 2)
-                    x2_trial_point<HELM, 2>(P2, sxyt, szwt, sgt, sxxt, sdn_me, U0, U1, U2, CB, R2, RF, KK, NKK, A0,
-                                            A1, A2, A3, A4, A5, A6);
-                else if (a.small_phase == 1)
-                    x2_trial_point<HELM, 1>(P2, sxyt, szwt, sgt, sxxt, sdn_me, U0, U1, U2, CB, R2, RF, KK, NKK, A0,
-                                            A1, A2, A3, A4, A5, A6);
-                else
-                    x2_trial_point<HELM, 0>(P2, sxyt, szwt, sgt, sxxt, sdn_me, U0, U1, U2, CB, R2, RF, KK, NKK, A0,
-                                            A1, A2, A3, A4, A5, A6);
+                x2_trial_point<HELM, PH>(P2, sxyt, szwt, sgt, sxxt, sdn_me, U0, U1, U2, CB, R2, RF, KK, NKK, A0, A1,
+                                         A2, A3, A4, A5, A6);
                 const float sv_re = A0.x + A0.y, sv_im = A1.x + A1.y;
                 const float sk_re = A2.x + A2.y, sk_im = A3.x + A3.y;
                 const float s2_re = ndni * ((A4.x + A4.y) - (A6.x + A6.y)), s2_im = ndni * (A5.x + A5.y);
@@ -1788,10 +1781,14 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
             const int P2 = (fa.Q2 + 1) / 2;
             size_t smem = 3 * FAR_TI * P2 * sizeof(float4) + FAR_TI * P2 * sizeof(float2) +
                           P2 * FAR_THREADS * sizeof(float2) + fa.Q2 * 3 * sizeof(float);
-            if (helm)
-                far_vkg_sym_x2_kernel<true><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+            if (!helm)
+                far_vkg_sym_x2_kernel<false, 2><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+            else if (fa.small_phase == 2)
+                far_vkg_sym_x2_kernel<true, 2><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+            else if (fa.small_phase == 1)
+                far_vkg_sym_x2_kernel<true, 1><<<grid, FAR_THREADS, smem, s>>>(fa, va);
             else
-                far_vkg_sym_x2_kernel<false><<<grid, FAR_THREADS, smem, s>>>(fa, va);
+                far_vkg_sym_x2_kernel<true, 0><<<grid, FAR_THREADS, smem, s>>>(fa, va);
         } else {
             size_t smem = FAR_TI * fa.Q2 * (sizeof(double4) + 2 * sizeof(double)) + fa.Q2 * 3 * sizeof(double);
             if (helm)
