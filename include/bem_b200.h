@@ -189,6 +189,9 @@ int bem_gemv(bem_ctx* ctx, int a_dtype, const void* A, int64_t m, int64_t n, int
  * (device, bem_lu_dinv_elems(n) elements of the dtype's complex-pair width:
  * 2 x float / 2 x double per element).  No grid-wide synchronisation. */
 int64_t bem_lu_dinv_elems(int64_t n);
+/* Queued without synchronisation.  A tensor-core wait of the trailing updates
+ * that ran out of its iteration cap is reported (BEM_ERR_TIMEOUT) by the next
+ * bem_lu_solve_tiled or bem_refine_solve on the same context. */
 int bem_lu_factor_tiled(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, void* dinv,
                         int32_t* info, void* stream);
 /* x = U^{-1} L^{-1} P b for one FP64 right-hand side b (overwritten), with the
@@ -221,7 +224,11 @@ int bem_lu_solve_tiled_static(int dtype, const void* LU, int64_t n, int64_t lda,
  * the low-precision factors (LU_lo, piv[, dinv]) of A_hi: tile-pivoted factors
  * when dinv != NULL, else partial-pivoting factors.  A_hi: F64/C128, LU_lo:
  * F32/C64.  iters/relres: host pointers (may be NULL).  Returns
- * BEM_ERR_NOCONVERGE if maxit is reached or the residual stops decreasing. */
+ * BEM_ERR_NOCONVERGE if maxit is reached or the residual stops decreasing.
+ * With tile-pivoted factors the iterations are queued in batches and the
+ * convergence test runs on the device, so the call synchronises the stream
+ * once per batch of three iterations (and reports a timeout of the preceding
+ * bem_lu_factor_tiled); with partial-pivoting factors once per iteration. */
 int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv,
                      const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit,
                      int* iters, double* relres, void* stream);

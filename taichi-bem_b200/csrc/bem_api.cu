@@ -20,6 +20,12 @@ int bem_check_cuda(bem_ctx* ctx, cudaError_t e, const char* what) {
     return bem_fail(ctx, BEM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+int bem_take_factor_error(bem_ctx* ctx, int32_t value, cudaStream_t s) {
+    if (value == 0) return BEM_OK;
+    cudaMemsetAsync(ctx->flags + 4, 0, sizeof(int32_t), s);
+    return bem_fail(ctx, BEM_ERR_TIMEOUT, "tiled lu: a tensor-core wait of the factorisation hit its iteration cap");
+}
+
 int bem_ws_reserve(bem_ctx* ctx, size_t bytes) {
     if (bytes <= ctx->ws_bytes) return BEM_OK;
     if (ctx->ws) cudaFree(ctx->ws);

@@ -57,6 +57,13 @@ struct bem_ctx {
 int bem_fail(bem_ctx* ctx, int code, const std::string& msg);
 int bem_check_cuda(bem_ctx* ctx, cudaError_t e, const char* what);
 int bem_ws_reserve(bem_ctx* ctx, size_t bytes);
+// Reports (BEM_ERR_TIMEOUT) and clears a tensor-core wait of an earlier
+// bem_lu_factor_tiled that ran out (flags[4], read by the caller after a
+// synchronisation as `value`).
+int bem_take_factor_error(bem_ctx* ctx, int32_t value, cudaStream_t s);
+// Asynchronous preconditioner step of the refinement (bem_tilelu.cu).
+int bem_tiled_precond_async(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
+                            const void* dinv, const double* r, double** out, const int* skip, cudaStream_t s);
 
 // Launch wrappers (bem_assembly.cu)
 int bem_launch_geometry(bem_ctx* ctx, cudaStream_t s);

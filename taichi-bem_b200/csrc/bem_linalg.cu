@@ -589,6 +589,99 @@ __global__ void axpy_kernel(double* y, const double* x, int64_t n, double a) {
     if (i < n) y[i] += a * x[i];
 }
 
+// ---- asynchronous refinement: state and step kernels ----------------------
+// Every kernel of an iteration returns at once when `done` is set, so the
+// host can queue several iterations and synchronise once.
+struct RefState {
+    double bn2;    // ||b||^2
+    double rn2;    // ||r||^2 of the current iteration (accumulated)
+    double prev2;  // ||r||^2 of the previous iteration
+    double rel2;   // last ||r||^2 / ||b||^2
+    int done;      // 0 running, 1 converged, 2 stagnated, 3 maxit
+    int it;        // iterations completed
+};
+
+__global__ void ref_init_kernel(RefState* st) {
+    st->bn2 = st->rn2 = st->prev2 = st->rel2 = 0.0;
+    st->done = 0;
+    st->it = 0;
+}
+
+__global__ void ref_start_kernel(RefState* st) {
+    st->prev2 = st->bn2;
+    if (st->bn2 == 0.0) st->done = 1;  // b = 0: x = 0 is exact
+}
+
+__global__ void ref_axpy_kernel(double* y, const double* x, int64_t n, const RefState* st) {
+    if (st->done) return;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) y[i] += x[i];
+}
+
+__global__ void ref_sumsq_kernel(const double* v, int64_t n, RefState* st) {
+    if (st->done) return;
+    __shared__ double s[8];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += v[i] * v[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
+        atomicAdd(&st->rn2, t);
+    }
+}
+
+// r = b - A x, one warp per row (the FP64 residual of the refinement)
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) ref_residual_kernel(const T* A, int64_t n, int64_t lda, const double* x,
+                                                            const double* b, double* r, const RefState* st) {
+    if (st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= n) return;
+    double sr = 0.0, si = 0.0;
+    const T* a = A + (C ? 2 : 1) * row * lda;
+    for (int64_t q = lane; q < n; q += 32) {
+        El<T, C> e = ld<T, C>(a, q);
+        double xr = C ? x[2 * q] : x[q], xi = C ? x[2 * q + 1] : 0.0;
+        sr += (double)e.re * xr - (C ? (double)e.im * xi : 0.0);
+        if (C) si += (double)e.re * xi + (double)e.im * xr;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        if (C) si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) {
+        if (C) {
+            r[2 * row] = b[2 * row] - sr;
+            r[2 * row + 1] = b[2 * row + 1] - si;
+        } else {
+            r[row] = b[row] - sr;
+        }
+    }
+}
+
+// convergence test of one iteration: relative residual <= tol (done = 1),
+// stagnation after three iterations (residual above half the previous, 2),
+// iteration cap (3)
+__global__ void ref_decide_kernel(RefState* st, double tol2, int maxit) {
+    if (st->done) return;
+    st->it += 1;
+    const double rn2 = st->rn2;
+    st->rn2 = 0.0;
+    st->rel2 = rn2 / st->bn2;
+    if (rn2 <= tol2 * st->bn2)
+        st->done = 1;
+    else if (st->it >= 3 && rn2 > 0.25 * st->prev2)
+        st->done = 2;
+    else if (st->it >= maxit)
+        st->done = 3;
+    st->prev2 = rn2;
+}
+
 struct LinWs {
     GridBar* bar;
     PivSlot* slots;  // [2][PANEL_MAXB]
@@ -727,6 +820,74 @@ int lu_solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t*
     return check_flag(ctx, s, "lu_solve");
 }
 
+// Refinement with the tile-pivoted factor, queued in batches of iterations
+// with one synchronisation per batch (normally one per call): the convergence
+// test runs on the device and the remaining kernels of a finished refinement
+// return at once.  Same iterations and stopping rules as the synchronous
+// loop of bem_refine_solve.
+int refine_async(bem_ctx* ctx, bool C, const void* A_hi, const void* LU_lo, const int32_t* piv, const void* dinv,
+                 int64_t n, int64_t lda, const double* b, double* x, double tol, int maxit, int* iters,
+                 double* relres, cudaStream_t s) {
+    const int W = C ? 2 : 1;
+    const int64_t nd = W * n;
+    // r (nd) and the state
+    double* r = nullptr;
+    if (int rc = bem_check_cuda(ctx, cudaMallocAsync((void**)&r, sizeof(double) * nd + 64, s), "refine alloc"))
+        return rc;
+    RefState* st = reinterpret_cast<RefState*>(r + nd);
+    int rc = BEM_OK;
+    const unsigned vblocks = (unsigned)((nd + 255) / 256);
+    const unsigned sblocks = (unsigned)std::min<int64_t>(ctx->num_sms * 4, (nd + 255) / 256);
+    ref_init_kernel<<<1, 1, 0, s>>>(st);
+    sumsq_kernel<<<sblocks, 256, 0, s>>>(b, nd, &st->bn2);
+    ref_start_kernel<<<1, 1, 0, s>>>(st);
+    ctx->launches += 3;
+    cudaMemsetAsync(ctx->flags + 3, 0, sizeof(int32_t), s);
+    cudaMemsetAsync(x, 0, sizeof(double) * nd, s);
+    cudaMemcpyAsync(r, b, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s);
+    const int* skip = &st->done;
+    RefState h{};
+    int32_t flg[2] = {0, 0};
+    int queued = 0;
+    while (rc == BEM_OK) {
+        const int batch = std::min(3, maxit - queued);
+        for (int i = 0; i < batch && rc == BEM_OK; ++i) {
+            double* d = nullptr;
+            rc = bem_tiled_precond_async(ctx, C ? BEM_C64 : BEM_F32, LU_lo, n, lda, piv, dinv, r, &d, skip, s);
+            if (rc) break;
+            ref_axpy_kernel<<<vblocks, 256, 0, s>>>(x, d, nd, st);
+            const unsigned rblocks = (unsigned)((n + 7) / 8);
+            if (C)
+                ref_residual_kernel<double, true><<<rblocks, 256, 0, s>>>((const double*)A_hi, n, lda, x, b, r, st);
+            else
+                ref_residual_kernel<double, false><<<rblocks, 256, 0, s>>>((const double*)A_hi, n, lda, x, b, r, st);
+            ref_sumsq_kernel<<<sblocks, 256, 0, s>>>(r, nd, st);
+            ref_decide_kernel<<<1, 1, 0, s>>>(st, tol * tol, maxit);
+            ctx->launches += 4;
+            rc = bem_check_cuda(ctx, cudaGetLastError(), "refinement step");
+            ++queued;
+        }
+        if (rc) break;
+        cudaMemcpyAsync(&h, st, sizeof(RefState), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&flg[0], ctx->flags + 3, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&flg[1], ctx->flags + 4, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "refinement");
+        if (rc) break;
+        if ((rc = bem_take_factor_error(ctx, flg[1], s))) break;
+        if (flg[0] != 0) {
+            rc = bem_fail(ctx, BEM_ERR_TIMEOUT, "tiled solve: a ready-flag wait hit its iteration cap");
+            break;
+        }
+        if (h.done != 0 || queued >= maxit) break;
+    }
+    cudaFreeAsync(r, s);
+    if (rc) return rc;
+    if (iters) *iters = h.it;
+    if (relres) *relres = std::sqrt(h.rel2);
+    if (h.done != 1) return bem_fail(ctx, BEM_ERR_NOCONVERGE, "refinement did not reach tol in maxit iterations");
+    return BEM_OK;
+}
+
 template <typename T, bool C>
 int gemv_t(bem_ctx* ctx, const T* A, int64_t m, int64_t n, int64_t lda, const double* x, double* y, double alpha,
            double beta, cudaStream_t s) {
@@ -796,6 +957,8 @@ int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* L
     const int W = C ? 2 : 1;
     const int64_t nd = W * n;
     cudaStream_t s = (cudaStream_t)stream;
+    if (dinv) return refine_async(ctx, C, A_hi, LU_lo, piv, dinv, n, lda, (const double*)b, (double*)x, tol, maxit,
+                                  iters, relres, s);
     // workspace beyond the lu_solve scratch: r (nd), d (nd), norms (2)
     double* r = nullptr;
     if (int rc = bem_check_cuda(ctx, cudaMallocAsync((void**)&r, sizeof(double) * (2 * nd + 4), s), "refine alloc"))

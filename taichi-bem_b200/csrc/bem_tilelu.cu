@@ -497,7 +497,11 @@ constexpr size_t solve_smem_bytes(size_t elem) { return 2 * elem * LU_T * SOLVE_
 
 template <typename T, bool C>
 __global__ void __launch_bounds__(256) tile_solve_kernel(const T* LU, int64_t lda, int n, const CE<T>* dinv,
-                                                         double* x, int* flags, int epoch, int32_t* err) {
+                                                         double* x, int* flags, int epoch, int32_t* err,
+                                                         const int* skip) {
+    // skip != NULL: a device word set by the asynchronous refinement once it
+    // has converged; the later, already queued solves return at once
+    if (skip != nullptr && *skip != 0) return;
     constexpr int RW = LU_T / 8;  // rows per warp in the streamed part
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CE<T>* sB = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][SOLVE_LD] last dependency block
@@ -756,17 +760,10 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
         if (int rc = update(c2, c2 + next, rest2, rest2 - next, k0, (int64_t)m1 + m2)) return rc;
         if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "tiled lu step")) return rc;
     }
-    // the tensor-core update records a bounded-wait timeout in flags[4]
-    int32_t tc_err = 0;
-    if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(&tc_err, ctx->flags + 4, sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                                     s), "flag readback"))
-        return rc;
-    if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "tiled lu")) return rc;
-    if (tc_err != 0) {
-        cudaMemsetAsync(ctx->flags + 4, 0, sizeof(int32_t), s);
-        return bem_fail(ctx, BEM_ERR_TIMEOUT, "tiled lu: a tensor-core wait hit its iteration cap");
-    }
-    return BEM_OK;
+    // No synchronisation: a tensor-core update whose bounded wait ran out
+    // records it in flags[4], which the next solve on this context reads
+    // (bem_take_factor_error) after its own synchronisation.
+    return bem_check_cuda(ctx, cudaGetLastError(), "tiled lu");
 }
 
 template <typename T, bool C>
@@ -801,7 +798,8 @@ int solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t* pi
     P = std::min(P, ctx->num_sms);
     int ni = (int)n, epoch = 1;
     int32_t* err = ctx->flags + 3;
-    void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err};
+    const int* no_skip = nullptr;
+    void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err, (void*)&no_skip};
     if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args,
                                                                 ssmem, s),
                                 "tile_solve_kernel"))
@@ -810,10 +808,65 @@ int solve_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t* pi
     if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(b, x, sizeof(double) * W * n, cudaMemcpyDeviceToDevice, s),
                                 "tiled solve copy"))
         return rc;
-    int32_t e = 0;
-    cudaMemcpyAsync(&e, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    int32_t e[2] = {0, 0};
+    cudaMemcpyAsync(&e[0], err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&e[1], ctx->flags + 4, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "tiled solve")) return rc;
-    if (e != 0) return bem_fail(ctx, BEM_ERR_TIMEOUT, "tiled solve: a ready-flag wait hit its iteration cap");
+    if (int rc = bem_take_factor_error(ctx, e[1], s)) return rc;
+    if (e[0] != 0) return bem_fail(ctx, BEM_ERR_TIMEOUT, "tiled solve: a ready-flag wait hit its iteration cap");
+    return BEM_OK;
+}
+
+// One preconditioner application of the asynchronous refinement:
+// out = (P^T L U)^{-1} r with the tile-pivoted factor, left in the solve
+// workspace (*out), queued without synchronisation and skipped on the device
+// when *skip != 0.  The caller resets ctx->flags[3] once before its loop and
+// reads it after its final synchronisation.
+__global__ void permute_if_kernel(const double* b, const int32_t* perm, double* x, int n, int W, const int* skip) {
+    if (*skip != 0) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = perm[i];
+    for (int w = 0; w < W; ++w) x[W * i + w] = b[W * s + w];
+}
+
+template <typename T, bool C>
+int precond_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t* piv, const CE<T>* dinv,
+              const double* r, double** out, const int* skip, cudaStream_t s) {
+    const int W = C ? 2 : 1;
+    const int nbk = (int)((n + LU_T - 1) / LU_T);
+    size_t off_flags = ((size_t)n * 4 + 255) & ~size_t(255);
+    size_t off_x = off_flags + (((size_t)2 * nbk * 4 + 255) & ~size_t(255));
+    size_t total = off_x + sizeof(double) * W * (size_t)n;
+    if (int rc = bem_ws_reserve(ctx, total)) return rc;
+    char* base = (char*)ctx->ws;
+    int32_t* perm = (int32_t*)base;
+    int* flags = (int*)(base + off_flags);
+    double* x = (double*)(base + off_x);
+    if ((size_t)n * sizeof(int32_t) > 200 * 1024) return bem_fail(ctx, BEM_ERR_INVALID, "tiled solve: n > 51200");
+    const unsigned ptiles = (unsigned)((n + LU_T - 1) / LU_T);
+    tile_piv_to_perm_kernel<<<(ptiles + 127) / 128, 128, 0, s>>>(piv, perm, (int)n);
+    permute_if_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(r, perm, x, (int)n, W, skip);
+    cudaMemsetAsync(flags, 0, sizeof(int) * 2 * nbk, s);
+    ctx->launches += 2;
+    const size_t ssmem = solve_smem_bytes(sizeof(CE<T>));
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(tile_solve_kernel<T, C>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem),
+                                "tile_solve_kernel smem"))
+        return rc;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, ssmem);
+    int P = std::max(1, std::min(nbk, per_sm * ctx->num_sms));
+    P = std::min(P, ctx->num_sms);
+    int ni = (int)n, epoch = 1;
+    int32_t* err = ctx->flags + 3;
+    void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err, (void*)&skip};
+    if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args,
+                                                                ssmem, s),
+                                "tile_solve_kernel"))
+        return rc;
+    ctx->launches++;
+    *out = x;
     return BEM_OK;
 }
 
@@ -854,6 +907,17 @@ int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64
 }
 
 }  // extern "C"
+
+int bem_tiled_precond_async(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
+                            const void* dinv, const double* r, double** out, const int* skip, cudaStream_t s) {
+    switch (dtype) {
+        case BEM_F64: return precond_t<double, false>(ctx, (const double*)LU, n, lda, piv, (const CE<double>*)dinv, r, out, skip, s);
+        case BEM_C128: return precond_t<double, true>(ctx, (const double*)LU, n, lda, piv, (const CE<double>*)dinv, r, out, skip, s);
+        case BEM_F32: return precond_t<float, false>(ctx, (const float*)LU, n, lda, piv, (const CE<float>*)dinv, r, out, skip, s);
+        case BEM_C64: return precond_t<float, true>(ctx, (const float*)LU, n, lda, piv, (const CE<float>*)dinv, r, out, skip, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "tiled precond: unknown dtype");
+    }
+}
 
 // ----------------------------------------------------------------------------
 // Allocation-free variant of bem_lu_solve_tiled.
@@ -942,7 +1006,8 @@ int solve_static_t(const T* LU, int64_t n, int64_t lda, const int32_t* piv, cons
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_solve_kernel<T, C>, 256, ssmem);
     int P = std::max(1, std::min(nbk, std::min(per_sm * sms, sms)));
     int ni = (int)n, epoch = 1;
-    void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err};
+    const int* no_skip = nullptr;
+    void* args[] = {(void*)&LU, &lda, &ni, (void*)&dinv, &x, &flags, &epoch, &err, (void*)&no_skip};
     if (cudaLaunchCooperativeKernel((const void*)tile_solve_kernel<T, C>, P, 256, args, ssmem, s) != cudaSuccess) {
         cudaGetLastError();
         return BEM_ERR_CUDA;
