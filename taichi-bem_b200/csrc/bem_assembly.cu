@@ -871,6 +871,121 @@ __global__ void mass_kernel(MassArgs a) {
     }
 }
 
+// Fused near field of the Dirichlet pass: V (P0 x P0, dense, `v`) and the
+// matrix-free K g (P0 rows, NBD data bases on the trial panel, `k`) of one
+// near pair from the same Sauter-Schwab points.  Each point's r, 1/r and
+// e^{ikr} serve both integrands; the values and their accumulation are those
+// of near_kernel<BEM_OP_V, HELM, 1, 1> and near_kernel<BEM_OP_K, HELM, 1, NBD>
+// (the swapped coincide term takes K's kernel with -d, as there).  One warp
+// per near pair.
+template <bool HELM, int NBD>
+__global__ void __launch_bounds__(128) near_vkg_kernel(NearArgs v, NearArgs k) {
+    const int lane = threadIdx.x & 31;
+    const int64_t pid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (pid >= v.n_near) return;
+    const int4 e = v.near[pid];
+    const int gi = e.x, gj = e.y, rel = e.z;
+    const int li = v.test_local[gi], lj = v.trial_local[gj];
+    if (li < 0 || lj < 0) return;  // warp-uniform
+    const int permx = v.quirk ? (0 | (1 << 2) | (2 << 4)) : (e.w & 63);
+    const int permy = v.quirk ? (0 | (1 << 2) | (2 << 4)) : ((e.w >> 6) & 63);
+    NearPanel X, Y;
+    load_near_panel(X, v, gi, permx);
+    load_near_panel(Y, v, gj, permy);
+    int sy[NBD];
+#pragma unroll
+    for (int b = 0; b < NBD; ++b) sy[b] = NBD == 1 ? -1 : Y.slot[b];
+    double av_re = 0.0, av_im = 0.0, ak_re[NBD], ak_im[NBD];
+#pragma unroll
+    for (int b = 0; b < NBD; ++b) ak_re[b] = ak_im[b] = 0.0;
+    const double kk = v.k;
+    auto add = [&](double r1x, double r2x, double r1y, double r2y, double wj, bool second, double px1, double px2,
+                   double py1, double py2) {
+        double x[3], yv[3];
+        for (int c = 0; c < 3; ++c) {
+            x[c] = (1.0 - r1x) * X.x1[c] + (r1x - r2x) * X.x2[c] + r2x * X.x3[c];
+            yv[c] = (1.0 - r1y) * Y.x1[c] + (r1y - r2y) * Y.x2[c] + r2y * Y.x3[c];
+        }
+        const double dx = x[0] - yv[0], dy = x[1] - yv[1], dz = x[2] - yv[2];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        double r, rinv;
+        dev_r_rinv(r2, r, rinv);
+        // K: grad_G_y(x, y, n_y); the swapped coincide term grad_G_y(y, x, n_y)
+        const double dn = (second ? -1.0 : 1.0) * (dx * Y.n[0] + dy * Y.n[1] + dz * Y.n[2]);
+        const double t = dn * rinv * rinv * rinv;
+        double vre, vim, kre, kim;
+        if (HELM) {
+            const double kr = kk * r;
+            double sn, cs;
+            dev_sincos(kr, &sn, &cs);
+            vre = rinv * cs;
+            vim = rinv * sn;
+            kre = t * (cs + kr * sn);
+            kim = t * (sn - kr * cs);
+        } else {
+            vre = rinv;
+            vim = 0.0;
+            kre = t;
+            kim = 0.0;
+        }
+        av_re += vre * wj;
+        av_im += vim * wj;
+        (void)px1;
+        (void)px2;
+#pragma unroll
+        for (int b = 0; b < NBD; ++b) {
+            const double phy = NBD == 1 ? 1.0 : shape_slot(py1, py2, sy[b]);
+            ak_re[b] += (kre * wj) * phy;
+            ak_im[b] += (kim * wj) * phy;
+        }
+    };
+    const int Q = v.Q;
+    const int Q4 = Q * Q * Q * Q;
+    for (int p = lane; p < Q4; p += 32) {
+        int iw = p % Q, iz = (p / Q) % Q, iy = (p / (Q * Q)) % Q, ix = p / (Q * Q * Q);
+        const double xsi = v.gp[ix], eta1 = v.gp[iy], eta2 = v.gp[iz], eta3 = v.gp[iw];
+        const double weight = (v.gw[ix] * v.gw[iy] * (X.area * 2.0)) * (v.gw[iz] * v.gw[iw] * (Y.area * 2.0));
+        near_points(rel, v.quirk != 0, xsi, eta1, eta2, eta3, weight, add);
+    }
+    av_re = warp_sum(av_re);
+    av_im = warp_sum(av_im);
+#pragma unroll
+    for (int b = 0; b < NBD; ++b) {
+        ak_re[b] = warp_sum(ak_re[b]);
+        ak_im[b] = warp_sum(ak_im[b]);
+    }
+    if (lane != 0) return;
+    {
+        const int row = v.test_dof[li], col = v.trial_dof[lj];
+        if (row >= 0 && col >= 0)
+            add_entry<HELM>(v.out, (int64_t)row * v.ld + col, v.scale * BEM_INV4PI * av_re,
+                            v.scale * BEM_INV4PI * av_im, true);
+    }
+    const int row = k.test_dof[li];
+    if (row < 0) return;
+    double cr = 0.0, ci = 0.0;
+#pragma unroll
+    for (int b = 0; b < NBD; ++b) {
+        const int col = k.trial_dof[lj * NBD + b];
+        if (col < 0) continue;
+        const double vr = ak_re[b] * BEM_INV4PI, vi = ak_im[b] * BEM_INV4PI;
+        if (HELM) {
+            double xr = k.x[2 * col], xi = k.x[2 * col + 1];
+            if (k.conj_x) xi = -xi;
+            cr += vr * xr - vi * xi;
+            ci += vr * xi + vi * xr;
+        } else {
+            cr += vr * k.x[col];
+        }
+    }
+    if (HELM) {
+        atomicAdd(k.y + 2 * row, k.scale * cr);
+        atomicAdd(k.y + 2 * row + 1, k.scale * ci);
+    } else {
+        atomicAdd(k.y + row, k.scale * cr);
+    }
+}
+
 // ----------------------------------------------------------------------------
 // Fused Dirichlet-system pass: V (P0 x P0, dense) and the matrix-free K g
 // (P0 test rows, g interpolated from P1 vertex data) over the same separate
@@ -1850,20 +1965,18 @@ int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
         nk.scale = scale_k;
         nk.conj_x = conj_g;
         if (helm) {
-            near_kernel<BEM_OP_V, true, 1, 1><<<blocks, 128, 0, sn>>>(nv);
             if (data->nb == 3)
-                near_kernel<BEM_OP_K, true, 1, 3><<<blocks, 128, 0, sn>>>(nk);
+                near_vkg_kernel<true, 3><<<blocks, 128, 0, sn>>>(nv, nk);
             else
-                near_kernel<BEM_OP_K, true, 1, 1><<<blocks, 128, 0, sn>>>(nk);
+                near_vkg_kernel<true, 1><<<blocks, 128, 0, sn>>>(nv, nk);
         } else {
-            near_kernel<BEM_OP_V, false, 1, 1><<<blocks, 128, 0, sn>>>(nv);
             if (data->nb == 3)
-                near_kernel<BEM_OP_K, false, 1, 3><<<blocks, 128, 0, sn>>>(nk);
+                near_vkg_kernel<false, 3><<<blocks, 128, 0, sn>>>(nv, nk);
             else
-                near_kernel<BEM_OP_K, false, 1, 1><<<blocks, 128, 0, sn>>>(nk);
+                near_vkg_kernel<false, 1><<<blocks, 128, 0, sn>>>(nv, nk);
         }
-        ctx->launches += 2;
-        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "near_kernel launch")) return rc;
+        ctx->launches++;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "near_vkg_kernel launch")) return rc;
     }
     if (side) {
         cudaEventRecord(ctx->ev_diag, ctx->aux);
