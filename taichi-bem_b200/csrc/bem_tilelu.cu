@@ -3,12 +3,15 @@
 //
 // Factorisation, per diagonal block k (LU_T = 64 columns):
 //   diag   : one CTA factors the 64x64 diagonal block with partial pivoting
-//            restricted to the block's rows, and forms the explicit inverses
-//            Linv_k (unit lower) and Uinv_k (upper), stored in `dinv`;
+//            restricted to the block's rows;
 //   laswp  : the block's row swaps applied to the other columns;
-//   U12 = Linv_k A12 and L21 = A21 Uinv_k: one CTA per 64-wide tile, products
-//            out of shared memory (no sequential substitution);
+//   U12 = L11^{-1} A12 and L21 = A21 U11^{-1}: one CTA per 64-wide tile,
+//            substitution against the factored diagonal block, the tile held
+//            in registers (one CTA barrier per step);
 //   update : A22 -= L21 U12 (the trailing GEMM of bem_gemm.cuh).
+// After the last block, one launch forms the explicit inverses Linv_k (unit
+// lower) and Uinv_k (upper) of every diagonal block (`dinv`, used by the
+// solves), one CTA per block, off the factorisation's dependency chain.
 // No grid-wide synchronisation is needed.  Pivoting within the diagonal tile
 // is weaker than full partial pivoting; the FP64 iterative refinement that
 // consumes this factor corrects the difference (and reports non-convergence).
@@ -62,7 +65,7 @@ __device__ __forceinline__ CE<T> cinv(CE<T> a) {
 }
 
 // --------------------------------------------------------------------------
-// diagonal tile: GEPP inside the tile + explicit inverses
+// diagonal tile: GEPP inside the tile; explicit inverses of the factored tiles
 // --------------------------------------------------------------------------
 // Pivot key of a candidate: |re| + |im| as float bits (monotonic for
 // non-negative floats) above 63 - row, so that atomicMax picks the largest
@@ -77,10 +80,12 @@ __device__ __forceinline__ unsigned long long pivot_key(CE<T> v, int r) {
 
 constexpr int DIAG_LD = LU_T + 1;  // padded row stride: column reads hit distinct banks
 constexpr int DIAG_PW = 8;         // panel width of the blocked factorisation
-constexpr size_t diag_smem_bytes(size_t elem) { return elem * (LU_T * DIAG_LD + LU_T * LU_T); }
+constexpr size_t diag_smem_bytes(size_t elem) { return elem * LU_T * DIAG_LD; }
+// tile_inv_kernel: the factored block and the inverse being built
+constexpr size_t inv_smem_bytes(size_t elem) { return elem * (LU_T * DIAG_LD + LU_T * LU_T); }
 
 // One CTA of 256 threads factors the 64x64 diagonal tile (GEPP restricted to
-// the tile's rows) and forms the explicit inverses.  Blocked by panels of
+// the tile's rows).  Blocked by panels of
 // DIAG_PW columns:
 //   panel  : the 64 x DIAG_PW panel in registers (two elements per thread);
 //            per column a pivot max over packed keys (shuffles, then across
@@ -92,16 +97,13 @@ constexpr size_t diag_smem_bytes(size_t elem) { return elem * (LU_T * DIAG_LD + 
 //            (one thread per column);
 //   update : rank-DIAG_PW update of the trailing block, one column per thread
 //            with the column's U12 values held in registers.
-// Inverses: Linv (unit lower) and Uinv (upper) by block substitution over
-// DIAG_PW-row blocks against the identity, one after the other in one buffer.
-// Shared memory stays under 65 KB so the kernel fits beside the trailing
-// GEMM's CTAs on an SM.
+// The explicit inverses are formed later, by tile_inv_kernel.  Shared memory
+// (33 KB for complex FP32) leaves room for the trailing GEMM's CTAs on an SM.
 template <typename T, bool C>
 __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n, int k0, int32_t* piv,
-                                                        CE<T>* dinv, int32_t* info) {
+                                                        int32_t* info) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CE<T>* S = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][DIAG_LD]
-    CE<T>* X = S + LU_T * DIAG_LD;                  // [LU_T][LU_T] inverse being built
     __shared__ int s_zero_pivot;                    // first zero pivot of this tile (1-based), 0 = none
     __shared__ unsigned long long s_wkey[8];        // per-warp pivot keys
     __shared__ CE<T> s_rowj[DIAG_PW], s_rowp[DIAG_PW];
@@ -247,11 +249,38 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
             __syncthreads();
         }
     }
+    if (tid == 0 && s_zero_pivot != 0 && *info == 0) *info = s_zero_pivot;
+    for (int e = tid; e < LU_T * LU_T; e += blockDim.x) {
+        const int r = e / LU_T, cc = e - r * LU_T;
+        if (r < m && cc < m) stE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + cc, S[r * DIAG_LD + cc]);
+    }
+}
+
+
+// Explicit inverses Linv (unit lower) and Uinv (upper) of every factored
+// diagonal block, one CTA per block (blockIdx.x = block), by block
+// substitution over DIAG_PW-row blocks against the identity.  Runs once the
+// factorisation is complete: later row swaps never touch a diagonal block.
+template <typename T, bool C>
+__global__ void __launch_bounds__(256) tile_inv_kernel(const T* A, int64_t lda, int n, CE<T>* dinv) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CE<T>* S = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][DIAG_LD] factored block
+    CE<T>* X = S + LU_T * DIAG_LD;                  // [LU_T][LU_T] inverse being built
+    const int k0 = blockIdx.x * LU_T;
+    const int m = min(LU_T, n - k0);
+    const int tid = threadIdx.x;
+    for (int e = tid; e < LU_T * LU_T; e += blockDim.x) {
+        const int r = e / LU_T, c = e - r * LU_T;
+        CE<T> v = CE<T>{T(0), T(0)};
+        if (r < m && c < m) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c);
+        S[r * DIAG_LD + c] = v;
+    }
+    __syncthreads();
+    CE<T>* D = dinv + (size_t)blockIdx.x * 2 * LU_T * LU_T;
     // ---- explicit inverses by block substitution against the identity ----
     // Linv: for row block i: X_i = L_ii^{-1} (E_i - sum_{k<i} L_ik X_k)
     // Uinv: for row block i (descending): X_i = U_ii^{-1} (E_i - sum_{k>i} U_ik X_k)
     // thread: column c = tid & 63, rows (tid >> 6) * 2 + {0, 1} of the block
-    CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T;
     __shared__ CE<T> s_rdiag[LU_T];  // 1 / U[r][r], formed in parallel off the substitution chain
     if (tid < LU_T) s_rdiag[tid] = tid < m ? cinv(S[tid * DIAG_LD + tid]) : CE<T>{T(1), T(0)};
     const int c = tid & 63, rq = (tid >> 6) * 2;
@@ -332,11 +361,6 @@ __global__ void __launch_bounds__(256) tile_diag_kernel(T* A, int64_t lda, int n
         for (int e = tid; e < LU_T * LU_T; e += blockDim.x) D[which * LU_T * LU_T + e] = X[e];
         __syncthreads();
     }
-    if (tid == 0 && s_zero_pivot != 0 && *info == 0) *info = s_zero_pivot;
-    for (int e = tid; e < LU_T * LU_T; e += blockDim.x) {
-        const int r = e / LU_T, cc = e - r * LU_T;
-        if (r < m && cc < m) stE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + cc, S[r * DIAG_LD + cc]);
-    }
 }
 
 template <typename T, bool C>
@@ -353,59 +377,104 @@ __global__ void tile_laswp_kernel(T* A, int64_t lda, int n, int k0, int m, const
     }
 }
 
-// blockIdx.y = 0: U12 tile (rows k0.., 64 columns) <- Linv * tile
-// blockIdx.y = 1: L21 tile (64 rows, columns k0..) <- tile * Uinv
-// Both products run in one launch (they touch disjoint parts of A).  Thread
-// (tx, ty) owns outputs rows ty + 16 i, columns tx + 16 j: the column operand
-// is read as 16 consecutive elements per half-warp and the row operand from a
-// padded row stride, so the shared-memory reads are free of bank conflicts.
+// blockIdx.y = 0: U12 tile (rows k0.., 64 columns) <- L11^{-1} tile (unit lower)
+// blockIdx.y = 1: L21 tile (64 rows, columns k0..) <- tile U11^{-1} (upper)
+// Both run in one launch (they touch disjoint parts of A).  The factored
+// diagonal block is staged in shared memory and the tile is held in
+// registers: thread (tx, ty) owns rows ty + 16 i, columns tx + 16 j.  Step q
+// publishes the finished row q (mode 0) or column q, scaled by 1/U_qq
+// (mode 1), through a double-buffered shared vector and updates the entries
+// below / right of it: one CTA barrier per step.
 constexpr int APPLY_LD = LU_T + 1;
-constexpr size_t apply_smem_bytes(size_t elem) { return 2 * elem * LU_T * APPLY_LD; }
+constexpr size_t apply_smem_bytes(size_t elem) { return elem * LU_T * APPLY_LD; }
 
 template <typename T, bool C>
-__global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int n, int k0, int m,
-                                                         const CE<T>* dinv) {
+__global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int n, int k0, int m) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    CE<T>* M = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][APPLY_LD] inverse
-    CE<T>* X = M + LU_T * APPLY_LD;                 // [LU_T][APPLY_LD] tile
+    CE<T>* M = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][APPLY_LD] factored diagonal block
+    __shared__ CE<T> s_vec[2][LU_T];
+    __shared__ CE<T> s_rdiag[LU_T];
     const int mode = blockIdx.y;
-    const CE<T>* D = dinv + (size_t)(k0 / LU_T) * 2 * LU_T * LU_T + (mode == 0 ? 0 : LU_T * LU_T);
     const int base = k0 + m + blockIdx.x * LU_T;  // first column (mode 0) / row (mode 1) of the tile
     const int cnt = min(LU_T, n - base);
     for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
         const int r = e / LU_T, c = e - r * LU_T;
-        M[r * APPLY_LD + c] = D[e];
         CE<T> v = CE<T>{T(0), T(0)};
-        if (mode == 0) {
-            if (r < m && c < cnt) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + base + c);
-        } else {
-            if (r < cnt && c < m) v = ldE<T, C>(A, (int64_t)(base + r) * lda + k0 + c);
-        }
-        X[r * APPLY_LD + c] = v;
+        if (r < m && c < m) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c);
+        M[r * APPLY_LD + c] = v;
     }
-    __syncthreads();
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const CE<T>* Rop = mode == 0 ? M : X;  // row operand (left factor)
-    const CE<T>* Cop = mode == 0 ? X : M;  // column operand (right factor)
-    CE<T> acc[4][4];
+    CE<T> x[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = CE<T>{T(0), T(0)};
-    for (int q = 0; q < m; ++q) {
-        CE<T> a[4], b[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            a[i] = Rop[(ty + 16 * i) * APPLY_LD + q];
-            b[i] = Cop[q * APPLY_LD + tx + 16 * i];
+        for (int j = 0; j < 4; ++j) {
+            const int r = ty + 16 * i, c = tx + 16 * j;
+            CE<T> v = CE<T>{T(0), T(0)};
+            if (mode == 0) {
+                if (r < m && c < cnt) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + base + c);
+            } else {
+                if (r < cnt && c < m) v = ldE<T, C>(A, (int64_t)(base + r) * lda + k0 + c);
+            }
+            x[i][j] = v;
         }
+    __syncthreads();
+    if (mode == 1 && threadIdx.x < LU_T)
+        s_rdiag[threadIdx.x] = threadIdx.x < m ? cinv(M[threadIdx.x * APPLY_LD + threadIdx.x]) : CE<T>{T(0), T(0)};
+    __syncthreads();
+    for (int q = 0; q < m; ++q) {
+        CE<T>* v = s_vec[q & 1];
+        if (mode == 0) {
+            // row q is final: its owners publish it, then rows r > q take L_rq x_q
+            if (ty == (q & 15)) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 4; ++i)
+                    if (ty + 16 * i == q) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) v[tx + 16 * j] = x[i][j];
+                    }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = ty + 16 * i;
+                if (r <= q) continue;
+                const CE<T> l = M[r * APPLY_LD + q];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const CE<T> u = v[tx + 16 * j];
+                    x[i][j].re -= l.re * u.re - (C ? l.im * u.im : T(0));
+                    if (C) x[i][j].im -= l.re * u.im + l.im * u.re;
+                }
+            }
+        } else {
+            // column q: scaled by 1/U_qq by its owners and published, then
+            // columns c > q take x_q U_qc
+            if (tx == (q & 15)) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (tx + 16 * j == q) {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            x[i][j] = cmul(x[i][j], s_rdiag[q]);
+                            v[ty + 16 * i] = x[i][j];
+                        }
+                    }
+            }
+            __syncthreads();
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                acc[i][j].re += a[i].re * b[j].re - (C ? a[i].im * b[j].im : T(0));
-                if (C) acc[i][j].im += a[i].re * b[j].im + a[i].im * b[j].re;
+                const int c = tx + 16 * j;
+                if (c <= q) continue;
+                const CE<T> u = M[q * APPLY_LD + c];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const CE<T> l = v[ty + 16 * i];
+                    x[i][j].re -= l.re * u.re - (C ? l.im * u.im : T(0));
+                    if (C) x[i][j].im -= l.re * u.im + l.im * u.re;
+                }
             }
+        }
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -413,9 +482,9 @@ __global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int 
         for (int j = 0; j < 4; ++j) {
             const int r = ty + 16 * i, c = tx + 16 * j;
             if (mode == 0) {
-                if (r < m && c < cnt) stE<T, C>(A, (int64_t)(k0 + r) * lda + base + c, acc[i][j]);
+                if (r < m && c < cnt) stE<T, C>(A, (int64_t)(k0 + r) * lda + base + c, x[i][j]);
             } else {
-                if (r < cnt && c < m) stE<T, C>(A, (int64_t)(base + r) * lda + k0 + c, acc[i][j]);
+                if (r < cnt && c < m) stE<T, C>(A, (int64_t)(base + r) * lda + k0 + c, x[i][j]);
             }
         }
 }
@@ -700,6 +769,8 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
     const size_t dsmem = diag_smem_bytes(sizeof(CE<T>));
     const size_t asmem = apply_smem_bytes(sizeof(CE<T>));
     cudaFuncSetAttribute(tile_diag_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem);
+    const size_t ismem = inv_smem_bytes(sizeof(CE<T>));
+    cudaFuncSetAttribute(tile_inv_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ismem);
     cudaFuncSetAttribute(tile_apply_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem);
     if (int rc = bem_lookahead_stream(ctx)) return rc;
     const int ni = (int)n;
@@ -714,7 +785,7 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
     auto diag_aside = [&](int64_t k0) {
         cudaEventRecord(ctx->ev_next, s);
         cudaStreamWaitEvent(ctx->aux, ctx->ev_next, 0);
-        tile_diag_kernel<T, C><<<1, 256, dsmem, ctx->aux>>>(A, lda, ni, (int)k0, piv, dinv, info);
+        tile_diag_kernel<T, C><<<1, 256, dsmem, ctx->aux>>>(A, lda, ni, (int)k0, piv, info);
         cudaEventRecord(ctx->ev_diag, ctx->aux);
         ctx->launches++;
     };
@@ -725,7 +796,7 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
         const int64_t rest = n - k0 - m;
         if (rest > 0) {
             const unsigned tiles = (unsigned)((rest + LU_T - 1) / LU_T);
-            tile_apply_kernel<T, C><<<dim3(tiles, 2), 256, asmem, s>>>(A, lda, ni, (int)k0, m, dinv);
+            tile_apply_kernel<T, C><<<dim3(tiles, 2), 256, asmem, s>>>(A, lda, ni, (int)k0, m);
             ctx->launches++;
         }
     };
@@ -736,7 +807,7 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
     // the read-modify-write traffic of the trailing GEMMs).  The update's first
     // tile column goes first so that the next pair's diagonal tile overlaps the
     // rest of it.
-    tile_diag_kernel<T, C><<<1, 256, dsmem, s>>>(A, lda, ni, 0, piv, dinv, info);
+    tile_diag_kernel<T, C><<<1, 256, dsmem, s>>>(A, lda, ni, 0, piv, info);
     ctx->launches++;
     bool on_aux = false;
     for (int64_t k0 = 0; k0 < n; k0 += 2 * LU_T) {
@@ -760,6 +831,9 @@ int factor_t(bem_ctx* ctx, T* A, int64_t n, int64_t lda, int32_t* piv, CE<T>* di
         if (int rc = update(c2, c2 + next, rest2, rest2 - next, k0, (int64_t)m1 + m2)) return rc;
         if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "tiled lu step")) return rc;
     }
+    // explicit inverses of every diagonal block (for the solves)
+    tile_inv_kernel<T, C><<<(unsigned)((n + LU_T - 1) / LU_T), 256, ismem, s>>>(A, lda, ni, dinv);
+    ctx->launches++;
     // No synchronisation: a tensor-core update whose bounded wait ran out
     // records it in flags[4], which the next solve on this context reads
     // (bem_take_factor_error) after its own synchronisation.
