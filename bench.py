@@ -6,7 +6,7 @@ exp(i k d.x) with a seeded random unit direction d.  One step = the whole hot
 path of BEMManager.run with inputs resident in HBM: single-layer assembly V
 (26.2 M complex entries; separate pairs in FP32, coincident/edge/vertex pairs
 in FP64), the matrix-free right-hand side 1/2 M g + K g, the FP32 LU factor and
-FP64 iterative refinement to relative residual 1e-12.
+FP64 iterative refinement to relative residual 1e-9.
 
   value  = V entries / time-to-solution (entries/s), device-timed with CUDA
            events per step, L2 flushed (256 MiB write) between steps;
@@ -67,79 +67,73 @@ def _dist():
     return ws, rank, local
 
 
+_NVML_CHILD = r"""
+import sys, time
+try:
+    import pynvml
+    pynvml.nvmlInit()
+    h = pynvml.nvmlDeviceGetHandleByPciBusId(sys.argv[1].encode())
+    smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+except Exception as exc:
+    print("fail", exc, flush=True)
+    sys.exit(0)
+print("ready", smax, flush=True)
+sys.stdin.readline()
+while True:
+    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+    mask = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+    print("S", sm, mask, flush=True)
+    time.sleep(0.2)
+"""
+
+
 class ClockSampler:
     """SM clocks and clock-event (throttle) reasons of this process's GPU
-    during the timed region: NVML polled every 200 ms from a background thread
-    (initialised and primed with one sample before the timed region starts,
-    so that no start-up work overlaps it); nvidia-smi in loop mode when NVML is
-    not available."""
+    during the timed region, polled every 200 ms through NVML by a separate
+    Python process (a thread of this process would compete with the
+    launching thread for the interpreter lock and delay its launches).  The
+    child initialises NVML before the timed region and starts sampling when
+    told to; nvidia-smi in loop mode is the fallback when NVML is missing."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
     def __init__(self, device_index):
         self.dev = device_index
-        self.samples, self.reasons, self.smax = [], set(), None
-        self.proc = self.thread = None
-
-    def _nvml_handle(self):
-        import pynvml
-        import torch
-        pynvml.nvmlInit()
-        p = torch.cuda.get_device_properties(self.dev)
-        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0".encode()
-        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
-
-    def _sample(self):
-        nv, h = self.nvml
-        self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
-        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-        for name, bit in self.REASONS.items():
-            if mask & bit:
-                self.reasons.add(name)
+        self.proc = None
+        self.source = None
+        self.smax = None
 
     def start(self):
-        import threading
+        import torch
+        p = torch.cuda.get_device_properties(self.dev)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
         try:
-            self.nvml = self._nvml_handle()
-            nv, h = self.nvml
-            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
-            self._sample()
-            self.samples, self.reasons = [], set()  # the priming sample precedes the timed region
-        except Exception:
-            self.nvml = None
-            try:
-                self.proc = subprocess.Popen(
-                    ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,"
-                     "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                     "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                     "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
-                    stderr=subprocess.DEVNULL, text=True)
-                time.sleep(2.0)
-            except OSError:
-                self.proc = None
-            return
-        self.stop_flag = threading.Event()
-
-        def loop():
-            while not self.stop_flag.wait(0.2):
-                try:
-                    self._sample()
-                except Exception:
-                    break
-
-        self.thread = threading.Thread(target=loop, daemon=True)
-        self.thread.start()
+            self.proc = subprocess.Popen([sys.executable, "-c", _NVML_CHILD, bus], stdin=subprocess.PIPE,
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            first = self.proc.stdout.readline().split()
+            if first and first[0] == "ready":
+                self.smax = float(first[1])
+                self.source = "nvml"
+                self.proc.stdin.write("go\n")
+                self.proc.stdin.flush()
+                return
+            self.proc.wait(timeout=5)
+        except (OSError, subprocess.TimeoutExpired, ValueError, IndexError):
+            pass
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi"
+            time.sleep(2.0)
+        except OSError:
+            self.proc = None
 
     def stop(self):
-        if self.thread is not None:
-            self.stop_flag.set()
-            self.thread.join(timeout=2.0)
-            try:
-                self._sample()
-            except Exception:
-                pass
-            return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
-                    "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
@@ -148,22 +142,34 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
-            parts = [q.strip() for q in line.split(",")]
-            if len(parts) < 6:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                smax = float(parts[1])
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[2:6]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
+        sm, reasons = [], set()
+        smax = self.smax
+        if self.source == "nvml":
+            for line in out.strip().splitlines():
+                parts = line.split()
+                if len(parts) != 3 or parts[0] != "S":
+                    continue
+                sm.append(float(parts[1]))
+                mask = int(parts[2])
+                for name, bit in self.REASONS.items():
+                    if mask & bit:
+                        reasons.add(name)
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in out.strip().splitlines():
+                parts = [q.strip() for q in line.split(",")]
+                if len(parts) < 6:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    smax = float(parts[1])
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[2:6]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm), "source": "nvidia-smi"}
+                "samples": len(sm), "source": self.source}
 
 
 def cpu_reference(steps: int, warmup: int, threads: int | None = None, sample_rows: int | None = None,

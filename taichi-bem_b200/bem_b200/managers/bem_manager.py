@@ -605,10 +605,13 @@ class BEMManager:
                                        rc._rhs_vec, scale=1.0, scale_k=1.0, conj_g=self.conj_data)
 
     def run(self):
-        """BEMManager.run (BEM_manager.py:990-1030) without the GUI colouring."""
+        """BEMManager.run (BEM_manager.py:990-1030) without the GUI colouring.
+        The exact traces do not depend on the solution, so they are queued
+        before the solve, whose refinement is the step's one host
+        synchronisation; only the per-vertex splat follows it."""
         self.assemble_system()
-        self.solve()
         self.compute_analytical_raw_solved()
+        self.solve()
         self.splat_u_from_raw_solved_to_vertices()
 
     def assemble_system(self):
