@@ -118,3 +118,37 @@ def test_tiled_fp32_factor_with_refinement(engine, cplx):
     it, rr = engine.refine_solve(A_hi, LU, piv, bd, xd, tol=1e-13, maxit=30, dinv=dinv)
     assert rr <= 1e-13
     assert rel_err(xd.cpu().numpy(), np.linalg.solve(A, b)) < 1e-11
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_async_refinement_stopping_rules(engine, cplx):
+    """The device-side stopping test of the tiled refinement: b = 0 returns
+    x = 0 after no iteration; an iteration cap below the needed count reports
+    BEM_ERR_NOCONVERGE with the residual reached; a later call on the same
+    factor converges (the state of a call does not leak into the next); and
+    the iteration count matches the synchronous loop's rule (stop at the
+    first residual below tol)."""
+    from bem_b200._lib import BemError
+    n = 300
+    A = _mat(n, cplx, 5) + 2 * n ** 0.5 * np.eye(n)
+    A_hi = torch.as_tensor(A, device="cuda").contiguous()
+    LU = A_hi.to(torch.complex64 if cplx else torch.float32).contiguous()
+    piv, dinv, _ = engine.lu_factor_tiled(LU)
+    zero = torch.zeros(n, dtype=A_hi.dtype, device="cuda")
+    x = torch.full_like(zero, 7.0)
+    it, rr = engine.refine_solve(A_hi, LU, piv, zero, x, tol=1e-12, maxit=10, dinv=dinv)
+    assert it == 0 and rr == 0.0 and float(x.abs().max()) == 0.0
+    rng = np.random.default_rng(8)
+    b = rng.standard_normal(n) + (1j * rng.standard_normal(n) if cplx else 0)
+    bd = torch.as_tensor(b, device="cuda").contiguous()
+    with pytest.raises(BemError) as exc:
+        engine.refine_solve(A_hi, LU, piv, bd, torch.zeros_like(bd), tol=1e-14, maxit=1, dinv=dinv)
+    assert exc.value.code == -4
+    xd = torch.zeros_like(bd)
+    it, rr = engine.refine_solve(A_hi, LU, piv, bd, xd, tol=1e-12, maxit=20, dinv=dinv)
+    assert rr <= 1e-12 and 1 <= it <= 6
+    # the same stopping point as solving to a looser tolerance and counting
+    xl = torch.zeros_like(bd)
+    it_loose, rr_loose = engine.refine_solve(A_hi, LU, piv, bd, xl, tol=1e-6, maxit=20, dinv=dinv)
+    assert it_loose <= it and rr_loose <= 1e-6
+    assert rel_err(xd.cpu().numpy(), np.linalg.solve(A, b)) < 1e-10
