@@ -280,6 +280,29 @@ def profile_step(precision: str):
     core.kill()
 
 
+def profile_lu(n: int):
+    """Six tile-pivoted FP32 factorisations of one random complex n x n matrix
+    shifted by 40 I (seed 0), each timed with CUDA events (the command the LU
+    kernel summaries under profiles/ were captured with)."""
+    import torch
+    from bem_b200.engine import Engine
+    torch.manual_seed(0)
+    A = (torch.randn(n, n, dtype=torch.complex64, device="cuda") + 40 * torch.eye(n, device="cuda")).contiguous()
+    eng = Engine()
+    ts = []
+    for _ in range(6):
+        LU = A.clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.lu_factor_tiled(LU)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    print(json.dumps({"profile_lu": n, "factor_ms": ts}))
+    eng.close()
+
+
 def sweep_bench(n_k: int):
     """Config 3: the wavenumber sweep (managers/sweep.py) of the augmented
     transmission operator, mixed precision against the plain FP64 path; one
@@ -527,6 +550,8 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--profile-step", default=None, choices=["mixed", "fp64"],
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
+    ap.add_argument("--profile-lu", type=int, default=0,
+                    help="time six tiled FP32 factorisations of a random complex matrix of this size and exit")
     ap.add_argument("--workload", default="config2", choices=["config2", "sweep", "shape", "transmission", "disk2d"],
                     help="sweep: the config-3 wavenumber sweep, shape: the config-4 shape gradient, disk2d: the "
                          "2D operators (each its own JSON line)")
@@ -557,6 +582,9 @@ def main():
         return
     if args.profile_step:
         profile_step(args.profile_step)
+        return
+    if args.profile_lu:
+        profile_lu(args.profile_lu)
         return
 
     if args.impl == "reference":
