@@ -233,6 +233,22 @@ int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* L
                      const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit,
                      int* iters, double* relres, void* stream);
 
+/* GMRES-based refinement: restarted GMRES(restart) in FP64 on A_hi x = b,
+ * right-preconditioned by the low-precision factors of bem_refine_solve
+ * (tile-pivoted when dinv != NULL, else partial pivoting), Arnoldi with
+ * classical Gram-Schmidt applied twice.  For systems where plain refinement
+ * contracts too slowly (cond(A) times the FP32 unit roundoff near 1).  x
+ * (device, FP64) holds the initial guess and is overwritten.  Each restart
+ * begins from the true FP64 residual; once a restart cycle no longer halves
+ * it, a relative residual <= accept ends the iteration with BEM_OK.  Returns
+ * BEM_ERR_NOCONVERGE after maxit Arnoldi steps otherwise.  Synchronises the
+ * stream once per Arnoldi step.  The reference solves with
+ * torch.linalg.solve / lstsq (BEM_manager.py:1049-1056); this is the
+ * fallback the driver takes when refinement stagnates. */
+int bem_gmres_ir(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv,
+                 const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit, int restart,
+                 double accept, int* iters, double* relres, void* stream);
+
 /* ---- device probes ------------------------------------------------------------
  * No reference counterpart.  Measures the throughput of the pipes the assembly
  * kernels are bound by (they are neither HBM- nor tensor-core-bound):

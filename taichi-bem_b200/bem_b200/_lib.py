@@ -34,7 +34,7 @@ EXPORTS = [
     "bem_near_pair_count", "bem_mesh_geometry", "bem_assemble", "bem_apply", "bem_mass", "bem_lu_factor",
     "bem_lu_solve", "bem_gemv", "bem_refine_solve", "bem_measure_peaks", "bem_lu_dinv_elems",
     "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet", "bem_lu_solve_tiled_static",
-    "bem_adjoint_vertices", "bem_mesh_set_2d",
+    "bem_adjoint_vertices", "bem_mesh_set_2d", "bem_gmres_ir",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 
@@ -89,6 +89,8 @@ def load():
     L.bem_gemv.argtypes = [vp, i32, vp, i64, i64, i64, vp, vp, dbl, dbl, vp]
     L.bem_refine_solve.argtypes = [vp, i32, vp, vp, vp, vp, i64, i64, vp, vp, dbl, i32,
                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), vp]
+    L.bem_gmres_ir.argtypes = [vp, i32, vp, vp, vp, vp, i64, i64, vp, vp, dbl, i32, i32, dbl,
+                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), vp]
     L.bem_assemble_dirichlet.argtypes = [vp, ctypes.POINTER(OpDesc), ctypes.POINTER(Space), ctypes.POINTER(Space),
                                          vp, i64, dbl, ctypes.POINTER(Space), ctypes.POINTER(Space), vp, vp, dbl,
                                          i32, vp]

@@ -253,6 +253,21 @@ class Engine:
                                                 _ptr(dinv), _ptr(b), _stream_ptr()))
         return b
 
+    def gmres_solve(self, A_hi, LU_lo, piv, b, x, tol=1e-12, maxit=300, restart=60, dinv=None, accept=1e-8):
+        """Restarted GMRES in FP64 preconditioned by the low-precision factors
+        (bem_gmres_ir); x holds the initial guess.  Returns (iterations,
+        relative residual); raises BemError(BEM_ERR_NOCONVERGE) when neither
+        tol nor, after stagnation, `accept` is reached."""
+        it = ctypes.c_int(0)
+        rr = ctypes.c_double(0.0)
+        n = A_hi.shape[0]
+        assert b.is_contiguous() and x.is_contiguous() and b.dtype == A_hi.dtype == x.dtype
+        self._check(self.lib.bem_gmres_ir(self.ctx, _dtype_code(A_hi), _ptr(A_hi), _ptr(LU_lo), _ptr(piv),
+                                          _ptr(dinv), n, A_hi.stride(0), _ptr(b), _ptr(x), float(tol), int(maxit),
+                                          int(restart), float(accept), ctypes.byref(it), ctypes.byref(rr),
+                                          _stream_ptr()))
+        return it.value, rr.value
+
     def refine_solve(self, A_hi, LU_lo, piv, b, x, tol=1e-12, maxit=50, dinv=None, accept=None):
         """FP64 iterative refinement (bem_refine_solve); returns (iterations,
         relative residual).  When the residual stagnates above `tol` -- the
@@ -269,66 +284,6 @@ class Engine:
             return it.value, rr.value
         self._check(rc)
         return it.value, rr.value
-
-
-def gmres_ir(engine: Engine, A_hi: torch.Tensor, precond, b: torch.Tensor, x: torch.Tensor,
-             tol: float = 1e-12, maxit: int = 300, restart: int = 60, accept: float = 1e-8):
-    """GMRES-based iterative refinement: restarted GMRES in FP64 on
-    A_hi x = b, right-preconditioned by a low-precision LU (`precond(z)`
-    overwrites z with M^{-1} z: bem_lu_solve or bem_lu_solve_tiled), with
-    FP64 residuals and matrix-vector products (bem_gemv).  Converges where plain refinement contracts too slowly
-    (cond(A) u_fp32 near 1).  x is updated in place; returns (iterations,
-    relative residual).  When a restart cycle no longer halves the true FP64
-    residual (its floor is about eps * cond(A)), a residual <= `accept` is
-    returned; otherwise BemError(BEM_ERR_NOCONVERGE) is raised after maxit
-    iterations."""
-    n = A_hi.shape[0]
-    bnorm = float(torch.linalg.norm(b)) or 1.0
-    its = 0
-    rel = float("inf")
-    prev = float("inf")
-    while its < maxit:
-        r = b.clone()
-        engine.gemv(A_hi, x, r, alpha=-1.0, beta=1.0)
-        beta = float(torch.linalg.norm(r))
-        rel = beta / bnorm
-        if rel <= tol or (rel > 0.5 * prev and rel <= accept):
-            return its, rel
-        prev = rel
-        m = min(restart, maxit - its)
-        Vb = torch.zeros(n, m + 1, dtype=b.dtype, device=b.device)
-        Zb = torch.zeros(n, m, dtype=b.dtype, device=b.device)
-        H = torch.zeros(m + 1, m, dtype=b.dtype, device=b.device)
-        Vb[:, 0] = r / beta
-        e1 = torch.zeros(m + 1, dtype=b.dtype, device=b.device)
-        e1[0] = beta
-        y = None
-        for j in range(m):
-            z = Vb[:, j].clone()
-            precond(z)
-            Zb[:, j] = z
-            w = torch.zeros_like(z)
-            engine.gemv(A_hi, z, w)
-            for _ in range(2):  # classical Gram-Schmidt, twice
-                h = Vb[:, :j + 1].conj().transpose(0, 1) @ w
-                w = w - Vb[:, :j + 1] @ h
-                H[:j + 1, j] += h
-            hn = torch.linalg.norm(w)
-            H[j + 1, j] = hn
-            its += 1
-            if float(hn) > 0.0:
-                Vb[:, j + 1] = w / hn
-            y = torch.linalg.lstsq(H[:j + 2, :j + 1], e1[:j + 2, None]).solution[:, 0]
-            est = float(torch.linalg.norm(e1[:j + 2] - H[:j + 2, :j + 1] @ y)) / bnorm
-            if est <= 0.5 * tol or float(hn) == 0.0:
-                break
-        x += Zb[:, :y.numel()] @ y
-    r = b.clone()
-    engine.gemv(A_hi, x, r, alpha=-1.0, beta=1.0)
-    rel = float(torch.linalg.norm(r)) / bnorm
-    if rel <= max(tol, accept):
-        return its, rel
-    raise L.BemError(-4, f"GMRES-IR did not reach tol {tol:g} in {maxit} iterations (relres {rel:.3e})")
 
 
 def measure_peaks(engine: Engine):

@@ -31,7 +31,7 @@ from .. import _lib as L
 from ..BEM_functions.layers import (AdjDoubleLayer2d, AdjDoubleLayer3d, DoubleLayer2d, DoubleLayer3d,
                                     HypersingularLayer2d, HypersingularLayer3d, IdentityLayer2d, IdentityLayer3d,
                                     RHSConstructor2d, RHSConstructor3d, SingleLayer2d, SingleLayer3d)
-from ..engine import DeviceSpace, Engine, gmres_ir
+from ..engine import DeviceSpace, Engine
 from ..utils.types import AssembleType, CellFluxType, KernelType, ScopeType, VertAttachType
 
 
@@ -326,10 +326,9 @@ class BEMManager:
                     # plain refinement contracts too slowly (cond(A) u_fp32 near 1):
                     # GMRES in FP64 with the same factor as preconditioner
                     x.zero_()
-                    LUp, pp = state["LU"], state["piv"]
-                    it, rr = gmres_ir(self.engine, A, lambda z: self.engine.lu_solve(LUp, pp, z), c, x,
-                                      tol=self.refine_tol, maxit=max(self.refine_maxit, 300),
-                                      accept=self.refine_accept)
+                    it, rr = self.engine.gmres_solve(A, state["LU"], state["piv"], c, x, tol=self.refine_tol,
+                                                     maxit=max(self.refine_maxit, 300), restart=60,
+                                                     accept=self.refine_accept)
                     kind = "fp32 partial pivoting + GMRES-IR"
             xs.append(x)
             its.append(it)

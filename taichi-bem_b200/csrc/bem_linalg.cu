@@ -16,6 +16,9 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <complex>
+#include <vector>
+
 #include <cmath>
 #include <vector>
 
@@ -888,6 +891,248 @@ int refine_async(bem_ctx* ctx, bool C, const void* A_hi, const void* LU_lo, cons
     return BEM_OK;
 }
 
+// ---- GMRES: block inner products and updates on FP64 vectors ------------
+// out[i] = sum_q conj(V_i[q]) w[q] for the k vectors V_i (stride nd doubles);
+// grid (chunks, k), partial sums of a chunk added atomically
+template <bool C>
+__global__ void gm_dot_kernel(const double* V, int64_t nd, int k, const double* w, double* out) {
+    __shared__ double s_re[8], s_im[8];
+    const int i = blockIdx.y;
+    const double* v = V + (int64_t)i * nd;
+    const int W = C ? 2 : 1;
+    const int64_t n = nd / W;
+    double re = 0.0, im = 0.0;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        if (C) {
+            const double vr = v[2 * q], vi = v[2 * q + 1], wr = w[2 * q], wi = w[2 * q + 1];
+            re += vr * wr + vi * wi;
+            im += vr * wi - vi * wr;
+        } else {
+            re += v[q] * w[q];
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_re[threadIdx.x >> 5] = re;
+        s_im[threadIdx.x >> 5] = im;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tr = 0.0, ti = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+            tr += s_re[q];
+            ti += s_im[q];
+        }
+        atomicAdd(out + 2 * i, tr);
+        if (C) atomicAdd(out + 2 * i + 1, ti);
+    }
+}
+
+// w[q] -= sum_i V_i[q] h_i (h: k complex values, interleaved; real part only
+// when !C)
+template <bool C>
+__global__ void gm_update_kernel(double* w, const double* V, int64_t nd, int k, const double* h) {
+    const int W = C ? 2 : 1;
+    const int64_t n = nd / W;
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    double ar = 0.0, ai = 0.0;
+    for (int i = 0; i < k; ++i) {
+        const double* v = V + (int64_t)i * nd;
+        const double hr = h[2 * i], hi = h[2 * i + 1];
+        if (C) {
+            const double vr = v[2 * q], vi = v[2 * q + 1];
+            ar += vr * hr - vi * hi;
+            ai += vr * hi + vi * hr;
+        } else {
+            ar += v[q] * hr;
+        }
+    }
+    if (C) {
+        w[2 * q] -= ar;
+        w[2 * q + 1] -= ai;
+    } else {
+        w[q] -= ar;
+    }
+}
+
+__global__ void gm_scale_kernel(double* dst, const double* src, int64_t nd, double a) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < nd) dst[i] = a * src[i];
+}
+
+// Restarted GMRES(m) in FP64 on A_hi x = b, right-preconditioned by the
+// low-precision factors (tile-pivoted when dinv != NULL, else partial
+// pivoting).  Arnoldi with classical Gram-Schmidt applied twice, Givens
+// rotations of the Hessenberg matrix on the host.  Each restart starts from
+// the true FP64 residual; a restart cycle that no longer halves it ends the
+// iteration once the residual is <= accept (its floor is about
+// eps * cond(A)).
+int gmres_run(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv, const void* dinv,
+              int64_t n, int64_t lda, const double* b, double* x, double tol, int maxit, int restart, double accept,
+              int* iters, double* relres, cudaStream_t s) {
+    const bool C = dtype_hi == BEM_C128;
+    const int W = C ? 2 : 1;
+    const int64_t nd = W * n;
+    const int m = std::max(1, std::min(restart, 200));
+    const int lo_dtype = C ? BEM_C64 : BEM_F32;
+    // V (m+1 vectors), Z (m vectors), w, r, dots (2 (m+1) doubles)
+    const size_t doubles = (size_t)(2 * m + 3) * nd + 2 * (m + 2);
+    double* buf = nullptr;
+    if (int rc = bem_check_cuda(ctx, cudaMallocAsync((void**)&buf, sizeof(double) * doubles, s), "gmres alloc"))
+        return rc;
+    double* V = buf;
+    double* Z = V + (size_t)(m + 1) * nd;
+    double* w = Z + (size_t)m * nd;
+    double* r = w + nd;
+    double* dots = r + nd;
+    const unsigned vblocks = (unsigned)((n + 255) / 256);
+    const unsigned sblocks = (unsigned)std::min<int64_t>(ctx->num_sms * 4, (nd + 255) / 256);
+    const unsigned dchunks = (unsigned)std::min<int64_t>(ctx->num_sms, (n + 255) / 256);
+    int rc = BEM_OK;
+    auto norm = [&](const double* v, double* out) -> int {
+        cudaMemsetAsync(dots, 0, sizeof(double), s);
+        sumsq_kernel<<<sblocks, 256, 0, s>>>(v, nd, dots);
+        ctx->launches++;
+        double h = 0.0;
+        if (int e = bem_check_cuda(ctx, cudaMemcpyAsync(&h, dots, sizeof(double), cudaMemcpyDeviceToHost, s),
+                                   "gmres norm"))
+            return e;
+        if (int e = bem_check_cuda(ctx, cudaStreamSynchronize(s), "gmres norm")) return e;
+        *out = std::sqrt(h);
+        return BEM_OK;
+    };
+    auto residual = [&](double* out_norm) -> int {
+        if (int e = bem_check_cuda(ctx, cudaMemcpyAsync(r, b, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s),
+                                   "r=b"))
+            return e;
+        if (int e = bem_gemv(ctx, dtype_hi, A_hi, n, n, lda, x, r, -1.0, 1.0, s)) return e;
+        return norm(r, out_norm);
+    };
+    auto precond = [&](double* z) -> int {
+        return dinv ? bem_lu_solve_tiled(ctx, lo_dtype, LU_lo, n, lda, piv, dinv, z, s)
+                    : bem_lu_solve(ctx, lo_dtype, LU_lo, n, lda, piv, z, 1, 1, s);
+    };
+    using cplx = std::complex<double>;
+    double bnorm = 0.0;
+    rc = norm(b, &bnorm);
+    if (bnorm == 0.0) bnorm = 1.0;
+    int its = 0;
+    double rel = 0.0, prev = INFINITY;
+    bool done = false;
+    std::vector<cplx> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), y(m);
+    std::vector<double> hbuf(2 * (m + 1));
+    while (rc == BEM_OK && its < maxit) {
+        double beta = 0.0;
+        if ((rc = residual(&beta))) break;
+        rel = beta / bnorm;
+        if (rel <= tol || (rel > 0.5 * prev && rel <= accept)) {
+            done = true;
+            break;
+        }
+        prev = rel;
+        const int mm = std::min(m, maxit - its);
+        gm_scale_kernel<<<(unsigned)((nd + 255) / 256), 256, 0, s>>>(V, r, nd, 1.0 / beta);
+        ctx->launches++;
+        std::fill(H.begin(), H.end(), cplx(0.0));
+        std::fill(g.begin(), g.end(), cplx(0.0));
+        g[0] = beta;
+        int jd = 0;
+        for (int j = 0; j < mm && rc == BEM_OK; ++j) {
+            double* Vj = V + (size_t)j * nd;
+            double* Zj = Z + (size_t)j * nd;
+            if ((rc = bem_check_cuda(ctx, cudaMemcpyAsync(Zj, Vj, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s),
+                                     "z=v")))
+                break;
+            if ((rc = precond(Zj))) break;
+            if ((rc = bem_gemv(ctx, dtype_hi, A_hi, n, n, lda, Zj, w, 1.0, 0.0, s))) break;
+            for (int pass = 0; pass < 2 && rc == BEM_OK; ++pass) {
+                cudaMemsetAsync(dots, 0, sizeof(double) * 2 * (j + 1), s);
+                if (C)
+                    gm_dot_kernel<true><<<dim3(dchunks, j + 1), 256, 0, s>>>(V, nd, j + 1, w, dots);
+                else
+                    gm_dot_kernel<false><<<dim3(dchunks, j + 1), 256, 0, s>>>(V, nd, j + 1, w, dots);
+                if (C)
+                    gm_update_kernel<true><<<vblocks, 256, 0, s>>>(w, V, nd, j + 1, dots);
+                else
+                    gm_update_kernel<false><<<vblocks, 256, 0, s>>>(w, V, nd, j + 1, dots);
+                ctx->launches += 2;
+                if ((rc = bem_check_cuda(ctx, cudaMemcpyAsync(hbuf.data(), dots, sizeof(double) * 2 * (j + 1),
+                                                              cudaMemcpyDeviceToHost, s), "gmres dots")))
+                    break;
+                if ((rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "gmres dots"))) break;
+                for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] += cplx(hbuf[2 * i], C ? hbuf[2 * i + 1] : 0.0);
+            }
+            if (rc) break;
+            double hn = 0.0;
+            if ((rc = norm(w, &hn))) break;
+            ++its;
+            jd = j + 1;
+            if (hn > 0.0) {
+                gm_scale_kernel<<<(unsigned)((nd + 255) / 256), 256, 0, s>>>(V + (size_t)(j + 1) * nd, w, nd,
+                                                                              1.0 / hn);
+                ctx->launches++;
+            }
+            // Givens rotations: the earlier ones on column j, a new one for H[j+1][j]
+            for (int i = 0; i < j; ++i) {
+                const cplx a = H[(size_t)i * m + j], c2 = H[(size_t)(i + 1) * m + j];
+                H[(size_t)i * m + j] = std::conj(cs[i]) * a + std::conj(sn[i]) * c2;
+                H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * c2;
+            }
+            const cplx a = H[(size_t)j * m + j];
+            const double den = std::sqrt(std::norm(a) + hn * hn);
+            if (den > 0.0) {
+                cs[j] = a / den;
+                sn[j] = cplx(hn / den, 0.0);
+            } else {
+                cs[j] = 1.0;
+                sn[j] = 0.0;
+            }
+            H[(size_t)j * m + j] = std::conj(cs[j]) * a + std::conj(sn[j]) * hn;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = std::conj(cs[j]) * g[j];
+            const double est = std::abs(g[j + 1]) / bnorm;
+            if (est <= 0.5 * tol || hn == 0.0) break;
+        }
+        if (rc) break;
+        // y = R^{-1} g, x += Z y
+        for (int i = jd - 1; i >= 0; --i) {
+            cplx t = g[i];
+            for (int q = i + 1; q < jd; ++q) t -= H[(size_t)i * m + q] * y[q];
+            const cplx d = H[(size_t)i * m + i];
+            y[i] = std::abs(d) > 0.0 ? t / d : cplx(0.0);
+        }
+        for (int i = 0; i < jd; ++i) {
+            hbuf[2 * i] = -y[i].real();
+            hbuf[2 * i + 1] = -y[i].imag();
+        }
+        if ((rc = bem_check_cuda(ctx, cudaMemcpyAsync(dots, hbuf.data(), sizeof(double) * 2 * jd,
+                                                      cudaMemcpyHostToDevice, s), "gmres y")))
+            break;
+        if (C)
+            gm_update_kernel<true><<<vblocks, 256, 0, s>>>(x, Z, nd, jd, dots);
+        else
+            gm_update_kernel<false><<<vblocks, 256, 0, s>>>(x, Z, nd, jd, dots);
+        ctx->launches++;
+        if ((rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "gmres update"))) break;
+    }
+    if (rc == BEM_OK && !done) {
+        double rn = 0.0;
+        rc = residual(&rn);
+        rel = rn / bnorm;
+    }
+    cudaFreeAsync(buf, s);
+    if (rc) return rc;
+    if (iters) *iters = its;
+    if (relres) *relres = rel;
+    if (!done && rel > std::max(tol, accept))
+        return bem_fail(ctx, BEM_ERR_NOCONVERGE, "GMRES-IR did not reach tol in maxit iterations");
+    return BEM_OK;
+}
+
 template <typename T, bool C>
 int gemv_t(bem_ctx* ctx, const T* A, int64_t m, int64_t n, int64_t lda, const double* x, double* y, double alpha,
            double beta, cudaStream_t s) {
@@ -1020,6 +1265,18 @@ int bem_refine_solve(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* L
     if (rc == BEM_OK && rnorm > tol * bnorm)
         return bem_fail(ctx, BEM_ERR_NOCONVERGE, "refinement did not reach tol in maxit iterations");
     return rc;
+}
+
+int bem_gmres_ir(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv,
+                 const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit, int restart,
+                 double accept, int* iters, double* relres, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A_hi || !LU_lo || !piv || !b || !x || n <= 0 || lda < n || maxit < 1 || restart < 1 || !(tol > 0))
+        return bem_fail(ctx, BEM_ERR_INVALID, "gmres_ir: bad arguments");
+    if (dtype_hi != BEM_F64 && dtype_hi != BEM_C128)
+        return bem_fail(ctx, BEM_ERR_INVALID, "gmres_ir: A_hi must be F64 or C128");
+    return gmres_run(ctx, dtype_hi, A_hi, LU_lo, piv, dinv, n, lda, (const double*)b, (double*)x, tol, maxit,
+                     restart, accept, iters, relres, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -152,3 +152,46 @@ def test_async_refinement_stopping_rules(engine, cplx):
     it_loose, rr_loose = engine.refine_solve(A_hi, LU, piv, bd, xl, tol=1e-6, maxit=20, dinv=dinv)
     assert it_loose <= it and rr_loose <= 1e-6
     assert rel_err(xd.cpu().numpy(), np.linalg.solve(A, b)) < 1e-10
+
+
+def _illcond(n, cplx, cond, seed):
+    """Q diag(s) Q^H with singular values log-spaced from 1 to 1/cond."""
+    rng = np.random.default_rng(seed)
+    Z = rng.standard_normal((n, n)) + (1j * rng.standard_normal((n, n)) if cplx else 0)
+    Q, _ = np.linalg.qr(Z)
+    s = np.logspace(0, -np.log10(cond), n)
+    return (Q * s) @ Q.conj().T
+
+
+@pytest.mark.parametrize("tiled", [False, True])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_gmres_ir(engine, cplx, tiled):
+    """bem_gmres_ir on a system with cond(A) = 1e6, where the FP32 factor's
+    refinement contracts slowly (cond * u_fp32 ~ 0.06): the solution against
+    numpy's FP64 solve, b = 0, and the iteration cap."""
+    from bem_b200._lib import BemError
+    n = 256
+    A = _illcond(n, cplx, 1e6, 31)
+    rng = np.random.default_rng(6)
+    b = rng.standard_normal(n) + (1j * rng.standard_normal(n) if cplx else 0)
+    A_hi = torch.as_tensor(A, device="cuda").contiguous()
+    LU = A_hi.to(torch.complex64 if cplx else torch.float32).contiguous()
+    if tiled:
+        piv, dinv, _ = engine.lu_factor_tiled(LU)
+    else:
+        piv, _ = engine.lu_factor(LU)
+        dinv = None
+    bd = torch.as_tensor(b, device="cuda").contiguous()
+    xd = torch.zeros_like(bd)
+    # the FP64 residual of this system bottoms out near eps * cond(A) = 1e-10
+    it, rr = engine.gmres_solve(A_hi, LU, piv, bd, xd, tol=1e-10, maxit=200, restart=30, dinv=dinv)
+    assert rr <= 1e-10 and it >= 1
+    assert rel_err(xd.cpu().numpy(), np.linalg.solve(A, b)) < 1e-7
+    zero = torch.zeros_like(bd)
+    x0 = torch.zeros_like(bd)
+    it0, rr0 = engine.gmres_solve(A_hi, LU, piv, zero, x0, tol=1e-12, maxit=10, restart=5, dinv=dinv)
+    assert it0 == 0 and rr0 == 0.0 and float(x0.abs().max()) == 0.0
+    with pytest.raises(BemError) as exc:
+        engine.gmres_solve(A_hi, LU, piv, bd, torch.zeros_like(bd), tol=1e-15, maxit=1, restart=1, dinv=dinv,
+                           accept=0.0)
+    assert exc.value.code == -4
