@@ -380,113 +380,140 @@ __global__ void tile_laswp_kernel(T* A, int64_t lda, int n, int k0, int m, const
 // blockIdx.y = 0: U12 tile (rows k0.., 64 columns) <- L11^{-1} tile (unit lower)
 // blockIdx.y = 1: L21 tile (64 rows, columns k0..) <- tile U11^{-1} (upper)
 // Both run in one launch (they touch disjoint parts of A).  The factored
-// diagonal block is staged in shared memory and the tile is held in
-// registers: thread (tx, ty) owns rows ty + 16 i, columns tx + 16 j.  Step q
-// publishes the finished row q (mode 0) or column q, scaled by 1/U_qq
-// (mode 1), through a double-buffered shared vector and updates the entries
-// below / right of it: one CTA barrier per step.
+// diagonal block and the tile are staged in shared memory and the
+// substitution is blocked by APPLY_B rows (mode 0) or columns (mode 1): the
+// block's own triangle is solved by one thread per column (row), sequentially
+// over the APPLY_B entries, then every thread applies the block's rank-APPLY_B
+// update to its entries below (right of) it -- two CTA barriers per block.
 constexpr int APPLY_LD = LU_T + 1;
-constexpr size_t apply_smem_bytes(size_t elem) { return elem * LU_T * APPLY_LD; }
+constexpr int APPLY_B = 8;
+constexpr size_t apply_smem_bytes(size_t elem) { return 2 * elem * LU_T * APPLY_LD; }
 
 template <typename T, bool C>
 __global__ void __launch_bounds__(256) tile_apply_kernel(T* A, int64_t lda, int n, int k0, int m) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CE<T>* M = reinterpret_cast<CE<T>*>(smem_raw);  // [LU_T][APPLY_LD] factored diagonal block
-    __shared__ CE<T> s_vec[2][LU_T];
+    CE<T>* X = M + LU_T * APPLY_LD;                 // [LU_T][APPLY_LD] the tile
     __shared__ CE<T> s_rdiag[LU_T];
     const int mode = blockIdx.y;
     const int base = k0 + m + blockIdx.x * LU_T;  // first column (mode 0) / row (mode 1) of the tile
     const int cnt = min(LU_T, n - base);
     for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
         const int r = e / LU_T, c = e - r * LU_T;
-        CE<T> v = CE<T>{T(0), T(0)};
-        if (r < m && c < m) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c);
-        M[r * APPLY_LD + c] = v;
-    }
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    CE<T> x[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int r = ty + 16 * i, c = tx + 16 * j;
-            CE<T> v = CE<T>{T(0), T(0)};
-            if (mode == 0) {
-                if (r < m && c < cnt) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + base + c);
-            } else {
-                if (r < cnt && c < m) v = ldE<T, C>(A, (int64_t)(base + r) * lda + k0 + c);
-            }
-            x[i][j] = v;
+        CE<T> d = CE<T>{T(0), T(0)}, v = CE<T>{T(0), T(0)};
+        if (r < m && c < m) d = ldE<T, C>(A, (int64_t)(k0 + r) * lda + k0 + c);
+        if (mode == 0) {
+            if (r < m && c < cnt) v = ldE<T, C>(A, (int64_t)(k0 + r) * lda + base + c);
+        } else {
+            if (r < cnt && c < m) v = ldE<T, C>(A, (int64_t)(base + r) * lda + k0 + c);
         }
+        M[r * APPLY_LD + c] = d;
+        X[r * APPLY_LD + c] = v;
+    }
     __syncthreads();
     if (mode == 1 && threadIdx.x < LU_T)
         s_rdiag[threadIdx.x] = threadIdx.x < m ? cinv(M[threadIdx.x * APPLY_LD + threadIdx.x]) : CE<T>{T(0), T(0)};
     __syncthreads();
-    for (int q = 0; q < m; ++q) {
-        CE<T>* v = s_vec[q & 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int t = threadIdx.x;
+    for (int b0 = 0; b0 < m; b0 += APPLY_B) {
+        const int bw = min(APPLY_B, m - b0);
         if (mode == 0) {
-            // row q is final: its owners publish it, then rows r > q take L_rq x_q
-            if (ty == (q & 15)) {
+            // rows b0..b0+bw-1: X_b <- L_bb^{-1} X_b, one thread per column
+            if (t < LU_T) {
+                CE<T> y[APPLY_B];
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (ty + 16 * i == q) {
+                for (int i = 0; i < APPLY_B; ++i) {
+                    if (i >= bw) break;
+                    CE<T> v = X[(b0 + i) * APPLY_LD + t];
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) v[tx + 16 * j] = x[i][j];
+                    for (int q = 0; q < i; ++q) {
+                        const CE<T> l = M[(b0 + i) * APPLY_LD + b0 + q];
+                        v.re -= l.re * y[q].re - (C ? l.im * y[q].im : T(0));
+                        if (C) v.im -= l.re * y[q].im + l.im * y[q].re;
                     }
+                    y[i] = v;
+                    X[(b0 + i) * APPLY_LD + t] = v;
+                }
             }
             __syncthreads();
+            // rows below the block: X_r -= L_rb X_b
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int r = ty + 16 * i;
-                if (r <= q) continue;
-                const CE<T> l = M[r * APPLY_LD + q];
+                if (r < b0 + bw) continue;
+                CE<T> l[APPLY_B];
+#pragma unroll
+                for (int q = 0; q < APPLY_B; ++q)
+                    l[q] = q < bw ? M[r * APPLY_LD + b0 + q] : CE<T>{T(0), T(0)};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const CE<T> u = v[tx + 16 * j];
-                    x[i][j].re -= l.re * u.re - (C ? l.im * u.im : T(0));
-                    if (C) x[i][j].im -= l.re * u.im + l.im * u.re;
+                    const int c = tx + 16 * j;
+                    CE<T> v = X[r * APPLY_LD + c];
+#pragma unroll
+                    for (int q = 0; q < APPLY_B; ++q) {
+                        if (q >= bw) break;
+                        const CE<T> u = X[(b0 + q) * APPLY_LD + c];
+                        v.re -= l[q].re * u.re - (C ? l[q].im * u.im : T(0));
+                        if (C) v.im -= l[q].re * u.im + l[q].im * u.re;
+                    }
+                    X[r * APPLY_LD + c] = v;
                 }
             }
+            __syncthreads();
         } else {
-            // column q: scaled by 1/U_qq by its owners and published, then
-            // columns c > q take x_q U_qc
-            if (tx == (q & 15)) {
+            // columns b0..b0+bw-1: X_b <- X_b U_bb^{-1}, one thread per row
+            if (t < LU_T) {
+                CE<T> y[APPLY_B];
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (tx + 16 * j == q) {
+                for (int j = 0; j < APPLY_B; ++j) {
+                    if (j >= bw) break;
+                    CE<T> v = X[t * APPLY_LD + b0 + j];
 #pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            x[i][j] = cmul(x[i][j], s_rdiag[q]);
-                            v[ty + 16 * i] = x[i][j];
-                        }
+                    for (int q = 0; q < j; ++q) {
+                        const CE<T> u = M[(b0 + q) * APPLY_LD + b0 + j];
+                        v.re -= y[q].re * u.re - (C ? y[q].im * u.im : T(0));
+                        if (C) v.im -= y[q].re * u.im + y[q].im * u.re;
                     }
+                    y[j] = cmul(v, s_rdiag[b0 + j]);
+                    X[t * APPLY_LD + b0 + j] = y[j];
+                }
             }
             __syncthreads();
+            // columns right of the block: X_c -= X_b U_bc
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int c = tx + 16 * j;
-                if (c <= q) continue;
-                const CE<T> u = M[q * APPLY_LD + c];
+                if (c < b0 + bw) continue;
+                CE<T> u[APPLY_B];
+#pragma unroll
+                for (int q = 0; q < APPLY_B; ++q)
+                    u[q] = q < bw ? M[(b0 + q) * APPLY_LD + c] : CE<T>{T(0), T(0)};
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    const CE<T> l = v[ty + 16 * i];
-                    x[i][j].re -= l.re * u.re - (C ? l.im * u.im : T(0));
-                    if (C) x[i][j].im -= l.re * u.im + l.im * u.re;
+                    const int r = ty + 16 * i;
+                    CE<T> v = X[r * APPLY_LD + c];
+#pragma unroll
+                    for (int q = 0; q < APPLY_B; ++q) {
+                        if (q >= bw) break;
+                        const CE<T> l = X[r * APPLY_LD + b0 + q];
+                        v.re -= l.re * u[q].re - (C ? l.im * u[q].im : T(0));
+                        if (C) v.im -= l.re * u[q].im + l.im * u[q].re;
+                    }
+                    X[r * APPLY_LD + c] = v;
                 }
             }
+            __syncthreads();
         }
     }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int r = ty + 16 * i, c = tx + 16 * j;
-            if (mode == 0) {
-                if (r < m && c < cnt) stE<T, C>(A, (int64_t)(k0 + r) * lda + base + c, x[i][j]);
-            } else {
-                if (r < cnt && c < m) stE<T, C>(A, (int64_t)(base + r) * lda + k0 + c, x[i][j]);
-            }
+    for (int e = threadIdx.x; e < LU_T * LU_T; e += blockDim.x) {
+        const int r = e / LU_T, c = e - r * LU_T;
+        if (mode == 0) {
+            if (r < m && c < cnt) stE<T, C>(A, (int64_t)(k0 + r) * lda + base + c, X[r * APPLY_LD + c]);
+        } else {
+            if (r < cnt && c < m) stE<T, C>(A, (int64_t)(base + r) * lda + k0 + c, X[r * APPLY_LD + c]);
         }
+    }
 }
 
 // --------------------------------------------------------------------------
