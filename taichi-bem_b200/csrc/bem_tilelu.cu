@@ -6,8 +6,8 @@
 //            restricted to the block's rows;
 //   laswp  : the block's row swaps applied to the other columns;
 //   U12 = L11^{-1} A12 and L21 = A21 U11^{-1}: one CTA per 64-wide tile,
-//            substitution against the factored diagonal block, the tile held
-//            in registers (one CTA barrier per step);
+//            substitution against the factored diagonal block, blocked by 8
+//            rows (columns), in shared memory (two CTA barriers per block);
 //   update : A22 -= L21 U12 (the trailing GEMM of bem_gemm.cuh).
 // After the last block, one launch forms the explicit inverses Linv_k (unit
 // lower) and Uinv_k (upper) of every diagonal block (`dinv`, used by the
