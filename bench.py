@@ -74,6 +74,9 @@ try:
     pynvml.nvmlInit()
     h = pynvml.nvmlDeviceGetHandleByPciBusId(sys.argv[1].encode())
     smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+    # the first query of each counter is the slow one: make it before the timed region
+    pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+    pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
 except Exception as exc:
     print("fail", exc, flush=True)
     sys.exit(0)

@@ -25,6 +25,7 @@
 // the main loop, so that the latency of that read overlaps the MMAs instead
 // of following them (two CTAs per SM instead of three, about 10 % less time
 // per update).
+#include <algorithm>
 #include <cstdlib>
 
 #include "bem_gemm.cuh"
@@ -98,7 +99,8 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
 
 __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__ Cm, const float* __restrict__ Am,
                                                              const float* __restrict__ Bm, int m, int n_real,
-                                                             int k_real, int64_t ldf, int cplx, int32_t* err) {
+                                                             int k_real, int64_t ldf, int cplx, int chunks_per,
+                                                             int32_t* err) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar[TC_STAGES];
     __shared__ uint32_t tmem_slot;
@@ -129,8 +131,14 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
     // the C tile of this thread's epilogue: TMEM lane row e_row, 64 columns from e_cbase
     const int e_row = 32 * (warp & 3) + lane;
     const int e_cbase = 64 * (warp >> 2);
+    // split K (gridDim.z > 1): this CTA takes chunks [c_begin, c_end) and adds
+    // its partial product to C atomically, so it reads no C tile ahead
+    const bool split = gridDim.z > 1;
+    const int nchunks_all = (k_real + TC_KC - 1) / TC_KC;
+    const int c_begin = blockIdx.z * chunks_per;
+    const int c_end = min(nchunks_all, c_begin + chunks_per);
     float cpre[64];
-    {
+    if (!split) {
         const int gr = m0 + e_row;
         const float* crow = Cm + (int64_t)(gr < m ? gr : 0) * ldf;
 #pragma unroll
@@ -151,7 +159,7 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
             }
         }
     }
-    const int nchunks = (k_real + TC_KC - 1) / TC_KC;
+    const int nchunks = c_end - c_begin;  // local chunk lc is global chunk c_begin + lc
     // Software pipeline: the global loads of chunk c+1 are issued into
     // registers right after chunk c is stored, so their latency overlaps the
     // MMAs of chunk c and the wait for the stage to be free again.
@@ -203,7 +211,7 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
             }
         }
     };
-    if (nchunks > 0) load_chunk(0);
+    if (nchunks > 0) load_chunk(c_begin);
     for (int c = 0; c < nchunks; ++c) {
         const int stage = c & 1;
         unsigned char* st = smem + stage * TC_STAGE_BYTES;
@@ -246,7 +254,7 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
             *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + 16 * u) = hi;
             *reinterpret_cast<float4*>(st + 3 * TC_TILE_BYTES + 16 * u) = lo;
         }
-        if (c + 1 < nchunks) load_chunk(c + 1);
+        if (c + 1 < nchunks) load_chunk(c_begin + c + 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -275,7 +283,7 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!s_abort) {
+    if (!s_abort && nchunks > 0) {
         // epilogue: warp w reads TMEM lanes 32*(w%4).. (rows), columns half (w/4)
         const int row = 32 * (warp & 3) + lane;
         const int cbase = 64 * (warp >> 2);
@@ -293,7 +301,16 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
                 : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             const int gr = m0 + row;
-            if (gr < m) {
+            if (gr < m && split) {
+                // partial product of this CTA's K range, added atomically
+                float* crow = Cm + (int64_t)gr * ldf;
+                const int gc0 = n0 + cbase + cc;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int gc = gc0 + i;
+                    if (gc < n_real) atomicAdd(crow + gc, -__uint_as_float(v[i]));
+                }
+            } else if (gr < m) {
                 float* crow = Cm + (int64_t)gr * ldf;
                 const int gc0 = n0 + cbase + cc;
                 if (gc0 + 16 <= n_real && ((reinterpret_cast<uintptr_t>(crow + gc0) & 15) == 0)) {
@@ -349,7 +366,17 @@ int bem_gemm_tc_update(bem_ctx* ctx, float* C, const float* A, const float* B, i
     const size_t smem = (size_t)TC_STAGES * TC_STAGE_BYTES;
     cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)((n_real + TC_BN - 1) / TC_BN), (unsigned)((m + TC_BM - 1) / TC_BM));
-    gemm_tc_kernel<<<grid, TC_THREADS, smem, s>>>(C, A, B, (int)m, (int)n_real, (int)k_real, ldf, cplx ? 1 : 0,
+    // Skinny updates (the LU's tile-column and tile-row strips) fill few
+    // CTAs: split K over up to four CTAs per C tile, each adding its partial
+    // product atomically, until the grid covers the SMs.
+    const int nchunks = (int)((k_real + TC_KC - 1) / TC_KC);
+    const int64_t tiles = (int64_t)grid.x * grid.y;
+    int splits = 1;
+    if (tiles < ctx->num_sms && nchunks >= 4)
+        splits = (int)std::min<int64_t>(std::min<int64_t>(4, nchunks / 2), std::max<int64_t>(1, ctx->num_sms / tiles));
+    const int per = (nchunks + splits - 1) / splits;
+    grid.z = (unsigned)((nchunks + per - 1) / per);
+    gemm_tc_kernel<<<grid, TC_THREADS, smem, s>>>(C, A, B, (int)m, (int)n_real, (int)k_real, ldf, cplx ? 1 : 0, per,
                                                   ctx->flags + 4);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gemm_tc_kernel");
