@@ -25,6 +25,11 @@
 // the main loop, so that the latency of that read overlaps the MMAs instead
 // of following them (two CTAs per SM instead of three, about 10 % less time
 // per update).
+//
+// Updates with fewer C tiles than SMs (the LU's next tile column and tile-row
+// strip) split K over up to four CTAs per tile (gridDim.z); each adds its
+// partial product to C with FP32 atomics instead of the read-ahead
+// read-modify-write.
 #include <algorithm>
 #include <cstdlib>
 
