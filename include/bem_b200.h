@@ -255,6 +255,26 @@ int bem_gmres_ir(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo
                  const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit, int restart,
                  double accept, int* iters, double* relres, void* stream);
 
+/* ---- post-processing (headless) ------------------------------------------------
+ * The two kernels the reference runs at the end of BEMManager.run for its
+ * GGUI window (BEM_manager.py:1028-1029), writing plain device buffers; there
+ * is no window.  Both queue one launch without synchronising.
+ *
+ * BEMManager.compute_color (BEM_manager.py:527-587).  solved, exact [nv*n]
+ * doubles per vertex (n = 1 real, 2 complex interleaved); vert_types [nv]
+ * int32 (VertAttachType); show = BEMManager._show (-1 default, 0 Neumann,
+ * 1 Dirichlet).  solved is shifted IN PLACE at the Dirichlet-to-be-solved
+ * vertices (every vertex when show = 1) by mean(exact) - mean(solved) over
+ * those vertices, as the reference does.  Writes the colours [nv*3] float
+ * (r, g, b) of the solved, exact and difference values. */
+int bem_compute_color(bem_ctx* ctx, int n, double* solved, const double* exact, const int32_t* vert_types, int show,
+                      float* solved_color, float* exact_color, float* diff_color, void* stream);
+/* BEMManager.set_mesh_instances (BEM_manager.py:589-606): the mesh's vertices
+ * as [nv*3] float (z = 0 on a 2D mesh) into solved_vertices, moved by -2.2
+ * along x into exact_vertices and by +2.2 into diff_vertices. */
+int bem_set_mesh_instances(bem_ctx* ctx, float* solved_vertices, float* exact_vertices, float* diff_vertices,
+                           void* stream);
+
 /* ---- device probes ------------------------------------------------------------
  * No reference counterpart.  Measures the throughput of the pipes the assembly
  * kernels are bound by (they are neither HBM- nor tensor-core-bound):

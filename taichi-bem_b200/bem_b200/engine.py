@@ -208,6 +208,35 @@ class Engine:
                                           out.stride(0), float(scale), _ptr(out_t), float(scale_t), None, None, 0,
                                           _stream_ptr()))
 
+    # -- post-processing ---------------------------------------------------------------
+    def _vertex_buffers(self, *bufs):
+        for b in bufs:
+            if not (b.is_cuda and b.dtype == torch.float32 and b.is_contiguous() and b.shape == (self.nv, 3)):
+                raise ValueError("colour/position buffers must be contiguous float32 [nv, 3] on the device")
+
+    def compute_color(self, solved, exact, vert_types, show, solved_color, exact_color, diff_color):
+        """BEMManager.compute_color (BEM_manager.py:527-587): shifts `solved`
+        in place and writes the three colour buffers [nv, 3] float32."""
+        for t in (solved, exact):
+            if not (t.is_cuda and t.is_contiguous() and t.dtype in (torch.float64, torch.complex128)
+                    and t.numel() == self.nv):
+                raise ValueError("solved/exact must be contiguous float64 or complex128 [nv] on the device")
+        if solved.dtype != exact.dtype:
+            raise ValueError("solved and exact must have the same dtype")
+        if not (vert_types.is_cuda and vert_types.dtype == torch.int32 and vert_types.numel() == self.nv):
+            raise ValueError("vert_types must be int32 [nv] on the device")
+        self._vertex_buffers(solved_color, exact_color, diff_color)
+        n = 2 if solved.is_complex() else 1
+        self._check(self.lib.bem_compute_color(self.ctx, n, _ptr(solved), _ptr(exact), _ptr(vert_types), int(show),
+                                               _ptr(solved_color), _ptr(exact_color), _ptr(diff_color),
+                                               _stream_ptr()))
+
+    def set_mesh_instances(self, solved_vertices, exact_vertices, diff_vertices):
+        """BEMManager.set_mesh_instances (BEM_manager.py:589-606)."""
+        self._vertex_buffers(solved_vertices, exact_vertices, diff_vertices)
+        self._check(self.lib.bem_set_mesh_instances(self.ctx, _ptr(solved_vertices), _ptr(exact_vertices),
+                                                    _ptr(diff_vertices), _stream_ptr()))
+
     # -- dense solve ---------------------------------------------------------------
     def lu_factor(self, A: torch.Tensor):
         """In-place LU with partial pivoting; returns (piv, info) device int32."""

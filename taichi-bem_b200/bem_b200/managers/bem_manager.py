@@ -134,6 +134,10 @@ class BEMManager:
         self.raw_analytical_solved = z(n)
         self.solved = z(self.num_of_vertices)
         self.analytical_solved = z(self.num_of_vertices)
+        # colour and position buffers of the reference's window (BEM_manager.py:132-138), kept headless
+        for name in ("solved_vert_color", "solved_vertices", "analytical_vert_color", "analytical_vertices",
+                     "diff_vert_color", "diff_vertices"):
+            setattr(self, name, torch.zeros(self.num_of_vertices, 3, dtype=torch.float32, device=self.device))
         # BIO objects of the mesh's dimension (BEM_manager.py:175-191)
         if self._dim == 2:
             self.identity_layer = IdentityLayer2d(self)
@@ -444,6 +448,22 @@ class BEMManager:
             else:
                 splat_p1("D", self._Dirichlet_offset_j, int(VertAttachType.NEUMANN_TOBESOLVED))
 
+    def compute_color(self):
+        """BEMManager.compute_color (BEM_manager.py:527-587) into the headless
+        colour buffers.  As in the reference, `solved` at the Dirichlet-to-be-
+        solved vertices (every vertex when show is Dirichlet) is shifted onto
+        the mean of the exact traces there: a Neumann problem fixes the
+        Dirichlet trace only up to a constant."""
+        vt = self.cached("vert_types", lambda: self.mesh.vertice_types, dtype=torch.int32)
+        self.engine.compute_color(self.solved, self.analytical_solved, vt, self._show, self.solved_vert_color,
+                                  self.analytical_vert_color, self.diff_vert_color)
+
+    def set_mesh_instances(self):
+        """BEMManager.set_mesh_instances (BEM_manager.py:589-606): the vertex
+        positions of the solved, exact (x - 2.2) and difference (x + 2.2)
+        copies of the mesh."""
+        self.engine.set_mesh_instances(self.solved_vertices, self.analytical_vertices, self.diff_vertices)
+
     # -- driver ----------------------------------------------------------------------------
     def _fusable(self) -> bool:
         """Dirichlet problem with P0 Neumann unknowns: V and K g share every
@@ -604,14 +624,17 @@ class BEMManager:
                                        rc._rhs_vec, scale=1.0, scale_k=1.0, conj_g=self.conj_data)
 
     def run(self):
-        """BEMManager.run (BEM_manager.py:990-1030) without the GUI colouring.
-        The exact traces do not depend on the solution, so they are queued
-        before the solve, whose refinement is the step's one host
-        synchronisation; only the per-vertex splat follows it."""
+        """BEMManager.run (BEM_manager.py:990-1030).  The exact traces do not
+        depend on the solution, so they are queued before the solve, whose
+        refinement is the step's one host synchronisation; the per-vertex
+        splat and the colour and position buffers of the reference's window
+        (headless here) follow it."""
         self.assemble_system()
         self.compute_analytical_raw_solved()
         self.solve()
         self.splat_u_from_raw_solved_to_vertices()
+        self.compute_color()
+        self.set_mesh_instances()
 
     def assemble_system(self):
         """The part of `run` before the solve (BEM_manager.py:990-1018): the

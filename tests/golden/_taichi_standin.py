@@ -17,8 +17,11 @@ the product imports it.
 """
 from __future__ import annotations
 
+import ast
+import inspect
 import math
 import sys
+import textwrap
 import types
 
 import numpy as np
@@ -36,7 +39,36 @@ def data_oriented(cls):
 
 
 def kernel(fn):
-    return fn
+    """Identity, except for kernels that reduce into a kernel-scope local with
+    ``ti.atomic_max(local, value)``: Taichi updates that local in place, which a
+    Python call cannot do, so those statements are rewritten as
+    ``local = max(local, value)`` (the sequential form of the same reduction)."""
+    try:
+        src = textwrap.dedent(inspect.getsource(fn))
+    except (OSError, TypeError):
+        return fn
+    if "atomic_max" not in src:
+        return fn
+    tree = ast.parse(src)
+    fdef = tree.body[0]
+    fdef.decorator_list = []
+
+    class _Rewrite(ast.NodeTransformer):
+        def visit_Expr(self, node):
+            c = node.value
+            if (isinstance(c, ast.Call) and isinstance(c.func, ast.Attribute) and c.func.attr == "atomic_max"
+                    and isinstance(c.args[0], ast.Name)):
+                name = c.args[0].id
+                new = ast.Assign(targets=[ast.Name(name, ast.Store())],
+                                 value=ast.Call(ast.Name("max", ast.Load()), [ast.Name(name, ast.Load()), c.args[1]], []))
+                return ast.copy_location(new, node)
+            return node
+
+    tree = ast.fix_missing_locations(_Rewrite().visit(tree))
+    ast.increment_lineno(tree, fn.__code__.co_firstlineno - 1)
+    ns = {}
+    exec(compile(tree, inspect.getsourcefile(fn), "exec"), fn.__globals__, ns)
+    return ns[fdef.name]
 
 
 def func(fn):
@@ -55,7 +87,7 @@ def init(*args, **kwargs):
     return None
 
 
-def atomic_max(a, b):  # only used by the GUI colouring kernel (not on the hot path)
+def atomic_max(a, b):  # on a local, rewritten by ``kernel``; on anything else, the new maximum
     return max(a, b)
 
 

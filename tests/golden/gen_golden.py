@@ -5,12 +5,14 @@ pywavefront are not installed here, so ``_taichi_standin.install()`` registers
 a sequential FP64 stand-in for the Taichi API subset the reference uses; the
 reference's ``src/managers`` and ``src/BEM_functions`` modules are then
 imported unmodified from the reference checkout and driven through the same
-method sequence as ``BEMManager.run`` (``src/managers/BEM_manager.py:990-1018``),
-stopping before the GUI colouring kernels.
+method sequence as ``BEMManager.run`` (``src/managers/BEM_manager.py:990-1029``),
+including the two GUI kernels at its end (``compute_color``, which shifts
+``solved``, and ``set_mesh_instances``); ``solved`` is stored both before
+(``solved``) and after (``colour_solved``) the shift.
 
 Usage (in a container that has the reference checkout):
 
-    python tests/golden/gen_golden.py --ref /root/reference [--only NAME]
+    python tests/golden/gen_golden.py --ref /root/reference [--only NAME] [--colour-only]
 
 Writes ``tests/golden/<case>.npz``.  Every array needed to re-run a case
 (vertices after the reference's own normalisation, panels, BVP maps, Gauss
@@ -165,45 +167,86 @@ CASES = {
 }
 
 
-def run_case(ref, name):
+def _setup(ref, name, tmp, patched):
+    """The reference's MeshManager and BEMManager for one case, initialised
+    (mesh loaded, fields allocated, boundary callbacks set) but not run."""
     mesh, over, data_kind = CASES[name]
+    os.makedirs(os.path.join(tmp, "assets"))
+    if mesh == "cube":
+        shutil.copy(os.path.join(ref, "assets", "cube.obj"), os.path.join(tmp, "assets", "cube.obj"))
+    elif mesh.startswith("disk"):
+        pass
+    else:
+        v, f = icosphere(int(mesh[3:]))
+        write_obj(os.path.join(tmp, "assets", mesh + ".obj"), v, f)
+    params = dict(dim=3, object=mesh, GaussQR=5, n_i=1, n_o=1, k=0.0, kernel="Laplace", boundary="Dirichlet",
+                  scope="Interior", show="Default", Q_Neumann=0, Q_Dirichlet=1, log_to_disk=False,
+                  make_video=False, show_wireframe=False, vis=False)
+    params.update(over)
+    from src.managers.mesh_manager import MeshManager
+    from src.managers.BEM_manager import BEMManager
+
+    dim = int(params["dim"])
+    if mesh.startswith("disk"):
+        # the reference's own disk generator with N segments instead of its default 256
+        n_seg = int(mesh[4:])
+        disk = MeshManager.load_analytical_disk
+        patched.append((MeshManager, "load_analytical_disk", disk))
+        MeshManager.load_analytical_disk = lambda self, r=1.0, N=n_seg: disk(self, r, N)
+    core = _Core(tmp, params)
+    core._mesh_manager = MeshManager(core)
+    core._BEM_manager = BEMManager(core)
+    core._mesh_manager.initialization()
+    rng = np.random.default_rng(0)
+    d = rng.standard_normal(dim)
+    d = d / np.linalg.norm(d)
+    fD, fN = make_data(data_kind, float(params.get("k", 0.0)), d)
+    bem = core._BEM_manager
+    bem.initialization(fD, fN)
+    return bem, core._mesh_manager, params, d, data_kind
+
+
+def _colour(bem, out):
+    """The GUI preparation that ends BEMManager.run (BEM_manager.py:1028-1029):
+    compute_color shifts ``solved`` and fills the colour fields,
+    set_mesh_instances fills the three position fields."""
+    bem.compute_color()
+    bem.set_mesh_instances()
+    out["colour_solved"] = bem.solved.to_numpy()
+    for key in ("solved_vert_color", "analytical_vert_color", "diff_vert_color", "solved_vertices",
+                "analytical_vertices", "diff_vertices"):
+        out[key] = getattr(bem, key).to_numpy()
+
+
+def colour_case(ref, name):
+    """Adds the colouring outputs to an existing fixture: the case's managers
+    are set up again, ``solved`` / ``analytical_solved`` are loaded from the
+    fixture, and the reference's two GUI kernels are run on them."""
+    path = os.path.join(HERE, name + ".npz")
+    out = dict(np.load(path))
     tmp = tempfile.mkdtemp(prefix="bemgold_")
     patched = []
     try:
-        os.makedirs(os.path.join(tmp, "assets"))
-        if mesh == "cube":
-            shutil.copy(os.path.join(ref, "assets", "cube.obj"), os.path.join(tmp, "assets", "cube.obj"))
-        elif mesh.startswith("disk"):
-            pass
-        else:
-            v, f = icosphere(int(mesh[3:]))
-            write_obj(os.path.join(tmp, "assets", mesh + ".obj"), v, f)
-        params = dict(dim=3, object=mesh, GaussQR=5, n_i=1, n_o=1, k=0.0, kernel="Laplace", boundary="Dirichlet",
-                      scope="Interior", show="Default", Q_Neumann=0, Q_Dirichlet=1, log_to_disk=False,
-                      make_video=False, show_wireframe=False, vis=False)
-        params.update(over)
-        from src.managers.mesh_manager import MeshManager
-        from src.managers.BEM_manager import BEMManager
+        bem, mm, params, d, data_kind = _setup(ref, name, tmp, patched)
+        bem.solved.from_numpy(out["solved"])
+        bem.analytical_solved.from_numpy(out["analytical_solved"])
+        _colour(bem, out)
+        np.savez_compressed(path, **out)
+        print(f"{name}: colouring added", flush=True)
+    finally:
+        for owner, attr, val in patched:
+            setattr(owner, attr, val)
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def run_case(ref, name):
+    tmp = tempfile.mkdtemp(prefix="bemgold_")
+    patched = []
+    try:
         from src.BEM_functions.utils import AssembleType, ScopeType
 
+        bem, mm, params, d, data_kind = _setup(ref, name, tmp, patched)
         dim = int(params["dim"])
-        if mesh.startswith("disk"):
-            # the reference's own disk generator with N segments instead of its default 256
-            n_seg = int(mesh[4:])
-            disk = MeshManager.load_analytical_disk
-            patched.append((MeshManager, "load_analytical_disk", disk))
-            MeshManager.load_analytical_disk = lambda self, r=1.0, N=n_seg: disk(self, r, N)
-        core = _Core(tmp, params)
-        core._mesh_manager = MeshManager(core)
-        core._BEM_manager = BEMManager(core)
-        core._mesh_manager.initialization()
-        rng = np.random.default_rng(0)
-        d = rng.standard_normal(dim)
-        d = d / np.linalg.norm(d)
-        fD, fN = make_data(data_kind, float(params.get("k", 0.0)), d)
-        bem = core._BEM_manager
-        bem.initialization(fD, fN)
-        mm = core._mesh_manager
 
         out = {}
         snaps = []
@@ -222,7 +265,7 @@ def run_case(ref, name):
         bem.matrix_layer_forward = forward
 
         t0 = time.time()
-        # Same sequence as BEMManager.run (src/managers/BEM_manager.py:990-1018).
+        # Same sequence as BEMManager.run (src/managers/BEM_manager.py:990-1029).
         bem._mat_A.fill(0)
         if bem._is_transmission > 0:
             bem.matrix_layer_forward(k=bem._k, sqrt_n=bem._sqrt_no, scope_type=int(ScopeType.EXTERIOR))
@@ -253,6 +296,7 @@ def run_case(ref, name):
         bem.splat_u_from_raw_solved_to_vertices()
         out["solved"] = bem.solved.to_numpy()
         out["analytical_solved"] = bem.analytical_solved.to_numpy()
+        _colour(bem, out)
         elapsed = time.time() - t0
 
         for idx, (scope, sqrt_n, snap) in enumerate(snaps):
@@ -282,8 +326,8 @@ def run_case(ref, name):
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(f"{name}: done in {elapsed:.1f}s", flush=True)
     finally:
-        for owner, name, val in patched:
-            setattr(owner, name, val)
+        for owner, attr, val in patched:
+            setattr(owner, attr, val)
         shutil.rmtree(tmp, ignore_errors=True)
 
 
@@ -291,12 +335,17 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--colour-only", action="store_true",
+                    help="add the GUI colouring outputs to the existing fixtures without re-running the cases")
     args = ap.parse_args()
     _taichi_standin.install()
     sys.path.insert(0, args.ref)
     names = [args.only] if args.only else list(CASES)
     for name in names:
-        run_case(args.ref, name)
+        if args.colour_only:
+            colour_case(args.ref, name)
+        else:
+            run_case(args.ref, name)
 
 
 if __name__ == "__main__":

@@ -55,3 +55,25 @@ def test_relation_rule_cube():
             shared = len(set(tris[i]) & set(tris[j]))
             want = 1 if i == j else {0: 0, 1: 2, 2: 3, 3: 3}[shared]
             assert O.relation(tris, i, j) == want
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_post_oracle_matches_reference(name):
+    """oracle/post.py against the reference's compute_color and
+    set_mesh_instances run on the fixture's own per-vertex traces."""
+    from oracle import post as OP
+    d = load_fixture(name)
+    params = eval(str(d["params"]))
+    transmission = "Full" in params["boundary"] or "Transmission" in params["kernel"]
+    show = {"Neumann": 0, "Dirichlet": 1, "Default": -1}[params.get("show", "Default")]
+    if show == -1 and transmission:
+        show = 0  # BEM_manager.py:52-53
+    s, sc, ac, dc = OP.compute_color(d["solved"], d["analytical_solved"], d["vertice_types"], show)
+    want = to_complex(d["colour_solved"])
+    assert np.abs(s - want).max() <= 1e-15 * max(np.abs(to_complex(d["solved"])).max(), 1.0)
+    # the reference's colour/position fields hold FP64 here; the oracle rounds to float32 as ti.f32 does
+    for got, key in ((sc, "solved_vert_color"), (ac, "analytical_vert_color"), (dc, "diff_vert_color")):
+        assert np.abs(got - d[key]).max() <= 2e-7, key
+    for got, key in zip(OP.set_mesh_instances(d["vertices"]), ("solved_vertices", "analytical_vertices",
+                                                              "diff_vertices")):
+        assert np.abs(got - d[key]).max() <= 4e-7, key
