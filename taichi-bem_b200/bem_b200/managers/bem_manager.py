@@ -286,6 +286,12 @@ class BEMManager:
         if self.solve_precision == "fp64":
             LU = A.clone()
             piv, info = self.engine.lu_factor(LU)
+            zero_pivot = int(info.item())  # the solves below synchronise the stream anyway
+            if zero_pivot > 0:
+                # torch.linalg.solve raises on an exactly singular matrix (BEM_manager.py:1056)
+                raise torch.linalg.LinAlgError(
+                    "linalg.solve: The solver failed because the input matrix is singular "
+                    f"(zero pivot in column {zero_pivot - 1}).")
             xs = []
             for c in cols:
                 x = c.clone()

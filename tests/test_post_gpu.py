@@ -129,6 +129,8 @@ def test_driver_colour_buffers(name):
     (the singular interior Neumann problem leaves its constant to rounding)."""
     from bem_b200.managers import CoreManager
     d = load_fixture(name)
+    if "solve_error" in d:
+        pytest.skip("exactly singular: the reference's run() raises in its solve, before the colouring")
     params = eval(str(d["params"]))
     params.update(vertices=d["vertices"], panels=d["panels"])
     fD, fN = torch_callbacks(str(d["data_kind"]), float(params.get("k", 0.0)), d["direction"])
