@@ -10,11 +10,11 @@
  *   - calls are stream-ordered on the given stream and return BEM_OK (0) or
  *     a negative BEM_ERR_* code; the message of the last failure is
  *     bem_last_error(ctx);
- *   - the assembly, apply, mass, gemv, tiled-factorisation and adjoint calls
- *     queue their work without synchronising.  The mesh uploads, the
- *     partial-pivoting factorisation and solves, the tiled solves, the
- *     refinement and GMRES synchronise the stream (to read a device status
- *     word or a residual norm).  A call that has to grow the context's
+ *   - the assembly, apply, mass, gemv, tiled-factorisation, adjoint and
+ *     post-processing calls queue their work without synchronising.  The
+ *     mesh uploads, the partial-pivoting factorisation and solves, the tiled
+ *     solves, the refinement and GMRES synchronise the stream (to read a
+ *     device status word or a residual norm).  A call that has to grow the context's
  *     workspace allocates device memory, which synchronises the device;
  *   - complex values are interleaved (re, im) doubles, as torch.complex128
  *     and the reference's ti.Vector(2) [re, im];

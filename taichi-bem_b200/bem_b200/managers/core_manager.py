@@ -4,8 +4,12 @@ Same constructor argument (the `simulation_parameters` dict of the demos),
 same lifecycle (`initialization(fD, fN)`, `run()`, `kill()`).  The reference's
 interactive GGUI window and video output (core_manager.py:58-139) need a
 graphics stack and are not part of this build: `vis`, `make_video` and
-`show_wireframe` are accepted and ignored, and the per-vertex results stay in
-device tensors (`BEMManager.solved`, `.analytical_solved`).
+`show_wireframe` are accepted and ignored.  What the window would draw stays
+in device tensors: the per-vertex results (`BEMManager.solved`,
+`.analytical_solved`) and the colour and position buffers that `run()` fills
+as the reference's does (`.solved_vert_color`, `.analytical_vert_color`,
+`.diff_vert_color`, `.solved_vertices`, `.analytical_vertices`,
+`.diff_vertices`, each [nv, 3] float32).
 
 Boundary-data callbacks are vectorised: fD(x[m,dim] float64 tensor[, sqrt_n])
 and fN(x[m,dim], normal[m,dim][, sqrt_n]) return m real (Laplace) or complex
