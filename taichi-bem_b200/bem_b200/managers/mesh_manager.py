@@ -88,16 +88,24 @@ class MeshManager:
             cr = np.stack([e[:, 1], -e[:, 0]], axis=1)
             self.panel_normals = cr / np.linalg.norm(cr, axis=1)[:, None]
         else:
-            cr = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 1]])
+            a = v[f[:, 1]] - v[f[:, 0]]
+            b = v[f[:, 2]] - v[f[:, 1]]
+            cr = np.empty_like(a)  # a x b, component by component (as np.cross, without its overhead)
+            cr[:, 0] = a[:, 1] * b[:, 2] - a[:, 2] * b[:, 1]
+            cr[:, 1] = a[:, 2] * b[:, 0] - a[:, 0] * b[:, 2]
+            cr[:, 2] = a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]
             nrm = np.linalg.norm(cr, axis=1)
             if (nrm <= 0).any():
                 raise ValueError(f"degenerate panel {int(np.argmin(nrm))} (zero area)")
             self.panel_areas = 0.5 * nrm
             self.panel_normals = cr / nrm[:, None]
-        self.vert_areas = np.zeros(self.num_of_vertices)
-        np.add.at(self.vert_areas, f.reshape(-1), np.repeat(self.panel_areas / float(d), d))
-        vn = np.zeros((self.num_of_vertices, d))
-        np.add.at(vn, f.reshape(-1), np.repeat(self.panel_normals, d, axis=0))
+        # per-vertex sums over the incident panels (bincount adds in element
+        # order, as a sequential scatter does)
+        fv = f.reshape(-1)
+        nv = self.num_of_vertices
+        self.vert_areas = np.bincount(fv, weights=np.repeat(self.panel_areas / float(d), d), minlength=nv)
+        pn = np.repeat(self.panel_normals, d, axis=0)
+        vn = np.stack([np.bincount(fv, weights=pn[:, c], minlength=nv) for c in range(d)], axis=1)
         self.vert_normals = vn / np.linalg.norm(vn, axis=1)[:, None]
         if self._boundary_type == "Full" or self._is_transmission > 0:
             self.set_full_bvp()
