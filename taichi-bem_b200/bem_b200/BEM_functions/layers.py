@@ -28,6 +28,7 @@ import numpy as np
 import torch
 
 from .. import _lib as L
+from ..engine import upload
 from ..utils.types import CellFluxType, ScopeType
 
 _N = int(CellFluxType.NEUMANN_TOBESOLVED)
@@ -241,9 +242,8 @@ class RHSConstructor3d(_Layer):
 
     def _eval(self, fn, x, *args):
         b = self._BEM_manager
-        xt = x if isinstance(x, torch.Tensor) else torch.as_tensor(x, dtype=torch.float64, device=b.device)
-        targs = [torch.as_tensor(a, dtype=torch.float64, device=b.device) if isinstance(a, np.ndarray) else a
-                 for a in args]
+        xt = x if isinstance(x, torch.Tensor) else upload(x, b.device, torch.float64)
+        targs = [upload(a, b.device, torch.float64) if isinstance(a, np.ndarray) else a for a in args]
         val = fn(xt, *targs)
         return torch.as_tensor(val, device=b.device).to(b.torch_dtype).reshape(-1)
 

@@ -23,6 +23,20 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
 
 
+def upload(a, device, dtype=None) -> torch.Tensor:
+    """A host array (numpy or list) as a tensor on `device`.  For a CUDA
+    device the values are staged in pinned memory and copied on the current
+    stream without blocking the host: kernels already queued keep the GPU busy
+    while the host prepares the next launch (a pageable copy would wait for
+    them to finish).  torch's caching host allocator keeps the staging block
+    until the copy has run."""
+    t = torch.as_tensor(np.ascontiguousarray(a) if isinstance(a, np.ndarray) else a, dtype=dtype)
+    device = torch.device(device)
+    if device.type != "cuda":
+        return t.to(device)
+    return t.pin_memory().to(device, non_blocking=True)
+
+
 def _dtype_code(t: torch.Tensor) -> int:
     return {torch.float64: L.F64, torch.complex128: L.C128, torch.float32: L.F32,
             torch.complex64: L.C64}[t.dtype]
@@ -50,8 +64,8 @@ class DeviceSpace:
             raise ValueError("negative panel index")
         if pn.size != np.unique(pn).size:
             raise ValueError("a panel may appear only once per space")
-        p = torch.as_tensor(pn, device=device)
-        d = torch.as_tensor(dn, device=device)
+        p = upload(pn, device)
+        d = upload(dn, device)
         return DeviceSpace(p, int(nb), d, int(pn.max()) if pn.size else -1, int(dn.max()) if dn.size else -1)
 
     def shifted(self, offset: int):

@@ -31,7 +31,7 @@ from .. import _lib as L
 from ..BEM_functions.layers import (AdjDoubleLayer2d, AdjDoubleLayer3d, DoubleLayer2d, DoubleLayer3d,
                                     HypersingularLayer2d, HypersingularLayer3d, IdentityLayer2d, IdentityLayer3d,
                                     RHSConstructor2d, RHSConstructor3d, SingleLayer2d, SingleLayer3d)
-from ..engine import DeviceSpace, Engine
+from ..engine import DeviceSpace, Engine, upload
 from ..utils.types import AssembleType, CellFluxType, KernelType, ScopeType, VertAttachType
 
 
@@ -180,7 +180,7 @@ class BEMManager:
         it instead of copying from pageable host memory)."""
         t = self._dev_cache.get(key)
         if t is None:
-            t = torch.as_tensor(np.ascontiguousarray(make()), device=self.device)
+            t = upload(np.ascontiguousarray(make()), self.device)
             if dtype is not None:
                 t = t.to(dtype)
             self._dev_cache[key] = t

@@ -10,6 +10,8 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from .engine import upload
+
 
 def plane_wave_direction(seed: int = 0) -> np.ndarray:
     g = torch.Generator().manual_seed(seed)
@@ -20,11 +22,11 @@ def plane_wave_direction(seed: int = 0) -> np.ndarray:
 def laplace_point_source(x0=(2.0, 2.0, 2.0)):
     """u = 1/|x - x0| (harmonic inside the unit sphere); returns (fD, fN)."""
     def fD(x, s=1.0):
-        c = torch.as_tensor(x0, dtype=x.dtype, device=x.device)
+        c = upload(x0, x.device, x.dtype)
         return 1.0 / torch.linalg.norm(x - c, dim=1)
 
     def fN(x, n, s=1.0):
-        c = torch.as_tensor(x0, dtype=x.dtype, device=x.device)
+        c = upload(x0, x.device, x.dtype)
         d = x - c
         return -(d * n).sum(1) / torch.linalg.norm(d, dim=1) ** 3
     return fD, fN
@@ -35,11 +37,11 @@ def plane_wave(k: float, direction):
     dvec = np.asarray(direction, dtype=np.float64)
 
     def fD(x, s=1.0):
-        d = torch.as_tensor(dvec, dtype=x.dtype, device=x.device)
+        d = upload(dvec, x.device, x.dtype)
         return torch.exp(1j * (k * s) * (x @ d))
 
     def fN(x, n, s=1.0):
-        d = torch.as_tensor(dvec, dtype=x.dtype, device=x.device)
+        d = upload(dvec, x.device, x.dtype)
         return 1j * (k * s) * (n @ d) * torch.exp(1j * (k * s) * (x @ d))
     return fD, fN
 
@@ -54,11 +56,11 @@ class PlaneWave:
         self.d = np.asarray(direction, dtype=np.float64)
 
     def fD(self, x, s=1.0):
-        d = torch.as_tensor(self.d, dtype=x.dtype, device=x.device)
+        d = upload(self.d, x.device, x.dtype)
         return torch.exp(1j * (self.k * s) * (x @ d))
 
     def fN(self, x, n, s=1.0):
-        d = torch.as_tensor(self.d, dtype=x.dtype, device=x.device)
+        d = upload(self.d, x.device, x.dtype)
         return 1j * (self.k * s) * (n @ d) * torch.exp(1j * (self.k * s) * (x @ d))
 
 
