@@ -211,6 +211,18 @@ class BEMManager:
     def get_N_Neumann(self):
         return self.N_Neumann
 
+    def get_num_of_panels_Neumann(self):
+        return self.num_of_panels_Neumann
+
+    def get_num_of_panels_Dirichlet(self):
+        return self.num_of_panels_Dirichlet
+
+    def get_shape_func_degree_Neumann(self):
+        return self.shape_func_degree_Neumann
+
+    def get_shape_func_degree_Dirichlet(self):
+        return self.shape_func_degree_Dirichlet
+
     def get_mat_A(self):
         return self._mat_A
 
@@ -518,6 +530,36 @@ class BEMManager:
     def get_W_part(self, A):
         Do, M = self._Dirichlet_offset_i, self.M_Dirichlet
         return A[Do:Do + M, self._Dirichlet_offset_j:self._Dirichlet_offset_j + M]
+
+    # block writers, the inverse of get_*_part (BEM_manager.py:862-872)
+    def set_V_part(self, old_tensor, new_tensor):
+        self.get_V_part(old_tensor)[...] = new_tensor
+
+    def set_K_part(self, old_tensor, new_tensor):
+        self.get_K_part(old_tensor)[...] = new_tensor
+
+    def set_adj_K_part(self, old_tensor, new_tensor):
+        self.get_adj_K_part(old_tensor)[...] = new_tensor
+
+    def set_W_part(self, old_tensor, new_tensor):
+        self.get_W_part(old_tensor)[...] = new_tensor
+
+    def Jacobian_solver(self) -> float:
+        """One Jacobi sweep on _mat_A raw_solved = rhs, then the RMS of the new
+        residual, sqrt(sum |rhs - A u|^2 / n) (BEM_manager.py:803-821; the
+        reference defines it but its run never calls it).  The reference
+        updates raw_solved in place inside one parallel loop, so a row may
+        read neighbours of either sweep; here every row reads the previous
+        sweep (plain Jacobi): u <- u + (rhs - A u) / diag(A).  The products run
+        on the device through bem_gemv."""
+        n = self.N_Neumann + self.M_Dirichlet
+        A, u, b = self._mat_A, self.raw_solved, self.rhs[:n]
+        r = b.clone()
+        self.engine.gemv(A, u, r, alpha=-1.0, beta=1.0)
+        u += r / torch.diagonal(A)
+        r.copy_(b)
+        self.engine.gemv(A, u, r, alpha=-1.0, beta=1.0)
+        return float(torch.sqrt((r.abs() ** 2).sum() / n))
 
     # relative diagonal shift of the energy-scaling block before its Cholesky factorisation
     SCALING_SHIFT = 1e-10
