@@ -3,6 +3,6 @@ operator and driver surface of GeCao/taichi-BEM (``src/managers``,
 ``src/BEM_functions``).  Hot paths run in libbem_b200.so (hand-written CUDA)
 behind the C ABI in include/bem_b200.h."""
 from . import _lib
-from .meshes import icosphere, load_obj, perturbed_sphere
+from .meshes import analytical_disk, analytical_sphere, icosphere, load_obj, perturbed_sphere
 
-__all__ = ["_lib", "icosphere", "load_obj", "perturbed_sphere"]
+__all__ = ["_lib", "analytical_disk", "analytical_sphere", "icosphere", "load_obj", "perturbed_sphere"]

@@ -14,7 +14,7 @@ import re
 
 import numpy as np
 
-from ..meshes import analytical_disk, icosphere, load_obj, perturbed_sphere
+from ..meshes import analytical_disk, analytical_sphere, icosphere, load_obj, perturbed_sphere
 from ..utils.types import CellFluxType, VertAttachType
 
 _N = int(CellFluxType.NEUMANN_TOBESOLVED)
@@ -52,8 +52,12 @@ class MeshManager:
             return np.asarray(p["vertices"], np.float64), np.asarray(p["panels"], np.int32)
         if self._dim == 2:
             # the reference's 2D meshes are its analytical disk (mesh_manager.py:74-75)
-            return analytical_disk(float(p.get("disk_r", 1.0)), int(p.get("disk_N", 256)))
+            return self.load_analytical_disk(float(p.get("disk_r", 1.0)), int(p.get("disk_N", 256)))
         obj = str(p["object"])
+        if "analytical" in obj:
+            # any object name containing "analytical" selects the reference's
+            # latitude-longitude sphere (mesh_manager.py:77-78)
+            return self.load_analytical_sphere()
         m = re.fullmatch(r"icosphere(\d+)", obj)
         if m:
             return icosphere(int(m.group(1)))
@@ -61,10 +65,38 @@ class MeshManager:
         if m:
             return perturbed_sphere(int(m.group(1)), lmax=int(p.get("sh_lmax", 6)),
                                     amplitude=float(p.get("sh_amplitude", 0.05)), seed=int(p.get("seed", 0)))
-        path = obj if obj.endswith(".obj") else os.path.join(p.get("assets_path", "assets"), obj + ".obj")
+        return self.load_asset(scale=None, translate=None)
+
+    def _object_path(self):
+        obj = str(self._params["object"])
+        path = obj if obj.endswith(".obj") else os.path.join(self._params.get("assets_path", "assets"), obj + ".obj")
         if not os.path.exists(path):
             raise FileNotFoundError(f"mesh '{obj}' not found ({path})")
-        return load_obj(path, normalise=True)
+        return path
+
+    # the reference's mesh sources (mesh_manager.py:479-536)
+    def load_asset(self, scale=None, translate=None):
+        """OBJ asset: scaled by `scale` if given, moved by `translate` (default:
+        minus the vertex mean), and, without `scale`, normalised to
+        max |coordinate| = 1 (mesh_manager.py:479-494)."""
+        v, f = load_obj(self._object_path(), normalise=False)
+        if scale is not None:
+            v = v * scale
+        if translate is None:
+            translate = -v.mean(axis=0, keepdims=True)
+        v = v + translate
+        if scale is None:
+            v = v * (1.0 / np.abs(v).max())
+        return v, f
+
+    def load_analytical_sphere(self, r: float = 1.0, rows: int = 17, cols: int = 17):
+        return analytical_sphere(r, rows, cols)
+
+    def load_analytical_disk(self, r: float = 1.0, N: int = 256):
+        return analytical_disk(r, N)
+
+    def run_step(self):
+        pass
 
     def initialization(self):
         v, f = self._load()

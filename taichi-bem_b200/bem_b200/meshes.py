@@ -111,6 +111,35 @@ def load_obj(path: str, normalise: bool = True):
     return v, np.array(faces, dtype=np.int32)
 
 
+def analytical_sphere(r: float = 1.0, rows: int = 17, cols: int = 17):
+    """Latitude-longitude sphere of MeshManager.load_analytical_sphere
+    (src/managers/mesh_manager.py:496-518), same vertex and panel order: the
+    south pole (0, -r, 0); rings i = 1..rows-1 at polar angle pi i / rows,
+    each of `cols` vertices at azimuth 2 pi j / cols; the north pole last.
+    Panels: a fan from the south pole to ring 1, then two triangles per
+    (ring, column) quad, then a fan from the last ring to the north pole.
+    Returns (vertices [nv,3] float64, panels [nt,3] int32)."""
+    verts = [(0.0, -r, 0.0)]
+    panels = []
+    for i in range(1, rows):
+        theta = math.pi * i / rows
+        below, ring = 1 + (i - 2) * cols, 1 + (i - 1) * cols  # first vertex of rings i-1 and i
+        for j in range(cols):
+            phi = 2.0 * math.pi * j / cols
+            verts.append((r * math.cos(phi) * math.sin(theta), -r * math.cos(theta), r * math.sin(phi) * math.sin(theta)))
+            jn = (j + 1) % cols
+            if i == 1:
+                panels.append((0, ring + jn, ring + j))
+            else:
+                panels.append((below + j, below + jn, ring + j))
+                panels.append((below + jn, ring + jn, ring + j))
+    verts.append((0.0, r, 0.0))
+    last, north = 1 + (rows - 2) * cols, 1 + (rows - 1) * cols
+    for j in range(cols):
+        panels.append((last + j, last + (j + 1) % cols, north))
+    return np.array(verts, dtype=np.float64), np.array(panels, dtype=np.int32)
+
+
 def analytical_disk(r: float = 1.0, N: int = 256):
     """Boundary of the disk of radius r as N segments, counter-clockwise
     (MeshManager.load_analytical_disk, src/managers/mesh_manager.py:520-536):

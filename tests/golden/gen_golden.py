@@ -12,7 +12,7 @@ including the two GUI kernels at its end (``compute_color``, which shifts
 
 Usage (in a container that has the reference checkout):
 
-    python tests/golden/gen_golden.py --ref /root/reference [--only NAME] [--colour-only]
+    python tests/golden/gen_golden.py --ref /root/reference [--only NAME] [--colour-only] [--meshes]
 
 Writes ``tests/golden/<case>.npz``.  Every array needed to re-run a case
 (vertices after the reference's own normalisation, panels, BVP maps, Gauss
@@ -28,6 +28,7 @@ import shutil
 import sys
 import tempfile
 import time
+import types
 
 import numpy as np
 
@@ -331,15 +332,39 @@ def run_case(ref, name):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def mesh_fixture(ref):
+    """The reference's own analytic mesh generators
+    (MeshManager.load_analytical_sphere / load_analytical_disk,
+    src/managers/mesh_manager.py:496-536), called on an object that carries
+    only the dtype they read, into tests/golden/meshes_analytical.npz."""
+    from src.managers.mesh_manager import MeshManager
+
+    holder = types.SimpleNamespace(_np_dtype=np.float64)
+    out = {}
+    for tag, kw in (("sphere_default", {}), ("sphere_r07_5x6", dict(r=0.7, rows=5, cols=6))):
+        v, f = MeshManager.load_analytical_sphere(holder, **kw)
+        out[f"{tag}_vertices"], out[f"{tag}_panels"] = v, f
+    for tag, kw in (("disk_default", {}), ("disk_r05_37", dict(r=0.5, N=37))):
+        v, f = MeshManager.load_analytical_disk(holder, **kw)
+        out[f"{tag}_vertices"], out[f"{tag}_panels"] = v, f
+    np.savez_compressed(os.path.join(HERE, "meshes_analytical.npz"), **out)
+    print("meshes_analytical: done", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--meshes", action="store_true",
+                    help="only write the analytic-mesh fixture from the reference's generators")
     ap.add_argument("--colour-only", action="store_true",
                     help="add the GUI colouring outputs to the existing fixtures without re-running the cases")
     args = ap.parse_args()
     _taichi_standin.install()
     sys.path.insert(0, args.ref)
+    if args.meshes:
+        mesh_fixture(args.ref)
+        return
     names = [args.only] if args.only else list(CASES)
     for name in names:
         if args.colour_only:

@@ -1,0 +1,51 @@
+"""MeshManager's mesh sources on the host (no GPU): the reference's object
+names and normalisation (src/managers/mesh_manager.py:67-139,479-536)."""
+import numpy as np
+import pytest
+
+from bem_b200.meshes import analytical_disk, analytical_sphere
+
+
+def _mesh_manager(**params):
+    from bem_b200.managers import CoreManager
+    p = dict(dim=3, object="sphere", GaussQR=3, kernel="Laplace", boundary="Dirichlet", scope="Interior")
+    p.update(params)
+    core = CoreManager(p)  # no device work before initialization()
+    mm = core._mesh_manager
+    mm.initialization()
+    return mm
+
+
+@pytest.mark.parametrize("name", ["analytical_sphere", "my_analytical"])
+def test_analytical_object_names_load_the_reference_sphere(name):
+    mm = _mesh_manager(object=name)
+    v, f = analytical_sphere()
+    assert np.array_equal(mm.vertices, v) and np.array_equal(mm.panels, f)
+    assert (mm.num_of_vertices, mm.num_of_panels) == (2 + 16 * 17, 2 * 17 + 2 * 15 * 17)
+    # consistently oriented: the reference's generator turns every panel inward
+    cent = v[f].mean(axis=1)
+    assert ((cent * mm.panel_normals).sum(1) < 0).all()
+    assert 0.97 * 4 * np.pi < mm.panel_areas.sum() < 4 * np.pi  # an inscribed polyhedron
+
+
+def test_asset_is_centred_and_normalised(tmp_path):
+    v = np.array([[0, 0, 0], [2, 0, 0], [0, 4, 0], [0, 0, 6]], dtype=np.float64) + 10.0
+    f = np.array([[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]])
+    path = tmp_path / "tet.obj"
+    path.write_text("".join("v %.17g %.17g %.17g\n" % tuple(p) for p in v) + "".join("f %d %d %d\n" % tuple(t + 1) for t in f))
+    mm = _mesh_manager(object=str(path))
+    want = (v - v.mean(axis=0)) / np.abs(v - v.mean(axis=0)).max()
+    assert np.array_equal(mm.vertices, want)
+    a, _ = mm.load_asset(scale=2.0, translate=np.zeros((1, 3)))  # explicit scale: no normalisation
+    assert np.array_equal(a, v * 2.0)
+
+
+def test_2d_default_is_the_reference_disk():
+    mm = _mesh_manager(dim=2, object="disk")
+    v, f = analytical_disk()
+    assert np.array_equal(mm.vertices, v) and np.array_equal(mm.panels, f)
+
+
+def test_missing_asset_raises():
+    with pytest.raises(FileNotFoundError):
+        _mesh_manager(object="no_such_mesh_here")

@@ -1,5 +1,7 @@
 """Pin the CPU oracle to the reference: every golden fixture was produced by
 running the reference's own kernels (tests/golden/gen_golden.py)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -77,3 +79,17 @@ def test_post_oracle_matches_reference(name):
     for got, key in zip(OP.set_mesh_instances(d["vertices"]), ("solved_vertices", "analytical_vertices",
                                                               "diff_vertices")):
         assert np.abs(got - d[key]).max() <= 4e-7, key
+
+
+def test_analytic_meshes_match_reference_generators():
+    """bem_b200.meshes against the reference's own load_analytical_sphere /
+    load_analytical_disk output (tests/golden/meshes_analytical.npz): the
+    same vertices, bit for bit, and the same panels in the same order (the
+    P0 unknowns are numbered by panel)."""
+    from bem_b200.meshes import analytical_disk, analytical_sphere
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "meshes_analytical.npz"))
+    cases = {"sphere_default": analytical_sphere(), "sphere_r07_5x6": analytical_sphere(0.7, 5, 6),
+             "disk_default": analytical_disk(), "disk_r05_37": analytical_disk(0.5, 37)}
+    for tag, (v, f) in cases.items():
+        assert np.array_equal(v, d[f"{tag}_vertices"]), tag
+        assert np.array_equal(f, d[f"{tag}_panels"]), tag
