@@ -56,3 +56,30 @@ def test_driver_mixed_precision(name):
     assert rel_err(b.raw_solved.cpu().numpy(), ref) < 1e-5
     assert b.solve_info["relres"] <= 1e-12
     core.kill()
+
+
+@pytest.mark.parametrize("kernel,boundary", [("Laplace", "Dirichlet"), ("Helmholtz", "Neumann")])
+def test_driver_on_reference_analytic_sphere(kernel, boundary):
+    """The reference's latitude-longitude sphere (object "analytical_sphere":
+    poles shared by 17 panels, inward-oriented panels) through the driver,
+    against the oracle on the same mesh."""
+    from bem_b200.managers import CoreManager
+    from bem_b200.meshes import analytical_sphere
+    from oracle import oracle as O
+    from tests._util import data_callbacks
+    k = 1.3 if kernel == "Helmholtz" else 0.0
+    params = dict(dim=3, object="analytical_sphere", GaussQR=3, kernel=kernel, boundary=boundary, scope="Interior",
+                  k=k, Q_Neumann=0, Q_Dirichlet=1)
+    kind = "plane_wave" if kernel == "Helmholtz" else "laplace_point"
+    d = np.array([0.6, 0.0, 0.8])
+    v, f = analytical_sphere()
+    P = O.Problem(v, f, params, *data_callbacks(kind, k, d))
+    r = P.run()
+    core = CoreManager(params)
+    core.initialization(*torch_callbacks(kind, k, d))
+    b = core._BEM_manager
+    assert np.array_equal(core._mesh_manager.vertices, v)
+    b.assemble_system()
+    assert rel_err(b._mat_A.cpu().numpy(), r["A"]) < 1e-12
+    assert rel_err(b.rhs.cpu().numpy(), r["rhs"]) < 1e-12
+    core.kill()
