@@ -290,32 +290,40 @@ class BEMManager:
             self.rhs.copy_(self.rhs_constructor._rhs_vec)
 
     # -- solve --------------------------------------------------------------------------
+    def _lu_solve_fp64(self, A: torch.Tensor, b: torch.Tensor, cols) -> torch.Tensor:
+        """Partial-pivoting FP64 LU and solves.  An exact zero pivot raises
+        torch.linalg.LinAlgError, as the reference's torch.linalg.solve does
+        on a singular matrix (BEM_manager.py:1056)."""
+        LU = A.clone()
+        piv, info = self.engine.lu_factor(LU)
+        zero_pivot = int(info.item())  # the solves below synchronise the stream anyway
+        if zero_pivot > 0:
+            raise torch.linalg.LinAlgError(
+                "linalg.solve: The solver failed because the input matrix is singular "
+                f"(zero pivot in column {zero_pivot - 1}).")
+        xs = []
+        for c in cols:
+            x = c.clone()
+            self.engine.lu_solve(LU, piv, x)
+            xs.append(x)
+        self.solve_info = {"factor": "fp64", "info": info}
+        return xs[0] if b.dim() == 1 else torch.stack(xs, 1)
+
     def _lu_solve_square(self, A: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
         """x = A^{-1} b with the hand-written LU: FP64 factor (plain path) or
         FP32 factor + FP64 refinement against A (mixed path).  b is a vector
         or an n x nrhs matrix; A is factored once."""
         cols = [b.contiguous()] if b.dim() == 1 else [b[:, j].contiguous() for j in range(b.shape[1])]
         if self.solve_precision == "fp64":
-            LU = A.clone()
-            piv, info = self.engine.lu_factor(LU)
-            zero_pivot = int(info.item())  # the solves below synchronise the stream anyway
-            if zero_pivot > 0:
-                # torch.linalg.solve raises on an exactly singular matrix (BEM_manager.py:1056)
-                raise torch.linalg.LinAlgError(
-                    "linalg.solve: The solver failed because the input matrix is singular "
-                    f"(zero pivot in column {zero_pivot - 1}).")
-            xs = []
-            for c in cols:
-                x = c.clone()
-                self.engine.lu_solve(LU, piv, x)
-                xs.append(x)
-            self.solve_info = {"factor": "fp64", "info": info}
-            return xs[0] if b.dim() == 1 else torch.stack(xs, 1)
+            return self._lu_solve_fp64(A, b, cols)
         lo = torch.complex64 if A.is_complex() else torch.float32
         LU = A.to(lo)
         piv, dinv, info = self.engine.lu_factor_tiled(LU)
         kind = "fp32 tile-pivoted + refinement"
         state = {"LU": LU, "piv": piv, "dinv": dinv}
+
+        class _ZeroPivot(Exception):
+            pass
 
         def partial_pivoting():
             # tile pivoting restricts row swaps to the 64-row diagonal tiles; a
@@ -323,8 +331,12 @@ class BEMManager:
             # partial pivoting over full columns
             if state["dinv"] is not None:
                 state["LU"] = A.to(lo)
-                state["piv"], _ = self.engine.lu_factor(state["LU"])
+                state["piv"], pinfo = self.engine.lu_factor(state["LU"])
                 state["dinv"] = None
+                if int(pinfo.item()) > 0:
+                    # an exact zero pivot even with full-column pivoting: the FP64
+                    # factorisation decides (it raises if A is singular in FP64)
+                    raise _ZeroPivot()
 
         xs, its, rrs = [], [], []
         for c in cols:
@@ -336,7 +348,10 @@ class BEMManager:
             except L.BemError as exc:
                 if exc.code != -4:
                     raise
-                partial_pivoting()
+                try:
+                    partial_pivoting()
+                except _ZeroPivot:
+                    return self._lu_solve_fp64(A, b, cols)
                 x.zero_()
                 try:
                     it, rr = self.engine.refine_solve(A, state["LU"], state["piv"], c, x, tol=self.refine_tol,
@@ -355,6 +370,12 @@ class BEMManager:
             xs.append(x)
             its.append(it)
             rrs.append(rr)
+        if int(info.item()) > 0:
+            # the tile factor met an exact zero pivot (read after the refinement's
+            # synchronisation): refinement can still converge on a singular but
+            # consistent system, where the reference's torch.linalg.solve raises,
+            # so the FP64 factorisation decides
+            return self._lu_solve_fp64(A, b, cols)
         self.solve_info = {"factor": kind, "info": info, "refine_iters": max(its), "relres": max(rrs)}
         return xs[0] if b.dim() == 1 else torch.stack(xs, 1)
 

@@ -83,3 +83,15 @@ def test_driver_on_reference_analytic_sphere(kernel, boundary):
     assert rel_err(b._mat_A.cpu().numpy(), r["A"]) < 1e-12
     assert rel_err(b.rhs.cpu().numpy(), r["rhs"]) < 1e-12
     core.kill()
+
+
+@pytest.mark.parametrize("name", ["cube_helm_mix_ext_q4", "disk24_helm_mix_ext_q3"])
+def test_mixed_path_raises_on_singular_system(name):
+    """On the exactly singular fixtures the mixed path ends in the FP64
+    factorisation, which raises the reference's error type."""
+    d = load_fixture(name)
+    assert "solve_error" in d
+    core, b = _run(d, precision="mixed")
+    with pytest.raises(torch.linalg.LinAlgError, match="singular"):
+        b.run()
+    core.kill()
