@@ -49,3 +49,24 @@ def test_2d_default_is_the_reference_disk():
 def test_missing_asset_raises():
     with pytest.raises(FileNotFoundError):
         _mesh_manager(object="no_such_mesh_here")
+
+
+@pytest.mark.parametrize("mesh", ["icosphere2", "analytical_sphere", "disk"])
+@pytest.mark.parametrize("boundary", ["Dirichlet", "Neumann", "Mix", "Full"])
+@pytest.mark.parametrize("qn,qd", [(0, 1), (1, 1), (0, 0), (1, 0)])
+def test_partitions_match_the_oracle(mesh, boundary, qn, qd):
+    """The BVP partition, the DOF counts and the local<->global maps
+    (mesh_manager.py:166-389,415-445) and the per-vertex geometry, against the
+    oracle's restatement (pinned to the reference's fixtures)."""
+    from oracle import oracle as O
+    dim = 2 if mesh == "disk" else 3
+    mm = _mesh_manager(object=mesh, dim=dim, boundary=boundary, Q_Neumann=qn, Q_Dirichlet=qd)
+    om = O.Mesh(mm.vertices, mm.panels, boundary=boundary, Q_Neumann=qn, Q_Dirichlet=qd, dim=dim)
+    assert (mm.N_Neumann, mm.M_Dirichlet) == (om.N_N, om.M_D)
+    assert (mm.num_of_panels_Neumann, mm.num_of_panels_Dirichlet) == (om.nP_N, om.nP_D)
+    for ours, theirs in ((mm.panel_types, om.panel_types), (mm.vertice_types, om.vert_types),
+                         (mm.Dirichlet_index, om.D_index), (mm.Neumann_index, om.N_index),
+                         (mm.map_global_Neumann_to_local, om.map_N), (mm.map_global_Dirichlet_to_local, om.map_D)):
+        assert np.array_equal(np.asarray(ours), np.asarray(theirs))
+    assert np.allclose(mm.vert_areas, om.vert_areas, rtol=1e-14, atol=0)
+    assert np.allclose(mm.vert_normals, om.vert_normals, rtol=0, atol=1e-14)
