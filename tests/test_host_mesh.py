@@ -70,3 +70,39 @@ def test_partitions_match_the_oracle(mesh, boundary, qn, qd):
         assert np.array_equal(np.asarray(ours), np.asarray(theirs))
     assert np.allclose(mm.vert_areas, om.vert_areas, rtol=1e-14, atol=0)
     assert np.allclose(mm.vert_normals, om.vert_normals, rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("bad,exc", [
+    (dict(kernel="Stokes"), RuntimeError),             # BEM_manager.py:40-50
+    (dict(show="Both"), RuntimeError),
+    (dict(precision="fp16"), ValueError),
+    (dict(dim=4), NotImplementedError),
+    (dict(Q_Neumann=2), AssertionError),
+])
+def test_bad_configuration_is_rejected_on_the_host(bad, exc):
+    from bem_b200.managers import CoreManager
+    p = dict(dim=3, object="icosphere1", GaussQR=3, kernel="Laplace", boundary="Dirichlet", scope="Interior")
+    p.update(bad)
+    with pytest.raises(exc):
+        CoreManager(p)
+
+
+def test_bad_boundary_type_is_rejected():
+    with pytest.raises(RuntimeError, match="Boundary Type"):
+        _mesh_manager(object="icosphere1", boundary="Robin")
+
+
+@pytest.mark.parametrize("case", ["nan_vertex", "index_out_of_range", "zero_area", "wrong_width"])
+def test_bad_mesh_is_rejected_on_the_host(case):
+    v, f = analytical_sphere(1.0, 4, 5)
+    v, f = v.copy(), f.copy()
+    if case == "nan_vertex":
+        v[3, 1] = np.nan
+    elif case == "index_out_of_range":
+        f[7, 2] = len(v)
+    elif case == "zero_area":
+        f[2] = [f[2, 0], f[2, 0], f[2, 1]]
+    else:
+        f = f[:, :2]
+    with pytest.raises(ValueError):
+        _mesh_manager(vertices=v, panels=f)
