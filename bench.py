@@ -285,8 +285,8 @@ def profile_step(precision: str):
     command the committed ncu summaries under profiles/ were captured with)."""
     import torch
     from bem_b200.managers import CoreManager
-    from bem_b200.workloads import config2
-    params, fD, fN = config2(precision=precision)
+    from bem_b200.workloads import helmholtz_dirichlet_s4
+    params, fD, fN = helmholtz_dirichlet_s4(precision=precision)
     core = CoreManager(params)
     core.initialization(fD, fN)
     b = core._BEM_manager
@@ -325,16 +325,16 @@ def profile_lu(n: int):
 
 
 def sweep_bench(n_k: int):
-    """Config 3: the wavenumber sweep (managers/sweep.py) of the augmented
+    """The wavenumber sweep (managers/sweep.py) of the augmented
     transmission operator, mixed precision against the plain FP64 path; one
     JSON line with per-k times, errors and the norm estimates."""
     import torch
     from bem_b200.managers import CoreManager
     from bem_b200.managers.sweep import wavenumber_sweep
-    from bem_b200.workloads import config3
+    from bem_b200.workloads import transmission_sweep_s4
     res = {}
     for prec in ("mixed", "fp64"):
-        params, fD, fN, ks = config3(prec, n_k)
+        params, fD, fN, ks = transmission_sweep_s4(prec, n_k)
         core = CoreManager(params)
         core.initialization(fD, fN)
         # mixed: Krylov norm estimates; plain: the reference's own full SVD per k
@@ -350,7 +350,7 @@ def sweep_bench(n_k: int):
             for a, b in zip(res["mixed"]["solutions"], res["fp64"]["solutions"])]
     nerr = [abs(a - b) / b for a, b in zip(res["mixed"]["inv_norm"], res["fp64"]["inv_norm"])]
     print(json.dumps({
-        "workload": "config 3: augmented transmission sweep, icosphere s4, P1/P1 (5124 unknowns), GaussQR=3, "
+        "workload": "augmented transmission sweep, icosphere s4, P1/P1 (5124 unknowns), GaussQR=3, "
                     "n_i=3, n_o=1, 4 complex Gaussian RHS per k",
         "n_k": len(res["mixed"]["k"]), "k_range": [res["mixed"]["k"][0], res["mixed"]["k"][-1]],
         "mixed_s": res["mixed"]["total_s"], "plain_fp64_s": res["fp64"]["total_s"],
@@ -366,7 +366,7 @@ def sweep_bench(n_k: int):
 
 
 def shape_bench(subdiv: int, n_check: int):
-    """Config 4: shape gradient of the Laplace Dirichlet problem on a radially
+    """The shape gradient of the Laplace Dirichlet problem on a radially
     perturbed icosphere (real spherical harmonics of degree <= 6, max |dr| =
     0.05), J = ||t - t_target||^2 with t_target from the unperturbed sphere,
     GaussQR = 5.  Times the mixed forward solve and the adjoint pass, and
@@ -419,7 +419,7 @@ def shape_bench(subdiv: int, n_check: int):
         errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
     gmax = float(G64.abs().max())
     print(json.dumps({
-        "workload": f"config 4: shape gradient, Laplace Dirichlet, perturbed icosphere s{subdiv} ({len(f)} panels), "
+        "workload": f"shape gradient, Laplace Dirichlet, perturbed icosphere s{subdiv} ({len(f)} panels), "
                     "GaussQR=5, J = ||t - t_target||^2",
         "forward_ms_mixed": fwd_ms, "adjoint_ms": bwd_ms, "forward_ms_fp64_assembly": fwd64_ms,
         "fd_check": {"vertices": n_check, "h": h, "max_rel_err": max(errs), "median_rel_err": float(np.median(errs))},
@@ -428,7 +428,7 @@ def shape_bench(subdiv: int, n_check: int):
 
 
 def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
-    """Config 5: the Helmholtz transmission system (k_out = 5, k_in = 7.5) on
+    """The Helmholtz transmission system (k_out = 5, k_in = 7.5) on
     icosphere s<subdiv> in mixed precision (FP32 far field, FP64 near field,
     TF32 tile LU + FP64 refinement on the square system), its error against
     the FP64-assembled system solved to FP64 accuracy, and dJ/dk of
@@ -436,9 +436,9 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
     import torch
     from bem_b200.managers import CoreManager
     from bem_b200.managers.sweep import solution_norm_k_gradient
-    from bem_b200.workloads import config5
+    from bem_b200.workloads import transmission_s5
     res = {}
-    params, pw = config5("mixed", subdiv, solver)
+    params, pw = transmission_s5("mixed", subdiv, solver)
     core = CoreManager(params)
     core.initialization(pw.fD, pw.fN)
     b = core._BEM_manager
@@ -456,7 +456,7 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
                    "rel_diff": abs(g["dJdk"] - g["dJdk_central_difference"]) / abs(g["dJdk_central_difference"]),
                    "adjoint_ms": g["adjoint_ms"], "delta": 1e-3}
     core.kill()
-    params, pw = config5("fp64", subdiv, solver)
+    params, pw = transmission_s5("fp64", subdiv, solver)
     params.update(solve_precision="mixed", refine_tol=1e-13)
     core = CoreManager(params)
     core.initialization(pw.fD, pw.fN)
@@ -466,7 +466,7 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
     res["rel_err_vs_fp64"] = {"l2": float(torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)),
                               "max": float((x_mixed - x64).abs().max() / x64.abs().max())}
     if plain:
-        params, pw = config5("fp64", subdiv, solver)
+        params, pw = transmission_s5("fp64", subdiv, solver)
         core = CoreManager(params)
         core.initialization(pw.fD, pw.fN)
         torch.cuda.synchronize()
@@ -476,7 +476,7 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
         res["plain_fp64_ms"] = (time.perf_counter() - t0) * 1e3
         res["speedup"] = res["plain_fp64_ms"] / res["mixed_ms"]
         core.kill()
-    print(json.dumps(dict(workload=f"config 5: Helmholtz transmission, icosphere s{subdiv}, {n} unknowns, k_out=5, "
+    print(json.dumps(dict(workload=f"Helmholtz transmission, icosphere s{subdiv}, {n} unknowns, k_out=5, "
                                    f"k_in=7.5, GaussQR=5, solver {solver}", **res)))
 
 
@@ -573,9 +573,11 @@ def main():
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
     ap.add_argument("--profile-lu", type=int, default=0,
                     help="time six tiled FP32 factorisations of a random complex matrix of this size and exit")
-    ap.add_argument("--workload", default="config2", choices=["config2", "sweep", "shape", "transmission", "disk2d"],
-                    help="sweep: the config-3 wavenumber sweep, shape: the config-4 shape gradient, disk2d: the "
-                         "2D operators (each its own JSON line)")
+    ap.add_argument("--workload", default="helmholtz_dirichlet_s4",
+                    choices=["helmholtz_dirichlet_s4", "sweep", "shape", "transmission", "disk2d"],
+                    help="helmholtz_dirichlet_s4: the headline line; sweep: the wavenumber sweep of the augmented "
+                         "transmission operator; shape: the shape gradient on a perturbed sphere; transmission: "
+                         "the Helmholtz transmission system; disk2d: the 2D operators (each its own JSON line)")
     ap.add_argument("--disk-n", type=int, default=8192, help="segments of the disk2d workload")
     ap.add_argument("--shape-subdiv", type=int, default=5, help="icosphere subdivision of the shape workload")
     ap.add_argument("--shape-check", type=int, default=32, help="vertices of the finite-difference check")
@@ -632,10 +634,10 @@ def main():
 
     from bem_b200.engine import measure_peaks
     from bem_b200.managers import CoreManager
-    from bem_b200.workloads import config2
+    from bem_b200.workloads import helmholtz_dirichlet_s4
 
     def make(precision, extra=None):
-        params, fD, fN = config2(precision=precision)
+        params, fD, fN = helmholtz_dirichlet_s4(precision=precision)
         params["device"] = f"cuda:{local}"
         if extra:
             params.update(extra)
@@ -704,7 +706,7 @@ def main():
     for s in range(5):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        params, fD, fN = config2(precision="mixed")
+        params, fD, fN = helmholtz_dirichlet_s4(precision="mixed")
         params.update(device=f"cuda:{local}", vertices=vpin.numpy(), panels=fpin.numpy())
         c2 = CoreManager(params)
         c2.initialization(fD, fN)

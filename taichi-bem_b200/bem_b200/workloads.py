@@ -72,21 +72,21 @@ def _base(**kw):
     return p
 
 
-def config1(precision="fp64"):
+def laplace_dirichlet_s3(precision="fp64"):
     """Laplace 3D interior Dirichlet on icosphere s3 (1280 panels), GaussQR=5,
     u = 1/|x - x0|, x0 = (2,2,2): V t = (1/2 M + K) g."""
     fD, fN = laplace_point_source()
     return _base(object="icosphere3", precision=precision), fD, fN
 
 
-def config2(precision="mixed", seed=0):
+def helmholtz_dirichlet_s4(precision="mixed", seed=0):
     """Helmholtz 3D interior Dirichlet, k = 3, icosphere s4 (5120 panels),
     GaussQR=5, plane wave exp(i k d.x) with a seeded random unit d."""
     fD, fN = plane_wave(3.0, plane_wave_direction(seed))
     return _base(object="icosphere4", kernel="Helmholtz", k=3.0, precision=precision), fD, fN
 
 
-def config3(precision="mixed", n_k=60):
+def transmission_sweep_s4(precision="mixed", n_k=60):
     """Wavenumber sweep of the augmented transmission operator on icosphere s4
     (5120 panels, P1 Neumann and Dirichlet: 5124 unknowns), k_i = 16 + i/30,
     with the reference sweep's parameters (demo_3d_plot_Sio.py: n_i = 3,
@@ -98,7 +98,7 @@ def config3(precision="mixed", n_k=60):
     return params, fD, fN, ks
 
 
-def config5(precision="mixed", subdiv=5, solver="square"):
+def transmission_s5(precision="mixed", subdiv=5, solver="square"):
     """Helmholtz transmission (2x2 block Calderon system), icosphere s5 (20480
     panels, P0 Neumann + P1 Dirichlet: 30722 unknowns), k_out = 5,
     n_i = 2.25 (k_in = 7.5), n_o = 1, GaussQR = 5, incident plane wave with a
@@ -111,4 +111,5 @@ def config5(precision="mixed", subdiv=5, solver="square"):
     return params, pw
 
 
-CONFIGS = {1: config1, 2: config2, 3: config3, 5: config5}
+WORKLOADS = {f.__name__: f for f in (laplace_dirichlet_s3, helmholtz_dirichlet_s4, transmission_sweep_s4,
+                                      transmission_s5)}

@@ -82,9 +82,9 @@ def test_reference_orientation_handling_leaves_an_O_h_error():
     assert 1e-4 < err[1] < err[0] < 1e-2
 
 
-def _config1_trace_error(s, quirk):
+def _point_source_trace_error(s, quirk):
     """Laplace interior Dirichlet on icosphere s with u = 1/|x - x0|,
-    x0 = (2, 2, 2) (config 1): l2 error of the P0 Neumann trace against
+    x0 = (2, 2, 2), GaussQR 4: l2 error of the P0 Neumann trace against
     du/dn at the centroids."""
     from tests._util import data_callbacks
     fD, fN = data_callbacks("laplace_point")
@@ -97,8 +97,8 @@ def _config1_trace_error(s, quirk):
     return np.linalg.norm(t - exact) / np.linalg.norm(exact)
 
 
-def test_config1_trace_converges_with_the_corrected_quadrature():
-    err = [_config1_trace_error(s, quirk=False) for s in (1, 2, 3)]
+def test_point_source_trace_converges_with_the_corrected_quadrature():
+    err = [_point_source_trace_error(s, quirk=False) for s in (1, 2, 3)]
     assert err[2] < 7e-3 and err[0] / err[1] > 2.5 and err[1] / err[2] > 2.5
 
 
@@ -108,5 +108,5 @@ def test_reference_quadrature_trace_does_not_converge():
     O(1/h), so the trace error stays O(1) under refinement (the reference's
     own fixtures show the same: its cube and icosphere solutions are O(1) away
     from their analytic traces)."""
-    err = [_config1_trace_error(s, quirk=True) for s in (1, 2)]
+    err = [_point_source_trace_error(s, quirk=True) for s in (1, 2)]
     assert min(err) > 0.3
