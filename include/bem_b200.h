@@ -88,7 +88,8 @@ typedef struct {
 int bem_ctx_create(bem_ctx** out_ctx);
 int bem_ctx_destroy(bem_ctx* ctx);
 const char* bem_last_error(const bem_ctx* ctx);
-/* Number of kernels this library launched through ctx since creation. */
+/* Number of kernels this library launched through ctx since creation (no
+ * reference counterpart). */
 int64_t bem_launch_count(const bem_ctx* ctx);
 
 /* ---- mesh ------------------------------------------------------------------
@@ -112,9 +113,12 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
  * Synchronous. */
 int bem_mesh_set_2d(bem_ctx* ctx, const double* verts, const int32_t* segs, int nv, int nt, int gauss_qr);
 /* Number of ordered panel pairs of the current mesh that share a vertex
- * (coincident + edge + vertex pairs; on a 2D mesh, coincident + vertex). */
+ * (coincident + edge + vertex pairs; on a 2D mesh, coincident + vertex): the
+ * pairs get_panels_relation (mesh_manager.py:538-573) does not call
+ * SEPARATE. */
 int64_t bem_near_pair_count(const bem_ctx* ctx);
-/* Copies the per-panel areas [nt] and unit normals [nt*3] (device pointers). */
+/* Copies the per-panel areas [nt] and unit normals [nt*3] (device pointers):
+ * MeshManager's panel_areas / panel_normals (mesh_manager.py:108-139). */
 int bem_mesh_geometry(const bem_ctx* ctx, double* areas, double* normals, void* stream);
 
 /* ---- assembly ---------------------------------------------------------------
@@ -181,33 +185,39 @@ int bem_adjoint_vertices(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
  * set to 0 or to 1+index of the first zero pivot. */
 int bem_lu_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, int32_t* info,
                   void* stream);
-/* Solve with the factors: b (n x nrhs, row-major, ldb) overwritten by x. */
+/* Solve with the factors: b (n x nrhs, row-major, ldb) overwritten by x (the
+ * solve half of torch.linalg.solve, BEM_manager.py:1056). */
 int bem_lu_solve(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                  void* b, int64_t nrhs, int64_t ldb, void* stream);
 /* y = alpha*A*x + beta*y for one vector (dtype of A: F64/C128/F32/C64; x, y in
- * the matching FP64 type F64/C128).  Used for the refinement residual. */
+ * the matching FP64 type F64/C128).  Replaces the product of assemble_rhs
+ * (BEM_manager.py:647-662) and Jacobian_solver (:803-821); also the
+ * refinement residual. */
 int bem_gemv(bem_ctx* ctx, int a_dtype, const void* A, int64_t m, int64_t n, int64_t lda,
              const void* x, void* y, double alpha, double beta, void* stream);
 
 /* Tile-pivoted LU (the low-precision factor of the mixed path; replaces the
- * same torch.linalg.solve call): partial pivoting restricted to each 64x64
+ * same torch.linalg.solve call, BEM_manager.py:1056): partial pivoting restricted to each 64x64
  * diagonal tile, explicit inverses of the diagonal tiles written to `dinv`
  * (device, bem_lu_dinv_elems(n) elements of the dtype's complex-pair width:
  * 2 x float / 2 x double per element).  No grid-wide synchronisation. */
 int64_t bem_lu_dinv_elems(int64_t n);
-/* Queued without synchronisation.  A tensor-core wait of the trailing updates
+/* The factorisation (replaces the factor half of torch.linalg.solve,
+ * BEM_manager.py:1056).  Queued without synchronisation.  A tensor-core wait
+ * of the trailing updates
  * that ran out of its iteration cap is reported (BEM_ERR_TIMEOUT) by the next
  * bem_lu_solve_tiled or bem_refine_solve on the same context. */
 int bem_lu_factor_tiled(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, void* dinv,
                         int32_t* info, void* stream);
-/* x = U^{-1} L^{-1} P b for one FP64 right-hand side b (overwritten), with the
+/* The solve half of torch.linalg.solve (BEM_manager.py:1056):
+ * x = U^{-1} L^{-1} P b for one FP64 right-hand side b (overwritten), with the
  * factors of bem_lu_factor_tiled; a persistent kernel driven by per-tile ready
  * flags (bounded waits; BEM_ERR_TIMEOUT if one runs out). */
 int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                        const void* dinv, void* b, void* stream);
 
-/* Allocation-free variant of bem_lu_solve_tiled (no counterpart in the
- * reference).  For callers that must not allocate device memory once they are
+/* Allocation-free variant of bem_lu_solve_tiled (no reference counterpart
+ * beyond the solve of BEM_manager.py:1056).  For callers that must not allocate device memory once they are
  * running -- for example an application whose device memory is owned by
  * another allocator, or a latency-critical loop where cudaMalloc's implicit
  * device synchronisation is not acceptable -- and that therefore cannot create
@@ -225,7 +235,8 @@ int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64
 int bem_lu_solve_tiled_static(int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                               const void* dinv, void* b, void* stream);
 
-/* Mixed-precision solve: x = A_hi^{-1} b to relative residual tol by FP64
+/* Mixed-precision solve, in place of torch.linalg.solve (BEM_manager.py:1056):
+ * x = A_hi^{-1} b to relative residual tol by FP64
  * iterative refinement on the residual b - A_hi x, each correction solved with
  * the low-precision factors (LU_lo, piv[, dinv]) of A_hi: tile-pivoted factors
  * when dinv != NULL, else partial-pivoting factors.  A_hi: F64/C128, LU_lo:

@@ -24,3 +24,15 @@ def test_header_and_library_agree():
 def test_library_is_sm100a():
     from bem_b200 import _lib
     assert os.path.getsize(_lib.LIB_PATH) > 0
+
+
+def test_every_entry_point_cites_what_it_replaces():
+    """Each declaration's comment names the reference interface it replaces
+    (file.py:line) or says it has no reference counterpart."""
+    import re
+    src = open(os.path.join(ROOT, "include", "bem_b200.h")).read()
+    for m in re.finditer(r"^(?:int|int64_t|const char\*)\s+(bem_\w+)\(", src, re.M):
+        before = src[:m.start()]
+        comment = before[before.rfind("/*"):before.rfind("*/")]
+        text = " ".join(comment.replace("*", " ").split())
+        assert re.search(r"\.py:\d+|:\d+-\d+|no reference counterpart", text, re.I), m.group(1)
