@@ -88,10 +88,10 @@ def perturbed_sphere(subdiv: int, lmax: int = 6, amplitude: float = 0.05, seed: 
 
 
 def load_obj(path: str, normalise: bool = True):
-    """Read `v`/`f` records (polygons fan-triangulated, 1-based indices,
-    `a/b/c` forms accepted).  With normalise=True the mesh is centred on the
-    vertex mean and scaled by 1/max|coordinate| as the reference's
-    MeshManager.load_asset does (mesh_manager.py:479-494)."""
+    """Read `v`/`f` records (polygons fan-triangulated, 1-based or negative
+    relative indices, `a/b/c` forms accepted).  With normalise=True the mesh
+    is centred on the vertex mean and scaled by 1/max|coordinate| as the
+    reference's MeshManager.load_asset does (mesh_manager.py:479-494)."""
     verts, faces = [], []
     with open(path) as fh:
         for line in fh:
@@ -101,7 +101,9 @@ def load_obj(path: str, normalise: bool = True):
             if parts[0] == "v":
                 verts.append([float(p) for p in parts[1:4]])
             elif parts[0] == "f":
-                idx = [int(p.split("/")[0]) - 1 for p in parts[1:]]
+                # 1-based, or negative: relative to the vertices read so far
+                idx = [int(p.split("/")[0]) for p in parts[1:]]
+                idx = [i - 1 if i > 0 else len(verts) + i for i in idx]
                 for t in range(1, len(idx) - 1):
                     faces.append([idx[0], idx[t], idx[t + 1]])
     v = np.array(verts, dtype=np.float64)

@@ -106,3 +106,18 @@ def test_bad_mesh_is_rejected_on_the_host(case):
         f = f[:, :2]
     with pytest.raises(ValueError):
         _mesh_manager(vertices=v, panels=f)
+
+
+def test_obj_reader_forms(tmp_path):
+    """`a/b/c` vertex references, negative (relative) indices and polygons,
+    fan-triangulated from their first vertex."""
+    from bem_b200.meshes import load_obj
+    text = ("v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nvn 0 0 1\nvt 0 0\n"
+            "f 1/1/1 2/1/1 3/1/1\n"      # slash forms
+            "f -4 -2 -1\n"               # relative: vertices 1, 3, 4
+            "f 1 2 3 4\n")               # quad -> (1,2,3), (1,3,4)
+    path = tmp_path / "forms.obj"
+    path.write_text(text)
+    v, f = load_obj(str(path), normalise=False)
+    assert v.shape == (4, 3)
+    assert f.tolist() == [[0, 1, 2], [0, 2, 3], [0, 1, 2], [0, 2, 3]]
