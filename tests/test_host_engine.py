@@ -41,3 +41,16 @@ def test_upload_keeps_values_and_casts():
     assert f.dtype == torch.float64 and f.tolist() == [1.5, 2.5]
     c = upload(np.array([1 + 2j]), "cpu")
     assert c.dtype == torch.complex128 and complex(c[0]) == 1 + 2j
+
+
+def test_complex_pack_round_trip():
+    """warp_tensor / unwarp_tensor (src/BEM_functions/utils/io.py:4-30):
+    [..., 2] <-> complex, [..., 1] <-> real, anything else rejected."""
+    from bem_b200.utils.io import unwarp_tensor, warp_tensor
+    z = torch.randn(5, 3, dtype=torch.complex128)
+    packed = unwarp_tensor(z)
+    assert packed.shape == (5, 3, 2) and torch.equal(warp_tensor(packed), z)
+    r = torch.randn(4, dtype=torch.float64)
+    assert unwarp_tensor(r).shape == (4, 1) and torch.equal(warp_tensor(unwarp_tensor(r)), r)
+    with pytest.raises(NotImplementedError):
+        warp_tensor(torch.zeros(2, 3))
