@@ -110,3 +110,34 @@ def test_reference_quadrature_trace_does_not_converge():
     from their analytic traces)."""
     err = [_point_source_trace_error(s, quirk=True) for s in (1, 2)]
     assert min(err) > 0.3
+
+
+def _apply_2d(N, op, helm, k, R=0.5, Q=4):
+    from bem_b200.meshes import analytical_disk
+    from oracle import oracle2d as O2
+    v, f = analytical_disk(R, N)
+    L = np.linalg.norm(v[f[:, 1]] - v[f[:, 0]], axis=1)
+    p0 = (np.arange(N, dtype=np.int32), 1, np.arange(N, dtype=np.int32))
+    y = np.zeros(N, complex if helm else float)
+    O2.assemble(v, f, {"V": O2.OP_V, "K": O2.OP_K}[op], helm, k, k * k, Q, p0, p0, x=np.ones(N, y.dtype), y=y)
+    return y / L
+
+
+def test_2d_single_layer_of_a_constant_on_a_circle():
+    """On the circle of radius R the single layer of 1 is -R log R (Laplace,
+    G = -log r / 2 pi) and (i pi R / 2) J_0(kR) H_0(kR) (Helmholtz,
+    G = (i/4) H_0(k r))."""
+    from scipy import special
+    R, k = 0.5, 2.0
+    lap = [np.abs(_apply_2d(N, "V", False, 0.0, R) + R * np.log(R)).max() / abs(R * np.log(R)) for N in (32, 64, 128)]
+    assert max(lap) < 2e-3
+    want = 0.5j * np.pi * R * special.jv(0, k * R) * special.hankel1(0, k * R)
+    helm = [np.abs(_apply_2d(N, "V", True, k, R) - want).max() / abs(want) for N in (32, 64, 128)]
+    assert helm[2] < 2e-4 and helm[0] / helm[1] > 3 and helm[1] / helm[2] > 3  # O(h^2)
+
+
+def test_2d_gauss_law_for_the_double_layer():
+    """K 1 = -1/2 on a closed polygon, to first order: the reference's scheme
+    integrates vertex-sharing segment pairs with the plain Q^2 rule."""
+    err = [np.abs(_apply_2d(N, "K", False, 0.0) + 0.5).max() for N in (32, 64, 128)]
+    assert err[2] < 4e-4 and err[0] / err[1] > 1.8 and err[1] / err[2] > 1.8
