@@ -141,3 +141,28 @@ def test_2d_gauss_law_for_the_double_layer():
     integrates vertex-sharing segment pairs with the plain Q^2 rule."""
     err = [np.abs(_apply_2d(N, "K", False, 0.0) + 0.5).max() for N in (32, 64, 128)]
     assert err[2] < 4e-4 and err[0] / err[1] > 1.8 and err[1] / err[2] > 1.8
+
+
+def test_hypersingular_of_a_constant_on_the_sphere():
+    """W 1 with P1 bases: the surface curls of a constant vanish, so Laplace
+    W 1 = 0 exactly and Helmholtz W 1 = -k^2 int G n_x.n_y dS, which on the
+    unit sphere (n_x.n_y = 1 - r^2/2, dS = 2 pi r dr) is
+    -k^2 (1/2 int_0^2 e^{ikr} dr - 1/4 int_0^2 r^2 e^{ikr} dr)."""
+    from scipy import integrate
+    k = 1.5
+    quad = lambda g: integrate.quad(lambda r: g(r) * np.cos(k * r), 0, 2)[0] + \
+        1j * integrate.quad(lambda r: g(r) * np.sin(k * r), 0, 2)[0]
+    want = -k * k * (0.5 * quad(lambda r: 1.0) - 0.25 * quad(lambda r: r * r))
+    err = []
+    for s in (2, 3):
+        v, f = icosphere(s)
+        nt, nv = len(f), len(v)
+        va = np.bincount(f.reshape(-1), weights=np.repeat(_areas(v, f) / 3.0, 3), minlength=nv)
+        p1 = (np.arange(nt, dtype=np.int32), 3, f.reshape(-1).astype(np.int32))
+        lap = np.zeros(nv)
+        O.assemble(v, f, O.OP_W, 0, 0.0, 0.0, 3, 0, p1, p1, x=np.ones(nv), y=lap)
+        assert np.abs(lap).max() < 1e-14
+        y = np.zeros(nv, complex)
+        O.assemble(v, f, O.OP_W, 1, k, k * k, 3, 0, p1, p1, x=np.ones(nv, complex), y=y)
+        err.append(np.abs(y / va - want).max() / abs(want))
+    assert err[1] < 7e-3 and err[0] / err[1] > 3.5  # O(h^2)
