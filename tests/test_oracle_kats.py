@@ -166,3 +166,25 @@ def test_hypersingular_of_a_constant_on_the_sphere():
         O.assemble(v, f, O.OP_W, 1, k, k * k, 3, 0, p1, p1, x=np.ones(nv, complex), y=y)
         err.append(np.abs(y / va - want).max() / abs(want))
     assert err[1] < 7e-3 and err[0] / err[1] > 3.5  # O(h^2)
+
+
+def test_double_layer_and_its_adjoint_of_a_constant_on_the_sphere():
+    """On the unit sphere (x - y).n_y = (y - x).n_x = -r^2/2, so K 1 and K' 1
+    share the closed form -1/4 int_0^2 (1 - ikr) e^{ikr} dr (-1/2 at k = 0).
+    K' takes the flat panel's normal at the test point, so unlike K it has no
+    exact solid-angle identity on a polyhedron and converges to first order
+    for Laplace."""
+    from scipy import integrate
+    k = 1.5
+    quad = lambda g: integrate.quad(lambda r: (g(r) * np.exp(1j * k * r)).real, 0, 2)[0] + \
+        1j * integrate.quad(lambda r: (g(r) * np.exp(1j * k * r)).imag, 0, 2)[0]
+    want = -0.25 * quad(lambda r: 1 - 1j * k * r)
+    err = {}
+    for s in (2, 3):
+        v, f = icosphere(s)
+        err[("K", s)] = np.abs(_apply(v, f, O.OP_K, True, k, quirk=0) - want).max() / abs(want)
+        err[("KP", s)] = np.abs(_apply(v, f, O.OP_KP, True, k, quirk=0) - want).max() / abs(want)
+        err[("KPL", s)] = np.abs(_apply(v, f, O.OP_KP, False, 0.0, quirk=0) + 0.5).max() / 0.5
+    assert err[("K", 3)] < 6e-3 and err[("K", 2)] / err[("K", 3)] > 3.5
+    assert err[("KP", 3)] < 9e-3 and err[("KP", 2)] / err[("KP", 3)] > 2.5
+    assert err[("KPL", 3)] < 8e-3 and err[("KPL", 2)] / err[("KPL", 3)] > 1.5
