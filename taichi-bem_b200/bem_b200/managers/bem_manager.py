@@ -14,8 +14,9 @@ Extra simulation_parameters keys (all optional):
              or "mixed" (separate pairs in FP32, near field in FP64, FP32 LU
              with FP64 iterative refinement against the FP64-stored matrix)
   quirk:     True (default) reproduces the reference's quadrature exactly;
-             False uses the corrected Sauter-Schwab orientation and g (not
-             conj g) in the Helmholtz right-hand side
+             False uses the corrected Sauter-Schwab orientation, g (not
+             conj g) in the Helmholtz right-hand side, and honours the
+             `show` parameter (which the reference's own code ignores)
   solver:    "lstsq" (transmission default, the reference's least squares on
              [A; P+_i] via normal equations) or "lu" (square A)
   refine_tol / refine_maxit: iterative-refinement controls of the mixed path
@@ -54,8 +55,14 @@ class BEMManager:
         show = p.get("show", "Default")
         if show not in ("Neumann", "Dirichlet", "Default"):
             raise RuntimeError("The supported type for visualization is only Neumann/Dirichlet/Default")
-        self._show = {"Neumann": int(VertAttachType.NEUMANN_TOBESOLVED),
-                      "Dirichlet": int(VertAttachType.DIRICHLET_TOBESOLVED), "Default": -1}[show]
+        self.quirk = bool(p.get("quirk", True))
+        self.show = {"Neumann": int(VertAttachType.NEUMANN_TOBESOLVED),
+                     "Dirichlet": int(VertAttachType.DIRICHLET_TOBESOLVED), "Default": -1}[show]
+        # The reference stores the parameter in `show` and reads `_show`, which
+        # stays -1 (BEM_manager.py:28,43-50): the parameter has no effect on
+        # the splat and the colouring.  quirk=True reproduces that; quirk=False
+        # honours the parameter.
+        self._show = -1 if self.quirk else self.show
         if self._show == -1 and self._is_transmission:
             self._show = int(VertAttachType.NEUMANN_TOBESOLVED)
         self._k = float(p.get("k", 0.0)) if self._n == 2 else 0.0
@@ -76,7 +83,6 @@ class BEMManager:
         # precision of the dense solve ("fp64": partial-pivoting LU; "mixed":
         # FP32 tile LU + FP64 refinement), by default the assembly's
         self.solve_precision = p.get("solve_precision", self.precision)
-        self.quirk = bool(p.get("quirk", True))
         # one sweep for V and K g in the Dirichlet problem (the plain path keeps
         # one kernel per operator)
         self.fuse = bool(p.get("fuse", self.precision == "mixed"))

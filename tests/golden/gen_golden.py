@@ -165,6 +165,9 @@ CASES = {
                                              GaussQR=3, k=3.0, Q_Neumann=1), "plane_wave"),
     "disk256_lap_dir_q3": ("disk256", dict(dim=2, kernel="Laplace", boundary="Dirichlet", scope="Interior",
                                            GaussQR=3), "laplace_2d"),
+    # the colouring's show = "Dirichlet" branch (every vertex shifted)
+    "disk32_lap_mix_showD_q3": ("disk32", dict(dim=2, kernel="Laplace", boundary="Mix", scope="Interior",
+                                               GaussQR=3, show="Dirichlet"), "laplace_2d"),
 }
 
 

@@ -121,3 +121,21 @@ def test_obj_reader_forms(tmp_path):
     v, f = load_obj(str(path), normalise=False)
     assert v.shape == (4, 3)
     assert f.tolist() == [[0, 1, 2], [0, 2, 3], [0, 1, 2], [0, 2, 3]]
+
+
+@pytest.mark.parametrize("show,quirk,transmission,want", [
+    ("Dirichlet", True, False, -1),   # the reference reads _show, never set from the parameter
+    ("Neumann", True, False, -1),
+    ("Default", True, True, 0),       # transmission: Neumann (BEM_manager.py:52-53)
+    ("Dirichlet", False, False, 1),   # corrected mode honours the parameter
+    ("Neumann", False, False, 0),
+    ("Dirichlet", False, True, 1),
+])
+def test_show_parameter_follows_the_reference(show, quirk, transmission, want):
+    from bem_b200.managers import CoreManager
+    p = dict(dim=3, object="icosphere1", GaussQR=3, scope="Interior", show=show, quirk=quirk,
+             kernel="Helmholtz_Transmission" if transmission else "Laplace",
+             boundary="Full" if transmission else "Dirichlet", k=1.0, n_i=1.0, n_o=1.0)
+    b = CoreManager(p)._BEM_manager
+    assert b._show == want
+    assert b.show == {"Neumann": 0, "Dirichlet": 1, "Default": -1}[show]
