@@ -206,9 +206,15 @@ int64_t bem_lu_dinv_elems(int64_t n);
  * BEM_manager.py:1056).  Queued without synchronisation.  A tensor-core wait
  * of the trailing updates
  * that ran out of its iteration cap is reported (BEM_ERR_TIMEOUT) by the next
- * bem_lu_solve_tiled or bem_refine_solve on the same context. */
+ * bem_lu_solve_tiled, bem_refine_solve or bem_lu_factor_status on the same
+ * context. */
 int bem_lu_factor_tiled(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, void* dinv,
                         int32_t* info, void* stream);
+/* Status of the last bem_lu_factor_tiled on ctx (no reference counterpart):
+ * synchronises the stream and returns BEM_ERR_TIMEOUT if a tensor-core wait of
+ * that factorisation ran out of its iteration cap (the factors are then not
+ * valid), else BEM_OK.  Reading the status clears it. */
+int bem_lu_factor_status(bem_ctx* ctx, void* stream);
 /* The solve half of torch.linalg.solve (BEM_manager.py:1056):
  * x = U^{-1} L^{-1} P b for one FP64 right-hand side b (overwritten), with the
  * factors of bem_lu_factor_tiled; a persistent kernel driven by per-tile ready
@@ -226,11 +232,18 @@ int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64
  * (about 0.65 MB, held by every GPU that loads the library until the process
  * exits); larger n is rejected with BEM_ERR_INVALID.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current; make that first call before any stream capture.  All calls
+ * device current and caches it per device ordinal, i.e. for the runtime's
+ * primary context of that device; a caller that switches the current device
+ * between driver-API contexts of one device is not supported.  All calls
  * share the one array, so calls that overlap on the GPU (other streams, other
- * host threads) race; serialise them.  Same arguments and result as
- * bem_lu_solve_tiled; returns BEM_OK, BEM_ERR_INVALID, BEM_ERR_CUDA or
- * BEM_ERR_TIMEOUT. */
+ * host threads) race; serialise them.  Every call synchronises the stream (it
+ * reads its wait status back to the host).  Same arguments as
+ * bem_lu_solve_tiled without the context.  Unlike bem_lu_solve_tiled it
+ * cannot see the factorisation's own status, which lives in the context: a
+ * factor whose tensor-core wait timed out is not reported here, so check
+ * bem_lu_factor_status on the factor's context before the first solve with a
+ * new factor.  Returns BEM_OK, BEM_ERR_INVALID, BEM_ERR_CUDA or
+ * BEM_ERR_TIMEOUT (a wait of this solve ran out). */
 #define BEM_STATIC_SOLVE_MAX_N 32768
 int bem_lu_solve_tiled_static(int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                               const void* dinv, void* b, void* stream);
@@ -292,6 +305,10 @@ int bem_set_mesh_instances(bem_ctx* ctx, float* solved_vertices, float* exact_ve
  * out[0] = FP32 FMA TFLOP/s, out[1] = FP64 FMA TFLOP/s, out[2] = MUFU (rsqrt)
  * Gop/s.  Synchronous; allocates a small buffer. */
 int bem_measure_peaks(bem_ctx* ctx, double* out, void* stream);
+/* No reference counterpart.  *version = the binary architecture (major*10 +
+ * minor, cudaFuncGetAttributes' binaryVersion) of this library's device code
+ * as loaded on the current device: 100 for the sm_100a build.  Needs a GPU. */
+int bem_binary_version(int* version);
 
 #ifdef __cplusplus
 }

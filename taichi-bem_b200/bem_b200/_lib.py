@@ -35,6 +35,7 @@ EXPORTS = [
     "bem_lu_solve", "bem_gemv", "bem_refine_solve", "bem_measure_peaks", "bem_lu_dinv_elems",
     "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet", "bem_lu_solve_tiled_static",
     "bem_adjoint_vertices", "bem_mesh_set_2d", "bem_gmres_ir", "bem_compute_color", "bem_set_mesh_instances",
+    "bem_lu_factor_status", "bem_binary_version",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 
@@ -99,6 +100,8 @@ def load():
     L.bem_lu_dinv_elems.restype = i64
     L.bem_lu_factor_tiled.argtypes = [vp, i32, vp, i64, i64, vp, vp, vp, vp]
     L.bem_lu_solve_tiled.argtypes = [vp, i32, vp, i64, i64, vp, vp, vp, vp]
+    L.bem_lu_factor_status.argtypes = [vp, vp]
+    L.bem_binary_version.argtypes = [ctypes.POINTER(ctypes.c_int)]
     L.bem_measure_peaks.argtypes = [vp, ctypes.POINTER(ctypes.c_double), vp]
     L.bem_compute_color.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp]
     L.bem_set_mesh_instances.argtypes = [vp, vp, vp, vp, vp]

@@ -14,9 +14,10 @@ Extra simulation_parameters keys (all optional):
              or "mixed" (separate pairs in FP32, near field in FP64, FP32 LU
              with FP64 iterative refinement against the FP64-stored matrix)
   quirk:     True (default) reproduces the reference's quadrature exactly;
-             False uses the corrected Sauter-Schwab orientation, g (not
-             conj g) in the Helmholtz right-hand side, and honours the
-             `show` parameter (which the reference's own code ignores)
+             False uses the corrected Sauter-Schwab orientation and g (not
+             conj g) in the Helmholtz right-hand side
+  honour_show: whether the `show` parameter selects the splat and colouring
+             (the reference's own code ignores it); default: not quirk
   solver:    "lstsq" (transmission default, the reference's least squares on
              [A; P+_i] via normal equations) or "lu" (square A)
   refine_tol / refine_maxit: iterative-refinement controls of the mixed path
@@ -60,9 +61,11 @@ class BEMManager:
                      "Dirichlet": int(VertAttachType.DIRICHLET_TOBESOLVED), "Default": -1}[show]
         # The reference stores the parameter in `show` and reads `_show`, which
         # stays -1 (BEM_manager.py:28,43-50): the parameter has no effect on
-        # the splat and the colouring.  quirk=True reproduces that; quirk=False
-        # honours the parameter.
-        self._show = -1 if self.quirk else self.show
+        # the splat and the colouring.  honour_show=False reproduces that;
+        # honour_show=True applies the parameter.  By default it follows quirk
+        # (reference behaviour with the reference quadrature).
+        self.honour_show = bool(p.get("honour_show", not self.quirk))
+        self._show = self.show if self.honour_show else -1
         if self._show == -1 and self._is_transmission:
             self._show = int(VertAttachType.NEUMANN_TOBESOLVED)
         self._k = float(p.get("k", 0.0)) if self._n == 2 else 0.0

@@ -9,8 +9,7 @@ def warp_tensor(x: torch.Tensor):
     if n_ == 2:
         return torch.complex(x[..., 0], x[..., 1])
     raise NotImplementedError(
-        "A Tensor with shape = (*, {}) can not be warped, we only support 1 (Scalar) or 2 (Complex) for the last dim"
-        .format(n_))
+        f"warp_tensor: last dimension {n_} is neither 1 (real values) nor 2 (interleaved complex pairs)")
 
 
 def unwarp_tensor(x: torch.Tensor):

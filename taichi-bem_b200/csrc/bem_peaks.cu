@@ -72,3 +72,18 @@ extern "C" int bem_measure_peaks(bem_ctx* ctx, double* out, void* stream) {
     out[2] = fmas / (msmu * 1e-3) / 1e9;         // MUFU (rsqrt) Gop/s
     return BEM_OK;
 }
+
+// Architecture of the device code this library runs on the current device:
+// the binaryVersion (major*10 + minor) of one of its kernels, as the runtime
+// reports it after loading the module.  100 for the sm_100a build.
+extern "C" int bem_binary_version(int* version) {
+    if (!version) return BEM_ERR_INVALID;
+    cudaFuncAttributes attr;
+    cudaError_t e = cudaFuncGetAttributes(&attr, mufu_probe);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    *version = attr.binaryVersion;
+    return BEM_OK;
+}

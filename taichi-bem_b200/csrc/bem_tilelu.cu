@@ -975,6 +975,17 @@ int precond_t(bem_ctx* ctx, const T* LU, int64_t n, int64_t lda, const int32_t* 
 
 extern "C" {
 
+int bem_lu_factor_status(bem_ctx* ctx, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    int32_t e = 0;
+    if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(&e, ctx->flags + 4, sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                                "factor status"))
+        return rc;
+    if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "factor status")) return rc;
+    return bem_take_factor_error(ctx, e, s);
+}
+
 int64_t bem_lu_dinv_elems(int64_t n) { return ((n + LU_T - 1) / LU_T) * 2 * LU_T * LU_T; }
 
 int bem_lu_factor_tiled(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, void* dinv,
@@ -1090,6 +1101,7 @@ int solve_static_t(const T* LU, int64_t n, int64_t lda, const int32_t* piv, cons
     double* x = sc->x;
     tile_piv_to_perm_kernel<<<(unsigned)((nbk + 127) / 128), 128, 0, s>>>(piv, perm, (int)n);
     permute_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, perm, x, (int)n, W);
+    if (cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;
     // the array keeps the previous call's contents: the flags and the error
     // word must start at zero
     if (cudaMemsetAsync(flags, 0, sizeof(int) * 2 * nbk, s) != cudaSuccess ||

@@ -12,7 +12,7 @@ including the two GUI kernels at its end (``compute_color``, which shifts
 
 Usage (in a container that has the reference checkout):
 
-    python tests/golden/gen_golden.py --ref /root/reference [--only NAME] [--colour-only] [--meshes]
+    python tests/golden/gen_golden.py --ref <path of the reference checkout> [--only NAME] [--colour-only] [--meshes]
 
 Writes ``tests/golden/<case>.npz``.  Every array needed to re-run a case
 (vertices after the reference's own normalisation, panels, BVP maps, Gauss
@@ -356,7 +356,7 @@ def mesh_fixture(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="path of the reference checkout (its src/ is imported)")
     ap.add_argument("--only", default=None)
     ap.add_argument("--meshes", action="store_true",
                     help="only write the analytic-mesh fixture from the reference's generators")

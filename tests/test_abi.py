@@ -21,9 +21,13 @@ def test_header_and_library_agree():
         assert hasattr(lib, n), n
 
 
-def test_library_is_sm100a():
-    from bem_b200 import _lib
-    assert os.path.getsize(_lib.LIB_PATH) > 0
+def test_build_targets_sm100a_only():
+    """The library's only device target is sm_100a (the Makefile's -gencode);
+    the GPU side of this check is tests/test_linalg_gpu.py's binary-version
+    query."""
+    mk = open(os.path.join(ROOT, "taichi-bem_b200", "Makefile")).read()
+    arches = re.findall(r"arch=(compute_\w+),code=(sm_\w+)", mk)
+    assert arches == [("compute_100a", "sm_100a")], arches
 
 
 def test_every_entry_point_cites_what_it_replaces():

@@ -54,3 +54,21 @@ def test_complex_pack_round_trip():
     assert unwarp_tensor(r).shape == (4, 1) and torch.equal(warp_tensor(unwarp_tensor(r)), r)
     with pytest.raises(NotImplementedError):
         warp_tensor(torch.zeros(2, 3))
+
+
+@pytest.mark.parametrize("quirk,honour,show,want", [
+    (True, None, "Dirichlet", -1),    # reference behaviour: the parameter is stored, not read
+    (False, None, "Dirichlet", 1),    # default follows quirk
+    (True, True, "Neumann", 0),       # reference quadrature, show honoured
+    (False, False, "Neumann", -1),    # corrected quadrature, reference colouring
+])
+def test_show_parameter_is_its_own_switch(quirk, honour, show, want):
+    """`honour_show` decides whether `show` selects the splat and colouring,
+    independently of the quadrature quirk flag (BEM_manager.py:28,43-50)."""
+    from bem_b200.managers import CoreManager
+    p = dict(dim=3, object="icosphere1", GaussQR=3, kernel="Laplace", boundary="Dirichlet", scope="Interior",
+             show=show, quirk=quirk, device="cpu")
+    if honour is not None:
+        p["honour_show"] = honour
+    b = CoreManager(p)._BEM_manager
+    assert b._show == want

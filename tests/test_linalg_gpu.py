@@ -195,3 +195,29 @@ def test_gmres_ir(engine, cplx, tiled):
         engine.gmres_solve(A_hi, LU, piv, bd, torch.zeros_like(bd), tol=1e-15, maxit=1, restart=1, dinv=dinv,
                            accept=0.0)
     assert exc.value.code == -4
+
+
+def test_device_code_is_sm100a():
+    """The device code the runtime loaded is the sm_100a build (binaryVersion 100)."""
+    import ctypes
+    from bem_b200 import _lib
+    L = _lib.load()
+    torch.zeros(1, device="cuda")
+    v = ctypes.c_int(0)
+    assert L.bem_binary_version(ctypes.byref(v)) == 0
+    assert v.value == 100
+
+
+def test_factor_status_after_tiled_factor(engine):
+    """bem_lu_factor_status reads (and clears) the tiled factorisation's
+    tensor-core wait status: BEM_OK for a factor that completed."""
+    from bem_b200 import _lib
+    n = 256
+    A = torch.as_tensor(_mat(n, True, 5), dtype=torch.complex64, device="cuda")
+    engine.lu_factor_tiled(A)
+    L = _lib.load()
+    assert L.bem_lu_factor_status(engine.ctx, ctypes_stream()) == 0
+
+
+def ctypes_stream():
+    return torch.cuda.current_stream().cuda_stream
