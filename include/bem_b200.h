@@ -91,6 +91,14 @@ const char* bem_last_error(const bem_ctx* ctx);
 /* Number of kernels this library launched through ctx since creation (no
  * reference counterpart). */
 int64_t bem_launch_count(const bem_ctx* ctx);
+/* Launch-shape choices of this context (no reference counterpart), set by the
+ * autotuner (bem_b200/tuning.py) after timing the candidates on this GPU;
+ * value 0 restores the built-in default.  Keys:
+ *   BEM_TUNE_CALDERON_GROUP  wavenumbers per launch of the fused Calderon
+ *                            sweep (1 or 2) */
+#define BEM_TUNE_CALDERON_GROUP 0
+#define BEM_TUNE_KEYS 8
+int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value);
 
 /* ---- mesh ------------------------------------------------------------------
  * Replaces MeshManager.initialization geometry (mesh_manager.py:84-139) and the
@@ -133,6 +141,26 @@ int bem_mesh_geometry(const bem_ctx* ctx, double* areas, double* normals, void* 
 int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                  int out_dtype, void* out, int64_t ld, double scale, void* out_t, double scale_t,
                  void* stream);
+
+/* Fused Calderon-block assembly of the transmission operator.  For each
+ * wavenumber w < nk (nk = 1 or 2; kernel wavenumber k[w], W mass coefficient
+ * k2[w]) adds to out[w] (BEM_F64 for Laplace or BEM_C128, row-major, ld) the
+ * block operator c = coef[w] times M(k) = [K -V; -W -K'] with the reference's
+ * placement (matA_add_M, BEM_manager.py:608-628):
+ *   out_NN += -c V,  out_ND += c K,  out_DN += -c K^T,  out_DD += -c W,
+ * rows and columns given by the dof tables of `neu` (P0, nb = 1) and `dir`
+ * (P1, nb = 3), two spaces over the same panel list.  Replaces
+ * matrix_layer_forward (BEM_manager.py:829-844: SingleLayer3d.forward,
+ * DoubleLayer3d.forward, HypersingularLayer3d.forward, one Taichi kernel per
+ * operator and scope) followed by assemble_matA(ADD_P_MINUS / ADD_P_PLUS)
+ * without the identity term (bem_mass adds that).  Separate pairs run in ONE
+ * sweep over unordered panel pairs whose point evaluations serve V, K, K^T
+ * and W; near pairs take the FP64 Sauter-Schwab kernels.  op gives kernel,
+ * precision and quirk (op->op is ignored).  3D only; queued without
+ * synchronising. */
+int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk, const double* k, const double* k2,
+                          const bem_space* neu, const bem_space* dir, void* const* out, const double* coef,
+                          int64_t ld, void* stream);
 
 /* Matrix-free apply: y[row] += scale * sum_col A(row,col) * x[col]
  * (x conjugated when conj_x != 0, the reference's cmul(integrand, cconj(g))).

@@ -35,9 +35,10 @@ EXPORTS = [
     "bem_lu_solve", "bem_gemv", "bem_refine_solve", "bem_measure_peaks", "bem_lu_dinv_elems",
     "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet", "bem_lu_solve_tiled_static",
     "bem_adjoint_vertices", "bem_mesh_set_2d", "bem_gmres_ir", "bem_compute_color", "bem_set_mesh_instances",
-    "bem_lu_factor_status", "bem_binary_version",
+    "bem_lu_factor_status", "bem_binary_version", "bem_ctx_set_tuning", "bem_assemble_calderon",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
+TUNE_CALDERON_GROUP = 0  # BEM_TUNE_CALDERON_GROUP
 
 
 class BemError(RuntimeError):
@@ -102,6 +103,10 @@ def load():
     L.bem_lu_solve_tiled.argtypes = [vp, i32, vp, i64, i64, vp, vp, vp, vp]
     L.bem_lu_factor_status.argtypes = [vp, vp]
     L.bem_binary_version.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    L.bem_ctx_set_tuning.argtypes = [vp, i32, i32]
+    L.bem_assemble_calderon.argtypes = [vp, ctypes.POINTER(OpDesc), i32, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Space), ctypes.POINTER(Space),
+                                        ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_double), i64, vp]
     L.bem_measure_peaks.argtypes = [vp, ctypes.POINTER(ctypes.c_double), vp]
     L.bem_compute_color.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp]
     L.bem_set_mesh_instances.argtypes = [vp, vp, vp, vp, vp]

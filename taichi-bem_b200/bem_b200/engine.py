@@ -195,6 +195,30 @@ class Engine:
                                                     ctypes.byref(ds), _ptr(g), _ptr(y), float(scale_k),
                                                     int(bool(conj_g)), _stream_ptr()))
 
+    def assemble_calderon(self, desc: L.OpDesc, ks, k2s, neu: DeviceSpace, dir_: DeviceSpace, outs, coefs):
+        """outs[w] += coefs[w] * [K -V; -W -K'](ks[w]) with the reference's
+        block placement (bem_assemble_calderon): one sweep over the unordered
+        separate panel pairs serves V, K, K^T and W of every wavenumber."""
+        nk = len(ks)
+        assert 1 <= nk <= 2 and len(k2s) == nk == len(outs) == len(coefs)
+        o0 = outs[0]
+        for o in outs:
+            assert o.is_cuda and o.dim() == 2 and o.stride(1) == 1 and o.dtype == o0.dtype
+            assert o.stride(0) == o0.stride(0) and o.shape == o0.shape
+        self._check_spaces(neu, neu, o0.shape[0], o0.shape[1])
+        self._check_spaces(dir_, dir_, o0.shape[0], o0.shape[1])
+        kk = (ctypes.c_double * nk)(*[float(v) for v in ks])
+        k2 = (ctypes.c_double * nk)(*[float(v) for v in k2s])
+        cf = (ctypes.c_double * nk)(*[float(v) for v in coefs])
+        po = (ctypes.c_void_p * nk)(*[o.data_ptr() for o in outs])
+        ns, ds = neu.c(), dir_.c()
+        self._check(self.lib.bem_assemble_calderon(self.ctx, ctypes.byref(desc), nk, kk, k2, ctypes.byref(ns),
+                                                   ctypes.byref(ds), po, cf, o0.stride(0), _stream_ptr()))
+
+    def set_tuning(self, key: int, value: int):
+        """A launch-shape choice of this context (bem_ctx_set_tuning)."""
+        self._check(self.lib.bem_ctx_set_tuning(self.ctx, int(key), int(value)))
+
     def adjoint_vertices(self, desc: L.OpDesc, test: DeviceSpace, trial: DeviceSpace, lam: torch.Tensor,
                          u: torch.Tensor, grad: torch.Tensor):
         """grad [nv, 3] += d/dX sum lam[r] A(r, c) u[c] (Laplace V or K, FP64)."""

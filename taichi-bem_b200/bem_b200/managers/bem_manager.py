@@ -90,6 +90,11 @@ class BEMManager:
         # one kernel per operator)
         self.fuse = bool(p.get("fuse", self.precision == "mixed"))
         self.solver = p.get("solver", "lstsq" if self._is_transmission else "lu")
+        # transmission: V, K, K^T and W of both scopes from one sweep over the
+        # unordered panel pairs (bem_assemble_calderon) straight into _mat_A
+        # and _mat_P, instead of one kernel per operator and scope
+        self.fuse_calderon = bool(p.get("fuse_calderon", True))
+        self._mat_P = None
         # relative residual at which FP64 refinement stops: 1e-9 in mixed
         # precision (its contribution to the solution error is at most
         # cond(A) * 1e-9, ~1e-7 for cond(A) ~ 1e2, the order of the FP32
@@ -392,10 +397,13 @@ class BEMManager:
         n = self.N_Neumann + self.M_Dirichlet
         if self._is_transmission:
             # the reference stacks [A; P+_i] and calls lstsq (BEM_manager.py:1039-1050)
-            A_top = self._mat_A.clone()
-            self._mat_A.zero_()
-            self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
-            P = self._mat_A.clone()
+            if self._mat_P is not None and self._calderon_fusable():
+                A_top, P = self._mat_A, self._mat_P
+            else:
+                A_top = self._mat_A.clone()
+                self._mat_A.zero_()
+                self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
+                P = self._mat_A.clone()
             if self.solver == "lstsq":
                 # normal equations of the stacked system: (A^H A + P^H P) x = A^H b_top
                 AH = A_top.conj().transpose(0, 1)
@@ -404,7 +412,8 @@ class BEMManager:
                 sol = self._lu_solve_square(Mn, bn)
             else:
                 sol = self._lu_solve_square(A_top.contiguous(), self.rhs[:n].contiguous())
-            self._mat_A.copy_(A_top)
+            if A_top is not self._mat_A:
+                self._mat_A.copy_(A_top)
         else:
             sol = self._lu_solve_square(self._mat_A, self.rhs)
         self.raw_solved.copy_(sol)
@@ -714,11 +723,57 @@ class BEMManager:
         self.compute_color()
         self.set_mesh_instances()
 
+    def _calderon_fusable(self) -> bool:
+        """Transmission with P0 Neumann and P1 Dirichlet unknowns on one
+        panel loop: every operator block comes from the same panel pairs."""
+        if not (self.fuse_calderon and self._is_transmission and self._dim == 3 and self.N_Neumann > 0
+                and self.M_Dirichlet > 0 and self.shape_func_degree_Neumann == 0
+                and self.shape_func_degree_Dirichlet == 1):
+            return False
+        key = "calderon_fusable"
+        if key not in self._dev_cache:
+            mm = self.mesh
+            self._dev_cache[key] = bool(np.array_equal(mm.loop_panels("N"), mm.loop_panels("D")))
+        return self._dev_cache[key]
+
+    def _assemble_transmission_fused(self):
+        """matrix_layer_forward + assemble_matA(ADD_P_MINUS) at sqrt_no, the
+        right-hand side, then matrix_layer_forward + assemble_matA(ADD_P_PLUS)
+        at sqrt_ni (BEM_manager.py:995-1006), with the operators of both
+        scopes from one call: _mat_A receives P-_o = 1/2 M - M_o and _mat_P
+        receives P+_i = 1/2 M + M_i; rhs[:n] = P-_o conj(f), as the reference
+        forms it before the interior scope is added; then _mat_A += _mat_P."""
+        n = self.N_Neumann + self.M_Dirichlet
+        if self._mat_P is None:
+            self._mat_P = torch.zeros(n, n, dtype=self.torch_dtype, device=self.device)
+        else:
+            self._mat_P.zero_()
+        neu = self.space("charge", 0, "N", int(CellFluxType.NEUMANN_TOBESOLVED), offset=self._Neumann_offset_i)
+        dir_ = self.space("charge", 1, "D", int(CellFluxType.DIRICHLET_TOBESOLVED), offset=self._Dirichlet_offset_i)
+        desc = self.op_desc(L.OP_V, self._k, 1.0)
+        ks, k2s = [], []
+        for sqrt_n in (self._sqrt_no, self._sqrt_ni):
+            d = self.op_desc(L.OP_V, self._k, sqrt_n)
+            ks.append(d.k)
+            k2s.append(d.k2)
+        self.engine.assemble_calderon(desc, ks, k2s, neu, dir_, [self._mat_A, self._mat_P], [-1.0, 1.0])
+        # the identity parts of ADD_P_MINUS and ADD_P_PLUS (identity_layer_3d.py:148-196)
+        md = self.space("charge", 1, "D", int(CellFluxType.DIRICHLET_TOBESOLVED), offset=self._Dirichlet_offset_j)
+        for X in (self._mat_A, self._mat_P):
+            self.engine.mass(neu, md, out=X, scale=0.5, out_t=X, scale_t=0.5)
+        self.rhs_constructor.set_boundaries(scope_type=int(ScopeType.INTERIOR), sqrt_ni=self._sqrt_ni,
+                                            sqrt_no=self._sqrt_no)
+        self.assemble_rhs()
+        self._mat_A.add_(self._mat_P)
+        self.set_scope_type(int(ScopeType.INTERIOR))
+
     def assemble_system(self):
         """The part of `run` before the solve (BEM_manager.py:990-1018): the
         operator into _mat_A and the right-hand side into rhs, at self._k."""
         self._mat_A.zero_()
-        if self._is_transmission:
+        if self._is_transmission and self._calderon_fusable():
+            self._assemble_transmission_fused()
+        elif self._is_transmission:
             self.matrix_layer_forward(k=self._k, sqrt_n=self._sqrt_no, scope_type=int(ScopeType.EXTERIOR))
             self.assemble_matA(assemble_type=int(AssembleType.ADD_P_MINUS), multiplier=1.0)
             self.rhs_constructor.set_boundaries(scope_type=int(ScopeType.INTERIOR), sqrt_ni=self._sqrt_ni,
@@ -744,6 +799,7 @@ class BEMManager:
             if obj is not None:
                 obj.kill()
         self._mat_A = None
+        self._mat_P = None
         self.rhs = None
         self.raw_solved = None
         if getattr(self, "engine", None) is not None:

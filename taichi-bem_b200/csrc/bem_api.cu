@@ -166,6 +166,15 @@ int bem_lookahead_stream(bem_ctx* ctx) {
 
 extern "C" {
 
+int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (key < 0 || key >= BEM_TUNE_KEYS) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: unknown key");
+    if (key == BEM_TUNE_CALDERON_GROUP && value != 0 && value != 1 && value != 2)
+        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon group must be 1 or 2");
+    ctx->tune[key] = value;
+    return BEM_OK;
+}
+
 int bem_ctx_create(bem_ctx** out_ctx) {
     if (!out_ctx) return BEM_ERR_INVALID;
     *out_ctx = nullptr;

@@ -19,6 +19,7 @@ struct bem_ctx {
     int64_t launches = 0;
     int device = 0;
     int num_sms = 148;
+    int tune[BEM_TUNE_KEYS] = {0};  // launch-shape choices (bem_ctx_set_tuning); 0 = built-in default
 
     // ---- mesh (device) ----
     int dim = 3;                 // 3: triangles (bem_mesh_set), 2: segments (bem_mesh_set_2d)
@@ -74,6 +75,14 @@ int bem_lookahead_stream(bem_ctx* ctx);
 int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                         int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t, const void* x,
                         void* y, int conj_x, cudaStream_t s);
+// bem_launch_assemble restricted to the near-pair (coincident / edge / vertex)
+// kernel when near_only (the far pairs then come from a fused sweep).
+int bem_launch_assemble_parts(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                              int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t,
+                              const void* x, void* y, int conj_x, cudaStream_t s, bool near_only);
+// Class of the bound on the FP32 split phase |k (r - R)| <= k (rho_i + rho_j):
+// 2 when <= 0.3 (short polynomials), 1 when <= 0.78 < pi/4 (no reduction), 0 otherwise
+int bem_phase_class(double bound);
 int bem_launch_dirichlet(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                          void* out, int64_t ld, double scale, const bem_space* rows, const bem_space* data,
                          const void* g, void* y, double scale_k, int conj_g, cudaStream_t s);

@@ -25,7 +25,7 @@ def _run(d, **extra):
 @pytest.mark.parametrize("name", FIXTURES)
 def test_driver_matches_reference_fp64(name, fuse):
     d = load_fixture(name)
-    core, b = _run(d, fuse=fuse)
+    core, b = _run(d, fuse=fuse, fuse_calderon=fuse)
     b._mat_A.zero_()
     if "solve_error" in d:
         # the reference's torch.linalg.solve raised on this exactly singular system
