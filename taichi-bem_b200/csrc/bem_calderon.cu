@@ -454,8 +454,10 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
         a.out[w] = (double*)out[w];
     }
     a.ld = ld;
-    if (nk == 2 && ctx->tune[BEM_TUNE_CALDERON_GROUP] == 2) return dispatch_calderon<2>(ctx, a, fp32, helm, s);
-    // default: one wavenumber per launch (fewer registers, more resident warps)
+    // default: both wavenumbers in one launch (measured faster than one launch
+    // per wavenumber on the 20480-panel transmission problem: 652 vs 769 ms
+    // mixed, 1602 vs 1736 ms FP64); group 1 keeps one per launch
+    if (nk == 2 && ctx->tune[BEM_TUNE_CALDERON_GROUP] != 1) return dispatch_calderon<2>(ctx, a, fp32, helm, s);
     for (int w = 0; w < nk; ++w) {
         CalArgs b = a;
         b.k[0] = a.k[w];
