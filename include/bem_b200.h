@@ -307,6 +307,37 @@ int bem_gmres_ir(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo
                  const void* dinv, int64_t n, int64_t lda, const void* b, void* x, double tol, int maxit, int restart,
                  double accept, int* iters, double* relres, void* stream);
 
+/* ---- least squares of the transmission system ------------------------------------
+ * The reference solves the stacked system [A; P+_i] x = rhs (2n rows) with
+ * torch.linalg.lstsq (BEM_manager.py:1039-1050).  Here: the column-equilibrated
+ * normal equations N z = g, N = D (A^H A + P^H P) D, x = D z, with D the
+ * power-of-two column scaling of [A; P].
+ *
+ * Normal matrix (the Gram half of that lstsq call): colscale (device [n]
+ * doubles) receives D; out (n x n, ldo) receives the full Hermitian N.
+ * A, P: BEM_C128 (16-byte aligned) or BEM_F64, n x n, ld.  out_dtype
+ * BEM_C64 / BEM_F32 forms N on the tcgen05 tensor cores from FP16 hi/lo
+ * splits of the scaled columns (about 22 significant bits per product, FP32
+ * accumulation in segments of 4096 products; the FP16 split operands use a
+ * context workspace of 8 n^2 bytes); BEM_C128 / BEM_F64 forms it in FP64 on
+ * the FP64 tensor cores (DMMA).  Queued without synchronising; a tensor-core
+ * wait that runs out is reported by the next bem_lstsq_refine. */
+int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld, double* colscale,
+             int out_dtype, void* out, int64_t ldo, void* stream);
+/* The solve half of the same lstsq call (BEM_manager.py:1049): x (device, n,
+ * FP64 real or complex, holding the initial guess) is refined by flexible
+ * GMRES(restart) in FP64 on the scaled normal equations, with FP64 products
+ * against A and P and preconditioned by the tile-pivoted factors (LU, piv,
+ * dinv of bem_lu_factor_tiled, dtype lu_dtype, leading dimension ldlu) of the
+ * normal matrix from bem_gram.  b: device [2n] (the stacked right-hand side).
+ * Stops at relative normal-equation residual tol, or, once a restart cycle no
+ * longer halves it, at <= accept.  iters, relres: host pointers (may be NULL).
+ * Synchronises the stream once per Arnoldi step. */
+int bem_lstsq_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld,
+                     const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
+                     const void* dinv, const void* b, void* x, double tol, int maxit, int restart, double accept,
+                     int* iters, double* relres, void* stream);
+
 /* ---- post-processing (headless) ------------------------------------------------
  * The two kernels the reference runs at the end of BEMManager.run for its
  * GGUI window (BEM_manager.py:1028-1029), writing plain device buffers; there

@@ -215,6 +215,34 @@ class Engine:
         self._check(self.lib.bem_assemble_calderon(self.ctx, ctypes.byref(desc), nk, kk, k2, ctypes.byref(ns),
                                                    ctypes.byref(ds), po, cf, o0.stride(0), _stream_ptr()))
 
+    def gram(self, A: torch.Tensor, P: torch.Tensor, out: torch.Tensor, colscale: torch.Tensor):
+        """out = D (A^H A + P^H P) D (full Hermitian), colscale = D (bem_gram):
+        FP16-split tensor-core products when out is complex64/float32, FP64
+        tensor-core products when it is complex128/float64."""
+        n = A.shape[0]
+        for M in (A, P):
+            assert M.is_cuda and M.shape == (n, n) and M.stride(1) == 1 and M.stride(0) == A.stride(0)
+            assert M.dtype == A.dtype
+        assert out.shape == (n, n) and out.stride(1) == 1 and colscale.dtype == torch.float64
+        assert colscale.numel() == n and colscale.is_contiguous()
+        self._check(self.lib.bem_gram(self.ctx, _dtype_code(A), _ptr(A), _ptr(P), n, A.stride(0), _ptr(colscale),
+                                      _dtype_code(out), _ptr(out), out.stride(0), _stream_ptr()))
+        return out, colscale
+
+    def lstsq_refine(self, A, P, colscale, LU, piv, dinv, b, x, tol=1e-14, maxit=60, restart=30, accept=1e-10):
+        """Flexible GMRES in FP64 on the scaled normal equations of
+        min ||[A; P] x - b|| (bem_lstsq_refine); x holds the initial guess.
+        Returns (iterations, relative normal-equation residual)."""
+        n = A.shape[0]
+        assert b.numel() == 2 * n and b.is_contiguous() and x.is_contiguous() and x.numel() == n
+        it = ctypes.c_int(0)
+        rr = ctypes.c_double(0.0)
+        self._check(self.lib.bem_lstsq_refine(self.ctx, _dtype_code(A), _ptr(A), _ptr(P), n, A.stride(0),
+                                              _ptr(colscale), _dtype_code(LU), _ptr(LU), LU.stride(0), _ptr(piv),
+                                              _ptr(dinv), _ptr(b), _ptr(x), float(tol), int(maxit), int(restart),
+                                              float(accept), ctypes.byref(it), ctypes.byref(rr), _stream_ptr()))
+        return it.value, rr.value
+
     def set_tuning(self, key: int, value: int):
         """A launch-shape choice of this context (bem_ctx_set_tuning)."""
         self._check(self.lib.bem_ctx_set_tuning(self.ctx, int(key), int(value)))

@@ -19,7 +19,8 @@ Extra simulation_parameters keys (all optional):
   honour_show: whether the `show` parameter selects the splat and colouring
              (the reference's own code ignores it); default: not quirk
   solver:    "lstsq" (transmission default, the reference's least squares on
-             [A; P+_i] via normal equations) or "lu" (square A)
+             [A; P+_i] by the column-equilibrated normal equations on this
+             library's kernels) or "lu" (square A)
   refine_tol / refine_maxit: iterative-refinement controls of the mixed path
 """
 from __future__ import annotations
@@ -94,6 +95,12 @@ class BEMManager:
         # unordered panel pairs (bem_assemble_calderon) straight into _mat_A
         # and _mat_P, instead of one kernel per operator and scope
         self.fuse_calderon = bool(p.get("fuse_calderon", True))
+        # least squares of the transmission system: relative residual of the
+        # scaled normal equations at which the FP64 iteration stops, the level
+        # accepted once it stagnates, and its step cap
+        self.lstsq_tol = float(p.get("lstsq_tol", 1e-14))
+        self.lstsq_accept = float(p.get("lstsq_accept", 1e-10))
+        self.lstsq_maxit = int(p.get("lstsq_maxit", 90))
         self._mat_P = None
         # relative residual at which FP64 refinement stops: 1e-9 in mixed
         # precision (its contribution to the solution error is at most
@@ -393,6 +400,34 @@ class BEMManager:
         self.solve_info = {"factor": kind, "info": info, "refine_iters": max(its), "relres": max(rrs)}
         return xs[0] if b.dim() == 1 else torch.stack(xs, 1)
 
+    def _lstsq(self, A: torch.Tensor, P: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+        """min ||[A; P] x - b|| (the reference's torch.linalg.lstsq on the
+        stacked transmission system, BEM_manager.py:1039-1050) by the
+        column-equilibrated normal equations: the normal matrix on the tensor
+        cores (FP16-split products in mixed precision, FP64 products on the
+        plain path), its tile LU (FP32 / FP64), and flexible GMRES in FP64 on
+        the normal equations against the FP64-stored A and P."""
+        n = A.shape[0]
+        mixed = self.solve_precision == "mixed"
+        if A.is_complex():
+            lo = torch.complex64 if mixed else torch.complex128
+        else:
+            lo = torch.float32 if mixed else torch.float64
+        d = torch.empty(n, dtype=torch.float64, device=A.device)
+        Nm = torch.empty(n, n, dtype=lo, device=A.device)
+        self.engine.gram(A, P, Nm, d)
+        piv, dinv, info = self.engine.lu_factor_tiled(Nm)
+        x = torch.zeros(n, dtype=A.dtype, device=A.device)
+        its, rr = self.engine.lstsq_refine(A, P, d, Nm, piv, dinv, b, x, tol=self.lstsq_tol,
+                                           maxit=self.lstsq_maxit, restart=30, accept=self.lstsq_accept)
+        if int(info.item()) > 0:
+            raise torch.linalg.LinAlgError("linalg.lstsq: the normal matrix of the stacked system is singular")
+        self.solve_info = {"factor": ("fp16-split tensor-core normal matrix, fp32 tile LU" if mixed else
+                                      "fp64 tensor-core normal matrix, fp64 tile LU") + ", fp64 flexible GMRES",
+                           "info": info, "refine_iters": its, "relres": rr}
+        del Nm, dinv
+        return x
+
     def solve(self):
         n = self.N_Neumann + self.M_Dirichlet
         if self._is_transmission:
@@ -405,11 +440,7 @@ class BEMManager:
                 self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
                 P = self._mat_A.clone()
             if self.solver == "lstsq":
-                # normal equations of the stacked system: (A^H A + P^H P) x = A^H b_top
-                AH = A_top.conj().transpose(0, 1)
-                Mn = (AH @ A_top + P.conj().transpose(0, 1) @ P).contiguous()
-                bn = (AH @ self.rhs[:n]).contiguous()
-                sol = self._lu_solve_square(Mn, bn)
+                sol = self._lstsq(A_top.contiguous(), P.contiguous(), self.rhs.contiguous())
             else:
                 sol = self._lu_solve_square(A_top.contiguous(), self.rhs[:n].contiguous())
             if A_top is not self._mat_A:

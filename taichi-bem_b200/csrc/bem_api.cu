@@ -201,6 +201,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
     if (ctx->ev_diag) cudaEventDestroy(ctx->ev_diag);
     if (ctx->aux) cudaStreamDestroy(ctx->aux);
     if (ctx->ws) cudaFree(ctx->ws);
+    if (ctx->big_ws) cudaFree(ctx->big_ws);
     if (ctx->flags) cudaFree(ctx->flags);
     delete ctx;
     return BEM_OK;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 
 #include "../../include/bem_b200.h"
@@ -49,6 +50,8 @@ struct bem_ctx {
     int32_t* flags = nullptr;        // [16] device-side status words
     void* ws = nullptr;              // linear-algebra workspace
     size_t ws_bytes = 0;
+    void* big_ws = nullptr;          // FP16 split operands of the least-squares normal matrix
+    size_t big_ws_bytes = 0;
     // high-priority side stream and events of the LU lookahead (made on first use)
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_next = nullptr, ev_diag = nullptr;
@@ -62,6 +65,15 @@ int bem_ws_reserve(bem_ctx* ctx, size_t bytes);
 // bem_lu_factor_tiled that ran out (flags[4], read by the caller after a
 // synchronisation as `value`).
 int bem_take_factor_error(bem_ctx* ctx, int32_t value, cudaStream_t s);
+// Flexible restarted GMRES(restart) in FP64 on op(x) = b, right-preconditioned
+// by precond (applied in place to a vector; it may differ between
+// applications, as a low-precision solve does): Arnoldi with classical
+// Gram-Schmidt twice, Givens rotations on the host.  Each restart starts from
+// the true residual b - op(x); a cycle that no longer halves it ends the
+// iteration once it is <= accept.  x holds the initial guess (bem_linalg.cu).
+int bem_fgmres(bem_ctx* ctx, bool C, int64_t n, const std::function<int(const double*, double*)>& apply_op,
+               const std::function<int(double*)>& precond, const double* b, double* x, double tol, int maxit,
+               int restart, double accept, int* iters, double* relres, cudaStream_t s);
 // Asynchronous preconditioner step of the refinement (bem_tilelu.cu).
 int bem_tiled_precond_async(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                             const void* dinv, const double* r, double** out, const int* skip, cudaStream_t s);

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <complex>
+#include <functional>
 #include <vector>
 
 #include <cmath>
@@ -971,14 +972,14 @@ __global__ void gm_scale_kernel(double* dst, const double* src, int64_t nd, doub
 // the true FP64 residual; a restart cycle that no longer halves it ends the
 // iteration once the residual is <= accept (its floor is about
 // eps * cond(A)).
-int gmres_run(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv, const void* dinv,
-              int64_t n, int64_t lda, const double* b, double* x, double tol, int maxit, int restart, double accept,
-              int* iters, double* relres, cudaStream_t s) {
-    const bool C = dtype_hi == BEM_C128;
+}  // namespace
+
+int bem_fgmres(bem_ctx* ctx, bool C, int64_t n, const std::function<int(const double*, double*)>& apply_op,
+               const std::function<int(double*)>& precond, const double* b, double* x, double tol, int maxit,
+               int restart, double accept, int* iters, double* relres, cudaStream_t s) {
     const int W = C ? 2 : 1;
     const int64_t nd = W * n;
     const int m = std::max(1, std::min(restart, 200));
-    const int lo_dtype = C ? BEM_C64 : BEM_F32;
     // V (m+1 vectors), Z (m vectors), w, r, dots (2 (m+1) doubles)
     const size_t doubles = (size_t)(2 * m + 3) * nd + 2 * (m + 2);
     double* buf = nullptr;
@@ -1005,16 +1006,15 @@ int gmres_run(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, c
         *out = std::sqrt(h);
         return BEM_OK;
     };
+    // r = b - op(x), with w as the scratch of op(x)
     auto residual = [&](double* out_norm) -> int {
+        if (int e = apply_op(x, w)) return e;
         if (int e = bem_check_cuda(ctx, cudaMemcpyAsync(r, b, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s),
                                    "r=b"))
             return e;
-        if (int e = bem_gemv(ctx, dtype_hi, A_hi, n, n, lda, x, r, -1.0, 1.0, s)) return e;
+        axpy_kernel<<<(unsigned)((nd + 255) / 256), 256, 0, s>>>(r, w, nd, -1.0);
+        ctx->launches++;
         return norm(r, out_norm);
-    };
-    auto precond = [&](double* z) -> int {
-        return dinv ? bem_lu_solve_tiled(ctx, lo_dtype, LU_lo, n, lda, piv, dinv, z, s)
-                    : bem_lu_solve(ctx, lo_dtype, LU_lo, n, lda, piv, z, 1, 1, s);
     };
     using cplx = std::complex<double>;
     double bnorm = 0.0;
@@ -1048,7 +1048,7 @@ int gmres_run(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, c
                                      "z=v")))
                 break;
             if ((rc = precond(Zj))) break;
-            if ((rc = bem_gemv(ctx, dtype_hi, A_hi, n, n, lda, Zj, w, 1.0, 0.0, s))) break;
+            if ((rc = apply_op(Zj, w))) break;
             for (int pass = 0; pass < 2 && rc == BEM_OK; ++pass) {
                 cudaMemsetAsync(dots, 0, sizeof(double) * 2 * (j + 1), s);
                 if (C)
@@ -1131,6 +1131,23 @@ int gmres_run(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, c
     if (!done && rel > std::max(tol, accept))
         return bem_fail(ctx, BEM_ERR_NOCONVERGE, "GMRES-IR did not reach tol in maxit iterations");
     return BEM_OK;
+}
+
+namespace {
+
+int gmres_run(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, const int32_t* piv, const void* dinv,
+              int64_t n, int64_t lda, const double* b, double* x, double tol, int maxit, int restart, double accept,
+              int* iters, double* relres, cudaStream_t s) {
+    const bool C = dtype_hi == BEM_C128;
+    const int lo_dtype = C ? BEM_C64 : BEM_F32;
+    auto op = [&](const double* z, double* w) -> int {
+        return bem_gemv(ctx, dtype_hi, A_hi, n, n, lda, z, w, 1.0, 0.0, s);
+    };
+    auto precond = [&](double* z) -> int {
+        return dinv ? bem_lu_solve_tiled(ctx, lo_dtype, LU_lo, n, lda, piv, dinv, z, s)
+                    : bem_lu_solve(ctx, lo_dtype, LU_lo, n, lda, piv, z, 1, 1, s);
+    };
+    return bem_fgmres(ctx, C, n, op, precond, b, x, tol, maxit, restart, accept, iters, relres, s);
 }
 
 template <typename T, bool C>

@@ -1,0 +1,857 @@
+// Least squares of the stacked transmission system [A; P] x = [b1; b2]
+// (the reference's torch.linalg.lstsq, BEM_manager.py:1039-1050), by the
+// column-equilibrated normal equations
+//     N z = g,   N = D (A^H A + P^H P) D,   g = D (A^H b1 + P^H b2),   x = D z,
+// with D = diag(2^-e_p) the power of two nearest to 1/||column p of [A; P]||.
+//
+// Mixed precision: N is formed on the tcgen05 tensor cores from FP16 hi/lo
+// splits of the scaled columns (x = hi + 2^-11 lo, both FP16, so each product
+// keeps about 22 bits: hi*hi + 2^-11 (hi*lo + lo*hi)), accumulated in FP32 in
+// TMEM, factored by the FP32 tile LU, and the solution is refined by flexible
+// GMRES in FP64 on the normal equations with FP64 products against the
+// FP64-stored A and P.  Plain FP64: N by FP64 tensor-core (DMMA) products,
+// the FP64 tile LU, and the same FP64 iteration (it converges in one or two
+// steps).
+//
+// The normal matrix is Hermitian; its real form is S = T T^T with T the
+// transposed real view of G = [A; P] D (row 2p + c of T is the real (c = 0)
+// or imaginary (c = 1) part of column p of G), and
+//     N[p][q] = (S[2p][2q] + S[2p+1][2q+1]) + i (S[2p][2q+1] - S[2p+1][2q]).
+// Only tiles on or below the diagonal of S are computed; a mirror pass writes
+// the conjugate transpose above the diagonal.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "bem_internal.cuh"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// column scaling
+// ---------------------------------------------------------------------------
+constexpr int CN_ROWS = 512;  // rows of [A; P] per block of the column-norm pass
+
+// cn2[p] += sum over a chunk of rows of |G_kp|^2 (G = [A; P], complex or real)
+template <bool C>
+__global__ void colnorm_kernel(const double* A, const double* P, int64_t ld, int n, double* cn2) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int W = C ? 2 : 1;
+    const int k0 = blockIdx.y * CN_ROWS, k1 = min(2 * n, k0 + CN_ROWS);
+    double acc = 0.0;
+    for (int k = k0; k < k1; ++k) {
+        const double* row = (k < n ? A + (int64_t)k * ld * W : P + (int64_t)(k - n) * ld * W);
+        if (C) {
+            const double2 v = reinterpret_cast<const double2*>(row)[p];
+            acc += v.x * v.x + v.y * v.y;
+        } else {
+            const double v = row[p];
+            acc += v * v;
+        }
+    }
+    atomicAdd(cn2 + p, acc);
+}
+
+// d[p] = 2^-e with e the integer nearest to log2 ||column p|| (1 for a zero column)
+__global__ void colscale_kernel(const double* cn2, double* d, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const double c = cn2[p];
+    d[p] = c > 0.0 ? ldexp(1.0, -(int)rint(0.5 * log2(c))) : 1.0;
+}
+
+// ---------------------------------------------------------------------------
+// FP16 hi/lo split of the scaled, transposed real view: T[2p + c][k]
+// ---------------------------------------------------------------------------
+// Block: 32 columns p x 64 rows k of G (complex), through shared memory, so
+// that reads run along p and writes along k.  Padding rows (p >= n) and
+// columns (k >= 2n) of T are written as zeros.
+template <bool C>
+__global__ void __launch_bounds__(256) split_kernel(const double* A, const double* P, int64_t ld, int n,
+                                                    const double* d, __half* Thi, __half* Tlo, int64_t ldt) {
+    __shared__ double2 tile[64][33];
+    const int p0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int W = C ? 2 : 1;
+    for (int kk = warp; kk < 64; kk += 8) {
+        const int k = k0 + kk, p = p0 + lane;
+        double2 v = make_double2(0.0, 0.0);
+        if (p < n && k < 2 * n) {
+            const double* row = (k < n ? A + (int64_t)k * ld * W : P + (int64_t)(k - n) * ld * W);
+            const double s = d[p];
+            if (C) {
+                v = reinterpret_cast<const double2*>(row)[p];
+                v.x *= s;
+                v.y *= s;
+            } else {
+                v.x = row[p] * s;
+            }
+        }
+        tile[kk][lane] = v;
+    }
+    __syncthreads();
+    // T rows of this block: 2 * 32 (complex) or 32 (real); each warp writes one
+    // row segment of 64 k values as 32 half2
+    const int trows = C ? 64 : 32;
+    for (int rr = warp; rr < trows; rr += 8) {
+        const int pl = C ? rr >> 1 : rr, c = C ? rr & 1 : 0;
+        const int64_t i = C ? 2 * (int64_t)(p0 + pl) + c : (int64_t)(p0 + pl);
+        const double2 v0 = tile[2 * lane][pl], v1 = tile[2 * lane + 1][pl];
+        const float f0 = (float)(c ? v0.y : v0.x), f1 = (float)(c ? v1.y : v1.x);
+        const __half h0 = __float2half_rn(f0), h1 = __float2half_rn(f1);
+        const __half l0 = __float2half_rn((f0 - __half2float(h0)) * 2048.0f);
+        const __half l1 = __float2half_rn((f1 - __half2float(h1)) * 2048.0f);
+        const int64_t off = i * ldt + k0 + 2 * lane;
+        *reinterpret_cast<__half2*>(Thi + off) = __halves2half2(h0, h1);
+        *reinterpret_cast<__half2*>(Tlo + off) = __halves2half2(l0, l1);
+    }
+}
+
+// lower-triangle tile t (row-major order, diagonal included) -> (bi, bj), bi >= bj
+__device__ __forceinline__ void tri_tile(int t, int& bi, int& bj) {
+    int i = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while (i * (i + 1) / 2 > t) --i;
+    while ((i + 1) * (i + 2) / 2 <= t) ++i;
+    bi = i;
+    bj = t - i * (i + 1) / 2;
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 Gram kernel: S_tile = T[rows bi] T[rows bj]^T over all K
+// ---------------------------------------------------------------------------
+// Warp 0 is the TMA producer, warp 1 allocates TMEM and issues the MMAs
+// (one elected thread), warps 2-5 are the epilogue (warp w reads TMEM lanes
+// 32 (w % 4) ..).  A stage holds the hi and lo 128 x 64 FP16 tiles of both
+// operands, loaded by TMA with the 128-byte swizzle into 1024-byte aligned
+// shared memory; the matching UMMA descriptors are K-major SWIZZLE_128B
+// (8-row groups 1024 bytes apart), advanced by 32 bytes per K = 16 step.
+// Per K = 16 step three MMAs: D1 += A_hi B_hi, D2 += A_hi B_lo + A_lo B_hi.
+// K is accumulated in segments of GT_KSEG stages; two TMEM accumulator sets
+// alternate, so the epilogue adds segment g (D1 + 2^-11 D2) to its FP32
+// running sums while the MMAs of segment g + 1 run.  Segmenting bounds the
+// number of FP32 accumulation steps that any TMEM sum sees.
+constexpr int GT_BM = 128;
+constexpr int GT_BK = 64;
+constexpr int GT_STAGES = 3;
+constexpr int GT_TILE = GT_BM * GT_BK * 2;  // bytes of one 128 x 64 FP16 tile
+constexpr int GT_STAGE = 4 * GT_TILE;
+constexpr int GT_KSEG = 64;
+constexpr int GT_THREADS = 192;
+constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
+constexpr uint32_t GT_SPIN_CAP = 1u << 24;
+constexpr size_t GT_SMEM = (size_t)GT_STAGES * GT_STAGE + 1024;
+// instruction descriptor, kind::f16: D F32 (bit 4), A and B F16 (0), both
+// K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t GT_IDESC = (1u << 4) | ((uint32_t)(GT_BM >> 3) << 17) | ((uint32_t)(GT_BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int* abort) {
+    for (uint32_t it = 0; it < GT_SPIN_CAP; ++it) {
+        if (mbar_try(addr, parity)) return true;
+        if ((it & 1023u) == 1023u && *abort) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+    uint64_t dsc = 0;
+    dsc |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    dsc |= (uint64_t)1 << 16;              // leading byte offset (not used by swizzled K-major layouts)
+    dsc |= (uint64_t)(1024u >> 4) << 32;   // stride byte offset: 8 rows of 128 bytes
+    dsc |= (uint64_t)1 << 46;              // descriptor version
+    dsc |= (uint64_t)2 << 61;              // SWIZZLE_128B
+    return dsc;
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(GT_IDESC), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap* map, uint32_t mbar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(mbar), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t u[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]), "=r"(u[8]),
+          "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(u[i]);
+}
+
+// out: complex (C, interleaved float pairs) or real N x N FP32 matrix, ld in elements
+template <bool C>
+__global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
+                                                                 const __grid_constant__ CUtensorMap tm_lo,
+                                                                 int nchunks, float* out, int64_t ldo, int n,
+                                                                 int32_t* err) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int s_abort;
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                           ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int bi, bj;
+    tri_tile(blockIdx.x, bi, bj);
+    const int nseg = (nchunks + GT_KSEG - 1) / GT_KSEG;
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(GT_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < GT_STAGES; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full_bar[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty_bar[s])) : "memory");
+        }
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&acc_full[b])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&acc_empty[b])) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0) {
+        // ---- TMA producer ----
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_hi)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_lo)) : "memory");
+            for (int c = 0; c < nchunks; ++c) {
+                const int s = c % GT_STAGES;
+                if (c >= GT_STAGES &&
+                    !mbar_wait(smem_u32(&empty_bar[s]), (uint32_t)((c / GT_STAGES - 1) & 1), &s_abort)) {
+                    s_abort = 1;
+                    break;
+                }
+                const uint32_t fb = smem_u32(&full_bar[s]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(GT_STAGE)
+                             : "memory");
+                const uint32_t st = smem_u32(smem + (size_t)s * GT_STAGE);
+                const int x = c * GT_BK;
+                tma_load(st, &tm_hi, fb, x, bi * GT_BM);
+                tma_load(st + GT_TILE, &tm_lo, fb, x, bi * GT_BM);
+                tma_load(st + 2 * GT_TILE, &tm_hi, fb, x, bj * GT_BM);
+                tma_load(st + 3 * GT_TILE, &tm_lo, fb, x, bj * GT_BM);
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            int c = 0;
+            for (int g = 0; g < nseg && !s_abort; ++g) {
+                const int buf = g & 1;
+                if (g >= 2 && !mbar_wait(smem_u32(&acc_empty[buf]), (uint32_t)((g / 2 - 1) & 1), &s_abort)) {
+                    s_abort = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d1 = tmem + (uint32_t)(buf * 256), d2 = d1 + 128;
+                const int cend = min(nchunks, (g + 1) * GT_KSEG);
+                for (int first = 1; c < cend; ++c, first = 0) {
+                    const int s = c % GT_STAGES;
+                    if (!mbar_wait(smem_u32(&full_bar[s]), (uint32_t)((c / GT_STAGES) & 1), &s_abort)) {
+                        s_abort = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t st = smem_u32(smem + (size_t)s * GT_STAGE);
+#pragma unroll
+                    for (int ks = 0; ks < GT_BK / 16; ++ks) {
+                        const uint32_t ko = 32u * ks;
+                        const uint64_t a_hi = desc_sw128(st + ko), a_lo = desc_sw128(st + GT_TILE + ko);
+                        const uint64_t b_hi = desc_sw128(st + 2 * GT_TILE + ko),
+                                       b_lo = desc_sw128(st + 3 * GT_TILE + ko);
+                        const uint32_t acc = (first && ks == 0) ? 0u : 1u;
+                        mma_f16(d1, a_hi, b_hi, acc);
+                        mma_f16(d2, a_hi, b_lo, acc);
+                        mma_f16(d2, a_lo, b_hi, 1u);
+                    }
+                    asm volatile(
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                            smem_u32(&empty_bar[s]))
+                        : "memory");
+                }
+                if (s_abort) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&acc_full[buf]))
+                             : "memory");
+            }
+        }
+    } else {
+        // ---- epilogue: running FP32 sums of the segments, then the complex combine ----
+        const int q = warp & 3;
+        float acc[GT_BM];
+#pragma unroll
+        for (int i = 0; i < GT_BM; ++i) acc[i] = 0.f;
+        bool ok = true;
+        for (int g = 0; g < nseg; ++g) {
+            const int buf = g & 1;
+            // every lane waits; the vote keeps the warp's TMEM loads and shuffles uniform
+            const bool got = mbar_wait(smem_u32(&acc_full[buf]), (uint32_t)((g / 2) & 1), &s_abort);
+            if (!__all_sync(0xffffffffu, got)) {
+                ok = false;
+                s_abort = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * 256);
+#pragma unroll
+            for (int cc = 0; cc < GT_BM; cc += 16) {
+                float v1[16], v2[16];
+                tmem_ld16(base + cc, v1);
+                tmem_ld16(base + 128 + cc, v2);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int i = 0; i < 16; ++i) acc[cc + i] += fmaf(v2[i], 4.8828125e-4f, v1[i]);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[buf])) : "memory");
+        }
+        if (ok) {
+            const int r = bi * GT_BM + 32 * q + lane;  // real row of S
+            if (C) {
+                // rows 2p (even lane) and 2p + 1 (odd lane); the even lane writes
+                // complex columns 0..31 of the tile, the odd lane 32..63
+                const int p = r >> 1;
+                const bool odd = lane & 1;
+#pragma unroll
+                for (int m = 0; m < GT_BM / 2; ++m) {
+                    const float a = acc[2 * m], b = acc[2 * m + 1];
+                    const float pa = __shfl_xor_sync(0xffffffffu, a, 1), pb = __shfl_xor_sync(0xffffffffu, b, 1);
+                    const bool mine = odd ? (m >= GT_BM / 4) : (m < GT_BM / 4);
+                    const int qc = (bj * GT_BM >> 1) + m;
+                    if (mine && p < n && qc < n) {
+                        // even: (a, b) = S[2p][2q, 2q+1], partner = S[2p+1]; odd: the roles swap
+                        const float re = odd ? (pa + b) : (a + pb);
+                        const float im = odd ? (pb - a) : (b - pa);
+                        *reinterpret_cast<float2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_float2(re, im);
+                    }
+                }
+            } else if (r < n) {
+#pragma unroll
+                for (int m = 0; m < GT_BM; ++m) {
+                    const int qc = bj * GT_BM + m;
+                    if (qc < n) out[(int64_t)r * ldo + qc] = acc[m];
+                }
+            }
+        }
+    }
+    if (s_abort && tid == 0) atomicExch(err, BEM_ERR_TIMEOUT);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GT_TMEM_COLS) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// FP64 Gram kernel (plain path): DMMA m8n8k4 on 128 x 128 real tiles of
+// S = R^T R, R the real view of [A; P] (rows k), read directly; the column
+// scaling is applied in the epilogue.
+// ---------------------------------------------------------------------------
+constexpr int GD_BM = 128, GD_BK = 16, GD_LD = GD_BM + 8;
+constexpr int GD_SMEM = 2 * 2 * GD_BK * GD_LD * (int)sizeof(double);
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const uint32_t d = smem_u32(dst);
+    const int bytes = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+    const uint32_t d = smem_u32(dst);
+    const int bytes = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <bool C>
+__global__ void __launch_bounds__(256) gram_f64_kernel(const double* A, const double* P, int64_t ld, int n,
+                                                       const double* d, double* out, int64_t ldo) {
+    extern __shared__ __align__(16) double sm[];
+    double* As = sm;                       // [2][GD_BK][GD_LD]
+    double* Bs = sm + 2 * GD_BK * GD_LD;   // [2][GD_BK][GD_LD]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int bi, bj;
+    tri_tile(blockIdx.x, bi, bj);
+    const int W = C ? 2 : 1;
+    const int ncol = W * n;       // real columns of R
+    const int K = 2 * n;          // rows of R
+    const int i0 = bi * GD_BM, j0 = bj * GD_BM;
+    const int wi = warp & 1, wj = warp >> 1;  // warp tile 64 x 32
+    double acc[8][4][2];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+
+    // stage loader: 16 rows x 128 doubles of each operand (2048 pairs of
+    // doubles), 16 bytes per cp.async for complex rows (16-byte aligned), two
+    // 8-byte copies for real rows (any even or odd leading dimension)
+    auto load = [&](int stage, int k0) {
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+            const int u = tid + 256 * h;  // operand (u >> 10), row, pair of doubles
+            const int opnd = u >> 10, v = u & 1023;
+            const int kr = v >> 6, cp = (v & 63) * 2;
+            const int k = k0 + kr;
+            const int col = (opnd ? j0 : i0) + cp;
+            const double* row = (k < n ? A + (int64_t)k * ld * W : P + (int64_t)(k - n) * ld * W);
+            double* dst = (opnd ? Bs : As) + (stage * GD_BK + kr) * GD_LD + cp;
+            if (C) {
+                const bool ok = k < K && col < ncol;
+                cp_async16(dst, ok ? row + col : A, ok);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const bool ok = k < K && col + e < ncol;
+                    cp_async8(dst + e, ok ? row + col + e : A, ok);
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int nk = (K + GD_BK - 1) / GD_BK;
+    load(0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+        const int stage = kt & 1;
+        if (kt + 1 < nk) {
+            load(stage ^ 1, (kt + 1) * GD_BK);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const double* as = As + stage * GD_BK * GD_LD;
+        const double* bs = Bs + stage * GD_BK * GD_LD;
+#pragma unroll
+        for (int k4 = 0; k4 < GD_BK; k4 += 4) {
+            const int kr = k4 + (lane & 3);
+            double af[8], bf[4];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) af[a] = as[kr * GD_LD + wi * 64 + a * 8 + (lane >> 2)];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bf[b] = bs[kr * GD_LD + wj * 32 + b * 8 + (lane >> 2)];
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+        }
+        __syncthreads();
+    }
+    // epilogue: acc[a][b][e] = S[i0 + wi*64 + a*8 + lane/4][j0 + wj*32 + b*8 + 2*(lane%4) + e]
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int r = i0 + wi * 64 + a * 8 + (lane >> 2);
+            const int cc = j0 + wj * 32 + b * 8 + 2 * (lane & 3);
+            if (C) {
+                // rows 2p / 2p+1 sit in lanes L / L + 4
+                const double o0 = __shfl_xor_sync(0xffffffffu, acc[a][b][0], 4);
+                const double o1 = __shfl_xor_sync(0xffffffffu, acc[a][b][1], 4);
+                if (((lane >> 2) & 1) == 0) {
+                    const int p = r >> 1, qc = cc >> 1;
+                    if (p < n && qc < n) {
+                        const double s = d[p] * d[qc];
+                        const double re = acc[a][b][0] + o1, im = acc[a][b][1] - o0;
+                        *reinterpret_cast<double2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_double2(s * re, s * im);
+                    }
+                }
+            } else if (r < n) {
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                    if (cc + e < n) out[(int64_t)r * ldo + cc + e] = d[r] * d[cc + e] * acc[a][b][e];
+            }
+        }
+}
+
+// N[p][q] = conj(N[q][p]) for q > p (T = float or double; C: complex pairs)
+template <typename T, bool C>
+__global__ void mirror_kernel(T* out, int64_t ldo, int n) {
+    const int bx = blockIdx.x, by = blockIdx.y;
+    if (bx < by) return;  // blocks with column block >= row block
+    __shared__ T re[32][33], im[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    const int W = C ? 2 : 1;
+    for (int yy = ty; yy < 32; yy += 8) {
+        // source: rows from the column block, columns from the row block (the lower part)
+        const int sr = bx * 32 + yy, sc = by * 32 + tx;
+        if (sr < n && sc < n) {
+            re[yy][tx] = out[W * ((int64_t)sr * ldo + sc)];
+            if (C) im[yy][tx] = out[W * ((int64_t)sr * ldo + sc) + 1];
+        }
+    }
+    __syncthreads();
+    for (int yy = ty; yy < 32; yy += 8) {
+        const int dr = by * 32 + yy, dc = bx * 32 + tx;
+        if (dr < n && dc < n && dc > dr) {
+            out[W * ((int64_t)dr * ldo + dc)] = re[tx][yy];
+            if (C) out[W * ((int64_t)dr * ldo + dc) + 1] = -im[tx][yy];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// products of the refinement
+// ---------------------------------------------------------------------------
+// y[p] (+)= scale_p * sum_k conj(M1[k][p]) x1[k] + conj(M2[k][p]) x2[k] over a
+// chunk of rows k (grid.y), added atomically; columns along threads
+constexpr int GH_ROWS = 256;
+template <bool C>
+__global__ void __launch_bounds__(256) gemvh2_kernel(const double* M1, const double* M2, int64_t ld, int n,
+                                                     const double* x1, const double* x2, double* y) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int k0 = blockIdx.y * GH_ROWS, k1 = min(2 * n, k0 + GH_ROWS);
+    double ar = 0.0, ai = 0.0;
+    for (int k = k0; k < k1; ++k) {
+        const bool top = k < n;
+        const int kk = top ? k : k - n;
+        const double* row = (top ? M1 : M2) + (int64_t)kk * ld * (C ? 2 : 1);
+        const double* xv = top ? x1 : x2;
+        if (C) {
+            const double2 m = reinterpret_cast<const double2*>(row)[p];
+            const double xr = xv[2 * kk], xi = xv[2 * kk + 1];
+            ar += m.x * xr + m.y * xi;
+            ai += m.x * xi - m.y * xr;
+        } else {
+            ar += row[p] * xv[kk];
+        }
+    }
+    if (C) {
+        atomicAdd(y + 2 * p, ar);
+        atomicAdd(y + 2 * p + 1, ai);
+    } else {
+        atomicAdd(y + p, ar);
+    }
+}
+
+// v[p] *= d[p] (complex pairs when C)
+template <bool C>
+__global__ void dscale_kernel(double* v, const double* d, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (C) {
+        v[2 * p] *= d[p];
+        v[2 * p + 1] *= d[p];
+    } else {
+        v[p] *= d[p];
+    }
+}
+
+// dst = src / d (d a power of two: exact)
+template <bool C>
+__global__ void dunscale_copy_kernel(double* dst, const double* src, const double* d, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (C) {
+        dst[2 * p] = src[2 * p] / d[p];
+        dst[2 * p + 1] = src[2 * p + 1] / d[p];
+    } else {
+        dst[p] = src[p] / d[p];
+    }
+}
+
+template <bool C>
+__global__ void dscale_copy_kernel(double* dst, const double* src, const double* d, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (C) {
+        dst[2 * p] = src[2 * p] * d[p];
+        dst[2 * p + 1] = src[2 * p + 1] * d[p];
+    } else {
+        dst[p] = src[p] * d[p];
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+int big_ws(bem_ctx* ctx, size_t bytes, void** out) {
+    if (bytes > ctx->big_ws_bytes) {
+        if (ctx->big_ws) cudaFree(ctx->big_ws);
+        ctx->big_ws = nullptr;
+        ctx->big_ws_bytes = 0;
+        if (int rc = bem_check_cuda(ctx, cudaMalloc(&ctx->big_ws, bytes), "cudaMalloc(normal-matrix workspace)"))
+            return rc;
+        ctx->big_ws_bytes = bytes;
+    }
+    *out = ctx->big_ws;
+    return BEM_OK;
+}
+
+int column_scale(bem_ctx* ctx, bool C, const double* A, const double* P, int64_t ld, int n, double* d,
+                 cudaStream_t s) {
+    // cn2 lives in d itself, then is replaced by the scale
+    if (int rc = bem_check_cuda(ctx, cudaMemsetAsync(d, 0, sizeof(double) * n, s), "colnorm memset")) return rc;
+    dim3 grid((unsigned)((n + 255) / 256), (unsigned)((2 * n + CN_ROWS - 1) / CN_ROWS));
+    if (C)
+        colnorm_kernel<true><<<grid, 256, 0, s>>>(A, P, ld, n, d);
+    else
+        colnorm_kernel<false><<<grid, 256, 0, s>>>(A, P, ld, n, d);
+    colscale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d, d, n);
+    ctx->launches += 2;
+    return bem_check_cuda(ctx, cudaGetLastError(), "column scale");
+}
+
+template <bool C>
+int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n, const double* d, float* out,
+               int64_t ldo, cudaStream_t s) {
+    const int W = C ? 2 : 1;
+    const int64_t rows = (int64_t)W * n;                    // rows of T
+    const int64_t Rp = (rows + GT_BM - 1) / GT_BM * GT_BM;  // padded rows
+    const int64_t Kp = (2 * (int64_t)n + GT_BK - 1) / GT_BK * GT_BK;
+    if (Kp > (int64_t)1 << 31 || Rp / GT_BM > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "gram: n too large");
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_tiled();
+    if (!enc) return bem_fail(ctx, BEM_ERR_CUDA, "gram: cuTensorMapEncodeTiled is not available");
+    void* ws = nullptr;
+    const size_t arr = (size_t)Rp * (size_t)Kp * sizeof(__half);
+    if (int rc = big_ws(ctx, 2 * arr, &ws)) return rc;
+    __half* Thi = static_cast<__half*>(ws);
+    __half* Tlo = reinterpret_cast<__half*>(static_cast<char*>(ws) + arr);
+    {
+        // the split covers every T row block of 32 columns (64 rows when complex) and K in blocks of 64
+        const int64_t pcols = Rp / W;
+        dim3 grid((unsigned)(pcols / 32), (unsigned)(Kp / 64));
+        split_kernel<C><<<grid, 256, 0, s>>>(A, P, ld, n, d, Thi, Tlo, Kp);
+        ctx->launches++;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "split_kernel")) return rc;
+    }
+    CUtensorMap tm[2];
+    for (int h = 0; h < 2; ++h) {
+        cuuint64_t gdim[2] = {(cuuint64_t)Kp, (cuuint64_t)Rp};
+        cuuint64_t gstride[1] = {(cuuint64_t)Kp * sizeof(__half)};
+        cuuint32_t box[2] = {(cuuint32_t)GT_BK, (cuuint32_t)GT_BM};
+        cuuint32_t estr[2] = {1, 1};
+        CUresult r = enc(&tm[h], CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h ? (void*)Tlo : (void*)Thi, gdim, gstride, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return bem_fail(ctx, BEM_ERR_CUDA, "gram: cuTensorMapEncodeTiled failed");
+    }
+    const int tr = (int)(Rp / GT_BM);
+    const int64_t tiles = (int64_t)tr * (tr + 1) / 2;
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          (int)GT_SMEM),
+                                "gram_tc_kernel smem"))
+        return rc;
+    cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
+    gram_tc_kernel<C><<<(unsigned)tiles, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), out, ldo, n,
+                                                                   ctx->flags + 5);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "gram_tc_kernel");
+}
+
+template <bool C>
+int gram_fp64(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n, const double* d, double* out,
+              int64_t ldo, cudaStream_t s) {
+    const int W = C ? 2 : 1;
+    const int64_t rows = (int64_t)W * n;
+    const int tr = (int)((rows + GD_BM - 1) / GD_BM);
+    const int64_t tiles = (int64_t)tr * (tr + 1) / 2;
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_f64_kernel<C>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, GD_SMEM),
+                                "gram_f64_kernel smem"))
+        return rc;
+    gram_f64_kernel<C><<<(unsigned)tiles, 256, GD_SMEM, s>>>(A, P, ld, n, d, out, ldo);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "gram_f64_kernel");
+}
+
+template <typename T, bool C>
+int mirror(bem_ctx* ctx, T* out, int64_t ldo, int n, cudaStream_t s) {
+    const unsigned nb = (unsigned)((n + 31) / 32);
+    mirror_kernel<T, C><<<dim3(nb, nb), dim3(32, 8), 0, s>>>(out, ldo, n);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "mirror_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld, double* colscale,
+             int out_dtype, void* out, int64_t ldo, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A || !P || !colscale || !out || n <= 0 || ld < n || ldo < n || n > (1 << 28))
+        return bem_fail(ctx, BEM_ERR_INVALID, "gram: bad arguments");
+    const bool C = dtype == BEM_C128;
+    if (!C && dtype != BEM_F64) return bem_fail(ctx, BEM_ERR_INVALID, "gram: A and P must be F64 or C128");
+    if (C && ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(P)) & 15))
+        return bem_fail(ctx, BEM_ERR_INVALID, "gram: complex A and P must be 16-byte aligned");
+    const bool want_c = out_dtype == BEM_C64 || out_dtype == BEM_C128;
+    if (want_c != C || (out_dtype != BEM_C64 && out_dtype != BEM_C128 && out_dtype != BEM_F32 && out_dtype != BEM_F64))
+        return bem_fail(ctx, BEM_ERR_INVALID, "gram: output dtype does not match the input");
+    cudaStream_t s = (cudaStream_t)stream;
+    const double* a = (const double*)A;
+    const double* p = (const double*)P;
+    const int ni = (int)n;
+    if (int rc = column_scale(ctx, C, a, p, ld, ni, colscale, s)) return rc;
+    const bool lo = out_dtype == BEM_C64 || out_dtype == BEM_F32;
+    int rc;
+    if (lo) {
+        rc = C ? gram_mixed<true>(ctx, a, p, ld, ni, colscale, (float*)out, ldo, s)
+               : gram_mixed<false>(ctx, a, p, ld, ni, colscale, (float*)out, ldo, s);
+        if (!rc) rc = C ? mirror<float, true>(ctx, (float*)out, ldo, ni, s) : mirror<float, false>(ctx, (float*)out, ldo, ni, s);
+    } else {
+        rc = C ? gram_fp64<true>(ctx, a, p, ld, ni, colscale, (double*)out, ldo, s)
+               : gram_fp64<false>(ctx, a, p, ld, ni, colscale, (double*)out, ldo, s);
+        if (!rc)
+            rc = C ? mirror<double, true>(ctx, (double*)out, ldo, ni, s) : mirror<double, false>(ctx, (double*)out, ldo, ni, s);
+    }
+    return rc;
+}
+
+int bem_lstsq_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld,
+                     const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
+                     const void* dinv, const void* b, void* x, double tol, int maxit, int restart, double accept,
+                     int* iters, double* relres, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A || !P || !colscale || !LU || !piv || !dinv || !b || !x || n <= 0 || ld < n || ldlu < n)
+        return bem_fail(ctx, BEM_ERR_INVALID, "lstsq_refine: bad arguments");
+    const bool C = dtype == BEM_C128;
+    if (!C && dtype != BEM_F64) return bem_fail(ctx, BEM_ERR_INVALID, "lstsq_refine: A and P must be F64 or C128");
+    const bool lu_c = lu_dtype == BEM_C64 || lu_dtype == BEM_C128;
+    if (lu_c != C) return bem_fail(ctx, BEM_ERR_INVALID, "lstsq_refine: factor dtype does not match");
+    // a timed-out tensor-core wait of the normal matrix leaves it invalid
+    {
+        int32_t e = 0;
+        cudaStream_t s0 = (cudaStream_t)stream;
+        cudaMemcpyAsync(&e, ctx->flags + 5, sizeof(int32_t), cudaMemcpyDeviceToHost, s0);
+        if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s0), "gram status")) return rc;
+        if (e != 0) {
+            cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s0);
+            return bem_fail(ctx, BEM_ERR_TIMEOUT, "gram: a tensor-core wait hit its iteration cap");
+        }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int W = C ? 2 : 1;
+    const int ni = (int)n;
+    const int64_t nd = (int64_t)W * n;
+    const double* a = (const double*)A;
+    const double* p = (const double*)P;
+    const double* bb = (const double*)b;
+    double* xx = (double*)x;
+    // scratch: u (n), t1, t2 (n each), g (n), z (n)
+    double* buf = nullptr;
+    if (int rc = bem_check_cuda(ctx, cudaMallocAsync((void**)&buf, sizeof(double) * 5 * nd, s), "lstsq alloc"))
+        return rc;
+    double* u = buf;
+    double* t1 = u + nd;
+    double* t2 = t1 + nd;
+    double* g = t2 + nd;
+    double* z = g + nd;
+    const unsigned vb = (unsigned)((n + 255) / 256);
+    const dim3 hgrid(vb, (unsigned)((2 * n + GH_ROWS - 1) / GH_ROWS));
+    auto gemvh = [&](const double* x1, const double* x2, double* y) -> int {
+        if (int e = bem_check_cuda(ctx, cudaMemsetAsync(y, 0, sizeof(double) * nd, s), "gemvh memset")) return e;
+        if (C)
+            gemvh2_kernel<true><<<hgrid, 256, 0, s>>>(a, p, ld, ni, x1, x2, y);
+        else
+            gemvh2_kernel<false><<<hgrid, 256, 0, s>>>(a, p, ld, ni, x1, x2, y);
+        if (C)
+            dscale_kernel<true><<<vb, 256, 0, s>>>(y, colscale, ni);
+        else
+            dscale_kernel<false><<<vb, 256, 0, s>>>(y, colscale, ni);
+        ctx->launches += 2;
+        return bem_check_cuda(ctx, cudaGetLastError(), "gemvh2_kernel");
+    };
+    // op(z) = D (A^H A + P^H P) D z
+    auto op = [&](const double* zz, double* w) -> int {
+        if (C)
+            dscale_copy_kernel<true><<<vb, 256, 0, s>>>(u, zz, colscale, ni);
+        else
+            dscale_copy_kernel<false><<<vb, 256, 0, s>>>(u, zz, colscale, ni);
+        ctx->launches++;
+        if (int e = bem_gemv(ctx, dtype, A, n, n, ld, u, t1, 1.0, 0.0, s)) return e;
+        if (int e = bem_gemv(ctx, dtype, P, n, n, ld, u, t2, 1.0, 0.0, s)) return e;
+        return gemvh(t1, t2, w);
+    };
+    auto precond = [&](double* v) -> int { return bem_lu_solve_tiled(ctx, lu_dtype, LU, n, ldlu, piv, dinv, v, s); };
+    int rc = gemvh(bb, bb + nd, g);
+    // x holds the initial guess in the original variables: z0 = x / d
+    if (!rc) {
+        if (C)
+            dunscale_copy_kernel<true><<<vb, 256, 0, s>>>(z, xx, colscale, ni);
+        else
+            dunscale_copy_kernel<false><<<vb, 256, 0, s>>>(z, xx, colscale, ni);
+        ctx->launches++;
+        rc = bem_check_cuda(ctx, cudaGetLastError(), "lstsq init");
+    }
+    if (!rc) rc = bem_fgmres(ctx, C, n, op, precond, g, z, tol, maxit, restart, accept, iters, relres, s);
+    if (!rc || rc == BEM_ERR_NOCONVERGE) {
+        const int keep = rc;
+        if (C)
+            dscale_copy_kernel<true><<<vb, 256, 0, s>>>(xx, z, colscale, ni);
+        else
+            dscale_copy_kernel<false><<<vb, 256, 0, s>>>(xx, z, colscale, ni);
+        ctx->launches++;
+        rc = bem_check_cuda(ctx, cudaGetLastError(), "lstsq x = D z");
+        if (!rc) rc = keep;
+    }
+    cudaFreeAsync(buf, s);
+    return rc;
+}
+
+}  // extern "C"
