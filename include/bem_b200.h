@@ -95,8 +95,11 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  * autotuner (bem_b200/tuning.py) after timing the candidates on this GPU;
  * value 0 restores the built-in default.  Keys:
  *   BEM_TUNE_CALDERON_GROUP  wavenumbers per launch of the fused Calderon
- *                            sweep (1 or 2; default 2) */
+ *                            sweep (1 or 2; default 2)
+ *   BEM_TUNE_GRAM_KSEG       64-wide K stages per TMEM accumulation segment of
+ *                            the tensor-core normal matrix (>= 1) */
 #define BEM_TUNE_CALDERON_GROUP 0
+#define BEM_TUNE_GRAM_KSEG 1
 #define BEM_TUNE_KEYS 8
 int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value);
 

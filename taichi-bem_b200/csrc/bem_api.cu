@@ -171,6 +171,7 @@ int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value) {
     if (key < 0 || key >= BEM_TUNE_KEYS) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: unknown key");
     if (key == BEM_TUNE_CALDERON_GROUP && value != 0 && value != 1 && value != 2)
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon group must be 1 or 2");
+    if (key == BEM_TUNE_GRAM_KSEG && value < 0) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: negative segment");
     ctx->tune[key] = value;
     return BEM_OK;
 }

@@ -126,23 +126,28 @@ __device__ __forceinline__ void tri_tile(int t, int& bi, int& bj) {
 // tcgen05 Gram kernel: S_tile = T[rows bi] T[rows bj]^T over all K
 // ---------------------------------------------------------------------------
 // Warp 0 is the TMA producer, warp 1 allocates TMEM and issues the MMAs
-// (one elected thread), warps 2-5 are the epilogue (warp w reads TMEM lanes
-// 32 (w % 4) ..).  A stage holds the hi and lo 128 x 64 FP16 tiles of both
+// (one elected thread), warps 2-9 are the epilogue (warp w reads TMEM lanes
+// 32 (w % 4) .. and half (w - 2) / 4 of the columns).  A stage holds the hi and lo 128 x 64 FP16 tiles of both
 // operands, loaded by TMA with the 128-byte swizzle into 1024-byte aligned
 // shared memory; the matching UMMA descriptors are K-major SWIZZLE_128B
 // (8-row groups 1024 bytes apart), advanced by 32 bytes per K = 16 step.
 // Per K = 16 step three MMAs: D1 += A_hi B_hi, D2 += A_hi B_lo + A_lo B_hi.
-// K is accumulated in segments of GT_KSEG stages; two TMEM accumulator sets
-// alternate, so the epilogue adds segment g (D1 + 2^-11 D2) to its FP32
-// running sums while the MMAs of segment g + 1 run.  Segmenting bounds the
-// number of FP32 accumulation steps that any TMEM sum sees.
+// K is accumulated in segments of kseg stages; two TMEM accumulator sets
+// alternate, so the epilogue adds segment g (D1 + 2^-11 D2, formed in FP32)
+// to its FP64 running sums while the MMAs of segment g + 1 run.  The tensor
+// core's FP32 accumulation does not round to nearest: its error grows with
+// the number of MMA steps a TMEM sum sees (measured on the 30722-unknown
+// normal matrix: 2e-5 relative for segments of 64 stages, 2e-6 for 4), so
+// the default folds every stage (4 MMA steps per sum), and the FP64 running
+// sums keep the segment count from adding its own rounding.
 constexpr int GT_BM = 128;
 constexpr int GT_BK = 64;
 constexpr int GT_STAGES = 3;
 constexpr int GT_TILE = GT_BM * GT_BK * 2;  // bytes of one 128 x 64 FP16 tile
 constexpr int GT_STAGE = 4 * GT_TILE;
-constexpr int GT_KSEG = 64;
-constexpr int GT_THREADS = 192;
+constexpr int GT_KSEG_DEFAULT = 1;
+constexpr int GT_EPI_WARPS = 8;
+constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
 constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
 constexpr uint32_t GT_SPIN_CAP = 1u << 24;
 constexpr size_t GT_SMEM = (size_t)GT_STAGES * GT_STAGE + 1024;
@@ -218,8 +223,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 template <bool C>
 __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
                                                                  const __grid_constant__ CUtensorMap tm_lo,
-                                                                 int nchunks, float* out, int64_t ldo, int n,
-                                                                 int32_t* err) {
+                                                                 int nchunks, int kseg, float* out, int64_t ldo,
+                                                                 int n, int32_t* err) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
@@ -229,7 +234,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     int bi, bj;
     tri_tile(blockIdx.x, bi, bj);
-    const int nseg = (nchunks + GT_KSEG - 1) / GT_KSEG;
+    const int nseg = (nchunks + kseg - 1) / kseg;
 
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -244,7 +249,8 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         }
         for (int b = 0; b < 2; ++b) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&acc_full[b])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&acc_empty[b])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acc_empty[b])), "r"(GT_EPI_WARPS)
+                         : "memory");
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
@@ -289,7 +295,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d1 = tmem + (uint32_t)(buf * 256), d2 = d1 + 128;
-                const int cend = min(nchunks, (g + 1) * GT_KSEG);
+                const int cend = min(nchunks, (g + 1) * kseg);
                 for (int first = 1; c < cend; ++c, first = 0) {
                     const int s = c % GT_STAGES;
                     if (!mbar_wait(smem_u32(&full_bar[s]), (uint32_t)((c / GT_STAGES) & 1), &s_abort)) {
@@ -321,11 +327,12 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
             }
         }
     } else {
-        // ---- epilogue: running FP32 sums of the segments, then the complex combine ----
-        const int q = warp & 3;
-        float acc[GT_BM];
+        // ---- epilogue: FP64 running sums of the segments, then the complex combine ----
+        constexpr int EC = GT_BM / 2;  // columns per epilogue thread
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        double acc[EC];
 #pragma unroll
-        for (int i = 0; i < GT_BM; ++i) acc[i] = 0.f;
+        for (int i = 0; i < EC; ++i) acc[i] = 0.0;
         bool ok = true;
         for (int g = 0; g < nseg; ++g) {
             const int buf = g & 1;
@@ -337,15 +344,15 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * 256);
+            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * 256 + half * EC);
 #pragma unroll
-            for (int cc = 0; cc < GT_BM; cc += 16) {
+            for (int cc = 0; cc < EC; cc += 16) {
                 float v1[16], v2[16];
                 tmem_ld16(base + cc, v1);
                 tmem_ld16(base + 128 + cc, v2);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int i = 0; i < 16; ++i) acc[cc + i] += fmaf(v2[i], 4.8828125e-4f, v1[i]);
+                for (int i = 0; i < 16; ++i) acc[cc + i] += (double)fmaf(v2[i], 4.8828125e-4f, v1[i]);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
@@ -353,29 +360,30 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         }
         if (ok) {
             const int r = bi * GT_BM + 32 * q + lane;  // real row of S
+            const int c0 = bj * GT_BM + half * EC;     // first real column of this thread
             if (C) {
                 // rows 2p (even lane) and 2p + 1 (odd lane); the even lane writes
-                // complex columns 0..31 of the tile, the odd lane 32..63
+                // the first half of this thread's complex columns, the odd lane the second
                 const int p = r >> 1;
                 const bool odd = lane & 1;
 #pragma unroll
-                for (int m = 0; m < GT_BM / 2; ++m) {
-                    const float a = acc[2 * m], b = acc[2 * m + 1];
-                    const float pa = __shfl_xor_sync(0xffffffffu, a, 1), pb = __shfl_xor_sync(0xffffffffu, b, 1);
-                    const bool mine = odd ? (m >= GT_BM / 4) : (m < GT_BM / 4);
-                    const int qc = (bj * GT_BM >> 1) + m;
+                for (int m = 0; m < EC / 2; ++m) {
+                    const double a = acc[2 * m], b = acc[2 * m + 1];
+                    const double pa = __shfl_xor_sync(0xffffffffu, a, 1), pb = __shfl_xor_sync(0xffffffffu, b, 1);
+                    const bool mine = odd ? (m >= EC / 4) : (m < EC / 4);
+                    const int qc = (c0 >> 1) + m;
                     if (mine && p < n && qc < n) {
                         // even: (a, b) = S[2p][2q, 2q+1], partner = S[2p+1]; odd: the roles swap
-                        const float re = odd ? (pa + b) : (a + pb);
-                        const float im = odd ? (pb - a) : (b - pa);
-                        *reinterpret_cast<float2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_float2(re, im);
+                        const double re = odd ? (pa + b) : (a + pb);
+                        const double im = odd ? (pb - a) : (b - pa);
+                        *reinterpret_cast<float2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_float2((float)re, (float)im);
                     }
                 }
             } else if (r < n) {
 #pragma unroll
-                for (int m = 0; m < GT_BM; ++m) {
-                    const int qc = bj * GT_BM + m;
-                    if (qc < n) out[(int64_t)r * ldo + qc] = acc[m];
+                for (int m = 0; m < EC; ++m) {
+                    const int qc = c0 + m;
+                    if (qc < n) out[(int64_t)r * ldo + qc] = (float)acc[m];
                 }
             }
         }
@@ -697,8 +705,9 @@ int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n
                                 "gram_tc_kernel smem"))
         return rc;
     cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
-    gram_tc_kernel<C><<<(unsigned)tiles, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), out, ldo, n,
-                                                                   ctx->flags + 5);
+    const int kseg = ctx->tune[BEM_TUNE_GRAM_KSEG] > 0 ? ctx->tune[BEM_TUNE_GRAM_KSEG] : GT_KSEG_DEFAULT;
+    gram_tc_kernel<C><<<(unsigned)tiles, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, out, ldo,
+                                                                   n, ctx->flags + 5);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_tc_kernel");
 }
