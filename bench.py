@@ -1,27 +1,31 @@
 """Benchmark: Galerkin BEM assembly + solve on B200.
 
-Workload (one GPU): Helmholtz 3D interior Dirichlet, k = 3, unit icosphere
-subdivision 4 (5120 panels, 2562 vertices), GaussQR = 5, plane-wave data
-exp(i k d.x) with a seeded random unit direction d.  One step = the whole hot
-path of BEMManager.run with inputs resident in HBM: single-layer assembly V
-(26.2 M complex entries; separate pairs in FP32, coincident/edge/vertex pairs
-in FP64), the matrix-free right-hand side 1/2 M g + K g, the FP32 LU factor and
-FP64 iterative refinement to relative residual 1e-9.
+Headline workload (one GPU, the default): the Helmholtz transmission problem
+on the unit icosphere of subdivision 5 (20480 panels, 10242 vertices, 30722
+unknowns: P1 Dirichlet + P0 Neumann traces), k_out = 5, k_in = 7.5, GaussQR =
+5, incident plane wave with a seeded direction.  One step = BEMManager.run
+with inputs resident in HBM: the fused Calderon sweep (V, K, K^T, W at both
+wavenumbers; separate pairs in FP32, coincident/edge/vertex pairs in FP64)
+into A = P-_o + P+_i and P+_i, the identity blocks and right-hand side, and
+the reference's least squares on the stacked [A; P+_i]: FP16-split
+tensor-core normal matrix, FP32 tile LU, FP64 flexible GMRES.
 
-  value  = V entries / time-to-solution (entries/s), device-timed with CUDA
-           events per step, L2 flushed (256 MiB write) between steps;
-  e2e    = the same metric through the public API (CoreManager with host mesh
-           and host-resident results: mesh upload, set-up, run, solution read
-           back), one full lifecycle per step, median of four after one
-           discarded;
-  plain_fp64 = the same step on the plain FP64 path (all quadrature and the LU
-           in FP64), whose solution is the FP64 oracle the mixed result's
-           relative error is quoted against.
+  value  = stacked-system entries (2 n^2) / time-to-solution (entries/s),
+           device-timed with CUDA events per step, 256 MiB L2 flush between
+           steps (the inputs are larger than L2 anyway);
+  e2e    = the same metric through the public API (CoreManager with a host
+           mesh: mesh upload, set-up, run, solution read back), one full
+           lifecycle per step, median of two after one discarded;
+  plain_fp64 = the same step on the plain FP64 path (FP64 sweep, FP64
+           tensor-core normal matrix, FP64 tile LU), whose solution is the
+           FP64 oracle the mixed result's relative error is quoted against.
 
-`--impl reference` times the reference's CPU algorithm (the oracle's FP32
-restatement of its loops, all host threads) on a bounded sample of the same
-workload.  Multi-GPU: one independent replica per rank (the dense solve does
-not shard); value = sum over ranks.
+`--workload dirichlet_s4` gives the Helmholtz interior Dirichlet line (5120
+panels); the other workloads print their own lines.  `--impl reference`
+times the reference's CPU algorithm (the oracle's FP32 restatement of its
+loops, all host threads) on a bounded sample of the same workload.
+Multi-GPU: one independent replica per rank (the dense solve does not
+shard); value = sum over ranks.
 """
 from __future__ import annotations
 
@@ -56,8 +60,38 @@ WORKLOAD = "Helmholtz 3D interior Dirichlet k=3, icosphere s4 (5120 panels), Gau
 FLOPS_PER_EVAL = 78
 MUFU_PER_EVAL = 2
 # dram__bytes_read.sum + dram__bytes_write.sum of far_vkg_sym_x2_kernel on this
-# workload (423.5 MB + 379.3 MB, profiles/far_vkg_sym_helmholtz_s4.md)
+# workload (423.5 MB + 379.3 MB, one ncu capture of --profile-step mixed)
 FAR_SWEEP_DRAM_BYTES = 802.8e6
+
+TRANS_WORKLOAD = ("Helmholtz transmission 2x2 block Calderon system, icosphere s5 (20480 panels, 10242 vertices, "
+                  "30722 unknowns), k_out=5, k_in=7.5 (n_i=2.25), GaussQR=5, incident plane wave, least squares on "
+                  "the stacked [A; P+_i] (61444 x 30722)")
+# Algorithmic FP32 work per evaluation of the fused Calderon sweep
+# (far_calderon_kernel<float, 2, Helmholtz>), counted once from its scalar
+# source and kept fixed: the pair-frame geometry (e, s, r^2, r and 1/r with the
+# Newton step, d.n_j, the split phase, w/r, w/r^3, t_j) 24 flops, and per
+# wavenumber the phase 1, sine/cosine polynomials 21, k r 1, G 2,
+# (1 - ikr) e^{ikr} 4 and the 14 test-point sums 26 = 55; two wavenumbers:
+# 134 flops and 3 MUFU operations (reciprocal square root, reciprocal, and
+# none per wavenumber).  One evaluation serves V, K, K^T and W of both
+# wavenumbers.
+CAL_FLOPS_PER_EVAL = 134
+
+
+def _measured_peaks():
+    """The driver-measured peaks of this pool's B200s (MEASURED_PEAKS.json),
+    else the fallback figures of the pool's profiling recipe."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "source": "measured"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+MEASURED = _measured_peaks()
 
 
 def _dist():
@@ -563,6 +597,317 @@ def disk2d_bench(n_seg: int, gauss_qr: int, k: float, reps: int = 5):
     }))
 
 
+def reference_line(args, workload, fn):
+    """The reference arm: the reference's algorithm on the host cores (the
+    oracle's FP32 restatement of its loops), one JSON line."""
+    base = {"metric": METRIC, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": {"workload": workload, "host": "cpu"}}
+    cb = fn(args.steps, max(1, min(args.warmup, 1)))
+    base.update(value=cb["value"], unit="entries/s", ms_per_step=cb["seconds_per_sample"] * 1e3,
+                cpu_baseline=cb, e2e={"value": cb["value"], "unit": "entries/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0})
+    print(json.dumps(base))
+
+
+def cpu_reference_transmission(steps: int, warmup: int, threads: int | None = None, target_s: float = 10.0):
+    """The reference's transmission assembly on the host: the oracle's FP32
+    restatement of its loops (one outer iteration per test panel, serial
+    over trial panels x GaussQR^4, per-basis recompute) for V, K and W at both
+    wavenumbers, on a sample of test panels; its time is scaled by the
+    sampled fraction of the test panels to the whole assembly, and the rate
+    is the stacked system's 2 n^2 entries over that time (the assembly alone,
+    without the reference's least-squares solve: a bound in the CPU's
+    favour)."""
+    import numpy as np
+
+    from bem_b200 import icosphere
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    O.set_threads(threads)
+    v, f = icosphere(5)
+    nt, nv = len(f), len(v)
+    n = nt + nv
+    Q = 5
+    panels = np.arange(nt, dtype=np.int32)
+    p1dof = f.reshape(-1).astype(np.int32)
+
+    def one(rows):
+        tp = panels[:rows]
+        t0 = time.perf_counter()
+        for sqrt_n in (1.0, 1.5):
+            k = 5.0 * sqrt_n
+            V = np.zeros((rows, nt), np.complex128)
+            O.assemble(v, f, O.OP_V, True, k, k * k, Q, True, (tp, 1, tp.copy()), (panels, 1, panels.copy()), out=V,
+                       fp32=True)
+            K = np.zeros((rows, nv), np.complex128)
+            O.assemble(v, f, O.OP_K, True, k, k * k, Q, True, (tp, 1, tp.copy()), (panels, 3, p1dof), out=K,
+                       fp32=True)
+            # W rows per (test panel, vertex) slot: the same work as the vertex rows, in a compact output
+            W = np.zeros((3 * rows, nv), np.complex128)
+            O.assemble(v, f, O.OP_W, True, k, k * k, Q, True, (tp, 3, np.arange(3 * rows, dtype=np.int32)),
+                       (panels, 3, p1dof), out=W, fp32=True)
+        return time.perf_counter() - t0
+
+    t1 = one(threads)
+    rows = int(min(nt, threads * max(1, round(target_s / max(t1, 1e-3)))))
+    for _ in range(warmup):
+        one(max(1, rows // 4))
+    times = [one(rows) for _ in range(steps)]
+    t = statistics.mean(times)
+    full_s = t * nt / rows
+    value = 2.0 * n * n / full_s
+    return {"value": value, "unit": "entries/s", "cores": threads, "kind": "port",
+            "sample": f"V, K and W rows of {rows} of {nt} test panels at both wavenumbers, FP32, {steps} timed "
+                      f"samples; whole assembly extrapolated to {full_s:.1f} s",
+            "seconds_per_sample": t}
+
+
+def transmission_headline(args, ws, rank, local):
+    """The north-star line: the Helmholtz transmission problem on icosphere s5
+    (TRANS_WORKLOAD), mixed precision (FP32 far field in the fused Calderon
+    sweep, FP64 near field, FP16-split tensor-core normal matrix, FP32 tile
+    LU, FP64 flexible GMRES on the normal equations) against the plain FP64
+    path (FP64 sweep, FP64 tensor-core normal matrix, FP64 tile LU, the same
+    FP64 iteration), whose solution is the FP64 oracle of the error."""
+    import torch
+    import torch.distributed as dist
+
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from bem_b200.engine import measure_peaks
+    from bem_b200.managers import CoreManager
+    from bem_b200.workloads import transmission_s5
+    subdiv = args.trans_subdiv
+
+    def make(precision, vertices=None, panels=None):
+        params, pw = transmission_s5(precision, subdiv, "lstsq")
+        params["device"] = f"cuda:{local}"
+        if vertices is not None:
+            params.update(vertices=vertices, panels=panels)
+        core = CoreManager(params)
+        core.initialization(pw.fD, pw.fN)
+        return core
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    # ---- mixed path: device-timed steps ----
+    core = make("mixed")
+    b = core._BEM_manager
+    eng = b.engine
+    n = b.N_Neumann + b.M_Dirichlet
+    nt = b.num_of_panels
+    entries = 2 * n * n  # the stacked system [A; P+_i]
+    peaks = measure_peaks(eng)
+    for _ in range(args.warmup):
+        b.run()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = eng.launches
+    evs = [(ev(), ev()) for _ in range(args.steps)]
+    for s_ in range(args.steps):
+        flush.fill_(1.0)
+        evs[s_][0].record()
+        b.run()
+        evs[s_][1].record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = eng.launches - launches0
+    step_ms = [a.elapsed_time(z) for a, z in evs]
+    info = {k: (v.item() if hasattr(v, "item") else v) for k, v in b.solve_info.items()}
+    sol_mixed = b.raw_solved.clone()
+    ms, value = replicas_aggregate(statistics.mean(step_ms), entries, ws, dev)
+
+    # ---- phases of one step, each kernel phase timed on its own ----
+    phases = {}
+
+    def timed(name, fn):
+        e0, e1 = ev(), ev()
+        torch.cuda.synchronize()
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        phases[name] = e0.elapsed_time(e1)
+        return r
+
+    timed("assemble_calderon_mass_rhs", b.assemble_system)
+    A, P = b._mat_A, b._mat_P
+    d = torch.empty(n, dtype=torch.float64, device=dev)
+    Nm = torch.empty(n, n, dtype=torch.complex64, device=dev)
+    timed("normal_matrix_tensor_cores", lambda: eng.gram(A, P, Nm, d))
+    piv, dinv, _ = timed("tile_lu_fp32", lambda: eng.lu_factor_tiled(Nm))
+    x = torch.zeros(n, dtype=A.dtype, device=dev)
+    timed("fgmres_fp64", lambda: eng.lstsq_refine(A, P, d, Nm, piv, dinv, b.rhs, x, tol=b.lstsq_tol,
+                                                  maxit=b.lstsq_maxit, accept=b.lstsq_accept))
+    del Nm, piv, dinv
+    # the far-field sweep alone (both wavenumbers in one launch), for its roofline
+    neu = b.space("charge", 0, "N", 0, offset=b._Neumann_offset_i)
+    dir_ = b.space("charge", 1, "D", 1, offset=b._Dirichlet_offset_i)
+    from bem_b200 import _lib as L
+    desc = b.op_desc(L.OP_V, b._k, 1.0)
+    ks, k2s = [], []
+    for sqrt_n in (b._sqrt_no, b._sqrt_ni):
+        dd = b.op_desc(L.OP_V, b._k, sqrt_n)
+        ks.append(dd.k)
+        k2s.append(dd.k2)
+    A.zero_()
+    P.zero_()
+    timed("calderon_sweep_with_near", lambda: eng.assemble_calderon(desc, ks, k2s, neu, dir_, [A, P], [-1.0, 1.0]))
+    near = eng.near_pairs
+    core.kill()
+    del core, b, A, P
+    torch.cuda.empty_cache()
+
+    # ---- e2e through the public API: host mesh in, solution out, one lifecycle per step ----
+    from bem_b200 import icosphere
+    vh, fh = icosphere(subdiv)
+    vpin = torch.as_tensor(vh).pin_memory()
+    fpin = torch.as_tensor(fh).pin_memory()
+    e2e_ms, d2h = [], 0
+    h2d = vh.nbytes + fh.nbytes
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c2 = make("mixed", vpin.numpy(), fpin.numpy())
+        c2._BEM_manager.run()
+        host = c2._BEM_manager.raw_solved.to("cpu")
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        d2h = host.numel() * host.element_size()
+        c2.kill()
+        del c2
+        torch.cuda.empty_cache()
+    e2e, e2e_value = replicas_aggregate(statistics.median(e2e_ms[1:]), entries, ws, dev)
+
+    # ---- plain FP64 path (its solution is the FP64 oracle of the error) ----
+    core64 = make("fp64")
+    b64 = core64._BEM_manager
+    b64.run()
+    torch.cuda.synchronize()
+    ms64 = []
+    for _ in range(args.plain_steps):
+        flush.fill_(1.0)
+        e0, e1 = ev(), ev()
+        e0.record()
+        b64.run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms64.append(e0.elapsed_time(e1))
+    sol64 = b64.raw_solved.clone()
+    info64 = {k: (v.item() if hasattr(v, "item") else v) for k, v in b64.solve_info.items()}
+    p64 = {}
+    e0, e1 = ev(), ev()
+    e0.record()
+    b64.assemble_system()
+    e1.record()
+    torch.cuda.synchronize()
+    p64["assemble_calderon_mass_rhs"] = e0.elapsed_time(e1)
+    A64, P64 = b64._mat_A, b64._mat_P
+    N64 = torch.empty(n, n, dtype=torch.complex128, device=dev)
+    d64 = torch.empty(n, dtype=torch.float64, device=dev)
+    e0, e1 = ev(), ev()
+    e0.record()
+    b64.engine.gram(A64, P64, N64, d64)
+    e1.record()
+    torch.cuda.synchronize()
+    p64["normal_matrix_fp64_dmma"] = e0.elapsed_time(e1)
+    del N64
+    qr = None
+    if args.qr_check:
+        # numpy-free FP64 QR least squares of the same stacked system (cuSOLVER
+        # via torch, used here only as the checker of the normal-equation solution)
+        G = torch.cat([A64, P64], 0)
+        xq = torch.linalg.lstsq(G, b64.rhs.unsqueeze(1)).solution.squeeze(1)
+        qr = {"fp64_normal_eq_vs_qr_l2": float(torch.linalg.norm(sol64 - xq) / torch.linalg.norm(xq)),
+              "mixed_vs_qr_l2": float(torch.linalg.norm(sol_mixed - xq) / torch.linalg.norm(xq)),
+              "mixed_vs_qr_max": float((sol_mixed - xq).abs().max() / xq.abs().max())}
+        del G, xq
+    core64.kill()
+    del core64, b64, A64, P64
+    torch.cuda.empty_cache()
+    rel2 = float(torch.linalg.norm(sol_mixed - sol64) / torch.linalg.norm(sol64))
+    relm = float((sol_mixed - sol64).abs().max() / sol64.abs().max())
+
+    # ---- rooflines of the kernels of the step ----
+    tr = (2 * n + 127) // 128
+    gram_flops = 8.0 * n ** 3  # the Hermitian product (A^H A + P^H P): 2n x n complex
+    q4 = 625
+    evals = (nt * nt - near) // 2 * q4
+    kern = {
+        "gram_tc_kernel": {"bound": "tensor", "ms": phases["normal_matrix_tensor_cores"],
+                           "achieved": gram_flops / (phases["normal_matrix_tensor_cores"] * 1e-3) / 1e12,
+                           "peak": MEASURED["bf16_tflops"], "unit": "TFLOP/s",
+                           "note": "algorithmic 8 n^3 flops of the Hermitian product; the tensor pipe executes "
+                                   "three FP16 products per product (hi hi, hi lo, lo hi) on "
+                                   f"{tr * (tr + 1) // 2} lower 128 x 128 real tiles"},
+        "tile_lu_fp32": {"bound": "tensor", "ms": phases["tile_lu_fp32"],
+                         "achieved": 8.0 / 3.0 * n ** 3 / (phases["tile_lu_fp32"] * 1e-3) / 1e12,
+                         "peak": MEASURED["bf16_tflops"], "unit": "TFLOP/s",
+                         "note": "8/3 n^3 flops of the complex LU; trailing updates as 3xTF32 tcgen05 products"},
+        "far_calderon_kernel": {"bound": "fp32", "ms": phases["calderon_sweep_with_near"],
+                                "achieved": evals * CAL_FLOPS_PER_EVAL / (phases["calderon_sweep_with_near"] * 1e-3)
+                                / 1e12, "peak": peaks[0], "unit": "TFLOP/s",
+                                "note": f"{CAL_FLOPS_PER_EVAL} flops per evaluation, {evals} evaluations; timed "
+                                        "with its FP64 near-pair kernels in one call"},
+    }
+    for kv in kern.values():
+        kv["frac"] = kv["achieved"] / kv["peak"]
+    top = max(kern, key=lambda k_: kern[k_]["ms"])
+    roof = dict(kern[top])
+    roof["kernel"] = top
+    roof["traffic"] = None
+    roof["peak_source"] = ("MEASURED_PEAKS.json bf16_tflops (burst)" if roof["bound"] == "tensor" else
+                           "bem_measure_peaks FP32 FMA probe on this GPU")
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_reference_transmission(1, 0)
+        except Exception as exc:  # the baseline never blocks the GPU line
+            cpu = {"value": None, "error": repr(exc)}
+    if ws > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "c64 far field / c128 near field, FP16-split tensor-core normal matrix, FP32 tile LU, FP64 "
+                     "refinement",
+            "data": "synthetic (generated icosphere, analytic plane wave)",
+            "config": {"workload": TRANS_WORKLOAD, "unknowns": n, "stacked_entries": entries, "precision": "mixed",
+                       "quirk": "reference quadrature", "l2": "inputs larger than L2; 256 MiB flush between steps",
+                       "parallelism": f"replicas x{ws}"},
+            "time_to_solution_ms": ms, "step_ms": step_ms, "ms_per_step_median": statistics.median(step_ms),
+            "breakdown_ms": phases,
+            "plain_fp64": {"time_to_solution_ms": statistics.mean(ms64), "step_ms": ms64, "breakdown_ms": p64,
+                           "solve": info64},
+            "speedup_vs_plain_fp64": statistics.mean(ms64) / ms,
+            "rel_err_vs_fp64": {"l2_rel": rel2, "max_abs_rel": relm},
+            "qr_check": qr,
+            "solve": info,
+            "e2e": {"value": e2e_value, "unit": "entries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e},
+            "roofline": roof, "kernels": kern,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -573,17 +918,24 @@ def main():
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
     ap.add_argument("--profile-lu", type=int, default=0,
                     help="time six tiled FP32 factorisations of a random complex matrix of this size and exit")
-    ap.add_argument("--workload", default="helmholtz_dirichlet_s4",
-                    choices=["helmholtz_dirichlet_s4", "sweep", "shape", "transmission", "disk2d"],
-                    help="helmholtz_dirichlet_s4: the headline line; sweep: the wavenumber sweep of the augmented "
-                         "transmission operator; shape: the shape gradient on a perturbed sphere; transmission: "
-                         "the Helmholtz transmission system; disk2d: the 2D operators (each its own JSON line)")
+    ap.add_argument("--workload", default="transmission_s5",
+                    choices=["transmission_s5", "dirichlet_s4", "sweep", "shape", "transmission_square", "disk2d"],
+                    help="transmission_s5: the headline line (the 20480-panel transmission problem); dirichlet_s4: "
+                         "Helmholtz interior Dirichlet on 5120 panels; sweep: the wavenumber sweep of the "
+                         "augmented transmission operator; shape: the shape gradient on a perturbed sphere; "
+                         "transmission_square: the square transmission system with dJ/dk; disk2d: the 2D operators "
+                         "(each its own JSON line)")
+    ap.add_argument("--plain-steps", type=int, default=1, help="timed steps of the plain FP64 comparator")
+    ap.add_argument("--qr-check", action="store_true",
+                    help="also solve the FP64 stacked system by QR (torch.linalg.lstsq) as a checker")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the timed CPU baseline")
     ap.add_argument("--disk-n", type=int, default=8192, help="segments of the disk2d workload")
     ap.add_argument("--shape-subdiv", type=int, default=5, help="icosphere subdivision of the shape workload")
     ap.add_argument("--shape-check", type=int, default=32, help="vertices of the finite-difference check")
     ap.add_argument("--trans-subdiv", type=int, default=5, help="icosphere subdivision of the transmission workload")
     ap.add_argument("--trans-plain", action="store_true", help="also time the plain FP64 path (FP64 LU)")
-    ap.add_argument("--trans-solver", default="square", choices=["square", "lstsq"])
+    ap.add_argument("--trans-solver", default="square", choices=["square", "lstsq"],
+                    help="solver of the transmission_square workload")
     ap.add_argument("--sweep-k", type=int, default=60, help="number of wavenumbers of the sweep workload")
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -595,7 +947,7 @@ def main():
         if rank == 0:
             shape_bench(args.shape_subdiv, args.shape_check)
         return
-    if args.workload == "transmission":
+    if args.workload == "transmission_square":
         if rank == 0:
             transmission_bench(args.trans_subdiv, args.trans_plain, args.trans_solver)
         return
@@ -610,19 +962,23 @@ def main():
         profile_lu(args.profile_lu)
         return
 
-    if args.impl == "reference":
-        if rank != 0:
+    if args.workload == "dirichlet_s4":
+        if args.impl == "reference":
+            if rank == 0:
+                reference_line(args, WORKLOAD, cpu_reference)
             return
-        base = {"metric": METRIC, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic", "config": {"workload": WORKLOAD, "host": "cpu"}}
-        cb = cpu_reference(args.steps, max(1, min(args.warmup, 1)))
-        base.update(value=cb["value"], unit="entries/s", ms_per_step=cb["seconds_per_sample"] * 1e3,
-                    cpu_baseline=cb, e2e={"value": cb["value"], "unit": "entries/s", "h2d_bytes_per_step": 0,
-                                          "d2h_bytes_per_step": 0})
-        print(json.dumps(base))
+        dirichlet_headline(args, ws, rank, local)
         return
+    if args.impl == "reference":
+        if rank == 0:
+            reference_line(args, TRANS_WORKLOAD, cpu_reference_transmission)
+        return
+    transmission_headline(args, ws, rank, local)
 
+
+def dirichlet_headline(args, ws, rank, local):
+    """The config-2 line (Helmholtz interior Dirichlet, icosphere s4): see
+    WORKLOAD."""
     import torch
     import torch.distributed as dist
 
