@@ -375,7 +375,8 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                     if (mine && p < n && qc < n) {
                         // even: (a, b) = S[2p][2q, 2q+1], partner = S[2p+1]; odd: the roles swap
                         const double re = odd ? (pa + b) : (a + pb);
-                        const double im = odd ? (pb - a) : (b - pa);
+                        // a Hermitian matrix has a real diagonal (the two products are equal in exact arithmetic)
+                        const double im = p == qc ? 0.0 : (odd ? (pb - a) : (b - pa));
                         *reinterpret_cast<float2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_float2((float)re, (float)im);
                     }
                 }
@@ -510,7 +511,7 @@ __global__ void __launch_bounds__(256) gram_f64_kernel(const double* A, const do
                     const int p = r >> 1, qc = cc >> 1;
                     if (p < n && qc < n) {
                         const double s = d[p] * d[qc];
-                        const double re = acc[a][b][0] + o1, im = acc[a][b][1] - o0;
+                        const double re = acc[a][b][0] + o1, im = p == qc ? 0.0 : acc[a][b][1] - o0;
                         *reinterpret_cast<double2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_double2(s * re, s * im);
                     }
                 }
