@@ -743,9 +743,9 @@ def transmission_headline(args, ws, rank, local):
     timed("assemble_calderon_mass_rhs", b.assemble_system)
     A, P = b._mat_A, b._mat_P
     d = torch.empty(n, dtype=torch.float64, device=dev)
-    Nm = torch.empty(n, n, dtype=torch.complex64, device=dev)
-    timed("normal_matrix_tensor_cores", lambda: eng.gram(A, P, Nm, d))
-    piv, dinv, _ = timed("tile_lu_fp32", lambda: eng.lu_factor_tiled(Nm))
+    Nm = torch.empty(n, n, dtype=torch.complex128, device=dev)
+    timed("normal_matrix_tensor_cores", lambda: eng.gram(A, P, Nm, d, tensor_cores=True))
+    piv, dinv, _ = timed("tile_lu_fp64", lambda: eng.lu_factor_tiled(Nm))
     x = torch.zeros(n, dtype=A.dtype, device=dev)
     timed("fgmres_fp64", lambda: eng.lstsq_refine(A, P, d, Nm, piv, dinv, b.rhs, x, tol=b.lstsq_tol,
                                                   maxit=b.lstsq_maxit, accept=b.lstsq_accept))
@@ -817,7 +817,7 @@ def transmission_headline(args, ws, rank, local):
     d64 = torch.empty(n, dtype=torch.float64, device=dev)
     e0, e1 = ev(), ev()
     e0.record()
-    b64.engine.gram(A64, P64, N64, d64)
+    b64.engine.gram(A64, P64, N64, d64, tensor_cores=False)
     e1.record()
     torch.cuda.synchronize()
     p64["normal_matrix_fp64_dmma"] = e0.elapsed_time(e1)
@@ -850,10 +850,11 @@ def transmission_headline(args, ws, rank, local):
                            "note": "algorithmic 8 n^3 flops of the Hermitian product; the tensor pipe executes "
                                    "three FP16 products per product (hi hi, hi lo, lo hi) on "
                                    f"{tr * (tr + 1) // 2} lower 128 x 128 real tiles"},
-        "tile_lu_fp32": {"bound": "tensor", "ms": phases["tile_lu_fp32"],
-                         "achieved": 8.0 / 3.0 * n ** 3 / (phases["tile_lu_fp32"] * 1e-3) / 1e12,
-                         "peak": MEASURED["bf16_tflops"], "unit": "TFLOP/s",
-                         "note": "8/3 n^3 flops of the complex LU; trailing updates as 3xTF32 tcgen05 products"},
+        "tile_lu_fp64": {"bound": "fp64", "ms": phases["tile_lu_fp64"],
+                         "achieved": 8.0 / 3.0 * n ** 3 / (phases["tile_lu_fp64"] * 1e-3) / 1e12,
+                         "peak": peaks[1], "unit": "TFLOP/s",
+                         "note": "8/3 n^3 flops of the complex LU; trailing updates on DMMA; peak = the FP64 FMA "
+                                 "probe (DMMA runs at the FP64 FMA rate on B200)"},
         "far_calderon_kernel": {"bound": "fp32", "ms": phases["calderon_sweep_with_near"],
                                 "achieved": evals * CAL_FLOPS_PER_EVAL / (phases["calderon_sweep_with_near"] * 1e-3)
                                 / 1e12, "peak": peaks[0], "unit": "TFLOP/s",
@@ -866,8 +867,9 @@ def transmission_headline(args, ws, rank, local):
     roof = dict(kern[top])
     roof["kernel"] = top
     roof["traffic"] = None
-    roof["peak_source"] = ("MEASURED_PEAKS.json bf16_tflops (burst)" if roof["bound"] == "tensor" else
-                           "bem_measure_peaks FP32 FMA probe on this GPU")
+    roof["peak_source"] = {"tensor": "MEASURED_PEAKS.json bf16_tflops (burst)",
+                           "fp32": "bem_measure_peaks FP32 FMA probe on this GPU",
+                           "fp64": "bem_measure_peaks FP64 FMA probe on this GPU"}[roof["bound"]]
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -882,7 +884,7 @@ def transmission_headline(args, ws, rank, local):
             "metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "c64 far field / c128 near field, FP16-split tensor-core normal matrix, FP32 tile LU, FP64 "
+            "dtype": "c64 far field / c128 near field, FP16-split tensor-core normal matrix, FP64 tile LU, FP64 "
                      "refinement",
             "data": "synthetic (generated icosphere, analytic plane wave)",
             "config": {"workload": TRANS_WORKLOAD, "unknowns": n, "stacked_entries": entries, "precision": "mixed",

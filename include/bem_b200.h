@@ -317,16 +317,17 @@ int bem_gmres_ir(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo
  * power-of-two column scaling of [A; P].
  *
  * Normal matrix (the Gram half of that lstsq call): colscale (device [n]
- * doubles) receives D; out (n x n, ldo) receives the full Hermitian N.
- * A, P: BEM_C128 (16-byte aligned) or BEM_F64, n x n, ld.  out_dtype
- * BEM_C64 / BEM_F32 forms N on the tcgen05 tensor cores from FP16 hi/lo
- * splits of the scaled columns (about 22 significant bits per product, FP32
- * accumulation in segments of 4096 products; the FP16 split operands use a
- * context workspace of 8 n^2 bytes); BEM_C128 / BEM_F64 forms it in FP64 on
- * the FP64 tensor cores (DMMA).  Queued without synchronising; a tensor-core
- * wait that runs out is reported by the next bem_lstsq_refine. */
+ * doubles) receives D; out (n x n, ldo; BEM_C64 / BEM_C128 for complex,
+ * BEM_F32 / BEM_F64 for real input) receives the full Hermitian N.
+ * A, P: BEM_C128 (16-byte aligned) or BEM_F64, n x n, ld.  method
+ * BEM_PREC_MIXED forms N on the tcgen05 tensor cores from FP16 hi/lo splits
+ * of the scaled columns (about 22 significant bits per product, TMEM sums of
+ * one 64-wide K stage folded into FP64; the split operands use a context
+ * workspace of 8 n^2 bytes); BEM_PREC_FP64 forms it in FP64 on the FP64
+ * tensor cores (DMMA).  Queued without synchronising; a tensor-core wait
+ * that runs out is reported by the next bem_lstsq_refine. */
 int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld, double* colscale,
-             int out_dtype, void* out, int64_t ldo, void* stream);
+             int method, int out_dtype, void* out, int64_t ldo, void* stream);
 /* The solve half of the same lstsq call (BEM_manager.py:1049): x (device, n,
  * FP64 real or complex, holding the initial guess) is refined by flexible
  * GMRES(restart) in FP64 on the scaled normal equations, with FP64 products

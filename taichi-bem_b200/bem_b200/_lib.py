@@ -106,7 +106,7 @@ def load():
     L.bem_lu_factor_status.argtypes = [vp, vp]
     L.bem_binary_version.argtypes = [ctypes.POINTER(ctypes.c_int)]
     L.bem_ctx_set_tuning.argtypes = [vp, i32, i32]
-    L.bem_gram.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, vp, i64, vp]
+    L.bem_gram.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, i32, vp, i64, vp]
     L.bem_lstsq_refine.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, vp, i64, vp, vp, vp, vp, dbl, i32, i32, dbl,
                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), vp]
     L.bem_assemble_calderon.argtypes = [vp, ctypes.POINTER(OpDesc), i32, ctypes.POINTER(ctypes.c_double),

@@ -215,18 +215,19 @@ class Engine:
         self._check(self.lib.bem_assemble_calderon(self.ctx, ctypes.byref(desc), nk, kk, k2, ctypes.byref(ns),
                                                    ctypes.byref(ds), po, cf, o0.stride(0), _stream_ptr()))
 
-    def gram(self, A: torch.Tensor, P: torch.Tensor, out: torch.Tensor, colscale: torch.Tensor):
-        """out = D (A^H A + P^H P) D (full Hermitian), colscale = D (bem_gram):
-        FP16-split tensor-core products when out is complex64/float32, FP64
-        tensor-core products when it is complex128/float64."""
+    def gram(self, A: torch.Tensor, P: torch.Tensor, out: torch.Tensor, colscale: torch.Tensor, tensor_cores=True):
+        """out = D (A^H A + P^H P) D (full Hermitian, complex64/128 or
+        float32/64), colscale = D (bem_gram): FP16-split tcgen05 products with
+        FP64 sums (tensor_cores) or FP64 DMMA products."""
         n = A.shape[0]
         for M in (A, P):
             assert M.is_cuda and M.shape == (n, n) and M.stride(1) == 1 and M.stride(0) == A.stride(0)
             assert M.dtype == A.dtype
         assert out.shape == (n, n) and out.stride(1) == 1 and colscale.dtype == torch.float64
         assert colscale.numel() == n and colscale.is_contiguous()
+        method = L.PREC_MIXED if tensor_cores else L.PREC_FP64
         self._check(self.lib.bem_gram(self.ctx, _dtype_code(A), _ptr(A), _ptr(P), n, A.stride(0), _ptr(colscale),
-                                      _dtype_code(out), _ptr(out), out.stride(0), _stream_ptr()))
+                                      method, _dtype_code(out), _ptr(out), out.stride(0), _stream_ptr()))
         return out, colscale
 
     def lstsq_refine(self, A, P, colscale, LU, piv, dinv, b, x, tol=1e-14, maxit=60, restart=30, accept=1e-10):

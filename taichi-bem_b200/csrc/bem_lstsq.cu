@@ -219,11 +219,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(u[i]);
 }
 
-// out: complex (C, interleaved float pairs) or real N x N FP32 matrix, ld in elements
-template <bool C>
+// out: complex (C, interleaved pairs) or real N x N matrix of OT (float or double), ld in elements
+template <bool C, typename OT>
 __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
                                                                  const __grid_constant__ CUtensorMap tm_lo,
-                                                                 int nchunks, int kseg, float* out, int64_t ldo,
+                                                                 int nchunks, int kseg, OT* out, int64_t ldo,
                                                                  int n, int32_t* err) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
@@ -377,14 +377,15 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                         const double re = odd ? (pa + b) : (a + pb);
                         // a Hermitian matrix has a real diagonal (the two products are equal in exact arithmetic)
                         const double im = p == qc ? 0.0 : (odd ? (pb - a) : (b - pa));
-                        *reinterpret_cast<float2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_float2((float)re, (float)im);
+                        out[2 * ((int64_t)p * ldo + qc)] = (OT)re;
+                        out[2 * ((int64_t)p * ldo + qc) + 1] = (OT)im;
                     }
                 }
             } else if (r < n) {
 #pragma unroll
                 for (int m = 0; m < EC; ++m) {
                     const int qc = c0 + m;
-                    if (qc < n) out[(int64_t)r * ldo + qc] = (float)acc[m];
+                    if (qc < n) out[(int64_t)r * ldo + qc] = (OT)acc[m];
                 }
             }
         }
@@ -422,9 +423,9 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-template <bool C>
+template <bool C, typename OT>
 __global__ void __launch_bounds__(256) gram_f64_kernel(const double* A, const double* P, int64_t ld, int n,
-                                                       const double* d, double* out, int64_t ldo) {
+                                                       const double* d, OT* out, int64_t ldo) {
     extern __shared__ __align__(16) double sm[];
     double* As = sm;                       // [2][GD_BK][GD_LD]
     double* Bs = sm + 2 * GD_BK * GD_LD;   // [2][GD_BK][GD_LD]
@@ -512,13 +513,14 @@ __global__ void __launch_bounds__(256) gram_f64_kernel(const double* A, const do
                     if (p < n && qc < n) {
                         const double s = d[p] * d[qc];
                         const double re = acc[a][b][0] + o1, im = p == qc ? 0.0 : acc[a][b][1] - o0;
-                        *reinterpret_cast<double2*>(out + 2 * ((int64_t)p * ldo + qc)) = make_double2(s * re, s * im);
+                        out[2 * ((int64_t)p * ldo + qc)] = (OT)(s * re);
+                        out[2 * ((int64_t)p * ldo + qc) + 1] = (OT)(s * im);
                     }
                 }
             } else if (r < n) {
 #pragma unroll
                 for (int e = 0; e < 2; ++e)
-                    if (cc + e < n) out[(int64_t)r * ldo + cc + e] = d[r] * d[cc + e] * acc[a][b][e];
+                    if (cc + e < n) out[(int64_t)r * ldo + cc + e] = (OT)(d[r] * d[cc + e] * acc[a][b][e]);
             }
         }
 }
@@ -665,8 +667,8 @@ int column_scale(bem_ctx* ctx, bool C, const double* A, const double* P, int64_t
     return bem_check_cuda(ctx, cudaGetLastError(), "column scale");
 }
 
-template <bool C>
-int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n, const double* d, float* out,
+template <bool C, typename OT>
+int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n, const double* d, OT* out,
                int64_t ldo, cudaStream_t s) {
     const int W = C ? 2 : 1;
     const int64_t rows = (int64_t)W * n;                    // rows of T
@@ -701,30 +703,30 @@ int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n
     }
     const int tr = (int)(Rp / GT_BM);
     const int64_t tiles = (int64_t)tr * (tr + 1) / 2;
-    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc_kernel<C, OT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                           (int)GT_SMEM),
                                 "gram_tc_kernel smem"))
         return rc;
     cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
     const int kseg = ctx->tune[BEM_TUNE_GRAM_KSEG] > 0 ? ctx->tune[BEM_TUNE_GRAM_KSEG] : GT_KSEG_DEFAULT;
-    gram_tc_kernel<C><<<(unsigned)tiles, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, out, ldo,
+    gram_tc_kernel<C, OT><<<(unsigned)tiles, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, out, ldo,
                                                                    n, ctx->flags + 5);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_tc_kernel");
 }
 
-template <bool C>
-int gram_fp64(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n, const double* d, double* out,
+template <bool C, typename OT>
+int gram_fp64(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n, const double* d, OT* out,
               int64_t ldo, cudaStream_t s) {
     const int W = C ? 2 : 1;
     const int64_t rows = (int64_t)W * n;
     const int tr = (int)((rows + GD_BM - 1) / GD_BM);
     const int64_t tiles = (int64_t)tr * (tr + 1) / 2;
-    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_f64_kernel<C>,
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_f64_kernel<C, OT>,
                                                           cudaFuncAttributeMaxDynamicSharedMemorySize, GD_SMEM),
                                 "gram_f64_kernel smem"))
         return rc;
-    gram_f64_kernel<C><<<(unsigned)tiles, 256, GD_SMEM, s>>>(A, P, ld, n, d, out, ldo);
+    gram_f64_kernel<C, OT><<<(unsigned)tiles, 256, GD_SMEM, s>>>(A, P, ld, n, d, out, ldo);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_f64_kernel");
 }
@@ -742,7 +744,7 @@ int mirror(bem_ctx* ctx, T* out, int64_t ldo, int n, cudaStream_t s) {
 extern "C" {
 
 int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld, double* colscale,
-             int out_dtype, void* out, int64_t ldo, void* stream) {
+             int method, int out_dtype, void* out, int64_t ldo, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
     if (!A || !P || !colscale || !out || n <= 0 || ld < n || ldo < n || n > (1 << 28))
         return bem_fail(ctx, BEM_ERR_INVALID, "gram: bad arguments");
@@ -750,6 +752,8 @@ int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, i
     if (!C && dtype != BEM_F64) return bem_fail(ctx, BEM_ERR_INVALID, "gram: A and P must be F64 or C128");
     if (C && ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(P)) & 15))
         return bem_fail(ctx, BEM_ERR_INVALID, "gram: complex A and P must be 16-byte aligned");
+    if (method != BEM_PREC_MIXED && method != BEM_PREC_FP64)
+        return bem_fail(ctx, BEM_ERR_INVALID, "gram: method must be BEM_PREC_MIXED or BEM_PREC_FP64");
     const bool want_c = out_dtype == BEM_C64 || out_dtype == BEM_C128;
     if (want_c != C || (out_dtype != BEM_C64 && out_dtype != BEM_C128 && out_dtype != BEM_F32 && out_dtype != BEM_F64))
         return bem_fail(ctx, BEM_ERR_INVALID, "gram: output dtype does not match the input");
@@ -759,16 +763,22 @@ int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, i
     const int ni = (int)n;
     if (int rc = column_scale(ctx, C, a, p, ld, ni, colscale, s)) return rc;
     const bool lo = out_dtype == BEM_C64 || out_dtype == BEM_F32;
+    const bool tc = method == BEM_PREC_MIXED;
     int rc;
     if (lo) {
-        rc = C ? gram_mixed<true>(ctx, a, p, ld, ni, colscale, (float*)out, ldo, s)
-               : gram_mixed<false>(ctx, a, p, ld, ni, colscale, (float*)out, ldo, s);
-        if (!rc) rc = C ? mirror<float, true>(ctx, (float*)out, ldo, ni, s) : mirror<float, false>(ctx, (float*)out, ldo, ni, s);
+        float* o = (float*)out;
+        rc = tc ? (C ? gram_mixed<true, float>(ctx, a, p, ld, ni, colscale, o, ldo, s)
+                     : gram_mixed<false, float>(ctx, a, p, ld, ni, colscale, o, ldo, s))
+                : (C ? gram_fp64<true, float>(ctx, a, p, ld, ni, colscale, o, ldo, s)
+                     : gram_fp64<false, float>(ctx, a, p, ld, ni, colscale, o, ldo, s));
+        if (!rc) rc = C ? mirror<float, true>(ctx, o, ldo, ni, s) : mirror<float, false>(ctx, o, ldo, ni, s);
     } else {
-        rc = C ? gram_fp64<true>(ctx, a, p, ld, ni, colscale, (double*)out, ldo, s)
-               : gram_fp64<false>(ctx, a, p, ld, ni, colscale, (double*)out, ldo, s);
-        if (!rc)
-            rc = C ? mirror<double, true>(ctx, (double*)out, ldo, ni, s) : mirror<double, false>(ctx, (double*)out, ldo, ni, s);
+        double* o = (double*)out;
+        rc = tc ? (C ? gram_mixed<true, double>(ctx, a, p, ld, ni, colscale, o, ldo, s)
+                     : gram_mixed<false, double>(ctx, a, p, ld, ni, colscale, o, ldo, s))
+                : (C ? gram_fp64<true, double>(ctx, a, p, ld, ni, colscale, o, ldo, s)
+                     : gram_fp64<false, double>(ctx, a, p, ld, ni, colscale, o, ldo, s));
+        if (!rc) rc = C ? mirror<double, true>(ctx, o, ldo, ni, s) : mirror<double, false>(ctx, o, ldo, ni, s);
     }
     return rc;
 }
