@@ -328,6 +328,21 @@ int bem_gmres_ir(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo
  * that runs out is reported by the next bem_lstsq_refine. */
 int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld, double* colscale,
              int method, int out_dtype, void* out, int64_t ldo, void* stream);
+/* Cholesky factor of a Hermitian positive definite A = L L^H (the factor half
+ * of the lstsq call, BEM_manager.py:1049, applied to the normal matrix of
+ * bem_gram), in place, left in the tile-LU form of bem_lu_factor_tiled
+ * (unit lower L D^{-1} below the diagonal, U = D L^H on and above it,
+ * identity tile pivots in piv, explicit inverses of the 64 x 64 diagonal
+ * tiles in dinv, bem_lu_dinv_elems(n) elements), so bem_lu_solve_tiled,
+ * bem_refine_solve and bem_lstsq_refine take it.  A: BEM_C128 or BEM_F64 (the
+ * lower triangle is read).  Panels of 256 columns in FP64 on the FP64 tensor
+ * cores (DMMA); the trailing rank-256 Hermitian updates on the FP64 tensor
+ * cores (method BEM_PREC_FP64) or on tcgen05 from FP16 hi/lo splits of the
+ * panel with FP64 sums subtracted from the FP64 Schur complement
+ * (BEM_PREC_MIXED).  info: device int32, 0 or 1 + the first column whose
+ * pivot was not positive.  Queued without synchronising. */
+int bem_chol_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int method, int32_t* piv, void* dinv,
+                    int32_t* info, void* stream);
 /* The solve half of the same lstsq call (BEM_manager.py:1049): x (device, n,
  * FP64 real or complex, holding the initial guess) is refined by flexible
  * GMRES(restart) in FP64 on the scaled normal equations, with FP64 products

@@ -230,6 +230,20 @@ class Engine:
                                       method, _dtype_code(out), _ptr(out), out.stride(0), _stream_ptr()))
         return out, colscale
 
+    def chol_factor(self, A: torch.Tensor, tensor_cores=True):
+        """In-place Cholesky of the Hermitian positive definite A (complex128
+        or float64, lower triangle read), left in the tile-LU form; returns
+        (piv, dinv, info) like lu_factor_tiled (bem_chol_factor)."""
+        n = A.shape[0]
+        assert A.is_cuda and A.shape == (n, n) and A.stride(1) == 1 and A.dtype in (torch.complex128, torch.float64)
+        piv = torch.empty(n, dtype=torch.int32, device=A.device)
+        info = torch.zeros(1, dtype=torch.int32, device=A.device)
+        dinv = torch.empty(int(self.lib.bem_lu_dinv_elems(n)), dtype=torch.complex128, device=A.device)
+        method = L.PREC_MIXED if tensor_cores else L.PREC_FP64
+        self._check(self.lib.bem_chol_factor(self.ctx, _dtype_code(A), _ptr(A), n, A.stride(0), method, _ptr(piv),
+                                             _ptr(dinv), _ptr(info), _stream_ptr()))
+        return piv, dinv, info
+
     def lstsq_refine(self, A, P, colscale, LU, piv, dinv, b, x, tol=1e-14, maxit=60, restart=30, accept=1e-10):
         """Flexible GMRES in FP64 on the scaled normal equations of
         min ||[A; P] x - b|| (bem_lstsq_refine); x holds the initial guess.

@@ -409,20 +409,24 @@ class BEMManager:
         the normal equations against the FP64-stored A and P."""
         n = A.shape[0]
         mixed = self.solve_precision == "mixed"
-        # the factor is FP64 on both paths: the normal matrix of the
-        # 30722-unknown transmission problem has cond ~3e6, where an FP32
-        # factorisation no longer preconditions (measured: FGMRES stalls)
+        # the factor is a Cholesky with an FP64 Schur complement on both
+        # paths: the normal matrix of the 30722-unknown transmission problem
+        # has cond ~3e6, where an FP32 factorisation no longer preconditions
+        # (measured: FGMRES stalls); the mixed path forms its O(n^3) updates
+        # on the tcgen05 tensor cores
         d = torch.empty(n, dtype=torch.float64, device=A.device)
         Nm = torch.empty(n, n, dtype=A.dtype, device=A.device)
         self.engine.gram(A, P, Nm, d, tensor_cores=mixed)
-        piv, dinv, info = self.engine.lu_factor_tiled(Nm)
+        piv, dinv, info = self.engine.chol_factor(Nm, tensor_cores=mixed)
         x = torch.zeros(n, dtype=A.dtype, device=A.device)
         its, rr = self.engine.lstsq_refine(A, P, d, Nm, piv, dinv, b, x, tol=self.lstsq_tol,
                                            maxit=self.lstsq_maxit, restart=30, accept=self.lstsq_accept)
         if int(info.item()) > 0:
-            raise torch.linalg.LinAlgError("linalg.lstsq: the normal matrix of the stacked system is singular")
-        self.solve_info = {"factor": ("fp16-split tcgen05 normal matrix" if mixed else "fp64 DMMA normal matrix")
-                           + ", fp64 tile LU (DMMA updates), fp64 flexible GMRES",
+            raise torch.linalg.LinAlgError("linalg.lstsq: the stacked system is rank deficient (its normal matrix "
+                                           f"has no positive pivot in column {int(info.item()) - 1})")
+        self.solve_info = {"factor": ("fp16-split tcgen05 normal matrix, Cholesky with tcgen05 updates" if mixed
+                                      else "fp64 DMMA normal matrix, Cholesky with DMMA updates")
+                           + " (FP64 Schur complement), fp64 flexible GMRES",
                            "info": info, "refine_iters": its, "relres": rr}
         del Nm, dinv
         return x

@@ -74,6 +74,14 @@ int bem_take_factor_error(bem_ctx* ctx, int32_t value, cudaStream_t s);
 int bem_fgmres(bem_ctx* ctx, bool C, int64_t n, const std::function<int(const double*, double*)>& apply_op,
                const std::function<int(double*)>& precond, const double* b, double* x, double tol, int maxit,
                int restart, double accept, int* iters, double* relres, cudaStream_t s);
+// out[p][q] -= sum_k L[p][k] conj(L[q][k]) (FP64 out, lower 64 x 64 tiles;
+// real when !C) on the tcgen05 tensor cores from FP16 hi/lo splits of the
+// panel L (m x kb, ld), FP64 sums (bem_lstsq.cu).
+int bem_herk_tc_update(bem_ctx* ctx, bool C, const double* L, int64_t ld, int m, int kb, double* out, int64_t ldo,
+                       cudaStream_t s);
+// Explicit inverses of the 64 x 64 diagonal tiles of a tile-LU factor into
+// dinv (bem_tilelu.cu); dtype BEM_F64/C128/F32/C64.
+int bem_tile_inverses(bem_ctx* ctx, int dtype, const void* A, int64_t n, int64_t lda, void* dinv, cudaStream_t s);
 // Asynchronous preconditioner step of the refinement (bem_tilelu.cu).
 int bem_tiled_precond_async(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                             const void* dinv, const double* r, double** out, const int* skip, cudaStream_t s);

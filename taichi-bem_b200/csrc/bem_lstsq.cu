@@ -113,6 +113,30 @@ __global__ void __launch_bounds__(256) split_kernel(const double* A, const doubl
     }
 }
 
+// FP16 hi/lo split of a panel L (m x kb, row-major, ld) for the Hermitian
+// update L L^H: T[2p + c][k] = (Re, -Im)[c] of L[p][k] (real: T[p][k] =
+// L[p][k]), zero padding to Rp x Kp.  Rows of L map to rows of T: no
+// transposition.  Grid: (Kp / 64, rows of T / 4), 256 threads (4 rows x 64 k).
+template <bool C>
+__global__ void __launch_bounds__(256) panel_split_kernel(const double* L, int64_t ld, int m, int kb, __half* Thi,
+                                                          __half* Tlo, int64_t Kp, int64_t Rp) {
+    const int k = blockIdx.x * 64 + (threadIdx.x & 63);
+    const int64_t i = (int64_t)blockIdx.y * 4 + (threadIdx.x >> 6);
+    if (i >= Rp) return;
+    double v = 0.0;
+    if (C) {
+        const int64_t p = i >> 1;
+        const int c = (int)(i & 1);
+        if (p < m && k < kb) v = c ? -L[2 * (p * ld + k) + 1] : L[2 * (p * ld + k)];
+    } else if (i < m && k < kb) {
+        v = L[i * ld + k];
+    }
+    const float f = (float)v;
+    const __half h = __float2half_rn(f);
+    Thi[i * Kp + k] = h;
+    Tlo[i * Kp + k] = __float2half_rn((f - __half2float(h)) * 2048.0f);
+}
+
 // lower-triangle tile t (row-major order, diagonal included) -> (bi, bj), bi >= bj
 __device__ __forceinline__ void tri_tile(int t, int& bi, int& bj) {
     int i = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
@@ -224,7 +248,8 @@ template <bool C, typename OT>
 __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
                                                                  const __grid_constant__ CUtensorMap tm_lo,
                                                                  int nchunks, int kseg, OT* out, int64_t ldo,
-                                                                 int n, int32_t* err) {
+                                                                 int n, double alpha, int accumulate,
+                                                                 int32_t* err) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
@@ -377,15 +402,19 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                         const double re = odd ? (pa + b) : (a + pb);
                         // a Hermitian matrix has a real diagonal (the two products are equal in exact arithmetic)
                         const double im = p == qc ? 0.0 : (odd ? (pb - a) : (b - pa));
-                        out[2 * ((int64_t)p * ldo + qc)] = (OT)re;
-                        out[2 * ((int64_t)p * ldo + qc) + 1] = (OT)im;
+                        OT* o = out + 2 * ((int64_t)p * ldo + qc);
+                        o[0] = (OT)(accumulate ? (double)o[0] + alpha * re : alpha * re);
+                        o[1] = (OT)(accumulate ? (double)o[1] + alpha * im : alpha * im);
                     }
                 }
             } else if (r < n) {
 #pragma unroll
                 for (int m = 0; m < EC; ++m) {
                     const int qc = c0 + m;
-                    if (qc < n) out[(int64_t)r * ldo + qc] = (OT)acc[m];
+                    if (qc < n) {
+                        OT* o = out + (int64_t)r * ldo + qc;
+                        *o = (OT)(accumulate ? (double)*o + alpha * acc[m] : alpha * acc[m]);
+                    }
                 }
             }
         }
@@ -668,6 +697,10 @@ int column_scale(bem_ctx* ctx, bool C, const double* A, const double* P, int64_t
 }
 
 template <bool C, typename OT>
+int launch_gram_tc(bem_ctx* ctx, __half* Thi, __half* Tlo, int64_t Rp, int64_t Kp, OT* out, int64_t ldo, int n,
+                   double alpha, int accumulate, cudaStream_t s);
+
+template <bool C, typename OT>
 int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n, const double* d, OT* out,
                int64_t ldo, cudaStream_t s) {
     const int W = C ? 2 : 1;
@@ -675,8 +708,6 @@ int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n
     const int64_t Rp = (rows + GT_BM - 1) / GT_BM * GT_BM;  // padded rows
     const int64_t Kp = (2 * (int64_t)n + GT_BK - 1) / GT_BK * GT_BK;
     if (Kp > (int64_t)1 << 31 || Rp / GT_BM > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "gram: n too large");
-    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_tiled();
-    if (!enc) return bem_fail(ctx, BEM_ERR_CUDA, "gram: cuTensorMapEncodeTiled is not available");
     void* ws = nullptr;
     const size_t arr = (size_t)Rp * (size_t)Kp * sizeof(__half);
     if (int rc = big_ws(ctx, 2 * arr, &ws)) return rc;
@@ -690,6 +721,16 @@ int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n
         ctx->launches++;
         if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "split_kernel")) return rc;
     }
+    return launch_gram_tc<C, OT>(ctx, Thi, Tlo, Rp, Kp, out, ldo, n, 1.0, 0, s);
+}
+
+// The tcgen05 product over split operands Thi / Tlo (Rp x Kp FP16, row
+// stride Kp): out = alpha S (+ out when accumulate), lower tiles of S.
+template <bool C, typename OT>
+int launch_gram_tc(bem_ctx* ctx, __half* Thi, __half* Tlo, int64_t Rp, int64_t Kp, OT* out, int64_t ldo, int n,
+                   double alpha, int accumulate, cudaStream_t s) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_tiled();
+    if (!enc) return bem_fail(ctx, BEM_ERR_CUDA, "gram: cuTensorMapEncodeTiled is not available");
     CUtensorMap tm[2];
     for (int h = 0; h < 2; ++h) {
         cuuint64_t gdim[2] = {(cuuint64_t)Kp, (cuuint64_t)Rp};
@@ -710,7 +751,7 @@ int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n
     cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
     const int kseg = ctx->tune[BEM_TUNE_GRAM_KSEG] > 0 ? ctx->tune[BEM_TUNE_GRAM_KSEG] : GT_KSEG_DEFAULT;
     gram_tc_kernel<C, OT><<<(unsigned)tiles, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, out, ldo,
-                                                                   n, ctx->flags + 5);
+                                                                       n, alpha, accumulate, ctx->flags + 5);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_tc_kernel");
 }
@@ -740,6 +781,29 @@ int mirror(bem_ctx* ctx, T* out, int64_t ldo, int n, cudaStream_t s) {
 }
 
 }  // namespace
+
+int bem_herk_tc_update(bem_ctx* ctx, bool C, const double* L, int64_t ld, int m, int kb, double* out, int64_t ldo,
+                       cudaStream_t s) {
+    if (m <= 0 || kb <= 0) return BEM_OK;
+    const int W = C ? 2 : 1;
+    const int64_t Rp = ((int64_t)W * m + GT_BM - 1) / GT_BM * GT_BM;
+    const int64_t Kp = ((int64_t)kb + GT_BK - 1) / GT_BK * GT_BK;
+    if (Rp / GT_BM > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "herk update: m too large");
+    void* ws = nullptr;
+    const size_t arr = (size_t)Rp * (size_t)Kp * sizeof(__half);
+    if (int rc = big_ws(ctx, 2 * arr, &ws)) return rc;
+    __half* Thi = static_cast<__half*>(ws);
+    __half* Tlo = reinterpret_cast<__half*>(static_cast<char*>(ws) + arr);
+    dim3 grid((unsigned)(Kp / 64), (unsigned)((Rp + 3) / 4));
+    if (C)
+        panel_split_kernel<true><<<grid, 256, 0, s>>>(L, ld, m, kb, Thi, Tlo, Kp, Rp);
+    else
+        panel_split_kernel<false><<<grid, 256, 0, s>>>(L, ld, m, kb, Thi, Tlo, Kp, Rp);
+    ctx->launches++;
+    if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "panel_split_kernel")) return rc;
+    return C ? launch_gram_tc<true, double>(ctx, Thi, Tlo, Rp, Kp, out, ldo, m, -1.0, 1, s)
+             : launch_gram_tc<false, double>(ctx, Thi, Tlo, Rp, Kp, out, ldo, m, -1.0, 1, s);
+}
 
 extern "C" {
 

@@ -1020,6 +1020,25 @@ int bem_lu_solve_tiled(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64
 
 }  // extern "C"
 
+template <typename T, bool C>
+int tile_inverses_t(bem_ctx* ctx, const T* A, int64_t n, int64_t lda, CE<T>* dinv, cudaStream_t s) {
+    const size_t ismem = inv_smem_bytes(sizeof(CE<T>));
+    cudaFuncSetAttribute(tile_inv_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ismem);
+    tile_inv_kernel<T, C><<<(unsigned)((n + LU_T - 1) / LU_T), 256, ismem, s>>>(A, lda, (int)n, dinv);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "tile_inv_kernel");
+}
+
+int bem_tile_inverses(bem_ctx* ctx, int dtype, const void* A, int64_t n, int64_t lda, void* dinv, cudaStream_t s) {
+    switch (dtype) {
+        case BEM_F64: return tile_inverses_t<double, false>(ctx, (const double*)A, n, lda, (CE<double>*)dinv, s);
+        case BEM_C128: return tile_inverses_t<double, true>(ctx, (const double*)A, n, lda, (CE<double>*)dinv, s);
+        case BEM_F32: return tile_inverses_t<float, false>(ctx, (const float*)A, n, lda, (CE<float>*)dinv, s);
+        case BEM_C64: return tile_inverses_t<float, true>(ctx, (const float*)A, n, lda, (CE<float>*)dinv, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "tile inverses: unknown dtype");
+    }
+}
+
 int bem_tiled_precond_async(bem_ctx* ctx, int dtype, const void* LU, int64_t n, int64_t lda, const int32_t* piv,
                             const void* dinv, const double* r, double** out, const int* skip, cudaStream_t s) {
     switch (dtype) {
