@@ -161,15 +161,17 @@ __device__ __forceinline__ void tri_tile(int t, int& bi, int& bj) {
 // to its FP64 running sums while the MMAs of segment g + 1 run.  The tensor
 // core's FP32 accumulation does not round to nearest: its error grows with
 // the number of MMA steps a TMEM sum sees (measured on the 30722-unknown
-// normal matrix: 2e-5 relative for segments of 64 stages, 2e-6 for 4), so
-// the default folds every stage (4 MMA steps per sum), and the FP64 running
-// sums keep the segment count from adding its own rounding.
+// normal matrix: 2e-5 relative for segments of 64 stages, 1.5e-6 for 4,
+// 8e-7 for 2, 4e-7 for 1), so the default folds every two stages (8 MMA steps
+// per sum: the fastest setting at which the least-squares iteration still
+// converges in about 6 steps), and the FP64 running sums keep the segment
+// count from adding its own rounding.
 constexpr int GT_BM = 128;
 constexpr int GT_BK = 64;
 constexpr int GT_STAGES = 3;
 constexpr int GT_TILE = GT_BM * GT_BK * 2;  // bytes of one 128 x 64 FP16 tile
 constexpr int GT_STAGE = 4 * GT_TILE;
-constexpr int GT_KSEG_DEFAULT = 1;
+constexpr int GT_KSEG_DEFAULT = 2;
 constexpr int GT_EPI_WARPS = 8;
 constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
 constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
@@ -387,35 +389,49 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
             const int r = bi * GT_BM + 32 * q + lane;  // real row of S
             const int c0 = bj * GT_BM + half * EC;     // first real column of this thread
             if (C) {
-                // rows 2p (even lane) and 2p + 1 (odd lane); the even lane writes
-                // the first half of this thread's complex columns, the odd lane the second
+                // rows 2p (even lane) and 2p + 1 (odd lane): the even lane takes the
+                // first EC / 4 of this thread's complex columns, the odd lane the rest
+                constexpr int NQ = EC / 4;
                 const int p = r >> 1;
                 const bool odd = lane & 1;
+                double vre[NQ], vim[NQ];
 #pragma unroll
                 for (int m = 0; m < EC / 2; ++m) {
                     const double a = acc[2 * m], b = acc[2 * m + 1];
                     const double pa = __shfl_xor_sync(0xffffffffu, a, 1), pb = __shfl_xor_sync(0xffffffffu, b, 1);
-                    const bool mine = odd ? (m >= EC / 4) : (m < EC / 4);
-                    const int qc = (c0 >> 1) + m;
-                    if (mine && p < n && qc < n) {
+                    if (odd == (m >= NQ)) {
                         // even: (a, b) = S[2p][2q, 2q+1], partner = S[2p+1]; odd: the roles swap
-                        const double re = odd ? (pa + b) : (a + pb);
+                        const int qc = (c0 >> 1) + m;
+                        vre[m % NQ] = odd ? (pa + b) : (a + pb);
                         // a Hermitian matrix has a real diagonal (the two products are equal in exact arithmetic)
-                        const double im = p == qc ? 0.0 : (odd ? (pb - a) : (b - pa));
-                        OT* o = out + 2 * ((int64_t)p * ldo + qc);
-                        o[0] = (OT)(accumulate ? (double)o[0] + alpha * re : alpha * re);
-                        o[1] = (OT)(accumulate ? (double)o[1] + alpha * im : alpha * im);
+                        vim[m % NQ] = p == qc ? 0.0 : (odd ? (pb - a) : (b - pa));
+                    }
+                }
+                const int qbase = (c0 >> 1) + (odd ? NQ : 0);
+                OT* orow = out + 2 * ((int64_t)p * ldo + qbase);
+                // the old values first (independent loads in flight together), then the stores
+                double ore[NQ], oim[NQ];
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    const bool in = p < n && qbase + j < n;
+                    ore[j] = (accumulate && in) ? (double)orow[2 * j] : 0.0;
+                    oim[j] = (accumulate && in) ? (double)orow[2 * j + 1] : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    if (p < n && qbase + j < n) {
+                        orow[2 * j] = (OT)(ore[j] + alpha * vre[j]);
+                        orow[2 * j + 1] = (OT)(oim[j] + alpha * vim[j]);
                     }
                 }
             } else if (r < n) {
+                OT* orow = out + (int64_t)r * ldo + c0;
+                double old[EC];
 #pragma unroll
-                for (int m = 0; m < EC; ++m) {
-                    const int qc = c0 + m;
-                    if (qc < n) {
-                        OT* o = out + (int64_t)r * ldo + qc;
-                        *o = (OT)(accumulate ? (double)*o + alpha * acc[m] : alpha * acc[m]);
-                    }
-                }
+                for (int m = 0; m < EC; ++m) old[m] = (accumulate && c0 + m < n) ? (double)orow[m] : 0.0;
+#pragma unroll
+                for (int m = 0; m < EC; ++m)
+                    if (c0 + m < n) orow[m] = (OT)(old[m] + alpha * acc[m]);
             }
         }
     }
