@@ -149,6 +149,9 @@ __device__ __forceinline__ void tri_tile(int t, int& bi, int& bj) {
 // ---------------------------------------------------------------------------
 // tcgen05 Gram kernel: S_tile = T[rows bi] T[rows bj]^T over all K
 // ---------------------------------------------------------------------------
+// Persistent: one CTA per SM takes tiles blockIdx.x, + gridDim.x, ...; the
+// stage ring and the TMEM accumulator sets run on across tiles, so loads and
+// MMAs of the next tile overlap the epilogue of the last one.
 // Warp 0 is the TMA producer, warp 1 allocates TMEM and issues the MMAs
 // (one elected thread), warps 2-9 are the epilogue (warp w reads TMEM lanes
 // 32 (w % 4) .. and half (w - 2) / 4 of the columns).  A stage holds the hi and lo 128 x 64 FP16 tiles of both
@@ -249,8 +252,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 template <bool C, typename OT>
 __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
                                                                  const __grid_constant__ CUtensorMap tm_lo,
-                                                                 int nchunks, int kseg, OT* out, int64_t ldo,
-                                                                 int n, double alpha, int accumulate,
+                                                                 int nchunks, int kseg, int ntiles, OT* out,
+                                                                 int64_t ldo, int n, double alpha, int accumulate,
                                                                  int32_t* err) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
@@ -259,9 +262,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                            ~uintptr_t(1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    int bi, bj;
-    tri_tile(blockIdx.x, bi, bj);
-    const int nseg = (nchunks + kseg - 1) / kseg;
+    const int nseg = (nchunks + kseg - 1) / kseg;  // per tile
 
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -292,40 +293,47 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         if (lane == 0) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_hi)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_lo)) : "memory");
-            for (int c = 0; c < nchunks; ++c) {
-                const int s = c % GT_STAGES;
-                if (c >= GT_STAGES &&
-                    !mbar_wait(smem_u32(&empty_bar[s]), (uint32_t)((c / GT_STAGES - 1) & 1), &s_abort)) {
-                    s_abort = 1;
-                    break;
+            uint32_t cg = 0;  // chunks issued by this CTA (the stage ring runs across tiles)
+            for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
+                int bi, bj;
+                tri_tile(t, bi, bj);
+                for (int c = 0; c < nchunks; ++c, ++cg) {
+                    const int s = (int)(cg % GT_STAGES);
+                    if (cg >= GT_STAGES &&
+                        !mbar_wait(smem_u32(&empty_bar[s]), (uint32_t)((cg / GT_STAGES - 1) & 1), &s_abort)) {
+                        s_abort = 1;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(&full_bar[s]);
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(GT_STAGE)
+                                 : "memory");
+                    const uint32_t st = smem_u32(smem + (size_t)s * GT_STAGE);
+                    const int x = c * GT_BK;
+                    tma_load(st, &tm_hi, fb, x, bi * GT_BM);
+                    tma_load(st + GT_TILE, &tm_lo, fb, x, bi * GT_BM);
+                    tma_load(st + 2 * GT_TILE, &tm_hi, fb, x, bj * GT_BM);
+                    tma_load(st + 3 * GT_TILE, &tm_lo, fb, x, bj * GT_BM);
                 }
-                const uint32_t fb = smem_u32(&full_bar[s]);
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(GT_STAGE)
-                             : "memory");
-                const uint32_t st = smem_u32(smem + (size_t)s * GT_STAGE);
-                const int x = c * GT_BK;
-                tma_load(st, &tm_hi, fb, x, bi * GT_BM);
-                tma_load(st + GT_TILE, &tm_lo, fb, x, bi * GT_BM);
-                tma_load(st + 2 * GT_TILE, &tm_hi, fb, x, bj * GT_BM);
-                tma_load(st + 3 * GT_TILE, &tm_lo, fb, x, bj * GT_BM);
             }
         }
     } else if (warp == 1) {
         // ---- MMA issuer ----
         if (lane == 0) {
+            uint32_t cg = 0, gg = 0;  // chunks and segments consumed by this CTA
+            for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
             int c = 0;
-            for (int g = 0; g < nseg && !s_abort; ++g) {
-                const int buf = g & 1;
-                if (g >= 2 && !mbar_wait(smem_u32(&acc_empty[buf]), (uint32_t)((g / 2 - 1) & 1), &s_abort)) {
+            for (int g = 0; g < nseg && !s_abort; ++g, ++gg) {
+                const int buf = (int)(gg & 1);
+                if (gg >= 2 && !mbar_wait(smem_u32(&acc_empty[buf]), (uint32_t)((gg / 2 - 1) & 1), &s_abort)) {
                     s_abort = 1;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d1 = tmem + (uint32_t)(buf * 256), d2 = d1 + 128;
                 const int cend = min(nchunks, (g + 1) * kseg);
-                for (int first = 1; c < cend; ++c, first = 0) {
-                    const int s = c % GT_STAGES;
-                    if (!mbar_wait(smem_u32(&full_bar[s]), (uint32_t)((c / GT_STAGES) & 1), &s_abort)) {
+                for (int first = 1; c < cend; ++c, ++cg, first = 0) {
+                    const int s = (int)(cg % GT_STAGES);
+                    if (!mbar_wait(smem_u32(&full_bar[s]), (uint32_t)((cg / GT_STAGES) & 1), &s_abort)) {
                         s_abort = 1;
                         break;
                     }
@@ -352,19 +360,24 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                                  smem_u32(&acc_full[buf]))
                              : "memory");
             }
+            }
         }
     } else {
         // ---- epilogue: FP64 running sums of the segments, then the complex combine ----
         constexpr int EC = GT_BM / 2;  // columns per epilogue thread
         const int q = warp & 3, half = (warp - 2) >> 2;
+        uint32_t gg = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        int bi, bj;
+        tri_tile(t, bi, bj);
         double acc[EC];
 #pragma unroll
         for (int i = 0; i < EC; ++i) acc[i] = 0.0;
-        bool ok = true;
-        for (int g = 0; g < nseg; ++g) {
-            const int buf = g & 1;
+        for (int g = 0; g < nseg; ++g, ++gg) {
+            const int buf = (int)(gg & 1);
             // every lane waits; the vote keeps the warp's TMEM loads and shuffles uniform
-            const bool got = mbar_wait(smem_u32(&acc_full[buf]), (uint32_t)((g / 2) & 1), &s_abort);
+            const bool got = mbar_wait(smem_u32(&acc_full[buf]), (uint32_t)((gg / 2) & 1), &s_abort);
             if (!__all_sync(0xffffffffu, got)) {
                 ok = false;
                 s_abort = 1;
@@ -433,6 +446,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                 for (int m = 0; m < EC; ++m)
                     if (c0 + m < n) orow[m] = (OT)(old[m] + alpha * acc[m]);
             }
+        }
         }
     }
     if (s_abort && tid == 0) atomicExch(err, BEM_ERR_TIMEOUT);
@@ -766,8 +780,10 @@ int launch_gram_tc(bem_ctx* ctx, __half* Thi, __half* Tlo, int64_t Rp, int64_t K
         return rc;
     cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
     const int kseg = ctx->tune[BEM_TUNE_GRAM_KSEG] > 0 ? ctx->tune[BEM_TUNE_GRAM_KSEG] : GT_KSEG_DEFAULT;
-    gram_tc_kernel<C, OT><<<(unsigned)tiles, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, out, ldo,
-                                                                       n, alpha, accumulate, ctx->flags + 5);
+    // persistent: one CTA per SM (its shared memory and 512 TMEM columns allow no second), tiles in turn
+    const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctx->num_sms);
+    gram_tc_kernel<C, OT><<<grid, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, (int)tiles, out,
+                                                            ldo, n, alpha, accumulate, ctx->flags + 5);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_tc_kernel");
 }
