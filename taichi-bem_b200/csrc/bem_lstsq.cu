@@ -159,29 +159,25 @@ __device__ __forceinline__ void tri_tile(int t, int& bi, int& bj) {
 // shared memory; the matching UMMA descriptors are K-major SWIZZLE_128B
 // (8-row groups 1024 bytes apart), advanced by 32 bytes per K = 16 step.
 // Per K = 16 step three MMAs: D1 += A_hi B_hi, D2 += A_hi B_lo + A_lo B_hi.
-// K is accumulated in segments of kseg stages.  The tensor core's FP32
-// accumulation does not round to nearest: its error grows with the number of
-// MMA steps a TMEM sum sees (measured on the 30722-unknown normal matrix: 2e-5
-// relative for segments of 64 stages, 1.5e-6 for 4, 4e-7 for 1).  So the
-// hi*hi sum D1 is folded every segment (default: every stage, 4 MMA steps per
-// sum) into compensated (Kahan) FP32 sums in the epilogue's registers, two
-// TMEM sets alternating so the MMAs of segment g + 1 run while segment g is
-// read; the cross terms D2, scaled by 2^-11 in the result, accumulate over
-// GT_D2SEG segments in two further TMEM sets.  The epilogue reads 64 of the
-// 128 D1 columns of its lane quadrant per segment and does four FP32 adds per
-// value, so it stays shorter than the segment's MMAs.
+// K is accumulated in segments of kseg stages; two TMEM accumulator sets
+// alternate, so the epilogue adds segment g (D1 + 2^-11 D2, formed in FP32)
+// to its FP64 running sums while the MMAs of segment g + 1 run.  The tensor
+// core's FP32 accumulation does not round to nearest: its error grows with
+// the number of MMA steps a TMEM sum sees (measured on the 30722-unknown
+// normal matrix: 2e-5 relative for segments of 64 stages, 1.5e-6 for 4,
+// 8e-7 for 2, 4e-7 for 1), so the default folds every two stages (8 MMA steps
+// per sum: the fastest setting at which the least-squares iteration still
+// converges in about 6 steps), and the FP64 running sums keep the segment
+// count from adding its own rounding.
 constexpr int GT_BM = 128;
 constexpr int GT_BK = 64;
 constexpr int GT_STAGES = 3;
 constexpr int GT_TILE = GT_BM * GT_BK * 2;  // bytes of one 128 x 64 FP16 tile
 constexpr int GT_STAGE = 4 * GT_TILE;
-constexpr int GT_KSEG_DEFAULT = 1;
+constexpr int GT_KSEG_DEFAULT = 2;
 constexpr int GT_EPI_WARPS = 8;
-// segments per fold of the cross-term sums (hi*lo + lo*hi, scaled by 2^-11 in
-// the result, so their longer TMEM chains add ~1e-8 relative)
-constexpr int GT_D2SEG = 16;
 constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
-constexpr uint32_t GT_TMEM_COLS = 512;  // D1 (hi*hi) x 2 sets + D2 (cross terms) x 2 sets, 128 columns each
+constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
 constexpr uint32_t GT_SPIN_CAP = 1u << 24;
 constexpr size_t GT_SMEM = (size_t)GT_STAGES * GT_STAGE + 1024;
 // instruction descriptor, kind::f16: D F32 (bit 4), A and B F16 (0), both
@@ -261,7 +257,6 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                                                                  int32_t* err) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
-    __shared__ __align__(8) uint64_t d2_full[2], d2_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int s_abort;
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -283,9 +278,6 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         for (int b = 0; b < 2; ++b) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&acc_full[b])) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acc_empty[b])), "r"(GT_EPI_WARPS)
-                         : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&d2_full[b])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&d2_empty[b])), "r"(GT_EPI_WARPS)
                          : "memory");
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -327,25 +319,17 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
     } else if (warp == 1) {
         // ---- MMA issuer ----
         if (lane == 0) {
-            uint32_t cg = 0, gg = 0, sg = 0;  // chunks, segments and D2 super-segments consumed by this CTA
+            uint32_t cg = 0, gg = 0;  // chunks and segments consumed by this CTA
             for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
             int c = 0;
             for (int g = 0; g < nseg && !s_abort; ++g, ++gg) {
                 const int buf = (int)(gg & 1);
-                const int b2 = (int)(sg & 1);
-                const bool ss_first = (g % GT_D2SEG) == 0;
-                const bool ss_last = ((g + 1) % GT_D2SEG) == 0 || g == nseg - 1;
                 if (gg >= 2 && !mbar_wait(smem_u32(&acc_empty[buf]), (uint32_t)((gg / 2 - 1) & 1), &s_abort)) {
                     s_abort = 1;
                     break;
                 }
-                if (ss_first && sg >= 2 &&
-                    !mbar_wait(smem_u32(&d2_empty[b2]), (uint32_t)((sg / 2 - 1) & 1), &s_abort)) {
-                    s_abort = 1;
-                    break;
-                }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d1 = tmem + (uint32_t)(buf * 128), d2 = tmem + 256u + (uint32_t)(b2 * 128);
+                const uint32_t d1 = tmem + (uint32_t)(buf * 256), d2 = d1 + 128;
                 const int cend = min(nchunks, (g + 1) * kseg);
                 for (int first = 1; c < cend; ++c, ++cg, first = 0) {
                     const int s = (int)(cg % GT_STAGES);
@@ -361,10 +345,9 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                         const uint64_t a_hi = desc_sw128(st + ko), a_lo = desc_sw128(st + GT_TILE + ko);
                         const uint64_t b_hi = desc_sw128(st + 2 * GT_TILE + ko),
                                        b_lo = desc_sw128(st + 3 * GT_TILE + ko);
-                        const uint32_t acc1 = (first && ks == 0) ? 0u : 1u;
-                        const uint32_t acc2 = (first && ks == 0 && ss_first) ? 0u : 1u;
-                        mma_f16(d1, a_hi, b_hi, acc1);
-                        mma_f16(d2, a_hi, b_lo, acc2);
+                        const uint32_t acc = (first && ks == 0) ? 0u : 1u;
+                        mma_f16(d1, a_hi, b_hi, acc);
+                        mma_f16(d2, a_hi, b_lo, acc);
                         mma_f16(d2, a_lo, b_hi, 1u);
                     }
                     asm volatile(
@@ -376,13 +359,6 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&acc_full[buf]))
                              : "memory");
-                if (ss_last) {
-                    asm volatile(
-                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                            smem_u32(&d2_full[b2]))
-                        : "memory");
-                    ++sg;
-                }
             }
             }
         }
@@ -390,16 +366,14 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         // ---- epilogue: FP64 running sums of the segments, then the complex combine ----
         constexpr int EC = GT_BM / 2;  // columns per epilogue thread
         const int q = warp & 3, half = (warp - 2) >> 2;
-        uint32_t gg = 0, sg = 0;
+        uint32_t gg = 0;
         bool ok = true;
-        const uint32_t lane_base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(half * EC);
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         int bi, bj;
         tri_tile(t, bi, bj);
-        // hi*hi segments in compensated (Kahan) FP32 sums s1 - c1, cross terms in s2
-        float s1[EC], c1[EC], s2[EC];
+        double acc[EC];
 #pragma unroll
-        for (int i = 0; i < EC; ++i) s1[i] = c1[i] = s2[i] = 0.f;
+        for (int i = 0; i < EC; ++i) acc[i] = 0.0;
         for (int g = 0; g < nseg; ++g, ++gg) {
             const int buf = (int)(gg & 1);
             // every lane waits; the vote keeps the warp's TMEM loads and shuffles uniform
@@ -410,56 +384,20 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * 256 + half * EC);
 #pragma unroll
-            for (int cc = 0; cc < EC; cc += 32) {
+            for (int cc = 0; cc < EC; cc += 16) {
                 float v1[16], v2[16];
-                tmem_ld16(lane_base + (uint32_t)(buf * 128 + cc), v1);
-                tmem_ld16(lane_base + (uint32_t)(buf * 128 + cc + 16), v2);
+                tmem_ld16(base + cc, v1);
+                tmem_ld16(base + 128 + cc, v2);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float y1 = v1[i] - c1[cc + i], t1 = s1[cc + i] + y1;
-                    c1[cc + i] = (t1 - s1[cc + i]) - y1;
-                    s1[cc + i] = t1;
-                    const float y2 = v2[i] - c1[cc + 16 + i], t2 = s1[cc + 16 + i] + y2;
-                    c1[cc + 16 + i] = (t2 - s1[cc + 16 + i]) - y2;
-                    s1[cc + 16 + i] = t2;
-                }
+                for (int i = 0; i < 16; ++i) acc[cc + i] += (double)fmaf(v2[i], 4.8828125e-4f, v1[i]);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[buf])) : "memory");
-            if (((g + 1) % GT_D2SEG) == 0 || g == nseg - 1) {
-                const int b2 = (int)(sg & 1);
-                const bool got2 = mbar_wait(smem_u32(&d2_full[b2]), (uint32_t)((sg / 2) & 1), &s_abort);
-                if (!__all_sync(0xffffffffu, got2)) {
-                    ok = false;
-                    s_abort = 1;
-                    break;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-                for (int cc = 0; cc < EC; cc += 32) {
-                    float v1[16], v2[16];
-                    tmem_ld16(lane_base + 256u + (uint32_t)(b2 * 128 + cc), v1);
-                    tmem_ld16(lane_base + 256u + (uint32_t)(b2 * 128 + cc + 16), v2);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        s2[cc + i] += v1[i];
-                        s2[cc + 16 + i] += v2[i];
-                    }
-                }
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncwarp();
-                if (lane == 0)
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&d2_empty[b2])) : "memory");
-                ++sg;
-            }
         }
-        double acc[EC];
-#pragma unroll
-        for (int i = 0; i < EC; ++i) acc[i] = ((double)s1[i] - (double)c1[i]) + 4.8828125e-4 * (double)s2[i];
         if (ok) {
             const int r = bi * GT_BM + 32 * q + lane;  // real row of S
             const int c0 = bj * GT_BM + half * EC;     // first real column of this thread
