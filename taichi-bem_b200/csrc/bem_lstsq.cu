@@ -180,6 +180,7 @@ constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
 constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
 constexpr uint32_t GT_SPIN_CAP = 1u << 24;
 constexpr size_t GT_SMEM = (size_t)GT_STAGES * GT_STAGE + 1024;
+constexpr int GT_STG_LD = 64 + 1;  // padded row of the epilogue's staging buffer (doubles)
 // instruction descriptor, kind::f16: D F32 (bit 4), A and B F16 (0), both
 // K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
 constexpr uint32_t GT_IDESC = (1u << 4) | ((uint32_t)(GT_BM >> 3) << 17) | ((uint32_t)(GT_BM >> 4) << 24);
@@ -248,6 +249,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(u[i]);
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+    uint32_t u[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7])
+                 : "r"(taddr)
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(u[i]);
+}
+
 // out: complex (C, interleaved pairs) or real N x N matrix of OT (float or double), ld in elements
 template <bool C, typename OT>
 __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
@@ -259,6 +270,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int s_abort;
+    __shared__ double s_stage[GT_EPI_WARPS][8 * GT_STG_LD];  // epilogue staging, eight real rows per warp
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                            ~uintptr_t(1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -386,13 +398,13 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * 256 + half * EC);
 #pragma unroll
-            for (int cc = 0; cc < EC; cc += 16) {
-                float v1[16], v2[16];
-                tmem_ld16(base + cc, v1);
-                tmem_ld16(base + 128 + cc, v2);
+            for (int cc = 0; cc < EC; cc += 8) {
+                float v1[8], v2[8];
+                tmem_ld8(base + cc, v1);
+                tmem_ld8(base + 128 + cc, v2);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int i = 0; i < 16; ++i) acc[cc + i] += (double)fmaf(v2[i], 4.8828125e-4f, v1[i]);
+                for (int i = 0; i < 8; ++i) acc[cc + i] += (double)fmaf(v2[i], 4.8828125e-4f, v1[i]);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
@@ -402,40 +414,46 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
             const int r = bi * GT_BM + 32 * q + lane;  // real row of S
             const int c0 = bj * GT_BM + half * EC;     // first real column of this thread
             if (C) {
-                // rows 2p (even lane) and 2p + 1 (odd lane): the even lane takes the
-                // first EC / 4 of this thread's complex columns, the odd lane the rest
-                constexpr int NQ = EC / 4;
-                const int p = r >> 1;
-                const bool odd = lane & 1;
-                double vre[NQ], vim[NQ];
+                // coalesced read-modify-write: the warp's 32 real rows pass through
+                // shared memory eight at a time (four complex rows); lane l then forms
+                // complex column l of each,
+                //   N[p][q] = (S[2p][2q] + S[2p+1][2q+1]) + i (S[2p][2q+1] - S[2p+1][2q]),
+                // so each access covers 32 contiguous complex entries
+                double* stg = s_stage[warp - 2];  // [8][GT_STG_LD]
+                const int pw0 = (bi * GT_BM + 32 * q) >> 1;  // first complex row of this warp
+                const int qc = (c0 >> 1) + lane;
 #pragma unroll
-                for (int m = 0; m < EC / 2; ++m) {
-                    const double a = acc[2 * m], b = acc[2 * m + 1];
-                    const double pa = __shfl_xor_sync(0xffffffffu, a, 1), pb = __shfl_xor_sync(0xffffffffu, b, 1);
-                    if (odd == (m >= NQ)) {
-                        // even: (a, b) = S[2p][2q, 2q+1], partner = S[2p+1]; odd: the roles swap
-                        const int qc = (c0 >> 1) + m;
-                        vre[m % NQ] = odd ? (pa + b) : (a + pb);
-                        // a Hermitian matrix has a real diagonal (the two products are equal in exact arithmetic)
-                        vim[m % NQ] = p == qc ? 0.0 : (odd ? (pb - a) : (b - pa));
+                for (int c4 = 0; c4 < 4; ++c4) {
+                    if ((lane >> 3) == c4) {
+#pragma unroll
+                        for (int m = 0; m < EC; ++m) stg[(lane & 7) * GT_STG_LD + m] = acc[m];
                     }
-                }
-                const int qbase = (c0 >> 1) + (odd ? NQ : 0);
-                OT* orow = out + 2 * ((int64_t)p * ldo + qbase);
-                // the old values first (independent loads in flight together), then the stores
-                double ore[NQ], oim[NQ];
+                    __syncwarp();
+                    double nre[4], nim[4], ore[4], oim[4];
 #pragma unroll
-                for (int j = 0; j < NQ; ++j) {
-                    const bool in = p < n && qbase + j < n;
-                    ore[j] = (accumulate && in) ? (double)orow[2 * j] : 0.0;
-                    oim[j] = (accumulate && in) ? (double)orow[2 * j + 1] : 0.0;
-                }
-#pragma unroll
-                for (int j = 0; j < NQ; ++j) {
-                    if (p < n && qbase + j < n) {
-                        orow[2 * j] = (OT)(ore[j] + alpha * vre[j]);
-                        orow[2 * j + 1] = (OT)(oim[j] + alpha * vim[j]);
+                    for (int ri = 0; ri < 4; ++ri) {
+                        const double* e = stg + (2 * ri) * GT_STG_LD + 2 * lane;
+                        const double* o = stg + (2 * ri + 1) * GT_STG_LD + 2 * lane;
+                        const int pr = pw0 + 4 * c4 + ri;
+                        nre[ri] = e[0] + o[1];
+                        nim[ri] = pr == qc ? 0.0 : e[1] - o[0];  // a Hermitian matrix has a real diagonal
+                        ore[ri] = oim[ri] = 0.0;
+                        if (accumulate && pr < n && qc < n) {
+                            const OT* ot = out + 2 * ((int64_t)pr * ldo + qc);
+                            ore[ri] = (double)ot[0];
+                            oim[ri] = (double)ot[1];
+                        }
                     }
+#pragma unroll
+                    for (int ri = 0; ri < 4; ++ri) {
+                        const int pr = pw0 + 4 * c4 + ri;
+                        if (pr < n && qc < n) {
+                            OT* ot = out + 2 * ((int64_t)pr * ldo + qc);
+                            ot[0] = (OT)(ore[ri] + alpha * nre[ri]);
+                            ot[1] = (OT)(oim[ri] + alpha * nim[ri]);
+                        }
+                    }
+                    __syncwarp();
                 }
             } else if (r < n) {
                 OT* orow = out + (int64_t)r * ldo + c0;
