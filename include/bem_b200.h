@@ -97,9 +97,11 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  *   BEM_TUNE_CALDERON_GROUP  wavenumbers per launch of the fused Calderon
  *                            sweep (1 or 2; default 2)
  *   BEM_TUNE_GRAM_KSEG       64-wide K stages per TMEM accumulation segment of
- *                            the tensor-core normal matrix (>= 1) */
+ *                            the tensor-core normal matrix (>= 1)
+ *   BEM_TUNE_CHOL_NB         panel width of bem_chol_factor (a multiple of 64) */
 #define BEM_TUNE_CALDERON_GROUP 0
 #define BEM_TUNE_GRAM_KSEG 1
+#define BEM_TUNE_CHOL_NB 2
 #define BEM_TUNE_KEYS 8
 int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value);
 
@@ -335,8 +337,8 @@ int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, i
  * identity tile pivots in piv, explicit inverses of the 64 x 64 diagonal
  * tiles in dinv, bem_lu_dinv_elems(n) elements), so bem_lu_solve_tiled,
  * bem_refine_solve and bem_lstsq_refine take it.  A: BEM_C128 or BEM_F64 (the
- * lower triangle is read).  Panels of 256 columns in FP64 on the FP64 tensor
- * cores (DMMA); the trailing rank-256 Hermitian updates on the FP64 tensor
+ * lower triangle is read).  Panels of 512 columns (BEM_TUNE_CHOL_NB) in FP64
+ * on the FP64 tensor cores (DMMA); the trailing Hermitian updates on the FP64 tensor
  * cores (method BEM_PREC_FP64) or on tcgen05 from FP16 hi/lo splits of the
  * panel with FP64 sums subtracted from the FP64 Schur complement
  * (BEM_PREC_MIXED).  info: device int32, 0 or 1 + the first column whose

@@ -172,6 +172,8 @@ int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value) {
     if (key == BEM_TUNE_CALDERON_GROUP && value != 0 && value != 1 && value != 2)
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon group must be 1 or 2");
     if (key == BEM_TUNE_GRAM_KSEG && value < 0) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: negative segment");
+    if (key == BEM_TUNE_CHOL_NB && (value < 0 || value % 64 != 0 || value > 4096))
+        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: panel width must be a multiple of 64 up to 4096");
     ctx->tune[key] = value;
     return BEM_OK;
 }

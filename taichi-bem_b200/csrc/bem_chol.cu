@@ -4,14 +4,14 @@
 // persistent triangular solve (bem_lu_solve_tiled) and the refinement calls
 // take it unchanged.
 //
-// Right-looking, panels of CH_NB = 256 columns, each factored in sub-blocks
-// of 64 in FP64:
+// Right-looking, panels of 512 columns by default (BEM_TUNE_CHOL_NB), each
+// factored in sub-blocks of 64 in FP64:
 //   chol64_kernel     the 64 x 64 diagonal block in shared memory, and the
 //                     inverse of its factor;
 //   dmma_gemm_kernel  L21 = A21 L11^{-H} (a product with that inverse) and the
 //                     update of the panel's remaining columns, on the FP64
 //                     tensor cores (DMMA);
-// then the trailing Hermitian rank-256 update A22 -= L21 L21^H of the lower
+// then the trailing Hermitian rank-512 update A22 -= L21 L21^H of the lower
 // triangle, the step that carries the O(n^3) work:
 //   BEM_PREC_FP64   DMMA products (dmma_gemm_kernel, lower tiles only);
 //   BEM_PREC_MIXED  tcgen05 products of FP16 hi/lo splits of the panel (the
@@ -35,7 +35,7 @@
 namespace {
 
 constexpr int CH_IB = 64;   // diagonal sub-block
-constexpr int CH_NB = 256;  // panel width (columns per trailing update)
+constexpr int CH_NB_DEFAULT = 512;  // panel width (columns per trailing update)
 constexpr int CH_LD = CH_IB + 1;
 
 struct cd {
@@ -93,16 +93,21 @@ __global__ void __launch_bounds__(256) chol64_kernel(double* A, int64_t lda, int
             M[i * CH_LD + j] = cd{v.re * rd, v.im * rd};
         }
         __syncthreads();
-        const int w = nb - j - 1;
-        for (int e = tid; e < w * w; e += blockDim.x) {
-            const int i = j + 1 + e / w, c = j + 1 + e % w;
-            if (c > i) continue;
-            const cd a = M[i * CH_LD + j], b = M[c * CH_LD + j];
-            // M[i][c] -= a conj(b)
-            cd v = M[i * CH_LD + c];
-            v.re -= a.re * b.re + a.im * b.im;
-            v.im -= a.im * b.re - a.re * b.im;
-            M[i * CH_LD + c] = v;
+        // rank-1 update of the trailing lower triangle: row i = j + 1 + tid % 64,
+        // columns j + 1 + tid / 64, + 4, ... up to i
+        {
+            const int i = j + 1 + (tid & 63);
+            if (i < nb) {
+                const cd a = M[i * CH_LD + j];
+                for (int c = j + 1 + (tid >> 6); c <= i; c += 4) {
+                    const cd b = M[c * CH_LD + j];
+                    // M[i][c] -= a conj(b)
+                    cd v = M[i * CH_LD + c];
+                    v.re -= a.re * b.re + a.im * b.im;
+                    v.im -= a.im * b.re - a.re * b.im;
+                    M[i * CH_LD + c] = v;
+                }
+            }
         }
         __syncthreads();
     }
@@ -110,25 +115,31 @@ __global__ void __launch_bounds__(256) chol64_kernel(double* A, int64_t lda, int
         const int r = e / nb, c = e - r * nb;
         if (c <= r) st_c<C>(A, (int64_t)r * lda + c, M[r * CH_LD + c]);
     }
-    // X = L^{-1} (lower), one thread per column: X[r][c] = (delta_rc - sum_{c<=q<r} L[r][q] X[q][c]) / L[r][r]
-    if (tid < CH_IB) {
-        const int c = tid;
+    // X = L^{-1} (lower), row by row: X[r][c] = (delta_rc - sum_{c<=q<r} L[r][q] X[q][c]) / L[r][r];
+    // four threads per column split the sum over q and combine by shuffles
+    {
+        const int c = tid >> 2, part = tid & 3;
         for (int r = 0; r < CH_IB; ++r) {
-            cd v{r == c ? 1.0 : 0.0, 0.0};
-            if (r > c) {
-                v = cd{0.0, 0.0};
-                for (int q = c; q < r; ++q) {
+            cd v{0.0, 0.0};
+            if (r > c)
+                for (int q = c + part; q < r; q += 4) {
                     const cd l = M[r * CH_LD + q], x = X[q * CH_IB + c];
                     v.re -= l.re * x.re - l.im * x.im;
                     v.im -= l.re * x.im + l.im * x.re;
                 }
+            v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
+            v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
+            v.re += __shfl_xor_sync(0xffffffffu, v.re, 2);
+            v.im += __shfl_xor_sync(0xffffffffu, v.im, 2);
+            if (part == 0) {
+                if (r == c) v = cd{1.0, 0.0};
+                if (r < c) v = cd{0.0, 0.0};
+                const double d = M[r * CH_LD + r].re;  // real positive (identity padding beyond nb)
+                X[r * CH_IB + c] = cd{v.re / d, v.im / d};
             }
-            if (r < c) v = cd{0.0, 0.0};
-            const double d = M[r * CH_LD + r].re;  // real positive (identity padding beyond nb)
-            X[r * CH_IB + c] = cd{v.re / d, v.im / d};
+            __syncthreads();
         }
     }
-    __syncthreads();
     for (int e = tid; e < CH_IB * CH_IB; e += blockDim.x) st_c<C>(inv, e, X[e]);
 }
 
@@ -312,8 +323,9 @@ int chol_t(bem_ctx* ctx, double* A, int64_t n, int64_t lda, bool tensor_cores, i
                                 "chol64 smem"))
         return rc;
     auto at = [&](int64_t r, int64_t c) { return A + W * (r * lda + c); };
-    for (int64_t k0 = 0; k0 < n; k0 += CH_NB) {
-        const int64_t kb = std::min<int64_t>(CH_NB, n - k0);
+    const int nbw = ctx->tune[BEM_TUNE_CHOL_NB] > 0 ? ctx->tune[BEM_TUNE_CHOL_NB] : CH_NB_DEFAULT;
+    for (int64_t k0 = 0; k0 < n; k0 += nbw) {
+        const int64_t kb = std::min<int64_t>(nbw, n - k0);
         for (int64_t j0 = k0; j0 < k0 + kb; j0 += CH_IB) {
             const int jb = (int)std::min<int64_t>(CH_IB, k0 + kb - j0);
             chol64_kernel<C><<<1, 256, smem, s>>>(at(j0, j0), lda, jb, inv, info, (int)j0);
