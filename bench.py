@@ -859,7 +859,7 @@ def transmission_headline(args, ws, rank, local):
         "cholesky": {"bound": "tensor", "ms": phases["cholesky_tensor_cores"],
                      "achieved": 4.0 / 3.0 * n ** 3 / (phases["cholesky_tensor_cores"] * 1e-3) / 1e12,
                      "peak": MEASURED["bf16_tflops"], "unit": "TFLOP/s",
-                     "note": "4/3 n^3 flops of the complex Cholesky; panels in FP64 on DMMA, trailing rank-512 "
+                     "note": "4/3 n^3 flops of the complex Cholesky; panels in FP64 on DMMA, trailing rank-1024 "
                              "updates on tcgen05 (three FP16 products per product) into the FP64 Schur complement"},
         "far_calderon_kernel": {"bound": "fp32", "ms": phases["calderon_sweep_with_near"],
                                 "achieved": evals * CAL_FLOPS_PER_EVAL / (phases["calderon_sweep_with_near"] * 1e-3)

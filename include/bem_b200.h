@@ -337,7 +337,7 @@ int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, i
  * identity tile pivots in piv, explicit inverses of the 64 x 64 diagonal
  * tiles in dinv, bem_lu_dinv_elems(n) elements), so bem_lu_solve_tiled,
  * bem_refine_solve and bem_lstsq_refine take it.  A: BEM_C128 or BEM_F64 (the
- * lower triangle is read).  Panels of 512 columns (BEM_TUNE_CHOL_NB) in FP64
+ * lower triangle is read).  Panels of 1024 columns (BEM_TUNE_CHOL_NB) in FP64
  * on the FP64 tensor cores (DMMA); the trailing Hermitian updates on the FP64 tensor
  * cores (method BEM_PREC_FP64) or on tcgen05 from FP16 hi/lo splits of the
  * panel with FP64 sums subtracted from the FP64 Schur complement

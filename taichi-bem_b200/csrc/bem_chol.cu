@@ -4,14 +4,14 @@
 // persistent triangular solve (bem_lu_solve_tiled) and the refinement calls
 // take it unchanged.
 //
-// Right-looking, panels of 512 columns by default (BEM_TUNE_CHOL_NB), each
+// Right-looking, panels of 1024 columns by default (BEM_TUNE_CHOL_NB), each
 // factored in sub-blocks of 64 in FP64:
 //   chol64_kernel     the 64 x 64 diagonal block in shared memory, and the
 //                     inverse of its factor;
 //   dmma_gemm_kernel  L21 = A21 L11^{-H} (a product with that inverse) and the
 //                     update of the panel's remaining columns, on the FP64
 //                     tensor cores (DMMA);
-// then the trailing Hermitian rank-512 update A22 -= L21 L21^H of the lower
+// then the trailing Hermitian rank-1024 update A22 -= L21 L21^H of the lower
 // triangle, the step that carries the O(n^3) work:
 //   BEM_PREC_FP64   DMMA products (dmma_gemm_kernel, lower tiles only);
 //   BEM_PREC_MIXED  tcgen05 products of FP16 hi/lo splits of the panel (the
@@ -35,7 +35,7 @@
 namespace {
 
 constexpr int CH_IB = 64;   // diagonal sub-block
-constexpr int CH_NB_DEFAULT = 512;  // panel width (columns per trailing update)
+constexpr int CH_NB_DEFAULT = 1024;  // panel width (columns per trailing update; measured 510 / 410 / 384 ms for 256 / 512 / 1024 on the 30722-unknown normal matrix)
 constexpr int CH_LD = CH_IB + 1;
 
 struct cd {
