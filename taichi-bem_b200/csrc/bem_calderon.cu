@@ -25,7 +25,8 @@
 // rescaled in FP64; the sums over the test points run in FP32, the sums over
 // the trial points in FP64.  FP64 (plain path) evaluates d = x - y directly.
 // Coincident / edge / vertex pairs are left to the FP64 Sauter-Schwab
-// kernels (bem_launch_assemble_parts, near only).
+// kernels (bem_launch_assemble_parts, near only), which run on the side
+// stream while the sweep runs.
 #include <cmath>
 
 #include "bem_farfield.cuh"
@@ -409,7 +410,15 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
     cudaStream_t s = (cudaStream_t)stream;
     const bool fp32 = op->precision == BEM_PREC_MIXED;
     const bool helm = op->kernel == BEM_KERNEL_HELMHOLTZ;
-    // near pairs: the FP64 Sauter-Schwab kernels of each operator, per wavenumber
+    // near pairs: the FP64 Sauter-Schwab kernels of each operator, per
+    // wavenumber, on the high-priority side stream, concurrently with the far
+    // sweep (different pipes; they write other V entries, and every entry they
+    // share with the sweep -- the P1 columns and rows -- is added atomically);
+    // the caller's stream waits for both
+    if (int rc = bem_lookahead_stream(ctx)) return rc;
+    if (int rc = bem_check_cuda(ctx, cudaEventRecord(ctx->ev_next, s), "calderon fork")) return rc;
+    if (int rc = bem_check_cuda(ctx, cudaStreamWaitEvent(ctx->aux, ctx->ev_next, 0), "calderon fork")) return rc;
+    const cudaStream_t sn = ctx->aux;
     for (int w = 0; w < nk; ++w) {
         bem_op_desc d = *op;
         d.k = k[w];
@@ -417,15 +426,15 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
         const double c = coef[w];
         d.op = BEM_OP_V;
         if (int rc = bem_launch_assemble_parts(ctx, &d, neu, neu, 0, out[w], ld, -c, nullptr, 0.0, nullptr, nullptr, 0,
-                                               s, true))
+                                               sn, true))
             return rc;
         d.op = BEM_OP_K;
         if (int rc = bem_launch_assemble_parts(ctx, &d, neu, dir, 0, out[w], ld, c, out[w], -c, nullptr, nullptr, 0,
-                                               s, true))
+                                               sn, true))
             return rc;
         d.op = BEM_OP_W;
         if (int rc = bem_launch_assemble_parts(ctx, &d, dir, dir, 0, out[w], ld, -c, nullptr, 0.0, nullptr, nullptr, 0,
-                                               s, true))
+                                               sn, true))
             return rc;
     }
     CalArgs a{};
@@ -457,14 +466,21 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
     // default: both wavenumbers in one launch (measured faster than one launch
     // per wavenumber on the 20480-panel transmission problem: 652 vs 769 ms
     // mixed, 1602 vs 1736 ms FP64); group 1 keeps one per launch
-    if (nk == 2 && ctx->tune[BEM_TUNE_CALDERON_GROUP] != 1) return dispatch_calderon<2>(ctx, a, fp32, helm, s);
-    for (int w = 0; w < nk; ++w) {
-        CalArgs b = a;
-        b.k[0] = a.k[w];
-        b.k2[0] = a.k2[w];
-        b.coef[0] = a.coef[w];
-        b.out[0] = a.out[w];
-        if (int rc = dispatch_calderon<1>(ctx, b, fp32, helm, s)) return rc;
+    int rc = BEM_OK;
+    if (nk == 2 && ctx->tune[BEM_TUNE_CALDERON_GROUP] != 1) {
+        rc = dispatch_calderon<2>(ctx, a, fp32, helm, s);
+    } else {
+        for (int w = 0; w < nk && !rc; ++w) {
+            CalArgs b = a;
+            b.k[0] = a.k[w];
+            b.k2[0] = a.k2[w];
+            b.coef[0] = a.coef[w];
+            b.out[0] = a.out[w];
+            rc = dispatch_calderon<1>(ctx, b, fp32, helm, s);
+        }
     }
-    return BEM_OK;
+    // join: the caller's stream waits for the near-pair kernels
+    if (int e = bem_check_cuda(ctx, cudaEventRecord(ctx->ev_diag, sn), "calderon join")) return e;
+    if (int e = bem_check_cuda(ctx, cudaStreamWaitEvent(s, ctx->ev_diag, 0), "calderon join")) return e;
+    return rc;
 }
