@@ -94,8 +94,10 @@ int64_t bem_launch_count(const bem_ctx* ctx);
 /* Launch-shape choices of this context (no reference counterpart), set by the
  * autotuner (bem_b200/tuning.py) after timing the candidates on this GPU;
  * value 0 restores the built-in default.  Keys:
- *   BEM_TUNE_CALDERON_GROUP  wavenumbers per launch of the fused Calderon
- *                            sweep (1 or 2; default 2)
+ *   BEM_TUNE_CALDERON_GROUP  form of the fused Calderon sweep: 1 scalar, one
+ *                            wavenumber per launch; 2 scalar, both in one
+ *                            launch (the FP64 default); 3 packed FP32x2, one
+ *                            wavenumber per launch (the mixed Helmholtz default)
  *   BEM_TUNE_GRAM_KSEG       64-wide K stages per TMEM accumulation segment of
  *                            the tensor-core normal matrix (>= 1)
  *   BEM_TUNE_CHOL_NB         panel width of bem_chol_factor (a multiple of 64) */

@@ -63,6 +63,106 @@ __device__ __forceinline__ void hats(const double* m, double* v) {
     v[2] = m[2];
 }
 
+// Entries of one unordered separate pair (i = li, j = lj) for wavenumber w
+// from its FP64 moments Mr / Mi (layout of far_calderon_kernel), added to
+// out[w] with the reference's block placement.  rotate: multiply by the pair
+// frame's e^{ikR} (FP32 pair frame).
+template <bool HELM>
+__device__ __forceinline__ void calderon_epilogue(const CalArgs& a, int w, int li, int lj, int gi, int gj,
+                                                  const double* ni64, const double* nj64, double pf, double Rd,
+                                                  const double* Mr, const double* Mi, bool rotate) {
+    const int nri = a.ndof[li], nrj = a.ndof[lj];
+    int di[3], dj[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        di[c] = a.ddof[3 * li + c];
+        dj[c] = a.ddof[3 * lj + c];
+    }
+    const double nd = ni64[0] * nj64[0] + ni64[1] * nj64[1] + ni64[2] * nj64[2];
+    // pair factor and e^{ikR}, then 1/(4 pi)
+    double fr_ = pf * BEM_INV4PI, fi_ = 0.0;
+    if (rotate) {
+        double sR, cR;
+        sincos(a.k[w] * Rd, &sR, &cR);
+        fi_ = fr_ * sR;
+        fr_ = fr_ * cR;
+    }
+    double vr[15], vi[15];
+#pragma unroll
+    for (int m = 0; m < 15; ++m) {
+        vr[m] = Mr[m] * fr_ - Mi[m] * fi_;
+        vi[m] = Mr[m] * fi_ + Mi[m] * fr_;
+    }
+    double* X = a.out[w];
+    const double c = a.coef[w];
+    const int64_t ld = a.ld;
+    // V (P0 x P0): one writer per entry
+    if (nri >= 0 && nrj >= 0) {
+        add_entry<HELM>(X, (int64_t)nri * ld + nrj, -c * vr[0], -c * vi[0], false);
+        add_entry<HELM>(X, (int64_t)nrj * ld + nri, -c * vr[0], -c * vi[0], false);
+    }
+    // K_ij (row N_i, trial hats of j) and K_ji (row N_j, trial hats of i), with their -K^T
+    double kyr[3], kyi[3], kxr[3], kxi[3];
+    hats(vr + 1, kyr);
+    hats(vi + 1, kyi);
+    hats(vr + 4, kxr);
+    hats(vi + 4, kxi);
+#pragma unroll
+    for (int h = 0; h < 3; ++h) {
+        if (nri >= 0 && dj[h] >= 0) {
+            add_entry<HELM>(X, (int64_t)nri * ld + dj[h], c * kyr[h], c * kyi[h], true);
+            add_entry<HELM>(X, (int64_t)dj[h] * ld + nri, -c * kyr[h], -c * kyi[h], true);
+        }
+        if (nrj >= 0 && di[h] >= 0) {
+            add_entry<HELM>(X, (int64_t)nrj * ld + di[h], c * kxr[h], c * kxi[h], true);
+            add_entry<HELM>(X, (int64_t)di[h] * ld + nrj, -c * kxr[h], -c * kxi[h], true);
+        }
+    }
+    // W (P1 x P1) and its transpose
+    double pr[3][3], pim[3][3];
+    if (HELM) {
+        // moments (x-side in {tot,1,2}) x (y-side in {tot,1,2}) -> hat values
+        const double tr[3][3] = {{vr[0], vr[7], vr[8]}, {vr[9], vr[10], vr[11]}, {vr[12], vr[13], vr[14]}};
+        const double ti[3][3] = {{vi[0], vi[7], vi[8]}, {vi[9], vi[10], vi[11]}, {vi[12], vi[13], vi[14]}};
+        double rr[3][3], ri[3][3];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            hats(tr[x], rr[x]);
+            hats(ti[x], ri[x]);
+        }
+#pragma unroll
+        for (int y = 0; y < 3; ++y) {
+            const double cr[3] = {rr[0][y], rr[1][y], rr[2][y]}, ci[3] = {ri[0][y], ri[1][y], ri[2][y]};
+            double hr[3], hi[3];
+            hats(cr, hr);
+            hats(ci, hi);
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                pr[x][y] = hr[x];
+                pim[x][y] = hi[x];
+            }
+        }
+    }
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        if (di[x] < 0) continue;
+        const double* cx = a.curl + 9 * gi + 3 * x;
+#pragma unroll
+        for (int y = 0; y < 3; ++y) {
+            if (dj[y] < 0) continue;
+            const double* cy = a.curl + 9 * gj + 3 * y;
+            const double cc = cx[0] * cy[0] + cx[1] * cy[1] + cx[2] * cy[2];  // curl_x(i) . curl_y(j)
+            double wr_ = vr[0] * cc, wi_ = vi[0] * cc;
+            if (HELM) {
+                wr_ -= a.k2[w] * nd * pr[x][y];
+                wi_ -= a.k2[w] * nd * pim[x][y];
+            }
+            add_entry<HELM>(X, (int64_t)di[x] * ld + dj[y], -c * wr_, -c * wi_, true);
+            add_entry<HELM>(X, (int64_t)dj[y] * ld + di[x], -c * wr_, -c * wi_, true);
+        }
+    }
+}
+
 template <typename T, int NK, bool HELM, int PH>
 __global__ void __launch_bounds__(FAR_THREADS) far_calderon_kernel(CalArgs a) {
     using V4 = typename V4T<T>::type;
@@ -272,105 +372,210 @@ __global__ void __launch_bounds__(FAR_THREADS) far_calderon_kernel(CalArgs a) {
         }
 
         // ---- epilogue: entries of every block, per wavenumber ----
-        const int nri = a.ndof[li], nrj = a.ndof[lj];
-        int di[3], dj[3];
 #pragma unroll
+        for (int w = 0; w < NK; ++w)
+            calderon_epilogue<HELM>(a, w, li, lj, gi, gj, ni64, nj64, pf, Rd, Mr[w], Mi[w], SPLIT && HELM);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Packed FP32x2 form of the Helmholtz sweep (mixed precision, one
+// wavenumber per launch): two test points (q, q + 1) in the two lanes of every
+// FFMA2 / FMUL2 / FADD2, as in the packed Dirichlet sweep, with the same
+// pair-frame algebra as far_calderon_kernel<float, 1, true, PH>:
+//   s = |x_a|^2 + x_a.U_b + C_b,  U_b = 2D - 2y_b,  C_b = -y_b.(2D - y_b)
+//   d.n_j = D.n_j + x_a.(n_j - n_i).
+// The lanes are summed after the loop over the test points; an odd Q^2 is
+// padded by a copy of the last point with weight 0.  PH: 2 short polynomial
+// (phase <= 0.3), 1 full polynomial (<= pi/4), 0 argument reduction.
+// ---------------------------------------------------------------------------
+template <int PH>
+__global__ void __launch_bounds__(FAR_THREADS) far_calderon_x2_kernel(CalArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int Q2 = a.Q2;
+    const int P2 = (Q2 + 1) / 2;
+    float4* sxy = reinterpret_cast<float4*>(smem_raw);          // [FAR_TI][P2] (x0 x1 y0 y1)
+    float4* szw = sxy + FAR_TI * P2;                             // [FAR_TI][P2] (z0 z1 w0 w1)
+    float2* sxx = reinterpret_cast<float2*>(szw + FAR_TI * P2);  // [FAR_TI][P2] |x|^2
+    float4* sph = reinterpret_cast<float4*>(sxx + FAR_TI * P2);  // [P2] (phi1_0 phi1_1 phi2_0 phi2_1)
+    __shared__ int s_gi[FAR_TI];
+    __shared__ int s_tri[FAR_TI][3];
+    __shared__ double s_cen[FAR_TI][3];
+    __shared__ double s_nrm[FAR_TI][3];
+
+    const int n = a.n;
+    const int j0 = blockIdx.x * FAR_THREADS;
+    const int li0 = blockIdx.y * FAR_TI;
+    if (j0 + FAR_THREADS - 1 <= li0) return;
+    const int lj = j0 + threadIdx.x;
+    const float4* pts = reinterpret_cast<const float4*>(a.pts);
+    const float* phi = reinterpret_cast<const float*>(a.phi);
+    if (threadIdx.x < FAR_TI) {
+        const int li = li0 + threadIdx.x;
+        const int gi = li < n ? a.panels[li] : -1;
+        s_gi[threadIdx.x] = gi;
         for (int c = 0; c < 3; ++c) {
-            di[c] = a.ddof[3 * li + c];
-            dj[c] = a.ddof[3 * lj + c];
+            s_tri[threadIdx.x][c] = gi >= 0 ? a.tris[3 * gi + c] : -1;
+            s_cen[threadIdx.x][c] = gi >= 0 ? a.centroid[3 * gi + c] : 0.0;
+            s_nrm[threadIdx.x][c] = gi >= 0 ? a.normal[3 * gi + c] : 0.0;
         }
-        const double nd = ni64[0] * nj64[0] + ni64[1] * nj64[1] + ni64[2] * nj64[2];
-        double cc[3][3];  // curl_a(i) . curl_b(j)
-#pragma unroll
-        for (int x = 0; x < 3; ++x)
-#pragma unroll
-            for (int y = 0; y < 3; ++y) {
-                const double* cx = a.curl + 9 * gi + 3 * x;
-                const double* cy = a.curl + 9 * gj + 3 * y;
-                cc[x][y] = cx[0] * cy[0] + cx[1] * cy[1] + cx[2] * cy[2];
-            }
-#pragma unroll
-        for (int w = 0; w < NK; ++w) {
-            // pair factor and e^{ikR}, then 1/(4 pi)
-            double fr_ = pf * BEM_INV4PI, fi_ = 0.0;
-            if (SPLIT && HELM) {
-                double sR, cR;
-                sincos(a.k[w] * Rd, &sR, &cR);
-                fi_ = fr_ * sR;
-                fr_ = fr_ * cR;
-            }
-            double vr[15], vi[15];
-#pragma unroll
-            for (int m = 0; m < 15; ++m) {
-                vr[m] = Mr[w][m] * fr_ - Mi[w][m] * fi_;
-                vi[m] = Mr[w][m] * fi_ + Mi[w][m] * fr_;
-            }
-            double* X = a.out[w];
-            const double c = a.coef[w];
-            const int64_t ld = a.ld;
-            // V (P0 x P0): one writer per entry
-            if (nri >= 0 && nrj >= 0) {
-                add_entry<HELM>(X, (int64_t)nri * ld + nrj, -c * vr[0], -c * vi[0], false);
-                add_entry<HELM>(X, (int64_t)nrj * ld + nri, -c * vr[0], -c * vi[0], false);
-            }
-            // K_ij (row N_i, trial hats of j) and K_ji (row N_j, trial hats of i), with their -K^T
-            double kyr[3], kyi[3], kxr[3], kxi[3];
-            hats(vr + 1, kyr);
-            hats(vi + 1, kyi);
-            hats(vr + 4, kxr);
-            hats(vi + 4, kxi);
-#pragma unroll
-            for (int h = 0; h < 3; ++h) {
-                if (nri >= 0 && dj[h] >= 0) {
-                    add_entry<HELM>(X, (int64_t)nri * ld + dj[h], c * kyr[h], c * kyi[h], true);
-                    add_entry<HELM>(X, (int64_t)dj[h] * ld + nri, -c * kyr[h], -c * kyi[h], true);
-                }
-                if (nrj >= 0 && di[h] >= 0) {
-                    add_entry<HELM>(X, (int64_t)nrj * ld + di[h], c * kxr[h], c * kxi[h], true);
-                    add_entry<HELM>(X, (int64_t)di[h] * ld + nrj, -c * kxr[h], -c * kxi[h], true);
-                }
-            }
-            // W (P1 x P1) and its transpose
-            double pr[3][3], pim[3][3];
-            if (HELM) {
-                // moments (x-side in {tot,1,2}) x (y-side in {tot,1,2}) -> hat values
-                const double tr[3][3] = {{vr[0], vr[7], vr[8]}, {vr[9], vr[10], vr[11]}, {vr[12], vr[13], vr[14]}};
-                const double ti[3][3] = {{vi[0], vi[7], vi[8]}, {vi[9], vi[10], vi[11]}, {vi[12], vi[13], vi[14]}};
-                double rr[3][3], ri[3][3];
-#pragma unroll
-                for (int x = 0; x < 3; ++x) {
-                    hats(tr[x], rr[x]);
-                    hats(ti[x], ri[x]);
-                }
-#pragma unroll
-                for (int y = 0; y < 3; ++y) {
-                    const double cr[3] = {rr[0][y], rr[1][y], rr[2][y]}, ci[3] = {ri[0][y], ri[1][y], ri[2][y]};
-                    double hr[3], hi[3];
-                    hats(cr, hr);
-                    hats(ci, hi);
-#pragma unroll
-                    for (int x = 0; x < 3; ++x) {
-                        pr[x][y] = hr[x];
-                        pim[x][y] = hi[x];
-                    }
-                }
-            }
-#pragma unroll
-            for (int x = 0; x < 3; ++x) {
-                if (di[x] < 0) continue;
-#pragma unroll
-                for (int y = 0; y < 3; ++y) {
-                    if (dj[y] < 0) continue;
-                    double wr_ = vr[0] * cc[x][y], wi_ = vi[0] * cc[x][y];
-                    if (HELM) {
-                        wr_ -= a.k2[w] * nd * pr[x][y];
-                        wi_ -= a.k2[w] * nd * pim[x][y];
-                    }
-                    add_entry<HELM>(X, (int64_t)di[x] * ld + dj[y], -c * wr_, -c * wi_, true);
-                    add_entry<HELM>(X, (int64_t)dj[y] * ld + di[x], -c * wr_, -c * wi_, true);
-                }
-            }
+    }
+    for (int p = threadIdx.x; p < P2; p += FAR_THREADS) {
+        const int q0 = 2 * p, q1 = 2 * p + 1 < Q2 ? 2 * p + 1 : Q2 - 1;
+        const float pad = 2 * p + 1 < Q2 ? 1.f : 0.f;
+        sph[p] = make_float4(phi[3 * q0 + 1], pad * phi[3 * q1 + 1], phi[3 * q0 + 2], pad * phi[3 * q1 + 2]);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < FAR_TI * P2; idx += FAR_THREADS) {
+        const int t = idx / P2, p = idx - t * P2;
+        const int q0 = 2 * p, q1 = 2 * p + 1 < Q2 ? 2 * p + 1 : Q2 - 1;
+        float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
+        if (li0 + t < n) {
+            x0 = pts[(size_t)s_gi[t] * Q2 + q0];
+            x1 = pts[(size_t)s_gi[t] * Q2 + q1];
+            if (2 * p + 1 >= Q2) x1.w = 0.f;  // padding point: weight 0
         }
+        sxy[idx] = make_float4(x0.x, x1.x, x0.y, x1.y);
+        szw[idx] = make_float4(x0.z, x1.z, x0.w, x1.w);
+        sxx[idx] = make_float2(fmaf(x0.x, x0.x, fmaf(x0.y, x0.y, x0.z * x0.z)),
+                               fmaf(x1.x, x1.x, fmaf(x1.y, x1.y, x1.z * x1.z)));
+    }
+    __syncthreads();
+
+    const bool valid_j = lj < n;
+    const int gj = valid_j ? a.panels[lj] : 0;
+    int tri_j[3];
+    double cen_j[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        tri_j[c] = a.tris[3 * gj + c];
+        cen_j[c] = a.centroid[3 * gj + c];
+    }
+    const double nj64[3] = {a.normal[3 * gj + 0], a.normal[3 * gj + 1], a.normal[3 * gj + 2]};
+    const float4* ptsj = pts + (size_t)gj * Q2;
+    const float2 KK = f2((float)a.k[0]), NKK = f2(-(float)a.k[0]);
+
+    for (int t = 0; t < FAR_TI; ++t) {
+        const int li = li0 + t;
+        if (li >= n) break;
+        const int gi = s_gi[t];
+        const bool sep = valid_j && li < lj && (bem_relation(s_tri[t], tri_j, gi == gj) == REL_SEPARATE);
+        if (!sep) continue;
+        const double Dx = s_cen[t][0] - cen_j[0], Dy = s_cen[t][1] - cen_j[1], Dz = s_cen[t][2] - cen_j[2];
+        const double ni64[3] = {s_nrm[t][0], s_nrm[t][1], s_nrm[t][2]};
+        const float ux = (float)(2.0 * Dx), uy = (float)(2.0 * Dy), uz = (float)(2.0 * Dz);
+        const double R2d = Dx * Dx + Dy * Dy + Dz * Dz;
+        const double Rd = sqrt(R2d);
+        const float2 R2 = f2((float)R2d), RF = f2((float)Rd);
+        const double pf = 4.0 * a.area[gi] * a.area[gj] * a.wcorr;
+        const double Dni64 = Dx * ni64[0] + Dy * ni64[1] + Dz * ni64[2];
+        const float2 DNJ = f2((float)(Dx * nj64[0] + Dy * nj64[1] + Dz * nj64[2]));
+        const float2 MX = f2((float)(nj64[0] - ni64[0])), MY = f2((float)(nj64[1] - ni64[1])),
+                     MZ = f2((float)(nj64[2] - ni64[2]));
+        const float4* sxyt = sxy + t * P2;
+        const float4* szwt = szw + t * P2;
+        const float2* sxxt = sxx + t * P2;
+
+        double Mr[15], Mi[15];
+#pragma unroll
+        for (int m = 0; m < 15; ++m) Mr[m] = Mi[m] = 0.0;
+
+        for (int b = 0; b < Q2; ++b) {
+            const float4 yb = ptsj[b];
+            const float wx = ux - yb.x, wy = uy - yb.y, wz = uz - yb.z;
+            const float2 U0 = f2(wx - yb.x), U1 = f2(wy - yb.y), U2 = f2(wz - yb.z);
+            const float2 CB = f2(-fmaf(yb.x, wx, fmaf(yb.y, wy, yb.z * wz)));
+            // [0] G, [1] phi1 G, [2] phi2 G, [3] d.n_j F/r^3, [4] F/r^3, [5] phi1 F/r^3, [6] phi2 F/r^3
+            float2 Ar[7], Ai[7];
+#pragma unroll
+            for (int m = 0; m < 7; ++m) Ar[m] = Ai[m] = f2(0.f);
+#pragma unroll 2
+            for (int p = 0; p < P2; ++p) {
+                const float4 xy = sxyt[p], zw = szwt[p], ph = sph[p];
+                const float2 X = make_float2(xy.x, xy.y), Y = make_float2(xy.z, xy.w);
+                const float2 Z = make_float2(zw.x, zw.y), Wt = make_float2(zw.z, zw.w);
+                const float2 P1 = make_float2(ph.x, ph.y), P2v = make_float2(ph.z, ph.w);
+                const float2 sq = ffma2(X, U0, ffma2(Y, U1, ffma2(Z, U2, fadd2(sxxt[p], CB))));
+                float2 r, rinv;
+                dev_r_rinv2(fadd2(R2, sq), r, rinv);
+                const float2 dnj = ffma2(X, MX, ffma2(Y, MY, ffma2(Z, MZ, DNJ)));
+                const float2 rr = fadd2(r, RF);
+                const float2 phase = fmul2(KK, fmul2(sq, make_float2(__fdividef(1.0f, rr.x), __fdividef(1.0f, rr.y))));
+                const float2 wr = fmul2(Wt, rinv);
+                const float2 wr3 = fmul2(wr, fmul2(rinv, rinv));
+                const float2 tj = fmul2(wr3, dnj);
+                float2 sn, cs;
+                if (PH == 2) {
+                    dev_sincos_poly2<true>(phase, sn, cs);
+                } else if (PH == 1) {
+                    dev_sincos_poly2<false>(phase, sn, cs);
+                } else {
+                    dev_sincos(phase.x, &sn.x, &cs.x);
+                    dev_sincos(phase.y, &sn.y, &cs.y);
+                }
+                const float2 kr = fmul2(KK, r), nkr = fmul2(NKK, r);
+                const float2 gr = fmul2(wr, cs), gi_ = fmul2(wr, sn);
+                const float2 fr = ffma2(kr, sn, cs), fi = ffma2(nkr, cs, sn);
+                Ar[0] = fadd2(Ar[0], gr);
+                Ai[0] = fadd2(Ai[0], gi_);
+                Ar[1] = ffma2(P1, gr, Ar[1]);
+                Ai[1] = ffma2(P1, gi_, Ai[1]);
+                Ar[2] = ffma2(P2v, gr, Ar[2]);
+                Ai[2] = ffma2(P2v, gi_, Ai[2]);
+                Ar[3] = ffma2(tj, fr, Ar[3]);
+                Ai[3] = ffma2(tj, fi, Ai[3]);
+                const float2 hr = fmul2(wr3, fr), hi = fmul2(wr3, fi);
+                Ar[4] = fadd2(Ar[4], hr);
+                Ai[4] = fadd2(Ai[4], hi);
+                Ar[5] = ffma2(P1, hr, Ar[5]);
+                Ai[5] = ffma2(P1, hi, Ai[5]);
+                Ar[6] = ffma2(P2v, hr, Ar[6]);
+                Ai[6] = ffma2(P2v, hi, Ai[6]);
+            }
+            float sr[7], si[7];
+#pragma unroll
+            for (int m = 0; m < 7; ++m) {
+                sr[m] = Ar[m].x + Ar[m].y;
+                si[m] = Ai[m].x + Ai[m].y;
+            }
+            const double wb = double(yb.w);
+            const double wb1 = wb * a.phi64[3 * b + 1], wb2 = wb * a.phi64[3 * b + 2];
+            const double ndni =
+                -(Dni64 - (double(yb.x) * ni64[0] + double(yb.y) * ni64[1] + double(yb.z) * ni64[2]));
+            const double wbn = wb * ndni;
+            const double g0r = sr[0], g0i = si[0], g1r = sr[1], g1i = si[1], g2r = sr[2], g2i = si[2];
+            Mr[0] += wb * g0r;
+            Mi[0] += wb * g0i;
+            Mr[1] += wb * double(sr[3]);
+            Mi[1] += wb * double(si[3]);
+            Mr[2] += wb1 * double(sr[3]);
+            Mi[2] += wb1 * double(si[3]);
+            Mr[3] += wb2 * double(sr[3]);
+            Mi[3] += wb2 * double(si[3]);
+            Mr[4] += wbn * double(sr[4]);
+            Mi[4] += wbn * double(si[4]);
+            Mr[5] += wbn * double(sr[5]);
+            Mi[5] += wbn * double(si[5]);
+            Mr[6] += wbn * double(sr[6]);
+            Mi[6] += wbn * double(si[6]);
+            Mr[7] += wb1 * g0r;
+            Mi[7] += wb1 * g0i;
+            Mr[8] += wb2 * g0r;
+            Mi[8] += wb2 * g0i;
+            Mr[9] += wb * g1r;
+            Mi[9] += wb * g1i;
+            Mr[10] += wb1 * g1r;
+            Mi[10] += wb1 * g1i;
+            Mr[11] += wb2 * g1r;
+            Mi[11] += wb2 * g1i;
+            Mr[12] += wb * g2r;
+            Mi[12] += wb * g2i;
+            Mr[13] += wb1 * g2r;
+            Mi[13] += wb1 * g2i;
+            Mr[14] += wb2 * g2r;
+            Mi[14] += wb2 * g2i;
+        }
+        calderon_epilogue<true>(a, 0, li, lj, gi, gj, ni64, nj64, pf, Rd, Mr, Mi, true);
     }
 }
 
@@ -382,6 +587,17 @@ int launch_calderon(bem_ctx* ctx, const CalArgs& a, cudaStream_t s) {
     far_calderon_kernel<T, NK, HELM, PH><<<grid, FAR_THREADS, smem, s>>>(a);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "far_calderon_kernel launch");
+}
+
+template <int PH>
+int launch_calderon_x2(bem_ctx* ctx, const CalArgs& a, cudaStream_t s) {
+    dim3 grid((a.n + FAR_THREADS - 1) / FAR_THREADS, (a.n + FAR_TI - 1) / FAR_TI);
+    if (grid.y > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "calderon: too many panels for one launch");
+    const int P2 = (a.Q2 + 1) / 2;
+    const size_t smem = (size_t)FAR_TI * P2 * (2 * sizeof(float4) + sizeof(float2)) + (size_t)P2 * sizeof(float4);
+    far_calderon_x2_kernel<PH><<<grid, FAR_THREADS, smem, s>>>(a);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "far_calderon_x2_kernel launch");
 }
 
 template <int NK>
@@ -450,8 +666,10 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
     a.wcorr = ctx->wcorr32;
     double kmax = 0.0;
     for (int w = 0; w < nk; ++w) kmax = std::fmax(kmax, std::fabs(k[w]));
-    // 1: the phase k (r - R) is bounded by pi/4, so the sine/cosine needs no argument reduction
-    a.small_phase = fp32 && helm ? (bem_phase_class(kmax * 2.0 * ctx->rho_max) != 0 ? 1 : 0) : 0;
+    // class of the bound on the phase k (r - R): 2 (<= 0.3: short polynomial), 1 (<= pi/4: no argument
+    // reduction), 0 (reduction)
+    const int phase_class = fp32 && helm ? bem_phase_class(kmax * 2.0 * ctx->rho_max) : 0;
+    a.small_phase = phase_class != 0 ? 1 : 0;
     a.pts = fp32 ? (const void*)ctx->pts32 : (const void*)ctx->pts64;
     a.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
     a.phi64 = ctx->phi64;
@@ -463,11 +681,23 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
         a.out[w] = (double*)out[w];
     }
     a.ld = ld;
-    // default: both wavenumbers in one launch (measured faster than one launch
-    // per wavenumber on the 20480-panel transmission problem: 652 vs 769 ms
-    // mixed, 1602 vs 1736 ms FP64); group 1 keeps one per launch
+    // FP64 (and Laplace) default: both wavenumbers in one launch (measured
+    // faster than one launch per wavenumber on the 20480-panel transmission
+    // problem: 1602 vs 1736 ms FP64); group 1 keeps one per launch
     int rc = BEM_OK;
-    if (nk == 2 && ctx->tune[BEM_TUNE_CALDERON_GROUP] != 1) {
+    const int variant = ctx->tune[BEM_TUNE_CALDERON_GROUP];
+    if (fp32 && helm && (variant == 0 || variant == 3)) {
+        // default of the mixed Helmholtz sweep: packed FP32x2, one wavenumber per launch
+        for (int w = 0; w < nk && !rc; ++w) {
+            CalArgs b = a;
+            b.k[0] = a.k[w];
+            b.k2[0] = a.k2[w];
+            b.coef[0] = a.coef[w];
+            b.out[0] = a.out[w];
+            rc = phase_class == 2 ? launch_calderon_x2<2>(ctx, b, s)
+                                  : (phase_class == 1 ? launch_calderon_x2<1>(ctx, b, s) : launch_calderon_x2<0>(ctx, b, s));
+        }
+    } else if (nk == 2 && variant != 1) {
         rc = dispatch_calderon<2>(ctx, a, fp32, helm, s);
     } else {
         for (int w = 0; w < nk && !rc; ++w) {

@@ -79,8 +79,9 @@ def test_fused_matches_per_operator_path(precision):
 
 
 def test_laplace_full_and_grouped_wavenumbers():
-    """Laplace "Full" problems take the same path (k = 0), and one launch with
-    both wavenumbers (tuning group 2) equals two single-wavenumber launches."""
+    """Laplace "Full" problems take the same path (k = 0), and the forms of the
+    sweep agree: one launch with both wavenumbers (tuning group 2), one per
+    wavenumber (1), and the packed FP32x2 sweep (3, mixed precision)."""
     from bem_b200 import _lib as L
     core, b, v, f = _problem(2, "fp64", Q=3, kernel="Laplace")
     b.assemble_system()
@@ -89,12 +90,13 @@ def test_laplace_full_and_grouped_wavenumbers():
     core.kill()
     for prec in ("fp64", "mixed"):
         outs = []
-        for group in (1, 2):
+        for group in ((1, 2) if prec == "fp64" else (1, 2, 3)):
             core, b, *_ = _problem(2, prec)
             b.engine.set_tuning(L.TUNE_CALDERON_GROUP, group)
             b.assemble_system()
             outs.append((b._mat_A.clone(), b._mat_P.clone()))
             core.kill()
         tol = 1e-13 if prec == "fp64" else 1e-6
-        assert rel_err(outs[0][0].cpu().numpy(), outs[1][0].cpu().numpy()) < tol
-        assert rel_err(outs[0][1].cpu().numpy(), outs[1][1].cpu().numpy()) < tol
+        for o in outs[1:]:
+            assert rel_err(outs[0][0].cpu().numpy(), o[0].cpu().numpy()) < tol
+            assert rel_err(outs[0][1].cpu().numpy(), o[1].cpu().numpy()) < tol
