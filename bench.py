@@ -8,7 +8,9 @@ with inputs resident in HBM: the fused Calderon sweep (V, K, K^T, W at both
 wavenumbers; separate pairs in FP32, coincident/edge/vertex pairs in FP64)
 into A = P-_o + P+_i and P+_i, the identity blocks and right-hand side, and
 the reference's least squares on the stacked [A; P+_i]: FP16-split
-tensor-core normal matrix, FP32 tile LU, FP64 flexible GMRES.
+tensor-core normal matrix (FP64 segment sums), Cholesky with FP64 panels and
+tensor-core trailing updates into an FP64 Schur complement, FP64 flexible
+GMRES on the normal equations.
 
   value  = stacked-system entries (2 n^2) / time-to-solution (entries/s),
            device-timed with CUDA events per step, 256 MiB L2 flush between
@@ -17,8 +19,9 @@ tensor-core normal matrix, FP32 tile LU, FP64 flexible GMRES.
            mesh: mesh upload, set-up, run, solution read back), one full
            lifecycle per step, median of two after one discarded;
   plain_fp64 = the same step on the plain FP64 path (FP64 sweep, FP64
-           tensor-core normal matrix, FP64 tile LU), whose solution is the
-           FP64 oracle the mixed result's relative error is quoted against.
+           DMMA normal matrix, Cholesky with DMMA updates, FP64 GMRES), whose
+           solution is the FP64 oracle the mixed result's relative error is
+           quoted against.
 
 `--workload dirichlet_s4` gives the Helmholtz interior Dirichlet line (5120
 panels); the other workloads print their own lines.  `--impl reference`
@@ -314,13 +317,20 @@ def phase_breakdown(b):
     return out
 
 
-def profile_step(precision: str):
+def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5):
     """One warm-up and one timed step of the workload, nothing else (the
-    command the committed ncu summaries under profiles/ were captured with)."""
+    command the committed ncu summaries under profiles/ were captured with):
+    the Dirichlet problem on 5120 panels, or the transmission least-squares
+    problem on the icosphere of subdivision `subdiv` (assembly and solve)."""
     import torch
     from bem_b200.managers import CoreManager
-    from bem_b200.workloads import helmholtz_dirichlet_s4
-    params, fD, fN = helmholtz_dirichlet_s4(precision=precision)
+    if workload == "dirichlet_s4":
+        from bem_b200.workloads import helmholtz_dirichlet_s4
+        params, fD, fN = helmholtz_dirichlet_s4(precision=precision)
+    else:
+        from bem_b200.workloads import transmission_s5
+        params, pw = transmission_s5(precision, subdiv, "lstsq")
+        fD, fN = pw.fD, pw.fN
     core = CoreManager(params)
     core.initialization(fD, fN)
     b = core._BEM_manager
@@ -964,7 +974,7 @@ def main():
             disk2d_bench(args.disk_n, 5, 3.0)
         return
     if args.profile_step:
-        profile_step(args.profile_step)
+        profile_step(args.profile_step, args.workload, args.trans_subdiv)
         return
     if args.profile_lu:
         profile_lu(args.profile_lu)

@@ -681,13 +681,15 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
         a.out[w] = (double*)out[w];
     }
     a.ld = ld;
-    // FP64 (and Laplace) default: both wavenumbers in one launch (measured
-    // faster than one launch per wavenumber on the 20480-panel transmission
-    // problem: 1602 vs 1736 ms FP64); group 1 keeps one per launch
+    // default with two wavenumbers: both in one scalar launch (measured on the
+    // 20480-panel transmission problem: FP64 1602 vs 1736 ms for one launch
+    // per wavenumber; mixed 656 ms, against 802 ms scalar and 750 ms packed
+    // FP32x2 per wavenumber); with one wavenumber the packed sweep is the
+    // mixed Helmholtz default
     int rc = BEM_OK;
     const int variant = ctx->tune[BEM_TUNE_CALDERON_GROUP];
-    if (fp32 && helm && (variant == 0 || variant == 3)) {
-        // default of the mixed Helmholtz sweep: packed FP32x2, one wavenumber per launch
+    if (fp32 && helm && (variant == 3 || (variant == 0 && nk == 1))) {
+        // packed FP32x2, one wavenumber per launch
         for (int w = 0; w < nk && !rc; ++w) {
             CalArgs b = a;
             b.k[0] = a.k[w];
