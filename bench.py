@@ -370,42 +370,61 @@ def profile_lu(n: int):
 
 def sweep_bench(n_k: int):
     """The wavenumber sweep (managers/sweep.py) of the augmented
-    transmission operator, mixed precision against the plain FP64 path; one
-    JSON line with per-k times, errors and the norm estimates."""
+    transmission operator over n_k wavenumbers, mixed precision against the
+    plain FP64 path, both with the same FP64 block-Krylov norm estimator;
+    one JSON line with per-k times, phases, errors and the norm estimates.
+    Each arm first lets the autotuner choose its Cholesky panel width
+    (cached per device and problem) and runs one untimed k."""
     import torch
     from bem_b200.managers import CoreManager
     from bem_b200.managers.sweep import wavenumber_sweep
+    from bem_b200.tuning import Autotuner
     from bem_b200.workloads import transmission_sweep_s4
-    res = {}
+    res, tuned = {}, {}
     for prec in ("mixed", "fp64"):
         params, fD, fN, ks = transmission_sweep_s4(prec, n_k)
+        params["solver"] = "lstsq"
         core = CoreManager(params)
         core.initialization(fD, fN)
-        # mixed: Krylov norm estimates; plain: the reference's own full SVD per k
-        kw = dict(nrhs=4, seed=0, norm_tol=1e-8, norm_method="iterative" if prec == "mixed" else "svd")
-        wavenumber_sweep(core._BEM_manager, ks[:1], **kw)  # warm-up
+        bm = core._BEM_manager
+        bm._k = ks[0]
+        tuned[prec] = bm.autotune(Autotuner(bm.engine))
+        kw = dict(nrhs=4, seed=0, norm_tol=1e-8, norm_method="iterative")
+        wavenumber_sweep(bm, ks[:1], **kw)  # warm-up
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res[prec] = wavenumber_sweep(core._BEM_manager, ks, **kw)
+        res[prec] = wavenumber_sweep(bm, ks, **kw)
         torch.cuda.synchronize()
         res[prec]["total_s"] = time.perf_counter() - t0
+        res[prec]["launches"] = bm.engine.launches
         core.kill()
     errs = [float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
             for a, b in zip(res["mixed"]["solutions"], res["fp64"]["solutions"])]
     nerr = [abs(a - b) / b for a, b in zip(res["mixed"]["inv_norm"], res["fp64"]["inv_norm"])]
+
+    def phases(r):
+        return {ph: statistics.mean(x[ph] for x in r["phase_ms"]) for ph in ("assemble", "norm", "lstsq")}
+
     print(json.dumps({
-        "workload": "augmented transmission sweep, icosphere s4, P1/P1 (5124 unknowns), GaussQR=3, "
-                    "n_i=3, n_o=1, 4 complex Gaussian RHS per k",
+        "workload": "augmented transmission sweep A_I, icosphere s4, P1/P1 (5124 unknowns, stacked 10248 x 5124), "
+                    "GaussQR=3, n_i=3, n_o=1, k = 16 + i/30, 4 complex Gaussian RHS per k",
         "n_k": len(res["mixed"]["k"]), "k_range": [res["mixed"]["k"][0], res["mixed"]["k"][-1]],
         "mixed_s": res["mixed"]["total_s"], "plain_fp64_s": res["fp64"]["total_s"],
         "speedup": res["fp64"]["total_s"] / res["mixed"]["total_s"],
         "ms_per_k_mixed": statistics.mean(res["mixed"]["ms"]), "ms_per_k_fp64": statistics.mean(res["fp64"]["ms"]),
+        "phase_ms_per_k": {"mixed": phases(res["mixed"]), "fp64": phases(res["fp64"])},
         "solution_rel_err_max": max(errs), "inv_norm_rel_diff_max": max(nerr),
         "inv_norm": res["mixed"]["inv_norm"], "cond": res["mixed"]["cond"],
-        "norm_method": {"mixed": "block Krylov of (S^H S)^{-1} (8-vector blocks, FP64 LU solves) and of S^H S, "
-                                 "Rayleigh-Ritz, stop at 1e-8 relative change",
-                        "plain_fp64": "full SVD per k (torch.linalg.svdvals), as the reference"},
+        "norm_method": "both arms: energy-scaled operator by FP64 DMMA products, block Krylov of (S^H S)^{-1} "
+                       "(8-vector blocks, FP64 LU solves) and of S^H S, Ritz values from the CGS2 R of S Q, "
+                       "stop at 1e-8 relative change",
+        "lstsq": {"mixed": "FP32 far-field assembly, FP16-split tcgen05 normal matrix, Cholesky with tcgen05 updates, "
+                           "FP64 flexible GMRES per RHS",
+                  "fp64": "FP64 assembly, DMMA normal matrix, Cholesky with DMMA updates, FP64 flexible GMRES "
+                          "per RHS"},
+        "autotuned": tuned,
         "norm_krylov_blocks": res["mixed"]["iterations"],
+        "gpu_launches": {"mixed": res["mixed"]["launches"], "fp64": res["fp64"]["launches"]},
     }))
 
 
@@ -715,6 +734,8 @@ def transmission_headline(args, ws, rank, local):
     nt = b.num_of_panels
     entries = 2 * n * n  # the stacked system [A; P+_i]
     peaks = measure_peaks(eng)
+    # launch shapes chosen by the autotuner (timed here, in the warm-up, unless cached)
+    tuned = {"mixed": b.autotune()}
     for _ in range(args.warmup):
         b.run()
     torch.cuda.synchronize()
@@ -789,6 +810,7 @@ def transmission_headline(args, ws, rank, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         c2 = make("mixed", vpin.numpy(), fpin.numpy())
+        c2._BEM_manager.autotune()  # the cached choices
         c2._BEM_manager.run()
         host = c2._BEM_manager.raw_solved.to("cpu")
         torch.cuda.synchronize()
@@ -802,6 +824,7 @@ def transmission_headline(args, ws, rank, local):
     # ---- plain FP64 path (its solution is the FP64 oracle of the error) ----
     core64 = make("fp64")
     b64 = core64._BEM_manager
+    tuned["fp64"] = b64.autotune()
     b64.run()
     torch.cuda.synchronize()
     ms64 = []
@@ -911,6 +934,7 @@ def transmission_headline(args, ws, rank, local):
             "plain_fp64": {"time_to_solution_ms": statistics.mean(ms64), "step_ms": ms64, "breakdown_ms": p64,
                            "solve": info64},
             "speedup_vs_plain_fp64": statistics.mean(ms64) / ms,
+            "autotuned": tuned,
             "rel_err_vs_fp64": {"l2_rel": rel2, "max_abs_rel": relm},
             "qr_check": qr,
             "solve": info,

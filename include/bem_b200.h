@@ -348,6 +348,25 @@ int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, i
  * pivot was not positive.  Queued without synchronising. */
 int bem_chol_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int method, int32_t* piv, void* dinv,
                     int32_t* info, void* stream);
+/* C += alpha op(A) op(B) in FP64 on the FP64 tensor cores (DMMA), dtype
+ * BEM_F64 or BEM_C128, row-major: op(A) = A (m x k, lda) or, with conj_a, A^H
+ * (A stored k x m); op(B) = B (k x n, ldb) or, with conj_b, B^H (B stored
+ * n x k).  Products with few output tiles split K (FP64 atomic sums, so the
+ * last bits depend on the order).  The matrix products of the reference's
+ * operator-norm analysis (compute_inv_norm, BEM_manager.py:874-920: the
+ * scaled operator L^{-1} A L^{-H}) and of the Krylov estimators that replace
+ * its SVD.  Queued without synchronising. */
+int bem_gemm(bem_ctx* ctx, int dtype, int conj_a, int conj_b, int64_t m, int64_t n, int64_t k, double alpha,
+             const void* A, int64_t lda, const void* B, int64_t ldb, void* C, int64_t ldc, void* stream);
+/* X = L^{-1} with A = L L^H (the torch.linalg.inv(torch.linalg.cholesky(MV))
+ * of compute_inv_norm, BEM_manager.py:885-899): the FP64 Cholesky of A in
+ * place (L in the lower triangle; the upper triangle is left as it was),
+ * then the lower-triangular inverse into X (n x n, ldx; zero above the
+ * diagonal), both on the FP64 tensor cores.  A, X: BEM_F64 or BEM_C128.
+ * info: device int32, 0 or 1 + the first column whose pivot was not
+ * positive (X is then not valid).  Queued without synchronising. */
+int bem_chol_inverse(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, void* X, int64_t ldx, int32_t* info,
+                     void* stream);
 /* The solve half of the same lstsq call (BEM_manager.py:1049): x (device, n,
  * FP64 real or complex, holding the initial guess) is refined by flexible
  * GMRES(restart) in FP64 on the scaled normal equations, with FP64 products

@@ -244,6 +244,36 @@ class Engine:
                                              _ptr(dinv), _ptr(info), _stream_ptr()))
         return piv, dinv, info
 
+    def gemm(self, A, B, C, alpha=1.0, conj_a=False, conj_b=False):
+        """C += alpha op(A) op(B) in FP64 on the FP64 tensor cores (bem_gemm);
+        op(X) = X^H where conj_x.  A, B, C: complex128 or float64 (all the
+        same), row-major with unit column stride."""
+        dt = C.dtype
+        assert dt in (torch.complex128, torch.float64) and A.dtype == dt and B.dtype == dt
+        assert A.is_cuda and B.is_cuda and C.is_cuda and A.stride(1) == 1 and B.stride(1) == 1 and C.stride(1) == 1
+        m, n = C.shape
+        k = A.shape[0] if conj_a else A.shape[1]
+        assert (A.shape[1] if conj_a else A.shape[0]) == m
+        assert (B.shape[1] if conj_b else B.shape[0]) == k and (B.shape[0] if conj_b else B.shape[1]) == n
+        self._check(self.lib.bem_gemm(self.ctx, _dtype_code(C), int(bool(conj_a)), int(bool(conj_b)), m, n, k,
+                                      float(alpha), _ptr(A), A.stride(0), _ptr(B), B.stride(0), _ptr(C), C.stride(0),
+                                      _stream_ptr()))
+        return C
+
+    def chol_inverse(self, A: torch.Tensor, X: torch.Tensor | None = None):
+        """L^{-1} for A = L L^H (bem_chol_inverse): A (complex128 or float64,
+        lower triangle read) is overwritten by L in its lower triangle.
+        Returns (X, info)."""
+        n = A.shape[0]
+        assert A.is_cuda and A.shape == (n, n) and A.stride(1) == 1 and A.dtype in (torch.complex128, torch.float64)
+        if X is None:
+            X = torch.empty_like(A)
+        assert X.shape == (n, n) and X.stride(1) == 1 and X.dtype == A.dtype
+        info = torch.zeros(1, dtype=torch.int32, device=A.device)
+        self._check(self.lib.bem_chol_inverse(self.ctx, _dtype_code(A), _ptr(A), n, A.stride(0), _ptr(X), X.stride(0),
+                                              _ptr(info), _stream_ptr()))
+        return X, info
+
     def lstsq_refine(self, A, P, colscale, LU, piv, dinv, b, x, tol=1e-14, maxit=60, restart=30, accept=1e-10):
         """Flexible GMRES in FP64 on the scaled normal equations of
         min ||[A; P] x - b|| (bem_lstsq_refine); x holds the initial guess.

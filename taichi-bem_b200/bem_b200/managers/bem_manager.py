@@ -118,8 +118,9 @@ class BEMManager:
         self.device = torch.device(p.get("device", "cuda"))
         self.torch_dtype = torch.complex128 if self._n == 2 else torch.float64
         self.conj_data = (self._n == 2) and self.quirk
-        self._L1_inv_H = None
-        self._L2_inv_H = None
+        # L^{-1} of the energy scalings of A_I and A_II (compute_inv_norm)
+        self._L1_inv = None
+        self._L2_inv = None
         self.solve_info = {}
         self.initialized = False
 
@@ -405,8 +406,15 @@ class BEMManager:
         stacked transmission system, BEM_manager.py:1039-1050) by the
         column-equilibrated normal equations: the normal matrix on the tensor
         cores (FP16-split products in mixed precision, FP64 products on the
-        plain path), its tile LU (FP32 / FP64), and flexible GMRES in FP64 on
-        the normal equations against the FP64-stored A and P."""
+        plain path), its Cholesky, and flexible GMRES in FP64 on the normal
+        equations against the FP64-stored A and P."""
+        return self.lstsq_multi(A, P, b.view(-1, 1))[:, 0]
+
+    def lstsq_multi(self, A: torch.Tensor, P: torch.Tensor, B: torch.Tensor) -> torch.Tensor:
+        """min ||[A; P] x - b|| for each column b of B (2n x nrhs): one normal
+        matrix and Cholesky, one flexible GMRES per column (see _lstsq).
+        Returns X (n x nrhs); solve_info holds the last column's iterations
+        and residual and the largest iteration count."""
         n = A.shape[0]
         mixed = self.solve_precision == "mixed"
         # the factor is a Cholesky with an FP64 Schur complement on both
@@ -418,18 +426,23 @@ class BEMManager:
         Nm = torch.empty(n, n, dtype=A.dtype, device=A.device)
         self.engine.gram(A, P, Nm, d, tensor_cores=mixed)
         piv, dinv, info = self.engine.chol_factor(Nm, tensor_cores=mixed)
-        x = torch.zeros(n, dtype=A.dtype, device=A.device)
-        its, rr = self.engine.lstsq_refine(A, P, d, Nm, piv, dinv, b, x, tol=self.lstsq_tol,
-                                           maxit=self.lstsq_maxit, restart=30, accept=self.lstsq_accept)
         if int(info.item()) > 0:
             raise torch.linalg.LinAlgError("linalg.lstsq: the stacked system is rank deficient (its normal matrix "
                                            f"has no positive pivot in column {int(info.item()) - 1})")
+        X = torch.zeros(n, B.shape[1], dtype=A.dtype, device=A.device)
+        its_max = 0
+        for c in range(B.shape[1]):
+            x = torch.zeros(n, dtype=A.dtype, device=A.device)
+            its, rr = self.engine.lstsq_refine(A, P, d, Nm, piv, dinv, B[:, c].contiguous(), x, tol=self.lstsq_tol,
+                                               maxit=self.lstsq_maxit, restart=30, accept=self.lstsq_accept)
+            X[:, c] = x
+            its_max = max(its_max, its)
         self.solve_info = {"factor": ("fp16-split tcgen05 normal matrix, Cholesky with tcgen05 updates" if mixed
                                       else "fp64 DMMA normal matrix, Cholesky with DMMA updates")
                            + " (FP64 Schur complement), fp64 flexible GMRES",
-                           "info": info, "refine_iters": its, "relres": rr}
+                           "info": info, "refine_iters": its, "relres": rr, "refine_iters_max": its_max}
         del Nm, dinv
-        return x
+        return X
 
     def solve(self):
         n = self.N_Neumann + self.M_Dirichlet
@@ -650,60 +663,72 @@ class BEMManager:
     def compute_inv_norm(self, A: torch.Tensor, A_type: int, method: str = "svd", return_cond: bool = False):
         """||A^{-1}|| in the energy-scaled norm (BEM_manager.py:874-920).
 
-        The scaling L^{-H} (L the Cholesky factor of blockdiag(W, V) of A for
-        A_type 1, of blockdiag(K', K) for A_type 2, shifted by `_shifted`) is
-        formed on the first call
-        and kept, as in the reference; the reference's sweep makes that call at
-        k = 0.  The scaled operator L^{-1} A L^{-H} (block-diagonal left factor
-        for the augmented 2n x n operator) has its smallest singular value
-        sigma_min; the result is 1 / sigma_min.  method "svd" takes all
-        singular values as the reference does; "iterative" estimates the
-        extreme ones by inverse / power iteration with this library's LU
-        (managers/sweep.py); "none" only forms the scaling.  With
+        The scaling (L the Cholesky factor of blockdiag(W, V) of A for A_type
+        1, of blockdiag(K', K) for A_type 2, shifted by `_shifted`) is formed
+        on the first call and kept, as in the reference (whose sweep makes that
+        call at k = 0): L^{-1} by bem_chol_inverse.  The scaled operator
+        S = L^{-1} A L^{-H} (block-diagonal left factor for the augmented
+        2n x n operator) is formed by bem_gemm in FP64; its smallest singular
+        value sigma_min gives the result 1 / sigma_min.  method "svd" takes all
+        singular values as the reference does (torch.linalg.svdvals, the
+        reference's own call); "iterative" estimates the extreme ones by
+        block Krylov spaces on this library's kernels
+        (sweep.extreme_singular_values); "none" only forms the scaling.  With
         return_cond the result is (1 / sigma_min, sigma_max / sigma_min,
-        iterations)."""
+        Krylov blocks)."""
         n = self.N_Neumann + self.M_Dirichlet
         top = A[:n]
-        if self._L1_inv_H is None and A_type == 1:
+        if self._L1_inv is None and A_type == 1:
             MV = torch.zeros_like(top)
             Do, No = self._Dirichlet_offset_i, self._Neumann_offset_i
             MV[Do:Do + self.M_Dirichlet, self._Dirichlet_offset_j:self._Dirichlet_offset_j + self.M_Dirichlet] = \
                 self.get_W_part(top)
             MV[No:No + self.N_Neumann, self._Neumann_offset_j:self._Neumann_offset_j + self.N_Neumann] = \
                 self.get_V_part(top)
-            MV = (MV + MV.transpose(0, 1)) / 2.0
-            self._L1_inv_H = torch.linalg.inv(torch.linalg.cholesky(self._shifted(MV), upper=False)) \
-                .transpose(0, 1).conj()
-            self._L2_inv_H = None
-        elif self._L2_inv_H is None and A_type == 2:
+            self._L1_inv = self._scaling_inverse((MV + MV.transpose(0, 1)) / 2.0)
+            self._L2_inv = None
+        elif self._L2_inv is None and A_type == 2:
             MV = torch.block_diag(self.get_adj_K_part(top), self.get_K_part(top))
-            self._L2_inv_H = torch.linalg.inv(torch.linalg.cholesky(self._shifted(MV), upper=False)) \
-                .transpose(0, 1).conj()
-            self._L1_inv_H = None
+            self._L2_inv = self._scaling_inverse(MV)
+            self._L1_inv = None
         if method == "none":
             return None
-        Linv_H = self._L1_inv_H if A_type == 1 else self._L2_inv_H
-        S = A @ Linv_H
-        LH = Linv_H.transpose(0, 1).conj().contiguous()
-        if A.shape[0] == n:
-            S = LH @ S
-        elif A.shape[0] == 2 * n:
-            S = torch.cat((LH @ S[:n], LH @ S[n:]), 0)
-        else:
-            raise NotImplementedError("We only support Non-Augmentd matrix and Augmented Matrix for Norm analysis")
+        Linv = self._L1_inv if A_type == 1 else self._L2_inv
+        if A.shape[0] not in (n, 2 * n):
+            raise NotImplementedError("the norm analysis takes the square operator (n x n) or the augmented one "
+                                      "(2n x n)")
+        blocks = []
+        T = torch.zeros(n, n, dtype=A.dtype, device=A.device)
+        for r0 in range(0, A.shape[0], n):
+            T.zero_()
+            self.engine.gemm(Linv, A[r0:r0 + n].contiguous(), T)
+            Sb = torch.zeros(n, n, dtype=A.dtype, device=A.device)
+            self.engine.gemm(T, Linv, Sb, conj_b=True)
+            blocks.append(Sb)
+        del T
         if method == "svd":
-            sv = torch.linalg.svdvals(S)
+            sv = torch.linalg.svdvals(torch.cat(blocks, 0))
             smin, smax, its = float(sv.min()), float(sv.max()), 0
         elif method == "iterative":
-            from .sweep import smallest_singular_value
-            smin, smax, its = smallest_singular_value(self.engine, S.contiguous(), tol=self.norm_tol,
-                                                      maxit=self.norm_maxit)
+            from .sweep import extreme_singular_values
+            smin, smax, its = extreme_singular_values(self.engine, blocks, tol=self.norm_tol, maxit=self.norm_maxit)
         else:
             raise ValueError(method)
         inv = 1.0 / smin if smin > 0 else float("inf")
         if return_cond:
             return inv, smax * inv, its
         return inv
+
+    def _scaling_inverse(self, MV: torch.Tensor) -> torch.Tensor:
+        """L^{-1} for the Cholesky factor L of MV, shifted (`_shifted`; the
+        lower triangle is read, as torch.linalg.cholesky reads it), on this
+        library's FP64 Cholesky and triangular inverse (bem_chol_inverse)."""
+        H = self._shifted(MV).contiguous()
+        X, info = self.engine.chol_inverse(H)
+        if int(info.item()) != 0:
+            raise torch.linalg.LinAlgError("the energy-scaling block is not positive definite (Cholesky pivot "
+                                           f"{int(info.item()) - 1})")
+        return X
 
     def get_mat_A1_inv_norm(self, k: float, method: str = "svd"):
         """A_I = P^-_o - P^+_i (BEM_manager.py:922-936)."""
@@ -824,6 +849,49 @@ class BEMManager:
                                                 sqrt_no=self._sqrt_no)
             self.rhs_layer_forward(k=self._k, scope_type=self._scope_type)
             self.assemble_rhs()
+
+    def autotune(self, tuner=None) -> dict:
+        """Choose the launch shapes of this problem's hot calls on this GPU
+        (bem_b200.tuning): the form of the fused Calderon sweep (transmission
+        problems it takes; candidates 2: both wavenumbers in one scalar
+        launch, 3: packed FP32x2 per wavenumber, 1: scalar per wavenumber),
+        timed on assemble_system, and for the least-squares solver the
+        Cholesky panel width (512, 1024, 2048), timed on the factorisation of
+        this problem's normal matrix.  Cached choices are applied without
+        timing.  Returns {key name: value}."""
+        from ..tuning import Autotuner
+        tuner = tuner or Autotuner(self.engine)
+        n = self.N_Neumann + self.M_Dirichlet
+        wl = f"{self._simulation_parameters['kernel']}/n{n}/Q{self._GaussQR}/{self.precision}-{self.solve_precision}"
+        out = {}
+        if self._is_transmission and self._calderon_fusable():
+            out["calderon_group"] = tuner.tune(wl + "/calderon", L.TUNE_CALDERON_GROUP, [2, 3, 1],
+                                               self.assemble_system)
+        nbs = [512, 1024, 2048]
+        if self._is_transmission and self.solver == "lstsq" and tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs):
+            out["chol_nb"] = tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs)
+        elif self._is_transmission and self.solver == "lstsq":
+            mixed = self.solve_precision == "mixed"
+            self.assemble_system()
+            if self._mat_P is not None and self._calderon_fusable():
+                A, P = self._mat_A, self._mat_P
+            else:
+                A = self._mat_A.clone()
+                self._mat_A.zero_()
+                self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
+                P = self._mat_A.clone()
+            Nm = torch.empty(n, n, dtype=A.dtype, device=A.device)
+            d = torch.empty(n, dtype=torch.float64, device=A.device)
+            self.engine.gram(A, P, Nm, d, tensor_cores=mixed)
+            W = torch.empty_like(Nm)
+
+            def factor():
+                W.copy_(Nm)
+                self.engine.chol_factor(W, tensor_cores=mixed)
+
+            out["chol_nb"] = tuner.tune(wl + "/chol", L.TUNE_CHOL_NB, nbs, factor)
+            del W, Nm, A, P
+        return out
 
     def kill(self):
         self.initialized = False

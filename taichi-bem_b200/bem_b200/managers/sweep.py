@@ -1,91 +1,197 @@
 """Wavenumber sweeps of the transmission operator: operator-norm and
-condition estimates and batched augmented least-squares solves.
+condition estimates and augmented least-squares solves, on this library's
+kernels.
 
 The reference computes ||A^{-1}|| in an energy-scaled norm with a full SVD
 of the scaled (augmented) operator for every wavenumber
 (`compute_inv_norm`, `BEM_manager.py:874-920`, driven by
-`demo/demo_3d_plot_Sio.py:66-104`).  Here the extreme singular values come
-from block Krylov spaces of the Gram matrix G = S^H S and of its inverse,
-applied with this library's LU factor and triangular solves
-(`smallest_singular_value`); the Ritz values converge to the SVD's smallest
-and largest singular values.
+`demo/demo_3d_plot_Sio.py:63-104`).  Here the extreme singular values come
+from block Krylov spaces of the Gram matrix G = S^H S and of its inverse
+(`extreme_singular_values`); the Ritz values converge to the SVD's smallest
+and largest singular values.  Every O(n^3) and O(n^2) step runs on this
+library's FP64 kernels: the scaled operator by bem_gemm (DMMA), G by
+bem_gram (DMMA), its LU by bem_lu_factor, the bases by classical
+Gram-Schmidt with one re-orthogonalisation (CGS2) on bem_gemm products.  The
+host sees only the p x p triangle of the Ritz step (p <= a few hundred), whose
+singular values numpy takes.
 """
 from __future__ import annotations
 
 import math
 import time
 
+import numpy as np
 import torch
 
 from ..utils.types import AssembleType, ScopeType
 
 
-def _orthonormalize(X: torch.Tensor) -> torch.Tensor:
-    """Orthonormal basis of the block's columns (Householder QR of the n x p
-    block; inverse iteration makes the columns nearly parallel, where
-    Gram-Schmidt or Cholesky-QR lose orthogonality or break down)."""
-    return torch.linalg.qr(X, mode="reduced")[0]
+class Basis:
+    """Orthonormal columns Q (n x j, FP64 real or complex, at most `cap`)
+    grown column by column by CGS2 on bem_gemm products:
+        h = Q^H v,  v -= Q h   (twice),   r_jj = ||v||,  q_j = v / r_jj,
+    so that appended columns W satisfy W = Q R with R upper triangular (kept
+    on the host when `keep_r`).  A column whose norm falls below 1e-13 of its
+    original norm (numerically inside span(Q)) is replaced by a seeded random
+    vector, with a zero column in R."""
 
+    def __init__(self, engine, n, cap, dtype, device, seed=0, keep_r=False):
+        self.engine = engine
+        self.Q = torch.zeros(n, cap, dtype=dtype, device=device)
+        self.j = 0
+        self.cap = cap
+        self.keep_r = keep_r
+        self.R = np.zeros((cap, cap), np.complex128 if dtype.is_complex else np.float64)
+        self.gen = torch.Generator(device=device).manual_seed(seed)
+        self._h = torch.zeros(cap, 1, dtype=dtype, device=device)
+        self._nrm = torch.zeros(1, 1, dtype=dtype, device=device)
 
-def _krylov_ritz(S: torch.Tensor, apply, X0: torch.Tensor, maxblocks: int, which: int, tol: float):
-    """Grow a block Krylov basis Q = [X0, op X0, op^2 X0, ...] (fully
-    re-orthogonalised) of the Hermitian operator `apply`, and after 2, 4, 8 ...
-    blocks take the Ritz value of G = S^H S on span(Q) from the singular values
-    of S Q: the smallest (which = 0) or largest (which = -1).  Stops
-    when it changes by less than `tol` (relative) or at `maxblocks` blocks.
-    Returns (Ritz value, blocks)."""
-    blocks = [_orthonormalize(X0)]
-    SQ = [S @ blocks[0]]
-    prev, check = None, 2
-    while True:
-        if len(blocks) == min(check, maxblocks):
-            # singular values of S Q (Q orthonormal): min / max of |S x| over span(Q)
-            sv = torch.linalg.svdvals(torch.cat(SQ, 1))
-            lam = float(sv[-1] if which == 0 else sv[0]) ** 2
-            if (prev is not None and abs(lam - prev) <= tol * abs(lam)) or len(blocks) >= maxblocks:
-                return lam, len(blocks)
-            prev, check = lam, 2 * check
-        W = apply(blocks[-1])
-        Q = torch.cat(blocks, 1)
+    @property
+    def active(self) -> torch.Tensor:
+        return self.Q[:, :self.j]
+
+    def _norm(self, v) -> float:
+        self._nrm.zero_()
+        self.engine.gemm(v, v, self._nrm, conj_a=True)
+        return math.sqrt(max(float(self._nrm.real.item() if self._nrm.is_complex() else self._nrm.item()), 0.0))
+
+    def _project(self, v, r):
+        if self.j == 0:
+            return
         for _ in range(2):
-            W = W - Q @ (Q.conj().transpose(0, 1) @ W)
-        blocks.append(_orthonormalize(W))
-        SQ.append(S @ blocks[-1])
+            h = self._h[:self.j]
+            h.zero_()
+            self.engine.gemm(self.active, v, h, conj_a=True)
+            self.engine.gemm(self.active, h, v, alpha=-1.0)
+            if r is not None:
+                r[:self.j] += h[:, 0].cpu().numpy()
+
+    def append(self, W: torch.Tensor) -> int:
+        """Append the columns of W (n x p); returns the number appended (the
+        basis stops at `cap`)."""
+        added = 0
+        for c in range(W.shape[1]):
+            if self.j >= self.cap:
+                break
+            v = W[:, c:c + 1].contiguous()
+            nrm0 = self._norm(v)
+            r = np.zeros(self.cap, self.R.dtype) if self.keep_r else None
+            self._project(v, r)
+            nrm = self._norm(v)
+            r_jj = nrm
+            if not nrm > 1e-13 * nrm0:
+                # inside the span: W's column is Q r (r_jj = 0); the basis
+                # continues with a random direction
+                r_jj = 0.0
+                v = torch.randn(v.shape, dtype=torch.float64, device=v.device, generator=self.gen)
+                if self.Q.is_complex():
+                    v = torch.complex(v, torch.randn(v.shape, dtype=torch.float64, device=v.device,
+                                                     generator=self.gen))
+                v = v.contiguous()
+                self._project(v, None)
+                nrm = self._norm(v)
+            self.Q[:, self.j:self.j + 1] = v / nrm
+            if self.keep_r:
+                r[self.j] = r_jj
+                self.R[:, self.j] = r
+            self.j += 1
+            added += 1
+        return added
 
 
-def smallest_singular_value(engine, S: torch.Tensor, block: int = 8, tol: float = 1e-10, tol_max: float = 1e-7,
+def _ritz(engine, S_blocks, Q: torch.Tensor, rbasis: Basis, which: int) -> float:
+    """Append S q for the new columns q of Q to `rbasis` (the CGS2 basis of
+    S Q with its R) and return the extreme squared singular value of S Q,
+    i.e. the Ritz value of G = S^H S on span(Q): relative accuracy eps
+    cond(S), where the Gram form Q^H G Q would have eps cond(S)^2."""
+    n = Q.shape[0]
+    SQ = torch.zeros(sum(b.shape[0] for b in S_blocks), Q.shape[1], dtype=Q.dtype, device=Q.device)
+    r0 = 0
+    for B in S_blocks:
+        engine.gemm(B, Q, SQ[r0:r0 + B.shape[0]])
+        r0 += B.shape[0]
+    assert r0 == SQ.shape[0] and n == S_blocks[0].shape[1]
+    rbasis.append(SQ)
+    sv = np.linalg.svd(rbasis.R[:rbasis.j, :rbasis.j], compute_uv=False)
+    return float(sv[-1] if which == 0 else sv[0]) ** 2
+
+
+def _krylov_ritz(engine, S_blocks, apply, X0, maxblocks: int, which: int, tol: float, seed: int):
+    """Grow a block Krylov basis [X0, op X0, op^2 X0, ...] (CGS2) of the
+    Hermitian operator `apply`; after 2, 4, 8 ... blocks take the Ritz value
+    of G = S^H S on the basis: the smallest (which = 0) or largest (-1)
+    squared singular value of S Q.  Stops when it changes by less than `tol`
+    (relative) or at `maxblocks` blocks.  Returns (Ritz value, blocks)."""
+    n, p = X0.shape
+    cap = p * maxblocks
+    basis = Basis(engine, n, cap, X0.dtype, X0.device, seed=seed)
+    rbasis = Basis(engine, sum(b.shape[0] for b in S_blocks), cap, X0.dtype, X0.device, seed=seed + 1,
+                   keep_r=True)
+    basis.append(X0)
+    done_cols, nblocks = 0, 1
+    prev, check, lam = None, 2, 0.0
+    while True:
+        if nblocks == min(check, maxblocks):
+            lam = _ritz(engine, S_blocks, basis.Q[:, done_cols:basis.j].contiguous(), rbasis, which)
+            done_cols = basis.j
+            if (prev is not None and abs(lam - prev) <= tol * abs(lam)) or nblocks >= maxblocks:
+                return lam, nblocks
+            prev, check = lam, 2 * check
+        last = basis.Q[:, basis.j - p:basis.j].contiguous()
+        if basis.append(apply(last)) == 0:
+            return lam, nblocks
+        nblocks += 1
+
+
+def extreme_singular_values(engine, S_blocks, block: int = 8, tol: float = 1e-10, tol_max: float = 1e-7,
                             maxit: int = 24, seed: int = 0, info: dict | None = None):
-    """(sigma_min, sigma_max, Krylov blocks) of S (m x n, m >= n).
+    """(sigma_min, sigma_max, Krylov blocks) of S = [S_0; S_1; ...] (row
+    blocks, each m_i x n, sum m_i >= n).
 
-    sigma_min^2 is the smallest eigenvalue of G = S^H S.  A block Krylov
-    space of G^{-1} (block size `block`; each step one multi-right-hand-side
-    solve with the FP64 LU of G, bem_lu_factor / bem_lu_solve) is grown until
-    the smallest Ritz value of G on it changes by less than `tol` (relative)
-    between two sizes, at most `maxit` blocks.  sigma_max^2 likewise from the
-    Krylov space of G itself (`tol_max`).  The Ritz values come from the
-    singular values of the thin matrix S Q, with relative error eps * cond(S)
-    (a Gram matrix Q^H G Q would carry eps * cond(S)^2).
-    """
-    n = S.shape[1]
-    G = (S.conj().transpose(0, 1) @ S).contiguous()
-    gen = torch.Generator(device=S.device).manual_seed(seed)
+    sigma_min^2 is the smallest eigenvalue of G = S^H S.  G is formed by the
+    FP64 normal-matrix kernel (bem_gram, column scaling D: G^ = D G D) or, for
+    one block, bem_gemm; its LU (bem_lu_factor, FP64) gives G^{-1} = D G^^{-1}
+    D.  A block Krylov space of G^{-1} (block size `block`, one
+    multi-right-hand-side solve per step) is grown until the smallest Ritz
+    value changes by less than `tol` (relative) between two sizes, at most
+    `maxit` blocks; sigma_max^2 likewise from the Krylov space of G
+    (`tol_max`)."""
+    n = S_blocks[0].shape[1]
+    dt, dev = S_blocks[0].dtype, S_blocks[0].device
+    G = torch.zeros(n, n, dtype=dt, device=dev)
+    d = torch.ones(n, dtype=torch.float64, device=dev)
+    if len(S_blocks) == 2 and S_blocks[0].shape[0] == n and S_blocks[1].shape[0] == n:
+        engine.gram(S_blocks[0], S_blocks[1], G, d, tensor_cores=False)
+    else:
+        for B in S_blocks:
+            engine.gemm(B, B, G, conj_a=True)
+    gen = torch.Generator(device=dev).manual_seed(seed)
     p = min(block, n)
-    X = torch.randn(n, p, dtype=torch.float64, device=S.device, generator=gen)
-    if S.is_complex():
-        X = torch.complex(X, torch.randn(n, p, dtype=torch.float64, device=S.device, generator=gen))
+    X = torch.randn(n, p, dtype=torch.float64, device=dev, generator=gen)
+    if dt.is_complex:
+        X = torch.complex(X, torch.randn(n, p, dtype=torch.float64, device=dev, generator=gen))
+    dcol = d.to(dt).view(n, 1)
     LU = G.clone()
     piv, finfo = engine.lu_factor(LU)
+    nmax = max(1, min(maxit, n // p))
+
+    def apply_g(V):
+        # G V = D^{-1} G^ D^{-1} V
+        Y = torch.zeros_like(V)
+        engine.gemm(G, (V / dcol).contiguous(), Y)
+        return Y / dcol
+
+    lam_max, _ = _krylov_ritz(engine, S_blocks, apply_g, X, nmax, -1, tol_max, seed + 10)
     if int(finfo.item()) != 0:
-        return 0.0, math.sqrt(float(torch.linalg.matrix_norm(G, 2).real)), 0
+        return 0.0, math.sqrt(max(lam_max, 0.0)), 0
 
     def solve(V):
-        Y = V.clone().contiguous()
+        # G^{-1} V = D G^^{-1} D V
+        Y = (V * dcol).contiguous()
         engine.lu_solve(LU, piv, Y)
-        return Y
+        return Y * dcol
 
-    nmax = max(1, min(maxit, n // p))
-    lam_min, nb_min = _krylov_ritz(S, solve, X, nmax, 0, tol)
-    lam_max, _ = _krylov_ritz(S, lambda V: G @ V, X, nmax, -1, tol_max)
+    lam_min, nb_min = _krylov_ritz(engine, S_blocks, solve, X, nmax, 0, tol, seed + 20)
     if info is not None:
         info["blocks"] = nb_min
     return math.sqrt(max(lam_min, 0.0)), math.sqrt(max(lam_max, 0.0)), nb_min
@@ -101,22 +207,26 @@ def transmission_operator(bm, k: float, A_type: int = 1, augmented: bool = True)
     bm.assemble_matA(assemble_type=int(AssembleType.ADD_P_MINUS), multiplier=1.0)
     bm.matrix_layer_forward(k=k, sqrt_n=bm._sqrt_ni, scope_type=int(ScopeType.INTERIOR))
     bm.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=-1.0 if A_type == 1 else 1.0)
-    A = bm._mat_A.clone()
+    n = bm._mat_A.shape[0]
     if not augmented:
-        return A
+        return bm._mat_A.clone()
+    At = torch.empty(2 * n, n, dtype=bm._mat_A.dtype, device=bm._mat_A.device)
+    At[:n].copy_(bm._mat_A)
     bm._mat_A.zero_()
     bm.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
-    return torch.cat((A, bm._mat_A), 0)
+    At[n:].copy_(bm._mat_A)
+    return At
 
 
 def wavenumber_sweep(bm, ks, nrhs: int = 4, seed: int = 0, A_type: int = 1, scaling_k: float = 0.0,
                      norm_method: str = "iterative", norm_tol: float | None = None, norm_maxit: int | None = None):
-    """For each k in `ks`: the augmented transmission operator [A(k); P^+_i(k)],
-    the inverse norm and condition number of its energy-scaled form, and the
+    """For each k in `ks`: the augmented transmission operator [A(k); P^+_i(k)]
+    (get_augment_mat_A{1,2}_inv_norm, BEM_manager.py:952-988), the inverse
+    norm and condition number of its energy-scaled form, and the
     least-squares solutions of [A; P^+_i] x = [b; 0] for `nrhs` seed-fixed
-    complex Gaussian right-hand sides b.  The least-squares problems are
-    solved through their normal equations with the manager's solver (mixed
-    precision: FP32 tile LU + FP64 refinement; fp64: partial-pivoting LU).
+    complex Gaussian right-hand sides b, by the manager's least-squares
+    solver (normal matrix, Cholesky, flexible GMRES in FP64; tensor cores in
+    mixed precision, DMMA on the plain path), one factorisation per k.
 
     The energy scaling is formed once, at `scaling_k` (the reference forms it
     on its first call, which the reference's sweep makes at k = 0).  norm_tol
@@ -126,32 +236,38 @@ def wavenumber_sweep(bm, ks, nrhs: int = 4, seed: int = 0, A_type: int = 1, scal
         bm.norm_tol = norm_tol
     if norm_maxit is not None:
         bm.norm_maxit = norm_maxit
-    bm._L1_inv_H = bm._L2_inv_H = None
+    bm._L1_inv = bm._L2_inv = None
     if A_type == 1:
         bm.get_mat_A1_inv_norm(scaling_k, method="none")
     else:
         bm.get_mat_A2_inv_norm(scaling_k, method="none")
     gen = torch.Generator(device=bm.device).manual_seed(seed)
-    out = {"k": [], "inv_norm": [], "cond": [], "solutions": [], "ms": [], "iterations": []}
+    out = {"k": [], "inv_norm": [], "cond": [], "solutions": [], "rhs": [], "ms": [], "iterations": [],
+           "phase_ms": []}
     for k in ks:
         torch.cuda.synchronize(bm.device)
         t0 = time.perf_counter()
         At = transmission_operator(bm, float(k), A_type, augmented=True)
-        inv_norm, cond, its = bm.compute_inv_norm(At, A_type, method=norm_method, return_cond=True)
-        b = torch.complex(torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen),
-                          torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen))
-        A, P = At[:n], At[n:]
-        AH = A.conj().transpose(0, 1)
-        Gn = (AH @ A + P.conj().transpose(0, 1) @ P).contiguous()
-        rhs = (AH @ b).contiguous()
-        X = bm._lu_solve_square(Gn, rhs)
         torch.cuda.synchronize(bm.device)
-        out["ms"].append((time.perf_counter() - t0) * 1e3)
+        t1 = time.perf_counter()
+        inv_norm, cond, its = bm.compute_inv_norm(At, A_type, method=norm_method, return_cond=True)
+        torch.cuda.synchronize(bm.device)
+        t2 = time.perf_counter()
+        B = torch.zeros(2 * n, nrhs, dtype=torch.complex128, device=bm.device)
+        B[:n] = torch.complex(torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen),
+                              torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen))
+        X = bm.lstsq_multi(At[:n], At[n:], B)
+        torch.cuda.synchronize(bm.device)
+        t3 = time.perf_counter()
+        out["ms"].append((t3 - t0) * 1e3)
+        out["phase_ms"].append({"assemble": (t1 - t0) * 1e3, "norm": (t2 - t1) * 1e3, "lstsq": (t3 - t2) * 1e3})
         out["k"].append(float(k))
         out["inv_norm"].append(inv_norm)
         out["cond"].append(cond)
         out["iterations"].append(its)
         out["solutions"].append(X)
+        out["rhs"].append(B[:n])
+        del At
     return out
 
 

@@ -155,11 +155,18 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-template <bool CPLX, bool CONJT, bool LOWER>
+// C (m x n, ldc) += alpha op(A) op(B) on the FP64 tensor cores (DMMA,
+// m8n8k4), 64 x 64 tiles per CTA, 8-wide K stages.  op(A) = A (m x k) or
+// A^H (A stored k x m, CONJA); op(B) = B (k x n) or B^H (B stored n x k,
+// CONJT).  LOWER skips the tiles strictly above the diagonal shifted by
+// `diag`.  blockIdx.z takes the K range [z kchunk, (z + 1) kchunk); with more
+// than one range the tiles are added with FP64 atomics (split K for thin
+// products).
+template <bool CPLX, bool CONJA, bool CONJT, bool LOWER>
 __global__ void __launch_bounds__(256) dmma_gemm_kernel(double* __restrict__ Cm, int64_t ldc,
                                                          const double* __restrict__ Am, int64_t lda,
                                                          const double* __restrict__ Bm, int64_t ldb, int64_t m,
-                                                         int64_t n, int k, double alpha, int64_t diag) {
+                                                         int64_t n, int k, double alpha, int64_t diag, int kchunk) {
     constexpr int W = CPLX ? 2 : 1;
     constexpr int NP = CPLX ? 2 : 1;
     __shared__ double sA[NP][DG_BK][DG_LDS];
@@ -179,45 +186,60 @@ __global__ void __launch_bounds__(256) dmma_gemm_kernel(double* __restrict__ Cm,
     const int ar_ = tid >> 2, ak_ = (tid & 3) * 2;
     const int bk_ = tid >> 5, bc_ = (tid & 31) * 2;
     double ra[2][NP], rb[2][NP];
+    const int kbeg = (int)blockIdx.z * kchunk, kend = min(k, kbeg + kchunk);
     auto fetch = [&](int k0) {
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            const int64_t gr = m0 + ar_;
+            if (CONJA) {
+                // A^H: k row tid/32, row pair 2 (tid%32), read along A's rows (coalesced)
+                const int gka = k0 + bk_;
+                const int64_t gr = m0 + bc_ + e;
+                const bool ok = gr < m && gka < kend;
+                const int64_t ia = W * ((int64_t)gka * lda + gr);
+                ra[e][0] = ok ? Am[ia] : 0.0;
+                if (CPLX) ra[e][NP - 1] = ok ? -Am[ia + 1] : 0.0;
+            } else {
+                const int64_t gr = m0 + ar_;
+                const int gk = k0 + ak_ + e;
+                const bool ok = gr < m && gk < kend;
+                const int64_t ia = W * (gr * lda + gk);
+                ra[e][0] = ok ? Am[ia] : 0.0;
+                if (CPLX) ra[e][NP - 1] = ok ? Am[ia + 1] : 0.0;
+            }
             const int gk = k0 + ak_ + e;
-            const bool ok = gr < m && gk < k;
-            const int64_t ia = W * (gr * lda + gk);
-            ra[e][0] = ok ? Am[ia] : 0.0;
-            if (CPLX) ra[e][NP - 1] = ok ? Am[ia + 1] : 0.0;
             if (CONJT) {
                 const int64_t gc = n0 + ar_;
-                const bool okb = gc < n && gk < k;
+                const bool okb = gc < n && gk < kend;
                 const int64_t ib = W * (gc * ldb + gk);
                 rb[e][0] = okb ? Bm[ib] : 0.0;
                 if (CPLX) rb[e][NP - 1] = okb ? -Bm[ib + 1] : 0.0;
             } else {
                 const int gkb = k0 + bk_;
                 const int64_t gc = n0 + bc_ + e;
-                const bool okb = gkb < k && gc < n;
+                const bool okb = gkb < kend && gc < n;
                 const int64_t ib = W * ((int64_t)gkb * ldb + gc);
                 rb[e][0] = okb ? Bm[ib] : 0.0;
                 if (CPLX) rb[e][NP - 1] = okb ? Bm[ib + 1] : 0.0;
             }
         }
     };
-    fetch(0);
-    for (int k0 = 0; k0 < k; k0 += DG_BK) {
+    fetch(kbeg);
+    for (int k0 = kbeg; k0 < kend; k0 += DG_BK) {
 #pragma unroll
         for (int e = 0; e < 2; ++e)
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                sA[p][ak_ + e][ar_] = ra[e][p];
+                if (CONJA)
+                    sA[p][bk_][bc_ + e] = ra[e][p];
+                else
+                    sA[p][ak_ + e][ar_] = ra[e][p];
                 if (CONJT)
                     sB[p][ak_ + e][ar_] = rb[e][p];
                 else
                     sB[p][bk_][bc_ + e] = rb[e][p];
             }
         __syncthreads();
-        if (k0 + DG_BK < k) fetch(k0 + DG_BK);
+        if (k0 + DG_BK < kend) fetch(k0 + DG_BK);
 #pragma unroll
         for (int k4 = 0; k4 < DG_BK; k4 += 4) {
             const int kr = k4 + (lane & 3);
@@ -254,8 +276,14 @@ __global__ void __launch_bounds__(256) dmma_gemm_kernel(double* __restrict__ Cm,
             for (int e = 0; e < 2; ++e) {
                 const int64_t gc = n0 + 16 * wc + 8 * b + 2 * (lane & 3) + e;
                 if (gc >= n) continue;
-                Cm[W * (gr * ldc + gc)] += alpha * acc[a][b][0][e];
-                if (CPLX) Cm[W * (gr * ldc + gc) + 1] += alpha * acc[a][b][NP - 1][e];
+                double* c = Cm + W * (gr * ldc + gc);
+                if (gridDim.z > 1) {
+                    atomicAdd(c, alpha * acc[a][b][0][e]);
+                    if (CPLX) atomicAdd(c + 1, alpha * acc[a][b][NP - 1][e]);
+                } else {
+                    c[0] += alpha * acc[a][b][0][e];
+                    if (CPLX) c[1] += alpha * acc[a][b][NP - 1][e];
+                }
             }
         }
 }
@@ -293,20 +321,39 @@ __global__ void iota_kernel(int32_t* piv, int n) {
     if (i < n) piv[i] = i;
 }
 
-template <bool C, bool CONJT, bool LOWER>
-int gemm64(bem_ctx* ctx, double* Cm, int64_t ldc, const double* A, int64_t lda, const double* B, int64_t ldb,
-           int64_t m, int64_t n, int k, double alpha, int64_t diag, cudaStream_t s) {
+// C += alpha op(A) op(B) (see dmma_gemm_kernel); products with fewer tiles
+// than two waves of CTAs split K into ranges of at least 512.
+template <bool C, bool CONJA, bool CONJT, bool LOWER>
+int gemm64x(bem_ctx* ctx, double* Cm, int64_t ldc, const double* A, int64_t lda, const double* B, int64_t ldb,
+            int64_t m, int64_t n, int k, double alpha, int64_t diag, cudaStream_t s) {
     if (m <= 0 || n <= 0 || k <= 0) return BEM_OK;
     dim3 grid((unsigned)((n + DG_BM - 1) / DG_BM), (unsigned)((m + DG_BM - 1) / DG_BM));
     if (grid.y > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "dmma_gemm_kernel: m too large");
-    dmma_gemm_kernel<C, CONJT, LOWER><<<grid, 256, 0, s>>>(Cm, ldc, A, lda, B, ldb, m, n, k, alpha, diag);
+    const int64_t tiles = (int64_t)grid.x * grid.y;
+    int splits = 1;
+    if (!LOWER && tiles < 2 * (int64_t)ctx->num_sms)
+        splits = (int)std::max<int64_t>(1, std::min<int64_t>((2 * ctx->num_sms) / tiles, k / 512));
+    const int kchunk = (int)(((int64_t)k + splits - 1) / splits + DG_BK - 1) / DG_BK * DG_BK;
+    grid.z = (unsigned)(((int64_t)k + kchunk - 1) / kchunk);
+    dmma_gemm_kernel<C, CONJA, CONJT, LOWER><<<grid, 256, 0, s>>>(Cm, ldc, A, lda, B, ldb, m, n, k, alpha, diag,
+                                                                    kchunk);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "dmma_gemm_kernel");
 }
 
+template <bool C, bool CONJT, bool LOWER>
+int gemm64(bem_ctx* ctx, double* Cm, int64_t ldc, const double* A, int64_t lda, const double* B, int64_t ldb,
+           int64_t m, int64_t n, int k, double alpha, int64_t diag, cudaStream_t s) {
+    return gemm64x<C, false, CONJT, LOWER>(ctx, Cm, ldc, A, lda, B, ldb, m, n, k, alpha, diag, s);
+}
+
+// The blocked Cholesky.  With X == nullptr the factor is left in tile-LU
+// form (piv, dinv); otherwise L stays in the lower triangle and each diagonal
+// tile's inverse L_jj^{-1} is written into X's diagonal tile (X, ldx: the
+// start of bem_chol_inverse's triangular inverse).
 template <bool C>
 int chol_t(bem_ctx* ctx, double* A, int64_t n, int64_t lda, bool tensor_cores, int32_t* piv, double* dinv,
-           int32_t* info, cudaStream_t s) {
+           int32_t* info, cudaStream_t s, double* X = nullptr, int64_t ldx = 0) {
     const int W = C ? 2 : 1;
     const int ni = (int)n;
     // workspace: the inverse of the current 64 x 64 factor, the L21 product, the diagonal
@@ -331,6 +378,13 @@ int chol_t(bem_ctx* ctx, double* A, int64_t n, int64_t lda, bool tensor_cores, i
             chol64_kernel<C><<<1, 256, smem, s>>>(at(j0, j0), lda, jb, inv, info, (int)j0);
             ctx->launches++;
             if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "chol64_kernel")) return rc;
+            if (X)
+                if (int rc = bem_check_cuda(ctx, cudaMemcpy2DAsync(X + W * (j0 * ldx + j0), sizeof(double) * W * ldx,
+                                                                   inv, sizeof(double) * W * CH_IB,
+                                                                   sizeof(double) * W * jb, jb,
+                                                                   cudaMemcpyDeviceToDevice, s),
+                                            "diagonal inverse copy"))
+                    return rc;
             const int64_t r1 = j0 + jb, m1 = n - r1;
             if (m1 <= 0) continue;
             // L21 = A21 L11^{-H}: into tmp, then back into A21
@@ -361,6 +415,7 @@ int chol_t(bem_ctx* ctx, double* A, int64_t n, int64_t lda, bool tensor_cores, i
                 return rc;
         }
     }
+    if (X) return BEM_OK;
     // the factor in tile-LU form, identity tile pivots, inverses of the diagonal tiles
     diag_copy_kernel<C><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, lda, ni, dg);
     const unsigned nb16 = (unsigned)((n + 15) / 16);
@@ -371,7 +426,89 @@ int chol_t(bem_ctx* ctx, double* A, int64_t n, int64_t lda, bool tensor_cores, i
     return bem_tile_inverses(ctx, C ? BEM_C128 : BEM_F64, A, n, lda, dinv, s);
 }
 
+// X = L^{-1} for the lower triangle of L (n x n, lda) whose diagonal tiles'
+// inverses are already in X's diagonal tiles (the rest of X zero), by the
+// recursion on halves (rounded to 64 rows)
+//   L = [L11 0; L21 L22],  L^{-1} = [X11 0; -X22 L21 X11  X22],
+// the two products on the FP64 tensor cores; ws holds L21 X11.
+template <bool C>
+int tri_inv_rec(bem_ctx* ctx, const double* L, int64_t lda, double* X, int64_t ldx, int64_t lo, int64_t hi,
+                double* ws, cudaStream_t s) {
+    const int W = C ? 2 : 1;
+    if (hi - lo <= CH_IB) return BEM_OK;
+    const int64_t mid = lo + ((hi - lo) / 2 + CH_IB - 1) / CH_IB * CH_IB;
+    if (int rc = tri_inv_rec<C>(ctx, L, lda, X, ldx, lo, mid, ws, s)) return rc;
+    if (int rc = tri_inv_rec<C>(ctx, L, lda, X, ldx, mid, hi, ws, s)) return rc;
+    const int64_t m1 = mid - lo, m2 = hi - mid;
+    if (int rc = bem_check_cuda(ctx, cudaMemsetAsync(ws, 0, sizeof(double) * W * m2 * m1, s), "tri_inv ws")) return rc;
+    // ws = L21 X11 (X11 lower triangular: the product's K range is all of it)
+    if (int rc = gemm64x<C, false, false, false>(ctx, ws, m1, L + W * (mid * lda + lo), lda, X + W * (lo * ldx + lo),
+                                                 ldx, m2, m1, (int)m1, 1.0, 0, s))
+        return rc;
+    // X21 = -X22 ws
+    return gemm64x<C, false, false, false>(ctx, X + W * (mid * ldx + lo), ldx, X + W * (mid * ldx + mid), ldx, ws,
+                                           m1, m2, m1, (int)m2, -1.0, 0, s);
+}
+
 }  // namespace
+
+extern "C" int bem_gemm(bem_ctx* ctx, int dtype, int conj_a, int conj_b, int64_t m, int64_t n, int64_t k,
+                        double alpha, const void* A, int64_t lda, const void* B, int64_t ldb, void* Cm, int64_t ldc,
+                        void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (m < 0 || n < 0 || k < 0 || k > (1 << 30) || !Cm || ldc < n || (m > 0 && n > 0 && k > 0 && (!A || !B)))
+        return bem_fail(ctx, BEM_ERR_INVALID, "gemm: bad arguments");
+    if (lda < (conj_a ? m : k) || ldb < (conj_b ? k : n)) return bem_fail(ctx, BEM_ERR_INVALID, "gemm: bad leading dimension");
+    if (dtype != BEM_C128 && dtype != BEM_F64) return bem_fail(ctx, BEM_ERR_INVALID, "gemm: dtype must be F64 or C128");
+    cudaStream_t s = (cudaStream_t)stream;
+    const double* a = (const double*)A;
+    const double* b = (const double*)B;
+    double* c = (double*)Cm;
+    const int kk = (int)k;
+#define BEM_GEMM_CASE(CX, CA, CB) \
+    return gemm64x<CX, CA, CB, false>(ctx, c, ldc, a, lda, b, ldb, m, n, kk, alpha, 0, s)
+    if (dtype == BEM_C128) {
+        if (conj_a) {
+            if (conj_b) BEM_GEMM_CASE(true, true, true);
+            BEM_GEMM_CASE(true, true, false);
+        }
+        if (conj_b) BEM_GEMM_CASE(true, false, true);
+        BEM_GEMM_CASE(true, false, false);
+    }
+    if (conj_a) {
+        if (conj_b) BEM_GEMM_CASE(false, true, true);
+        BEM_GEMM_CASE(false, true, false);
+    }
+    if (conj_b) BEM_GEMM_CASE(false, false, true);
+    BEM_GEMM_CASE(false, false, false);
+#undef BEM_GEMM_CASE
+}
+
+extern "C" int bem_chol_inverse(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, void* X, int64_t ldx,
+                                int32_t* info, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!A || !X || !info || n <= 0 || lda < n || ldx < n || n > (1 << 28))
+        return bem_fail(ctx, BEM_ERR_INVALID, "chol_inverse: bad arguments");
+    if (dtype != BEM_C128 && dtype != BEM_F64)
+        return bem_fail(ctx, BEM_ERR_INVALID, "chol_inverse: A must be F64 or C128");
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool C = dtype == BEM_C128;
+    const int W = C ? 2 : 1;
+    if (int rc = bem_check_cuda(ctx, cudaMemset2DAsync(X, sizeof(double) * W * ldx, 0, sizeof(double) * W * n, n, s),
+                                "chol_inverse zero"))
+        return rc;
+    double* a = (double*)A;
+    double* x = (double*)X;
+    int rc = C ? chol_t<true>(ctx, a, n, lda, false, nullptr, nullptr, info, s, x, ldx)
+               : chol_t<false>(ctx, a, n, lda, false, nullptr, nullptr, info, s, x, ldx);
+    if (rc) return rc;
+    // the recursion's scratch: L21 X11 of the top level, at most (n/2 + 64)^2
+    const int64_t h = n / 2 + CH_IB;
+    void* ws = nullptr;
+    if (int e = bem_big_ws(ctx, sizeof(double) * W * h * h, &ws)) return e;
+    return C ? tri_inv_rec<true>(ctx, a, lda, x, ldx, 0, n, (double*)ws, s)
+             : tri_inv_rec<false>(ctx, a, lda, x, ldx, 0, n, (double*)ws, s);
+}
 
 extern "C" int bem_chol_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int method, int32_t* piv,
                                void* dinv, int32_t* info, void* stream) {

@@ -79,6 +79,9 @@ int bem_fgmres(bem_ctx* ctx, bool C, int64_t n, const std::function<int(const do
 // panel L (m x kb, ld), FP64 sums (bem_lstsq.cu).
 int bem_herk_tc_update(bem_ctx* ctx, bool C, const double* L, int64_t ld, int m, int kb, double* out, int64_t ldo,
                        cudaStream_t s);
+// A device buffer of at least `bytes` owned by the context (grown, never
+// shrunk; freed with it), for scratch that lives within one call.
+int bem_big_ws(bem_ctx* ctx, size_t bytes, void** out);
 // Explicit inverses of the 64 x 64 diagonal tiles of a tile-LU factor into
 // dinv (bem_tilelu.cu); dtype BEM_F64/C128/F32/C64.
 int bem_tile_inverses(bem_ctx* ctx, int dtype, const void* A, int64_t n, int64_t lda, void* dinv, cudaStream_t s);

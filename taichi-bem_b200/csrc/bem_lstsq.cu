@@ -832,6 +832,8 @@ int mirror(bem_ctx* ctx, T* out, int64_t ldo, int n, cudaStream_t s) {
 
 }  // namespace
 
+int bem_big_ws(bem_ctx* ctx, size_t bytes, void** out) { return big_ws(ctx, bytes, out); }
+
 int bem_herk_tc_update(bem_ctx* ctx, bool C, const double* L, int64_t ld, int m, int kb, double* out, int64_t ldo,
                        cudaStream_t s) {
     if (m <= 0 || kb <= 0) return BEM_OK;

@@ -52,8 +52,9 @@ def test_driver_mixed_precision(name):
     core, b = _run(d, precision="mixed")
     core.run()
     ref = to_complex(d["raw_solved"])
-    # FP32 far field: ~1e-7 relative entry error; refinement converges on the FP64-stored matrix
-    assert rel_err(b.raw_solved.cpu().numpy(), ref) < 1e-5
+    # FP32 far field: ~1e-7 relative entry error; refinement converges on the
+    # FP64-stored matrix; the bound is the stated mixed-precision tolerance
+    assert rel_err(b.raw_solved.cpu().numpy(), ref) < 1e-6
     assert b.solve_info["relres"] <= 1e-12
     core.kill()
 

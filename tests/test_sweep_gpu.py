@@ -106,3 +106,20 @@ def test_sweep_mixed_matches_fp64():
         assert rel_err(b_.cpu().numpy(), a.cpu().numpy()) < 1e-6
     for a, b_ in zip(out["fp64"]["inv_norm"], out["mixed"]["inv_norm"]):
         assert abs(a - b_) <= 1e-5 * a
+
+
+def test_sweep_solutions_match_oracle_lstsq():
+    """The sweep's mixed-precision least-squares solutions against numpy's
+    lstsq (the reference's torch.linalg.lstsq, BEM_manager.py:1049) of the
+    oracle's stacked [A_I; P+_i] with the same right-hand sides."""
+    from bem_b200.managers.sweep import wavenumber_sweep
+    core, v, f = _manager("mixed")
+    out = wavenumber_sweep(core._BEM_manager, KS, nrhs=2, seed=1)
+    core.kill()
+    for k, X, B in zip(KS, out["solutions"], out["rhs"]):
+        A, Pp, _ = _oracle_ops(v, f, k, 1)
+        n = A.shape[0]
+        Sa = np.concatenate([A, Pp], 0)
+        rhs = np.concatenate([B.cpu().numpy(), np.zeros((n, B.shape[1]))], 0)
+        ref = np.linalg.lstsq(Sa, rhs, rcond=None)[0]
+        assert rel_err(X.cpu().numpy(), ref) < 1e-6
