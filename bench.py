@@ -490,15 +490,18 @@ def shape_bench(subdiv: int, n_check: int):
     }))
 
 
-def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
+def transmission_bench(subdiv: int, plain: bool, solver: str = "lstsq"):
     """The Helmholtz transmission system (k_out = 5, k_in = 7.5) on
-    icosphere s<subdiv> in mixed precision (FP32 far field, FP64 near field,
-    TF32 tile LU + FP64 refinement on the square system), its error against
-    the FP64-assembled system solved to FP64 accuracy, and dJ/dk of
-    J = ||x||^2 by the adjoint against a central difference of J."""
+    icosphere s<subdiv> in mixed precision (solver "lstsq": the reference's
+    least squares, tensor-core normal matrix and Cholesky, FP64 GMRES;
+    "square": TF32 tile LU + FP64 refinement of the square system), its error
+    against the FP64 path, and dJ/dk of J = ||x||^2 by the adjoint with the
+    analytic operator derivative (managers/kderiv.py), in mixed precision and
+    in FP64, against the fourth-order central difference of the FP64 J
+    (delta = 5e-3)."""
     import torch
     from bem_b200.managers import CoreManager
-    from bem_b200.managers.sweep import solution_norm_k_gradient
+    from bem_b200.managers.kderiv import solution_norm_k_gradient
     from bem_b200.workloads import transmission_s5
     res = {}
     params, pw = transmission_s5("mixed", subdiv, solver)
@@ -514,18 +517,25 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "square"):
     res["refinement"] = {k: (v if not hasattr(v, "item") else v.item()) for k, v in b.solve_info.items()}
     x_mixed = b.raw_solved.clone()
     n = b.N_Neumann + b.M_Dirichlet
-    g = solution_norm_k_gradient(b, pw, delta=1e-3, check=True) if solver == "square" else None
-    res["dJdk"] = None if g is None else {"J": g["J"], "adjoint": g["dJdk"], "central_difference": g["dJdk_central_difference"],
-                   "rel_diff": abs(g["dJdk"] - g["dJdk_central_difference"]) / abs(g["dJdk_central_difference"]),
-                   "adjoint_ms": g["adjoint_ms"], "delta": 1e-3}
+    gm = solution_norm_k_gradient(b, pw, check=False)
     core.kill()
     params, pw = transmission_s5("fp64", subdiv, solver)
-    params.update(solve_precision="mixed", refine_tol=1e-13)
+    if solver == "square":
+        params.update(solve_precision="mixed", refine_tol=1e-13)
     core = CoreManager(params)
     core.initialization(pw.fD, pw.fN)
     core._BEM_manager.run()
     x64 = core._BEM_manager.raw_solved.clone()
+    g64 = solution_norm_k_gradient(core._BEM_manager, pw, check=True, delta=5e-3)
     core.kill()
+    cd = g64["dJdk_central_difference"]
+    res["dJdk"] = {"J": g64["J"], "central_difference_fp64": cd, "central_difference": g64["central_difference"],
+                   "adjoint_mixed": gm["dJdk"], "rel_diff_mixed": abs(gm["dJdk"] - cd) / abs(cd),
+                   "adjoint_fp64": g64["dJdk"], "rel_diff_fp64": abs(g64["dJdk"] - cd) / abs(cd),
+                   "mixed_ms": {k: gm[k] for k in ("solve_ms", "adjoint_solve_ms", "derivative_assembly_ms",
+                                                    "contraction_ms")},
+                   "fp64_ms": {k: g64[k] for k in ("solve_ms", "adjoint_solve_ms", "derivative_assembly_ms",
+                                                    "contraction_ms")}}
     res["rel_err_vs_fp64"] = {"l2": float(torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)),
                               "max": float((x_mixed - x64).abs().max() / x64.abs().max())}
     if plain:
@@ -961,11 +971,11 @@ def main():
     ap.add_argument("--profile-lu", type=int, default=0,
                     help="time six tiled FP32 factorisations of a random complex matrix of this size and exit")
     ap.add_argument("--workload", default="transmission_s5",
-                    choices=["transmission_s5", "dirichlet_s4", "sweep", "shape", "transmission_square", "disk2d"],
+                    choices=["transmission_s5", "dirichlet_s4", "sweep", "shape", "transmission_dk", "disk2d"],
                     help="transmission_s5: the headline line (the 20480-panel transmission problem); dirichlet_s4: "
                          "Helmholtz interior Dirichlet on 5120 panels; sweep: the wavenumber sweep of the "
                          "augmented transmission operator; shape: the shape gradient on a perturbed sphere; "
-                         "transmission_square: the square transmission system with dJ/dk; disk2d: the 2D operators "
+                         "transmission_dk: the transmission solve with dJ/dk through the adjoint; disk2d: the 2D operators "
                          "(each its own JSON line)")
     ap.add_argument("--plain-steps", type=int, default=1, help="timed steps of the plain FP64 comparator")
     ap.add_argument("--qr-check", action="store_true",
@@ -976,8 +986,8 @@ def main():
     ap.add_argument("--shape-check", type=int, default=32, help="vertices of the finite-difference check")
     ap.add_argument("--trans-subdiv", type=int, default=5, help="icosphere subdivision of the transmission workload")
     ap.add_argument("--trans-plain", action="store_true", help="also time the plain FP64 path (FP64 LU)")
-    ap.add_argument("--trans-solver", default="square", choices=["square", "lstsq"],
-                    help="solver of the transmission_square workload")
+    ap.add_argument("--trans-solver", default="lstsq", choices=["square", "lstsq"],
+                    help="solver of the transmission_dk workload")
     ap.add_argument("--sweep-k", type=int, default=60, help="number of wavenumbers of the sweep workload")
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -989,7 +999,7 @@ def main():
         if rank == 0:
             shape_bench(args.shape_subdiv, args.shape_check)
         return
-    if args.workload == "transmission_square":
+    if args.workload == "transmission_dk":
         if rank == 0:
             transmission_bench(args.trans_subdiv, args.trans_plain, args.trans_solver)
         return

@@ -69,6 +69,13 @@ typedef struct {
     int quirk;       /* 1: the reference's Sauter-Schwab orientation/basis handling;
                         0: shared vertex/edge moved to the map's singular point   */
     int precision;   /* BEM_PREC_*                                               */
+    int deriv_k;     /* 1: the derivative of the Helmholtz kernel in its
+                        wavenumber k at fixed k2 (dG/dk = i r G for V and W,
+                        whose k2 mass term keeps its coefficient; d/dk of
+                        grad G for K and K'), for bem_assemble and bem_apply
+                        only (no reference counterpart: the k-derivative of
+                        the operators of single_layer_3d.py:55-369 and
+                        BEM_manager.py:476-517); 0 otherwise            */
 } bem_op_desc;
 
 /* One side (test or trial) of an operator block: the reference's local panel
@@ -380,6 +387,13 @@ int bem_lstsq_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int6
                      const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
                      const void* dinv, const void* b, void* x, double tol, int maxit, int restart, double accept,
                      int* iters, double* relres, void* stream);
+/* The same iteration for a normal-equation right-hand side (no reference
+ * counterpart; the adjoint solve of the k-derivative of that lstsq):
+ * (A^H A + P^H P) x = g, g: device [n]. */
+int bem_normal_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld,
+                      const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
+                      const void* dinv, const void* g, void* x, double tol, int maxit, int restart, double accept,
+                      int* iters, double* relres, void* stream);
 
 /* ---- post-processing (headless) ------------------------------------------------
  * The two kernels the reference runs at the end of BEMManager.run for its

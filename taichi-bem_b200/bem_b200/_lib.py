@@ -36,7 +36,7 @@ EXPORTS = [
     "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet", "bem_lu_solve_tiled_static",
     "bem_adjoint_vertices", "bem_mesh_set_2d", "bem_gmres_ir", "bem_compute_color", "bem_set_mesh_instances",
     "bem_lu_factor_status", "bem_binary_version", "bem_ctx_set_tuning", "bem_assemble_calderon", "bem_gram",
-    "bem_lstsq_refine", "bem_chol_factor", "bem_gemm", "bem_chol_inverse",
+    "bem_lstsq_refine", "bem_chol_factor", "bem_gemm", "bem_chol_inverse", "bem_normal_refine",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 TUNE_CALDERON_GROUP = 0  # BEM_TUNE_CALDERON_GROUP
@@ -52,7 +52,7 @@ class BemError(RuntimeError):
 
 class OpDesc(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int), ("kernel", ctypes.c_int), ("k", ctypes.c_double), ("k2", ctypes.c_double),
-                ("quirk", ctypes.c_int), ("precision", ctypes.c_int)]
+                ("quirk", ctypes.c_int), ("precision", ctypes.c_int), ("deriv_k", ctypes.c_int)]
 
 
 class Space(ctypes.Structure):
@@ -113,6 +113,7 @@ def load():
     L.bem_gram.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, i32, vp, i64, vp]
     L.bem_lstsq_refine.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, vp, i64, vp, vp, vp, vp, dbl, i32, i32, dbl,
                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), vp]
+    L.bem_normal_refine.argtypes = list(L.bem_lstsq_refine.argtypes)
     L.bem_assemble_calderon.argtypes = [vp, ctypes.POINTER(OpDesc), i32, ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Space), ctypes.POINTER(Space),
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_double), i64, vp]

@@ -148,9 +148,11 @@ class Engine:
 
     # -- operators ------------------------------------------------------------
     @staticmethod
-    def op_desc(op, helmholtz, k=0.0, k2=0.0, quirk=True, precision=L.PREC_FP64):
+    def op_desc(op, helmholtz, k=0.0, k2=0.0, quirk=True, precision=L.PREC_FP64, deriv_k=False):
+        """deriv_k: the operator of the kernel's k-derivative at fixed k2
+        (Helmholtz; bem_assemble and bem_apply)."""
         return L.OpDesc(int(op), L.KERNEL_HELMHOLTZ if helmholtz else L.KERNEL_LAPLACE, float(k), float(k2),
-                        1 if quirk else 0, int(precision))
+                        1 if quirk else 0, int(precision), 1 if deriv_k else 0)
 
     def _check_spaces(self, test, trial, nrow, ncol):
         for sp in (test, trial):
@@ -243,6 +245,20 @@ class Engine:
         self._check(self.lib.bem_chol_factor(self.ctx, _dtype_code(A), _ptr(A), n, A.stride(0), method, _ptr(piv),
                                              _ptr(dinv), _ptr(info), _stream_ptr()))
         return piv, dinv, info
+
+    def normal_refine(self, A, P, colscale, LU, piv, dinv, g, x, tol=1e-14, maxit=60, restart=30, accept=1e-10):
+        """(A^H A + P^H P) x = g (g: n) by the flexible GMRES of lstsq_refine
+        (bem_normal_refine); x holds the initial guess.  Returns
+        (iterations, relative residual)."""
+        n = A.shape[0]
+        assert g.numel() == n and g.is_contiguous() and x.is_contiguous() and x.numel() == n
+        it = ctypes.c_int(0)
+        rr = ctypes.c_double(0.0)
+        self._check(self.lib.bem_normal_refine(self.ctx, _dtype_code(A), _ptr(A), _ptr(P), n, A.stride(0),
+                                               _ptr(colscale), _dtype_code(LU), _ptr(LU), LU.stride(0), _ptr(piv),
+                                               _ptr(dinv), _ptr(g), _ptr(x), float(tol), int(maxit), int(restart),
+                                               float(accept), ctypes.byref(it), ctypes.byref(rr), _stream_ptr()))
+        return it.value, rr.value
 
     def gemm(self, A, B, C, alpha=1.0, conj_a=False, conj_b=False):
         """C += alpha op(A) op(B) in FP64 on the FP64 tensor cores (bem_gemm);

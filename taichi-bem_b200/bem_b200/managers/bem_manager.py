@@ -118,6 +118,11 @@ class BEMManager:
         self.device = torch.device(p.get("device", "cuda"))
         self.torch_dtype = torch.complex128 if self._n == 2 else torch.float64
         self.conj_data = (self._n == 2) and self.quirk
+        # operator descriptors of the k-derivative pass (managers/kderiv.py):
+        # the kernel's k-derivative, and a replacement W mass coefficient k2
+        self._desc_deriv_k = False
+        self._desc_k2 = None
+        self._lstsq_factor = None
         # L^{-1} of the energy scalings of A_I and A_II (compute_inv_norm)
         self._L1_inv = None
         self._L2_inv = None
@@ -213,9 +218,11 @@ class BEMManager:
         uses_n = self._kernel_type == int(KernelType.HELMHOLTZ_TRANSMISSION)
         k_kernel = k * sqrt_n if uses_n else k
         k2 = k * k * sqrt_n * sqrt_n
+        if self._desc_k2 is not None:
+            k2 = self._desc_k2
         prec = L.PREC_MIXED if self.precision == "mixed" else L.PREC_FP64
         return Engine.op_desc(op, helm, k_kernel if helm else 0.0, k2 if helm else 0.0, quirk=self.quirk,
-                              precision=prec)
+                              precision=prec, deriv_k=self._desc_deriv_k)
 
     # -- accessors ------------------------------------------------------------------
     def get_GaussQR(self):
@@ -410,11 +417,12 @@ class BEMManager:
         equations against the FP64-stored A and P."""
         return self.lstsq_multi(A, P, b.view(-1, 1))[:, 0]
 
-    def lstsq_multi(self, A: torch.Tensor, P: torch.Tensor, B: torch.Tensor) -> torch.Tensor:
+    def lstsq_multi(self, A: torch.Tensor, P: torch.Tensor, B: torch.Tensor, keep_factor: bool = False) -> torch.Tensor:
         """min ||[A; P] x - b|| for each column b of B (2n x nrhs): one normal
         matrix and Cholesky, one flexible GMRES per column (see _lstsq).
         Returns X (n x nrhs); solve_info holds the last column's iterations
-        and residual and the largest iteration count."""
+        and residual and the largest iteration count.  With keep_factor the
+        factor stays in _lstsq_factor (normal_solve)."""
         n = A.shape[0]
         mixed = self.solve_precision == "mixed"
         # the factor is a Cholesky with an FP64 Schur complement on both
@@ -441,20 +449,38 @@ class BEMManager:
                                       else "fp64 DMMA normal matrix, Cholesky with DMMA updates")
                            + " (FP64 Schur complement), fp64 flexible GMRES",
                            "info": info, "refine_iters": its, "relres": rr, "refine_iters_max": its_max}
+        self._lstsq_factor = (A, P, d, Nm, piv, dinv) if keep_factor else None
         del Nm, dinv
         return X
+
+    def normal_solve(self, g: torch.Tensor) -> torch.Tensor:
+        """(A^H A + P^H P)^{-1} g with the factor kept by the last
+        lstsq_multi(keep_factor=True): the adjoint solve of the least-squares
+        problem, by the same FP64 flexible GMRES (bem_normal_refine)."""
+        A, P, d, Nm, piv, dinv = self._lstsq_factor
+        x = torch.zeros_like(g)
+        its, rr = self.engine.normal_refine(A, P, d, Nm, piv, dinv, g.contiguous(), x, tol=self.lstsq_tol,
+                                            maxit=self.lstsq_maxit, restart=30, accept=self.lstsq_accept)
+        self.solve_info["adjoint_iters"], self.solve_info["adjoint_relres"] = its, rr
+        return x
+
+    def transmission_blocks(self):
+        """(A, P+_i) of the assembled transmission system: the fused path's
+        two matrices, or A saved and P+_i assembled into _mat_A from the
+        interior layers (as the reference does before its lstsq,
+        BEM_manager.py:1039-1047)."""
+        if self._mat_P is not None and self._calderon_fusable():
+            return self._mat_A, self._mat_P
+        A_top = self._mat_A.clone()
+        self._mat_A.zero_()
+        self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
+        return A_top, self._mat_A.clone()
 
     def solve(self):
         n = self.N_Neumann + self.M_Dirichlet
         if self._is_transmission:
             # the reference stacks [A; P+_i] and calls lstsq (BEM_manager.py:1039-1050)
-            if self._mat_P is not None and self._calderon_fusable():
-                A_top, P = self._mat_A, self._mat_P
-            else:
-                A_top = self._mat_A.clone()
-                self._mat_A.zero_()
-                self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
-                P = self._mat_A.clone()
+            A_top, P = self.transmission_blocks()
             if self.solver == "lstsq":
                 sol = self._lstsq(A_top.contiguous(), P.contiguous(), self.rhs.contiguous())
             else:
@@ -873,13 +899,7 @@ class BEMManager:
         elif self._is_transmission and self.solver == "lstsq":
             mixed = self.solve_precision == "mixed"
             self.assemble_system()
-            if self._mat_P is not None and self._calderon_fusable():
-                A, P = self._mat_A, self._mat_P
-            else:
-                A = self._mat_A.clone()
-                self._mat_A.zero_()
-                self.assemble_matA(assemble_type=int(AssembleType.ADD_P_PLUS), multiplier=1.0)
-                P = self._mat_A.clone()
+            A, P = self.transmission_blocks()
             Nm = torch.empty(n, n, dtype=A.dtype, device=A.device)
             d = torch.empty(n, dtype=torch.float64, device=A.device)
             self.engine.gram(A, P, Nm, d, tensor_cores=mixed)

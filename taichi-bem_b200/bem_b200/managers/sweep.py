@@ -269,58 +269,3 @@ def wavenumber_sweep(bm, ks, nrhs: int = 4, seed: int = 0, A_type: int = 1, scal
         out["rhs"].append(B[:n])
         del At
     return out
-
-
-def solution_norm_k_gradient(bm, data=None, delta: float = 1e-3, check: bool = True):
-    """J(k) = ||x(k)||^2 for the manager's system A(k) x = b(k) at its
-    wavenumber k (square transmission system: solver "square"), and dJ/dk by
-    the adjoint method:
-        A^H lam = x,     dJ/dk = 2 Re lam^H (db/dk - (dA/dk) x),
-    with dA/dk x and db/dk from central differences (k +- delta) of the
-    assembled operator and right-hand side, and the adjoint solve by the
-    manager's solver on A^H.  `data` is the boundary-data object whose `k`
-    follows the operator's (e.g. workloads.PlaneWave).  With `check`, also the
-    central difference of J itself (two more solves).  Returns a dict."""
-    n = bm.N_Neumann + bm.M_Dirichlet
-    k0 = bm._k
-
-    def system(k):
-        bm._k = k
-        if data is not None:
-            data.k = k
-        bm.assemble_system()
-        return bm._mat_A.clone(), bm.rhs[:n].clone()
-
-    out = {}
-    torch.cuda.synchronize(bm.device)
-    t0 = time.perf_counter()
-    A, b = system(k0)
-    x = bm._lu_solve_square(A, b)
-    torch.cuda.synchronize(bm.device)
-    out["solve_ms"] = (time.perf_counter() - t0) * 1e3
-    out["solve_info"] = dict(bm.solve_info)
-    J = float(torch.vdot(x, x).real)
-    t1 = time.perf_counter()
-    Ap, bp = system(k0 + delta)
-    r = bp - Ap @ x
-    del Ap
-    Am, bm_ = system(k0 - delta)
-    r = (r - (bm_ - Am @ x)) / (2.0 * delta)  # db/dk - dA/dk x
-    del Am
-    lam = bm._lu_solve_square(A.conj().transpose(0, 1).contiguous(), x.contiguous())
-    dJ = 2.0 * float(torch.vdot(lam, r).real)
-    torch.cuda.synchronize(bm.device)
-    out["adjoint_ms"] = (time.perf_counter() - t1) * 1e3
-    out.update(J=J, dJdk=dJ, x=x)
-    if check:
-        Js = []
-        for k in (k0 + delta, k0 - delta):
-            Ak, bk = system(k)
-            xk = bm._lu_solve_square(Ak, bk)
-            Js.append(float(torch.vdot(xk, xk).real))
-            del Ak
-        out["dJdk_central_difference"] = (Js[0] - Js[1]) / (2.0 * delta)
-    bm._k = k0
-    if data is not None:
-        data.k = k0
-    return out

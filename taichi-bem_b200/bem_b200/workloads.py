@@ -63,6 +63,18 @@ class PlaneWave:
         d = upload(self.d, x.device, x.dtype)
         return 1j * (self.k * s) * (n @ d) * torch.exp(1j * (self.k * s) * (x @ d))
 
+    def dfD_dk(self, x, s=1.0):
+        """d fD / dk = i s (d.x) exp(i k s d.x)."""
+        d = upload(self.d, x.device, x.dtype)
+        xd = x @ d
+        return 1j * s * xd * torch.exp(1j * (self.k * s) * xd)
+
+    def dfN_dk(self, x, n, s=1.0):
+        """d fN / dk = i s (n.d) exp(i k s d.x) (1 + i k s d.x)."""
+        d = upload(self.d, x.device, x.dtype)
+        xd = x @ d
+        return 1j * s * (n @ d) * torch.exp(1j * (self.k * s) * xd) * (1.0 + 1j * (self.k * s) * xd)
+
 
 def _base(**kw):
     p = dict(dim=3, object="icosphere3", GaussQR=5, n_i=1, n_o=1, k=0.0, kernel="Laplace", boundary="Dirichlet",

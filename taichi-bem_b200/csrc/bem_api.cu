@@ -138,8 +138,14 @@ int check_space(bem_ctx* ctx, const bem_space* sp, const char* name) {
     return BEM_OK;
 }
 
-int check_op(bem_ctx* ctx, const bem_op_desc* op) {
+// allow_dk: the caller takes the k-derivative operators (deriv_k, 3D Helmholtz)
+int check_op(bem_ctx* ctx, const bem_op_desc* op, bool allow_dk = false) {
     if (!op) return bem_fail(ctx, BEM_ERR_INVALID, "op is NULL");
+    if (op->deriv_k) {
+        if (!allow_dk) return bem_fail(ctx, BEM_ERR_INVALID, "deriv_k is taken by bem_assemble and bem_apply only");
+        if (op->kernel != BEM_KERNEL_HELMHOLTZ || ctx->dim != 3)
+            return bem_fail(ctx, BEM_ERR_INVALID, "deriv_k needs the 3D Helmholtz kernel");
+    }
     if (op->op < BEM_OP_V || op->op > BEM_OP_W) return bem_fail(ctx, BEM_ERR_INVALID, "unknown operator");
     if (op->kernel != BEM_KERNEL_LAPLACE && op->kernel != BEM_KERNEL_HELMHOLTZ)
         return bem_fail(ctx, BEM_ERR_INVALID, "unknown kernel");
@@ -414,7 +420,7 @@ int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, con
                  void* out, int64_t ld, double scale, void* out_t, double scale_t, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
     if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
-    if (int rc = check_op(ctx, op)) return rc;
+    if (int rc = check_op(ctx, op, true)) return rc;
     if (int rc = check_space(ctx, test, "test")) return rc;
     if (int rc = check_space(ctx, trial, "trial")) return rc;
     int want = op->kernel == BEM_KERNEL_HELMHOLTZ ? BEM_C128 : BEM_F64;
@@ -432,7 +438,7 @@ int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const 
               const void* x, void* y, double scale, int conj_x, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
     if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
-    if (int rc = check_op(ctx, op)) return rc;
+    if (int rc = check_op(ctx, op, true)) return rc;
     if (int rc = check_space(ctx, test, "test")) return rc;
     if (int rc = check_space(ctx, trial, "trial")) return rc;
     int want = op->kernel == BEM_KERNEL_HELMHOLTZ ? BEM_C128 : BEM_F64;
@@ -501,7 +507,7 @@ int bem_adjoint_vertices(bem_ctx* ctx, const bem_op_desc* op, const bem_space* t
     if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
     if (!op || !lam || !u || !grad) return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: null argument");
     if (ctx->dim != 3) return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: triangle meshes only");
-    if (op->kernel != BEM_KERNEL_LAPLACE || (op->op != BEM_OP_V && op->op != BEM_OP_K))
+    if (op->kernel != BEM_KERNEL_LAPLACE || (op->op != BEM_OP_V && op->op != BEM_OP_K) || op->deriv_k)
         return bem_fail(ctx, BEM_ERR_INVALID, "adjoint: Laplace V or K only");
     if (int rc = check_space(ctx, test, "test")) return rc;
     if (int rc = check_space(ctx, trial, "trial")) return rc;

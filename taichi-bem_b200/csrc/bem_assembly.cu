@@ -110,8 +110,10 @@ __global__ void scatter_local_kernel(int n, const int32_t* __restrict__ panels, 
 //   V, W: e^{ikr}/r                           (G, BEM_manager.py:474-483)
 //   K:    (d.n_y)/r^3 (1 - ikr) e^{ikr}       (grad_G_y, BEM_manager.py:510-523)
 //   KP:   (-d.n_x)/r^3 (1 - ikr) e^{ikr}      (grad_G_y with x,y swapped and n_x)
+// and with dk (Helmholtz) their derivatives in k:
+//   V, W: i e^{ikr}  (= i r G)                K, KP: k (d.n)/r e^{ikr}
 template <int OP, bool HELM, typename T>
-__device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T& re, T& im) {
+__device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T& re, T& im, bool dk = false) {
     const T r2 = dx * dx + dy * dy + dz * dz;
     T r, rinv;
     dev_r_rinv(r2, r, rinv);
@@ -122,8 +124,8 @@ __device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T&
         } else {
             T s, c;
             dev_sincos(k * r, &s, &c);
-            re = rinv * c;
-            im = rinv * s;
+            re = dk ? -s : rinv * c;
+            im = dk ? c : rinv * s;
         }
     } else {
         T dn = dx * nx + dy * ny + dz * nz;
@@ -136,8 +138,14 @@ __device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T&
             T kr = k * r;
             T s, c;
             dev_sincos(kr, &s, &c);
-            re = t * (c + kr * s);
-            im = t * (s - kr * c);
+            if (dk) {
+                const T f = dn * k * rinv;
+                re = f * c;
+                im = f * s;
+            } else {
+                re = t * (c + kr * s);
+                im = t * (s - kr * c);
+            }
         }
     }
 }
@@ -146,7 +154,7 @@ __device__ __forceinline__ void kval(T dx, T dy, T dz, T nx, T ny, T nz, T k, T&
 // K'), Rf = R; the result lacks the pair's factor e^{ikR} (Frame::rotate).
 template <int OP, bool HELM>
 __device__ __forceinline__ void kval_split(float r2, float s, float dn, float k, float Rf, bool small, float& re,
-                                           float& im) {
+                                           float& im, bool dk = false) {
     float r, rinv;
     dev_r_rinv(r2, r, rinv);
     if (OP == BEM_OP_V || OP == BEM_OP_W) {
@@ -156,8 +164,8 @@ __device__ __forceinline__ void kval_split(float r2, float s, float dn, float k,
         } else {
             float sn, cs;
             dev_sincos_phase(k * __fdividef(s, r + Rf), small, &sn, &cs);
-            re = rinv * cs;
-            im = rinv * sn;
+            re = dk ? -sn : rinv * cs;
+            im = dk ? cs : rinv * sn;
         }
     } else {
         const float t = dn * rinv * rinv * rinv;
@@ -168,8 +176,14 @@ __device__ __forceinline__ void kval_split(float r2, float s, float dn, float k,
             const float kr = k * r;
             float sn, cs;
             dev_sincos_phase(k * __fdividef(s, r + Rf), small, &sn, &cs);
-            re = t * fmaf(kr, sn, cs);
-            im = t * fmaf(-kr, cs, sn);
+            if (dk) {
+                const float f = dn * k * rinv;
+                re = f * cs;
+                im = f * sn;
+            } else {
+                re = t * fmaf(kr, sn, cs);
+                im = t * fmaf(-kr, cs, sn);
+            }
         }
     }
 }
@@ -202,6 +216,7 @@ struct FarArgs {
     double* y;
     int conj_x;
     int skip_far;  // 1: launch only the near-pair kernel (bem_launch_assemble_parts)
+    int dk = 0;    // 1: the kernel's k-derivative (kval)
 };
 
 
@@ -315,9 +330,9 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kernel(FarArgs a) {
                         const T sq = e_x * (xa.x + wx) + e_y * (xa.y + wy) + e_z * (xa.z + wz);
                         // K: d.n_y = D.n_y + x_a.n_y (y_b lies in the plane of panel j)
                         const T dn = (OP == BEM_OP_K) ? fma(xa.x, mx, fma(xa.y, my, fma(xa.z, mz, Dn))) : dnb;
-                        kval_split<OP, HELM>(fr.R2 + sq, sq, dn, kk, fr.Rf, a.small_phase != 0, re, im);
+                        kval_split<OP, HELM>(fr.R2 + sq, sq, dn, kk, fr.Rf, a.small_phase != 0, re, im, a.dk != 0);
                     } else {
-                        kval<OP, HELM, T>(xa.x + ex, xa.y + ey, xa.z + ez, nx, ny, nz, kk, re, im);
+                        kval<OP, HELM, T>(xa.x + ex, xa.y + ey, xa.z + ez, nx, ny, nz, kk, re, im, a.dk != 0);
                     }
                     if (W_OP) {
                         c_re += xa.w * re;
@@ -477,6 +492,7 @@ struct NearArgs {
     const double* x;
     double* y;
     int conj_x;
+    int dk = 0;  // 1: the kernel's k-derivative (kval)
 };
 
 struct NearPanel {
@@ -551,13 +567,14 @@ __global__ void __launch_bounds__(128) near_kernel(NearArgs a) {
         if (OP == BEM_OP_K) {
             // first: grad_G_y(x, y, n_y); second: grad_G_y(y, x, n_y)
             double sgn = second ? -1.0 : 1.0;
-            kval<BEM_OP_K, HELM, double>(sgn * dx, sgn * dy, sgn * dz, nKy[0], nKy[1], nKy[2], a.k, re, im);
+            kval<BEM_OP_K, HELM, double>(sgn * dx, sgn * dy, sgn * dz, nKy[0], nKy[1], nKy[2], a.k, re, im, a.dk != 0);
         } else if (OP == BEM_OP_KP) {
             // first: grad_G_y(y, x, n_x); second: grad_G_y(x, y, n_x)
             double sgn = second ? -1.0 : 1.0;
-            kval<BEM_OP_KP, HELM, double>(sgn * dx, sgn * dy, sgn * dz, nKx[0], nKx[1], nKx[2], a.k, re, im);
+            kval<BEM_OP_KP, HELM, double>(sgn * dx, sgn * dy, sgn * dz, nKx[0], nKx[1], nKx[2], a.k, re, im,
+                                          a.dk != 0);
         } else {
-            kval<BEM_OP_V, HELM, double>(dx, dy, dz, 0.0, 0.0, 0.0, a.k, re, im);
+            kval<BEM_OP_V, HELM, double>(dx, dy, dz, 0.0, 0.0, 0.0, a.k, re, im, a.dk != 0);
         }
         re *= wj;
         im *= wj;
@@ -1609,6 +1626,7 @@ int bem_launch_assemble_parts(bem_ctx* ctx, const bem_op_desc* op, const bem_spa
     fa.Q2 = ctx->Q2;
     fa.k = op->k;
     fa.k2 = op->k2;
+    fa.dk = op->deriv_k ? 1 : 0;
     fa.mode = mode;
     fa.out = (double*)out;
     fa.ld = ld;
@@ -1636,6 +1654,7 @@ int bem_launch_assemble_parts(bem_ctx* ctx, const bem_op_desc* op, const bem_spa
     na.Q = ctx->Q;
     na.k = op->k;
     na.k2 = op->k2;
+    na.dk = op->deriv_k ? 1 : 0;
     na.quirk = op->quirk;
     na.mode = mode;
     na.out = (double*)out;

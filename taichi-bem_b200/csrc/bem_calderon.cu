@@ -615,7 +615,7 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
                                      const bem_space* neu, const bem_space* dir, void* const* out,
                                      const double* coef, int64_t ld, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
-    if (!op || !k || !k2 || !neu || !dir || !out || !coef || nk < 1 || nk > CAL_MAXK || ld <= 0)
+    if (!op || !k || !k2 || !neu || !dir || !out || !coef || nk < 1 || nk > CAL_MAXK || ld <= 0 || op->deriv_k)
         return bem_fail(ctx, BEM_ERR_INVALID, "assemble_calderon: bad arguments");
     if (ctx->nt <= 0 || ctx->dim != 3) return bem_fail(ctx, BEM_ERR_NOMESH, "assemble_calderon: no 3D mesh set");
     if (neu->nb != 1 || dir->nb != 3 || neu->n_panels != dir->n_panels || neu->n_panels <= 0)

@@ -899,10 +899,13 @@ int bem_gram(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, i
     return rc;
 }
 
-int bem_lstsq_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld,
-                     const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
-                     const void* dinv, const void* b, void* x, double tol, int maxit, int restart, double accept,
-                     int* iters, double* relres, void* stream) {
+// FGMRES on D (A^H A + P^H P) D z = g, x = D z, with g = D [A; P]^H b for
+// the stacked right-hand side b (2n), or g = D b for a normal-equation
+// right-hand side b (n; normal_rhs).
+static int normal_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld,
+                         const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
+                         const void* dinv, const void* b, bool normal_rhs, void* x, double tol, int maxit,
+                         int restart, double accept, int* iters, double* relres, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
     if (!A || !P || !colscale || !LU || !piv || !dinv || !b || !x || n <= 0 || ld < n || ldlu < n)
         return bem_fail(ctx, BEM_ERR_INVALID, "lstsq_refine: bad arguments");
@@ -965,7 +968,17 @@ int bem_lstsq_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int6
         return gemvh(t1, t2, w);
     };
     auto precond = [&](double* v) -> int { return bem_lu_solve_tiled(ctx, lu_dtype, LU, n, ldlu, piv, dinv, v, s); };
-    int rc = gemvh(bb, bb + nd, g);
+    int rc = BEM_OK;
+    if (normal_rhs) {
+        if (C)
+            dscale_copy_kernel<true><<<vb, 256, 0, s>>>(g, bb, colscale, ni);
+        else
+            dscale_copy_kernel<false><<<vb, 256, 0, s>>>(g, bb, colscale, ni);
+        ctx->launches++;
+        rc = bem_check_cuda(ctx, cudaGetLastError(), "normal rhs");
+    } else {
+        rc = gemvh(bb, bb + nd, g);
+    }
     // x holds the initial guess in the original variables: z0 = x / d
     if (!rc) {
         if (C)
@@ -991,3 +1004,19 @@ int bem_lstsq_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int6
 }
 
 }  // extern "C"
+
+int bem_lstsq_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld,
+                     const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
+                     const void* dinv, const void* b, void* x, double tol, int maxit, int restart, double accept,
+                     int* iters, double* relres, void* stream) {
+    return normal_refine(ctx, dtype, A, P, n, ld, colscale, lu_dtype, LU, ldlu, piv, dinv, b, false, x, tol, maxit,
+                         restart, accept, iters, relres, stream);
+}
+
+int bem_normal_refine(bem_ctx* ctx, int dtype, const void* A, const void* P, int64_t n, int64_t ld,
+                      const double* colscale, int lu_dtype, const void* LU, int64_t ldlu, const int32_t* piv,
+                      const void* dinv, const void* g, void* x, double tol, int maxit, int restart, double accept,
+                      int* iters, double* relres, void* stream) {
+    return normal_refine(ctx, dtype, A, P, n, ld, colscale, lu_dtype, LU, ldlu, piv, dinv, g, true, x, tol, maxit,
+                         restart, accept, iters, relres, stream);
+}
