@@ -140,6 +140,13 @@ int bem_mesh_set_2d(bem_ctx* ctx, const double* verts, const int32_t* segs, int 
  * pairs get_panels_relation (mesh_manager.py:538-573) does not call
  * SEPARATE. */
 int64_t bem_near_pair_count(const bem_ctx* ctx);
+/* The near-pair list itself (no reference counterpart; the pairs
+ * get_panels_relation, mesh_manager.py:538-573, does not classify as
+ * separate): bem_near_pair_count(ctx) entries of four int32 (test panel,
+ * trial panel, relation 1 coincident / 2 common vertex / 3 common edge,
+ * packed parameter orders), ordered by test then trial panel, copied into
+ * out (host or device memory).  Synchronous. */
+int bem_near_pair_list(const bem_ctx* ctx, int32_t* out);
 /* Copies the per-panel areas [nt] and unit normals [nt*3] (device pointers):
  * MeshManager's panel_areas / panel_normals (mesh_manager.py:108-139). */
 int bem_mesh_geometry(const bem_ctx* ctx, double* areas, double* normals, void* stream);

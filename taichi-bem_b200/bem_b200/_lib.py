@@ -36,7 +36,7 @@ EXPORTS = [
     "bem_lu_factor_tiled", "bem_lu_solve_tiled", "bem_assemble_dirichlet", "bem_lu_solve_tiled_static",
     "bem_adjoint_vertices", "bem_mesh_set_2d", "bem_gmres_ir", "bem_compute_color", "bem_set_mesh_instances",
     "bem_lu_factor_status", "bem_binary_version", "bem_ctx_set_tuning", "bem_assemble_calderon", "bem_gram",
-    "bem_lstsq_refine", "bem_chol_factor", "bem_gemm", "bem_chol_inverse", "bem_normal_refine",
+    "bem_lstsq_refine", "bem_chol_factor", "bem_gemm", "bem_chol_inverse", "bem_normal_refine", "bem_near_pair_list",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 TUNE_CALDERON_GROUP = 0  # BEM_TUNE_CALDERON_GROUP
@@ -108,6 +108,7 @@ def load():
     L.bem_binary_version.argtypes = [ctypes.POINTER(ctypes.c_int)]
     L.bem_ctx_set_tuning.argtypes = [vp, i32, i32]
     L.bem_chol_factor.argtypes = [vp, i32, vp, i64, i64, i32, vp, vp, vp, vp]
+    L.bem_near_pair_list.argtypes = [vp, vp]
     L.bem_gemm.argtypes = [vp, i32, i32, i32, i64, i64, i64, dbl, vp, i64, vp, i64, vp, i64, vp]
     L.bem_chol_inverse.argtypes = [vp, i32, vp, i64, i64, vp, i64, vp, vp]
     L.bem_gram.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, i32, vp, i64, vp]

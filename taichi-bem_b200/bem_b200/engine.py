@@ -140,6 +140,14 @@ class Engine:
     def near_pairs(self) -> int:
         return int(self.lib.bem_near_pair_count(self.ctx))
 
+    def near_pair_list(self) -> np.ndarray:
+        """The device-built near-pair list as int32 [n, 4]: (test panel,
+        trial panel, relation, packed parameter orders) (bem_near_pair_list)."""
+        out = np.zeros((self.near_pairs, 4), np.int32)
+        if out.size:
+            self._check(self.lib.bem_near_pair_list(self.ctx, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
     def geometry(self):
         areas = torch.empty(self.nt, dtype=torch.float64, device=self.device)
         normals = torch.empty(self.nt, self.dim, dtype=torch.float64, device=self.device)

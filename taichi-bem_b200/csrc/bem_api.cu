@@ -73,39 +73,6 @@ void gauss01(int n, double* p, double* w) {
     }
 }
 
-// Corrected-mode parameter orders of a near pair (packed 2 bits per slot):
-// shared vertex at slot 0 of both panels, or shared edge at slots (0,1) of
-// both panels with matching endpoints.
-int near_perm(const int32_t* a, const int32_t* b, int rel) {
-    int px[3] = {0, 1, 2}, py[3] = {0, 1, 2};
-    if (rel == REL_VERTEX) {
-        bool done = false;
-        for (int s = 0; s < 3 && !done; ++s)
-            for (int t = 0; t < 3 && !done; ++t)
-                if (a[s] == b[t]) {
-                    px[0] = s; px[1] = (s + 1) % 3; px[2] = (s + 2) % 3;
-                    py[0] = t; py[1] = (t + 1) % 3; py[2] = (t + 2) % 3;
-                    done = true;
-                }
-    } else if (rel == REL_EDGE) {
-        for (int s = 0; s < 3; ++s) {
-            int v0 = a[s], v1 = a[(s + 1) % 3], t0 = -1, t1 = -1;
-            for (int t = 0; t < 3; ++t) {
-                if (b[t] == v0) t0 = t;
-                if (b[t] == v1) t1 = t;
-            }
-            if (t0 >= 0 && t1 >= 0) {
-                px[0] = s; px[1] = (s + 1) % 3; px[2] = (s + 2) % 3;
-                py[0] = t0; py[1] = t1; py[2] = 3 - t0 - t1;
-                break;
-            }
-        }
-    }
-    int bx = px[0] | (px[1] << 2) | (px[2] << 4);
-    int by = py[0] | (py[1] << 2) | (py[2] << 4);
-    return bx | (by << 6);
-}
-
 void free_mesh(bem_ctx* ctx) {
     void* ptrs[] = {ctx->verts, ctx->tris, ctx->area, ctx->normal, ctx->centroid, ctx->curl, ctx->pts64,
                     ctx->pts32, ctx->phi64, ctx->phi32, ctx->gp, ctx->gw, ctx->near, ctx->test_local,
@@ -222,6 +189,15 @@ int64_t bem_launch_count(const bem_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int64_t bem_near_pair_count(const bem_ctx* ctx) { return ctx ? ctx->n_near : 0; }
 
+int bem_near_pair_list(const bem_ctx* cctx, int32_t* out) {
+    bem_ctx* ctx = const_cast<bem_ctx*>(cctx);
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!out) return bem_fail(ctx, BEM_ERR_INVALID, "near_pair_list: out is NULL");
+    if (ctx->n_near == 0 || ctx->dim != 3) return BEM_OK;
+    return bem_check_cuda(ctx, cudaMemcpy(out, ctx->near, sizeof(int4) * (size_t)ctx->n_near, cudaMemcpyDefault),
+                          "near_pair_list copy");
+}
+
 int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv, int nt, int gauss_qr) {
     if (!ctx) return BEM_ERR_INVALID;
     if (!verts || !tris || nv <= 0 || nt <= 0) return bem_fail(ctx, BEM_ERR_INVALID, "empty mesh");
@@ -230,26 +206,6 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
         if (!std::isfinite(verts[i])) return bem_fail(ctx, BEM_ERR_MESH, "non-finite vertex coordinate");
     for (int64_t i = 0; i < 3LL * nt; ++i)
         if (tris[i] < 0 || tris[i] >= nv) return bem_fail(ctx, BEM_ERR_MESH, "panel vertex index out of range");
-
-    // near-pair list: every ordered pair sharing at least one vertex index
-    std::vector<std::vector<int>> vp(nv);
-    for (int p = 0; p < nt; ++p)
-        for (int c = 0; c < 3; ++c) vp[tris[3 * p + c]].push_back(p);
-    std::vector<int4> near;
-    near.reserve((size_t)nt * 14);
-    std::vector<int> cand;
-    for (int i = 0; i < nt; ++i) {
-        cand.clear();
-        for (int c = 0; c < 3; ++c)
-            for (int j : vp[tris[3 * i + c]]) cand.push_back(j);
-        std::sort(cand.begin(), cand.end());
-        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-        for (int j : cand) {
-            int rel = bem_relation(tris + 3 * i, tris + 3 * j, i == j);
-            if (rel == REL_SEPARATE) continue;
-            near.push_back(make_int4(i, j, rel, near_perm(tris + 3 * i, tris + 3 * j, rel)));
-        }
-    }
 
     free_mesh(ctx);
     const int Q = gauss_qr, Q2 = Q * Q;
@@ -282,8 +238,7 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
         (rc = dmalloc(ctx, &ctx->pts64, (size_t)nt * Q2)) || (rc = dmalloc(ctx, &ctx->pts32, (size_t)nt * Q2)) ||
         (rc = dmalloc(ctx, &ctx->phi64, (size_t)Q2 * 3)) || (rc = dmalloc(ctx, &ctx->phi32, (size_t)Q2 * 3)) ||
         (rc = dmalloc(ctx, &ctx->gp, Q)) || (rc = dmalloc(ctx, &ctx->gw, Q)) ||
-        (rc = dmalloc(ctx, &ctx->near, near.size())) || (rc = dmalloc(ctx, &ctx->test_local, nt)) ||
-        (rc = dmalloc(ctx, &ctx->trial_local, nt))) {
+        (rc = dmalloc(ctx, &ctx->test_local, nt)) || (rc = dmalloc(ctx, &ctx->trial_local, nt))) {
         free_mesh(ctx);
         return rc;
     }
@@ -307,14 +262,17 @@ int bem_mesh_set(bem_ctx* ctx, const double* verts, const int32_t* tris, int nv,
         }
     }
     ctx->rho_max = rho;
-    ctx->n_near = (int64_t)near.size();
     cudaMemcpy(ctx->verts, verts, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->tris, tris, sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->gp, gp.data(), sizeof(double) * Q, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->gw, gw.data(), sizeof(double) * Q, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->phi64, phi64.data(), sizeof(double) * Q2 * 3, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->phi32, phi32.data(), sizeof(float) * Q2 * 3, cudaMemcpyHostToDevice);
-    if (!near.empty()) cudaMemcpy(ctx->near, near.data(), sizeof(int4) * near.size(), cudaMemcpyHostToDevice);
+    // near-pair list: every ordered pair sharing at least one vertex index (on the device)
+    if ((rc = bem_build_near_list(ctx, nv, nt))) {
+        free_mesh(ctx);
+        return rc;
+    }
     cudaMemset(ctx->flags, 0, 16 * sizeof(int32_t));
     if ((rc = bem_launch_geometry(ctx, 0))) return rc;
     if ((rc = bem_check_cuda(ctx, cudaDeviceSynchronize(), "mesh geometry"))) return rc;

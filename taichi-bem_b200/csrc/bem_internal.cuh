@@ -79,6 +79,9 @@ int bem_fgmres(bem_ctx* ctx, bool C, int64_t n, const std::function<int(const do
 // panel L (m x kb, ld), FP64 sums (bem_lstsq.cu).
 int bem_herk_tc_update(bem_ctx* ctx, bool C, const double* L, int64_t ld, int m, int kb, double* out, int64_t ldo,
                        cudaStream_t s);
+// The near-pair list of the uploaded triangle mesh (ctx->tris) into
+// ctx->near / ctx->n_near, built on the device (bem_mesh.cu); synchronous.
+int bem_build_near_list(bem_ctx* ctx, int nv, int nt);
 // A device buffer of at least `bytes` owned by the context (grown, never
 // shrunk; freed with it), for scratch that lives within one call.
 int bem_big_ws(bem_ctx* ctx, size_t bytes, void** out);

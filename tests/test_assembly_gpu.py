@@ -157,6 +157,48 @@ def test_near_pair_count_icosphere(engine):
     assert 12 * len(f) < n <= 13 * len(f)
 
 
+def _near_list_reference(f):
+    """The ordered pairs sharing a vertex index, by relation, in (i, j)
+    order: a numpy restatement of get_panels_relation
+    (mesh_manager.py:538-573) over the vertex-sharing candidates."""
+    from oracle import oracle as O
+    f = np.asarray(f)
+    nt = len(f)
+    by_v = {}
+    for p in range(nt):
+        for c in f[p]:
+            by_v.setdefault(int(c), []).append(p)
+    rows = []
+    for i in range(nt):
+        for j in sorted({j for c in f[i] for j in by_v[int(c)]}):
+            rel = O.relation(f, i, j)
+            if rel != 0:
+                rows.append((i, j, rel))
+    return np.array(rows, np.int32).reshape(-1, 3)
+
+
+@pytest.mark.parametrize("mesh", ["cube", "ico2", "analytical_sphere", "perturbed3"])
+def test_near_pair_list_matches_reference(engine, mesh):
+    """The device-built near-pair list: every vertex-sharing ordered pair with
+    the oracle's relation, in (test, trial) order; parameter orders in range."""
+    from bem_b200.meshes import analytical_sphere, perturbed_sphere
+    if mesh in MESHES:
+        v, f = MESHES[mesh]
+    elif mesh == "analytical_sphere":
+        v, f = analytical_sphere()
+    else:
+        v, f = perturbed_sphere(3, lmax=6, amplitude=0.05, seed=0)
+    engine.set_mesh(v, f, 3)
+    got = engine.near_pair_list()
+    ref = _near_list_reference(f)
+    assert got.shape[0] == ref.shape[0]
+    assert np.array_equal(got[:, :3], ref)
+    # packed orders: two 6-bit permutations of (0, 1, 2)
+    for sh in (0, 6):
+        perm = [(got[:, 3] >> (sh + 2 * s)) & 3 for s in range(3)]
+        assert np.all(np.sort(np.stack(perm, 1), 1) == np.array([0, 1, 2]))
+
+
 def test_bad_mesh_rejected(engine):
     from bem_b200._lib import BemError
     v = np.array([[0, 0, 0], [1, 0, 0], [2, 0, 0]], dtype=np.float64)  # collinear -> zero area
