@@ -498,7 +498,7 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "lstsq"):
     against the FP64 path, and dJ/dk of J = ||x||^2 by the adjoint with the
     analytic operator derivative (managers/kderiv.py), in mixed precision and
     in FP64, against the fourth-order central difference of the FP64 J
-    (delta = 5e-3)."""
+    (delta = 1e-3)."""
     import torch
     from bem_b200.managers import CoreManager
     from bem_b200.managers.kderiv import solution_norm_k_gradient
@@ -526,7 +526,7 @@ def transmission_bench(subdiv: int, plain: bool, solver: str = "lstsq"):
     core.initialization(pw.fD, pw.fN)
     core._BEM_manager.run()
     x64 = core._BEM_manager.raw_solved.clone()
-    g64 = solution_norm_k_gradient(core._BEM_manager, pw, check=True, delta=5e-3)
+    g64 = solution_norm_k_gradient(core._BEM_manager, pw, check=True, delta=1e-3)
     core.kill()
     cd = g64["dJdk_central_difference"]
     res["dJdk"] = {"J": g64["J"], "central_difference_fp64": cd, "central_difference": g64["central_difference"],

@@ -178,7 +178,11 @@ def solution_norm_k_gradient(bm, data, check: bool = True, delta: float = 1e-3):
     if check:
         Js = {s: _J(bm, data, k0 + s * delta) for s in (-2, -1, 1, 2)}
         out["dJdk_central_difference"] = (Js[-2] - 8.0 * Js[-1] + 8.0 * Js[1] - Js[2]) / (12.0 * delta)
-        out["central_difference"] = {"delta": delta, "order": 4}
+        # the second-order differences at delta and 2 delta: their spread shows
+        # the truncation error of the fourth-order one
+        out["central_difference"] = {"delta": delta, "order": 4,
+                                     "order2_delta": (Js[1] - Js[-1]) / (2.0 * delta),
+                                     "order2_2delta": (Js[2] - Js[-2]) / (4.0 * delta)}
     bm._k = k0
     data.k = k0
     return out

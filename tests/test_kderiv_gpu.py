@@ -75,7 +75,7 @@ def test_dJdk_matches_central_difference(solver):
         params.update(solve_precision="mixed", refine_tol=1e-13)
     core = CoreManager(params)
     core.initialization(pw.fD, pw.fN)
-    g = solution_norm_k_gradient(core._BEM_manager, pw, check=True, delta=5e-3)
+    g = solution_norm_k_gradient(core._BEM_manager, pw, check=True, delta=1e-3)
     core.kill()
     cd = g["dJdk_central_difference"]
     assert abs(g["dJdk"] - cd) <= 1e-6 * abs(cd), (g["dJdk"], cd)
