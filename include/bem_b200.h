@@ -108,10 +108,14 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  *                            a single-wavenumber mixed Helmholtz sweep)
  *   BEM_TUNE_GRAM_KSEG       64-wide K stages per TMEM accumulation segment of
  *                            the tensor-core normal matrix (>= 1)
- *   BEM_TUNE_CHOL_NB         panel width of bem_chol_factor (a multiple of 64) */
+ *   BEM_TUNE_CHOL_NB         panel width of bem_chol_factor (a multiple of 64)
+ *   BEM_TUNE_GRAM_BAND       tile columns per band of the normal-matrix tile
+ *                            order (tiles running together share the L2's
+ *                            operand panels); 1 gives row order */
 #define BEM_TUNE_CALDERON_GROUP 0
 #define BEM_TUNE_GRAM_KSEG 1
 #define BEM_TUNE_CHOL_NB 2
+#define BEM_TUNE_GRAM_BAND 3
 #define BEM_TUNE_KEYS 8
 int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value);
 

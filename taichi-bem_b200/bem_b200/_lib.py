@@ -42,6 +42,7 @@ STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 TUNE_CALDERON_GROUP = 0  # BEM_TUNE_CALDERON_GROUP
 TUNE_GRAM_KSEG = 1  # BEM_TUNE_GRAM_KSEG
 TUNE_CHOL_NB = 2  # BEM_TUNE_CHOL_NB
+TUNE_GRAM_BAND = 3  # BEM_TUNE_GRAM_BAND
 
 
 class BemError(RuntimeError):

@@ -9,7 +9,8 @@ cached choice without timing.  The cache file is
 $BEM_B200_TUNING_CACHE, else ~/.cache/bem_b200/tuning.json.
 
 Only keys that change the launch shape and not the result's accuracy are
-tuned this way (the Calderon sweep's form, the Cholesky panel width); the
+tuned this way (the Calderon sweep's form, the normal matrix's tile order,
+the Cholesky panel width); the
 normal matrix's accumulation segment (BEM_TUNE_GRAM_KSEG) trades accuracy
 for speed and keeps its built-in default.
 """
@@ -22,7 +23,8 @@ import statistics
 from . import _lib as L
 
 CACHE_ENV = "BEM_B200_TUNING_CACHE"
-KEY_NAMES = {L.TUNE_CALDERON_GROUP: "calderon_group", L.TUNE_GRAM_KSEG: "gram_kseg", L.TUNE_CHOL_NB: "chol_nb"}
+KEY_NAMES = {L.TUNE_CALDERON_GROUP: "calderon_group", L.TUNE_GRAM_KSEG: "gram_kseg", L.TUNE_CHOL_NB: "chol_nb",
+             L.TUNE_GRAM_BAND: "gram_band"}
 
 
 def cache_path() -> str:

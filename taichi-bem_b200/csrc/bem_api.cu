@@ -145,6 +145,8 @@ int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value) {
     if (key == BEM_TUNE_CALDERON_GROUP && (value < 0 || value > 3))
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon form must be 1, 2 or 3");
     if (key == BEM_TUNE_GRAM_KSEG && value < 0) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: negative segment");
+    if (key == BEM_TUNE_GRAM_BAND && (value < 0 || value > 4096))
+        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: band width must be in 0..4096");
     if (key == BEM_TUNE_CHOL_NB && (value < 0 || value % 64 != 0 || value > 4096))
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: panel width must be a multiple of 64 up to 4096");
     ctx->tune[key] = value;

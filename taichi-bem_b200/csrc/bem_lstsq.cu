@@ -138,12 +138,46 @@ __global__ void __launch_bounds__(256) panel_split_kernel(const double* L, int64
 }
 
 // lower-triangle tile t (row-major order, diagonal included) -> (bi, bj), bi >= bj
-__device__ __forceinline__ void tri_tile(int t, int& bi, int& bj) {
+__device__ __forceinline__ int tri_row(int t) {
     int i = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
     while (i * (i + 1) / 2 > t) --i;
     while ((i + 1) * (i + 2) / 2 <= t) ++i;
-    bi = i;
-    bj = t - i * (i + 1) / 2;
+    return i;
+}
+
+// Tile t of the lower triangle (bi >= bj) of a T x T tile grid, in bands of G
+// tile columns: band b (columns [bG, bG + w), w = min(G, T - bG)) runs down
+// its rows from bi = bG, each row's tiles in column order; the first w rows
+// are the band's triangle.  Tiles that run at the same time (consecutive t)
+// then share about G row panels and T_conc / G column panels, whose K chunks
+// the L2 serves to all of them, instead of one column panel per CTA streamed
+// from DRAM.  G <= 0: plain row order.
+__device__ __forceinline__ void tri_tile(int t, int T, int G, int& bi, int& bj) {
+    if (G <= 0 || G >= T) {
+        bi = tri_row(t);
+        bj = t - bi * (bi + 1) / 2;
+        return;
+    }
+    int b0 = 0;
+    for (;;) {
+        const int w = min(G, T - b0);
+        const int tri = w * (w + 1) / 2;
+        const int size = tri + (T - b0 - w) * w;
+        if (t < size) {
+            if (t < tri) {
+                const int r = tri_row(t);
+                bi = b0 + r;
+                bj = b0 + (t - r * (r + 1) / 2);
+            } else {
+                const int u = t - tri;
+                bi = b0 + w + u / w;
+                bj = b0 + u % w;
+            }
+            return;
+        }
+        t -= size;
+        b0 += w;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -175,6 +209,8 @@ constexpr int GT_STAGES = 3;
 constexpr int GT_TILE = GT_BM * GT_BK * 2;  // bytes of one 128 x 64 FP16 tile
 constexpr int GT_STAGE = 4 * GT_TILE;
 constexpr int GT_KSEG_DEFAULT = 2;
+// tile columns per band of the tile order (tri_tile): 12 x 12 tiles ~ one wave of 148 CTAs
+constexpr int GRAM_BAND_DEFAULT = 12;
 constexpr int GT_EPI_WARPS = 8;
 constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
 constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
@@ -250,9 +286,9 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
 template <bool C, typename OT>
 __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
                                                                  const __grid_constant__ CUtensorMap tm_lo,
-                                                                 int nchunks, int kseg, int ntiles, OT* out,
-                                                                 int64_t ldo, int n, double alpha, int accumulate,
-                                                                 int32_t* err) {
+                                                                 int nchunks, int kseg, int ntiles, int tgrid,
+                                                                 int band, OT* out, int64_t ldo, int n, double alpha,
+                                                                 int accumulate, int32_t* err) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
@@ -295,7 +331,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
             uint32_t cg = 0;  // chunks issued by this CTA (the stage ring runs across tiles)
             for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
                 int bi, bj;
-                tri_tile(t, bi, bj);
+                tri_tile(t, tgrid, band, bi, bj);
                 for (int c = 0; c < nchunks; ++c, ++cg) {
                     const int s = (int)(cg % GT_STAGES);
                     if (cg >= GT_STAGES &&
@@ -369,7 +405,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         bool ok = true;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         int bi, bj;
-        tri_tile(t, bi, bj);
+        tri_tile(t, tgrid, band, bi, bj);
         double acc[EC];
 #pragma unroll
         for (int i = 0; i < EC; ++i) acc[i] = 0.0;
@@ -489,13 +525,13 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 
 template <bool C, typename OT>
 __global__ void __launch_bounds__(256) gram_f64_kernel(const double* A, const double* P, int64_t ld, int n,
-                                                       const double* d, OT* out, int64_t ldo) {
+                                                       const double* d, OT* out, int64_t ldo, int tgrid, int band) {
     extern __shared__ __align__(16) double sm[];
     double* As = sm;                       // [2][GD_BK][GD_LD]
     double* Bs = sm + 2 * GD_BK * GD_LD;   // [2][GD_BK][GD_LD]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     int bi, bj;
-    tri_tile(blockIdx.x, bi, bj);
+    tri_tile(blockIdx.x, tgrid, band, bi, bj);
     const int W = C ? 2 : 1;
     const int ncol = W * n;       // real columns of R
     const int K = 2 * n;          // rows of R
@@ -785,10 +821,11 @@ int launch_gram_tc(bem_ctx* ctx, __half* Thi, __half* Tlo, int64_t Rp, int64_t K
         return rc;
     cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
     const int kseg = ctx->tune[BEM_TUNE_GRAM_KSEG] > 0 ? ctx->tune[BEM_TUNE_GRAM_KSEG] : GT_KSEG_DEFAULT;
+    const int band = ctx->tune[BEM_TUNE_GRAM_BAND] > 0 ? ctx->tune[BEM_TUNE_GRAM_BAND] : GRAM_BAND_DEFAULT;
     // persistent: one CTA per SM (its shared memory and 512 TMEM columns allow no second), tiles in turn
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctx->num_sms);
-    gram_tc_kernel<C, OT><<<grid, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, (int)tiles, out,
-                                                            ldo, n, alpha, accumulate, ctx->flags + 5);
+    gram_tc_kernel<C, OT><<<grid, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, (int)tiles, tr,
+                                                            band, out, ldo, n, alpha, accumulate, ctx->flags + 5);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_tc_kernel");
 }
@@ -804,7 +841,8 @@ int gram_fp64(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n,
                                                           cudaFuncAttributeMaxDynamicSharedMemorySize, GD_SMEM),
                                 "gram_f64_kernel smem"))
         return rc;
-    gram_f64_kernel<C, OT><<<(unsigned)tiles, 256, GD_SMEM, s>>>(A, P, ld, n, d, out, ldo);
+    const int band = ctx->tune[BEM_TUNE_GRAM_BAND] > 0 ? ctx->tune[BEM_TUNE_GRAM_BAND] : GRAM_BAND_DEFAULT;
+    gram_f64_kernel<C, OT><<<(unsigned)tiles, 256, GD_SMEM, s>>>(A, P, ld, n, d, out, ldo, tr, band);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_f64_kernel");
 }

@@ -76,9 +76,9 @@ def test_laplace_s3_full_V_and_Kg(engine):
 
 
 def test_laplace_s3_driver_against_oracle_driver():
-    """The whole plain FP64 driver (CoreManager, solver "square") on the
-    1280-panel problem against the oracle's driver: A, right-hand side and the
-    Neumann trace; the trace also against the analytic du/dn."""
+    """The whole plain FP64 driver (CoreManager) on the 1280-panel problem
+    against the oracle's driver: A, right-hand side and the Neumann trace;
+    the trace also against the analytic du/dn, in both quadrature modes."""
     from bem_b200 import icosphere
     from bem_b200.managers import CoreManager
     from bem_b200.workloads import laplace_dirichlet_s3
@@ -94,9 +94,20 @@ def test_laplace_s3_driver_against_oracle_driver():
     got = b.raw_solved.cpu().numpy()
     assert rel_err(got, r["raw_solved"]) < 1e-10
     ana = b.raw_analytical_solved.cpu().numpy()
-    # discretisation error of the P0 Neumann trace on 1280 panels
-    assert np.linalg.norm(got - ana) / np.linalg.norm(ana) < 0.05
     core.kill()
+    # the Neumann trace against the analytic du/dn: with the reference's
+    # near-pair quadrature (the default) the error is the reference's own,
+    # about 0.4 and not shrinking with the mesh; the corrected quadrature
+    # (quirk = 0) converges (5.2e-3 on these 1280 panels)
+    assert 0.2 < np.linalg.norm(got - ana) / np.linalg.norm(ana) < 0.5
+    params["quirk"] = 0
+    core = CoreManager(params)
+    core.initialization(fD, fN)
+    core._BEM_manager.run()
+    got0 = core._BEM_manager.raw_solved.cpu().numpy()
+    ana0 = core._BEM_manager.raw_analytical_solved.cpu().numpy()
+    core.kill()
+    assert np.linalg.norm(got0 - ana0) / np.linalg.norm(ana0) < 1e-2
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
