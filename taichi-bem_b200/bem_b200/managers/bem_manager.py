@@ -882,7 +882,7 @@ class BEMManager:
         problems it takes; candidates 2: both wavenumbers in one scalar
         launch, 3: packed FP32x2 per wavenumber, 1: scalar per wavenumber),
         timed on assemble_system, and for the least-squares solver the band
-        width of the normal matrix's tile order (12, 8, 16, 1), timed on the
+        width of the normal matrix's tile order (1, 12, 8, 16), timed on the
         normal matrix, and the Cholesky panel width (512, 1024, 2048), timed
         on its factorisation.  Cached choices are applied without
         timing.  Returns {key name: value}."""
@@ -896,16 +896,16 @@ class BEMManager:
                                                self.assemble_system)
         nbs = [512, 1024, 2048]
         if (self._is_transmission and self.solver == "lstsq" and tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs)
-                and tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [12, 8, 16, 1])):
+                and tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16])):
             out["chol_nb"] = tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs)
-            out["gram_band"] = tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [12, 8, 16, 1])
+            out["gram_band"] = tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16])
         elif self._is_transmission and self.solver == "lstsq":
             mixed = self.solve_precision == "mixed"
             self.assemble_system()
             A, P = self.transmission_blocks()
             Nm = torch.empty(n, n, dtype=A.dtype, device=A.device)
             d = torch.empty(n, dtype=torch.float64, device=A.device)
-            out["gram_band"] = tuner.tune(wl + "/gram", L.TUNE_GRAM_BAND, [12, 8, 16, 1],
+            out["gram_band"] = tuner.tune(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16],
                                           lambda: self.engine.gram(A, P, Nm, d, tensor_cores=mixed))
             W = torch.empty_like(Nm)
 

@@ -209,8 +209,12 @@ constexpr int GT_STAGES = 3;
 constexpr int GT_TILE = GT_BM * GT_BK * 2;  // bytes of one 128 x 64 FP16 tile
 constexpr int GT_STAGE = 4 * GT_TILE;
 constexpr int GT_KSEG_DEFAULT = 2;
-// tile columns per band of the tile order (tri_tile): 12 x 12 tiles ~ one wave of 148 CTAs
-constexpr int GRAM_BAND_DEFAULT = 12;
+// tile columns per band of the tile order (tri_tile).  Bands of 12 (12 x 12
+// tiles ~ one wave of 148 CTAs) cut the operand reads from DRAM 4x at 7682
+// unknowns, but single-column bands measured faster under CUDA events at the
+// default segment on 7682 and 30722 unknowns (14.4 vs 16.6 ms, 1147 vs
+// 1183 ms); the autotuner chooses per problem.
+constexpr int GRAM_BAND_DEFAULT = 1;
 constexpr int GT_EPI_WARPS = 8;
 constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
 constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
