@@ -10,7 +10,7 @@ from block Krylov spaces of the Gram matrix G = S^H S and of its inverse
 (`extreme_singular_values`); the Ritz values converge to the SVD's smallest
 and largest singular values.  Every O(n^3) and O(n^2) step runs on this
 library's FP64 kernels: the scaled operator by bem_gemm (DMMA), G by
-bem_gram (DMMA), its LU by bem_lu_factor, the bases by classical
+bem_gram (DMMA), its inverse by bem_chol_inverse, the bases by classical
 Gram-Schmidt with one re-orthogonalisation (CGS2) on bem_gemm products.  The
 host sees only the p x p triangle of the Ritz step (p <= a few hundred), whose
 singular values numpy takes.
@@ -30,41 +30,31 @@ class Basis:
     """Orthonormal columns Q (n x j, FP64 real or complex, at most `cap`)
     grown column by column by CGS2 on bem_gemm products:
         h = Q^H v,  v -= Q h   (twice),   r_jj = ||v||,  q_j = v / r_jj,
-    so that appended columns W satisfy W = Q R with R upper triangular (kept
-    on the host when `keep_r`).  A column whose norm falls below 1e-13 of its
-    original norm (numerically inside span(Q)) is replaced by a seeded random
-    vector, with a zero column in R."""
+    so that appended columns W satisfy W = Q R with R upper triangular, kept
+    on the device as its transpose Rt (Rt[c, i] = R[i, c]).  Norms and R stay
+    on the device, so appending synchronises nothing.  A column numerically
+    inside span(Q) leaves a tiny r_jj and, after the second projection, a
+    normalised rounding direction orthogonal to Q, which the basis keeps; an
+    exactly dependent column leaves r_jj = 0 and a zero column."""
 
-    def __init__(self, engine, n, cap, dtype, device, seed=0, keep_r=False):
+    def __init__(self, engine, n, cap, dtype, device):
         self.engine = engine
         self.Q = torch.zeros(n, cap, dtype=dtype, device=device)
+        self.Rt = torch.zeros(cap, cap, dtype=dtype, device=device)
         self.j = 0
         self.cap = cap
-        self.keep_r = keep_r
-        self.R = np.zeros((cap, cap), np.complex128 if dtype.is_complex else np.float64)
-        self.gen = torch.Generator(device=device).manual_seed(seed)
-        self._h = torch.zeros(cap, 1, dtype=dtype, device=device)
+        self._h = torch.zeros(cap, dtype=dtype, device=device)
         self._nrm = torch.zeros(1, 1, dtype=dtype, device=device)
 
     @property
     def active(self) -> torch.Tensor:
         return self.Q[:, :self.j]
 
-    def _norm(self, v) -> float:
+    def _norm(self, v) -> torch.Tensor:
+        """||v|| as a real device scalar."""
         self._nrm.zero_()
         self.engine.gemm(v, v, self._nrm, conj_a=True)
-        return math.sqrt(max(float(self._nrm.real.item() if self._nrm.is_complex() else self._nrm.item()), 0.0))
-
-    def _project(self, v, r):
-        if self.j == 0:
-            return
-        for _ in range(2):
-            h = self._h[:self.j]
-            h.zero_()
-            self.engine.gemm(self.active, v, h, conj_a=True)
-            self.engine.gemm(self.active, h, v, alpha=-1.0)
-            if r is not None:
-                r[:self.j] += h[:, 0].cpu().numpy()
+        return (self._nrm.real if self._nrm.is_complex() else self._nrm).reshape(()).clamp_min(0.0).sqrt()
 
     def append(self, W: torch.Tensor) -> int:
         """Append the columns of W (n x p); returns the number appended (the
@@ -73,30 +63,26 @@ class Basis:
         for c in range(W.shape[1]):
             if self.j >= self.cap:
                 break
+            col, j = self.j, self.j
             v = W[:, c:c + 1].contiguous()
-            nrm0 = self._norm(v)
-            r = np.zeros(self.cap, self.R.dtype) if self.keep_r else None
-            self._project(v, r)
-            nrm = self._norm(v)
-            r_jj = nrm
-            if not nrm > 1e-13 * nrm0:
-                # inside the span: W's column is Q r (r_jj = 0); the basis
-                # continues with a random direction
-                r_jj = 0.0
-                v = torch.randn(v.shape, dtype=torch.float64, device=v.device, generator=self.gen)
-                if self.Q.is_complex():
-                    v = torch.complex(v, torch.randn(v.shape, dtype=torch.float64, device=v.device,
-                                                     generator=self.gen))
-                v = v.contiguous()
-                self._project(v, None)
-                nrm = self._norm(v)
-            self.Q[:, self.j:self.j + 1] = v / nrm
-            if self.keep_r:
-                r[self.j] = r_jj
-                self.R[:, self.j] = r
+            if j > 0:
+                r = self.Rt[col, :j].view(j, 1)
+                h = self._h[:j].view(j, 1)
+                for _ in range(2):
+                    h.zero_()
+                    self.engine.gemm(self.active, v, h, conj_a=True)
+                    self.engine.gemm(self.active, h, v, alpha=-1.0)
+                    r.add_(h)
+            rjj = self._norm(v)
+            self.Rt[col, col] = rjj.to(self.Rt.dtype)
+            self.Q[:, col:col + 1] = v / rjj.clamp_min(1e-300).to(v.dtype)
             self.j += 1
             added += 1
         return added
+
+    def r_host(self):
+        """R's transpose (j x j) on the host: its singular values are R's."""
+        return self.Rt[:self.j, :self.j].cpu().numpy()
 
 
 def _ritz(engine, S_blocks, Q: torch.Tensor, rbasis: Basis, which: int) -> float:
@@ -112,7 +98,7 @@ def _ritz(engine, S_blocks, Q: torch.Tensor, rbasis: Basis, which: int) -> float
         r0 += B.shape[0]
     assert r0 == SQ.shape[0] and n == S_blocks[0].shape[1]
     rbasis.append(SQ)
-    sv = np.linalg.svd(rbasis.R[:rbasis.j, :rbasis.j], compute_uv=False)
+    sv = np.linalg.svd(rbasis.r_host(), compute_uv=False)
     return float(sv[-1] if which == 0 else sv[0]) ** 2
 
 
@@ -124,9 +110,8 @@ def _krylov_ritz(engine, S_blocks, apply, X0, maxblocks: int, which: int, tol: f
     (relative) or at `maxblocks` blocks.  Returns (Ritz value, blocks)."""
     n, p = X0.shape
     cap = p * maxblocks
-    basis = Basis(engine, n, cap, X0.dtype, X0.device, seed=seed)
-    rbasis = Basis(engine, sum(b.shape[0] for b in S_blocks), cap, X0.dtype, X0.device, seed=seed + 1,
-                   keep_r=True)
+    basis = Basis(engine, n, cap, X0.dtype, X0.device)
+    rbasis = Basis(engine, sum(b.shape[0] for b in S_blocks), cap, X0.dtype, X0.device)
     basis.append(X0)
     done_cols, nblocks = 0, 1
     prev, check, lam = None, 2, 0.0
@@ -150,9 +135,10 @@ def extreme_singular_values(engine, S_blocks, block: int = 8, tol: float = 1e-10
 
     sigma_min^2 is the smallest eigenvalue of G = S^H S.  G is formed by the
     FP64 normal-matrix kernel (bem_gram, column scaling D: G^ = D G D) or, for
-    one block, bem_gemm; its LU (bem_lu_factor, FP64) gives G^{-1} = D G^^{-1}
-    D.  A block Krylov space of G^{-1} (block size `block`, one
-    multi-right-hand-side solve per step) is grown until the smallest Ritz
+    one block, bem_gemm; the inverse of G^ (slightly shifted, see below) by
+    bem_chol_inverse gives the inverse iteration's operator, applied by two
+    bem_gemm products per block.  A block Krylov space of G^{-1} (block size
+    `block`) is grown until the smallest Ritz
     value changes by less than `tol` (relative) between two sizes, at most
     `maxit` blocks; sigma_max^2 likewise from the Krylov space of G
     (`tol_max`)."""
@@ -171,8 +157,6 @@ def extreme_singular_values(engine, S_blocks, block: int = 8, tol: float = 1e-10
     if dt.is_complex:
         X = torch.complex(X, torch.randn(n, p, dtype=torch.float64, device=dev, generator=gen))
     dcol = d.to(dt).view(n, 1)
-    LU = G.clone()
-    piv, finfo = engine.lu_factor(LU)
     nmax = max(1, min(maxit, n // p))
 
     def apply_g(V):
@@ -182,13 +166,34 @@ def extreme_singular_values(engine, S_blocks, block: int = 8, tol: float = 1e-10
         return Y / dcol
 
     lam_max, _ = _krylov_ritz(engine, S_blocks, apply_g, X, nmax, -1, tol_max, seed + 10)
-    if int(finfo.item()) != 0:
+
+    # The inverse iteration's operator: (G^ + s I)^{-1} = L^{-H} L^{-1} by the
+    # FP64 Cholesky and triangular inverse (bem_chol_inverse), with the
+    # smallest relative shift s (1e-12, then x100 up to 1e-8) at which the
+    # factorisation succeeds.  G^ is formed with rounding errors of about
+    # 1e-14 of its diagonal, and any FP64 factorisation of it resolves
+    # eigenvalues only down to that level (an LU's backward error acts as
+    # the same perturbation); the Ritz values come from S itself, so the
+    # shift steers the subspace and does not enter them.
+    dmax = float(torch.diagonal(G).real.max()) if dt.is_complex else float(torch.diagonal(G).max())
+    Linv = None
+    for shift in (1e-12, 1e-10, 1e-8):
+        H = G.clone()
+        H.diagonal().add_(shift * dmax)
+        Linv, cinfo = engine.chol_inverse(H)
+        del H
+        if int(cinfo.item()) == 0:
+            break
+        Linv = None
+    if Linv is None:
         return 0.0, math.sqrt(max(lam_max, 0.0)), 0
 
     def solve(V):
-        # G^{-1} V = D G^^{-1} D V
-        Y = (V * dcol).contiguous()
-        engine.lu_solve(LU, piv, Y)
+        # G^{-1} V ~ D (G^ + s I)^{-1} D V = D L^{-H} (L^{-1} (D V))
+        T1 = torch.zeros_like(V)
+        engine.gemm(Linv, (V * dcol).contiguous(), T1)
+        Y = torch.zeros_like(V)
+        engine.gemm(Linv, T1, Y, conj_a=True)
         return Y * dcol
 
     lam_min, nb_min = _krylov_ritz(engine, S_blocks, solve, X, nmax, 0, tol, seed + 20)
