@@ -369,13 +369,17 @@ int bem_chol_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, in
 /* C += alpha op(A) op(B) in FP64 on the FP64 tensor cores (DMMA), dtype
  * BEM_F64 or BEM_C128, row-major: op(A) = A (m x k, lda) or, with conj_a, A^H
  * (A stored k x m); op(B) = B (k x n, ldb) or, with conj_b, B^H (B stored
- * n x k).  Products with few output tiles split K (FP64 atomic sums, so the
- * last bits depend on the order).  The matrix products of the reference's
+ * n x k).  tri: bit 0 declares op(A) lower triangular, bit 1 op(B) upper
+ * triangular: each 64-wide tile's K range then ends with the diagonal tile,
+ * so entries beyond the diagonal must be zero within the diagonal tiles and
+ * are not read beyond them.  Products with few output tiles split K (FP64 atomic
+ * sums, so the last bits depend on the order).  The matrix products of the reference's
  * operator-norm analysis (compute_inv_norm, BEM_manager.py:874-920: the
  * scaled operator L^{-1} A L^{-H}) and of the Krylov estimators that replace
  * its SVD.  Queued without synchronising. */
-int bem_gemm(bem_ctx* ctx, int dtype, int conj_a, int conj_b, int64_t m, int64_t n, int64_t k, double alpha,
-             const void* A, int64_t lda, const void* B, int64_t ldb, void* C, int64_t ldc, void* stream);
+int bem_gemm(bem_ctx* ctx, int dtype, int conj_a, int conj_b, int tri, int64_t m, int64_t n, int64_t k,
+             double alpha, const void* A, int64_t lda, const void* B, int64_t ldb, void* C, int64_t ldc,
+             void* stream);
 /* X = L^{-1} with A = L L^H (the torch.linalg.inv(torch.linalg.cholesky(MV))
  * of compute_inv_norm, BEM_manager.py:885-899): the FP64 Cholesky of A in
  * place (L in the lower triangle; the upper triangle is left as it was),

@@ -110,7 +110,7 @@ def load():
     L.bem_ctx_set_tuning.argtypes = [vp, i32, i32]
     L.bem_chol_factor.argtypes = [vp, i32, vp, i64, i64, i32, vp, vp, vp, vp]
     L.bem_near_pair_list.argtypes = [vp, vp]
-    L.bem_gemm.argtypes = [vp, i32, i32, i32, i64, i64, i64, dbl, vp, i64, vp, i64, vp, i64, vp]
+    L.bem_gemm.argtypes = [vp, i32, i32, i32, i32, i64, i64, i64, dbl, vp, i64, vp, i64, vp, i64, vp]
     L.bem_chol_inverse.argtypes = [vp, i32, vp, i64, i64, vp, i64, vp, vp]
     L.bem_gram.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, i32, vp, i64, vp]
     L.bem_lstsq_refine.argtypes = [vp, i32, vp, vp, i64, i64, vp, i32, vp, i64, vp, vp, vp, vp, dbl, i32, i32, dbl,

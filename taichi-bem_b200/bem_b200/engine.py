@@ -268,10 +268,12 @@ class Engine:
                                                float(accept), ctypes.byref(it), ctypes.byref(rr), _stream_ptr()))
         return it.value, rr.value
 
-    def gemm(self, A, B, C, alpha=1.0, conj_a=False, conj_b=False):
+    def gemm(self, A, B, C, alpha=1.0, conj_a=False, conj_b=False, a_lower=False, b_upper=False):
         """C += alpha op(A) op(B) in FP64 on the FP64 tensor cores (bem_gemm);
-        op(X) = X^H where conj_x.  A, B, C: complex128 or float64 (all the
-        same), row-major with unit column stride."""
+        op(X) = X^H where conj_x; a_lower / b_upper declare op(A) lower / op(B)
+        upper triangular (the other side of the diagonal is not read).  A, B,
+        C: complex128 or float64 (all the same), row-major with unit column
+        stride."""
         dt = C.dtype
         assert dt in (torch.complex128, torch.float64) and A.dtype == dt and B.dtype == dt
         assert A.is_cuda and B.is_cuda and C.is_cuda and A.stride(1) == 1 and B.stride(1) == 1 and C.stride(1) == 1
@@ -279,7 +281,8 @@ class Engine:
         k = A.shape[0] if conj_a else A.shape[1]
         assert (A.shape[1] if conj_a else A.shape[0]) == m
         assert (B.shape[1] if conj_b else B.shape[0]) == k and (B.shape[0] if conj_b else B.shape[1]) == n
-        self._check(self.lib.bem_gemm(self.ctx, _dtype_code(C), int(bool(conj_a)), int(bool(conj_b)), m, n, k,
+        tri = (1 if a_lower else 0) | (2 if b_upper else 0)
+        self._check(self.lib.bem_gemm(self.ctx, _dtype_code(C), int(bool(conj_a)), int(bool(conj_b)), tri, m, n, k,
                                       float(alpha), _ptr(A), A.stride(0), _ptr(B), B.stride(0), _ptr(C), C.stride(0),
                                       _stream_ptr()))
         return C

@@ -727,9 +727,9 @@ class BEMManager:
         T = torch.zeros(n, n, dtype=A.dtype, device=A.device)
         for r0 in range(0, A.shape[0], n):
             T.zero_()
-            self.engine.gemm(Linv, A[r0:r0 + n].contiguous(), T)
+            self.engine.gemm(Linv, A[r0:r0 + n].contiguous(), T, a_lower=True)
             Sb = torch.zeros(n, n, dtype=A.dtype, device=A.device)
-            self.engine.gemm(T, Linv, Sb, conj_b=True)
+            self.engine.gemm(T, Linv, Sb, conj_b=True, b_upper=True)
             blocks.append(Sb)
         del T
         if method == "svd":

@@ -191,7 +191,7 @@ def extreme_singular_values(engine, S_blocks, block: int = 8, tol: float = 1e-10
     def solve(V):
         # G^{-1} V ~ D (G^ + s I)^{-1} D V = D L^{-H} (L^{-1} (D V))
         T1 = torch.zeros_like(V)
-        engine.gemm(Linv, (V * dcol).contiguous(), T1)
+        engine.gemm(Linv, (V * dcol).contiguous(), T1, a_lower=True)
         Y = torch.zeros_like(V)
         engine.gemm(Linv, T1, Y, conj_a=True)
         return Y * dcol

@@ -161,12 +161,14 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 // CONJT).  LOWER skips the tiles strictly above the diagonal shifted by
 // `diag`.  blockIdx.z takes the K range [z kchunk, (z + 1) kchunk); with more
 // than one range the tiles are added with FP64 atomics (split K for thin
-// products).
+// products).  tri & 1: op(A) is lower triangular, tri & 2: op(B) is upper
+// triangular; the K range of a tile then ends at its diagonal.
 template <bool CPLX, bool CONJA, bool CONJT, bool LOWER>
 __global__ void __launch_bounds__(256) dmma_gemm_kernel(double* __restrict__ Cm, int64_t ldc,
                                                          const double* __restrict__ Am, int64_t lda,
                                                          const double* __restrict__ Bm, int64_t ldb, int64_t m,
-                                                         int64_t n, int k, double alpha, int64_t diag, int kchunk) {
+                                                         int64_t n, int k, double alpha, int64_t diag, int kchunk,
+                                                         int tri = 0) {
     constexpr int W = CPLX ? 2 : 1;
     constexpr int NP = CPLX ? 2 : 1;
     __shared__ double sA[NP][DG_BK][DG_LDS];
@@ -186,7 +188,10 @@ __global__ void __launch_bounds__(256) dmma_gemm_kernel(double* __restrict__ Cm,
     const int ar_ = tid >> 2, ak_ = (tid & 3) * 2;
     const int bk_ = tid >> 5, bc_ = (tid & 31) * 2;
     double ra[2][NP], rb[2][NP];
-    const int kbeg = (int)blockIdx.z * kchunk, kend = min(k, kbeg + kchunk);
+    const int kbeg = (int)blockIdx.z * kchunk;
+    int kend = min(k, kbeg + kchunk);
+    if (tri & 1) kend = (int)min((int64_t)kend, m0 + DG_BM);
+    if (tri & 2) kend = (int)min((int64_t)kend, n0 + DG_BM);
     auto fetch = [&](int k0) {
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
@@ -325,7 +330,7 @@ __global__ void iota_kernel(int32_t* piv, int n) {
 // than two waves of CTAs split K into ranges of at least 512.
 template <bool C, bool CONJA, bool CONJT, bool LOWER>
 int gemm64x(bem_ctx* ctx, double* Cm, int64_t ldc, const double* A, int64_t lda, const double* B, int64_t ldb,
-            int64_t m, int64_t n, int k, double alpha, int64_t diag, cudaStream_t s) {
+            int64_t m, int64_t n, int k, double alpha, int64_t diag, cudaStream_t s, int tri = 0) {
     if (m <= 0 || n <= 0 || k <= 0) return BEM_OK;
     dim3 grid((unsigned)((n + DG_BM - 1) / DG_BM), (unsigned)((m + DG_BM - 1) / DG_BM));
     if (grid.y > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "dmma_gemm_kernel: m too large");
@@ -336,7 +341,7 @@ int gemm64x(bem_ctx* ctx, double* Cm, int64_t ldc, const double* A, int64_t lda,
     const int kchunk = (int)(((int64_t)k + splits - 1) / splits + DG_BK - 1) / DG_BK * DG_BK;
     grid.z = (unsigned)(((int64_t)k + kchunk - 1) / kchunk);
     dmma_gemm_kernel<C, CONJA, CONJT, LOWER><<<grid, 256, 0, s>>>(Cm, ldc, A, lda, B, ldb, m, n, k, alpha, diag,
-                                                                    kchunk);
+                                                                    kchunk, tri);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "dmma_gemm_kernel");
 }
@@ -452,7 +457,7 @@ int tri_inv_rec(bem_ctx* ctx, const double* L, int64_t lda, double* X, int64_t l
 
 }  // namespace
 
-extern "C" int bem_gemm(bem_ctx* ctx, int dtype, int conj_a, int conj_b, int64_t m, int64_t n, int64_t k,
+extern "C" int bem_gemm(bem_ctx* ctx, int dtype, int conj_a, int conj_b, int tri, int64_t m, int64_t n, int64_t k,
                         double alpha, const void* A, int64_t lda, const void* B, int64_t ldb, void* Cm, int64_t ldc,
                         void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
@@ -465,8 +470,9 @@ extern "C" int bem_gemm(bem_ctx* ctx, int dtype, int conj_a, int conj_b, int64_t
     const double* b = (const double*)B;
     double* c = (double*)Cm;
     const int kk = (int)k;
+    if (tri < 0 || tri > 3) return bem_fail(ctx, BEM_ERR_INVALID, "gemm: tri must be 0..3");
 #define BEM_GEMM_CASE(CX, CA, CB) \
-    return gemm64x<CX, CA, CB, false>(ctx, c, ldc, a, lda, b, ldb, m, n, kk, alpha, 0, s)
+    return gemm64x<CX, CA, CB, false>(ctx, c, ldc, a, lda, b, ldb, m, n, kk, alpha, 0, s, tri)
     if (dtype == BEM_C128) {
         if (conj_a) {
             if (conj_b) BEM_GEMM_CASE(true, true, true);

@@ -43,6 +43,27 @@ def test_gemm_matches_numpy(engine, cplx, conj_a, conj_b, m, n, k):
     assert rel_err(C.cpu().numpy(), ref) < 1e-13
 
 
+@pytest.mark.parametrize("conj_b", [False, True])
+@pytest.mark.parametrize("m,n,k", [(200, 150, 300), (300, 8, 300), (77, 77, 77)])
+def test_gemm_triangular_operands(engine, conj_b, m, n, k):
+    """tri flags: op(A) lower and op(B) upper triangular.  Zeros on the
+    other side of the diagonal within the 64-wide diagonal tiles, and
+    garbage (1e300) beyond them, where the product must not read."""
+    rng = np.random.default_rng(m * n + k)
+    i, c = np.indices((m, k))
+    A = np.where(c <= i, _rand(rng, (m, k), True), 0.0)
+    Ag = np.where(c >= (i // 64 + 1) * 64, 1e300, A)
+    r, j = np.indices((k, n))
+    Bop = np.where(r <= j, _rand(rng, (k, n), True), 0.0)
+    Bg = np.where(r >= (j // 64 + 1) * 64, 1e300, Bop)
+    ref = A @ Bop
+    B = Bg.conj().T.copy() if conj_b else Bg
+    C = torch.zeros(m, n, dtype=torch.complex128, device="cuda")
+    engine.gemm(torch.as_tensor(Ag, device="cuda"), torch.as_tensor(B, device="cuda"), C, conj_b=conj_b,
+                a_lower=True, b_upper=True)
+    assert rel_err(C.cpu().numpy(), ref) < 1e-13
+
+
 @pytest.mark.parametrize("cplx", [True, False])
 @pytest.mark.parametrize("n", [37, 300, 777])
 def test_chol_inverse(engine, cplx, n):
