@@ -123,6 +123,8 @@ class BEMManager:
         self._desc_deriv_k = False
         self._desc_k2 = None
         self._lstsq_factor = None
+        # the norm estimator's state carried between calls (the Cholesky shift of a sweep)
+        self._norm_info = {}
         # L^{-1} of the energy scalings of A_I and A_II (compute_inv_norm)
         self._L1_inv = None
         self._L2_inv = None
@@ -737,7 +739,8 @@ class BEMManager:
             smin, smax, its = float(sv.min()), float(sv.max()), 0
         elif method == "iterative":
             from .sweep import extreme_singular_values
-            smin, smax, its = extreme_singular_values(self.engine, blocks, tol=self.norm_tol, maxit=self.norm_maxit)
+            smin, smax, its = extreme_singular_values(self.engine, blocks, tol=self.norm_tol, maxit=self.norm_maxit,
+                                                      info=self._norm_info)
         else:
             raise ValueError(method)
         inv = 1.0 / smin if smin > 0 else float("inf")

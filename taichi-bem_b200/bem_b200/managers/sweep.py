@@ -128,6 +128,10 @@ def _krylov_ritz(engine, S_blocks, apply, X0, maxblocks: int, which: int, tol: f
         nblocks += 1
 
 
+# relative diagonal shifts tried, in order, for the inverse iteration's Cholesky
+SHIFTS = (0.0, 1e-15, 1e-13, 1e-11, 1e-9)
+
+
 def extreme_singular_values(engine, S_blocks, block: int = 8, tol: float = 1e-10, tol_max: float = 1e-7,
                             maxit: int = 24, seed: int = 0, info: dict | None = None):
     """(sigma_min, sigma_max, Krylov blocks) of S = [S_0; S_1; ...] (row
@@ -169,20 +173,26 @@ def extreme_singular_values(engine, S_blocks, block: int = 8, tol: float = 1e-10
 
     # The inverse iteration's operator: (G^ + s I)^{-1} = L^{-H} L^{-1} by the
     # FP64 Cholesky and triangular inverse (bem_chol_inverse), with the
-    # smallest relative shift s (1e-12, then x100 up to 1e-8) at which the
-    # factorisation succeeds.  G^ is formed with rounding errors of about
-    # 1e-14 of its diagonal, and any FP64 factorisation of it resolves
-    # eigenvalues only down to that level (an LU's backward error acts as
-    # the same perturbation); the Ritz values come from S itself, so the
-    # shift steers the subspace and does not enter them.
+    # smallest relative shift s of SHIFTS at which the factorisation succeeds
+    # (s = 0 when G^ is numerically positive definite), starting at
+    # info["shift_index"] when given (a sweep passes the previous k's).  G^ is
+    # formed with rounding errors of about 1e-14 of its diagonal, and any FP64
+    # factorisation of it resolves eigenvalues only down to that level (an
+    # LU's backward error acts as the same perturbation); the Ritz values
+    # come from S itself, so the shift steers the subspace and does not enter
+    # them.
     dmax = float(torch.diagonal(G).real.max()) if dt.is_complex else float(torch.diagonal(G).max())
     Linv = None
-    for shift in (1e-12, 1e-10, 1e-8):
+    start = int(info.get("shift_index", 0)) if info is not None else 0
+    for si in range(max(0, min(start, len(SHIFTS) - 1)), len(SHIFTS)):
         H = G.clone()
-        H.diagonal().add_(shift * dmax)
+        if SHIFTS[si] > 0:
+            H.diagonal().add_(SHIFTS[si] * dmax)
         Linv, cinfo = engine.chol_inverse(H)
         del H
         if int(cinfo.item()) == 0:
+            if info is not None:
+                info["shift_index"] = si
             break
         Linv = None
     if Linv is None:
