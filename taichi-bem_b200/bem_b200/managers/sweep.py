@@ -33,9 +33,12 @@ class Basis:
     so that appended columns W satisfy W = Q R with R upper triangular, kept
     on the device as its transpose Rt (Rt[c, i] = R[i, c]).  Norms and R stay
     on the device, so appending synchronises nothing.  A column numerically
-    inside span(Q) leaves a tiny r_jj and, after the second projection, a
-    normalised rounding direction orthogonal to Q, which the basis keeps; an
-    exactly dependent column leaves r_jj = 0 and a zero column."""
+    inside span(Q) (frequent in inverse and power iteration) leaves a tiny
+    r_jj, which R keeps, and a residual of rounding noise with components
+    along Q; the normalised q_j is therefore projected twice more and
+    normalised again (these last coefficients, of the order of r_jj, do not
+    enter R), which makes it orthogonal to Q whether or not the column was
+    dependent.  An exactly dependent column leaves r_jj = 0."""
 
     def __init__(self, engine, n, cap, dtype, device):
         self.engine = engine
@@ -75,7 +78,15 @@ class Basis:
                     r.add_(h)
             rjj = self._norm(v)
             self.Rt[col, col] = rjj.to(self.Rt.dtype)
-            self.Q[:, col:col + 1] = v / rjj.clamp_min(1e-300).to(v.dtype)
+            q = v / rjj.clamp_min(1e-300).to(v.dtype)
+            if j > 0:
+                h = self._h[:j].view(j, 1)
+                for _ in range(2):
+                    h.zero_()
+                    self.engine.gemm(self.active, q, h, conj_a=True)
+                    self.engine.gemm(self.active, h, q, alpha=-1.0)
+                q = q / self._norm(q).clamp_min(1e-300).to(q.dtype)
+            self.Q[:, col:col + 1] = q
             self.j += 1
             added += 1
         return added

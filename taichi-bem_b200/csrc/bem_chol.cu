@@ -35,6 +35,7 @@
 namespace {
 
 constexpr int CH_IB = 64;   // diagonal sub-block
+constexpr int CH_SP = 256;  // sub-panel width of the panel factorisation
 constexpr int CH_NB_DEFAULT = 1024;  // panel width (columns per trailing update; measured 510 / 410 / 384 ms for 256 / 512 / 1024 on the 30722-unknown normal matrix)
 constexpr int CH_LD = CH_IB + 1;
 
@@ -378,8 +379,13 @@ int chol_t(bem_ctx* ctx, double* A, int64_t n, int64_t lda, bool tensor_cores, i
     const int nbw = ctx->tune[BEM_TUNE_CHOL_NB] > 0 ? ctx->tune[BEM_TUNE_CHOL_NB] : CH_NB_DEFAULT;
     for (int64_t k0 = 0; k0 < n; k0 += nbw) {
         const int64_t kb = std::min<int64_t>(nbw, n - k0);
-        for (int64_t j0 = k0; j0 < k0 + kb; j0 += CH_IB) {
-            const int jb = (int)std::min<int64_t>(CH_IB, k0 + kb - j0);
+        // the panel in sub-panels of CH_SP columns: 64-wide steps update only
+        // their sub-panel's remaining columns (K = 64); the sub-panel then
+        // updates the rest of the panel in one product (K = CH_SP)
+        for (int64_t s0 = k0; s0 < k0 + kb; s0 += CH_SP) {
+        const int64_t sb = std::min<int64_t>(CH_SP, k0 + kb - s0);
+        for (int64_t j0 = s0; j0 < s0 + sb; j0 += CH_IB) {
+            const int jb = (int)std::min<int64_t>(CH_IB, s0 + sb - j0);
             chol64_kernel<C><<<1, 256, smem, s>>>(at(j0, j0), lda, jb, inv, info, (int)j0);
             ctx->launches++;
             if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "chol64_kernel")) return rc;
@@ -402,12 +408,19 @@ int chol_t(bem_ctx* ctx, double* A, int64_t n, int64_t lda, bool tensor_cores, i
                                                                cudaMemcpyDeviceToDevice, s),
                                         "L21 copy"))
                 return rc;
-            // the panel's remaining columns: A[r1:, r1:k0+kb] -= L21 L21[0:w]^H (lower part)
-            const int64_t w = k0 + kb - r1;
+            // the sub-panel's remaining columns: A[r1:, r1:s0+sb] -= L21 L21[0:w]^H (lower part)
+            const int64_t w = s0 + sb - r1;
             if (w > 0)
                 if (int rc = gemm64<C, true, true>(ctx, at(r1, r1), lda, at(r1, j0), lda, at(r1, j0), lda, m1, w, jb,
                                                    -1.0, 0, s))
                     return rc;
+        }
+        // the rest of the panel: A[r3:, r3:k0+kb] -= L_sub L_sub[0:w3]^H (lower part, K = sb)
+        const int64_t r3 = s0 + sb, w3 = k0 + kb - r3, m3 = n - r3;
+        if (w3 > 0 && m3 > 0)
+            if (int rc = gemm64<C, true, true>(ctx, at(r3, r3), lda, at(r3, s0), lda, at(r3, s0), lda, m3, w3,
+                                               (int)sb, -1.0, 0, s))
+                return rc;
         }
         // trailing Hermitian update of the lower triangle
         const int64_t r2 = k0 + kb, m2 = n - r2;

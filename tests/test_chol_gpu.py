@@ -47,6 +47,28 @@ def test_chol_solve_matches_numpy(engine, n, cplx, tensor_cores):
     assert err < (1e-5 if tensor_cores else 1e-11), err
 
 
+@pytest.mark.parametrize("nb", [256, 512, 1024])
+def test_chol_panels_and_subpanels(engine, nb):
+    """Several panels (BEM_TUNE_CHOL_NB) with partial sub-panels of 256
+    columns and a partial last panel, FP64 updates: to 1e-11."""
+    from bem_b200 import _lib as L
+    n = 1333
+    N = _hpd(n, True, 7)
+    A = torch.as_tensor(N, device="cuda")
+    F = A.clone()
+    engine.set_tuning(L.TUNE_CHOL_NB, nb)
+    try:
+        piv, dinv, info = engine.chol_factor(F, tensor_cores=False)
+    finally:
+        engine.set_tuning(L.TUNE_CHOL_NB, 0)
+    assert int(info.item()) == 0
+    b = np.random.default_rng(2).standard_normal(n) + 0j
+    x = torch.as_tensor(b, device="cuda").contiguous()
+    engine.lu_solve_tiled(F, piv, dinv, x)
+    ref = np.linalg.solve(N, b)
+    assert np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-11
+
+
 def test_chol_reports_indefinite(engine):
     """A matrix with a negative pivot sets info to 1 + that column."""
     N = _hpd(130, True, 3)

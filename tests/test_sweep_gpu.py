@@ -123,3 +123,30 @@ def test_sweep_solutions_match_oracle_lstsq():
         rhs = np.concatenate([B.cpu().numpy(), np.zeros((n, B.shape[1]))], 0)
         ref = np.linalg.lstsq(Sa, rhs, rcond=None)[0]
         assert rel_err(X.cpu().numpy(), ref) < 1e-6
+
+
+def test_krylov_estimates_with_a_complete_basis():
+    """The block-Krylov estimator when its bases fill the whole space
+    (icosphere s1, 8-vector blocks up to n): inverse and power iteration make
+    most columns numerically dependent, and the estimates must still be the
+    extreme singular values of the numpy SVD of the same scaled operator."""
+    from bem_b200.managers.sweep import extreme_singular_values
+    core, v, f = _manager("fp64")
+    b = core._BEM_manager
+    b.get_mat_A1_inv_norm(0.0, method="none")
+    from bem_b200.managers.sweep import transmission_operator
+    At = transmission_operator(b, KS[1], 1, augmented=True)
+    n = At.shape[1]
+    Linv = b._L1_inv
+    blocks = []
+    for r0 in (0, n):
+        T = torch.zeros(n, n, dtype=At.dtype, device=At.device)
+        b.engine.gemm(Linv, At[r0:r0 + n].contiguous(), T, a_lower=True)
+        Sb = torch.zeros_like(T)
+        b.engine.gemm(T, Linv, Sb, conj_b=True, b_upper=True)
+        blocks.append(Sb)
+    sv = np.linalg.svd(torch.cat(blocks, 0).cpu().numpy(), compute_uv=False)
+    smin, smax, its = extreme_singular_values(b.engine, blocks, tol=0.0, tol_max=0.0, maxit=n // 8)
+    core.kill()
+    assert abs(smin - sv[-1]) <= 1e-6 * sv[-1], (smin, sv[-1])
+    assert abs(smax - sv[0]) <= 1e-9 * sv[0], (smax, sv[0])
