@@ -705,10 +705,11 @@ def cpu_reference_transmission(steps: int, warmup: int, threads: int | None = No
 def transmission_headline(args, ws, rank, local):
     """The north-star line: the Helmholtz transmission problem on icosphere s5
     (TRANS_WORKLOAD), mixed precision (FP32 far field in the fused Calderon
-    sweep, FP64 near field, FP16-split tensor-core normal matrix, FP32 tile
-    LU, FP64 flexible GMRES on the normal equations) against the plain FP64
-    path (FP64 sweep, FP64 tensor-core normal matrix, FP64 tile LU, the same
-    FP64 iteration), whose solution is the FP64 oracle of the error."""
+    sweep, FP64 near field, FP16-split tensor-core normal matrix, Cholesky
+    with tensor-core updates into an FP64 Schur complement, FP64 flexible
+    GMRES on the normal equations) against the plain FP64 path (FP64 sweep,
+    DMMA normal matrix, Cholesky with DMMA updates, the same FP64
+    iteration), whose solution is the FP64 oracle of the error."""
     import torch
     import torch.distributed as dist
 
