@@ -104,8 +104,10 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  *   BEM_TUNE_CALDERON_GROUP  form of the fused Calderon sweep: 1 scalar, one
  *                            wavenumber per launch; 2 scalar, both in one
  *                            launch (the default for two wavenumbers); 3 packed
- *                            FP32x2, one wavenumber per launch (the default of
- *                            a single-wavenumber mixed Helmholtz sweep)
+ *                            FP32x2 over test points, one wavenumber per
+ *                            launch (the default of a single-wavenumber mixed
+ *                            Helmholtz sweep); 4 both wavenumbers packed into
+ *                            the FP32x2 lanes, one launch (mixed Helmholtz)
  *   BEM_TUNE_GRAM_KSEG       64-wide K stages per TMEM accumulation segment of
  *                            the tensor-core normal matrix (>= 1)
  *   BEM_TUNE_CHOL_NB         panel width of bem_chol_factor (a multiple of 64)

@@ -69,6 +69,8 @@ class SingleLayer3d(_Layer):
     def __init__(self, BEM_manager):
         super().__init__(BEM_manager)
         self._Vmat = None
+        # _Vmat is a view of the manager's _mat_A (the fused Dirichlet pass)
+        self._v_alias = False
 
     def get_V_mat(self):
         return self._Vmat
@@ -78,8 +80,9 @@ class SingleLayer3d(_Layer):
         if self.N_Neumann <= 0:
             return
         b = self._BEM_manager
-        if self._Vmat is None:
+        if self._Vmat is None or self._v_alias:
             self._Vmat = self._zeros(self.N_Neumann, self.N_Neumann)
+            self._v_alias = False
         else:
             self._Vmat.zero_()
         sp = b.space("charge", self._Q_Neumann, "N", _N)

@@ -264,13 +264,6 @@ class BEMManager:
         self._scope_type = scope_type
 
     # -- operators and block system ------------------------------------------------------
-    def matrix_layer_init(self):
-        for lay in (self.single_layer, self.double_layer, self.hypersingular_layer):
-            for name in ("_Vmat", "_Kmat", "_Wmat"):
-                t = getattr(lay, name, None)
-                if t is not None:
-                    t.zero_()
-
     def matrix_layer_forward(self, k: float, sqrt_n: float = 1.0, scope_type: int = int(ScopeType.NOT_DEFINED)):
         if scope_type == int(ScopeType.NOT_DEFINED):
             raise RuntimeError("Did not indicate a correct scope type!")
@@ -605,25 +598,40 @@ class BEMManager:
 
     def _run_dirichlet_fused(self):
         """matrix_layer_forward + assemble_matA(ADD_M, -1) + set_boundaries +
-        rhs_layer_forward + assemble_rhs with V and K g assembled in one pass."""
+        rhs_layer_forward + assemble_rhs with V and K g assembled in one pass.
+        The system matrix of this problem is V itself (P0 Neumann unknowns
+        only), so the sweep writes V straight into the zeroed _mat_A and the
+        single layer's _Vmat is a view of it (flagged, so that the layer's
+        own forward or matrix_layer_init give it its own storage again)
+        instead of a separate block zeroed, filled and copied."""
         rc = self.rhs_constructor
         rc.set_boundaries(scope_type=self._scope_type, sqrt_ni=self._sqrt_ni, sqrt_no=self._sqrt_no)
         lay = self.single_layer
-        if lay._Vmat is None:
-            lay._Vmat = lay._zeros(self.N_Neumann, self.N_Neumann)
+        direct = self._mat_A.shape == (self.N_Neumann, self.N_Neumann) and self._Neumann_offset_i == 0 \
+            and self._Neumann_offset_j == 0
+        if direct:
+            lay._Vmat = self._mat_A  # zeroed by assemble_system
+            lay._v_alias = True
         else:
-            lay._Vmat.zero_()
+            if lay._Vmat is None or lay._v_alias:
+                lay._Vmat = lay._zeros(self.N_Neumann, self.N_Neumann)
+                lay._v_alias = False
+            else:
+                lay._Vmat.zero_()
         rc._rhs_vec.zero_()
         self.fused_assembly_call()
         half = 0.5 if self._scope_type == int(ScopeType.INTERIOR) else -0.5
         rc.multiply_identity_to_vector(multiplier=half)
-        self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)
+        if not direct:
+            self.assemble_matA(assemble_type=int(AssembleType.ADD_M), multiplier=-1.0)
         self.assemble_rhs()
 
     # -- operator norms (BEM_manager.py:846-988) ------------------------------------
     def matrix_layer_init(self):
         """Zero the operator blocks (BEM_manager.py:823-827)."""
         for lay in (self.single_layer, self.double_layer, self.adj_double_layer, self.hypersingular_layer):
+            if getattr(lay, "_v_alias", False):
+                lay._Vmat, lay._v_alias = None, False  # a view of _mat_A: give the layer its own block
             for name in ("_Vmat", "_Kmat", "_Wmat"):
                 blk = getattr(lay, name, None)
                 if blk is not None:
@@ -883,7 +891,9 @@ class BEMManager:
         """Choose the launch shapes of this problem's hot calls on this GPU
         (bem_b200.tuning): the form of the fused Calderon sweep (transmission
         problems it takes; candidates 2: both wavenumbers in one scalar
-        launch, 3: packed FP32x2 per wavenumber, 1: scalar per wavenumber),
+        launch, 4: both packed into FP32x2 lanes, 3: packed FP32x2 per
+        wavenumber, 1: scalar per wavenumber; the packed forms in mixed
+        precision only),
         timed on assemble_system, and for the least-squares solver the band
         width of the normal matrix's tile order (1, 12, 8, 16), timed on the
         normal matrix, and the Cholesky panel width (512, 1024, 2048), timed
@@ -895,7 +905,8 @@ class BEMManager:
         wl = f"{self._simulation_parameters['kernel']}/n{n}/Q{self._GaussQR}/{self.precision}-{self.solve_precision}"
         out = {}
         if self._is_transmission and self._calderon_fusable():
-            out["calderon_group"] = tuner.tune(wl + "/calderon", L.TUNE_CALDERON_GROUP, [2, 3, 1],
+            groups = [2, 4, 3, 1] if self.precision == "mixed" else [2, 1]
+            out["calderon_group"] = tuner.tune(wl + "/calderon", L.TUNE_CALDERON_GROUP, groups,
                                                self.assemble_system)
         nbs = [512, 1024, 2048]
         if (self._is_transmission and self.solver == "lstsq" and tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs)

@@ -579,6 +579,216 @@ __global__ void __launch_bounds__(FAR_THREADS) far_calderon_x2_kernel(CalArgs a)
     }
 }
 
+// Both wavenumbers of the FP32 Helmholtz sweep packed into the two lanes of
+// FP32x2 instructions (x: k[0], y: k[1]): the pair-frame geometry of a point
+// pair (r, 1/r, the split phase, w/r, w/r^3, d.n_j) is formed once in scalar
+// FP32, and the per-wavenumber part -- the phase k (r - R), its sine and
+// cosine, (1 - ikr) e^{ikr} and the 14 sums over the test points -- runs on
+// FFMA2 / FMUL2 / FADD2, one instruction for both wavenumbers.  Same
+// algebra, summation order and FP64 moments as
+// far_calderon_kernel<float, 2, true, PH>; the test points' phi_1, phi_2 are
+// staged as broadcast pairs.  PH 2 / 1: the short / full sine and cosine
+// polynomials without argument reduction; PH 0: the reduced scalar form per
+// lane.
+template <int PH>
+__global__ void __launch_bounds__(FAR_THREADS) far_calderon_k2_kernel(CalArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* sx = reinterpret_cast<float4*>(smem_raw);     // [FAR_TI][Q2] test points
+    float4* sp = reinterpret_cast<float4*>(sx + FAR_TI * a.Q2);  // [Q2] (phi_1, phi_1, phi_2, phi_2)
+    __shared__ int s_gi[FAR_TI];
+    __shared__ int s_tri[FAR_TI][3];
+    __shared__ double s_cen[FAR_TI][3];
+    __shared__ double s_nrm[FAR_TI][3];
+
+    const int Q2 = a.Q2;
+    const int n = a.n;
+    const int j0 = blockIdx.x * FAR_THREADS;
+    const int li0 = blockIdx.y * FAR_TI;
+    if (j0 + FAR_THREADS - 1 <= li0) return;  // tile strictly below the diagonal
+    const int lj = j0 + threadIdx.x;
+    const float4* pts = reinterpret_cast<const float4*>(a.pts);
+    {
+        const float* phi = reinterpret_cast<const float*>(a.phi);
+        for (int q = threadIdx.x; q < Q2; q += FAR_THREADS) {
+            const float p1 = phi[3 * q + 1], p2 = phi[3 * q + 2];
+            sp[q] = make_float4(p1, p1, p2, p2);
+        }
+    }
+    if (threadIdx.x < FAR_TI) {
+        const int li = li0 + threadIdx.x;
+        const int gi = li < n ? a.panels[li] : -1;
+        s_gi[threadIdx.x] = gi;
+        for (int c = 0; c < 3; ++c) {
+            s_tri[threadIdx.x][c] = gi >= 0 ? a.tris[3 * gi + c] : -1;
+            s_cen[threadIdx.x][c] = gi >= 0 ? a.centroid[3 * gi + c] : 0.0;
+            s_nrm[threadIdx.x][c] = gi >= 0 ? a.normal[3 * gi + c] : 0.0;
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < FAR_TI * Q2; idx += FAR_THREADS) {
+        const int t = idx / Q2, q = idx - t * Q2;
+        if (li0 + t < n) sx[idx] = pts[(size_t)s_gi[t] * Q2 + q];
+    }
+    __syncthreads();
+
+    const bool valid_j = lj < n;
+    const int gj = valid_j ? a.panels[lj] : 0;
+    int tri_j[3];
+    double cen_j[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        tri_j[c] = a.tris[3 * gj + c];
+        cen_j[c] = a.centroid[3 * gj + c];
+    }
+    const double nj64[3] = {a.normal[3 * gj + 0], a.normal[3 * gj + 1], a.normal[3 * gj + 2]};
+    const float4* ptsj = pts + (size_t)gj * Q2;
+    const float2 kk = make_float2(float(a.k[0]), float(a.k[1]));
+    const float2 nkk = make_float2(-float(a.k[0]), -float(a.k[1]));
+
+    for (int t = 0; t < FAR_TI; ++t) {
+        const int li = li0 + t;
+        if (li >= n) break;  // uniform across the CTA
+        const int gi = s_gi[t];
+        const bool sep = valid_j && li < lj && (bem_relation(s_tri[t], tri_j, gi == gj) == REL_SEPARATE);
+        if (!sep) continue;
+        const double Dx = s_cen[t][0] - cen_j[0], Dy = s_cen[t][1] - cen_j[1], Dz = s_cen[t][2] - cen_j[2];
+        const double ni64[3] = {s_nrm[t][0], s_nrm[t][1], s_nrm[t][2]};
+        const float ux = float(2.0 * Dx), uy = float(2.0 * Dy), uz = float(2.0 * Dz);
+        const double R2d = Dx * Dx + Dy * Dy + Dz * Dz;
+        const float R2 = float(R2d);
+        const double Rd = sqrt(R2d);
+        const float Rf = float(Rd);
+        const double pf = 4.0 * a.area[gi] * a.area[gj] * a.wcorr;
+        const float Dnj = float(Dx * nj64[0] + Dy * nj64[1] + Dz * nj64[2]);
+        const double Dni64 = Dx * ni64[0] + Dy * ni64[1] + Dz * ni64[2];
+        const float mx = float(nj64[0] - ni64[0]), my = float(nj64[1] - ni64[1]), mz = float(nj64[2] - ni64[2]);
+        const float4* sxt = sx + t * Q2;
+
+        double Mr[2][15], Mi[2][15];
+#pragma unroll
+        for (int w = 0; w < 2; ++w)
+#pragma unroll
+            for (int m = 0; m < 15; ++m) Mr[w][m] = Mi[w][m] = 0.0;
+
+        for (int b = 0; b < Q2; ++b) {
+            const float4 yb = ptsj[b];
+            const float wx = ux - yb.x, wy = uy - yb.y, wz = uz - yb.z;
+            // packed sums over the test points (lanes: the two wavenumbers), as in
+            // far_calderon_kernel: [0] G, [1] phi1 G, [2] phi2 G, [3] d.n_j F/r^3,
+            // [4] F/r^3, [5] phi1 F/r^3, [6] phi2 F/r^3
+            float2 sr[7], si[7];
+#pragma unroll
+            for (int m = 0; m < 7; ++m) sr[m] = si[m] = make_float2(0.0f, 0.0f);
+#pragma unroll 5
+            for (int q = 0; q < Q2; ++q) {
+                const float4 xa = sxt[q];
+                const float4 pp = sp[q];
+                const float2 p1 = make_float2(pp.x, pp.y), p2 = make_float2(pp.z, pp.w);
+                float r, rinv;
+                const float e_x = xa.x - yb.x, e_y = xa.y - yb.y, e_z = xa.z - yb.z;
+                const float sq = e_x * (xa.x + wx) + e_y * (xa.y + wy) + e_z * (xa.z + wz);
+                dev_r_rinv(R2 + sq, r, rinv);
+                const float dnj = fmaf(xa.x, mx, fmaf(xa.y, my, fmaf(xa.z, mz, Dnj)));
+                const float ph = __fdividef(sq, r + Rf);
+                const float wr = xa.w * rinv;
+                const float wr3 = wr * (rinv * rinv);
+                const float tj = wr3 * dnj;
+                const float2 y = fmul2(kk, f2(ph));
+                float2 sn, cs;
+                if (PH == 2) {
+                    dev_sincos_poly2<true>(y, sn, cs);
+                } else if (PH == 1) {
+                    dev_sincos_poly2<false>(y, sn, cs);
+                } else {
+                    dev_sincos(y.x, &sn.x, &cs.x);
+                    dev_sincos(y.y, &sn.y, &cs.y);
+                }
+                const float2 rr = f2(r);
+                const float2 kr = fmul2(kk, rr), nkr = fmul2(nkk, rr);
+                const float2 w2 = f2(wr), w32 = f2(wr3);
+                const float2 gr = fmul2(w2, cs), gim = fmul2(w2, sn);
+                const float2 fr = ffma2(kr, sn, cs);
+                const float2 fi = ffma2(nkr, cs, sn);
+                const float2 t2 = f2(tj);
+                sr[0] = fadd2(sr[0], gr);
+                sr[1] = ffma2(p1, gr, sr[1]);
+                sr[2] = ffma2(p2, gr, sr[2]);
+                sr[3] = ffma2(t2, fr, sr[3]);
+                const float2 hr = fmul2(w32, fr);
+                sr[4] = fadd2(sr[4], hr);
+                sr[5] = ffma2(p1, hr, sr[5]);
+                sr[6] = ffma2(p2, hr, sr[6]);
+                si[0] = fadd2(si[0], gim);
+                si[1] = ffma2(p1, gim, si[1]);
+                si[2] = ffma2(p2, gim, si[2]);
+                si[3] = ffma2(t2, fi, si[3]);
+                const float2 hi = fmul2(w32, fi);
+                si[4] = fadd2(si[4], hi);
+                si[5] = ffma2(p1, hi, si[5]);
+                si[6] = ffma2(p2, hi, si[6]);
+            }
+            const double wb = double(yb.w);
+            const double wb1 = wb * a.phi64[3 * b + 1], wb2 = wb * a.phi64[3 * b + 2];
+            const double ndni =
+                -(Dni64 - (double(yb.x) * ni64[0] + double(yb.y) * ni64[1] + double(yb.z) * ni64[2]));
+            const double wbn = wb * ndni;
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+                const double s3r = w ? sr[3].y : sr[3].x, s3i = w ? si[3].y : si[3].x;
+                const double g0r = w ? sr[0].y : sr[0].x, g0i = w ? si[0].y : si[0].x;
+                const double g1r = w ? sr[1].y : sr[1].x, g1i = w ? si[1].y : si[1].x;
+                const double g2r = w ? sr[2].y : sr[2].x, g2i = w ? si[2].y : si[2].x;
+                const double h0r = w ? sr[4].y : sr[4].x, h0i = w ? si[4].y : si[4].x;
+                const double h1r = w ? sr[5].y : sr[5].x, h1i = w ? si[5].y : si[5].x;
+                const double h2r = w ? sr[6].y : sr[6].x, h2i = w ? si[6].y : si[6].x;
+                Mr[w][0] += wb * g0r;
+                Mi[w][0] += wb * g0i;
+                Mr[w][1] += wb * s3r;
+                Mi[w][1] += wb * s3i;
+                Mr[w][2] += wb1 * s3r;
+                Mi[w][2] += wb1 * s3i;
+                Mr[w][3] += wb2 * s3r;
+                Mi[w][3] += wb2 * s3i;
+                Mr[w][4] += wbn * h0r;
+                Mi[w][4] += wbn * h0i;
+                Mr[w][5] += wbn * h1r;
+                Mi[w][5] += wbn * h1i;
+                Mr[w][6] += wbn * h2r;
+                Mi[w][6] += wbn * h2i;
+                Mr[w][7] += wb1 * g0r;
+                Mi[w][7] += wb1 * g0i;
+                Mr[w][8] += wb2 * g0r;
+                Mi[w][8] += wb2 * g0i;
+                Mr[w][9] += wb * g1r;
+                Mi[w][9] += wb * g1i;
+                Mr[w][10] += wb1 * g1r;
+                Mi[w][10] += wb1 * g1i;
+                Mr[w][11] += wb2 * g1r;
+                Mi[w][11] += wb2 * g1i;
+                Mr[w][12] += wb * g2r;
+                Mi[w][12] += wb * g2i;
+                Mr[w][13] += wb1 * g2r;
+                Mi[w][13] += wb1 * g2i;
+                Mr[w][14] += wb2 * g2r;
+                Mi[w][14] += wb2 * g2i;
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < 2; ++w)
+            calderon_epilogue<true>(a, w, li, lj, gi, gj, ni64, nj64, pf, Rd, Mr[w], Mi[w], true);
+    }
+}
+
+template <int PH>
+int launch_calderon_k2(bem_ctx* ctx, const CalArgs& a, cudaStream_t s) {
+    dim3 grid((a.n + FAR_THREADS - 1) / FAR_THREADS, (a.n + FAR_TI - 1) / FAR_TI);
+    if (grid.y > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "calderon: too many panels for one launch");
+    const size_t smem = FAR_TI * a.Q2 * sizeof(float4) + a.Q2 * sizeof(float4);
+    far_calderon_k2_kernel<PH><<<grid, FAR_THREADS, smem, s>>>(a);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "far_calderon_k2_kernel launch");
+}
+
 template <typename T, int NK, bool HELM, int PH>
 int launch_calderon(bem_ctx* ctx, const CalArgs& a, cudaStream_t s) {
     dim3 grid((a.n + FAR_THREADS - 1) / FAR_THREADS, (a.n + FAR_TI - 1) / FAR_TI);
@@ -688,7 +898,11 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
     // mixed Helmholtz default
     int rc = BEM_OK;
     const int variant = ctx->tune[BEM_TUNE_CALDERON_GROUP];
-    if (fp32 && helm && (variant == 3 || (variant == 0 && nk == 1))) {
+    if (fp32 && helm && nk == 2 && variant == 4) {
+        // both wavenumbers packed into the FP32x2 lanes, one launch
+        rc = phase_class == 2 ? launch_calderon_k2<2>(ctx, a, s)
+                              : (phase_class == 1 ? launch_calderon_k2<1>(ctx, a, s) : launch_calderon_k2<0>(ctx, a, s));
+    } else if (fp32 && helm && (variant == 3 || (variant == 0 && nk == 1))) {
         // packed FP32x2, one wavenumber per launch
         for (int w = 0; w < nk && !rc; ++w) {
             CalArgs b = a;

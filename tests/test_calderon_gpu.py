@@ -81,7 +81,9 @@ def test_fused_matches_per_operator_path(precision):
 def test_laplace_full_and_grouped_wavenumbers():
     """Laplace "Full" problems take the same path (k = 0), and the forms of the
     sweep agree: one launch with both wavenumbers (tuning group 2), one per
-    wavenumber (1), and the packed FP32x2 sweep (3, mixed precision)."""
+    wavenumber (1), and the packed FP32x2 sweeps (3: over test points, one
+    wavenumber per launch; 4: the two wavenumbers in the two lanes; mixed
+    precision)."""
     from bem_b200 import _lib as L
     core, b, v, f = _problem(2, "fp64", Q=3, kernel="Laplace")
     b.assemble_system()
@@ -90,7 +92,7 @@ def test_laplace_full_and_grouped_wavenumbers():
     core.kill()
     for prec in ("fp64", "mixed"):
         outs = []
-        for group in ((1, 2) if prec == "fp64" else (1, 2, 3)):
+        for group in ((1, 2) if prec == "fp64" else (1, 2, 3, 4)):
             core, b, *_ = _problem(2, prec)
             b.engine.set_tuning(L.TUNE_CALDERON_GROUP, group)
             b.assemble_system()
