@@ -107,7 +107,8 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  *                            FP32x2 over test points, one wavenumber per
  *                            launch (the default of a single-wavenumber mixed
  *                            Helmholtz sweep); 4 both wavenumbers packed into
- *                            the FP32x2 lanes, one launch (mixed Helmholtz)
+ *                            the FP32x2 lanes, one launch (mixed Helmholtz);
+ *                            5 the same with its FP64 moments in shared memory
  *   BEM_TUNE_GRAM_KSEG       64-wide K stages per TMEM accumulation segment of
  *                            the tensor-core normal matrix (>= 1)
  *   BEM_TUNE_CHOL_NB         panel width of bem_chol_factor (a multiple of 64)

@@ -891,7 +891,8 @@ class BEMManager:
         """Choose the launch shapes of this problem's hot calls on this GPU
         (bem_b200.tuning): the form of the fused Calderon sweep (transmission
         problems it takes; candidates 2: both wavenumbers in one scalar
-        launch, 4: both packed into FP32x2 lanes, 3: packed FP32x2 per
+        launch, 4 / 5: both packed into FP32x2 lanes (moments in registers /
+        shared memory), 3: packed FP32x2 per
         wavenumber, 1: scalar per wavenumber; the packed forms in mixed
         precision only),
         timed on assemble_system, and for the least-squares solver the band
@@ -905,7 +906,7 @@ class BEMManager:
         wl = f"{self._simulation_parameters['kernel']}/n{n}/Q{self._GaussQR}/{self.precision}-{self.solve_precision}"
         out = {}
         if self._is_transmission and self._calderon_fusable():
-            groups = [2, 4, 3, 1] if self.precision == "mixed" else [2, 1]
+            groups = [2, 4, 5, 3, 1] if self.precision == "mixed" else [2, 1]
             out["calderon_group"] = tuner.tune(wl + "/calderon", L.TUNE_CALDERON_GROUP, groups,
                                                self.assemble_system)
         nbs = [512, 1024, 2048]

@@ -142,7 +142,7 @@ extern "C" {
 int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value) {
     if (!ctx) return BEM_ERR_INVALID;
     if (key < 0 || key >= BEM_TUNE_KEYS) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: unknown key");
-    if (key == BEM_TUNE_CALDERON_GROUP && (value < 0 || value > 4))
+    if (key == BEM_TUNE_CALDERON_GROUP && (value < 0 || value > 5))
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon form must be 1, 2 or 3");
     if (key == BEM_TUNE_GRAM_KSEG && value < 0) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: negative segment");
     if (key == BEM_TUNE_GRAM_BAND && (value < 0 || value > 4096))

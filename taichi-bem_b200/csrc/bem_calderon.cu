@@ -590,11 +590,15 @@ __global__ void __launch_bounds__(FAR_THREADS) far_calderon_x2_kernel(CalArgs a)
 // staged as broadcast pairs.  PH 2 / 1: the short / full sine and cosine
 // polynomials without argument reduction; PH 0: the reduced scalar form per
 // lane.
-template <int PH>
-__global__ void __launch_bounds__(FAR_THREADS) far_calderon_k2_kernel(CalArgs a) {
+template <int PH, bool SM>
+__global__ void __launch_bounds__(FAR_THREADS, SM ? 3 : 1) far_calderon_k2_kernel(CalArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* sx = reinterpret_cast<float4*>(smem_raw);     // [FAR_TI][Q2] test points
     float4* sp = reinterpret_cast<float4*>(sx + FAR_TI * a.Q2);  // [Q2] (phi_1, phi_1, phi_2, phi_2)
+    // SM: the FP64 moments over the trial points live in shared memory,
+    // [moment][thread] with moment (w * 15 + m) * 2 + (0 re, 1 im), so that
+    // three CTAs fit an SM; otherwise in registers
+    double* mom = reinterpret_cast<double*>(sp + a.Q2) + threadIdx.x;
     __shared__ int s_gi[FAR_TI];
     __shared__ int s_tri[FAR_TI][3];
     __shared__ double s_cen[FAR_TI][3];
@@ -665,10 +669,25 @@ __global__ void __launch_bounds__(FAR_THREADS) far_calderon_k2_kernel(CalArgs a)
         const float4* sxt = sx + t * Q2;
 
         double Mr[2][15], Mi[2][15];
+        if constexpr (SM) {
 #pragma unroll
-        for (int w = 0; w < 2; ++w)
+            for (int m = 0; m < 60; ++m) mom[m * FAR_THREADS] = 0.0;
+        } else {
 #pragma unroll
-            for (int m = 0; m < 15; ++m) Mr[w][m] = Mi[w][m] = 0.0;
+            for (int w = 0; w < 2; ++w)
+#pragma unroll
+                for (int m = 0; m < 15; ++m) Mr[w][m] = Mi[w][m] = 0.0;
+        }
+        auto acc = [&](int w, int m, double re, double im) {
+            if constexpr (SM) {
+                double* q = mom + ((w * 15 + m) * 2) * FAR_THREADS;
+                q[0] += re;
+                q[FAR_THREADS] += im;
+            } else {
+                Mr[w][m] += re;
+                Mi[w][m] += im;
+            }
+        };
 
         for (int b = 0; b < Q2; ++b) {
             const float4 yb = ptsj[b];
@@ -741,50 +760,48 @@ __global__ void __launch_bounds__(FAR_THREADS) far_calderon_k2_kernel(CalArgs a)
                 const double h0r = w ? sr[4].y : sr[4].x, h0i = w ? si[4].y : si[4].x;
                 const double h1r = w ? sr[5].y : sr[5].x, h1i = w ? si[5].y : si[5].x;
                 const double h2r = w ? sr[6].y : sr[6].x, h2i = w ? si[6].y : si[6].x;
-                Mr[w][0] += wb * g0r;
-                Mi[w][0] += wb * g0i;
-                Mr[w][1] += wb * s3r;
-                Mi[w][1] += wb * s3i;
-                Mr[w][2] += wb1 * s3r;
-                Mi[w][2] += wb1 * s3i;
-                Mr[w][3] += wb2 * s3r;
-                Mi[w][3] += wb2 * s3i;
-                Mr[w][4] += wbn * h0r;
-                Mi[w][4] += wbn * h0i;
-                Mr[w][5] += wbn * h1r;
-                Mi[w][5] += wbn * h1i;
-                Mr[w][6] += wbn * h2r;
-                Mi[w][6] += wbn * h2i;
-                Mr[w][7] += wb1 * g0r;
-                Mi[w][7] += wb1 * g0i;
-                Mr[w][8] += wb2 * g0r;
-                Mi[w][8] += wb2 * g0i;
-                Mr[w][9] += wb * g1r;
-                Mi[w][9] += wb * g1i;
-                Mr[w][10] += wb1 * g1r;
-                Mi[w][10] += wb1 * g1i;
-                Mr[w][11] += wb2 * g1r;
-                Mi[w][11] += wb2 * g1i;
-                Mr[w][12] += wb * g2r;
-                Mi[w][12] += wb * g2i;
-                Mr[w][13] += wb1 * g2r;
-                Mi[w][13] += wb1 * g2i;
-                Mr[w][14] += wb2 * g2r;
-                Mi[w][14] += wb2 * g2i;
+                acc(w, 0, wb * g0r, wb * g0i);
+                acc(w, 1, wb * s3r, wb * s3i);
+                acc(w, 2, wb1 * s3r, wb1 * s3i);
+                acc(w, 3, wb2 * s3r, wb2 * s3i);
+                acc(w, 4, wbn * h0r, wbn * h0i);
+                acc(w, 5, wbn * h1r, wbn * h1i);
+                acc(w, 6, wbn * h2r, wbn * h2i);
+                acc(w, 7, wb1 * g0r, wb1 * g0i);
+                acc(w, 8, wb2 * g0r, wb2 * g0i);
+                acc(w, 9, wb * g1r, wb * g1i);
+                acc(w, 10, wb1 * g1r, wb1 * g1i);
+                acc(w, 11, wb2 * g1r, wb2 * g1i);
+                acc(w, 12, wb * g2r, wb * g2i);
+                acc(w, 13, wb1 * g2r, wb1 * g2i);
+                acc(w, 14, wb2 * g2r, wb2 * g2i);
             }
         }
 #pragma unroll
-        for (int w = 0; w < 2; ++w)
+        for (int w = 0; w < 2; ++w) {
+            if constexpr (SM) {
+#pragma unroll
+                for (int m = 0; m < 15; ++m) {
+                    Mr[w][m] = mom[((w * 15 + m) * 2) * FAR_THREADS];
+                    Mi[w][m] = mom[((w * 15 + m) * 2 + 1) * FAR_THREADS];
+                }
+            }
             calderon_epilogue<true>(a, w, li, lj, gi, gj, ni64, nj64, pf, Rd, Mr[w], Mi[w], true);
+        }
     }
 }
 
-template <int PH>
+template <int PH, bool SM>
 int launch_calderon_k2(bem_ctx* ctx, const CalArgs& a, cudaStream_t s) {
     dim3 grid((a.n + FAR_THREADS - 1) / FAR_THREADS, (a.n + FAR_TI - 1) / FAR_TI);
     if (grid.y > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "calderon: too many panels for one launch");
-    const size_t smem = FAR_TI * a.Q2 * sizeof(float4) + a.Q2 * sizeof(float4);
-    far_calderon_k2_kernel<PH><<<grid, FAR_THREADS, smem, s>>>(a);
+    const size_t smem = FAR_TI * a.Q2 * sizeof(float4) + a.Q2 * sizeof(float4) +
+                        (SM ? 60 * FAR_THREADS * sizeof(double) : 0);
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(far_calderon_k2_kernel<PH, SM>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                "far_calderon_k2_kernel smem"))
+        return rc;
+    far_calderon_k2_kernel<PH, SM><<<grid, FAR_THREADS, smem, s>>>(a);
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "far_calderon_k2_kernel launch");
 }
@@ -899,9 +916,15 @@ extern "C" int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk
     int rc = BEM_OK;
     const int variant = ctx->tune[BEM_TUNE_CALDERON_GROUP];
     if (fp32 && helm && nk == 2 && variant == 4) {
-        // both wavenumbers packed into the FP32x2 lanes, one launch
-        rc = phase_class == 2 ? launch_calderon_k2<2>(ctx, a, s)
-                              : (phase_class == 1 ? launch_calderon_k2<1>(ctx, a, s) : launch_calderon_k2<0>(ctx, a, s));
+        // both wavenumbers packed into the FP32x2 lanes, one launch, moments in registers
+        rc = phase_class == 2 ? launch_calderon_k2<2, false>(ctx, a, s)
+                              : (phase_class == 1 ? launch_calderon_k2<1, false>(ctx, a, s)
+                                                  : launch_calderon_k2<0, false>(ctx, a, s));
+    } else if (fp32 && helm && nk == 2 && variant == 5) {
+        // the same with the moments in shared memory (three CTAs per SM)
+        rc = phase_class == 2 ? launch_calderon_k2<2, true>(ctx, a, s)
+                              : (phase_class == 1 ? launch_calderon_k2<1, true>(ctx, a, s)
+                                                  : launch_calderon_k2<0, true>(ctx, a, s));
     } else if (fp32 && helm && (variant == 3 || (variant == 0 && nk == 1))) {
         // packed FP32x2, one wavenumber per launch
         for (int w = 0; w < nk && !rc; ++w) {

@@ -92,7 +92,7 @@ def test_laplace_full_and_grouped_wavenumbers():
     core.kill()
     for prec in ("fp64", "mixed"):
         outs = []
-        for group in ((1, 2) if prec == "fp64" else (1, 2, 3, 4)):
+        for group in ((1, 2) if prec == "fp64" else (1, 2, 3, 4, 5)):
             core, b, *_ = _problem(2, prec)
             b.engine.set_tuning(L.TUNE_CALDERON_GROUP, group)
             b.assemble_system()
