@@ -368,10 +368,12 @@ def profile_lu(n: int):
     eng.close()
 
 
-def sweep_bench(n_k: int):
+def sweep_bench(n_k: int, k_batch: int = 4):
     """The wavenumber sweep (managers/sweep.py) of the augmented
     transmission operator over n_k wavenumbers, mixed precision against the
-    plain FP64 path, both with the same FP64 block-Krylov norm estimator;
+    plain FP64 path, both with the same FP64 block-Krylov norm estimator
+    (CGS2 column appends replayed from a CUDA graph) and the same k-batched
+    assembly (k_batch wavenumbers per group);
     one JSON line with per-k times, phases, errors and the norm estimates.
     Each arm first lets the autotuner choose its Cholesky panel width
     (cached per device and problem) and runs one untimed k."""
@@ -389,7 +391,7 @@ def sweep_bench(n_k: int):
         bm = core._BEM_manager
         bm._k = ks[0]
         tuned[prec] = bm.autotune(Autotuner(bm.engine))
-        kw = dict(nrhs=4, seed=0, norm_tol=1e-6, norm_maxit=32, norm_method="iterative")
+        kw = dict(nrhs=4, seed=0, norm_tol=1e-6, norm_maxit=32, norm_method="iterative", k_batch=k_batch)
         wavenumber_sweep(bm, ks[:1], **kw)  # warm-up
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -424,6 +426,9 @@ def sweep_bench(n_k: int):
                           "per RHS"},
         "autotuned": tuned,
         "norm_krylov_blocks": res["mixed"]["iterations"],
+        "k_batch": k_batch,
+        "assembly": "per group of k_batch wavenumbers k: V, K (with -K^T) and W each by one bem_assemble_batch call "
+                    "over the 2 k_batch media wavenumbers (one far launch per pair of wavenumbers, geometry shared)",
         "gpu_launches": {"mixed": res["mixed"]["launches"], "fp64": res["fp64"]["launches"]},
     }))
 
@@ -990,11 +995,13 @@ def main():
     ap.add_argument("--trans-solver", default="lstsq", choices=["square", "lstsq"],
                     help="solver of the transmission_dk workload")
     ap.add_argument("--sweep-k", type=int, default=60, help="number of wavenumbers of the sweep workload")
+    ap.add_argument("--k-batch", type=int, default=4,
+                    help="wavenumbers assembled together by the sweep workload (1: one k at a time)")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.workload == "sweep":
         if rank == 0:
-            sweep_bench(args.sweep_k)
+            sweep_bench(args.sweep_k, args.k_batch)
         return
     if args.workload == "shape":
         if rank == 0:

@@ -114,11 +114,20 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  *   BEM_TUNE_CHOL_NB         panel width of bem_chol_factor (a multiple of 64)
  *   BEM_TUNE_GRAM_BAND       tile columns per band of the normal-matrix tile
  *                            order (tiles running together share the L2's
- *                            operand panels); 1 gives row order */
+ *                            operand panels); 1 gives row order
+ *   BEM_TUNE_KBATCH_GROUP    wavenumbers per far-field launch of
+ *                            bem_assemble_batch: 2 or 4 (default 4 in mixed
+ *                            precision, 2 in FP64; P1 x P1 blocks always 2)
+ *   BEM_TUNE_GRAM_PAIR       form of the tensor-core normal matrix and
+ *                            Cholesky updates: 1 one CTA per 128 x 128 tile,
+ *                            2 CTA pairs (tcgen05 cta_group::2) on 256 x 128
+ *                            tiles, column order */
 #define BEM_TUNE_CALDERON_GROUP 0
 #define BEM_TUNE_GRAM_KSEG 1
 #define BEM_TUNE_CHOL_NB 2
 #define BEM_TUNE_GRAM_BAND 3
+#define BEM_TUNE_KBATCH_GROUP 4
+#define BEM_TUNE_GRAM_PAIR 5
 #define BEM_TUNE_KEYS 8
 int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value);
 
@@ -190,6 +199,26 @@ int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, con
 int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk, const double* k, const double* k2,
                           const bem_space* neu, const bem_space* dir, void* const* out, const double* coef,
                           int64_t ld, void* stream);
+
+/* Batched dense assembly over wavenumbers: for w < nk,
+ *   out[w][row*ld+col] += scale[w] * A(k[w])(row,col)   and, when out_t and
+ *   out_t[w] are not NULL, out_t[w][col*ld+row] += scale_t[w] * A(k[w])(row,col),
+ * A(k) the Helmholtz operator op->op with kernel wavenumber k[w] and W mass
+ * coefficient k2[w] (op->k and op->k2 are ignored).  k, k2, scale, scale_t,
+ * out and out_t are host arrays of nk entries; out/out_t hold device
+ * pointers to BEM_C128 blocks.  Every separate panel pair's geometry is
+ * evaluated once for 2 or 4 wavenumbers (BEM_TUNE_KBATCH_GROUP); near pairs
+ * take the FP64 Sauter-Schwab kernel per wavenumber.  Replaces the per-k
+ * operator forward passes of the reference's wavenumber sweep
+ * (demo/demo_3d_plot_Sio.py:63-82 -> get_mat_A1_inv_norm /
+ * get_augment_mat_A1_inv_norm, BEM_manager.py:922-988 ->
+ * matrix_layer_forward, BEM_manager.py:829-844, at the exterior and the
+ * interior wavenumber).  3D Helmholtz only; 1 <= nk <= BEM_MAX_KBATCH; queued
+ * without synchronising. */
+#define BEM_MAX_KBATCH 64
+int bem_assemble_batch(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                       int nk, const double* k, const double* k2, void* const* out, int64_t ld,
+                       const double* scale, void* const* out_t, const double* scale_t, void* stream);
 
 /* Matrix-free apply: y[row] += scale * sum_col A(row,col) * x[col]
  * (x conjugated when conj_x != 0, the reference's cmul(integrand, cconj(g))).

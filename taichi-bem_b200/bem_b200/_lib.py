@@ -37,12 +37,16 @@ EXPORTS = [
     "bem_adjoint_vertices", "bem_mesh_set_2d", "bem_gmres_ir", "bem_compute_color", "bem_set_mesh_instances",
     "bem_lu_factor_status", "bem_binary_version", "bem_ctx_set_tuning", "bem_assemble_calderon", "bem_gram",
     "bem_lstsq_refine", "bem_chol_factor", "bem_gemm", "bem_chol_inverse", "bem_normal_refine", "bem_near_pair_list",
+    "bem_assemble_batch",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 TUNE_CALDERON_GROUP = 0  # BEM_TUNE_CALDERON_GROUP
 TUNE_GRAM_KSEG = 1  # BEM_TUNE_GRAM_KSEG
 TUNE_CHOL_NB = 2  # BEM_TUNE_CHOL_NB
 TUNE_GRAM_BAND = 3  # BEM_TUNE_GRAM_BAND
+TUNE_KBATCH_GROUP = 4  # BEM_TUNE_KBATCH_GROUP
+TUNE_GRAM_PAIR = 5  # BEM_TUNE_GRAM_PAIR
+MAX_KBATCH = 64  # BEM_MAX_KBATCH
 
 
 class BemError(RuntimeError):
@@ -119,6 +123,9 @@ def load():
     L.bem_assemble_calderon.argtypes = [vp, ctypes.POINTER(OpDesc), i32, ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Space), ctypes.POINTER(Space),
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_double), i64, vp]
+    pd, pp = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_void_p)
+    L.bem_assemble_batch.argtypes = [vp, ctypes.POINTER(OpDesc), ctypes.POINTER(Space), ctypes.POINTER(Space), i32,
+                                     pd, pd, pp, i64, pd, pp, pd, vp]
     L.bem_measure_peaks.argtypes = [vp, ctypes.POINTER(ctypes.c_double), vp]
     L.bem_compute_color.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp]
     L.bem_set_mesh_instances.argtypes = [vp, vp, vp, vp, vp]

@@ -225,6 +225,37 @@ class Engine:
         self._check(self.lib.bem_assemble_calderon(self.ctx, ctypes.byref(desc), nk, kk, k2, ctypes.byref(ns),
                                                    ctypes.byref(ds), po, cf, o0.stride(0), _stream_ptr()))
 
+    def assemble_batch(self, desc: L.OpDesc, test: DeviceSpace, trial: DeviceSpace, ks, k2s, outs, scales,
+                       outs_t=None, scales_t=None):
+        """outs[w][row, col] += scales[w] * A(ks[w])(row, col) (and, where
+        outs_t[w] is given, outs_t[w][col, row] += scales_t[w] * A(ks[w])) for
+        the Helmholtz operator desc.op at every wavenumber of ks, W's mass
+        coefficient k2s[w] (bem_assemble_batch: each separate pair's geometry
+        evaluated once for 2 or 4 wavenumbers)."""
+        nk = len(ks)
+        assert 1 <= nk <= L.MAX_KBATCH and len(k2s) == nk == len(outs) == len(scales)
+        o0 = outs[0]
+        for o in outs:
+            assert o.is_cuda and o.dim() == 2 and o.stride(1) == 1 and o.dtype == o0.dtype == torch.complex128
+            assert o.stride(0) == o0.stride(0)
+            self._check_spaces(test, trial, o.shape[0], o.shape[1])
+        dbl = ctypes.c_double * nk
+        po = (ctypes.c_void_p * nk)(*[o.data_ptr() for o in outs])
+        pt, st = None, None
+        if outs_t is not None:
+            assert len(outs_t) == nk and scales_t is not None and len(scales_t) == nk
+            for o in outs_t:
+                if o is not None:
+                    assert o.dtype == o0.dtype and o.stride(0) == o0.stride(0) and o.stride(1) == 1
+                    self._check_spaces(trial, test, o.shape[0], o.shape[1])
+            pt = (ctypes.c_void_p * nk)(*[None if o is None else o.data_ptr() for o in outs_t])
+            st = dbl(*[float(v) for v in scales_t])
+        ts, rs = test.c(), trial.c()
+        self._check(self.lib.bem_assemble_batch(self.ctx, ctypes.byref(desc), ctypes.byref(ts), ctypes.byref(rs), nk,
+                                                dbl(*[float(v) for v in ks]), dbl(*[float(v) for v in k2s]), po,
+                                                o0.stride(0), dbl(*[float(v) for v in scales]), pt, st,
+                                                _stream_ptr()))
+
     def gram(self, A: torch.Tensor, P: torch.Tensor, out: torch.Tensor, colscale: torch.Tensor, tensor_cores=True):
         """out = D (A^H A + P^H P) D (full Hermitian, complex64/128 or
         float32/64), colscale = D (bem_gram): FP16-split tcgen05 products with

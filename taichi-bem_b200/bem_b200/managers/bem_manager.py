@@ -895,10 +895,12 @@ class BEMManager:
         shared memory), 3: packed FP32x2 per
         wavenumber, 1: scalar per wavenumber; the packed forms in mixed
         precision only),
-        timed on assemble_system, and for the least-squares solver the band
-        width of the normal matrix's tile order (1, 12, 8, 16), timed on the
-        normal matrix, and the Cholesky panel width (512, 1024, 2048), timed
-        on its factorisation.  Cached choices are applied without
+        timed on assemble_system, and for the least-squares solver the form
+        of the tensor-core normal matrix (2: CTA pairs on 256 x 128 tiles, 1:
+        one CTA per 128 x 128 tile; mixed precision), the band width of the
+        normal matrix's tile order (1, 12, 8, 16), timed on the normal matrix,
+        and the Cholesky panel width (512, 1024, 2048), timed on its
+        factorisation.  Cached choices are applied without
         timing.  Returns {key name: value}."""
         from ..tuning import Autotuner
         tuner = tuner or Autotuner(self.engine)
@@ -910,17 +912,27 @@ class BEMManager:
             out["calderon_group"] = tuner.tune(wl + "/calderon", L.TUNE_CALDERON_GROUP, groups,
                                                self.assemble_system)
         nbs = [512, 1024, 2048]
+        mixed = self.solve_precision == "mixed"
+        pairs = [2, 1] if mixed else [1]
         if (self._is_transmission and self.solver == "lstsq" and tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs)
-                and tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16])):
+                and tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16])
+                and (not mixed or tuner.cached(wl + "/gram_pair", L.TUNE_GRAM_PAIR, pairs))):
+            if mixed:
+                out["gram_pair"] = tuner.cached(wl + "/gram_pair", L.TUNE_GRAM_PAIR, pairs)
             out["chol_nb"] = tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs)
             out["gram_band"] = tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16])
         elif self._is_transmission and self.solver == "lstsq":
-            mixed = self.solve_precision == "mixed"
             self.assemble_system()
             A, P = self.transmission_blocks()
             Nm = torch.empty(n, n, dtype=A.dtype, device=A.device)
             d = torch.empty(n, dtype=torch.float64, device=A.device)
-            out["gram_band"] = tuner.tune(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16],
+            if mixed:
+                # the CTA-pair form (256 x 128 tiles, column order) against the
+                # one-CTA form; the band width below only shapes the latter
+                out["gram_pair"] = tuner.tune(wl + "/gram_pair", L.TUNE_GRAM_PAIR, pairs,
+                                              lambda: self.engine.gram(A, P, Nm, d, tensor_cores=True))
+            bands = [1] if out.get("gram_pair") == 2 else [1, 12, 8, 16]
+            out["gram_band"] = tuner.tune(wl + "/gram", L.TUNE_GRAM_BAND, bands,
                                           lambda: self.engine.gram(A, P, Nm, d, tensor_cores=mixed))
             W = torch.empty_like(Nm)
 

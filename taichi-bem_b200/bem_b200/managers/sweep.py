@@ -31,23 +31,35 @@ class Basis:
     grown column by column by CGS2 on bem_gemm products:
         h = Q^H v,  v -= Q h   (twice),   r_jj = ||v||,  q_j = v / r_jj,
     so that appended columns W satisfy W = Q R with R upper triangular, kept
-    on the device as its transpose Rt (Rt[c, i] = R[i, c]).  Norms and R stay
-    on the device, so appending synchronises nothing.  A column numerically
-    inside span(Q) (frequent in inverse and power iteration) leaves a tiny
-    r_jj, which R keeps, and a residual of rounding noise with components
-    along Q; the normalised q_j is therefore projected twice more and
-    normalised again (these last coefficients, of the order of r_jj, do not
-    enter R), which makes it orthogonal to Q whether or not the column was
-    dependent.  An exactly dependent column leaves r_jj = 0."""
+    on the device as its transpose Rt (Rt[c, i] = R[i, c]).  A column
+    numerically inside span(Q) (frequent in inverse and power iteration)
+    leaves a tiny r_jj, which R keeps, and a residual of rounding noise with
+    components along Q; the normalised q_j is therefore projected twice more
+    and normalised again (these last coefficients, of the order of r_jj, do
+    not enter R), which makes it orthogonal to Q whether or not the column was
+    dependent.  An exactly dependent column leaves r_jj = 0.
 
-    def __init__(self, engine, n, cap, dtype, device):
+    One append is a fixed sequence of about thirty small launches whose
+    shapes do not depend on j: the products run over all `cap` columns of Q,
+    whose columns j.. are still zero (so h_i = 0 for i >= j exactly), and the
+    column index lives on the device.  The sequence is captured once as a
+    CUDA graph (after one eager append, which sizes every buffer) and
+    replayed per column, so a column costs one graph launch instead of thirty
+    host-issued ones."""
+
+    def __init__(self, engine, n, cap, dtype, device, graph: bool = True):
         self.engine = engine
         self.Q = torch.zeros(n, cap, dtype=dtype, device=device)
         self.Rt = torch.zeros(cap, cap, dtype=dtype, device=device)
         self.j = 0
         self.cap = cap
-        self._h = torch.zeros(cap, dtype=dtype, device=device)
+        self._h = torch.zeros(cap, 1, dtype=dtype, device=device)
+        self._r = torch.zeros(cap, 1, dtype=dtype, device=device)
         self._nrm = torch.zeros(1, 1, dtype=dtype, device=device)
+        self._v = torch.zeros(n, 1, dtype=dtype, device=device)  # the graph's input column
+        self._jdev = torch.zeros(1, dtype=torch.long, device=device)
+        self._use_graph = graph and torch.device(device).type == "cuda"
+        self._graph = None
 
     @property
     def active(self) -> torch.Tensor:
@@ -59,6 +71,30 @@ class Basis:
         self.engine.gemm(v, v, self._nrm, conj_a=True)
         return (self._nrm.real if self._nrm.is_complex() else self._nrm).reshape(()).clamp_min(0.0).sqrt()
 
+    def _project(self, v):
+        """h = Q^H v, v -= Q h over all cap columns; returns h (a buffer)."""
+        h = self._h
+        h.zero_()
+        self.engine.gemm(self.Q, v, h, conj_a=True)
+        self.engine.gemm(self.Q, h, v, alpha=-1.0)
+        return h
+
+    def _append_fixed(self):
+        """Append the column in self._v at the device-side index j."""
+        v, r = self._v, self._r
+        r.zero_()
+        for _ in range(2):
+            r.add_(self._project(v))
+        rjj = self._norm(v)
+        q = v / rjj.clamp_min(1e-300).to(v.dtype)
+        for _ in range(2):
+            self._project(q)
+        q = q / self._norm(q).clamp_min(1e-300).to(q.dtype)
+        r.index_copy_(0, self._jdev, rjj.to(r.dtype).view(1, 1))
+        self.Rt.index_copy_(0, self._jdev, r.view(1, self.cap))
+        self.Q.index_copy_(1, self._jdev, q)
+        self._jdev.add_(1)
+
     def append(self, W: torch.Tensor) -> int:
         """Append the columns of W (n x p); returns the number appended (the
         basis stops at `cap`)."""
@@ -66,27 +102,25 @@ class Basis:
         for c in range(W.shape[1]):
             if self.j >= self.cap:
                 break
-            col, j = self.j, self.j
-            v = W[:, c:c + 1].contiguous()
-            if j > 0:
-                r = self.Rt[col, :j].view(j, 1)
-                h = self._h[:j].view(j, 1)
-                for _ in range(2):
-                    h.zero_()
-                    self.engine.gemm(self.active, v, h, conj_a=True)
-                    self.engine.gemm(self.active, h, v, alpha=-1.0)
-                    r.add_(h)
-            rjj = self._norm(v)
-            self.Rt[col, col] = rjj.to(self.Rt.dtype)
-            q = v / rjj.clamp_min(1e-300).to(v.dtype)
-            if j > 0:
-                h = self._h[:j].view(j, 1)
-                for _ in range(2):
-                    h.zero_()
-                    self.engine.gemm(self.active, q, h, conj_a=True)
-                    self.engine.gemm(self.active, h, q, alpha=-1.0)
-                q = q / self._norm(q).clamp_min(1e-300).to(q.dtype)
-            self.Q[:, col:col + 1] = q
+            self._v.copy_(W[:, c:c + 1])
+            if self._graph is not None:
+                self._graph.replay()
+            elif self._use_graph:
+                # the first append runs eagerly on a side stream (torch's
+                # capture recipe), then the same sequence is captured
+                side = torch.cuda.Stream(device=self.Q.device)
+                side.wait_stream(torch.cuda.current_stream(self.Q.device))
+                with torch.cuda.stream(side):
+                    self._append_fixed()
+                torch.cuda.current_stream(self.Q.device).wait_stream(side)
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self._append_fixed()
+                self._graph = g
+                # capture recorded the sequence without running it: the
+                # device index still points at the next column
+            else:
+                self._append_fixed()
             self.j += 1
             added += 1
         return added
@@ -244,8 +278,68 @@ def transmission_operator(bm, k: float, A_type: int = 1, augmented: bool = True)
     return At
 
 
+def transmission_operators(bm, ks, A_type: int = 1):
+    """[A(k); P^+_i(k)] (2n x n, new tensors) for every k of `ks`, equal to
+    transmission_operator(bm, k, A_type, augmented=True) up to the order of
+    the floating-point sums, with the operators of all wavenumbers assembled
+    together: per operator (V, K with its -K^T block, W) ONE bem_assemble_batch
+    call over the 2 len(ks) wavenumbers k sqrt(n_o) (into A) and k sqrt(n_i)
+    (into P), each separate panel pair's geometry evaluated once per launch.
+    With M(m) the block operator matA_add_M(m) places (BEM_manager.py:608-628),
+    linear in m:
+        P = M_int(+1) + 1/2 Id,   A = M_ext(-1) + m_A M_int(+1) + (1 + m_A)/2 Id,
+    m_A = -1 for A_I (A_type 1) and +1 for A_II (A_type 2), which is what the
+    reference's get_augment_mat_A{1,2}_inv_norm sequence (ADD_P_MINUS(1) at
+    the exterior wavenumber, ADD_P_PLUS(m_A) at the interior one, then
+    ADD_P_PLUS(1) for the appended block; BEM_manager.py:922-988) builds."""
+    from ..BEM_functions.layers import _D, _N
+    from .. import _lib as L
+    n = bm.N_Neumann + bm.M_Dirichlet
+    N, M = bm.N_Neumann, bm.M_Dirichlet
+    No, Do = bm._Neumann_offset_i, bm._Dirichlet_offset_i
+    m_A = -1.0 if A_type == 1 else 1.0
+    Qn, Qd = bm.shape_func_degree_Neumann, bm.shape_func_degree_Dirichlet
+    outs = []
+    for _ in ks:
+        outs.append(torch.zeros(2 * n, n, dtype=torch.complex128, device=bm.device))
+    A = [o[:n] for o in outs]
+    P = [o[n:] for o in outs]
+    # wavenumber list: (exterior of k_0, interior of k_0, exterior of k_1, ...)
+    wk, wk2, tgt, sgn = [], [], [], []
+    for i, k in enumerate(ks):
+        for sqrt_n, X, m in ((bm._sqrt_no, A[i], -1.0), (bm._sqrt_ni, P[i], 1.0)):
+            d = bm.op_desc(L.OP_V, float(k), sqrt_n)
+            wk.append(d.k)
+            wk2.append(d.k2)
+            tgt.append(X)
+            sgn.append(m)
+    desc = lambda op: bm.op_desc(op, float(ks[0]), bm._sqrt_no)  # kernel, precision, quirk
+    if N > 0:
+        sp = bm.space("charge", Qn, "N", _N, offset=No)
+        bm.engine.assemble_batch(desc(L.OP_V), sp, sp, wk, wk2, tgt, [-m for m in sgn])
+    if N > 0 and M > 0:
+        test = bm.space("charge", Qn, "N", _N, offset=No)
+        trial = bm.space("charge", Qd, "D", _D, offset=Do)
+        bm.engine.assemble_batch(desc(L.OP_K), test, trial, wk, wk2, tgt, list(sgn), outs_t=tgt,
+                                 scales_t=[-m for m in sgn])
+    if M > 0:
+        sp = bm.space("charge", Qd, "D", _D, offset=Do)
+        bm.engine.assemble_batch(desc(L.OP_W), sp, sp, wk, wk2, tgt, [-m for m in sgn])
+    if bm._is_transmission:
+        test = bm.space("charge", Qn, "N", _N, offset=No)
+        trial = bm.space("charge", Qd, "D", _D, offset=Do)
+    for i in range(len(ks)):
+        A[i].add_(P[i], alpha=m_A)
+        if bm._is_transmission:
+            bm.engine.mass(test, trial, out=P[i], scale=0.5, out_t=P[i], scale_t=0.5)
+            if m_A != -1.0:
+                bm.engine.mass(test, trial, out=A[i], scale=0.5 * (1.0 + m_A), out_t=A[i], scale_t=0.5 * (1.0 + m_A))
+    return outs
+
+
 def wavenumber_sweep(bm, ks, nrhs: int = 4, seed: int = 0, A_type: int = 1, scaling_k: float = 0.0,
-                     norm_method: str = "iterative", norm_tol: float | None = None, norm_maxit: int | None = None):
+                     norm_method: str = "iterative", norm_tol: float | None = None, norm_maxit: int | None = None,
+                     k_batch: int = 4):
     """For each k in `ks`: the augmented transmission operator [A(k); P^+_i(k)]
     (get_augment_mat_A{1,2}_inv_norm, BEM_manager.py:952-988), the inverse
     norm and condition number of its energy-scaled form, and the
@@ -254,9 +348,13 @@ def wavenumber_sweep(bm, ks, nrhs: int = 4, seed: int = 0, A_type: int = 1, scal
     solver (normal matrix, Cholesky, flexible GMRES in FP64; tensor cores in
     mixed precision, DMMA on the plain path), one factorisation per k.
 
-    The energy scaling is formed once, at `scaling_k` (the reference forms it
-    on its first call, which the reference's sweep makes at k = 0).  norm_tol
-    and norm_maxit override the manager's estimator settings for the sweep."""
+    The operators of `k_batch` consecutive wavenumbers are assembled together
+    (transmission_operators: one k-batched launch per operator and pair of
+    wavenumbers); k_batch <= 1 assembles each k on its own
+    (transmission_operator).  The energy scaling is formed once, at
+    `scaling_k` (the reference forms it on its first call, which the
+    reference's sweep makes at k = 0).  norm_tol and norm_maxit override the
+    manager's estimator settings for the sweep."""
     n = bm.N_Neumann + bm.M_Dirichlet
     if norm_tol is not None:
         bm.norm_tol = norm_tol
@@ -270,28 +368,36 @@ def wavenumber_sweep(bm, ks, nrhs: int = 4, seed: int = 0, A_type: int = 1, scal
     gen = torch.Generator(device=bm.device).manual_seed(seed)
     out = {"k": [], "inv_norm": [], "cond": [], "solutions": [], "rhs": [], "ms": [], "iterations": [],
            "phase_ms": []}
-    for k in ks:
+    ks = [float(k) for k in ks]
+    step = max(1, int(k_batch))
+    for g0 in range(0, len(ks), step):
+        group = ks[g0:g0 + step]
         torch.cuda.synchronize(bm.device)
-        t0 = time.perf_counter()
-        At = transmission_operator(bm, float(k), A_type, augmented=True)
+        ta = time.perf_counter()
+        if step > 1:
+            ops = transmission_operators(bm, group, A_type)
+        else:
+            ops = [transmission_operator(bm, group[0], A_type, augmented=True)]
         torch.cuda.synchronize(bm.device)
-        t1 = time.perf_counter()
-        inv_norm, cond, its = bm.compute_inv_norm(At, A_type, method=norm_method, return_cond=True)
-        torch.cuda.synchronize(bm.device)
-        t2 = time.perf_counter()
-        B = torch.zeros(2 * n, nrhs, dtype=torch.complex128, device=bm.device)
-        B[:n] = torch.complex(torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen),
-                              torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen))
-        X = bm.lstsq_multi(At[:n], At[n:], B)
-        torch.cuda.synchronize(bm.device)
-        t3 = time.perf_counter()
-        out["ms"].append((t3 - t0) * 1e3)
-        out["phase_ms"].append({"assemble": (t1 - t0) * 1e3, "norm": (t2 - t1) * 1e3, "lstsq": (t3 - t2) * 1e3})
-        out["k"].append(float(k))
-        out["inv_norm"].append(inv_norm)
-        out["cond"].append(cond)
-        out["iterations"].append(its)
-        out["solutions"].append(X)
-        out["rhs"].append(B[:n])
-        del At
+        t_asm = (time.perf_counter() - ta) * 1e3 / len(group)
+        for k, At in zip(group, ops):
+            t1 = time.perf_counter()
+            inv_norm, cond, its = bm.compute_inv_norm(At, A_type, method=norm_method, return_cond=True)
+            torch.cuda.synchronize(bm.device)
+            t2 = time.perf_counter()
+            B = torch.zeros(2 * n, nrhs, dtype=torch.complex128, device=bm.device)
+            B[:n] = torch.complex(torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen),
+                                  torch.randn(n, nrhs, dtype=torch.float64, device=bm.device, generator=gen))
+            X = bm.lstsq_multi(At[:n], At[n:], B)
+            torch.cuda.synchronize(bm.device)
+            t3 = time.perf_counter()
+            out["ms"].append(t_asm + (t3 - t1) * 1e3)
+            out["phase_ms"].append({"assemble": t_asm, "norm": (t2 - t1) * 1e3, "lstsq": (t3 - t2) * 1e3})
+            out["k"].append(k)
+            out["inv_norm"].append(inv_norm)
+            out["cond"].append(cond)
+            out["iterations"].append(its)
+            out["solutions"].append(X)
+            out["rhs"].append(B[:n])
+        del ops
     return out

@@ -10,7 +10,7 @@ $BEM_B200_TUNING_CACHE, else ~/.cache/bem_b200/tuning.json.
 
 Only keys that change the launch shape and not the result's accuracy are
 tuned this way (the Calderon sweep's form, the normal matrix's tile order,
-the Cholesky panel width); the
+the Cholesky panel width, the wavenumbers per k-batched launch); the
 normal matrix's accumulation segment (BEM_TUNE_GRAM_KSEG) trades accuracy
 for speed and keeps its built-in default.
 """
@@ -24,7 +24,8 @@ from . import _lib as L
 
 CACHE_ENV = "BEM_B200_TUNING_CACHE"
 KEY_NAMES = {L.TUNE_CALDERON_GROUP: "calderon_group", L.TUNE_GRAM_KSEG: "gram_kseg", L.TUNE_CHOL_NB: "chol_nb",
-             L.TUNE_GRAM_BAND: "gram_band"}
+             L.TUNE_GRAM_BAND: "gram_band", L.TUNE_KBATCH_GROUP: "kbatch_group",
+             L.TUNE_GRAM_PAIR: "gram_pair"}
 
 
 def cache_path() -> str:

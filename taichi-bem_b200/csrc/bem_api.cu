@@ -143,7 +143,11 @@ int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value) {
     if (!ctx) return BEM_ERR_INVALID;
     if (key < 0 || key >= BEM_TUNE_KEYS) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: unknown key");
     if (key == BEM_TUNE_CALDERON_GROUP && (value < 0 || value > 5))
-        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon form must be 1, 2 or 3");
+        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon form must be in 1..5");
+    if (key == BEM_TUNE_GRAM_PAIR && (value < 0 || value > 2))
+        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: normal-matrix form must be 1 or 2");
+    if (key == BEM_TUNE_KBATCH_GROUP && value != 0 && value != 2 && value != 4)
+        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: wavenumbers per batched launch must be 2 or 4");
     if (key == BEM_TUNE_GRAM_KSEG && value < 0) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: negative segment");
     if (key == BEM_TUNE_GRAM_BAND && (value < 0 || value > 4096))
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: band width must be in 0..4096");
@@ -392,6 +396,30 @@ int bem_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, con
                                      (cudaStream_t)stream);
     return bem_launch_assemble(ctx, op, test, trial, 0, out, ld, scale, out_t, scale_t, nullptr, nullptr, 0,
                                (cudaStream_t)stream);
+}
+
+int bem_assemble_batch(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                       int nk, const double* k, const double* k2, void* const* out, int64_t ld,
+                       const double* scale, void* const* out_t, const double* scale_t, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
+    if (int rc = check_op(ctx, op, false)) return rc;
+    if (ctx->dim != 3 || op->kernel != BEM_KERNEL_HELMHOLTZ)
+        return bem_fail(ctx, BEM_ERR_INVALID, "bem_assemble_batch takes the 3D Helmholtz kernel");
+    if (int rc = check_space(ctx, test, "test")) return rc;
+    if (int rc = check_space(ctx, trial, "trial")) return rc;
+    if (nk < 1 || nk > BEM_MAX_KBATCH) return bem_fail(ctx, BEM_ERR_INVALID, "nk must be in [1, BEM_MAX_KBATCH]");
+    if (!k || !k2 || !out || !scale || ld <= 0)
+        return bem_fail(ctx, BEM_ERR_INVALID, "k, k2, out or scale is NULL, or ld <= 0");
+    for (int w = 0; w < nk; ++w) {
+        if (!std::isfinite(k[w]) || !std::isfinite(k2[w]) || !std::isfinite(scale[w]))
+            return bem_fail(ctx, BEM_ERR_INVALID, "non-finite wavenumber or scale");
+        if (!out[w]) return bem_fail(ctx, BEM_ERR_INVALID, "out[w] is NULL");
+        if (out_t && out_t[w] && (!scale_t || !std::isfinite(scale_t[w])))
+            return bem_fail(ctx, BEM_ERR_INVALID, "out_t[w] given without a finite scale_t[w]");
+    }
+    return bem_launch_assemble_batch(ctx, op, test, trial, nk, k, k2, out, ld, scale, out_t, scale_t,
+                                     (cudaStream_t)stream);
 }
 
 int bem_apply(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial, int dtype,

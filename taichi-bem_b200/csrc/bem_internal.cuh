@@ -106,6 +106,11 @@ int bem_launch_assemble(bem_ctx* ctx, const bem_op_desc* op, const bem_space* te
 int bem_launch_assemble_parts(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
                               int mode, void* out, int64_t ld, double scale, void* out_t, double scale_t,
                               const void* x, void* y, int conj_x, cudaStream_t s, bool near_only);
+// One operator at nk Helmholtz wavenumbers (bem_kbatch.cu): far pairs in
+// k-batched launches, near pairs per wavenumber.
+int bem_launch_assemble_batch(bem_ctx* ctx, const bem_op_desc* op, const bem_space* test, const bem_space* trial,
+                              int nk, const double* k, const double* k2, void* const* out, int64_t ld,
+                              const double* scale, void* const* out_t, const double* scale_t, cudaStream_t s);
 // Class of the bound on the FP32 split phase |k (r - R)| <= k (rho_i + rho_j):
 // 2 when <= 0.3 (short polynomials), 1 when <= 0.78 < pi/4 (no reduction), 0 otherwise
 int bem_phase_class(double bound);

@@ -215,6 +215,9 @@ constexpr int GT_KSEG_DEFAULT = 2;
 // default segment on 7682 and 30722 unknowns (14.4 vs 16.6 ms, 1147 vs
 // 1183 ms); the autotuner chooses per problem.
 constexpr int GRAM_BAND_DEFAULT = 1;
+// form of the tensor-core Gram product (BEM_TUNE_GRAM_PAIR): 1 one CTA per
+// 128 x 128 tile (gram_tc_kernel), 2 CTA pairs on 256 x 128 tiles (gram_tc2_kernel)
+constexpr int GRAM_PAIR_DEFAULT = 1;
 constexpr int GT_EPI_WARPS = 8;
 constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
 constexpr uint32_t GT_TMEM_COLS = 512;  // 2 sets x (D1, D2) x 128 columns
@@ -502,6 +505,357 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
 }
 
 // ---------------------------------------------------------------------------
+// CTA-pair variant (tcgen05 cta_group::2, M = 256 over the two CTAs of a
+// cluster).  gram_tc_kernel floors where shared memory is busiest: per 64-wide
+// K stage its TMA writes 64 KB and its three MMAs read A (16 KB) and B
+// (16 KB) each, 160 KB against 813 clocks of tensor work at 128 B per clock.
+// Here the pair computes a 256 x 128 tile (rows: tile rows 2p and 2p + 1, one
+// per CTA; columns: tile column bj) with one MMA stream issued by the even
+// CTA: each CTA holds its own 128 A rows and HALF (64 rows) of the B panel,
+// and the hardware feeds both halves to both CTAs' MMAs, so per CTA and stage
+// the TMA writes 48 KB and the MMAs read 72 KB (120 KB for the same tensor
+// work).  Protocol (all waits bounded, as in gram_tc_kernel):
+//  * TMEM: 512 columns allocated by warp 1 of both CTAs (cta_group::2), two
+//    accumulator sets x (D1, D2) x 128 columns; each CTA's TMEM holds its own
+//    128 rows;
+//  * stage s: both producers load into their own shared memory with the
+//    cta_group::2 TMA form, completing bytes on the EVEN CTA's full_bar[s],
+//    where the even producer alone announces the pair's 96 KB; the even
+//    CTA's MMA thread waits on it, and its tcgen05.commit arrives on
+//    empty_bar[s] of both CTAs (multicast commit, mask 0b11);
+//  * accumulators: the commit after a segment arrives on acc_full of both
+//    CTAs; the eight epilogue warps of each CTA arrive on the EVEN CTA's
+//    acc_empty (count 16) after draining their TMEM;
+//  * teardown: a cluster barrier (neither CTA leaves while the other's MMAs
+//    may still read its shared memory), then both CTAs free the TMEM.
+// Tiles run in column order (the pairs of one tile column one after another,
+// the order of single-column bands, BEM_TUNE_GRAM_BAND = 1).  No load uses
+// cluster multicast; every tensor map covers this GPU's memory only.
+// ---------------------------------------------------------------------------
+constexpr int G2_STAGES = 4;
+constexpr int G2_ATILE = GT_BM * GT_BK * 2;            // 16 KB: 128 x 64 FP16 rows of this CTA
+constexpr int G2_BTILE = (GT_BM / 2) * GT_BK * 2;      // 8 KB: this CTA's 64-row half of the B panel
+constexpr int G2_STAGE = 2 * G2_ATILE + 2 * G2_BTILE;  // 48 KB per CTA and stage
+constexpr size_t G2_SMEM = (size_t)G2_STAGES * G2_STAGE + 1024;
+// kind::f16, D F32, M = 256 (the pair), N = 128
+constexpr uint32_t G2_IDESC = (1u << 4) | ((uint32_t)(GT_BM >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+
+// Pair tile t, column order over the lower triangle of a T x T grid of 128 x
+// 128 tiles: tile column bj holds row pairs p = floor(bj / 2) .. P - 1 (P =
+// ceil(T / 2)); columns 2c and 2c + 1 both hold P - c pairs.
+__device__ __forceinline__ void pair_tile(int t, int T, int& p, int& bj) {
+    const int P = (T + 1) >> 1;
+    for (int c = 0; c < P; ++c) {
+        const int cnt = P - c, ncol = min(2, T - 2 * c);
+        if (t < ncol * cnt) {
+            bj = 2 * c + t / cnt;
+            p = c + t % cnt;
+            return;
+        }
+        t -= ncol * cnt;
+    }
+    p = bj = 0;  // not reached for t < pair_tiles(T)
+}
+
+__host__ __device__ inline int64_t pair_tiles(int T) {
+    const int P = (T + 1) >> 1;
+    int64_t n = 0;
+    for (int c = 0; c < P; ++c) n += (int64_t)(T - 2 * c < 2 ? T - 2 * c : 2) * (P - c);
+    return n;
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_id_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_count_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t map_rank(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// try_wait with cluster-scope acquire: the barrier receives arrivals from the peer CTA
+__device__ __forceinline__ bool mbar_wait_cl(uint32_t addr, uint32_t parity, volatile int* abort) {
+    for (uint32_t it = 0; it < GT_SPIN_CAP; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 1023u) == 1023u && *abort) return false;
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_pair(uint32_t dst, const CUtensorMap* map, uint32_t mbar_leader, int x,
+                                              int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+        "%4}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(mbar_leader), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void mma_f16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(G2_IDESC), "r"(accumulate)
+        : "memory");
+}
+// tcgen05.commit of the pair's MMAs: one arrival on the barrier at this
+// shared address in both CTAs
+__device__ __forceinline__ void commit_pair(uint32_t bar) {
+    const uint16_t mask = 0x3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            bar),
+        "h"(mask)
+        : "memory");
+}
+
+template <bool C, typename OT>
+__global__ void __launch_bounds__(GT_THREADS, 1) gram_tc2_kernel(
+    const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+    const __grid_constant__ CUtensorMap tmb_hi, const __grid_constant__ CUtensorMap tmb_lo, int nchunks, int kseg,
+    int ntiles, int tgrid, OT* out, int64_t ldo, int n, double alpha, int accumulate, int32_t* err) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[G2_STAGES], empty_bar[G2_STAGES], acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int s_abort;
+    __shared__ double s_stage[GT_EPI_WARPS][8 * GT_STG_LD];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                           ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nseg = (nchunks + kseg - 1) / kseg;
+    const uint32_t rank = cluster_rank();
+    const int cid = (int)cluster_id_x(), ncl = (int)cluster_count_x();
+    const bool leader = rank == 0;
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(GT_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < G2_STAGES; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full_bar[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty_bar[s])) : "memory");
+        }
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&acc_full[b])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acc_empty[b])),
+                         "r"(2 * GT_EPI_WARPS)
+                         : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    // both CTAs' barriers are initialised before any TMA or arrival of the peer reaches them
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0) {
+        // ---- TMA producer (both CTAs) ----
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_hi)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_lo)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmb_hi)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmb_lo)) : "memory");
+            uint32_t cg = 0;
+            for (int t = cid; t < ntiles && !s_abort; t += ncl) {
+                int p, bj;
+                pair_tile(t, tgrid, p, bj);
+                const int arow = (2 * p + (int)rank) * GT_BM;        // this CTA's A rows
+                const int brow = bj * GT_BM + (int)rank * (GT_BM / 2);  // this CTA's half of the B panel
+                for (int c = 0; c < nchunks; ++c, ++cg) {
+                    const int s = (int)(cg % G2_STAGES);
+                    if (cg >= G2_STAGES &&
+                        !mbar_wait(smem_u32(&empty_bar[s]), (uint32_t)((cg / G2_STAGES - 1) & 1), &s_abort)) {
+                        s_abort = 1;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(&full_bar[s]);
+                    if (leader)
+                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                                     "r"(2 * G2_STAGE)
+                                     : "memory");
+                    const uint32_t fb0 = map_rank(fb, 0);
+                    const uint32_t st = smem_u32(smem + (size_t)s * G2_STAGE);
+                    const int x = c * GT_BK;
+                    tma_load_pair(st, &tm_hi, fb0, x, arow);
+                    tma_load_pair(st + G2_ATILE, &tm_lo, fb0, x, arow);
+                    tma_load_pair(st + 2 * G2_ATILE, &tmb_hi, fb0, x, brow);
+                    tma_load_pair(st + 2 * G2_ATILE + G2_BTILE, &tmb_lo, fb0, x, brow);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer (the even CTA) ----
+        if (lane == 0 && leader) {
+            uint32_t cg = 0, gg = 0;
+            for (int t = cid; t < ntiles && !s_abort; t += ncl) {
+                int c = 0;
+                for (int g = 0; g < nseg && !s_abort; ++g, ++gg) {
+                    const int buf = (int)(gg & 1);
+                    if (gg >= 2 &&
+                        !mbar_wait_cl(smem_u32(&acc_empty[buf]), (uint32_t)((gg / 2 - 1) & 1), &s_abort)) {
+                        s_abort = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t d1 = tmem + (uint32_t)(buf * 256), d2 = d1 + 128;
+                    const int cend = min(nchunks, (g + 1) * kseg);
+                    for (int first = 1; c < cend; ++c, ++cg, first = 0) {
+                        const int s = (int)(cg % G2_STAGES);
+                        if (!mbar_wait(smem_u32(&full_bar[s]), (uint32_t)((cg / G2_STAGES) & 1), &s_abort)) {
+                            s_abort = 1;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const uint32_t st = smem_u32(smem + (size_t)s * G2_STAGE);
+#pragma unroll
+                        for (int ks = 0; ks < GT_BK / 16; ++ks) {
+                            const uint32_t ko = 32u * ks;
+                            const uint64_t a_hi = desc_sw128(st + ko), a_lo = desc_sw128(st + G2_ATILE + ko);
+                            const uint64_t b_hi = desc_sw128(st + 2 * G2_ATILE + ko),
+                                           b_lo = desc_sw128(st + 2 * G2_ATILE + G2_BTILE + ko);
+                            const uint32_t acc = (first && ks == 0) ? 0u : 1u;
+                            mma_f16_pair(d1, a_hi, b_hi, acc);
+                            mma_f16_pair(d2, a_hi, b_lo, acc);
+                            mma_f16_pair(d2, a_lo, b_hi, 1u);
+                        }
+                        commit_pair(smem_u32(&empty_bar[s]));
+                    }
+                    if (s_abort) break;
+                    commit_pair(smem_u32(&acc_full[buf]));
+                }
+            }
+        }
+    } else {
+        // ---- epilogue (both CTAs): FP64 running sums of this CTA's 128 rows ----
+        constexpr int EC = GT_BM / 2;
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        uint32_t gg = 0;
+        bool ok = true;
+        for (int t = cid; t < ntiles && ok; t += ncl) {
+            int p, bj;
+            pair_tile(t, tgrid, p, bj);
+            const int bi = 2 * p + (int)rank;
+            double acc[EC];
+#pragma unroll
+            for (int i = 0; i < EC; ++i) acc[i] = 0.0;
+            for (int g = 0; g < nseg; ++g, ++gg) {
+                const int buf = (int)(gg & 1);
+                const bool got = mbar_wait(smem_u32(&acc_full[buf]), (uint32_t)((gg / 2) & 1), &s_abort);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    s_abort = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * 256 + half * EC);
+#pragma unroll
+                for (int cc = 0; cc < EC; cc += 8) {
+                    float v1[8], v2[8];
+                    tmem_ld8(base + cc, v1);
+                    tmem_ld8(base + 128 + cc, v2);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[cc + i] += (double)fmaf(v2[i], 4.8828125e-4f, v1[i]);
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0)
+                    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(
+                                     map_rank(smem_u32(&acc_empty[buf]), 0))
+                                 : "memory");
+            }
+            // the even CTA's half of the pair's diagonal column (bi < bj) lies above the diagonal
+            if (ok && bi >= bj) {
+                const int r = bi * GT_BM + 32 * q + lane;
+                const int c0 = bj * GT_BM + half * EC;
+                if (C) {
+                    double* stg = s_stage[warp - 2];
+                    const int pw0 = (bi * GT_BM + 32 * q) >> 1;
+                    const int qc = (c0 >> 1) + lane;
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4) {
+                        if ((lane >> 3) == c4) {
+#pragma unroll
+                            for (int m = 0; m < EC; ++m) stg[(lane & 7) * GT_STG_LD + m] = acc[m];
+                        }
+                        __syncwarp();
+                        double nre[4], nim[4], ore[4], oim[4];
+#pragma unroll
+                        for (int ri = 0; ri < 4; ++ri) {
+                            const double* e = stg + (2 * ri) * GT_STG_LD + 2 * lane;
+                            const double* o = stg + (2 * ri + 1) * GT_STG_LD + 2 * lane;
+                            const int pr = pw0 + 4 * c4 + ri;
+                            nre[ri] = e[0] + o[1];
+                            nim[ri] = pr == qc ? 0.0 : e[1] - o[0];
+                            ore[ri] = oim[ri] = 0.0;
+                            if (accumulate && pr < n && qc < n) {
+                                const OT* ot = out + 2 * ((int64_t)pr * ldo + qc);
+                                ore[ri] = (double)ot[0];
+                                oim[ri] = (double)ot[1];
+                            }
+                        }
+#pragma unroll
+                        for (int ri = 0; ri < 4; ++ri) {
+                            const int pr = pw0 + 4 * c4 + ri;
+                            if (pr < n && qc < n) {
+                                OT* ot = out + 2 * ((int64_t)pr * ldo + qc);
+                                ot[0] = (OT)(ore[ri] + alpha * nre[ri]);
+                                ot[1] = (OT)(oim[ri] + alpha * nim[ri]);
+                            }
+                        }
+                        __syncwarp();
+                    }
+                } else if (r < n) {
+                    OT* orow = out + (int64_t)r * ldo + c0;
+                    double old[EC];
+#pragma unroll
+                    for (int m = 0; m < EC; ++m) old[m] = (accumulate && c0 + m < n) ? (double)orow[m] : 0.0;
+#pragma unroll
+                    for (int m = 0; m < EC; ++m)
+                        if (c0 + m < n) orow[m] = (OT)(old[m] + alpha * acc[m]);
+                }
+            }
+        }
+    }
+    if (s_abort && tid == 0) atomicExch(err, BEM_ERR_TIMEOUT);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GT_TMEM_COLS) : "memory");
+}
+
+// ---------------------------------------------------------------------------
 // FP64 Gram kernel (plain path): DMMA m8n8k4 on 128 x 128 real tiles of
 // S = R^T R, R the real view of [A; P] (rows k), read directly; the column
 // scaling is applied in the epilogue.
@@ -780,7 +1134,8 @@ int gram_mixed(bem_ctx* ctx, const double* A, const double* P, int64_t ld, int n
                int64_t ldo, cudaStream_t s) {
     const int W = C ? 2 : 1;
     const int64_t rows = (int64_t)W * n;                    // rows of T
-    const int64_t Rp = (rows + GT_BM - 1) / GT_BM * GT_BM;  // padded rows
+    // padded rows: a whole number of 256-row CTA-pair tiles (the split writes the padding as zeros)
+    const int64_t Rp = (rows + 2 * GT_BM - 1) / (2 * GT_BM) * (2 * GT_BM);
     const int64_t Kp = (2 * (int64_t)n + GT_BK - 1) / GT_BK * GT_BK;
     if (Kp > (int64_t)1 << 31 || Rp / GT_BM > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "gram: n too large");
     void* ws = nullptr;
@@ -819,12 +1174,52 @@ int launch_gram_tc(bem_ctx* ctx, __half* Thi, __half* Tlo, int64_t Rp, int64_t K
     }
     const int tr = (int)(Rp / GT_BM);
     const int64_t tiles = (int64_t)tr * (tr + 1) / 2;
+    cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
+    const int kseg = ctx->tune[BEM_TUNE_GRAM_KSEG] > 0 ? ctx->tune[BEM_TUNE_GRAM_KSEG] : GT_KSEG_DEFAULT;
+    const int form = ctx->tune[BEM_TUNE_GRAM_PAIR] > 0 ? ctx->tune[BEM_TUNE_GRAM_PAIR] : GRAM_PAIR_DEFAULT;
+    if (form == 2 && ctx->num_sms >= 2) {
+        // CTA pairs: the B panel's tensor maps load 64-row halves
+        CUtensorMap tmb[2];
+        for (int h = 0; h < 2; ++h) {
+            cuuint64_t gdim[2] = {(cuuint64_t)Kp, (cuuint64_t)Rp};
+            cuuint64_t gstride[1] = {(cuuint64_t)Kp * sizeof(__half)};
+            cuuint32_t box[2] = {(cuuint32_t)GT_BK, (cuuint32_t)(GT_BM / 2)};
+            cuuint32_t estr[2] = {1, 1};
+            CUresult r = enc(&tmb[h], CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h ? (void*)Tlo : (void*)Thi, gdim, gstride,
+                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return bem_fail(ctx, BEM_ERR_CUDA, "gram: cuTensorMapEncodeTiled failed");
+        }
+        if (tr % 2) return bem_fail(ctx, BEM_ERR_INVALID, "gram: CTA pairs need an even number of tile rows");
+        const int64_t ptiles = pair_tiles(tr);
+        if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc2_kernel<C, OT>,
+                                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                              (int)G2_SMEM),
+                                    "gram_tc2_kernel smem"))
+            return rc;
+        const unsigned clusters = (unsigned)std::min<int64_t>(ptiles, ctx->num_sms / 2);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * clusters);
+        cfg.blockDim = dim3(GT_THREADS);
+        cfg.dynamicSmemBytes = G2_SMEM;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, gram_tc2_kernel<C, OT>, tm[0], tm[1], tmb[0], tmb[1],
+                                           (int)(Kp / GT_BK), kseg, (int)ptiles, tr, out, ldo, n, alpha, accumulate,
+                                           ctx->flags + 5);
+        ctx->launches++;
+        return bem_check_cuda(ctx, e, "gram_tc2_kernel");
+    }
     if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc_kernel<C, OT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                           (int)GT_SMEM),
                                 "gram_tc_kernel smem"))
         return rc;
-    cudaMemsetAsync(ctx->flags + 5, 0, sizeof(int32_t), s);
-    const int kseg = ctx->tune[BEM_TUNE_GRAM_KSEG] > 0 ? ctx->tune[BEM_TUNE_GRAM_KSEG] : GT_KSEG_DEFAULT;
     const int band = ctx->tune[BEM_TUNE_GRAM_BAND] > 0 ? ctx->tune[BEM_TUNE_GRAM_BAND] : GRAM_BAND_DEFAULT;
     // persistent: one CTA per SM (its shared memory and 512 TMEM columns allow no second), tiles in turn
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctx->num_sms);
@@ -867,7 +1262,7 @@ int bem_herk_tc_update(bem_ctx* ctx, bool C, const double* L, int64_t ld, int m,
                        cudaStream_t s) {
     if (m <= 0 || kb <= 0) return BEM_OK;
     const int W = C ? 2 : 1;
-    const int64_t Rp = ((int64_t)W * m + GT_BM - 1) / GT_BM * GT_BM;
+    const int64_t Rp = ((int64_t)W * m + 2 * GT_BM - 1) / (2 * GT_BM) * (2 * GT_BM);  // whole CTA-pair tiles
     const int64_t Kp = ((int64_t)kb + GT_BK - 1) / GT_BK * GT_BK;
     if (Rp / GT_BM > 65535) return bem_fail(ctx, BEM_ERR_INVALID, "herk update: m too large");
     void* ws = nullptr;

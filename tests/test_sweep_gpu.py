@@ -150,3 +150,37 @@ def test_krylov_estimates_with_a_complete_basis():
     core.kill()
     assert abs(smin - sv[-1]) <= 1e-6 * sv[-1], (smin, sv[-1])
     assert abs(smax - sv[0]) <= 1e-9 * sv[0], (smax, sv[0])
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.complex128])
+def test_basis_graph_replay_matches_eager(dtype):
+    """The CGS2 basis appended by CUDA-graph replays equals the eagerly
+    appended one, including numerically dependent columns; Q is orthonormal
+    and W = Q R."""
+    from bem_b200.engine import Engine
+    from bem_b200.managers.sweep import Basis
+    eng = Engine("cuda:0")
+    try:
+        n, cap = 300, 24
+        g = torch.Generator(device="cuda").manual_seed(3)
+        W = torch.randn(n, 16, dtype=torch.float64, device="cuda", generator=g)
+        if dtype.is_complex:
+            W = torch.complex(W, torch.randn(n, 16, dtype=torch.float64, device="cuda", generator=g))
+        W = torch.cat([W, W[:, :4] + 1e-13 * W[:, 4:8], W[:, 8:12] @ torch.ones(4, 4, dtype=dtype, device="cuda")],
+                      1)  # 24 columns, the last 8 nearly or exactly dependent
+        bases = []
+        for graph in (True, False):
+            b = Basis(eng, n, cap, dtype, "cuda", graph=graph)
+            assert b.append(W[:, :5]) == 5 and b.append(W[:, 5:]) == 19 and b.append(W[:, :1]) == 0
+            bases.append(b)
+        bg, be = bases
+        assert bg._graph is not None and be._graph is None
+        assert torch.allclose(bg.Q, be.Q, rtol=0, atol=1e-12)
+        assert torch.allclose(bg.Rt, be.Rt, rtol=0, atol=1e-12 * float(W.abs().max()) * n)
+        Q = bg.Q
+        eye = torch.eye(cap, dtype=dtype, device="cuda")
+        assert float((Q.conj().T @ Q - eye).abs().max()) < 1e-12
+        R = bg.Rt.T
+        assert float((Q[:, :16] @ R[:16, :16] - W[:, :16]).abs().max()) < 1e-12 * float(W.abs().max())
+    finally:
+        eng.close()
