@@ -220,6 +220,20 @@ int bem_assemble_batch(bem_ctx* ctx, const bem_op_desc* op, const bem_space* tes
                        int nk, const double* k, const double* k2, void* const* out, int64_t ld,
                        const double* scale, void* const* out_t, const double* scale_t, void* stream);
 
+/* One step of a growing orthonormal basis by classical Gram-Schmidt with
+ * one re-orthogonalisation (no reference counterpart: the reference takes
+ * full SVDs in compute_inv_norm, BEM_manager.py:874-920; this is the basis
+ * growth of this library's block-Krylov norm estimator).  Q is n x ldq
+ * (row-major, BEM_F64 or BEM_C128) whose first j columns are orthonormal; v
+ * (n entries, element stride ldv) is not modified.  Twice h = Q^H v,
+ * v' -= Q h, r += h; r_jj = ||v'||; q = v' / r_jj projected twice more and
+ * normalised; then Q[:, j] = q, Rt[j][0..j-1] = r, Rt[j][j] = r_jj (Rt
+ * row-major, ldr).  One cooperative launch, deterministic sums, queued
+ * without synchronising unless check != 0, which synchronises and reports a
+ * grid-barrier timeout of this or an earlier unchecked call. */
+int bem_cgs2_append(bem_ctx* ctx, int dtype, void* Q, int64_t n, int64_t ldq, int j, const void* v, int64_t ldv,
+                    void* Rt, int64_t ldr, int check, void* stream);
+
 /* Matrix-free apply: y[row] += scale * sum_col A(row,col) * x[col]
  * (x conjugated when conj_x != 0, the reference's cmul(integrand, cconj(g))).
  * Replaces apply_V_dot_N_boundary (single_layer_3d.py:435-498),

@@ -37,7 +37,7 @@ EXPORTS = [
     "bem_adjoint_vertices", "bem_mesh_set_2d", "bem_gmres_ir", "bem_compute_color", "bem_set_mesh_instances",
     "bem_lu_factor_status", "bem_binary_version", "bem_ctx_set_tuning", "bem_assemble_calderon", "bem_gram",
     "bem_lstsq_refine", "bem_chol_factor", "bem_gemm", "bem_chol_inverse", "bem_normal_refine", "bem_near_pair_list",
-    "bem_assemble_batch",
+    "bem_assemble_batch", "bem_cgs2_append",
 ]
 STATIC_SOLVE_MAX_N = 32768  # BEM_STATIC_SOLVE_MAX_N
 TUNE_CALDERON_GROUP = 0  # BEM_TUNE_CALDERON_GROUP
@@ -126,6 +126,7 @@ def load():
     pd, pp = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_void_p)
     L.bem_assemble_batch.argtypes = [vp, ctypes.POINTER(OpDesc), ctypes.POINTER(Space), ctypes.POINTER(Space), i32,
                                      pd, pd, pp, i64, pd, pp, pd, vp]
+    L.bem_cgs2_append.argtypes = [vp, i32, vp, i64, i64, i32, vp, i64, vp, i64, i32, vp]
     L.bem_measure_peaks.argtypes = [vp, ctypes.POINTER(ctypes.c_double), vp]
     L.bem_compute_color.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp]
     L.bem_set_mesh_instances.argtypes = [vp, vp, vp, vp, vp]

@@ -318,6 +318,19 @@ class Engine:
                                       _stream_ptr()))
         return C
 
+    def cgs2_append(self, Q: torch.Tensor, j: int, v: torch.Tensor, Rt: torch.Tensor, check: bool = False):
+        """Q[:, j] and Rt[j, :j + 1] of one CGS2 step against the first j
+        orthonormal columns of Q (bem_cgs2_append); v (a column, any element
+        stride) is not modified.  With check the call synchronises and
+        reports a device timeout."""
+        dt = Q.dtype
+        assert dt in (torch.complex128, torch.float64) and v.dtype == dt and Rt.dtype == dt
+        assert Q.is_cuda and Q.stride(1) == 1 and Rt.stride(1) == 1 and v.dim() in (1, 2)
+        n = Q.shape[0]
+        assert v.shape[0] == n and (v.dim() == 1 or v.shape[1] == 1) and 0 <= j < min(Q.shape[1], Rt.shape[0])
+        self._check(self.lib.bem_cgs2_append(self.ctx, _dtype_code(Q), _ptr(Q), n, Q.stride(0), int(j), _ptr(v),
+                                             v.stride(0), _ptr(Rt), Rt.stride(0), int(bool(check)), _stream_ptr()))
+
     def chol_inverse(self, A: torch.Tensor, X: torch.Tensor | None = None):
         """L^{-1} for A = L L^H (bem_chol_inverse): A (complex128 or float64,
         lower triangle read) is overwritten by L in its lower triangle.

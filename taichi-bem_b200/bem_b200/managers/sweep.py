@@ -28,7 +28,7 @@ from ..utils.types import AssembleType, ScopeType
 
 class Basis:
     """Orthonormal columns Q (n x j, FP64 real or complex, at most `cap`)
-    grown column by column by CGS2 on bem_gemm products:
+    grown column by column by CGS2 (bem_cgs2_append):
         h = Q^H v,  v -= Q h   (twice),   r_jj = ||v||,  q_j = v / r_jj,
     so that appended columns W satisfy W = Q R with R upper triangular, kept
     on the device as its transpose Rt (Rt[c, i] = R[i, c]).  A column
@@ -39,88 +39,33 @@ class Basis:
     not enter R), which makes it orthogonal to Q whether or not the column was
     dependent.  An exactly dependent column leaves r_jj = 0.
 
-    One append is a fixed sequence of about thirty small launches whose
-    shapes do not depend on j: the products run over all `cap` columns of Q,
-    whose columns j.. are still zero (so h_i = 0 for i >= j exactly), and the
-    column index lives on the device.  The sequence is captured once as a
-    CUDA graph (after one eager append, which sizes every buffer) and
-    replayed per column, so a column costs one graph launch instead of thirty
-    host-issued ones."""
+    Each column is one cooperative launch of this library (its ten grid
+    barriers replace about thirty small launches per column), queued without
+    a host synchronisation; the last column of each append checks the
+    device's timeout flag."""
 
-    def __init__(self, engine, n, cap, dtype, device, graph: bool = True):
+    def __init__(self, engine, n, cap, dtype, device):
         self.engine = engine
         self.Q = torch.zeros(n, cap, dtype=dtype, device=device)
         self.Rt = torch.zeros(cap, cap, dtype=dtype, device=device)
         self.j = 0
         self.cap = cap
-        self._h = torch.zeros(cap, 1, dtype=dtype, device=device)
-        self._r = torch.zeros(cap, 1, dtype=dtype, device=device)
-        self._nrm = torch.zeros(1, 1, dtype=dtype, device=device)
-        self._v = torch.zeros(n, 1, dtype=dtype, device=device)  # the graph's input column
-        self._jdev = torch.zeros(1, dtype=torch.long, device=device)
-        self._use_graph = graph and torch.device(device).type == "cuda"
-        self._graph = None
 
     @property
     def active(self) -> torch.Tensor:
         return self.Q[:, :self.j]
 
-    def _norm(self, v) -> torch.Tensor:
-        """||v|| as a real device scalar."""
-        self._nrm.zero_()
-        self.engine.gemm(v, v, self._nrm, conj_a=True)
-        return (self._nrm.real if self._nrm.is_complex() else self._nrm).reshape(()).clamp_min(0.0).sqrt()
-
-    def _project(self, v):
-        """h = Q^H v, v -= Q h over all cap columns; returns h (a buffer)."""
-        h = self._h
-        h.zero_()
-        self.engine.gemm(self.Q, v, h, conj_a=True)
-        self.engine.gemm(self.Q, h, v, alpha=-1.0)
-        return h
-
-    def _append_fixed(self):
-        """Append the column in self._v at the device-side index j."""
-        v, r = self._v, self._r
-        r.zero_()
-        for _ in range(2):
-            r.add_(self._project(v))
-        rjj = self._norm(v)
-        q = v / rjj.clamp_min(1e-300).to(v.dtype)
-        for _ in range(2):
-            self._project(q)
-        q = q / self._norm(q).clamp_min(1e-300).to(q.dtype)
-        r.index_copy_(0, self._jdev, rjj.to(r.dtype).view(1, 1))
-        self.Rt.index_copy_(0, self._jdev, r.view(1, self.cap))
-        self.Q.index_copy_(1, self._jdev, q)
-        self._jdev.add_(1)
-
     def append(self, W: torch.Tensor) -> int:
         """Append the columns of W (n x p); returns the number appended (the
         basis stops at `cap`)."""
+        W = W if W.stride(-1) == 1 or W.dim() == 1 else W.contiguous()
+        p = W.shape[1]
         added = 0
-        for c in range(W.shape[1]):
+        for c in range(p):
             if self.j >= self.cap:
                 break
-            self._v.copy_(W[:, c:c + 1])
-            if self._graph is not None:
-                self._graph.replay()
-            elif self._use_graph:
-                # the first append runs eagerly on a side stream (torch's
-                # capture recipe), then the same sequence is captured
-                side = torch.cuda.Stream(device=self.Q.device)
-                side.wait_stream(torch.cuda.current_stream(self.Q.device))
-                with torch.cuda.stream(side):
-                    self._append_fixed()
-                torch.cuda.current_stream(self.Q.device).wait_stream(side)
-                g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g):
-                    self._append_fixed()
-                self._graph = g
-                # capture recorded the sequence without running it: the
-                # device index still points at the next column
-            else:
-                self._append_fixed()
+            last = c == p - 1 or self.j + 1 >= self.cap
+            self.engine.cgs2_append(self.Q, self.j, W[:, c], self.Rt, check=last)
             self.j += 1
             added += 1
         return added

@@ -1150,6 +1150,220 @@ int gmres_run(bem_ctx* ctx, int dtype_hi, const void* A_hi, const void* LU_lo, c
     return bem_fgmres(ctx, C, n, op, precond, b, x, tol, maxit, restart, accept, iters, relres, s);
 }
 
+// ---------------------------------------------------------------------------
+// CGS2 column append of a growing orthonormal basis, one cooperative launch
+// (bem_cgs2_append).  With x = v:
+//   twice: h = Q^H x, x -= Q h, r += h;   r_jj = ||x||, x /= r_jj;
+//   twice: h = Q^H x, x -= Q h;           x /= ||x||;
+//   Q[:, j] = x, Rt[j, 0..j-1] = r, Rt[j, j] = r_jj.
+// CTA b owns the rows [b rb, (b + 1) rb) of x and keeps them in shared memory
+// for the whole step.  A projection is two grid barriers: the partial dot
+// products of every CTA over its rows (thread c takes column c, so the reads
+// of a Q row are coalesced) go to part[b][c]; CTA c % nblk sums column c over
+// the CTAs in a fixed order into h[c]; then every CTA forms its rows of Q h
+// (one warp per row, lanes over the columns).  Norms: per-CTA partial sums,
+// one barrier, the same fixed-order sum in every CTA.  Ten barriers per
+// column, no host synchronisation; the sums are deterministic.
+// ---------------------------------------------------------------------------
+constexpr int CG_THREADS = 256;
+
+template <bool C>
+struct Cx {
+    double re, im;
+};
+
+template <bool C>
+__device__ __forceinline__ Cx<C> cx_ld(const double* p, int64_t i) {
+    return C ? Cx<C>{p[2 * i], p[2 * i + 1]} : Cx<C>{p[i], 0.0};
+}
+template <bool C>
+__device__ __forceinline__ void cx_st(double* p, int64_t i, Cx<C> v) {
+    if (C) {
+        p[2 * i] = v.re;
+        p[2 * i + 1] = v.im;
+    } else {
+        p[i] = v.re;
+    }
+}
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < CG_THREADS / 32; ++w) t += red[w];
+    __syncthreads();
+    if (threadIdx.x == 0) red[0] = t;
+    __syncthreads();
+    const double out = red[0];
+    __syncthreads();
+    return out;
+}
+
+template <bool C>
+__global__ void __launch_bounds__(CG_THREADS) cgs2_append_kernel(double* Q, int64_t n, int64_t ldq, int j,
+                                                                  const double* v, int64_t ldv, double* Rt,
+                                                                  int64_t ldr, double* part, double* hbuf,
+                                                                  double* rbuf, double* npart, GridBar* bar,
+                                                                  int32_t* flag) {
+    extern __shared__ double cg_smem[];
+    __shared__ double red[CG_THREADS / 32];
+    const int W = C ? 2 : 1;
+    const unsigned nblk = gridDim.x;
+    const int b = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t rb = (n + nblk - 1) / nblk;
+    const int64_t r0 = (int64_t)b * rb, r1 = r0 + rb < n ? r0 + rb : n;
+    const int nr = r1 > r0 ? (int)(r1 - r0) : 0;
+    double* sx = cg_smem;                 // [rb] this CTA's rows of x
+    double* sh = cg_smem + (size_t)W * rb;  // [j] h
+    for (int i = tid; i < nr; i += CG_THREADS) {
+        const Cx<C> e = cx_ld<C>(v, (r0 + i) * ldv);
+        sx[W * i] = e.re;
+        if (C) sx[W * i + 1] = e.im;
+    }
+    __syncthreads();
+
+    auto project = [&](bool accumulate, bool first) -> bool {
+        // partial h over this CTA's rows
+        for (int c = tid; c < j; c += CG_THREADS) {
+            double ar = 0.0, ai = 0.0;
+#pragma unroll 4
+            for (int i = 0; i < nr; ++i) {
+                const Cx<C> q = cx_ld<C>(Q, (r0 + i) * ldq + c);
+                const double xr = sx[W * i], xi = C ? sx[W * i + 1] : 0.0;
+                ar += q.re * xr + q.im * xi;  // conj(q) x
+                if (C) ai += q.re * xi - q.im * xr;
+            }
+            cx_st<C>(part, (int64_t)b * j + c, Cx<C>{ar, ai});
+        }
+        if (!grid_barrier(bar, nblk, flag)) return false;
+        // column c: the fixed-order sum over the CTAs
+        for (int c = b; c < j; c += (int)nblk) {
+            double sr = 0.0, si = 0.0;
+            for (unsigned bb = tid; bb < nblk; bb += CG_THREADS) {
+                const Cx<C> e = cx_ld<C>(part, (int64_t)bb * j + c);
+                sr += e.re;
+                si += e.im;
+            }
+            sr = block_sum(sr, red);
+            if (C) si = block_sum(si, red);
+            if (tid == 0) {
+                cx_st<C>(hbuf, c, Cx<C>{sr, si});
+                if (accumulate) {
+                    Cx<C> r = first ? Cx<C>{0.0, 0.0} : cx_ld<C>(rbuf, c);
+                    cx_st<C>(rbuf, c, Cx<C>{r.re + sr, r.im + si});
+                }
+            }
+        }
+        if (!grid_barrier(bar, nblk, flag)) return false;
+        for (int c = tid; c < j; c += CG_THREADS) {
+            const Cx<C> e = cx_ld<C>(hbuf, c);
+            sh[W * c] = e.re;
+            if (C) sh[W * c + 1] = e.im;
+        }
+        __syncthreads();
+        // x -= Q h on this CTA's rows
+        for (int i = warp; i < nr; i += CG_THREADS / 32) {
+            double ar = 0.0, ai = 0.0;
+            for (int c = lane; c < j; c += 32) {
+                const Cx<C> q = cx_ld<C>(Q, (r0 + i) * ldq + c);
+                const double hr = sh[W * c], hi = C ? sh[W * c + 1] : 0.0;
+                ar += q.re * hr - q.im * hi;
+                if (C) ai += q.re * hi + q.im * hr;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                ar += __shfl_xor_sync(0xffffffffu, ar, o);
+                if (C) ai += __shfl_xor_sync(0xffffffffu, ai, o);
+            }
+            if (lane == 0) {
+                sx[W * i] -= ar;
+                if (C) sx[W * i + 1] -= ai;
+            }
+        }
+        __syncthreads();
+        return true;
+    };
+    auto norm = [&](double& out) -> bool {
+        double p = 0.0;
+        for (int i = tid; i < nr; i += CG_THREADS) {
+            p += sx[W * i] * sx[W * i];
+            if (C) p += sx[W * i + 1] * sx[W * i + 1];
+        }
+        p = block_sum(p, red);
+        if (tid == 0) npart[b] = p;
+        if (!grid_barrier(bar, nblk, flag)) return false;
+        double t = 0.0;
+        for (unsigned bb = tid; bb < nblk; bb += CG_THREADS) t += npart[bb];
+        t = block_sum(t, red);
+        out = sqrt(t > 0.0 ? t : 0.0);
+        return true;
+    };
+    auto scale = [&](double d) {
+        const double f = 1.0 / (d > 1e-300 ? d : 1e-300);
+        for (int i = tid; i < nr * W; i += CG_THREADS) sx[i] *= f;
+        __syncthreads();
+    };
+
+    double rjj = 0.0, qn = 0.0;
+    if (j > 0 && (!project(true, true) || !project(true, false))) return;
+    if (!norm(rjj)) return;
+    scale(rjj);
+    if (j > 0 && (!project(false, false) || !project(false, false))) return;
+    if (!norm(qn)) return;
+    scale(qn);
+    for (int i = tid; i < nr; i += CG_THREADS)
+        cx_st<C>(Q, (r0 + i) * ldq + j, Cx<C>{sx[W * i], C ? sx[W * i + 1] : 0.0});
+    if (b == 0) {
+        for (int c = tid; c < j; c += CG_THREADS) cx_st<C>(Rt, (int64_t)j * ldr + c, cx_ld<C>(rbuf, c));
+        if (tid == 0) cx_st<C>(Rt, (int64_t)j * ldr + j, Cx<C>{rjj, 0.0});
+    }
+}
+
+template <bool C>
+int cgs2_append_t(bem_ctx* ctx, double* Q, int64_t n, int64_t ldq, int j, const double* v, int64_t ldv,
+                  double* Rt, int64_t ldr, int check, cudaStream_t s) {
+    const int W = C ? 2 : 1;
+    int nblk0 = ctx->num_sms;
+    const int64_t rb0 = (n + nblk0 - 1) / nblk0;
+    const size_t smem = sizeof(double) * W * ((size_t)rb0 + (size_t)std::max(j, 1));
+    if (smem > 200 * 1024) return bem_fail(ctx, BEM_ERR_INVALID, "cgs2_append: n or j too large");
+    cudaFuncSetAttribute(cgs2_append_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int nblk = coop_blocks(ctx, (const void*)cgs2_append_kernel<C>, CG_THREADS, smem, ctx->num_sms);
+    if (nblk < 1) return bem_fail(ctx, BEM_ERR_CUDA, "cgs2_append_kernel cannot be made co-resident");
+    if (nblk != nblk0) return bem_fail(ctx, BEM_ERR_CUDA, "cgs2_append_kernel: fewer co-resident CTAs than SMs");
+    const size_t jb = (size_t)std::max(j, 1);
+    const size_t bytes = 256 + sizeof(double) * W * ((size_t)nblk * jb + 2 * jb) + sizeof(double) * nblk;
+    if (int rc = bem_ws_reserve(ctx, bytes)) return rc;
+    char* base = static_cast<char*>(ctx->ws);
+    GridBar* bar = reinterpret_cast<GridBar*>(base);
+    double* part = reinterpret_cast<double*>(base + 256);
+    double* hbuf = part + (size_t)W * nblk * jb;
+    double* rbuf = hbuf + (size_t)W * jb;
+    double* npart = rbuf + (size_t)W * jb;
+    if (int rc = bem_check_cuda(ctx, cudaMemsetAsync(bar, 0, sizeof(GridBar), s), "cgs2 barrier reset")) return rc;
+    int32_t* flag = ctx->flags + 7;
+    void* args[] = {&Q, &n, &ldq, &j, (void*)&v, &ldv, &Rt, &ldr, &part, &hbuf, &rbuf, &npart, &bar, &flag};
+    if (int rc = bem_check_cuda(ctx, cudaLaunchCooperativeKernel((const void*)cgs2_append_kernel<C>, nblk,
+                                                                CG_THREADS, args, smem, s),
+                                "cgs2_append_kernel"))
+        return rc;
+    ctx->launches++;
+    if (!check) return BEM_OK;
+    int32_t f = 0;
+    if (int rc = bem_check_cuda(ctx, cudaMemcpyAsync(&f, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                                "cgs2 flag readback"))
+        return rc;
+    if (int rc = bem_check_cuda(ctx, cudaStreamSynchronize(s), "cgs2_append")) return rc;
+    if (f != 0) {
+        cudaMemsetAsync(flag, 0, sizeof(int32_t), s);
+        return bem_fail(ctx, BEM_ERR_TIMEOUT, "cgs2_append: a grid barrier hit its iteration cap");
+    }
+    return BEM_OK;
+}
+
 template <typename T, bool C>
 int gemv_t(bem_ctx* ctx, const T* A, int64_t m, int64_t n, int64_t lda, const double* x, double* y, double alpha,
            double beta, cudaStream_t s) {
@@ -1162,6 +1376,21 @@ int gemv_t(bem_ctx* ctx, const T* A, int64_t m, int64_t n, int64_t lda, const do
 }  // namespace
 
 extern "C" {
+
+int bem_cgs2_append(bem_ctx* ctx, int dtype, void* Q, int64_t n, int64_t ldq, int j, const void* v, int64_t ldv,
+                    void* Rt, int64_t ldr, int check, void* stream) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (!Q || !v || !Rt || n <= 0 || j < 0 || ldq <= j || ldr <= j || ldv <= 0)
+        return bem_fail(ctx, BEM_ERR_INVALID, "cgs2_append: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (dtype) {
+        case BEM_F64:
+            return cgs2_append_t<false>(ctx, (double*)Q, n, ldq, j, (const double*)v, ldv, (double*)Rt, ldr, check, s);
+        case BEM_C128:
+            return cgs2_append_t<true>(ctx, (double*)Q, n, ldq, j, (const double*)v, ldv, (double*)Rt, ldr, check, s);
+        default: return bem_fail(ctx, BEM_ERR_INVALID, "cgs2_append: dtype must be BEM_F64 or BEM_C128");
+    }
+}
 
 int bem_lu_factor(bem_ctx* ctx, int dtype, void* A, int64_t n, int64_t lda, int32_t* piv, int32_t* info,
                   void* stream) {
