@@ -317,7 +317,7 @@ def phase_breakdown(b):
     return out
 
 
-def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5):
+def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5, calderon_group: int = 0):
     """One warm-up and one timed step of the workload, nothing else (the
     command the committed ncu summaries under profiles/ were captured with):
     the Dirichlet problem on 5120 panels, or the transmission least-squares
@@ -334,6 +334,9 @@ def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5
     core = CoreManager(params)
     core.initialization(fD, fN)
     b = core._BEM_manager
+    if calderon_group:
+        from bem_b200 import _lib as L
+        b.engine.set_tuning(L.TUNE_CALDERON_GROUP, calderon_group)
     b.run()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -974,6 +977,8 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--profile-step", default=None, choices=["mixed", "fp64"],
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
+    ap.add_argument("--calderon-group", type=int, default=0,
+                    help="form of the fused Calderon sweep in --profile-step (the BEM_TUNE_CALDERON_GROUP value)")
     ap.add_argument("--profile-lu", type=int, default=0,
                     help="time six tiled FP32 factorisations of a random complex matrix of this size and exit")
     ap.add_argument("--workload", default="transmission_s5",
@@ -1016,7 +1021,7 @@ def main():
             disk2d_bench(args.disk_n, 5, 3.0)
         return
     if args.profile_step:
-        profile_step(args.profile_step, args.workload, args.trans_subdiv)
+        profile_step(args.profile_step, args.workload, args.trans_subdiv, args.calderon_group)
         return
     if args.profile_lu:
         profile_lu(args.profile_lu)

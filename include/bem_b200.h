@@ -119,9 +119,10 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  *                            bem_assemble_batch: 2 or 4 (default 4 in mixed
  *                            precision, 2 in FP64; P1 x P1 blocks always 2)
  *   BEM_TUNE_GRAM_PAIR       form of the tensor-core normal matrix and
- *                            Cholesky updates: 1 one CTA per 128 x 128 tile,
- *                            2 CTA pairs (tcgen05 cta_group::2) on 256 x 128
- *                            tiles, column order */
+ *                            Cholesky updates: 1 one CTA per 128 x 128 tile
+ *                            (eight epilogue warps), 2 CTA pairs (tcgen05
+ *                            cta_group::2) on 256 x 128 tiles, column order,
+ *                            3 one CTA per tile with sixteen epilogue warps */
 #define BEM_TUNE_CALDERON_GROUP 0
 #define BEM_TUNE_GRAM_KSEG 1
 #define BEM_TUNE_CHOL_NB 2

@@ -896,8 +896,9 @@ class BEMManager:
         wavenumber, 1: scalar per wavenumber; the packed forms in mixed
         precision only),
         timed on assemble_system, and for the least-squares solver the form
-        of the tensor-core normal matrix (2: CTA pairs on 256 x 128 tiles, 1:
-        one CTA per 128 x 128 tile; mixed precision), the band width of the
+        of the tensor-core normal matrix (1: one CTA per 128 x 128 tile with
+        eight epilogue warps, 3: with sixteen, 2: CTA pairs on 256 x 128
+        tiles; mixed precision), the band width of the
         normal matrix's tile order (1, 12, 8, 16), timed on the normal matrix,
         and the Cholesky panel width (512, 1024, 2048), timed on its
         factorisation.  Cached choices are applied without
@@ -913,7 +914,7 @@ class BEMManager:
                                                self.assemble_system)
         nbs = [512, 1024, 2048]
         mixed = self.solve_precision == "mixed"
-        pairs = [2, 1] if mixed else [1]
+        pairs = [1, 3, 2] if mixed else [1]
         if (self._is_transmission and self.solver == "lstsq" and tuner.cached(wl + "/chol", L.TUNE_CHOL_NB, nbs)
                 and tuner.cached(wl + "/gram", L.TUNE_GRAM_BAND, [1, 12, 8, 16])
                 and (not mixed or tuner.cached(wl + "/gram_pair", L.TUNE_GRAM_PAIR, pairs))):
@@ -931,7 +932,7 @@ class BEMManager:
                 # one-CTA form; the band width below only shapes the latter
                 out["gram_pair"] = tuner.tune(wl + "/gram_pair", L.TUNE_GRAM_PAIR, pairs,
                                               lambda: self.engine.gram(A, P, Nm, d, tensor_cores=True))
-            bands = [1] if out.get("gram_pair") == 2 else [1, 12, 8, 16]
+            bands = [1] if out.get("gram_pair") == 2 else [1, 12, 8, 16]  # the pair form has one tile order
             out["gram_band"] = tuner.tune(wl + "/gram", L.TUNE_GRAM_BAND, bands,
                                           lambda: self.engine.gram(A, P, Nm, d, tensor_cores=mixed))
             W = torch.empty_like(Nm)

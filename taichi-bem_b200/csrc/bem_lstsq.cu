@@ -216,7 +216,8 @@ constexpr int GT_KSEG_DEFAULT = 2;
 // 1183 ms); the autotuner chooses per problem.
 constexpr int GRAM_BAND_DEFAULT = 1;
 // form of the tensor-core Gram product (BEM_TUNE_GRAM_PAIR): 1 one CTA per
-// 128 x 128 tile (gram_tc_kernel), 2 CTA pairs on 256 x 128 tiles (gram_tc2_kernel)
+// 128 x 128 tile (gram_tc_kernel, eight epilogue warps), 2 CTA pairs on 256 x
+// 128 tiles (gram_tc2_kernel), 3 one CTA per tile with sixteen epilogue warps
 constexpr int GRAM_PAIR_DEFAULT = 1;
 constexpr int GT_EPI_WARPS = 8;
 constexpr int GT_THREADS = 64 + 32 * GT_EPI_WARPS;
@@ -290,8 +291,8 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
 }
 
 // out: complex (C, interleaved pairs) or real N x N matrix of OT (float or double), ld in elements
-template <bool C, typename OT>
-__global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
+template <bool C, typename OT, int EW>
+__global__ void __launch_bounds__(64 + 32 * EW, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi,
                                                                  const __grid_constant__ CUtensorMap tm_lo,
                                                                  int nchunks, int kseg, int ntiles, int tgrid,
                                                                  int band, OT* out, int64_t ldo, int n, double alpha,
@@ -300,7 +301,9 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
     __shared__ __align__(8) uint64_t full_bar[GT_STAGES], empty_bar[GT_STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int s_abort;
-    __shared__ double s_stage[GT_EPI_WARPS][8 * GT_STG_LD];  // epilogue staging, eight real rows per warp
+    // EW epilogue warps: warp w reads TMEM lanes 32 (w % 4) .. and column group (w - 2) / 4 of EW / 4
+    constexpr int NCG = EW / 4, EC = GT_BM / NCG, STG_LD = EC + 1;
+    __shared__ double s_stage[EW][8 * STG_LD];  // epilogue staging, eight real rows per warp
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                            ~uintptr_t(1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -319,7 +322,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         }
         for (int b = 0; b < 2; ++b) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&acc_full[b])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acc_empty[b])), "r"(GT_EPI_WARPS)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acc_empty[b])), "r"(EW)
                          : "memory");
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -406,8 +409,7 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
         }
     } else {
         // ---- epilogue: FP64 running sums of the segments, then the complex combine ----
-        constexpr int EC = GT_BM / 2;  // columns per epilogue thread
-        const int q = warp & 3, half = (warp - 2) >> 2;
+        const int q = warp & 3, half = (warp - 2) >> 2;  // lane quarter, column group
         uint32_t gg = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
@@ -449,22 +451,26 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                 // complex column l of each,
                 //   N[p][q] = (S[2p][2q] + S[2p+1][2q+1]) + i (S[2p][2q+1] - S[2p+1][2q]),
                 // so each access covers 32 contiguous complex entries
-                double* stg = s_stage[warp - 2];  // [8][GT_STG_LD]
+                double* stg = s_stage[warp - 2];  // [8][STG_LD]
+                constexpr int CC = EC / 2;        // complex columns of the thread's column group
+                constexpr int RPL = 4 * CC / 32;  // complex rows per lane and round
+                const int lc = lane % CC, lr0 = (lane / CC) * RPL;
                 const int pw0 = (bi * GT_BM + 32 * q) >> 1;  // first complex row of this warp
-                const int qc = (c0 >> 1) + lane;
+                const int qc = (c0 >> 1) + lc;
 #pragma unroll
                 for (int c4 = 0; c4 < 4; ++c4) {
                     if ((lane >> 3) == c4) {
 #pragma unroll
-                        for (int m = 0; m < EC; ++m) stg[(lane & 7) * GT_STG_LD + m] = acc[m];
+                        for (int m = 0; m < EC; ++m) stg[(lane & 7) * STG_LD + m] = acc[m];
                     }
                     __syncwarp();
-                    double nre[4], nim[4], ore[4], oim[4];
+                    double nre[RPL], nim[RPL], ore[RPL], oim[RPL];
 #pragma unroll
-                    for (int ri = 0; ri < 4; ++ri) {
-                        const double* e = stg + (2 * ri) * GT_STG_LD + 2 * lane;
-                        const double* o = stg + (2 * ri + 1) * GT_STG_LD + 2 * lane;
-                        const int pr = pw0 + 4 * c4 + ri;
+                    for (int ri = 0; ri < RPL; ++ri) {
+                        const int rr = lr0 + ri;
+                        const double* e = stg + (2 * rr) * STG_LD + 2 * lc;
+                        const double* o = stg + (2 * rr + 1) * STG_LD + 2 * lc;
+                        const int pr = pw0 + 4 * c4 + rr;
                         nre[ri] = e[0] + o[1];
                         nim[ri] = pr == qc ? 0.0 : e[1] - o[0];  // a Hermitian matrix has a real diagonal
                         ore[ri] = oim[ri] = 0.0;
@@ -475,8 +481,8 @@ __global__ void __launch_bounds__(GT_THREADS, 1) gram_tc_kernel(const __grid_con
                         }
                     }
 #pragma unroll
-                    for (int ri = 0; ri < 4; ++ri) {
-                        const int pr = pw0 + 4 * c4 + ri;
+                    for (int ri = 0; ri < RPL; ++ri) {
+                        const int pr = pw0 + 4 * c4 + lr0 + ri;
                         if (pr < n && qc < n) {
                             OT* ot = out + 2 * ((int64_t)pr * ldo + qc);
                             ot[0] = (OT)(ore[ri] + alpha * nre[ri]);
@@ -1216,15 +1222,29 @@ int launch_gram_tc(bem_ctx* ctx, __half* Thi, __half* Tlo, int64_t Rp, int64_t K
         ctx->launches++;
         return bem_check_cuda(ctx, e, "gram_tc2_kernel");
     }
-    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc_kernel<C, OT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                          (int)GT_SMEM),
-                                "gram_tc_kernel smem"))
-        return rc;
     const int band = ctx->tune[BEM_TUNE_GRAM_BAND] > 0 ? ctx->tune[BEM_TUNE_GRAM_BAND] : GRAM_BAND_DEFAULT;
     // persistent: one CTA per SM (its shared memory and 512 TMEM columns allow no second), tiles in turn
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctx->num_sms);
-    gram_tc_kernel<C, OT><<<grid, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg, (int)tiles, tr,
-                                                            band, out, ldo, n, alpha, accumulate, ctx->flags + 5);
+    if (form == 3) {
+        // sixteen epilogue warps, 32 columns of FP64 running sums per thread
+        if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc_kernel<C, OT, 16>,
+                                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                              (int)GT_SMEM),
+                                    "gram_tc_kernel smem"))
+            return rc;
+        gram_tc_kernel<C, OT, 16><<<grid, 64 + 32 * 16, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg,
+                                                                       (int)tiles, tr, band, out, ldo, n, alpha,
+                                                                       accumulate, ctx->flags + 5);
+    } else {
+        if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(gram_tc_kernel<C, OT, GT_EPI_WARPS>,
+                                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                              (int)GT_SMEM),
+                                    "gram_tc_kernel smem"))
+            return rc;
+        gram_tc_kernel<C, OT, GT_EPI_WARPS><<<grid, GT_THREADS, GT_SMEM, s>>>(tm[0], tm[1], (int)(Kp / GT_BK), kseg,
+                                                                             (int)tiles, tr, band, out, ldo, n,
+                                                                             alpha, accumulate, ctx->flags + 5);
+    }
     ctx->launches++;
     return bem_check_cuda(ctx, cudaGetLastError(), "gram_tc_kernel");
 }

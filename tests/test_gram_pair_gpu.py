@@ -1,8 +1,8 @@
-"""The CTA-pair form of the tensor-core normal matrix (gram_tc2_kernel,
-tcgen05 cta_group::2 on 256 x 128 tiles, BEM_TUNE_GRAM_PAIR = 2) against the
-one-CTA form and the FP64 product: the normal matrix of the least squares
-(bem_gram) and the Cholesky whose trailing updates it forms
-(bem_chol_factor)."""
+"""The other forms of the tensor-core normal matrix (BEM_TUNE_GRAM_PAIR = 2:
+gram_tc2_kernel, tcgen05 cta_group::2 on 256 x 128 tiles; 3: one CTA with
+sixteen epilogue warps) against the default one-CTA form and the FP64
+product: the normal matrix of the least squares (bem_gram) and the Cholesky
+whose trailing updates it forms (bem_chol_factor)."""
 import numpy as np
 import pytest
 import torch
@@ -32,9 +32,10 @@ def _gram(engine, A, P, form, tensor_cores=True):
     return out, d
 
 
+@pytest.mark.parametrize("form", [2, 3])
 @pytest.mark.parametrize("cplx", [True, False])
 @pytest.mark.parametrize("n", [50, 130, 300, 1000])
-def test_pair_gram_matches_single_and_fp64(engine, n, cplx):
+def test_pair_gram_matches_single_and_fp64(engine, n, cplx, form):
     """Same products, different tile shape: the two tensor-core forms agree
     to the FP32 rounding of their TMEM sums, and both match the FP64 normal
     matrix to the split's accuracy."""
@@ -42,7 +43,7 @@ def test_pair_gram_matches_single_and_fp64(engine, n, cplx):
     dt = torch.complex128 if cplx else torch.float64
     A = torch.randn(n, n, dtype=dt, device="cuda", generator=g)
     P = torch.randn(n, n, dtype=dt, device="cuda", generator=g)
-    N2, d2 = _gram(engine, A, P, 2)
+    N2, d2 = _gram(engine, A, P, form)
     N1, d1 = _gram(engine, A, P, 1)
     N0, d0 = _gram(engine, A, P, 1, tensor_cores=False)
     assert torch.equal(d1, d2) and torch.equal(d0, d2)
@@ -55,9 +56,10 @@ def test_pair_gram_matches_single_and_fp64(engine, n, cplx):
         assert float(torch.diagonal(N2).imag.abs().max()) == 0.0
 
 
+@pytest.mark.parametrize("form", [2, 3])
 @pytest.mark.parametrize("cplx", [True, False])
 @pytest.mark.parametrize("n", [300, 1333])
-def test_pair_cholesky_updates(engine, n, cplx):
+def test_pair_cholesky_updates(engine, n, cplx, form):
     """The Cholesky's tcgen05 trailing updates in the pair form solve like the
     one-CTA form (FP64 Schur complement, split products)."""
     from bem_b200 import _lib as L
@@ -70,9 +72,9 @@ def test_pair_cholesky_updates(engine, n, cplx):
     b = rng.standard_normal(n) + (1j * rng.standard_normal(n) if cplx else 0)
     ref = np.linalg.solve(N, b)
     xs = []
-    for form in (2, 1):
+    for fm in (form, 1):
         F = torch.as_tensor(N, dtype=dt, device="cuda").clone()
-        engine.set_tuning(L.TUNE_GRAM_PAIR, form)
+        engine.set_tuning(L.TUNE_GRAM_PAIR, fm)
         try:
             piv, dinv, info = engine.chol_factor(F, tensor_cores=True)
         finally:
