@@ -371,23 +371,59 @@ def profile_lu(n: int):
     eng.close()
 
 
-def sweep_bench(n_k: int, k_batch: int = 4):
+def shard_wavenumbers(ks, rank: int, ws: int):
+    """Rank r's share of a wavenumber sweep: ks[r], ks[r + ws], ... .  Each k
+    is an independent unit (its own operators, norm estimate and least
+    squares), so the ranks exchange no data while they run."""
+    return list(ks[rank::ws])
+
+
+def sweep_gather(local: dict, ks, rank: int, ws: int) -> dict:
+    """Every rank's per-k lists (local[name][i] belongs to
+    shard_wavenumbers(ks, rank, ws)[i]) merged in the order of ks, on every
+    rank (one all_gather_object when ws > 1; reporting only, after the timed
+    region)."""
+    parts = [local]
+    if ws > 1:
+        import torch.distributed as dist
+        parts = [None] * ws
+        dist.all_gather_object(parts, local)
+    out = {}
+    for name in local:
+        merged = [None] * len(ks)
+        for r, part in enumerate(parts):
+            for i, v in zip(range(r, len(ks), ws), part[name]):
+                merged[i] = v
+        out[name] = merged
+    return out
+
+
+def sweep_bench(n_k: int, k_batch: int = 4, ws: int = 1, rank: int = 0, local: int = 0):
     """The wavenumber sweep (managers/sweep.py) of the augmented
     transmission operator over n_k wavenumbers, mixed precision against the
     plain FP64 path, both with the same FP64 block-Krylov norm estimator
-    (CGS2 column appends replayed from a CUDA graph) and the same k-batched
-    assembly (k_batch wavenumbers per group);
-    one JSON line with per-k times, phases, errors and the norm estimates.
-    Each arm first lets the autotuner choose its Cholesky panel width
-    (cached per device and problem) and runs one untimed k."""
+    (one fused CGS2 launch per basis column) and the same k-batched assembly
+    (k_batch wavenumbers per group); one JSON line with per-k times, phases,
+    errors and the norm estimates.  On ws ranks (one GPU each) rank r takes
+    the wavenumbers shard_wavenumbers(ks, r, ws) (no data exchange); each arm
+    is timed with CUDA events between two barriers and the job time is the
+    maximum over ranks.  Each arm first lets the autotuner choose its launch
+    shapes (cached per device and problem) and runs one untimed k."""
     import torch
     from bem_b200.managers import CoreManager
     from bem_b200.managers.sweep import wavenumber_sweep
     from bem_b200.tuning import Autotuner
     from bem_b200.workloads import transmission_sweep_s4
-    res, tuned = {}, {}
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    res, tuned, total_ms = {}, {}, {}
     for prec in ("mixed", "fp64"):
         params, fD, fN, ks = transmission_sweep_s4(prec, n_k)
+        mine = shard_wavenumbers(ks, rank, ws)
         params["solver"] = "lstsq"
         core = CoreManager(params)
         core.initialization(fD, fN)
@@ -395,44 +431,67 @@ def sweep_bench(n_k: int, k_batch: int = 4):
         bm._k = ks[0]
         tuned[prec] = bm.autotune(Autotuner(bm.engine))
         kw = dict(nrhs=4, seed=0, norm_tol=1e-6, norm_maxit=32, norm_method="iterative", k_batch=k_batch)
-        wavenumber_sweep(bm, ks[:1], **kw)  # warm-up
+        wavenumber_sweep(bm, mine[:1] or ks[:1], **kw)  # warm-up
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        res[prec] = wavenumber_sweep(bm, ks, **kw)
+        if ws > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res[prec] = wavenumber_sweep(bm, mine, **kw) if mine else {
+            "k": [], "inv_norm": [], "cond": [], "solutions": [], "ms": [], "phase_ms": [], "iterations": []}
+        e1.record()
         torch.cuda.synchronize()
-        res[prec]["total_s"] = time.perf_counter() - t0
+        if ws > 1:
+            dist.barrier()
+        total_ms[prec], _ = replicas_aggregate(e0.elapsed_time(e1), 1.0, ws, dev)
         res[prec]["launches"] = bm.engine.launches
         core.kill()
-    errs = [float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
-            for a, b in zip(res["mixed"]["solutions"], res["fp64"]["solutions"])]
-    nerr = [abs(a - b) / b for a, b in zip(res["mixed"]["inv_norm"], res["fp64"]["inv_norm"])]
+    local_lists = {
+        "sol_err": [float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+                    for a, b in zip(res["mixed"]["solutions"], res["fp64"]["solutions"])],
+        "norm_diff": [abs(a - b) / b for a, b in zip(res["mixed"]["inv_norm"], res["fp64"]["inv_norm"])],
+        "inv_norm": res["mixed"]["inv_norm"], "cond": res["mixed"]["cond"],
+        "blocks": res["mixed"]["iterations"],
+        "ms_mixed": res["mixed"]["ms"], "ms_fp64": res["fp64"]["ms"],
+        "phase_mixed": res["mixed"]["phase_ms"], "phase_fp64": res["fp64"]["phase_ms"],
+    }
+    g = sweep_gather(local_lists, ks, rank, ws)
+    launches = sweep_gather({"l": [[res["mixed"]["launches"], res["fp64"]["launches"]]]}, list(range(ws)), rank, ws)
+    if ws > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
 
-    def phases(r):
-        return {ph: statistics.mean(x[ph] for x in r["phase_ms"]) for ph in ("assemble", "norm", "lstsq")}
+    def phases(lst):
+        return {ph: statistics.mean(x[ph] for x in lst) for ph in ("assemble", "norm", "lstsq")}
 
+    mixed_s, fp64_s = total_ms["mixed"] * 1e-3, total_ms["fp64"] * 1e-3
     print(json.dumps({
         "workload": "augmented transmission sweep A_I, icosphere s4, P1/P1 (5124 unknowns, stacked 10248 x 5124), "
                     "GaussQR=3, n_i=3, n_o=1, k = 16 + i/30, 4 complex Gaussian RHS per k",
-        "n_k": len(res["mixed"]["k"]), "k_range": [res["mixed"]["k"][0], res["mixed"]["k"][-1]],
-        "mixed_s": res["mixed"]["total_s"], "plain_fp64_s": res["fp64"]["total_s"],
-        "speedup": res["fp64"]["total_s"] / res["mixed"]["total_s"],
-        "ms_per_k_mixed": statistics.mean(res["mixed"]["ms"]), "ms_per_k_fp64": statistics.mean(res["fp64"]["ms"]),
-        "phase_ms_per_k": {"mixed": phases(res["mixed"]), "fp64": phases(res["fp64"])},
-        "solution_rel_err_max": max(errs), "inv_norm_rel_diff_max": max(nerr),
-        "inv_norm": res["mixed"]["inv_norm"], "cond": res["mixed"]["cond"],
+        "n_k": len(ks), "k_range": [ks[0], ks[-1]], "n_gpus": ws,
+        "scaling": "strong" if ws > 1 else None,
+        "sharding": "rank r takes k_r, k_(r+N), ... (independent units, no data-path collective); job time = max over "
+                    "ranks of the CUDA-event time between two barriers",
+        "mixed_s": mixed_s, "plain_fp64_s": fp64_s, "speedup": fp64_s / mixed_s,
+        "ms_per_k_mixed": mixed_s * 1e3 / len(ks), "ms_per_k_fp64": fp64_s * 1e3 / len(ks),
+        "phase_ms_per_k": {"mixed": phases(g["phase_mixed"]), "fp64": phases(g["phase_fp64"])},
+        "solution_rel_err_max": max(g["sol_err"]), "inv_norm_rel_diff_max": max(g["norm_diff"]),
+        "inv_norm": g["inv_norm"], "cond": g["cond"],
         "norm_method": "both arms: energy-scaled operator by FP64 DMMA products, block Krylov of (S^H S)^{-1} "
-                       "(8-vector blocks, the FP64 Cholesky inverse of the scaled S^H S) and of S^H S, Ritz "
-                       "values from the CGS2 R of S Q, stop at 1e-6 relative change or 32 blocks",
+                       "(8-vector blocks, the FP64 Cholesky inverse of the scaled S^H S) and of S^H S, CGS2 bases "
+                       "(one cooperative launch per column), Ritz values from the CGS2 R of S Q, stop at 1e-6 "
+                       "relative change or 32 blocks",
         "lstsq": {"mixed": "FP32 far-field assembly, FP16-split tcgen05 normal matrix, Cholesky with tcgen05 updates, "
                            "FP64 flexible GMRES per RHS",
                   "fp64": "FP64 assembly, DMMA normal matrix, Cholesky with DMMA updates, FP64 flexible GMRES "
                           "per RHS"},
         "autotuned": tuned,
-        "norm_krylov_blocks": res["mixed"]["iterations"],
+        "norm_krylov_blocks": g["blocks"],
         "k_batch": k_batch,
         "assembly": "per group of k_batch wavenumbers k: V, K (with -K^T) and W each by one bem_assemble_batch call "
                     "over the 2 k_batch media wavenumbers (one far launch per pair of wavenumbers, geometry shared)",
-        "gpu_launches": {"mixed": res["mixed"]["launches"], "fp64": res["fp64"]["launches"]},
+        "gpu_launches": {"mixed": sum(x[0] for x in launches["l"]), "fp64": sum(x[1] for x in launches["l"])},
     }))
 
 
@@ -1005,8 +1064,7 @@ def main():
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.workload == "sweep":
-        if rank == 0:
-            sweep_bench(args.sweep_k, args.k_batch)
+        sweep_bench(args.sweep_k, args.k_batch, ws, rank, local)
         return
     if args.workload == "shape":
         if rank == 0:

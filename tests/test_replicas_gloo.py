@@ -68,3 +68,54 @@ def test_reference_arm_runs_on_rank_zero_only():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
                        env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def _sweep_worker(rank, ws, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
+    try:
+        sys.path.insert(0, ROOT)
+        import bench
+        ks = [16.0 + i / 30.0 for i in range(7)]
+        mine = bench.shard_wavenumbers(ks, rank, ws)
+        # per-k results a rank computes for its own wavenumbers
+        local = {"k": list(mine), "twice": [2.0 * k for k in mine]}
+        merged = bench.sweep_gather(local, ks, rank, ws)
+        out.put((rank, mine, merged))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sweep_shards_wavenumbers_and_gathers_in_order():
+    """The sweep workload on N ranks: rank r takes k_r, k_(r+N), ..., every k
+    exactly once, and the per-k results come back in the sweep's k order."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    ws = 3
+    procs = [ctx.Process(target=_sweep_worker, args=(r, ws, port, out)) for r in range(ws)]
+    for p in procs:
+        p.start()
+    try:
+        got = sorted((out.get(timeout=120) for _ in procs), key=lambda t: t[0])
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert [p.exitcode for p in procs] == [0] * ws
+    ks = [16.0 + i / 30.0 for i in range(7)]
+    shares = [mine for _, mine, _ in got]
+    assert sorted(k for sh in shares for k in sh) == ks and shares[0] == [ks[0], ks[3], ks[6]]
+    for _, _, merged in got:
+        assert merged["k"] == ks and merged["twice"] == [2.0 * k for k in ks]
+
+
+def test_sweep_gather_on_one_rank_is_the_identity():
+    sys.path.insert(0, ROOT)
+    import bench
+    ks = [1.0, 2.0, 3.0]
+    assert bench.shard_wavenumbers(ks, 0, 1) == ks
+    assert bench.sweep_gather({"x": [5, 6, 7]}, ks, 0, 1) == {"x": [5, 6, 7]}
