@@ -348,7 +348,7 @@ def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5
     core.kill()
 
 
-def profile_lu(n: int):
+def profile_lu(n: int, lu_update: int = 0):
     """Six tile-pivoted FP32 factorisations of one random complex n x n matrix
     shifted by 40 I (seed 0), each timed with CUDA events (the command the LU
     kernel summaries under profiles/ were captured with)."""
@@ -357,6 +357,9 @@ def profile_lu(n: int):
     torch.manual_seed(0)
     A = (torch.randn(n, n, dtype=torch.complex64, device="cuda") + 40 * torch.eye(n, device="cuda")).contiguous()
     eng = Engine()
+    if lu_update:
+        from bem_b200 import _lib as L
+        eng.set_tuning(L.TUNE_LU_UPDATE, lu_update)
     ts = []
     for _ in range(6):
         LU = A.clone()
@@ -1038,6 +1041,8 @@ def main():
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
     ap.add_argument("--calderon-group", type=int, default=0,
                     help="form of the fused Calderon sweep in --profile-step (the BEM_TUNE_CALDERON_GROUP value)")
+    ap.add_argument("--lu-update", type=int, default=0,
+                    help="form of the tile LU's large trailing updates in --profile-lu (BEM_TUNE_LU_UPDATE value)")
     ap.add_argument("--profile-lu", type=int, default=0,
                     help="time six tiled FP32 factorisations of a random complex matrix of this size and exit")
     ap.add_argument("--workload", default="transmission_s5",
@@ -1082,7 +1087,7 @@ def main():
         profile_step(args.profile_step, args.workload, args.trans_subdiv, args.calderon_group)
         return
     if args.profile_lu:
-        profile_lu(args.profile_lu)
+        profile_lu(args.profile_lu, args.lu_update)
         return
 
     if args.workload == "dirichlet_s4":

@@ -122,13 +122,18 @@ int64_t bem_launch_count(const bem_ctx* ctx);
  *                            Cholesky updates: 1 one CTA per 128 x 128 tile
  *                            (eight epilogue warps), 2 CTA pairs (tcgen05
  *                            cta_group::2) on 256 x 128 tiles, column order,
- *                            3 one CTA per tile with sixteen epilogue warps */
+ *                            3 one CTA per tile with sixteen epilogue warps
+ *   BEM_TUNE_LU_UPDATE       form of the FP32 tile LU's large trailing
+ *                            updates on the tensor cores: 1 register-staged
+ *                            operands, 2 TMA-fed persistent kernel over
+ *                            pre-split TF32 operands */
 #define BEM_TUNE_CALDERON_GROUP 0
 #define BEM_TUNE_GRAM_KSEG 1
 #define BEM_TUNE_CHOL_NB 2
 #define BEM_TUNE_GRAM_BAND 3
 #define BEM_TUNE_KBATCH_GROUP 4
 #define BEM_TUNE_GRAM_PAIR 5
+#define BEM_TUNE_LU_UPDATE 6
 #define BEM_TUNE_KEYS 8
 int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value);
 

@@ -46,6 +46,7 @@ TUNE_CHOL_NB = 2  # BEM_TUNE_CHOL_NB
 TUNE_GRAM_BAND = 3  # BEM_TUNE_GRAM_BAND
 TUNE_KBATCH_GROUP = 4  # BEM_TUNE_KBATCH_GROUP
 TUNE_GRAM_PAIR = 5  # BEM_TUNE_GRAM_PAIR
+TUNE_LU_UPDATE = 6  # BEM_TUNE_LU_UPDATE
 MAX_KBATCH = 64  # BEM_MAX_KBATCH
 
 

@@ -25,7 +25,7 @@ from . import _lib as L
 CACHE_ENV = "BEM_B200_TUNING_CACHE"
 KEY_NAMES = {L.TUNE_CALDERON_GROUP: "calderon_group", L.TUNE_GRAM_KSEG: "gram_kseg", L.TUNE_CHOL_NB: "chol_nb",
              L.TUNE_GRAM_BAND: "gram_band", L.TUNE_KBATCH_GROUP: "kbatch_group",
-             L.TUNE_GRAM_PAIR: "gram_pair"}
+             L.TUNE_GRAM_PAIR: "gram_pair", L.TUNE_LU_UPDATE: "lu_update"}
 
 
 def cache_path() -> str:

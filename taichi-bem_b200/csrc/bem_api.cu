@@ -146,6 +146,8 @@ int bem_ctx_set_tuning(bem_ctx* ctx, int key, int value) {
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: calderon form must be in 1..5");
     if (key == BEM_TUNE_GRAM_PAIR && (value < 0 || value > 3))
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: normal-matrix form must be 1, 2 or 3");
+    if (key == BEM_TUNE_LU_UPDATE && (value < 0 || value > 2))
+        return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: LU update form must be 1 or 2");
     if (key == BEM_TUNE_KBATCH_GROUP && value != 0 && value != 2 && value != 4)
         return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: wavenumbers per batched launch must be 2 or 4");
     if (key == BEM_TUNE_GRAM_KSEG && value < 0) return bem_fail(ctx, BEM_ERR_INVALID, "set_tuning: negative segment");

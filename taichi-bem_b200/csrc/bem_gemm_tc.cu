@@ -30,8 +30,12 @@
 // strip) split K over up to four CTAs per tile (gridDim.z); each adds its
 // partial product to C with FP32 atomics instead of the read-ahead
 // read-modify-write.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 
 #include "bem_gemm.cuh"
 
@@ -350,6 +354,268 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
                      : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed persistent form of the same update (BEM_TUNE_LU_UPDATE = 2).  The
+// operands are split once per update into TF32 hi / lo arrays in the K-major
+// layout the MMA reads: A's real view (m x 2k floats, its rows as they lie)
+// and the real expansion of B transposed, T_B[2q + b][2kk + a] =
+// [[re, im], [-im, re]][a][b] of B[kk][q], so that A T_B^T is the interleaved
+// complex product (lu_split_a_kernel, lu_split_b_kernel; zero padding to
+// whole 128 x 32 tiles).  One persistent kernel then runs over the C tiles:
+// warp 0 loads the four 128 x 32 FP32 tiles of a K stage by TMA
+// (cp.async.bulk.tensor, 128-byte swizzle, three stages of 64 KB) on an
+// mbarrier ring, warp 1 issues three kind::tf32 MMAs per K = 8 step into one
+// of two TMEM accumulators, and four epilogue warps move a finished tile out
+// of TMEM, release it to the MMAs and subtract it from C, while the MMAs of
+// the next tile run.  Every wait is bounded.  The tensor maps cover this
+// GPU's memory only and no load uses cluster multicast.
+// ---------------------------------------------------------------------------
+constexpr int LT_BK = 32;                   // floats per K stage: 128 bytes, one swizzle span
+constexpr int LT_TILE = TC_BM * LT_BK * 4;  // 16 KB
+constexpr int LT_STAGE = 4 * LT_TILE;       // A_hi, A_lo, B_hi, B_lo
+constexpr int LT_STAGES = 3;
+constexpr int LT_EPI_WARPS = 4;
+constexpr int LT_THREADS = 64 + 32 * LT_EPI_WARPS;
+constexpr uint32_t LT_TMEM_COLS = 256;  // two accumulators of 128 columns
+constexpr size_t LT_SMEM = (size_t)LT_STAGES * LT_STAGE + 1024;
+
+__device__ __forceinline__ uint64_t lt_desc_sw128(uint32_t saddr) {
+    uint64_t dsc = 0;
+    dsc |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    dsc |= (uint64_t)1 << 16;             // leading byte offset (unused by swizzled K-major layouts)
+    dsc |= (uint64_t)(1024u >> 4) << 32;  // stride byte offset: 8 rows of 128 bytes
+    dsc |= (uint64_t)1 << 46;             // descriptor version
+    dsc |= (uint64_t)2 << 61;             // SWIZZLE_128B
+    return dsc;
+}
+
+__device__ __forceinline__ void lt_tma_load(uint32_t dst, const CUtensorMap* map, uint32_t mbar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(mbar), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ bool lt_wait(uint32_t addr, uint32_t parity, volatile int* abort) {
+    for (uint32_t it = 0; it < TC_SPIN_CAP; ++it) {
+        if (mbar_try(addr, parity)) return true;
+        if ((it & 1023u) == 1023u && *abort) return false;
+    }
+    return false;
+}
+
+// A (m rows of kr floats, row stride ldf) -> hi / lo [Mp x Kp]
+__global__ void lu_split_a_kernel(const float* __restrict__ A, int64_t ldf, int m, int kr, float* hi, float* lo,
+                                  int Kp, int64_t total) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int r = (int)(i / Kp), c = (int)(i - (int64_t)r * Kp);
+    const float x = (r < m && c < kr) ? A[(int64_t)r * ldf + c] : 0.0f;
+    float h, l;
+    split_tf32(x, h, l);
+    hi[i] = h;
+    lo[i] = l;
+}
+
+// B (k x n, row stride ldf floats; complex interleaved when cplx) -> the rows
+// of T_B (one per real column of C) over the real K index, hi / lo [Np x Kp]
+__global__ void lu_split_b_kernel(const float* __restrict__ B, int64_t ldf, int k, int n, int cplx, float* hi,
+                                  float* lo, int Kp, int64_t total) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int qq = (int)(i / Kp), kk2 = (int)(i - (int64_t)qq * Kp);
+    float x = 0.0f;
+    if (cplx) {
+        const int q = qq >> 1, b = qq & 1, kk = kk2 >> 1, a = kk2 & 1;
+        if (q < n && kk < k) {
+            const float re = B[(int64_t)kk * ldf + 2 * q], im = B[(int64_t)kk * ldf + 2 * q + 1];
+            x = a == 0 ? (b == 0 ? re : im) : (b == 0 ? -im : re);
+        }
+    } else if (qq < n && kk2 < k) {
+        x = B[(int64_t)kk2 * ldf + qq];
+    }
+    float h, l;
+    split_tf32(x, h, l);
+    hi[i] = h;
+    lo[i] = l;
+}
+
+__global__ void __launch_bounds__(LT_THREADS, 1) lu_tc_kernel(const __grid_constant__ CUtensorMap ta_hi,
+                                                              const __grid_constant__ CUtensorMap ta_lo,
+                                                              const __grid_constant__ CUtensorMap tb_hi,
+                                                              const __grid_constant__ CUtensorMap tb_lo,
+                                                              int nchunks, int tiles_m, int ntiles, float* C,
+                                                              int64_t ldc, int m, int n_real, int32_t* err) {
+    extern __shared__ unsigned char lt_smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[LT_STAGES], empty_bar[LT_STAGES], acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int s_abort;
+    __shared__ float s_stg[LT_EPI_WARPS][32][33];  // epilogue staging, 32 rows x 32 columns per warp
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(lt_smem_raw) + 1023) &
+                                                           ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(LT_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < LT_STAGES; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full_bar[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&empty_bar[s])) : "memory");
+        }
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&acc_full[b])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_empty[b])),
+                         "r"(LT_EPI_WARPS)
+                         : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0) {
+        // ---- TMA producer ----
+        if (lane == 0) {
+            uint32_t cg = 0;
+            for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
+                const int ti = t % tiles_m, tj = t / tiles_m;
+                for (int c = 0; c < nchunks; ++c, ++cg) {
+                    const int s = (int)(cg % LT_STAGES);
+                    if (cg >= LT_STAGES &&
+                        !lt_wait(smem_addr(&empty_bar[s]), (uint32_t)((cg / LT_STAGES - 1) & 1), &s_abort)) {
+                        s_abort = 1;
+                        break;
+                    }
+                    const uint32_t fb = smem_addr(&full_bar[s]);
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(LT_STAGE)
+                                 : "memory");
+                    const uint32_t st = smem_addr(smem + (size_t)s * LT_STAGE);
+                    const int x = c * LT_BK;
+                    lt_tma_load(st, &ta_hi, fb, x, ti * TC_BM);
+                    lt_tma_load(st + LT_TILE, &ta_lo, fb, x, ti * TC_BM);
+                    lt_tma_load(st + 2 * LT_TILE, &tb_hi, fb, x, tj * TC_BN);
+                    lt_tma_load(st + 3 * LT_TILE, &tb_lo, fb, x, tj * TC_BN);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer: one accumulator per tile, two alternating ----
+        if (lane == 0) {
+            uint32_t cg = 0, gg = 0;
+            for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x, ++gg) {
+                const int buf = (int)(gg & 1);
+                if (gg >= 2 && !lt_wait(smem_addr(&acc_empty[buf]), (uint32_t)((gg / 2 - 1) & 1), &s_abort)) {
+                    s_abort = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(buf * TC_BN);
+                for (int c = 0; c < nchunks; ++c, ++cg) {
+                    const int s = (int)(cg % LT_STAGES);
+                    if (!lt_wait(smem_addr(&full_bar[s]), (uint32_t)((cg / LT_STAGES) & 1), &s_abort)) {
+                        s_abort = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t st = smem_addr(smem + (size_t)s * LT_STAGE);
+#pragma unroll
+                    for (int ks = 0; ks < LT_BK / 8; ++ks) {
+                        const uint32_t ko = 32u * ks;  // 8 floats
+                        const uint64_t a_hi = lt_desc_sw128(st + ko), a_lo = lt_desc_sw128(st + LT_TILE + ko);
+                        const uint64_t b_hi = lt_desc_sw128(st + 2 * LT_TILE + ko),
+                                       b_lo = lt_desc_sw128(st + 3 * LT_TILE + ko);
+                        mma_tf32(d, a_hi, b_hi, (c == 0 && ks == 0) ? 0u : 1u);
+                        mma_tf32(d, a_hi, b_lo, 1u);
+                        mma_tf32(d, a_lo, b_hi, 1u);
+                    }
+                    asm volatile(
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                            smem_addr(&empty_bar[s]))
+                        : "memory");
+                }
+                if (s_abort) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_addr(&acc_full[buf]))
+                             : "memory");
+            }
+        }
+    } else {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. ----
+        const int q = warp & 3;
+        uint32_t gg = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++gg) {
+            const int ti = t % tiles_m, tj = t / tiles_m;
+            const int buf = (int)(gg & 1);
+            const bool got = lt_wait(smem_addr(&acc_full[buf]), (uint32_t)((gg / 2) & 1), &s_abort);
+            if (!__all_sync(0xffffffffu, got)) {
+                s_abort = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float v[TC_BN];
+            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * TC_BN);
+#pragma unroll
+            for (int cc = 0; cc < TC_BN; cc += 32) {
+                uint32_t u[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]),
+                      "=r"(u[8]), "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]),
+                      "=r"(u[15]), "=r"(u[16]), "=r"(u[17]), "=r"(u[18]), "=r"(u[19]), "=r"(u[20]), "=r"(u[21]),
+                      "=r"(u[22]), "=r"(u[23]), "=r"(u[24]), "=r"(u[25]), "=r"(u[26]), "=r"(u[27]), "=r"(u[28]),
+                      "=r"(u[29]), "=r"(u[30]), "=r"(u[31])
+                    : "r"(base + (uint32_t)cc)
+                    : "memory");
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[cc + i] = __uint_as_float(u[i]);
+            }
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&acc_empty[buf])) : "memory");
+            // C -= tile, 32 columns at a time through shared memory, so that
+            // a warp's accesses run along rows of C (lane = column)
+            const int row0 = ti * TC_BM + 32 * q;
+            float(*stg)[33] = s_stg[warp - 2];
+#pragma unroll
+            for (int cc = 0; cc < TC_BN; cc += 32) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) stg[lane][i] = v[cc + i];
+                __syncwarp();
+                const int col = tj * TC_BN + cc + lane;
+                if (col < n_real) {
+                    // all 32 old values first (independent loads in flight), then the stores
+                    float old[32];
+#pragma unroll
+                    for (int rr = 0; rr < 32; ++rr)
+                        old[rr] = row0 + rr < m ? __ldcg(C + (int64_t)(row0 + rr) * ldc + col) : 0.0f;
+#pragma unroll
+                    for (int rr = 0; rr < 32; ++rr)
+                        if (row0 + rr < m) C[(int64_t)(row0 + rr) * ldc + col] = old[rr] - stg[rr][lane];
+                }
+                __syncwarp();
+            }
+        }
+    }
+    if (s_abort && tid == 0) atomicExch(err, BEM_ERR_TIMEOUT);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(LT_TMEM_COLS)
+                     : "memory");
+}
+
 bool tc_enabled() {
     static int state = -1;
     if (state < 0) {
@@ -357,6 +623,78 @@ bool tc_enabled() {
         state = (e && e[0] == '1') ? 0 : 1;
     }
     return state == 1;
+}
+
+}  // namespace
+
+namespace {
+
+// form of the large trailing updates (BEM_TUNE_LU_UPDATE): 1 register-staged
+// gemm_tc_kernel, 2 the TMA-fed persistent lu_tc_kernel (the default: measured
+// 13.3 vs 13.4 ms for a 5120^2 complex factorisation, 50.3 vs 57.1 ms at 10240^2)
+constexpr int LU_UPDATE_DEFAULT = 2;
+
+PFN_cuTensorMapEncodeTiled_v12000 lt_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+int lu_update_tma(bem_ctx* ctx, float* C, const float* A, const float* B, int64_t m, int64_t n, int64_t k,
+                  int64_t ldf, bool cplx, cudaStream_t s) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = lt_encode();
+    if (!enc) return 1;
+    const int64_t n_real = cplx ? 2 * n : n, k_real = cplx ? 2 * k : k;
+    const int64_t Mp = (m + TC_BM - 1) / TC_BM * TC_BM, Np = (n_real + TC_BN - 1) / TC_BN * TC_BN;
+    const int64_t Kp = (k_real + LT_BK - 1) / LT_BK * LT_BK;
+    void* ws = nullptr;
+    if (int rc = bem_big_ws(ctx, sizeof(float) * 2 * (size_t)(Mp + Np) * (size_t)Kp, &ws)) return rc;
+    float* ahi = static_cast<float*>(ws);
+    float* alo = ahi + Mp * Kp;
+    float* bhi = alo + Mp * Kp;
+    float* blo = bhi + Np * Kp;
+    {
+        const int64_t ta = Mp * Kp, tb = Np * Kp;
+        lu_split_a_kernel<<<(unsigned)((ta + 255) / 256), 256, 0, s>>>(A, ldf, (int)m, (int)k_real, ahi, alo,
+                                                                       (int)Kp, ta);
+        lu_split_b_kernel<<<(unsigned)((tb + 255) / 256), 256, 0, s>>>(B, ldf, (int)k, (int)n, cplx ? 1 : 0, bhi,
+                                                                       blo, (int)Kp, tb);
+        ctx->launches += 2;
+        if (int rc = bem_check_cuda(ctx, cudaGetLastError(), "lu_split kernels")) return rc;
+    }
+    CUtensorMap tm[4];
+    float* srcs[4] = {ahi, alo, bhi, blo};
+    for (int h = 0; h < 4; ++h) {
+        cuuint64_t gdim[2] = {(cuuint64_t)Kp, (cuuint64_t)(h < 2 ? Mp : Np)};
+        cuuint64_t gstride[1] = {(cuuint64_t)Kp * sizeof(float)};
+        cuuint32_t box[2] = {(cuuint32_t)LT_BK, (cuuint32_t)TC_BM};
+        cuuint32_t estr[2] = {1, 1};
+        CUresult r = enc(&tm[h], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, srcs[h], gdim, gstride, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return bem_fail(ctx, BEM_ERR_CUDA, "lu update: cuTensorMapEncodeTiled failed");
+    }
+    const int tiles_m = (int)(Mp / TC_BM);
+    const int64_t ntiles = (int64_t)tiles_m * (Np / TC_BN);
+    if (int rc = bem_check_cuda(ctx, cudaFuncSetAttribute(lu_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          (int)LT_SMEM),
+                                "lu_tc_kernel smem"))
+        return rc;
+    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, ctx->num_sms);
+    lu_tc_kernel<<<grid, LT_THREADS, LT_SMEM, s>>>(tm[0], tm[1], tm[2], tm[3], (int)(Kp / LT_BK), tiles_m,
+                                                   (int)ntiles, C, ldf, (int)m, (int)n_real, ctx->flags + 4);
+    ctx->launches++;
+    return bem_check_cuda(ctx, cudaGetLastError(), "lu_tc_kernel");
 }
 
 }  // namespace
@@ -376,6 +714,12 @@ int bem_gemm_tc_update(bem_ctx* ctx, float* C, const float* A, const float* B, i
     // product atomically, until the grid covers the SMs.
     const int nchunks = (int)((k_real + TC_KC - 1) / TC_KC);
     const int64_t tiles = (int64_t)grid.x * grid.y;
+    const int form = ctx->tune[BEM_TUNE_LU_UPDATE] > 0 ? ctx->tune[BEM_TUNE_LU_UPDATE] : LU_UPDATE_DEFAULT;
+    if (form == 2 && tiles >= ctx->num_sms) {
+        // large updates: the TMA-fed persistent kernel (skinny ones keep split K below)
+        const int rc = lu_update_tma(ctx, C, A, B, m, n, k, ldf, cplx, s);
+        if (rc <= 0) return rc;
+    }
     int splits = 1;
     if (tiles < ctx->num_sms && nchunks >= 4)
         splits = (int)std::min<int64_t>(std::min<int64_t>(4, nchunks / 2), std::max<int64_t>(1, ctx->num_sms / tiles));

@@ -40,3 +40,30 @@ def test_tiled_fp32_lu_residual(engine, n, cplx):
     res = np.abs(L @ U - A.astype(np.complex64 if cplx else np.float32)[perm]).max() / np.abs(A).max()
     # FP32 arithmetic (TF32 x 3 on the tensor cores): a few hundred ulps at most
     assert res < 5e-5
+
+
+@pytest.mark.parametrize("n,cplx", [(1500, True), (2000, False), (1100, True)])
+def test_tma_fed_update_lu_residual(engine, n, cplx):
+    """The TMA-fed persistent trailing update (BEM_TUNE_LU_UPDATE = 2: TF32
+    hi / lo operands split once per update, 128-byte-swizzled TMA stages,
+    tcgen05 kind::tf32, TMEM double buffer) on sizes whose large updates
+    cover more C tiles than SMs: P A = L U to FP32 accuracy, as the
+    register-staged form."""
+    from bem_b200 import _lib as L
+    rng = np.random.default_rng(n + cplx)
+    A = rng.standard_normal((n, n)) + (1j * rng.standard_normal((n, n)) if cplx else 0)
+    A = A + 2 * n ** 0.5 * np.eye(n)
+    dt = torch.complex64 if cplx else torch.float32
+    res = {}
+    for form in (2, 1):
+        LU = torch.as_tensor(A, device="cuda").to(dt).contiguous()
+        engine.set_tuning(L.TUNE_LU_UPDATE, form)
+        try:
+            piv, dinv, info = engine.lu_factor_tiled(LU)
+            torch.cuda.synchronize()
+        finally:
+            engine.set_tuning(L.TUNE_LU_UPDATE, 0)
+        assert int(info.item()) == 0
+        Lm, U, perm = _unpack(LU.cpu().numpy().astype(np.complex128 if cplx else np.float64), piv.cpu().numpy())
+        res[form] = np.abs(Lm @ U - A.astype(np.complex64 if cplx else np.float32)[perm]).max() / np.abs(A).max()
+    assert res[2] < 5e-5 and res[2] < 4 * res[1] + 1e-6, res
