@@ -317,7 +317,8 @@ def phase_breakdown(b):
     return out
 
 
-def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5, calderon_group: int = 0):
+def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5, calderon_group: int = 0,
+                 gram_form: int = 0):
     """One warm-up and one timed step of the workload, nothing else (the
     command the committed ncu summaries under profiles/ were captured with):
     the Dirichlet problem on 5120 panels, or the transmission least-squares
@@ -334,9 +335,11 @@ def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5
     core = CoreManager(params)
     core.initialization(fD, fN)
     b = core._BEM_manager
+    from bem_b200 import _lib as L
     if calderon_group:
-        from bem_b200 import _lib as L
         b.engine.set_tuning(L.TUNE_CALDERON_GROUP, calderon_group)
+    if gram_form:
+        b.engine.set_tuning(L.TUNE_GRAM_PAIR, gram_form)
     b.run()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1041,6 +1044,8 @@ def main():
                     help="run one warm-up and one step of the workload and exit (for ncu captures)")
     ap.add_argument("--calderon-group", type=int, default=0,
                     help="form of the fused Calderon sweep in --profile-step (the BEM_TUNE_CALDERON_GROUP value)")
+    ap.add_argument("--gram-form", type=int, default=0,
+                    help="form of the tensor-core normal matrix in --profile-step (BEM_TUNE_GRAM_PAIR value)")
     ap.add_argument("--lu-update", type=int, default=0,
                     help="form of the tile LU's large trailing updates in --profile-lu (BEM_TUNE_LU_UPDATE value)")
     ap.add_argument("--profile-lu", type=int, default=0,
@@ -1084,7 +1089,7 @@ def main():
             disk2d_bench(args.disk_n, 5, 3.0)
         return
     if args.profile_step:
-        profile_step(args.profile_step, args.workload, args.trans_subdiv, args.calderon_group)
+        profile_step(args.profile_step, args.workload, args.trans_subdiv, args.calderon_group, args.gram_form)
         return
     if args.profile_lu:
         profile_lu(args.profile_lu, args.lu_update)

@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
 // warp 0 loads the four 128 x 32 FP32 tiles of a K stage by TMA
 // (cp.async.bulk.tensor, 128-byte swizzle, three stages of 64 KB) on an
 // mbarrier ring, warp 1 issues three kind::tf32 MMAs per K = 8 step into one
-// of two TMEM accumulators, and four epilogue warps move a finished tile out
+// of two TMEM accumulators, and sixteen epilogue warps move a finished tile out
 // of TMEM, release it to the MMAs and subtract it from C, while the MMAs of
 // the next tile run.  Every wait is bounded.  The tensor maps cover this
 // GPU's memory only and no load uses cluster multicast.
@@ -374,7 +374,8 @@ constexpr int LT_BK = 32;                   // floats per K stage: 128 bytes, on
 constexpr int LT_TILE = TC_BM * LT_BK * 4;  // 16 KB
 constexpr int LT_STAGE = 4 * LT_TILE;       // A_hi, A_lo, B_hi, B_lo
 constexpr int LT_STAGES = 3;
-constexpr int LT_EPI_WARPS = 4;
+constexpr int LT_EPI_WARPS = 16;  // four per TMEM lane quarter, 32 columns each
+constexpr int LT_SR = 8;          // rows per pass of the epilogue's shared-memory transpose
 constexpr int LT_THREADS = 64 + 32 * LT_EPI_WARPS;
 constexpr uint32_t LT_TMEM_COLS = 256;  // two accumulators of 128 columns
 constexpr size_t LT_SMEM = (size_t)LT_STAGES * LT_STAGE + 1024;
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(LT_THREADS, 1) lu_tc_kernel(const __grid_const
     __shared__ __align__(8) uint64_t full_bar[LT_STAGES], empty_bar[LT_STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int s_abort;
-    __shared__ float s_stg[LT_EPI_WARPS][32][33];  // epilogue staging, 32 rows x 32 columns per warp
+    __shared__ float s_stg[LT_EPI_WARPS][LT_SR][33];  // epilogue staging, LT_SR rows x 32 columns per warp
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(lt_smem_raw) + 1023) &
                                                            ~uintptr_t(1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -548,8 +549,9 @@ __global__ void __launch_bounds__(LT_THREADS, 1) lu_tc_kernel(const __grid_const
             }
         }
     } else {
-        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. ----
-        const int q = warp & 3;
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. and column group (w - 2) / 4 ----
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        constexpr int EC = TC_BN / (LT_EPI_WARPS / 4);
         uint32_t gg = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++gg) {
             const int ti = t % tiles_m, tj = t / tiles_m;
@@ -560,10 +562,10 @@ __global__ void __launch_bounds__(LT_THREADS, 1) lu_tc_kernel(const __grid_const
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float v[TC_BN];
-            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * TC_BN);
+            float v[EC];
+            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * TC_BN + half * EC);
 #pragma unroll
-            for (int cc = 0; cc < TC_BN; cc += 32) {
+            for (int cc = 0; cc < EC; cc += 32) {
                 uint32_t u[32];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
@@ -589,22 +591,28 @@ __global__ void __launch_bounds__(LT_THREADS, 1) lu_tc_kernel(const __grid_const
             const int row0 = ti * TC_BM + 32 * q;
             float(*stg)[33] = s_stg[warp - 2];
 #pragma unroll
-            for (int cc = 0; cc < TC_BN; cc += 32) {
+            for (int cc = 0; cc < EC; cc += 32) {
 #pragma unroll
-                for (int i = 0; i < 32; ++i) stg[lane][i] = v[cc + i];
-                __syncwarp();
-                const int col = tj * TC_BN + cc + lane;
-                if (col < n_real) {
-                    // all 32 old values first (independent loads in flight), then the stores
-                    float old[32];
+                for (int hr = 0; hr < 32 / LT_SR; ++hr) {  // rows LT_SR hr .. of the warp's 32
+                    if (lane / LT_SR == hr) {
 #pragma unroll
-                    for (int rr = 0; rr < 32; ++rr)
-                        old[rr] = row0 + rr < m ? __ldcg(C + (int64_t)(row0 + rr) * ldc + col) : 0.0f;
+                        for (int i = 0; i < 32; ++i) stg[lane % LT_SR][i] = v[cc + i];
+                    }
+                    __syncwarp();
+                    const int col = tj * TC_BN + half * EC + cc + lane;
+                    const int rb = row0 + LT_SR * hr;
+                    if (col < n_real) {
+                        // all old values first (independent loads in flight), then the stores
+                        float old[LT_SR];
 #pragma unroll
-                    for (int rr = 0; rr < 32; ++rr)
-                        if (row0 + rr < m) C[(int64_t)(row0 + rr) * ldc + col] = old[rr] - stg[rr][lane];
+                        for (int rr = 0; rr < LT_SR; ++rr)
+                            old[rr] = rb + rr < m ? __ldcg(C + (int64_t)(rb + rr) * ldc + col) : 0.0f;
+#pragma unroll
+                        for (int rr = 0; rr < LT_SR; ++rr)
+                            if (rb + rr < m) C[(int64_t)(rb + rr) * ldc + col] = old[rr] - stg[rr][lane];
+                    }
+                    __syncwarp();
                 }
-                __syncwarp();
             }
         }
     }
@@ -631,7 +639,7 @@ namespace {
 
 // form of the large trailing updates (BEM_TUNE_LU_UPDATE): 1 register-staged
 // gemm_tc_kernel, 2 the TMA-fed persistent lu_tc_kernel (the default: measured
-// 13.3 vs 13.4 ms for a 5120^2 complex factorisation, 50.3 vs 57.1 ms at 10240^2)
+// 12.1 vs 13.4 ms for a 5120^2 complex factorisation, 39.9 vs 57.1 ms at 10240^2)
 constexpr int LU_UPDATE_DEFAULT = 2;
 
 PFN_cuTensorMapEncodeTiled_v12000 lt_encode() {
