@@ -646,22 +646,22 @@ __global__ void __launch_bounds__(256) tile_solve_kernel(const T* LU, int64_t ld
                     xr1 = (T)__ldcg(&x[W * (c0 + lane + 32)]);
                     if (C) xi1 = (T)__ldcg(&x[W * (c0 + lane + 32) + 1]);
                 }
+                // all 2 RW loads of the block first, so that they are in flight
+                // together, then the products (entries outside the block are zero)
+                CE<T> la[RW], lb[RW];
 #pragma unroll
                 for (int i = 0; i < RW; ++i) {
                     const int r = wid + 8 * i;
-                    if (r < m) {
-                        const T* row = LU + W * ((int64_t)(r0 + r) * lda + c0);
-                        if (lane < mj) {
-                            const CE<T> l = ldE<T, C>(row, lane);
-                            acc_re[i] += l.re * xr0 - l.im * xi0;
-                            acc_im[i] += l.re * xi0 + l.im * xr0;
-                        }
-                        if (lane + 32 < mj) {
-                            const CE<T> l = ldE<T, C>(row, lane + 32);
-                            acc_re[i] += l.re * xr1 - l.im * xi1;
-                            acc_im[i] += l.re * xi1 + l.im * xr1;
-                        }
-                    }
+                    const T* row = LU + W * ((int64_t)(r0 + r) * lda + c0);
+                    la[i] = (r < m && lane < mj) ? ldE<T, C>(row, lane) : CE<T>{T(0), T(0)};
+                    lb[i] = (r < m && lane + 32 < mj) ? ldE<T, C>(row, lane + 32) : CE<T>{T(0), T(0)};
+                }
+#pragma unroll
+                for (int i = 0; i < RW; ++i) {
+                    acc_re[i] += la[i].re * xr0 - la[i].im * xi0;
+                    acc_im[i] += la[i].re * xi0 + la[i].im * xr0;
+                    acc_re[i] += lb[i].re * xr1 - lb[i].im * xi1;
+                    acc_im[i] += lb[i].re * xi1 + lb[i].im * xr1;
                 }
             };
             const int nstream = ndep > 0 ? ndep - 1 : 0;  // all but the critical one
