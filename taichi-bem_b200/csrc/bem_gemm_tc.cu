@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(TC_THREADS) gemm_tc_kernel(float* __restrict__
 // of two TMEM accumulators, and sixteen epilogue warps move a finished tile out
 // of TMEM, release it to the MMAs and subtract it from C, while the MMAs of
 // the next tile run.  Every wait is bounded.  The tensor maps cover this
-// GPU's memory only and no load uses cluster multicast.
+// GPU's memory only, and each TMA load fills this CTA's own shared memory.
 // ---------------------------------------------------------------------------
 constexpr int LT_BK = 32;                   // floats per K stage: 128 bytes, one swizzle span
 constexpr int LT_TILE = TC_BM * LT_BK * 4;  // 16 KB

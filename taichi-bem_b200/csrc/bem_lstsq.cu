@@ -528,15 +528,16 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1) gram_tc_kernel(const __grid_c
 //    cta_group::2 TMA form, completing bytes on the EVEN CTA's full_bar[s],
 //    where the even producer alone announces the pair's 96 KB; the even
 //    CTA's MMA thread waits on it, and its tcgen05.commit arrives on
-//    empty_bar[s] of both CTAs (multicast commit, mask 0b11);
+//    empty_bar[s] of both CTAs (one commit to the CTA mask 0b11);
 //  * accumulators: the commit after a segment arrives on acc_full of both
 //    CTAs; the eight epilogue warps of each CTA arrive on the EVEN CTA's
 //    acc_empty (count 16) after draining their TMEM;
 //  * teardown: a cluster barrier (neither CTA leaves while the other's MMAs
 //    may still read its shared memory), then both CTAs free the TMEM.
 // Tiles run in column order (the pairs of one tile column one after another,
-// the order of single-column bands, BEM_TUNE_GRAM_BAND = 1).  No load uses
-// cluster multicast; every tensor map covers this GPU's memory only.
+// the order of single-column bands, BEM_TUNE_GRAM_BAND = 1).  Each TMA load
+// fills the issuing CTA's own shared memory, and every tensor map covers this
+// GPU's memory only.
 // ---------------------------------------------------------------------------
 constexpr int G2_STAGES = 4;
 constexpr int G2_ATILE = GT_BM * GT_BK * 2;            // 16 KB: 128 x 64 FP16 rows of this CTA
