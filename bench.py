@@ -320,7 +320,7 @@ def phase_breakdown(b):
 def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5, calderon_group: int = 0,
                  gram_form: int = 0):
     """One warm-up and one timed step of the workload, nothing else (the
-    command the committed ncu summaries under profiles/ were captured with):
+    command the committed ncu summaries were captured with):
     the Dirichlet problem on 5120 panels, or the transmission least-squares
     problem on the icosphere of subdivision `subdiv` (assembly and solve)."""
     import torch
@@ -354,7 +354,7 @@ def profile_step(precision: str, workload: str = "dirichlet_s4", subdiv: int = 5
 def profile_lu(n: int, lu_update: int = 0):
     """Six tile-pivoted FP32 factorisations of one random complex n x n matrix
     shifted by 40 I (seed 0), each timed with CUDA events (the command the LU
-    kernel summaries under profiles/ were captured with)."""
+    kernel summaries were captured with)."""
     import torch
     from bem_b200.engine import Engine
     torch.manual_seed(0)
