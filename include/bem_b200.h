@@ -210,7 +210,8 @@ int bem_assemble_calderon(bem_ctx* ctx, const bem_op_desc* op, int nk, const dou
  *   out[w][row*ld+col] += scale[w] * A(k[w])(row,col)   and, when out_t and
  *   out_t[w] are not NULL, out_t[w][col*ld+row] += scale_t[w] * A(k[w])(row,col),
  * A(k) the Helmholtz operator op->op with kernel wavenumber k[w] and W mass
- * coefficient k2[w] (op->k and op->k2 are ignored).  k, k2, scale, scale_t,
+ * coefficient k2[w] (op->k and op->k2 are ignored; with op->deriv_k the
+ * kernel's k-derivative at fixed k2, as in bem_assemble).  k, k2, scale, scale_t,
  * out and out_t are host arrays of nk entries; out/out_t hold device
  * pointers to BEM_C128 blocks.  Every separate panel pair's geometry is
  * evaluated once for 2 or 4 wavenumbers (BEM_TUNE_KBATCH_GROUP); near pairs

@@ -65,6 +65,67 @@ def k_derivative_M(bm, k: float, sqrt_n: float, scope_type: int, out: torch.Tens
         bm._mat_A = saved
 
 
+def k_derivative_M_media(bm, k: float, parts):
+    """For each (sqrt_n, out, multiplier) of `parts` (the exterior and the
+    interior medium): out += multiplier * dM/dk as k_derivative_M adds it,
+    with every operator of all media assembled together by bem_assemble_batch
+    (one call per operator; the separate pairs' geometry shared by the media's
+    wavenumbers): the kernels' k-derivatives of V, K (with -K^T) and W at the
+    media's wavenumbers, and dW/dk2 as W(k2 = 1) - W(k2 = 0) at each medium's
+    wavenumber (two batched terms of opposite sign into the same block)."""
+    from .. import _lib as L
+    from ..BEM_functions.layers import _D, _N
+    uses_n = bm._kernel_type == int(KernelType.HELMHOLTZ_TRANSMISSION)
+    N, M = bm.N_Neumann, bm.M_Dirichlet
+    No, Do = bm._Neumann_offset_i, bm._Dirichlet_offset_i
+    Qn, Qd = bm.shape_func_degree_Neumann, bm.shape_func_degree_Dirichlet
+    kap, k2s, outs, m = [], [], [], []
+    dk2 = []
+    for sqrt_n, out, mult in parts:
+        d = bm.op_desc(L.OP_V, k, sqrt_n)
+        kap.append(d.k)
+        k2s.append(d.k2)
+        outs.append(out)
+        m.append(mult * (sqrt_n if uses_n else 1.0))  # multiplier x d(kernel wavenumber)/dk
+        dk2.append(mult * 2.0 * k * sqrt_n * sqrt_n)   # multiplier x d(k2)/dk
+    bm._desc_deriv_k = True
+    try:
+        desc = lambda op: bm.op_desc(op, k, parts[0][0])  # kernel, precision, quirk, deriv_k
+        if N > 0:
+            sp = bm.space("charge", Qn, "N", _N, offset=No)
+            bm.engine.assemble_batch(desc(L.OP_V), sp, sp, kap, k2s, outs, [-x for x in m])
+        if N > 0 and M > 0:
+            test = bm.space("charge", Qn, "N", _N, offset=No)
+            trial = bm.space("charge", Qd, "D", _D, offset=Do)
+            bm.engine.assemble_batch(desc(L.OP_K), test, trial, kap, k2s, outs, list(m), outs_t=outs,
+                                     scales_t=[-x for x in m])
+        if M > 0:
+            sp = bm.space("charge", Qd, "D", _D, offset=Do)
+            bm.engine.assemble_batch(desc(L.OP_W), sp, sp, kap, k2s, outs, [-x for x in m])
+    finally:
+        bm._desc_deriv_k = False
+    if M > 0:
+        sp = bm.space("charge", Qd, "D", _D, offset=Do)
+        kk, kk2, oo, sc = [], [], [], []
+        for w, out in enumerate(outs):
+            # M's DD block is -W: out_DD += -dk2 (W(1) - W(0))
+            kk += [kap[w], kap[w]]
+            kk2 += [1.0, 0.0]
+            oo += [out, out]
+            sc += [-dk2[w], dk2[w]]
+        bm.engine.assemble_batch(desc_plain(bm, L.OP_W, k, parts[0][0]), sp, sp, kk, kk2, oo, sc)
+
+
+def desc_plain(bm, op, k, sqrt_n):
+    """The manager's operator descriptor without the k-derivative."""
+    saved = bm._desc_deriv_k
+    bm._desc_deriv_k = False
+    try:
+        return bm.op_desc(op, k, sqrt_n)
+    finally:
+        bm._desc_deriv_k = saved
+
+
 def _data_k_derivative(bm, data):
     """d f / dk of the transmission data vector f (rhs_constructor's
     _f_boundary) from the data object's analytic derivatives; f itself is
@@ -145,9 +206,8 @@ def solution_norm_k_gradient(bm, data, check: bool = True, delta: float = 1e-3):
     t1a = time.perf_counter()
     # the operators' derivatives: dP-_o = -dM_o (exterior), dP+_i = dM_i (interior)
     dPm = torch.zeros(n, n, dtype=A.dtype, device=A.device)
-    k_derivative_M(bm, k0, bm._sqrt_no, int(ScopeType.EXTERIOR), dPm, -1.0)
     dP = torch.zeros_like(dPm)
-    k_derivative_M(bm, k0, bm._sqrt_ni, int(ScopeType.INTERIOR), dP, 1.0)
+    k_derivative_M_media(bm, k0, [(bm._sqrt_no, dPm, -1.0), (bm._sqrt_ni, dP, 1.0)])
     # b = P-_o conj(f) (the reference's rhs, BEM_manager.py:647-662), P-_o = A - P
     df = _data_k_derivative(bm, data)
     fc = f.conj().resolve_conj() if bm.conj_data else f

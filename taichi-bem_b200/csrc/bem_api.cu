@@ -405,7 +405,7 @@ int bem_assemble_batch(bem_ctx* ctx, const bem_op_desc* op, const bem_space* tes
                        const double* scale, void* const* out_t, const double* scale_t, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
     if (ctx->nt == 0) return bem_fail(ctx, BEM_ERR_NOMESH, "no mesh set");
-    if (int rc = check_op(ctx, op, false)) return rc;
+    if (int rc = check_op(ctx, op, true)) return rc;
     if (ctx->dim != 3 || op->kernel != BEM_KERNEL_HELMHOLTZ)
         return bem_fail(ctx, BEM_ERR_INVALID, "bem_assemble_batch takes the 3D Helmholtz kernel");
     if (int rc = check_space(ctx, test, "test")) return rc;

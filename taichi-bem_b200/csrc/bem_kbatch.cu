@@ -41,6 +41,7 @@ struct KbArgs {
     const void* phi;
     const double* phi64;
     int Q2;
+    int dk;  // 1: the kernel's k-derivative at fixed k2 (as bem_assemble's deriv_k)
     int64_t ld;
     double k[KB_MAX], k2[KB_MAX], scale[KB_MAX], scale_t[KB_MAX];
     double* out[KB_MAX];    // nullptr: padding slot, evaluated but not written
@@ -49,17 +50,23 @@ struct KbArgs {
 
 // Helmholtz kernel value (without 1/(4 pi)) at one wavenumber from the
 // k-independent quantities of a point pair: rinv = 1/r, t = d.n / r^3 (K, K'),
-// ph = the phase argument (r - R in the FP32 pair frame, r in FP64).
+// ph = the phase argument (r - R in the FP32 pair frame, r in FP64).  With
+// dk the kernel's k-derivative: i e^{ikr} for V and W, k (d.n) e^{ikr} / r
+// for K and K' (d.n / r = t r^2).
 template <int OP, typename T>
-__device__ __forceinline__ void kb_value(T rinv, T r, T t, T ph, T k, bool small, T& re, T& im) {
+__device__ __forceinline__ void kb_value(T rinv, T r, T t, T ph, T k, bool small, bool dk, T& re, T& im) {
     T s, c;
     if constexpr (sizeof(T) == 4)
         dev_sincos_phase(k * ph, small, &s, &c);
     else
         dev_sincos(k * ph, &s, &c);
     if (OP == BEM_OP_V || OP == BEM_OP_W) {
-        re = rinv * c;
-        im = rinv * s;
+        re = dk ? -s : rinv * c;
+        im = dk ? c : rinv * s;
+    } else if (dk) {
+        const T f = t * k * r * r;
+        re = f * c;
+        im = f * s;
     } else {
         const T kr = k * r;
         re = t * fma(kr, s, c);
@@ -122,6 +129,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kbatch_kernel(KbArgs a) {
 #pragma unroll
     for (int w = 0; w < NKB; ++w) kk[w] = T(a.k[w]);
     const bool small = a.small_phase != 0;
+    const bool dk = a.dk != 0;
 
     for (int t = 0; t < FAR_TI; ++t) {
         const int li = li0 + t;
@@ -210,7 +218,7 @@ __global__ void __launch_bounds__(FAR_THREADS) far_kbatch_kernel(KbArgs a) {
 #pragma unroll
                     for (int w = 0; w < NKB; ++w) {
                         T re, im;
-                        kb_value<OP, T>(rinv, r, tt, ph, kk[w], small, re, im);
+                        kb_value<OP, T>(rinv, r, tt, ph, kk[w], small, dk, re, im);
                         if (W_OP) {
                             c_re[w] += xa.w * re;
                             c_im[w] += xa.w * im;
@@ -355,6 +363,7 @@ int bem_launch_assemble_batch(bem_ctx* ctx, const bem_op_desc* op, const bem_spa
     a.phi = fp32 ? (const void*)ctx->phi32 : (const void*)ctx->phi64;
     a.phi64 = ctx->phi64;
     a.Q2 = ctx->Q2;
+    a.dk = op->deriv_k ? 1 : 0;
     a.ld = ld;
     if (a.n_test > 0 && a.n_trial > 0) {
         for (int w0 = 0; w0 < nk; w0 += group) {
