@@ -310,7 +310,10 @@ int bem_gemv(bem_ctx* ctx, int a_dtype, const void* A, int64_t m, int64_t n, int
  * 2 x float / 2 x double per element).  No grid-wide synchronisation. */
 int64_t bem_lu_dinv_elems(int64_t n);
 /* The factorisation (replaces the factor half of torch.linalg.solve,
- * BEM_manager.py:1056).  Queued without synchronisation.  A tensor-core wait
+ * BEM_manager.py:1056).  Queued without synchronisation, except that the
+ * first factorisation of a size may grow the context's workspace for the
+ * split operands of its large trailing updates (BEM_TUNE_LU_UPDATE = 2, a
+ * device synchronisation).  A tensor-core wait
  * of the trailing updates
  * that ran out of its iteration cap is reported (BEM_ERR_TIMEOUT) by the next
  * bem_lu_solve_tiled, bem_refine_solve or bem_lu_factor_status on the same
